@@ -1,0 +1,1134 @@
+// Graph algorithms on the B2SR primitives with all state on the device.
+//
+// The reference loops (algorithm/bfs.cu:508-564, sssp.cu:420-470,
+// pr.cu:449-513, cc.cu:223-287) launch 5-9 kernels per iteration and copy a
+// convergence scalar to the host every iteration.  Here each iteration is one
+// fused BMV kernel over the balanced work items plus a small kernel that
+// finishes split block rows; the last block of that kernel (atomic ticket)
+// decides termination on the device.  K iterations are captured once into a
+// CUDA graph (every kernel exits at once when the device "done" flag is set)
+// and the host replays the graph, reading the flag from pinned memory once
+// per replay instead of once per iteration.
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "bmv.cuh"
+
+namespace gbo {
+
+// Loop control word in device memory.
+struct Ctrl {
+  int iter;       // iterations completed
+  int done;       // 1 once the loop has terminated
+  unsigned ticket;
+  int max_iter;
+  unsigned long long count;  // vertices changed in the current iteration
+  double err;                // error accumulator of the current iteration
+  double last_err;           // error of the last finished iteration
+  float tol;
+  float alpha;
+  float add;      // constant added to each PageRank entry
+  float add_scale;  // PPR: add_scale * v[i] added as well
+  int norm;       // 1 = L1, 2 = L2 error
+  int n;
+};
+
+}  // namespace gbo
+
+// Per-graph algorithm state (global scope: gbo_graph::algo is ::AlgoState*).
+struct AlgoState {
+  cudaStream_t cap = nullptr;  // capture stream
+  gbo::Ctrl* ctrl = nullptr;
+  gbo::Ctrl* h_ctrl = nullptr;  // pinned mirror
+  // BFS / SSSP
+  void* front = nullptr;   // 2 * nbr words (8 bytes each max)
+  void* visited = nullptr; // nbr words
+  int* level = nullptr;    // n
+  uint32_t* dist = nullptr;
+  // PR / PPR / CC vectors
+  float* pr = nullptr;     // 2 * n
+  const float* ppr_v = nullptr;
+  int* f = nullptr;
+  int* gf = nullptr;
+  int* mngf = nullptr;
+  double* acc64 = nullptr;  // PPR adjoint scatter accumulator
+  void* scratch = nullptr;  // split partials (nslots * b * 8 bytes)
+  cudaGraphExec_t exec[8] = {};
+  const void* exec_key[8] = {};
+  // events recorded around the main kernel of every captured iteration
+  cudaEvent_t ev[16] = {};
+  int ev_ready = 0;
+  // statistics of the last algorithm run
+  std::vector<float> step_ms;
+  int replays = 0;
+  long long launches = 0;
+  int launches_per_replay = 0;
+};
+
+namespace gbo {
+
+namespace {
+
+constexpr int kTPB = 256;
+constexpr int kStepsPerGraph = 8;
+
+enum AlgoId { A_BFS = 0, A_SSSP = 1, A_PR = 2, A_CC = 3, A_PPR_F = 4, A_PPR_B = 5 };
+
+template <int B>
+struct Lay {
+  static constexpr int W = B >= 32 ? 32 : B;
+  static constexpr int G = 32 / W;
+  static constexpr int RPL = B > 32 ? 2 : 1;
+};
+
+template <int B>
+__device__ __forceinline__ typename Word<B>::T full_word() {
+  using WT = typename Word<B>::T;
+  return (WT)((WT)~(WT)0 >> (sizeof(WT) * 8 - B));
+}
+
+template <int B>
+__device__ __forceinline__ bool bit_of(typename Word<B>::T w, int r) {
+  return (w >> (B - 1 - r)) & 1;
+}
+
+template <int B>
+__device__ __forceinline__ typename Word<B>::T gather_bits(bool p0, bool p1, unsigned lane) {
+  using L = Lay<B>;
+  if (L::RPL == 2) {
+    unsigned lo = __ballot_sync(0xffffffffu, p0);
+    unsigned hi = __ballot_sync(0xffffffffu, p1);
+    return (typename Word<B>::T)__brevll(((unsigned long long)hi << 32) | lo);
+  } else {
+    unsigned bal = __ballot_sync(0xffffffffu, p0);
+    unsigned g = lane / L::W;
+    unsigned seg = (bal >> (g * L::W)) & seg_mask<B>();
+    return (typename Word<B>::T)(__brev(seg) >> (32 - (B < 32 ? B : 32)));
+  }
+}
+
+template <int B, typename F>
+__device__ __forceinline__ void for_each_col(typename Word<B>::T w, F&& f) {
+  unsigned long long a = (unsigned long long)w << (64 - B);
+  while (a) {
+    int j = __clzll(a);
+    f(j);
+    a &= ~(0x8000000000000000ull >> j);
+  }
+}
+
+__device__ __forceinline__ long long item_index(unsigned lane, int W, int G) {
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  return warp * G + lane / W;
+}
+
+// Block-wide sum of `v` added to *dst once per block.
+__device__ __forceinline__ void block_add_u64(unsigned long long v, unsigned long long* dst) {
+  __shared__ unsigned long long sh;
+  if (threadIdx.x == 0) sh = 0;
+  __syncthreads();
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(&sh, v);
+  __syncthreads();
+  if (threadIdx.x == 0 && sh) atomicAdd(dst, sh);
+}
+
+__device__ __forceinline__ void block_add_f64(double v, double* dst) {
+  __shared__ double sh;
+  if (threadIdx.x == 0) sh = 0;
+  __syncthreads();
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(&sh, v);
+  __syncthreads();
+  if (threadIdx.x == 0 && sh != 0.0) atomicAdd(dst, sh);
+}
+
+// Called by every block of an iteration's last kernel after its work: the
+// last block to arrive closes the iteration.  No waiting: the ticket only
+// counts arrivals.
+template <typename Decide>
+__device__ __forceinline__ void close_iteration(Ctrl* ctrl, Decide decide) {
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned t = atomicAdd(&ctrl->ticket, 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    volatile Ctrl* c = ctrl;
+    const int it = c->iter + 1;
+    const bool stop = decide(c, it);
+    c->iter = it;
+    c->last_err = c->err;
+    c->err = 0.0;
+    c->count = 0ull;
+    c->ticket = 0u;
+    if (stop) c->done = 1;
+    __threadfence();
+  }
+}
+
+// ============================================================== BFS
+template <int B>
+__global__ void __launch_bounds__(kTPB) k_bfs_step(GView v, typename Word<B>::T* __restrict__ front,
+                                                   typename Word<B>::T* __restrict__ visited,
+                                                   int* __restrict__ level, Ctrl* __restrict__ ctrl,
+                                                   typename Word<B>::T* __restrict__ scratch) {
+  using WT = typename Word<B>::T;
+  using L = Lay<B>;
+  if (((volatile Ctrl*)ctrl)->done) return;
+  const int lvl = ((volatile Ctrl*)ctrl)->iter;
+  const WT* __restrict__ x = front + (size_t)(lvl & 1) * v.nbr;
+  WT* __restrict__ out = front + (size_t)((lvl + 1) & 1) * v.nbr;
+  const unsigned lane = threadIdx.x & 31;
+  const long long item = item_index(lane, L::W, L::G);
+  const bool active = item < v.nitems;
+  const int r = lane % L::W;
+  gbo_item it = active ? v.items[item] : gbo_item{0, 0, 0, -2};
+  const WT full = full_word<B>();
+  const WT vis = active ? visited[it.row] : full;
+  bool p0 = false, p1 = false;
+  if (active && (vis & full) != full) {
+    const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
+    const bool need0 = !bit_of<B>(vis, r);
+    const bool need1 = L::RPL == 2 && !bit_of<B>(vis, r + 32);
+    for (int t = it.t0; t < it.t1; ++t) {
+      const WT xs = x[v.colind[t]];
+      if (xs) {
+        if (need0 && !p0) p0 = (val[(size_t)t * B + r] & xs) != 0;
+        if (need1 && !p1) p1 = (val[(size_t)t * B + 32 + r] & xs) != 0;
+      }
+    }
+  }
+  const WT word = gather_bits<B>(p0, p1, lane);
+  unsigned long long cnt = 0;
+  if (active) {
+    if (it.slot >= 0) {
+      if (r == 0) scratch[it.slot] = word;
+    } else {
+      const WT nw = (WT)(word & ~vis & full);
+      const long long row0 = (long long)it.row * B + r;
+      if (bit_of<B>(nw, r) && row0 < v.nrows) level[row0] = lvl + 1;
+      if (L::RPL == 2 && bit_of<B>(nw, r + 32) && row0 + 32 < v.nrows) level[row0 + 32] = lvl + 1;
+      if (r == 0) {
+        out[it.row] = nw;
+        if (nw) visited[it.row] = (WT)(vis | nw);
+        cnt = popc_w(nw);
+      }
+    }
+  }
+  block_add_u64(cnt, &ctrl->count);
+}
+
+template <int B>
+__global__ void k_bfs_finish(GView v, typename Word<B>::T* __restrict__ front,
+                             typename Word<B>::T* __restrict__ visited, int* __restrict__ level,
+                             Ctrl* __restrict__ ctrl, const typename Word<B>::T* __restrict__ scratch) {
+  using WT = typename Word<B>::T;
+  if (((volatile Ctrl*)ctrl)->done) return;
+  const int lvl = ((volatile Ctrl*)ctrl)->iter;
+  WT* __restrict__ out = front + (size_t)((lvl + 1) & 1) * v.nbr;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long cnt = 0;
+  if (i < v.nsplit) {
+    const gbo_split sp = v.splits[i];
+    const WT full = full_word<B>();
+    const WT vis = visited[sp.row];
+    WT w = 0;
+    if ((vis & full) != full)
+      for (int q = 0; q < sp.nslots; ++q) w |= scratch[sp.slot0 + q];
+    const WT nw = (WT)(w & ~vis & full);
+    out[sp.row] = nw;
+    if (nw) {
+      visited[sp.row] = (WT)(vis | nw);
+      for (int r = 0; r < B; ++r) {
+        long long row = (long long)sp.row * B + r;
+        if (bit_of<B>(nw, r) && row < v.nrows) level[row] = lvl + 1;
+      }
+      cnt = popc_w(nw);
+    }
+  }
+  block_add_u64(cnt, &ctrl->count);
+  close_iteration(ctrl, [](volatile Ctrl* c, int it) {
+    return c->count == 0ull || it >= c->max_iter;
+  });
+}
+
+template <int B>
+__global__ void k_bfs_init(typename Word<B>::T* front, typename Word<B>::T* visited, int* level,
+                           int nbr, int n, int src, Ctrl* ctrl, int max_iter) {
+  using WT = typename Word<B>::T;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long k = i; k < n; k += stride) level[k] = (k == src) ? 0 : -1;
+  for (long long k = i; k < nbr; k += stride) {
+    WT w = (k == src / B) ? (WT)((WT)1 << (B - 1 - src % B)) : (WT)0;
+    front[k] = w;
+    front[nbr + k] = 0;
+    visited[k] = w;
+  }
+  if (i == 0) {
+    ctrl->iter = 0;
+    ctrl->done = 0;
+    ctrl->ticket = 0;
+    ctrl->max_iter = max_iter;
+    ctrl->count = 0;
+    ctrl->err = 0;
+    ctrl->last_err = 0;
+  }
+}
+
+// ============================================================= SSSP
+// Min-plus relaxation from the frontier: d'[i] = min over frontier
+// neighbours j of d[j] + 1, kept where it improves d[i].
+template <int B>
+__global__ void __launch_bounds__(kTPB) k_sssp_step(GView v, typename Word<B>::T* __restrict__ front,
+                                                    typename Word<B>::T* __restrict__ visited,
+                                                    uint32_t* __restrict__ dist, Ctrl* __restrict__ ctrl,
+                                                    uint32_t* __restrict__ scratch) {
+  using WT = typename Word<B>::T;
+  using L = Lay<B>;
+  if (((volatile Ctrl*)ctrl)->done) return;
+  const int lvl = ((volatile Ctrl*)ctrl)->iter;
+  const WT* __restrict__ x = front + (size_t)(lvl & 1) * v.nbr;
+  WT* __restrict__ out = front + (size_t)((lvl + 1) & 1) * v.nbr;
+  const unsigned lane = threadIdx.x & 31;
+  const long long item = item_index(lane, L::W, L::G);
+  const bool active = item < v.nitems;
+  const int r = lane % L::W;
+  gbo_item it = active ? v.items[item] : gbo_item{0, 0, 0, -2};
+  const WT full = full_word<B>();
+  const WT vis = active ? visited[it.row] : full;
+  uint32_t a0 = (uint32_t)kINF, a1 = (uint32_t)kINF;
+  if (active && (vis & full) != full) {
+    const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
+    for (int t = it.t0; t < it.t1; ++t) {
+      const int c = v.colind[t];
+      const WT xs = x[c];
+      if (xs) {
+        const long long base = (long long)c * B;
+        const WT m0 = val[(size_t)t * B + r] & xs;
+        for_each_col<B>(m0, [&](int j) {
+          uint32_t d = dist[base + j];
+          a0 = min(a0, d >= (uint32_t)kINF ? (uint32_t)kINF : d + 1u);
+        });
+        if (L::RPL == 2) {
+          const WT m1 = val[(size_t)t * B + 32 + r] & xs;
+          for_each_col<B>(m1, [&](int j) {
+            uint32_t d = dist[base + j];
+            a1 = min(a1, d >= (uint32_t)kINF ? (uint32_t)kINF : d + 1u);
+          });
+        }
+      }
+    }
+  }
+  const long long row0 = (long long)it.row * B + r;
+  bool n0 = false, n1 = false;
+  if (active && it.slot < 0) {
+    if (row0 < v.nrows && a0 < dist[row0]) { dist[row0] = a0; n0 = true; }
+    if (L::RPL == 2 && row0 + 32 < v.nrows && a1 < dist[row0 + 32]) { dist[row0 + 32] = a1; n1 = true; }
+  }
+  const WT word = gather_bits<B>(n0, n1, lane);
+  unsigned long long cnt = 0;
+  if (active) {
+    if (it.slot >= 0) {
+      scratch[(size_t)it.slot * B + r] = a0;
+      if (L::RPL == 2) scratch[(size_t)it.slot * B + 32 + r] = a1;
+    } else if (r == 0) {
+      out[it.row] = word;
+      if (word) visited[it.row] = (WT)(vis | word);
+      cnt = popc_w(word);
+    }
+  }
+  block_add_u64(cnt, &ctrl->count);
+}
+
+template <int B>
+__global__ void k_sssp_finish(GView v, typename Word<B>::T* __restrict__ front,
+                              typename Word<B>::T* __restrict__ visited, uint32_t* __restrict__ dist,
+                              Ctrl* __restrict__ ctrl, const uint32_t* __restrict__ scratch) {
+  using WT = typename Word<B>::T;
+  if (((volatile Ctrl*)ctrl)->done) return;
+  const int lvl = ((volatile Ctrl*)ctrl)->iter;
+  WT* __restrict__ out = front + (size_t)((lvl + 1) & 1) * v.nbr;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long cnt = 0;
+  if (i < v.nsplit) {
+    const gbo_split sp = v.splits[i];
+    const WT vis = visited[sp.row];
+    WT nw = 0;
+    for (int r = 0; r < B; ++r) {
+      uint32_t a = (uint32_t)kINF;
+      for (int q = 0; q < sp.nslots; ++q) a = min(a, scratch[(size_t)(sp.slot0 + q) * B + r]);
+      const long long row = (long long)sp.row * B + r;
+      if (row < v.nrows && a < dist[row]) {
+        dist[row] = a;
+        nw |= (WT)((WT)1 << (B - 1 - r));
+      }
+    }
+    out[sp.row] = nw;
+    if (nw) visited[sp.row] = (WT)(vis | nw);
+    cnt = popc_w(nw);
+  }
+  block_add_u64(cnt, &ctrl->count);
+  close_iteration(ctrl, [](volatile Ctrl* c, int it) {
+    return c->count == 0ull || it >= c->max_iter;
+  });
+}
+
+template <int B>
+__global__ void k_sssp_init(typename Word<B>::T* front, typename Word<B>::T* visited,
+                            uint32_t* dist, int nbr, int n, int src, Ctrl* ctrl, int max_iter) {
+  using WT = typename Word<B>::T;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long k = i; k < n; k += stride) dist[k] = (k == src) ? 0u : (uint32_t)kINF;
+  for (long long k = i; k < nbr; k += stride) {
+    WT w = (k == src / B) ? (WT)((WT)1 << (B - 1 - src % B)) : (WT)0;
+    front[k] = w;
+    front[nbr + k] = 0;
+    visited[k] = w;
+  }
+  if (i == 0) {
+    ctrl->iter = 0;
+    ctrl->done = 0;
+    ctrl->ticket = 0;
+    ctrl->max_iter = max_iter;
+    ctrl->count = 0;
+    ctrl->err = 0;
+    ctrl->last_err = 0;
+  }
+}
+
+// ============================================================ PageRank
+// p'[i] = alpha * sum_{j: P[i][j]} p[j] * inv[j] + add + add_scale * v[i].
+template <int B>
+__global__ void __launch_bounds__(kTPB) k_pr_step(GView v, float* __restrict__ pr,
+                                                  const float* __restrict__ inv,
+                                                  const float* __restrict__ pv,
+                                                  Ctrl* __restrict__ ctrl, double* __restrict__ scratch) {
+  using WT = typename Word<B>::T;
+  using L = Lay<B>;
+  if (((volatile Ctrl*)ctrl)->done) return;
+  const int itn = ((volatile Ctrl*)ctrl)->iter;
+  const double alpha = ctrl->alpha, add = ctrl->add, adds = ctrl->add_scale;
+  const int norm = ctrl->norm;
+  const int n = v.nrows;
+  const float* __restrict__ x = pr + (size_t)(itn & 1) * n;
+  float* __restrict__ y = pr + (size_t)((itn + 1) & 1) * n;
+  const unsigned lane = threadIdx.x & 31;
+  const long long item = item_index(lane, L::W, L::G);
+  double e = 0.0;
+  if (item < v.nitems) {
+    const int r = lane % L::W;
+    const gbo_item it = v.items[item];
+    const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
+    double a0 = 0.0, a1 = 0.0;
+    for (int t = it.t0; t < it.t1; ++t) {
+      const long long base = (long long)v.colind[t] * B;
+      const WT w0 = val[(size_t)t * B + r];
+      for_each_col<B>(w0, [&](int j) { a0 += (double)(x[base + j] * inv[base + j]); });
+      if (L::RPL == 2) {
+        const WT w1 = val[(size_t)t * B + 32 + r];
+        for_each_col<B>(w1, [&](int j) { a1 += (double)(x[base + j] * inv[base + j]); });
+      }
+    }
+    if (it.slot >= 0) {
+      scratch[(size_t)it.slot * B + r] = a0;
+      if (L::RPL == 2) scratch[(size_t)it.slot * B + 32 + r] = a1;
+    } else {
+      const long long row0 = (long long)it.row * B + r;
+      if (row0 < n) {
+        float yn = (float)(alpha * a0 + add + (pv ? adds * (double)pv[row0] : 0.0));
+        y[row0] = yn;
+        double d = (double)yn - (double)x[row0];
+        e += norm == 1 ? fabs(d) : d * d;
+      }
+      if (L::RPL == 2 && row0 + 32 < n) {
+        float yn = (float)(alpha * a1 + add + (pv ? adds * (double)pv[row0 + 32] : 0.0));
+        y[row0 + 32] = yn;
+        double d = (double)yn - (double)x[row0 + 32];
+        e += norm == 1 ? fabs(d) : d * d;
+      }
+    }
+  }
+  block_add_f64(e, &ctrl->err);
+}
+
+template <int B>
+__global__ void k_pr_finish(GView v, float* __restrict__ pr, const float* __restrict__ pv,
+                            Ctrl* __restrict__ ctrl, const double* __restrict__ scratch) {
+  if (((volatile Ctrl*)ctrl)->done) return;
+  const int itn = ((volatile Ctrl*)ctrl)->iter;
+  const double alpha = ctrl->alpha, add = ctrl->add, adds = ctrl->add_scale;
+  const int norm = ctrl->norm;
+  const int n = v.nrows;
+  const float* __restrict__ x = pr + (size_t)(itn & 1) * n;
+  float* __restrict__ y = pr + (size_t)((itn + 1) & 1) * n;
+  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0.0;
+  if (gid < (long long)v.nsplit * B) {
+    const gbo_split sp = v.splits[gid / B];
+    const int r = (int)(gid % B);
+    double a = 0.0;
+    for (int q = 0; q < sp.nslots; ++q) a += scratch[(size_t)(sp.slot0 + q) * B + r];
+    const long long row = (long long)sp.row * B + r;
+    if (row < n) {
+      float yn = (float)(alpha * a + add + (pv ? adds * (double)pv[row] : 0.0));
+      y[row] = yn;
+      double d = (double)yn - (double)x[row];
+      e += norm == 1 ? fabs(d) : d * d;
+    }
+  }
+  block_add_f64(e, &ctrl->err);
+  close_iteration(ctrl, [](volatile Ctrl* c, int it) {
+    double m = c->norm == 2 ? sqrt(c->err) : c->err;
+    return it >= c->max_iter || (c->tol >= 0.f && m <= (double)c->tol);
+  });
+}
+
+__global__ void k_pr_init(float* pr, const float* pv, int n, float init_const, float init_scale,
+                          Ctrl* ctrl, int max_iter, float tol, float alpha, float add,
+                          float add_scale, int norm) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long k = i; k < n; k += stride) {
+    pr[k] = init_const + (pv ? init_scale * pv[k] : 0.f);
+    pr[n + k] = 0.f;
+  }
+  if (i == 0) {
+    ctrl->iter = 0;
+    ctrl->done = max_iter <= 0 ? 1 : 0;
+    ctrl->ticket = 0;
+    ctrl->max_iter = max_iter;
+    ctrl->count = 0;
+    ctrl->err = 0;
+    ctrl->last_err = 0;
+    ctrl->tol = tol;
+    ctrl->alpha = alpha;
+    ctrl->add = add;
+    ctrl->add_scale = add_scale;
+    ctrl->norm = norm;
+    ctrl->n = n;
+  }
+}
+
+// ===================================================== PPR adjoint step
+// u'[j] = w[j] + alpha * inv[j] * sum_{i: P[i][j]} u[i]   (P^T by scatter)
+__global__ void k_adj_prep(float* __restrict__ pr, const float* __restrict__ w, int n,
+                           Ctrl* __restrict__ ctrl, double* __restrict__ acc) {
+  if (((volatile Ctrl*)ctrl)->done) return;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long k = i; k < n; k += stride) acc[k] = 0.0;
+}
+
+template <int B>
+__global__ void __launch_bounds__(kTPB) k_adj_scatter(GView v, const float* __restrict__ pr,
+                                                      Ctrl* __restrict__ ctrl, double* __restrict__ acc) {
+  using WT = typename Word<B>::T;
+  using L = Lay<B>;
+  if (((volatile Ctrl*)ctrl)->done) return;
+  const int itn = ((volatile Ctrl*)ctrl)->iter;
+  const int n = v.nrows;
+  const float* __restrict__ u = pr + (size_t)(itn & 1) * n;
+  const unsigned lane = threadIdx.x & 31;
+  const long long item = item_index(lane, L::W, L::G);
+  if (item >= v.nitems) return;
+  const int r = lane % L::W;
+  const gbo_item it = v.items[item];
+  const long long row0 = (long long)it.row * B + r;
+  const float u0 = row0 < n ? u[row0] : 0.f;
+  const float u1 = (L::RPL == 2 && row0 + 32 < n) ? u[row0 + 32] : 0.f;
+  if (u0 == 0.f && u1 == 0.f) return;
+  const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
+  for (int t = it.t0; t < it.t1; ++t) {
+    const long long base = (long long)v.colind[t] * B;
+    if (u0 != 0.f)
+      for_each_col<B>(val[(size_t)t * B + r], [&](int j) { atomicAdd(acc + base + j, (double)u0); });
+    if (L::RPL == 2 && u1 != 0.f)
+      for_each_col<B>(val[(size_t)t * B + 32 + r], [&](int j) { atomicAdd(acc + base + j, (double)u1); });
+  }
+}
+
+__global__ void k_adj_apply(float* __restrict__ pr, const float* __restrict__ w,
+                            const float* __restrict__ inv, int n, Ctrl* __restrict__ ctrl,
+                            const double* __restrict__ acc) {
+  if (((volatile Ctrl*)ctrl)->done) return;
+  const int itn = ((volatile Ctrl*)ctrl)->iter;
+  const float alpha = ctrl->alpha;
+  const float* __restrict__ x = pr + (size_t)(itn & 1) * n;
+  float* __restrict__ y = pr + (size_t)((itn + 1) & 1) * n;
+  double e = 0.0;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    float yn = (float)((double)w[k] + (double)alpha * (double)inv[k] * acc[k]);
+    y[k] = yn;
+    e += fabs((double)yn - (double)x[k]);
+  }
+  block_add_f64(e, &ctrl->err);
+  close_iteration(ctrl, [](volatile Ctrl* c, int it) {
+    return it >= c->max_iter || (c->tol >= 0.f && c->err <= (double)c->tol);
+  });
+}
+
+__global__ void k_scale_copy(const float* __restrict__ src, float* __restrict__ dst, int n, float s) {
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x)
+    dst[k] = s * src[k];
+}
+
+// ================================================================== CC
+// FastSV (Zhang, Azad, Hu 2020): min-neighbour grandparent, stochastic and
+// aggressive hooking, shortcutting, until the grandparents stop changing.
+template <int B>
+__global__ void __launch_bounds__(kTPB) k_cc_mngf(GView v, const int* __restrict__ gf,
+                                                  int* __restrict__ mngf, Ctrl* __restrict__ ctrl,
+                                                  int* __restrict__ scratch) {
+  using WT = typename Word<B>::T;
+  using L = Lay<B>;
+  if (((volatile Ctrl*)ctrl)->done) return;
+  const unsigned lane = threadIdx.x & 31;
+  const long long item = item_index(lane, L::W, L::G);
+  if (item >= v.nitems) return;
+  const int r = lane % L::W;
+  const gbo_item it = v.items[item];
+  const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
+  int a0 = kINF, a1 = kINF;
+  for (int t = it.t0; t < it.t1; ++t) {
+    const long long base = (long long)v.colind[t] * B;
+    for_each_col<B>(val[(size_t)t * B + r], [&](int j) { a0 = min(a0, gf[base + j]); });
+    if (L::RPL == 2) for_each_col<B>(val[(size_t)t * B + 32 + r], [&](int j) { a1 = min(a1, gf[base + j]); });
+  }
+  if (it.slot >= 0) {
+    scratch[(size_t)it.slot * B + r] = a0;
+    if (L::RPL == 2) scratch[(size_t)it.slot * B + 32 + r] = a1;
+    return;
+  }
+  const long long row0 = (long long)it.row * B + r;
+  if (row0 < v.nrows && a0 < mngf[row0]) mngf[row0] = a0;
+  if (L::RPL == 2 && row0 + 32 < v.nrows && a1 < mngf[row0 + 32]) mngf[row0 + 32] = a1;
+}
+
+template <int B>
+__global__ void k_cc_mngf_finish(GView v, int* __restrict__ mngf, Ctrl* __restrict__ ctrl,
+                                 const int* __restrict__ scratch) {
+  if (((volatile Ctrl*)ctrl)->done) return;
+  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= (long long)v.nsplit * B) return;
+  const gbo_split sp = v.splits[gid / B];
+  const int r = (int)(gid % B);
+  int a = kINF;
+  for (int q = 0; q < sp.nslots; ++q) a = min(a, scratch[(size_t)(sp.slot0 + q) * B + r]);
+  const long long row = (long long)sp.row * B + r;
+  if (row < v.nrows && a < mngf[row]) mngf[row] = a;
+}
+
+__global__ void k_cc_hook(int* __restrict__ f, const int* __restrict__ mngf, int n, Ctrl* ctrl) {
+  if (((volatile Ctrl*)ctrl)->done) return;
+  for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < n;
+       u += (long long)gridDim.x * blockDim.x) {
+    const int m = mngf[u];
+    const int fu = f[u];
+    if (m < fu) atomicMin(f + fu, m);  // stochastic hooking f[f[u]] <- mngf[u]
+  }
+}
+
+__global__ void k_cc_shortcut(int* __restrict__ f, const int* __restrict__ mngf,
+                              const int* __restrict__ gf, int n, Ctrl* ctrl) {
+  if (((volatile Ctrl*)ctrl)->done) return;
+  for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < n;
+       u += (long long)gridDim.x * blockDim.x) {
+    const int m = min(mngf[u], gf[u]);  // aggressive hooking + shortcutting
+    if (m < f[u]) atomicMin(f + u, m);
+  }
+}
+
+__global__ void k_cc_grand(const int* __restrict__ f, int* __restrict__ gf, int n, Ctrl* ctrl) {
+  if (((volatile Ctrl*)ctrl)->done) return;
+  unsigned long long changed = 0;
+  for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < n;
+       u += (long long)gridDim.x * blockDim.x) {
+    const int g2 = f[f[u]];
+    if (g2 != gf[u]) {
+      gf[u] = g2;
+      ++changed;
+    }
+  }
+  block_add_u64(changed, &ctrl->count);
+  close_iteration(ctrl, [](volatile Ctrl* c, int it) {
+    return c->count == 0ull || it >= c->max_iter;
+  });
+}
+
+__global__ void k_cc_init(int* f, int* gf, int* mngf, int n, Ctrl* ctrl, int max_iter) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long k = i; k < n; k += stride) {
+    f[k] = (int)k;
+    gf[k] = (int)k;
+    mngf[k] = (int)k;
+  }
+  if (i == 0) {
+    ctrl->iter = 0;
+    ctrl->done = 0;
+    ctrl->ticket = 0;
+    ctrl->max_iter = max_iter;
+    ctrl->count = 0;
+    ctrl->err = 0;
+    ctrl->last_err = 0;
+  }
+}
+
+// ================================================================ host
+unsigned grid_for_items(int nitems, int b) {
+  const int G = b >= 32 ? 1 : 32 / b;
+  long long warps = ((long long)nitems + G - 1) / G;
+  return blocks_for_warps(warps, kTPB / 32);
+}
+
+unsigned grid_vertex(long long n) {
+  unsigned g = blocks_for(n, kTPB);
+  unsigned cap = (unsigned)num_sms() * 8u;
+  return g < cap ? g : cap;
+}
+
+int get_state(gbo_graph* g, AlgoState** out) {
+  if (!g->algo) {
+    AlgoState* a = new AlgoState();
+    g->algo = a;
+    GBO_CUDA_TRY(cudaStreamCreateWithFlags(&a->cap, cudaStreamNonBlocking));
+    GBO_CUDA_TRY(cudaMalloc(&a->ctrl, sizeof(Ctrl)));
+    GBO_CUDA_TRY(cudaHostAlloc(&a->h_ctrl, sizeof(Ctrl), cudaHostAllocDefault));
+    const size_t sb = (size_t)g->nslots * (size_t)g->b * 8 + 64;
+    GBO_CUDA_TRY(cudaMalloc(&a->scratch, sb));
+    g->device_bytes += (long long)sb + (long long)sizeof(Ctrl);
+    for (auto& e : a->ev) GBO_CUDA_TRY(cudaEventCreate(&e));
+    a->ev_ready = 1;
+  }
+  *out = g->algo;
+  return GBO_OK;
+}
+
+int ensure_frontier(gbo_graph* g, AlgoState* a) {
+  if (!a->front) {
+    const size_t wb = 8;  // widest word
+    GBO_CUDA_TRY(cudaMalloc(&a->front, wb * 2 * (size_t)(g->nbr + 1)));
+    GBO_CUDA_TRY(cudaMalloc(&a->visited, wb * (size_t)(g->nbr + 1)));
+    g->device_bytes += (long long)(wb * 3 * (g->nbr + 1));
+  }
+  return GBO_OK;
+}
+
+int ensure_vec_i32(gbo_graph* g, int** p) {
+  if (!*p) {
+    GBO_CUDA_TRY(cudaMalloc(p, sizeof(int) * (size_t)(g->nrows > 0 ? g->nrows : 1)));
+    g->device_bytes += 4LL * g->nrows;
+  }
+  return GBO_OK;
+}
+
+// Capture kStepsPerGraph iterations of `body` once per (graph, algorithm).
+template <typename Body>
+int get_exec(AlgoState* a, int id, const void* key, Body body) {
+  if (a->exec[id] && a->exec_key[id] == key) return GBO_OK;
+  if (a->exec[id]) {
+    cudaGraphExecDestroy(a->exec[id]);
+    a->exec[id] = nullptr;
+  }
+  cudaGraph_t graph = nullptr;
+  GBO_CUDA_TRY(cudaStreamBeginCapture(a->cap, cudaStreamCaptureModeThreadLocal));
+  int st = GBO_OK;
+  int launches = 0;
+  for (int k = 0; k < kStepsPerGraph && st == GBO_OK; ++k) st = body(a->cap, k, &launches);
+  cudaError_t e = cudaStreamEndCapture(a->cap, &graph);
+  if (st != GBO_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return st;
+  }
+  if (e != cudaSuccess) return fail_cuda(e, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(&a->exec[id], graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return fail_cuda(e, "cudaGraphInstantiate");
+  a->exec_key[id] = key;
+  a->launches_per_replay = launches;
+  return GBO_OK;
+}
+
+// Brackets the main kernel of captured iteration k with events (timing of
+// the iteration's BMV launch, read back after each replay).
+struct StepTimer {
+  AlgoState* a;
+  cudaStream_t s;
+  int k;
+  void begin() const { cudaEventRecord(a->ev[2 * k], s); }
+  void end() const { cudaEventRecord(a->ev[2 * k + 1], s); }
+};
+
+// Replay the captured iterations until the device sets `done`.
+int run_until_done(AlgoState* a, int id, cudaStream_t s, int max_iter, int* iters) {
+  const long long max_launch = (long long)max_iter / kStepsPerGraph + 2;
+  a->step_ms.clear();
+  a->replays = 0;
+  a->launches = 1;  // the init kernel
+  int it0 = 0;
+  for (long long k = 0; k < max_launch; ++k) {
+    GBO_CUDA_TRY(cudaGraphLaunch(a->exec[id], s));
+    GBO_CUDA_TRY(cudaMemcpyAsync(a->h_ctrl, a->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
+    GBO_CUDA_TRY(cudaStreamSynchronize(s));
+    ++a->replays;
+    a->launches += a->launches_per_replay;
+    const int it1 = a->h_ctrl->iter;
+    for (int q = 0; q < it1 - it0 && q < kStepsPerGraph; ++q) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, a->ev[2 * q], a->ev[2 * q + 1]) != cudaSuccess) ms = -1.f;
+      a->step_ms.push_back(ms);
+    }
+    it0 = it1;
+    if (a->h_ctrl->done) break;
+  }
+  if (!a->h_ctrl->done) return fail(GBO_ERR_TIMEOUT, "iteration loop did not terminate");
+  if (iters) *iters = a->h_ctrl->iter;
+  return GBO_OK;
+}
+
+#define ALGO_DISPATCH_B(b, CALL) \
+  switch (b) {                  \
+    case 4: { constexpr int B = 4; CALL; } break;   \
+    case 8: { constexpr int B = 8; CALL; } break;   \
+    case 16: { constexpr int B = 16; CALL; } break; \
+    case 32: { constexpr int B = 32; CALL; } break; \
+    default: { constexpr int B = 64; CALL; } break; \
+  }
+
+template <int B>
+int bfs_impl(gbo_graph* g, int src, int32_t* d_level, int* h_depth, cudaStream_t s) {
+  using WT = typename Word<B>::T;
+  AlgoState* a = nullptr;
+  GBO_TRY(get_state(g, &a));
+  GBO_TRY(ensure_frontier(g, a));
+  GBO_TRY(ensure_vec_i32(g, &a->level));
+  GView v = view_of(g);
+  WT* front = (WT*)a->front;
+  WT* vis = (WT*)a->visited;
+  Ctrl* ctrl = a->ctrl;
+  int* level = a->level;
+  WT* scratch = (WT*)a->scratch;
+  const unsigned gi = grid_for_items(g->nitems, B);
+  const unsigned gs = blocks_for(g->nsplit, kTPB);
+  GBO_TRY(get_exec(a, A_BFS, nullptr, [&](cudaStream_t cs, int k, int* nl) -> int {
+    StepTimer tm{a, cs, k};
+    tm.begin();
+    if (g->nitems > 0) k_bfs_step<B><<<gi, kTPB, 0, cs>>>(v, front, vis, level, ctrl, scratch);
+    tm.end();
+    k_bfs_finish<B><<<gs, kTPB, 0, cs>>>(v, front, vis, level, ctrl, scratch);
+    *nl += (g->nitems > 0) + 1;
+    GBO_CUDA_TRY(cudaGetLastError());
+    return GBO_OK;
+  }));
+  const int max_iter = g->nrows + 1;
+  k_bfs_init<B><<<grid_vertex(std::max(g->nrows, g->nbr)), kTPB, 0, s>>>(front, vis, level, g->nbr,
+                                                                       g->nrows, src, ctrl, max_iter);
+  GBO_CUDA_TRY(cudaGetLastError());
+  int iters = 0;
+  GBO_TRY(run_until_done(a, A_BFS, s, max_iter, &iters));
+  if (g->nrows > 0)
+    GBO_CUDA_TRY(cudaMemcpyAsync(d_level, level, sizeof(int) * (size_t)g->nrows,
+                                 cudaMemcpyDeviceToDevice, s));
+  if (h_depth) *h_depth = iters;
+  return GBO_OK;
+}
+
+template <int B>
+int sssp_impl(gbo_graph* g, int src, uint32_t* d_dist, int* h_iters, cudaStream_t s) {
+  using WT = typename Word<B>::T;
+  AlgoState* a = nullptr;
+  GBO_TRY(get_state(g, &a));
+  GBO_TRY(ensure_frontier(g, a));
+  if (!a->dist) {
+    GBO_CUDA_TRY(cudaMalloc(&a->dist, sizeof(uint32_t) * (size_t)(g->nrows > 0 ? g->nrows : 1)));
+    g->device_bytes += 4LL * g->nrows;
+  }
+  GView v = view_of(g);
+  WT* front = (WT*)a->front;
+  WT* vis = (WT*)a->visited;
+  Ctrl* ctrl = a->ctrl;
+  uint32_t* dist = a->dist;
+  uint32_t* scratch = (uint32_t*)a->scratch;
+  const unsigned gi = grid_for_items(g->nitems, B);
+  const unsigned gs = blocks_for(g->nsplit, kTPB);
+  GBO_TRY(get_exec(a, A_SSSP, nullptr, [&](cudaStream_t cs, int k, int* nl) -> int {
+    StepTimer tm{a, cs, k};
+    tm.begin();
+    if (g->nitems > 0) k_sssp_step<B><<<gi, kTPB, 0, cs>>>(v, front, vis, dist, ctrl, scratch);
+    tm.end();
+    k_sssp_finish<B><<<gs, kTPB, 0, cs>>>(v, front, vis, dist, ctrl, scratch);
+    *nl += (g->nitems > 0) + 1;
+    GBO_CUDA_TRY(cudaGetLastError());
+    return GBO_OK;
+  }));
+  const int max_iter = g->nrows + 1;
+  k_sssp_init<B><<<grid_vertex(std::max(g->nrows, g->nbr)), kTPB, 0, s>>>(front, vis, dist, g->nbr,
+                                                                        g->nrows, src, ctrl, max_iter);
+  GBO_CUDA_TRY(cudaGetLastError());
+  GBO_TRY(run_until_done(a, A_SSSP, s, max_iter, h_iters));
+  if (g->nrows > 0)
+    GBO_CUDA_TRY(cudaMemcpyAsync(d_dist, dist, sizeof(uint32_t) * (size_t)g->nrows,
+                                 cudaMemcpyDeviceToDevice, s));
+  return GBO_OK;
+}
+
+// Shared by PageRank (v = NULL) and the PPR forward pass.
+template <int B>
+int pr_impl(gbo_graph* g, const float* d_v, float alpha, int max_iter, float tol, float* d_p,
+            int* h_iters, int norm, float init_const, float init_scale, float add, float add_scale,
+            int id, cudaStream_t s) {
+  AlgoState* a = nullptr;
+  GBO_TRY(get_state(g, &a));
+  if (!a->pr) {
+    GBO_CUDA_TRY(cudaMalloc(&a->pr, sizeof(float) * 2 * (size_t)(g->nrows > 0 ? g->nrows : 1)));
+    g->device_bytes += 8LL * g->nrows;
+  }
+  GView v = view_of(g);
+  float* pr = a->pr;
+  const float* inv = g->invdeg;
+  Ctrl* ctrl = a->ctrl;
+  double* scratch = (double*)a->scratch;
+  const unsigned gi = grid_for_items(g->nitems, B);
+  const unsigned gs = blocks_for((long long)g->nsplit * B, kTPB);
+  GBO_TRY(get_exec(a, id, d_v, [&](cudaStream_t cs, int k, int* nl) -> int {
+    StepTimer tm{a, cs, k};
+    tm.begin();
+    if (g->nitems > 0) k_pr_step<B><<<gi, kTPB, 0, cs>>>(v, pr, inv, d_v, ctrl, scratch);
+    tm.end();
+    k_pr_finish<B><<<gs, kTPB, 0, cs>>>(v, pr, d_v, ctrl, scratch);
+    *nl += (g->nitems > 0) + 1;
+    GBO_CUDA_TRY(cudaGetLastError());
+    return GBO_OK;
+  }));
+  k_pr_init<<<grid_vertex(g->nrows), kTPB, 0, s>>>(pr, d_v, g->nrows, init_const, init_scale, ctrl,
+                                                  max_iter, tol, alpha, add, add_scale, norm);
+  GBO_CUDA_TRY(cudaGetLastError());
+  int iters = 0;
+  if (max_iter > 0) GBO_TRY(run_until_done(a, id, s, max_iter, &iters));
+  if (g->nrows > 0)
+    GBO_CUDA_TRY(cudaMemcpyAsync(d_p, pr + (size_t)(iters & 1) * g->nrows,
+                                 sizeof(float) * (size_t)g->nrows, cudaMemcpyDeviceToDevice, s));
+  if (h_iters) *h_iters = iters;
+  return GBO_OK;
+}
+
+template <int B>
+int ppr_backward_impl(gbo_graph* g, const float* d_w, float alpha, float tol, int max_iter,
+                      float* d_grad, int* h_iters, cudaStream_t s) {
+  AlgoState* a = nullptr;
+  GBO_TRY(get_state(g, &a));
+  if (!a->pr) {
+    GBO_CUDA_TRY(cudaMalloc(&a->pr, sizeof(float) * 2 * (size_t)(g->nrows > 0 ? g->nrows : 1)));
+    g->device_bytes += 8LL * g->nrows;
+  }
+  if (!a->acc64) {
+    GBO_CUDA_TRY(cudaMalloc(&a->acc64, sizeof(double) * (size_t)(g->nrows > 0 ? g->nrows : 1)));
+    g->device_bytes += 8LL * g->nrows;
+  }
+  GView v = view_of(g);
+  float* pr = a->pr;
+  double* acc = a->acc64;
+  const float* inv = g->invdeg;
+  Ctrl* ctrl = a->ctrl;
+  const int n = g->nrows;
+  const unsigned gi = grid_for_items(g->nitems, B);
+  const unsigned gv = grid_vertex(n);
+  GBO_TRY(get_exec(a, A_PPR_B, d_w, [&](cudaStream_t cs, int k, int* nl) -> int {
+    StepTimer tm{a, cs, k};
+    k_adj_prep<<<gv, kTPB, 0, cs>>>(pr, d_w, n, ctrl, acc);
+    tm.begin();
+    if (g->nitems > 0) k_adj_scatter<B><<<gi, kTPB, 0, cs>>>(v, pr, ctrl, acc);
+    tm.end();
+    k_adj_apply<<<gv, kTPB, 0, cs>>>(pr, d_w, inv, n, ctrl, acc);
+    *nl += (g->nitems > 0) + 2;
+    GBO_CUDA_TRY(cudaGetLastError());
+    return GBO_OK;
+  }));
+  // u0 = w
+  k_pr_init<<<gv, kTPB, 0, s>>>(pr, d_w, n, 0.f, 1.f, ctrl, max_iter, tol, alpha, 0.f, 0.f, 1);
+  GBO_CUDA_TRY(cudaGetLastError());
+  int iters = 0;
+  if (max_iter > 0) GBO_TRY(run_until_done(a, A_PPR_B, s, max_iter, &iters));
+  if (n > 0) k_scale_copy<<<gv, kTPB, 0, s>>>(pr + (size_t)(iters & 1) * n, d_grad, n, 1.f - alpha);
+  GBO_CUDA_TRY(cudaGetLastError());
+  if (h_iters) *h_iters = iters;
+  return GBO_OK;
+}
+
+template <int B>
+int cc_impl(gbo_graph* g, int32_t* d_label, int* h_iters, cudaStream_t s) {
+  AlgoState* a = nullptr;
+  GBO_TRY(get_state(g, &a));
+  GBO_TRY(ensure_vec_i32(g, &a->f));
+  GBO_TRY(ensure_vec_i32(g, &a->gf));
+  GBO_TRY(ensure_vec_i32(g, &a->mngf));
+  GView v = view_of(g);
+  int *f = a->f, *gf = a->gf, *mngf = a->mngf;
+  Ctrl* ctrl = a->ctrl;
+  int* scratch = (int*)a->scratch;
+  const int n = g->nrows;
+  const unsigned gi = grid_for_items(g->nitems, B);
+  const unsigned gs = blocks_for((long long)g->nsplit * B, kTPB);
+  const unsigned gv = grid_vertex(n);
+  GBO_TRY(get_exec(a, A_CC, nullptr, [&](cudaStream_t cs, int k, int* nl) -> int {
+    StepTimer tm{a, cs, k};
+    tm.begin();
+    if (g->nitems > 0) k_cc_mngf<B><<<gi, kTPB, 0, cs>>>(v, gf, mngf, ctrl, scratch);
+    tm.end();
+    *nl += (g->nitems > 0) + (g->nsplit > 0) + 3;
+    if (g->nsplit > 0) k_cc_mngf_finish<B><<<gs, kTPB, 0, cs>>>(v, mngf, ctrl, scratch);
+    k_cc_hook<<<gv, kTPB, 0, cs>>>(f, mngf, n, ctrl);
+    k_cc_shortcut<<<gv, kTPB, 0, cs>>>(f, mngf, gf, n, ctrl);
+    k_cc_grand<<<gv, kTPB, 0, cs>>>(f, gf, n, ctrl);
+    GBO_CUDA_TRY(cudaGetLastError());
+    return GBO_OK;
+  }));
+  const int max_iter = n + 2;
+  k_cc_init<<<gv, kTPB, 0, s>>>(f, gf, mngf, n, ctrl, max_iter);
+  GBO_CUDA_TRY(cudaGetLastError());
+  GBO_TRY(run_until_done(a, A_CC, s, max_iter, h_iters));
+  if (n > 0)
+    GBO_CUDA_TRY(cudaMemcpyAsync(d_label, f, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, s));
+  return GBO_OK;
+}
+
+int check_algo_graph(const gbo_graph* g) {
+  if (!g) return fail(GBO_ERR_INVALID, "graph is NULL");
+  if (g->layout != GBO_LAYOUT_ROW) return fail(GBO_ERR_UNSUPPORTED, "algorithms need the ROW tile layout");
+  if (g->nrows != g->ncols) return fail(GBO_ERR_INVALID, "algorithms need a square matrix");
+  return GBO_OK;
+}
+
+}  // namespace
+
+void free_algo_state(gbo_graph* g) {
+  AlgoState* a = g->algo;
+  if (!a) return;
+  for (auto& e : a->exec)
+    if (e) cudaGraphExecDestroy(e);
+  for (auto& e : a->ev)
+    if (e) cudaEventDestroy(e);
+  cudaFree(a->ctrl);
+  cudaFreeHost(a->h_ctrl);
+  cudaFree(a->front);
+  cudaFree(a->visited);
+  cudaFree(a->level);
+  cudaFree(a->dist);
+  cudaFree(a->pr);
+  cudaFree(a->f);
+  cudaFree(a->gf);
+  cudaFree(a->mngf);
+  cudaFree(a->acc64);
+  cudaFree(a->scratch);
+  if (a->cap) cudaStreamDestroy(a->cap);
+  delete a;
+  g->algo = nullptr;
+}
+
+}  // namespace gbo
+
+using namespace gbo;
+
+extern "C" int gbo_bfs(const gbo_graph* gc, int src, int32_t* d_level, int* h_depth,
+                       gbo_stream_t stream) {
+  clear_error();
+  GBO_TRY(check_algo_graph(gc));
+  gbo_graph* g = const_cast<gbo_graph*>(gc);
+  if (src < 0 || src >= g->nrows) return fail(GBO_ERR_INVALID, "source vertex out of range");
+  if (!d_level) return fail(GBO_ERR_INVALID, "level is NULL");
+  int st = GBO_OK;
+  ALGO_DISPATCH_B(g->b, st = bfs_impl<B>(g, src, d_level, h_depth, as_stream(stream)));
+  return st;
+}
+
+extern "C" int gbo_sssp_unit(const gbo_graph* gc, int src, uint32_t* d_dist, int* h_iters,
+                             gbo_stream_t stream) {
+  clear_error();
+  GBO_TRY(check_algo_graph(gc));
+  gbo_graph* g = const_cast<gbo_graph*>(gc);
+  if (src < 0 || src >= g->nrows) return fail(GBO_ERR_INVALID, "source vertex out of range");
+  if (!d_dist) return fail(GBO_ERR_INVALID, "dist is NULL");
+  int st = GBO_OK;
+  ALGO_DISPATCH_B(g->b, st = sssp_impl<B>(g, src, d_dist, h_iters, as_stream(stream)));
+  return st;
+}
+
+extern "C" int gbo_pagerank(const gbo_graph* gc, float alpha, int max_iter, float tol, float* d_p,
+                            int* h_iters, gbo_stream_t stream) {
+  clear_error();
+  GBO_TRY(check_algo_graph(gc));
+  gbo_graph* g = const_cast<gbo_graph*>(gc);
+  if (!g->invdeg) return fail(GBO_ERR_INVALID, "graph has no out-degrees (wrapped without d_outdeg)");
+  if (!d_p && g->nrows > 0) return fail(GBO_ERR_INVALID, "p is NULL");
+  if (max_iter < 0) return fail(GBO_ERR_INVALID, "max_iter < 0");
+  const float n = (float)(g->nrows > 0 ? g->nrows : 1);
+  int st = GBO_OK;
+  ALGO_DISPATCH_B(g->b, st = pr_impl<B>(g, nullptr, alpha, max_iter, tol, d_p, h_iters, 2, 1.0f / n,
+                                         0.f, (1.0f - alpha) / n, 0.f, A_PR, as_stream(stream)));
+  return st;
+}
+
+extern "C" int gbo_cc(const gbo_graph* gc, int32_t* d_label, int* h_iters, gbo_stream_t stream) {
+  clear_error();
+  GBO_TRY(check_algo_graph(gc));
+  gbo_graph* g = const_cast<gbo_graph*>(gc);
+  if (!d_label && g->nrows > 0) return fail(GBO_ERR_INVALID, "label is NULL");
+  int st = GBO_OK;
+  ALGO_DISPATCH_B(g->b, st = cc_impl<B>(g, d_label, h_iters, as_stream(stream)));
+  return st;
+}
+
+extern "C" int gbo_ppr_forward(const gbo_graph* gc, const float* d_v, float alpha, float tol,
+                               int max_iter, float* d_p, int* h_iters, gbo_stream_t stream) {
+  clear_error();
+  GBO_TRY(check_algo_graph(gc));
+  gbo_graph* g = const_cast<gbo_graph*>(gc);
+  if (!g->invdeg) return fail(GBO_ERR_INVALID, "graph has no out-degrees");
+  if (g->nrows > 0 && (!d_v || !d_p)) return fail(GBO_ERR_INVALID, "NULL vector");
+  if (max_iter < 0) return fail(GBO_ERR_INVALID, "max_iter < 0");
+  int st = GBO_OK;
+  // p0 = (1-alpha) v;  p' = alpha P D^-1 p + (1-alpha) v
+  ALGO_DISPATCH_B(g->b, st = pr_impl<B>(g, d_v, alpha, max_iter, tol, d_p, h_iters, 1, 0.f,
+                                         1.f - alpha, 0.f, 1.f - alpha, A_PPR_F, as_stream(stream)));
+  return st;
+}
+
+extern "C" int gbo_ppr_backward(const gbo_graph* gc, const float* d_w, float alpha, float tol,
+                                int max_iter, float* d_grad_v, int* h_iters, gbo_stream_t stream) {
+  clear_error();
+  GBO_TRY(check_algo_graph(gc));
+  gbo_graph* g = const_cast<gbo_graph*>(gc);
+  if (!g->invdeg) return fail(GBO_ERR_INVALID, "graph has no out-degrees");
+  if (g->nrows > 0 && (!d_w || !d_grad_v)) return fail(GBO_ERR_INVALID, "NULL vector");
+  if (max_iter < 0) return fail(GBO_ERR_INVALID, "max_iter < 0");
+  int st = GBO_OK;
+  ALGO_DISPATCH_B(g->b, st = ppr_backward_impl<B>(g, d_w, alpha, tol, max_iter, d_grad_v, h_iters,
+                                                  as_stream(stream)));
+  return st;
+}
+
+extern "C" int gbo_graph_last_run(const gbo_graph* g, gbo_run_stats* stats) {
+  clear_error();
+  if (!g || !stats) return fail(GBO_ERR_INVALID, "NULL argument");
+  memset(stats, 0, sizeof(*stats));
+  const AlgoState* a = g->algo;
+  if (!a) return GBO_OK;
+  stats->iterations = a->h_ctrl ? a->h_ctrl->iter : 0;
+  stats->graph_replays = a->replays;
+  stats->kernel_launches = a->launches;
+  const int n = (int)a->step_ms.size();
+  stats->nsteps = n < GBO_MAX_STEP_TIMES ? n : GBO_MAX_STEP_TIMES;
+  for (int i = 0; i < stats->nsteps; ++i) stats->step_ms[i] = a->step_ms[(size_t)i];
+  return GBO_OK;
+}

@@ -1,0 +1,37 @@
+// Kernel-facing view of a graph and the BMV entry points used by the
+// algorithm loops and the C ABI.
+#pragma once
+
+#include "graph.cuh"
+
+namespace gbo {
+
+// Plain-old-data copy of the fields the kernels read (passed by value).
+struct GView {
+  int nrows, ncols, nbr, nbc;
+  const int* __restrict__ rowptr;
+  const int* __restrict__ colind;
+  const void* __restrict__ val;
+  const gbo_item* __restrict__ items;
+  int nitems;
+  const gbo_split* __restrict__ splits;
+  int nsplit;
+};
+
+GView view_of(const gbo_graph* g);
+
+// Scratch bytes the split-row partials of one BMV launch need.
+size_t bmv_scratch_bytes(const gbo_graph* g);
+
+int bmv_count(const gbo_graph* g, const void* x, void* y, int out_type, int accumulate,
+              void* scratch, cudaStream_t s);
+int bmv_masked(const gbo_graph* g, const void* x, const void* mask, void* out, void* scratch,
+               cudaStream_t s);
+int bmv_minplus(const gbo_graph* g, const uint32_t* x, uint32_t* y, void* scratch, cudaStream_t s);
+int bmv_minselect(const gbo_graph* g, const int32_t* x, int32_t* y, void* scratch, cudaStream_t s);
+int bmv_float(const gbo_graph* g, const float* x, float* y, float alpha, const float* scale,
+              float add, void* scratch, cudaStream_t s);
+int bmv_float_transposed(const gbo_graph* g, const float* x, float* y, float alpha,
+                         const float* scale, float add, cudaStream_t s);
+
+}  // namespace gbo

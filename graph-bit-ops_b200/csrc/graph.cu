@@ -1,0 +1,351 @@
+// Graph handle construction and the C ABI of the BMV primitives.
+#include <algorithm>
+#include <vector>
+
+#include "bmv.cuh"
+
+namespace gbo {
+
+namespace {
+
+// Device copy of a CSR given by host or device pointers, optionally filtered
+// to the lower triangle (row >= col) -- tril_csr (bsrbmm/bsrbmm.cu:1416).
+__global__ void k_tril_count(const int* __restrict__ rowptr, const int* __restrict__ colind,
+                             int nrows, int* __restrict__ cnt) {
+  const long long row = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned lane = threadIdx.x & 31;
+  if (row >= nrows) return;
+  int a = rowptr[row], e = rowptr[row + 1];
+  int c = 0;
+  for (int p = a + (int)lane; p < e; p += 32) c += colind[p] <= row;
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if (lane == 0) cnt[row] = c;
+}
+
+__global__ void k_tril_fill(const int* __restrict__ rowptr, const int* __restrict__ colind,
+                            int nrows, const int* __restrict__ newptr, int* __restrict__ newcol) {
+  const long long row = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned lane = threadIdx.x & 31;
+  if (row >= nrows) return;
+  int a = rowptr[row], e = rowptr[row + 1];
+  int out = newptr[row];
+  for (int base = a; base < e; base += 32) {
+    int p = base + (int)lane;
+    bool keep = p < e && colind[p] <= row;
+    unsigned bal = __ballot_sync(0xffffffffu, keep);
+    if (keep) newcol[out + __popc(bal & ((1u << lane) - 1u))] = colind[p];
+    out += __popc(bal);
+  }
+}
+
+struct DevCsr {
+  int* rowptr = nullptr;
+  int* colind = nullptr;
+  long long nnz = 0;
+  bool owned = false;
+  void release() {
+    if (owned) {
+      cudaFree(rowptr);
+      cudaFree(colind);
+    }
+    rowptr = colind = nullptr;
+    owned = false;
+  }
+};
+
+int upload_csr(const int* rowptr, const int* colind, int nrows, long long nnz, bool device,
+               cudaStream_t s, DevCsr* out) {
+  if (device) {
+    out->rowptr = const_cast<int*>(rowptr);
+    out->colind = const_cast<int*>(colind);
+    out->nnz = nnz;
+    out->owned = false;
+    return GBO_OK;
+  }
+  GBO_CUDA_TRY(cudaMalloc(&out->rowptr, sizeof(int) * ((size_t)nrows + 1)));
+  GBO_CUDA_TRY(cudaMalloc(&out->colind, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1)));
+  out->owned = true;
+  out->nnz = nnz;
+  GBO_CUDA_TRY(cudaMemcpyAsync(out->rowptr, rowptr, sizeof(int) * ((size_t)nrows + 1),
+                               cudaMemcpyHostToDevice, s));
+  if (nnz > 0)
+    GBO_CUDA_TRY(cudaMemcpyAsync(out->colind, colind, sizeof(int) * (size_t)nnz,
+                                 cudaMemcpyHostToDevice, s));
+  return GBO_OK;
+}
+
+int tril_device(const DevCsr& in, int nrows, cudaStream_t s, DevCsr* out) {
+  int* cnt = nullptr;
+  GBO_CUDA_TRY(cudaMallocAsync(&cnt, sizeof(int) * ((size_t)nrows + 1), s));
+  GBO_CUDA_TRY(cudaMalloc(&out->rowptr, sizeof(int) * ((size_t)nrows + 1)));
+  out->owned = true;
+  long long* tot = nullptr;
+  GBO_CUDA_TRY(cudaMallocAsync(&tot, sizeof(long long), s));
+  if (nrows > 0) k_tril_count<<<blocks_for_warps(nrows, 8), 256, 0, s>>>(in.rowptr, in.colind, nrows, cnt);
+  GBO_TRY(exclusive_scan_i32(cnt, out->rowptr, nrows, tot, s));
+  long long h = 0;
+  GBO_CUDA_TRY(cudaMemcpyAsync(&h, tot, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  GBO_CUDA_TRY(cudaStreamSynchronize(s));
+  out->nnz = h;
+  GBO_CUDA_TRY(cudaMalloc(&out->colind, sizeof(int) * (size_t)(h > 0 ? h : 1)));
+  if (nrows > 0)
+    k_tril_fill<<<blocks_for_warps(nrows, 8), 256, 0, s>>>(in.rowptr, in.colind, nrows, out->rowptr,
+                                                          out->colind);
+  GBO_CUDA_TRY(cudaGetLastError());
+  cudaFreeAsync(cnt, s);
+  cudaFreeAsync(tot, s);
+  return GBO_OK;
+}
+
+void destroy(gbo_graph* g) {
+  if (!g) return;
+  if (g->owns_b2sr) {
+    cudaFree(g->rowptr);
+    cudaFree(g->colind);
+    cudaFree(g->val);
+  }
+  if (g->owns_outdeg) cudaFree(g->outdeg);
+  cudaFree(g->invdeg);
+  cudaFree(g->items);
+  cudaFree(g->splits);
+  cudaFree(g->ws);
+  free_algo_state(g);
+  delete g;
+}
+
+}  // namespace
+
+// Host CSR transpose used when GBO_FLAG_TRANSPOSE is given with host pointers.
+int host_transpose(const int* rowptr, const int* colind, int nrows, int ncols, long long nnz,
+                   std::vector<int>* tptr, std::vector<int>* tcol);
+
+}  // namespace gbo
+
+using namespace gbo;
+
+extern "C" int gbo_graph_from_csr(const int* rowptr, const int* colind, int nrows, int ncols,
+                                  int nnz, int tile_bits, int flags, gbo_stream_t stream,
+                                  gbo_graph** out) {
+  clear_error();
+  if (!out) return fail(GBO_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  if (!valid_tile_bits(tile_bits)) return fail(GBO_ERR_INVALID, "tile_bits must be 4, 8, 16, 32 or 64");
+  if (nrows < 0 || ncols < 0 || nnz < 0 || !rowptr || (nnz > 0 && !colind))
+    return fail(GBO_ERR_INVALID, "gbo_graph_from_csr: bad CSR argument");
+  const bool device = flags & GBO_FLAG_DEVICE_PTRS;
+  const bool transpose = flags & GBO_FLAG_TRANSPOSE;
+  const bool lower = flags & GBO_FLAG_LOWER;
+  const int layout = (flags & GBO_FLAG_LAYOUT_COL) ? GBO_LAYOUT_COL : GBO_LAYOUT_ROW;
+  if (lower && nrows != ncols) return fail(GBO_ERR_INVALID, "GBO_FLAG_LOWER needs a square matrix");
+  cudaStream_t s = as_stream(stream);
+
+  // Transpose (CSC) on the host side of the boundary when given host arrays;
+  // device arrays are copied back first.  The packer needs sorted rows, and
+  // the host transpose emits them in ascending order like readMtx's csr2csc.
+  std::vector<int> tptr, tcol, hptr, hcol;
+  const int* src_ptr = rowptr;
+  const int* src_col = colind;
+  int prow = nrows, pcol = ncols;
+  bool src_device = device;
+  if (transpose) {
+    if (device) {
+      hptr.resize((size_t)nrows + 1);
+      hcol.resize((size_t)nnz);
+      GBO_CUDA_TRY(cudaMemcpyAsync(hptr.data(), rowptr, sizeof(int) * hptr.size(), cudaMemcpyDeviceToHost, s));
+      if (nnz) GBO_CUDA_TRY(cudaMemcpyAsync(hcol.data(), colind, sizeof(int) * hcol.size(), cudaMemcpyDeviceToHost, s));
+      GBO_CUDA_TRY(cudaStreamSynchronize(s));
+      src_ptr = hptr.data();
+      src_col = hcol.data();
+    }
+    GBO_TRY(host_transpose(src_ptr, src_col, nrows, ncols, nnz, &tptr, &tcol));
+    src_ptr = tptr.data();
+    src_col = tcol.data();
+    prow = ncols;
+    pcol = nrows;
+    src_device = false;
+  }
+
+  gbo_graph* g = new gbo_graph();
+  DevCsr csr, low;
+  int st = upload_csr(src_ptr, src_col, prow, nnz, src_device, s, &csr);
+  const DevCsr* use = &csr;
+  if (st == GBO_OK && lower) {
+    st = tril_device(csr, prow, s, &low);
+    use = &low;
+  }
+  if (st == GBO_OK) st = pack_into(g, use->rowptr, use->colind, prow, pcol, use->nnz, tile_bits, layout, s);
+  // out-degree of the graph P pulls over: column counts of P.  With
+  // GBO_FLAG_TRANSPOSE these are the row lengths of the given CSR
+  // (the reference reads csrRowPtr deltas, algorithm/bsrbmv.cu:1277).
+  if (st == GBO_OK) {
+    if (transpose) {
+      const int* hp = device ? hptr.data() : rowptr;
+      std::vector<int> deg((size_t)nrows);
+      for (int i = 0; i < nrows; ++i) deg[i] = hp[i + 1] - hp[i];
+      st = upload_outdeg(g, deg.data(), nrows, s);
+      if (st == GBO_OK) st = cudaStreamSynchronize(s) == cudaSuccess ? GBO_OK : fail(GBO_ERR_CUDA, "sync");
+    } else {
+      st = compute_outdeg_from_cols(g, use->colind, use->nnz, pcol, s);
+    }
+  }
+  if (st == GBO_OK) st = build_schedule(g, s);
+  if (st == GBO_OK) st = ensure_workspace(g, bmv_scratch_bytes(g), s);
+  if (st == GBO_OK) st = cudaStreamSynchronize(s) == cudaSuccess ? GBO_OK : fail(GBO_ERR_CUDA, "graph build sync");
+  low.release();
+  csr.release();
+  if (st != GBO_OK) {
+    destroy(g);
+    return st;
+  }
+  *out = g;
+  return GBO_OK;
+}
+
+extern "C" int gbo_graph_wrap_b2sr(int nrows, int ncols, int tile_bits, int layout, int nblocks,
+                                   const int* d_bsrRowPtr, const int* d_bsrColInd,
+                                   const void* d_bsrVal, const int* d_outdeg, gbo_stream_t stream,
+                                   gbo_graph** out) {
+  clear_error();
+  if (!out) return fail(GBO_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  if (!valid_tile_bits(tile_bits)) return fail(GBO_ERR_INVALID, "tile_bits must be 4, 8, 16, 32 or 64");
+  if (nrows < 0 || ncols < 0 || nblocks < 0 || !d_bsrRowPtr || (nblocks > 0 && (!d_bsrColInd || !d_bsrVal)))
+    return fail(GBO_ERR_INVALID, "gbo_graph_wrap_b2sr: bad argument");
+  if (layout != GBO_LAYOUT_ROW && layout != GBO_LAYOUT_COL) return fail(GBO_ERR_INVALID, "bad layout");
+  cudaStream_t s = as_stream(stream);
+  gbo_graph* g = new gbo_graph();
+  g->nrows = nrows;
+  g->ncols = ncols;
+  g->b = tile_bits;
+  g->layout = layout;
+  g->nbr = (nrows + tile_bits - 1) / tile_bits;
+  g->nbc = (ncols + tile_bits - 1) / tile_bits;
+  g->nblk = nblocks;
+  g->rowptr = const_cast<int*>(d_bsrRowPtr);
+  g->colind = const_cast<int*>(d_bsrColInd);
+  g->val = const_cast<void*>(d_bsrVal);
+  g->owns_b2sr = false;
+  g->owns_outdeg = false;
+  int st = GBO_OK;
+  if (d_outdeg) {
+    g->outdeg = const_cast<int*>(d_outdeg);
+    if (cudaMalloc(&g->invdeg, sizeof(float) * (size_t)(ncols > 0 ? ncols : 1)) != cudaSuccess)
+      st = fail(GBO_ERR_NOMEM, "invdeg");
+    if (st == GBO_OK) launch_invdeg(d_outdeg, ncols, g->invdeg, s);
+  }
+  if (st == GBO_OK) st = build_schedule(g, s);
+  if (st == GBO_OK) st = ensure_workspace(g, bmv_scratch_bytes(g), s);
+  if (st == GBO_OK) st = cudaStreamSynchronize(s) == cudaSuccess ? GBO_OK : fail(GBO_ERR_CUDA, "wrap sync");
+  if (st != GBO_OK) {
+    destroy(g);
+    return st;
+  }
+  *out = g;
+  return GBO_OK;
+}
+
+extern "C" int gbo_graph_free(gbo_graph* g) {
+  clear_error();
+  destroy(g);
+  return GBO_OK;
+}
+
+extern "C" int gbo_graph_get_info(const gbo_graph* g, gbo_graph_info* info) {
+  clear_error();
+  if (!g || !info) return fail(GBO_ERR_INVALID, "NULL argument");
+  info->nrows = g->nrows;
+  info->ncols = g->ncols;
+  info->tile_bits = g->b;
+  info->layout = g->layout;
+  info->nblockrows = g->nbr;
+  info->nblockcols = g->nbc;
+  info->nblocks = g->nblk;
+  info->nnz = g->nnz;
+  info->b2sr_bytes = 4LL * (g->nbr + 1) + 4LL * g->nblk + g->nblk * (long long)g->b * word_bytes(g->b);
+  info->device_bytes = g->device_bytes;
+  info->nsplit_rows = g->nsplit;
+  info->nitems = g->nitems;
+  return GBO_OK;
+}
+
+extern "C" int gbo_graph_b2sr(const gbo_graph* g, const int** r, const int** c, const void** v) {
+  clear_error();
+  if (!g) return fail(GBO_ERR_INVALID, "NULL graph");
+  if (r) *r = g->rowptr;
+  if (c) *c = g->colind;
+  if (v) *v = g->val;
+  return GBO_OK;
+}
+
+extern "C" int gbo_graph_outdeg(const gbo_graph* g, const int** d) {
+  clear_error();
+  if (!g || !d) return fail(GBO_ERR_INVALID, "NULL argument");
+  *d = g->outdeg;
+  return GBO_OK;
+}
+
+// ------------------------------------------------------------ BMV C ABI
+static int check_graph(const gbo_graph* g) {
+  if (!g) return fail(GBO_ERR_INVALID, "graph is NULL");
+  return GBO_OK;
+}
+
+extern "C" int gbo_bmv_count(const gbo_graph* g, const void* d_x_bits, void* d_y, int out_type,
+                             int accumulate, gbo_stream_t stream) {
+  clear_error();
+  GBO_TRY(check_graph(g));
+  if ((g->nrows > 0 && !d_y) || (g->nblk > 0 && !d_x_bits)) return fail(GBO_ERR_INVALID, "NULL vector");
+  if (out_type != GBO_OUT_I32 && out_type != GBO_OUT_F32) return fail(GBO_ERR_INVALID, "bad out_type");
+  if (g->layout != GBO_LAYOUT_ROW) return fail(GBO_ERR_UNSUPPORTED, "BMV needs the ROW tile layout");
+  return bmv_count(g, d_x_bits, d_y, out_type, accumulate, g->ws, as_stream(stream));
+}
+
+extern "C" int gbo_bmv_masked(const gbo_graph* g, const void* d_x_bits, const void* d_mask_bits,
+                              void* d_out_bits, gbo_stream_t stream) {
+  clear_error();
+  GBO_TRY(check_graph(g));
+  if ((g->nbr > 0 && !d_out_bits) || (g->nblk > 0 && !d_x_bits)) return fail(GBO_ERR_INVALID, "NULL vector");
+  if (g->layout != GBO_LAYOUT_ROW) return fail(GBO_ERR_UNSUPPORTED, "BMV needs the ROW tile layout");
+  return bmv_masked(g, d_x_bits, d_mask_bits, d_out_bits, g->ws, as_stream(stream));
+}
+
+extern "C" int gbo_bmv_minplus(const gbo_graph* g, const uint32_t* d_x, uint32_t* d_y,
+                               gbo_stream_t stream) {
+  clear_error();
+  GBO_TRY(check_graph(g));
+  if (g->nrows > 0 && (!d_x || !d_y)) return fail(GBO_ERR_INVALID, "NULL vector");
+  if (g->layout != GBO_LAYOUT_ROW) return fail(GBO_ERR_UNSUPPORTED, "BMV needs the ROW tile layout");
+  if (d_x == d_y) return fail(GBO_ERR_INVALID, "x and y must not alias");
+  return bmv_minplus(g, d_x, d_y, g->ws, as_stream(stream));
+}
+
+extern "C" int gbo_bmv_float(const gbo_graph* g, const float* d_x, float* d_y, float alpha,
+                             const float* d_scale, float add, gbo_stream_t stream) {
+  clear_error();
+  GBO_TRY(check_graph(g));
+  if (g->nrows > 0 && (!d_x || !d_y)) return fail(GBO_ERR_INVALID, "NULL vector");
+  if (g->layout != GBO_LAYOUT_ROW) return fail(GBO_ERR_UNSUPPORTED, "BMV needs the ROW tile layout");
+  if (d_x == d_y) return fail(GBO_ERR_INVALID, "x and y must not alias");
+  return bmv_float(g, d_x, d_y, alpha, d_scale, add, g->ws, as_stream(stream));
+}
+
+extern "C" int gbo_bmv_minselect(const gbo_graph* g, const int32_t* d_x, int32_t* d_y,
+                                 gbo_stream_t stream) {
+  clear_error();
+  GBO_TRY(check_graph(g));
+  if (g->nrows > 0 && (!d_x || !d_y)) return fail(GBO_ERR_INVALID, "NULL vector");
+  if (g->layout != GBO_LAYOUT_ROW) return fail(GBO_ERR_UNSUPPORTED, "BMV needs the ROW tile layout");
+  if (d_x == d_y) return fail(GBO_ERR_INVALID, "x and y must not alias");
+  return bmv_minselect(g, d_x, d_y, g->ws, as_stream(stream));
+}
+
+extern "C" int gbo_bmv_float_transposed(const gbo_graph* g, const float* d_x, float* d_y,
+                                        float alpha, const float* d_scale, float add,
+                                        gbo_stream_t stream) {
+  clear_error();
+  GBO_TRY(check_graph(g));
+  if (g->nrows > 0 && (!d_x || !d_y)) return fail(GBO_ERR_INVALID, "NULL vector");
+  if (g->layout != GBO_LAYOUT_ROW) return fail(GBO_ERR_UNSUPPORTED, "BMV needs the ROW tile layout");
+  if ((const void*)d_x == (const void*)d_y) return fail(GBO_ERR_INVALID, "x and y must not alias");
+  return bmv_float_transposed(g, d_x, d_y, alpha, d_scale, add, as_stream(stream));
+}

@@ -1,0 +1,83 @@
+// The device-resident B2SR graph behind the opaque gbo_graph handle, and the
+// warp work-item schedule that balances power-law block rows.
+#pragma once
+
+#include "common.cuh"
+
+// One warp-group work item: tiles [t0, t1) of block row `row`.  A block row
+// with more tiles than the chunk size is split into several items; those
+// write partial results into scratch `slot` and a reduce kernel combines
+// them in slot order (deterministic, also for floating point).
+struct __align__(16) gbo_item {
+  int row, t0, t1, slot;  // slot = -1: the item covers its whole row
+};
+// A split block row: its partial results live in slots [slot0, slot0+n).
+struct __align__(16) gbo_split {
+  int row, slot0, nslots, pad;
+};
+
+struct gbo_graph {
+  int nrows = 0, ncols = 0, b = 0, layout = GBO_LAYOUT_ROW;
+  int nbr = 0, nbc = 0;
+  long long nblk = 0, nnz = -1;
+  int* rowptr = nullptr;   // nbr+1
+  int* colind = nullptr;   // nblk
+  void* val = nullptr;     // nblk*b words
+  int* outdeg = nullptr;   // ncols (column counts of P), may be null
+  float* invdeg = nullptr; // 1/outdeg (0 where outdeg == 0), may be null
+  bool owns_b2sr = true;
+  bool owns_outdeg = true;
+  // balanced schedule
+  int chunk = 0;
+  int nitems = 0;
+  gbo_item* items = nullptr;
+  int nsplit = 0;
+  gbo_split* splits = nullptr;
+  int nslots = 0;
+  // per-handle workspace for BMV split partials (grown on demand)
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+  long long device_bytes = 0;
+  // device state and captured CUDA graphs of the iteration loops
+  struct AlgoState* algo = nullptr;
+};
+
+namespace gbo {
+
+// Chunk (tiles per work item) for a tile width.
+inline int chunk_for(int b) {
+  switch (b) {
+    case 4: return 2048;
+    case 8: return 1024;
+    case 16: return 512;
+    case 32: return 256;
+    default: return 128;
+  }
+}
+
+// Work items processed per warp: 32/b groups for b <= 32, one for b = 64.
+inline int groups_per_warp(int b) { return b >= 32 ? 1 : 32 / b; }
+
+// Build items/splits for g (rowptr must be set).  Allocates g->items/splits.
+int build_schedule(gbo_graph* g, cudaStream_t stream);
+
+// Ensure g->ws has at least `bytes` (contents undefined).
+int ensure_workspace(gbo_graph* g, size_t bytes, cudaStream_t stream);
+
+// Pack CSR (device pointers) into B2SR owned by g.  Sets nblk, rowptr, colind,
+// val.  Synchronises the stream once (to size the tile arrays).
+int pack_into(gbo_graph* g, const int* d_rowptr, const int* d_colind, int nrows, int ncols,
+              long long nnz, int b, int layout, cudaStream_t stream);
+
+// Column counts of a CSR (device) -> g->outdeg, g->invdeg.
+int compute_outdeg_from_cols(gbo_graph* g, const int* d_colind, long long nnz, int ncols,
+                             cudaStream_t stream);
+int compute_outdeg_from_rowptr(gbo_graph* g, const int* d_rowptr, int nrows, cudaStream_t stream);
+// Out-degrees given on the host (n ints) -> g->outdeg, g->invdeg.
+int upload_outdeg(gbo_graph* g, const int* h_deg, int n, cudaStream_t stream);
+// inv[i] = 1/deg[i] (0 where deg is 0).
+void launch_invdeg(const int* d_deg, int n, float* d_inv, cudaStream_t stream);
+// Release the algorithm state of g (called by gbo_graph_free).
+void free_algo_state(gbo_graph* g);
+
+}  // namespace gbo

@@ -1,0 +1,693 @@
+// B2SR packing on the device (replaces the host-serial csr2bsr_batch_*,
+// algorithm/csr2bsr_batch_bsrbmv.cu:9-946, and bsrbmm/csr2bsr_batch.cu).
+//
+// The reference walks block rows on the host, runs cuSPARSE csr2bsr into a
+// dense float b x b buffer per slab and packs it with ToBit*Col.  Here one
+// warp lane owns one CSR row of a slab of b rows (b <= 32: 32/b slabs per
+// warp; b = 64: each lane owns rows r and r+32).  Because CSR rows are
+// sorted, the slab's tiles come out in ascending block-column order by a
+// b-way merge: every step takes the smallest head block column m over the
+// slab's rows (a segmented shuffle min), each lane ORs the bits of all its
+// entries in block column m into its tile row word, and the group emits one
+// tile.  A count pass sizes each block row; a scan gives bsrRowPtr; a fill
+// pass writes bsrColInd and the tile words (one coalesced store of b words).
+#include <algorithm>
+#include "graph.cuh"
+
+namespace gbo {
+
+namespace {
+
+constexpr int kPackTPB = 256;
+
+template <int B>
+struct SlabMap {
+  // lanes per slab and slabs per warp
+  static constexpr int W = B >= 32 ? 32 : B;
+  static constexpr int G = 32 / W;
+  static constexpr int RPL = B > 32 ? 2 : 1;  // rows per lane
+};
+
+__device__ __forceinline__ int seg_min(int v, int width) {
+  for (int o = width >> 1; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Per-lane cursor over one CSR row.
+struct RowCursor {
+  long long pos, end;
+  int prev;
+};
+
+__device__ __forceinline__ void init_cursor(RowCursor& c, const int* __restrict__ rowptr, int row,
+                                            int nrows, long long nnz, unsigned* derr) {
+  c.pos = 0;
+  c.end = 0;
+  c.prev = -1;
+  if (row < nrows) {
+    long long a = rowptr[row], e = rowptr[row + 1];
+    if (a < 0 || e < a || e > nnz) {
+      atomicOr(derr, DERR_ROWPTR);
+    } else {
+      c.pos = a;
+      c.end = e;
+    }
+  }
+}
+
+template <int B>
+__device__ __forceinline__ int head_of(const RowCursor& c, const int* __restrict__ colind) {
+  return c.pos < c.end ? colind[c.pos] / B : kINF;
+}
+
+// Consume all entries of block column m from the cursor; OR their bits.
+template <int B, typename WT>
+__device__ __forceinline__ void consume(RowCursor& c, const int* __restrict__ colind, int m,
+                                        int ncols, WT& word, unsigned* derr, bool build) {
+  while (c.pos < c.end) {
+    int col = colind[c.pos];
+    if (col / B != m) break;
+    if (col < c.prev) atomicOr(derr, DERR_UNSORTED);
+    if (col < 0 || col >= ncols) atomicOr(derr, DERR_COL_BOUNDS);
+    c.prev = col;
+    if (build) word |= (WT)((WT)1 << (B - 1 - ((unsigned)col % B)));
+    ++c.pos;
+  }
+}
+
+// After a lane's row ends, any remaining (unsorted) entries are still
+// consumed by the merge; a head < previous column marks the row unsorted.
+template <int B>
+__device__ __forceinline__ void check_head(const RowCursor& c, const int* __restrict__ colind,
+                                           unsigned* derr) {
+  if (c.pos < c.end && c.prev >= 0 && colind[c.pos] < c.prev) atomicOr(derr, DERR_UNSORTED);
+}
+
+// COUNT (build=false) and FILL (build=true) share one body.
+template <int B, bool BUILD>
+__global__ void __launch_bounds__(kPackTPB) k_pack(const int* __restrict__ rowptr,
+                                                   const int* __restrict__ colind, int nrows,
+                                                   int ncols, long long nnz, int nbr,
+                                                   int* __restrict__ counts,
+                                                   const int* __restrict__ bsr_rowptr,
+                                                   int* __restrict__ bsr_colind,
+                                                   typename Word<B>::T* __restrict__ bsr_val,
+                                                   int layout, unsigned* derr) {
+  using WT = typename Word<B>::T;
+  using M = SlabMap<B>;
+  const unsigned lane = threadIdx.x & 31;
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int g = lane / M::W;          // slab within warp
+  const int r = lane % M::W;          // row within slab (first row for B=64)
+  const long long slab = warp * M::G + g;
+  if (warp * M::G >= nbr) return;     // whole warp idle (uniform)
+  const bool slab_ok = slab < nbr;
+
+  RowCursor c0, c1;
+  const long long row0 = slab * B + r;
+  init_cursor(c0, rowptr, slab_ok && row0 < nrows ? (int)row0 : nrows, nrows, nnz, derr);
+  if (M::RPL == 2) {
+    const long long row1 = slab * B + 32 + r;
+    init_cursor(c1, rowptr, slab_ok && row1 < nrows ? (int)row1 : nrows, nrows, nnz, derr);
+  }
+
+  long long out = 0;
+  if (BUILD && slab_ok) out = bsr_rowptr[slab];
+  int ntile = 0;
+
+  while (true) {
+    int h = head_of<B>(c0, colind);
+    if (M::RPL == 2) h = min(h, head_of<B>(c1, colind));
+    const int m = seg_min(h, M::W);
+    if (!__any_sync(0xffffffffu, m != kINF)) break;
+    WT w0 = 0, w1 = 0;
+    if (m != kINF) {
+      consume<B, WT>(c0, colind, m, ncols, w0, derr, BUILD);
+      check_head<B>(c0, colind, derr);
+      if (M::RPL == 2) {
+        consume<B, WT>(c1, colind, m, ncols, w1, derr, BUILD);
+        check_head<B>(c1, colind, derr);
+      }
+    }
+    if (BUILD) {
+      const long long tile = out + ntile;
+      if (layout == GBO_LAYOUT_ROW) {
+        if (m != kINF) {
+          if (r == 0) bsr_colind[tile] = m;
+          bsr_val[tile * B + r] = w0;
+          if (M::RPL == 2) bsr_val[tile * B + 32 + r] = w1;
+        }
+      } else {
+        // transpose the b x b bit tile with ballots: column word c has row r
+        // at bit (b-1-r).
+        if (M::RPL == 1) {
+          WT mine = 0;
+#pragma unroll 4
+          for (int cc = 0; cc < B; ++cc) {
+            unsigned bal = __ballot_sync(0xffffffffu, (w0 >> (B - 1 - cc)) & 1);
+            unsigned seg = (bal >> (g * M::W)) & seg_mask<B>();
+            unsigned colw = __brev(seg) >> (32 - (B < 32 ? B : 32));
+            if (r == cc) mine = (WT)colw;
+          }
+          if (m != kINF) {
+            if (r == 0) bsr_colind[tile] = m;
+            bsr_val[tile * B + r] = mine;
+          }
+        } else {
+          unsigned long long lo_w = 0, hi_w = 0;
+#pragma unroll 4
+          for (int cc = 0; cc < 64; ++cc) {
+            unsigned lo = __ballot_sync(0xffffffffu, (unsigned)((w0 >> (63 - cc)) & 1ull));
+            unsigned hi = __ballot_sync(0xffffffffu, (unsigned)((w1 >> (63 - cc)) & 1ull));
+            unsigned long long colw = __brevll(((unsigned long long)hi << 32) | lo);
+            if (cc == (int)r) lo_w = colw;
+            if (cc == (int)r + 32) hi_w = colw;
+          }
+          if (m != kINF) {
+            if (r == 0) bsr_colind[tile] = m;
+            bsr_val[tile * B + r] = (WT)lo_w;
+            bsr_val[tile * B + 32 + r] = (WT)hi_w;
+          }
+        }
+      }
+    }
+    if (m != kINF) ++ntile;
+  }
+  if (!BUILD && slab_ok && r == 0) counts[slab] = ntile;
+}
+
+// ---------------------------------------------------------------- scan
+constexpr int kScanTPB = 1024;
+
+__global__ void k_scan_block_sums(const int* __restrict__ in, long long n,
+                                  long long* __restrict__ sums) {
+  __shared__ long long sh[32];
+  long long i = (long long)blockIdx.x * kScanTPB + threadIdx.x;
+  long long v = i < n ? in[i] : 0;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    long long s = sh[threadIdx.x];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) sums[blockIdx.x] = s;
+  }
+}
+
+// Exclusive scan of up to kScanTPB*kScanTPB block sums by one block (loop).
+__global__ void k_scan_sums(long long* __restrict__ sums, long long nb, long long* total) {
+  __shared__ long long sh[32];
+  __shared__ long long carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (long long base = 0; base < nb; base += kScanTPB) {
+    long long i = base + threadIdx.x;
+    long long v = i < nb ? sums[i] : 0;
+    // inclusive warp scan
+    long long x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      long long y = __shfl_up_sync(0xffffffffu, x, o);
+      if ((threadIdx.x & 31) >= (unsigned)o) x += y;
+    }
+    if ((threadIdx.x & 31) == 31) sh[threadIdx.x >> 5] = x;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      long long s = sh[threadIdx.x];
+      for (int o = 1; o < 32; o <<= 1) {
+        long long y = __shfl_up_sync(0xffffffffu, s, o);
+        if (threadIdx.x >= (unsigned)o) s += y;
+      }
+      sh[threadIdx.x] = s;
+    }
+    __syncthreads();
+    long long warp_prefix = (threadIdx.x >> 5) ? sh[(threadIdx.x >> 5) - 1] : 0;
+    long long incl = x + warp_prefix + carry;
+    if (i < nb) sums[i] = incl - v;
+    __syncthreads();
+    if (threadIdx.x == kScanTPB - 1) carry = incl;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void k_scan_apply(const int* __restrict__ in, long long n,
+                             const long long* __restrict__ sums, int* __restrict__ out,
+                             const long long* __restrict__ total) {
+  __shared__ long long sh[32];
+  long long i = (long long)blockIdx.x * kScanTPB + threadIdx.x;
+  long long v = i < n ? in[i] : 0;
+  long long x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    long long y = __shfl_up_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) >= (unsigned)o) x += y;
+  }
+  if ((threadIdx.x & 31) == 31) sh[threadIdx.x >> 5] = x;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    long long s = sh[threadIdx.x];
+    for (int o = 1; o < 32; o <<= 1) {
+      long long y = __shfl_up_sync(0xffffffffu, s, o);
+      if (threadIdx.x >= (unsigned)o) s += y;
+    }
+    sh[threadIdx.x] = s;
+  }
+  __syncthreads();
+  long long warp_prefix = (threadIdx.x >> 5) ? sh[(threadIdx.x >> 5) - 1] : 0;
+  long long excl = x - v + warp_prefix + sums[blockIdx.x];
+  if (i < n) out[i] = (int)(excl > 2147483647LL ? 2147483647LL : excl);
+  if (i == 0) out[n] = (int)(*total > 2147483647LL ? 2147483647LL : *total);
+}
+
+// ------------------------------------------------------- vector packing
+template <int B>
+__global__ void k_pack_vec(const float* __restrict__ xf, const int32_t* __restrict__ xi, int n,
+                           typename Word<B>::T* __restrict__ bits, long long nwords) {
+  using WT = typename Word<B>::T;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned lane = threadIdx.x & 31;
+  bool v = false;
+  if (i < n) v = xf ? (xf[i] > 0.f) : (xi[i] > 0);
+  unsigned bal = __brev(__ballot_sync(0xffffffffu, v));  // element (base+k) at bit 31-k
+  const long long base = i - lane;                        // first element of this warp
+  if (B == 64) {
+    // two warps make one 64-bit word: even warp -> high half, odd warp -> low half
+    const long long word = base / 64;
+    if (lane == 0 && word < nwords) {
+      unsigned long long* wp = reinterpret_cast<unsigned long long*>(bits) + word;
+      unsigned long long part = ((base / 32) & 1) ? (unsigned long long)bal
+                                                  : ((unsigned long long)bal << 32);
+      atomicOr(wp, part);
+    }
+  } else {
+    constexpr int S = 32 / B;  // segments per warp chunk
+    if ((int)lane < S) {
+      const long long word = base / B + lane;
+      if (word < nwords) {
+        unsigned seg = (bal >> (32 - B * (lane + 1))) & seg_mask<B>();
+        bits[word] = (WT)seg;
+      }
+    }
+  }
+}
+
+template <int B>
+__global__ void k_unpack_vec(const typename Word<B>::T* __restrict__ bits, int n,
+                             int32_t* __restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  unsigned long long w = (unsigned long long)bits[i / B];
+  out[i] = (int32_t)((w >> (B - 1 - (i % B))) & 1ull);
+}
+
+// ------------------------------------------------------------ out-degree
+__global__ void k_col_hist(const int* __restrict__ colind, long long nnz, int ncols,
+                           int* __restrict__ deg) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nnz;
+       i += (long long)gridDim.x * blockDim.x) {
+    int c = colind[i];
+    if (c >= 0 && c < ncols) atomicAdd(deg + c, 1);
+  }
+}
+__global__ void k_row_len(const int* __restrict__ rowptr, int nrows, int* __restrict__ deg) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nrows) deg[i] = rowptr[i + 1] - rowptr[i];
+}
+__global__ void k_inv(const int* __restrict__ deg, int n, float* __restrict__ inv) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) inv[i] = deg[i] > 0 ? 1.0f / (float)deg[i] : 0.0f;
+}
+
+// ------------------------------------------------------------- schedule
+__global__ void k_sched_counts(const int* __restrict__ rowptr, int nbr, int chunk,
+                               int* __restrict__ nchunk, int* __restrict__ nslot,
+                               int* __restrict__ issplit) {
+  long long R = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (R >= nbr) return;
+  int len = rowptr[R + 1] - rowptr[R];
+  int k = len <= chunk ? 1 : (len + chunk - 1) / chunk;
+  nchunk[R] = k;
+  nslot[R] = k > 1 ? k : 0;
+  issplit[R] = k > 1 ? 1 : 0;
+}
+
+__global__ void k_sched_fill(const int* __restrict__ rowptr, int nbr, int chunk,
+                             const int* __restrict__ item_off, const int* __restrict__ slot_off,
+                             const int* __restrict__ split_off, gbo_item* __restrict__ items,
+                             gbo_split* __restrict__ splits) {
+  long long R = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (R >= nbr) return;
+  int t0 = rowptr[R], t1 = rowptr[R + 1];
+  int len = t1 - t0;
+  int k = len <= chunk ? 1 : (len + chunk - 1) / chunk;
+  int base = item_off[R];
+  if (k == 1) {
+    items[base] = gbo_item{(int)R, t0, t1, -1};
+  } else {
+    int s0 = slot_off[R];
+    for (int q = 0; q < k; ++q) {
+      int a = t0 + q * chunk;
+      int e = min(t1, a + chunk);
+      items[base + q] = gbo_item{(int)R, a, e, s0 + q};
+    }
+    splits[split_off[R]] = gbo_split{(int)R, s0, k, 0};
+  }
+}
+
+template <int B>
+int launch_pack(bool build, const int* rowptr, const int* colind, int nrows, int ncols,
+                long long nnz, int nbr, int* counts, const int* bsr_rowptr, int* bsr_colind,
+                void* bsr_val, int layout, unsigned* derr, cudaStream_t s) {
+  using M = SlabMap<B>;
+  long long warps = (nbr + M::G - 1) / M::G;
+  unsigned grid = blocks_for_warps(warps, kPackTPB / 32);
+  if (build)
+    k_pack<B, true><<<grid, kPackTPB, 0, s>>>(rowptr, colind, nrows, ncols, nnz, nbr, counts,
+                                              bsr_rowptr, bsr_colind,
+                                              reinterpret_cast<typename Word<B>::T*>(bsr_val),
+                                              layout, derr);
+  else
+    k_pack<B, false><<<grid, kPackTPB, 0, s>>>(rowptr, colind, nrows, ncols, nnz, nbr, counts,
+                                               bsr_rowptr, bsr_colind,
+                                               reinterpret_cast<typename Word<B>::T*>(bsr_val),
+                                               layout, derr);
+  GBO_CUDA_TRY(cudaGetLastError());
+  return GBO_OK;
+}
+
+int dispatch_pack(int b, bool build, const int* rowptr, const int* colind, int nrows, int ncols,
+                  long long nnz, int nbr, int* counts, const int* bsr_rowptr, int* bsr_colind,
+                  void* bsr_val, int layout, unsigned* derr, cudaStream_t s) {
+  switch (b) {
+    case 4: return launch_pack<4>(build, rowptr, colind, nrows, ncols, nnz, nbr, counts, bsr_rowptr, bsr_colind, bsr_val, layout, derr, s);
+    case 8: return launch_pack<8>(build, rowptr, colind, nrows, ncols, nnz, nbr, counts, bsr_rowptr, bsr_colind, bsr_val, layout, derr, s);
+    case 16: return launch_pack<16>(build, rowptr, colind, nrows, ncols, nnz, nbr, counts, bsr_rowptr, bsr_colind, bsr_val, layout, derr, s);
+    case 32: return launch_pack<32>(build, rowptr, colind, nrows, ncols, nnz, nbr, counts, bsr_rowptr, bsr_colind, bsr_val, layout, derr, s);
+    case 64: return launch_pack<64>(build, rowptr, colind, nrows, ncols, nnz, nbr, counts, bsr_rowptr, bsr_colind, bsr_val, layout, derr, s);
+  }
+  return fail(GBO_ERR_INVALID, "tile_bits must be 4, 8, 16, 32 or 64");
+}
+
+int derr_to_status(unsigned e) {
+  if (e & DERR_ROWPTR) return fail(GBO_ERR_BOUNDS, "CSR row pointers are not monotone within [0, nnz]");
+  if (e & DERR_COL_BOUNDS) return fail(GBO_ERR_BOUNDS, "CSR column index outside [0, ncols)");
+  if (e & DERR_UNSORTED) return fail(GBO_ERR_UNSORTED, "CSR column indices are not ascending inside a row");
+  return GBO_OK;
+}
+
+// Small device scratch for the scan + error word, stream-ordered.
+struct ScanScratch {
+  long long* sums = nullptr;
+  long long* total = nullptr;
+  unsigned* derr = nullptr;
+};
+
+}  // namespace
+
+int exclusive_scan_i32(const int* d_in, int* d_out, long long n, long long* d_total,
+                       cudaStream_t s) {
+  long long nb = (n + kScanTPB - 1) / kScanTPB;
+  if (nb < 1) nb = 1;
+  long long* sums = nullptr;
+  GBO_CUDA_TRY(cudaMallocAsync(&sums, sizeof(long long) * nb, s));
+  k_scan_block_sums<<<(unsigned)nb, kScanTPB, 0, s>>>(d_in, n, sums);
+  k_scan_sums<<<1, kScanTPB, 0, s>>>(sums, nb, d_total);
+  k_scan_apply<<<(unsigned)nb, kScanTPB, 0, s>>>(d_in, n, sums, d_out, d_total);
+  cudaError_t e = cudaGetLastError();
+  cudaFreeAsync(sums, s);
+  if (e != cudaSuccess) return fail_cuda(e, "scan kernels");
+  return GBO_OK;
+}
+
+// nnzb per block row: counts -> bsr_rowptr (device) and total (host).
+static int nnzb_impl(const int* rowptr, const int* colind, int nrows, int ncols, long long nnz,
+                     int b, int* bsr_rowptr, long long* h_total, cudaStream_t s) {
+  const int nbr = (nrows + b - 1) / b;
+  int* counts = nullptr;
+  long long* d_total = nullptr;
+  unsigned* derr = nullptr;
+  GBO_CUDA_TRY(cudaMallocAsync(&counts, sizeof(int) * (size_t)(nbr > 0 ? nbr : 1), s));
+  GBO_CUDA_TRY(cudaMallocAsync(&d_total, sizeof(long long) + sizeof(unsigned) * 2, s));
+  derr = reinterpret_cast<unsigned*>(d_total + 1);
+  GBO_CUDA_TRY(cudaMemsetAsync(derr, 0, sizeof(unsigned), s));
+  int st = GBO_OK;
+  if (nbr > 0) {
+    st = dispatch_pack(b, false, rowptr, colind, nrows, ncols, nnz, nbr, counts, nullptr, nullptr,
+                       nullptr, GBO_LAYOUT_ROW, derr, s);
+    if (st == GBO_OK) st = exclusive_scan_i32(counts, bsr_rowptr, nbr, d_total, s);
+  } else {
+    GBO_CUDA_TRY(cudaMemsetAsync(bsr_rowptr, 0, sizeof(int), s));
+    GBO_CUDA_TRY(cudaMemsetAsync(d_total, 0, sizeof(long long), s));
+  }
+  long long tot = 0;
+  unsigned herr = 0;
+  if (st == GBO_OK) {
+    cudaError_t e1 = cudaMemcpyAsync(&tot, d_total, sizeof(long long), cudaMemcpyDeviceToHost, s);
+    cudaError_t e2 = cudaMemcpyAsync(&herr, derr, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+    cudaError_t e3 = cudaStreamSynchronize(s);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
+      st = fail_cuda(e3 != cudaSuccess ? e3 : (e1 != cudaSuccess ? e1 : e2), "nnzb readback");
+  }
+  cudaFreeAsync(counts, s);
+  cudaFreeAsync(d_total, s);
+  if (st != GBO_OK) return st;
+  GBO_TRY(derr_to_status(herr));
+  if (tot > 2147483647LL) return fail(GBO_ERR_OVERFLOW, "more than 2^31-1 tiles; use a wider tile");
+  *h_total = tot;
+  return GBO_OK;
+}
+
+static int fill_impl(const int* rowptr, const int* colind, int nrows, int ncols, long long nnz,
+                     int b, int layout, const int* bsr_rowptr, int* bsr_colind, void* bsr_val,
+                     cudaStream_t s, bool check) {
+  const int nbr = (nrows + b - 1) / b;
+  if (nbr == 0) return GBO_OK;
+  unsigned* derr = nullptr;
+  GBO_CUDA_TRY(cudaMallocAsync(&derr, sizeof(unsigned), s));
+  GBO_CUDA_TRY(cudaMemsetAsync(derr, 0, sizeof(unsigned), s));
+  int st = dispatch_pack(b, true, rowptr, colind, nrows, ncols, nnz, nbr, nullptr, bsr_rowptr,
+                         bsr_colind, bsr_val, layout, derr, s);
+  unsigned herr = 0;
+  if (st == GBO_OK && check) {
+    cudaError_t e1 = cudaMemcpyAsync(&herr, derr, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+    cudaError_t e2 = cudaStreamSynchronize(s);
+    if (e1 != cudaSuccess || e2 != cudaSuccess) st = fail_cuda(e1 != cudaSuccess ? e1 : e2, "pack");
+  }
+  cudaFreeAsync(derr, s);
+  if (st != GBO_OK) return st;
+  return derr_to_status(herr);
+}
+
+int pack_into(gbo_graph* g, const int* d_rowptr, const int* d_colind, int nrows, int ncols,
+              long long nnz, int b, int layout, cudaStream_t s) {
+  g->nrows = nrows;
+  g->ncols = ncols;
+  g->b = b;
+  g->layout = layout;
+  g->nbr = (nrows + b - 1) / b;
+  g->nbc = (ncols + b - 1) / b;
+  g->nnz = nnz;
+  GBO_CUDA_TRY(cudaMalloc(&g->rowptr, sizeof(int) * (size_t)(g->nbr + 1)));
+  long long nblk = 0;
+  GBO_TRY(nnzb_impl(d_rowptr, d_colind, nrows, ncols, nnz, b, g->rowptr, &nblk, s));
+  g->nblk = nblk;
+  size_t vb = (size_t)nblk * (size_t)b * (size_t)word_bytes(b);
+  GBO_CUDA_TRY(cudaMalloc(&g->colind, sizeof(int) * (size_t)(nblk > 0 ? nblk : 1)));
+  // pad the tile array to 16 bytes so vector loads past the end stay inside
+  GBO_CUDA_TRY(cudaMalloc(&g->val, vb + 16));
+  g->device_bytes += sizeof(int) * (g->nbr + 1) + sizeof(int) * nblk + vb + 16;
+  GBO_TRY(fill_impl(d_rowptr, d_colind, nrows, ncols, nnz, b, layout, g->rowptr, g->colind,
+                    g->val, s, false));
+  return GBO_OK;
+}
+
+int compute_outdeg_from_cols(gbo_graph* g, const int* d_colind, long long nnz, int ncols,
+                             cudaStream_t s) {
+  GBO_CUDA_TRY(cudaMalloc(&g->outdeg, sizeof(int) * (size_t)(ncols > 0 ? ncols : 1)));
+  GBO_CUDA_TRY(cudaMalloc(&g->invdeg, sizeof(float) * (size_t)(ncols > 0 ? ncols : 1)));
+  g->device_bytes += 8LL * ncols;
+  GBO_CUDA_TRY(cudaMemsetAsync(g->outdeg, 0, sizeof(int) * (size_t)ncols, s));
+  if (nnz > 0) {
+    unsigned grid = (unsigned)std::min<long long>((nnz + 255) / 256, 148LL * 64);
+    k_col_hist<<<grid, 256, 0, s>>>(d_colind, nnz, ncols, g->outdeg);
+  }
+  if (ncols > 0) k_inv<<<blocks_for(ncols, 256), 256, 0, s>>>(g->outdeg, ncols, g->invdeg);
+  GBO_CUDA_TRY(cudaGetLastError());
+  return GBO_OK;
+}
+
+int compute_outdeg_from_rowptr(gbo_graph* g, const int* d_rowptr, int nrows, cudaStream_t s) {
+  GBO_CUDA_TRY(cudaMalloc(&g->outdeg, sizeof(int) * (size_t)(nrows > 0 ? nrows : 1)));
+  GBO_CUDA_TRY(cudaMalloc(&g->invdeg, sizeof(float) * (size_t)(nrows > 0 ? nrows : 1)));
+  g->device_bytes += 8LL * nrows;
+  if (nrows > 0) {
+    k_row_len<<<blocks_for(nrows, 256), 256, 0, s>>>(d_rowptr, nrows, g->outdeg);
+    k_inv<<<blocks_for(nrows, 256), 256, 0, s>>>(g->outdeg, nrows, g->invdeg);
+  }
+  GBO_CUDA_TRY(cudaGetLastError());
+  return GBO_OK;
+}
+
+void launch_invdeg(const int* d_deg, int n, float* d_inv, cudaStream_t s) {
+  if (n > 0) k_inv<<<blocks_for(n, 256), 256, 0, s>>>(d_deg, n, d_inv);
+}
+
+int upload_outdeg(gbo_graph* g, const int* h_deg, int n, cudaStream_t s) {
+  GBO_CUDA_TRY(cudaMalloc(&g->outdeg, sizeof(int) * (size_t)(n > 0 ? n : 1)));
+  GBO_CUDA_TRY(cudaMalloc(&g->invdeg, sizeof(float) * (size_t)(n > 0 ? n : 1)));
+  g->device_bytes += 8LL * n;
+  if (n > 0) {
+    GBO_CUDA_TRY(cudaMemcpyAsync(g->outdeg, h_deg, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, s));
+    launch_invdeg(g->outdeg, n, g->invdeg, s);
+  }
+  GBO_CUDA_TRY(cudaGetLastError());
+  return GBO_OK;
+}
+
+int build_schedule(gbo_graph* g, cudaStream_t s) {
+  const int nbr = g->nbr;
+  g->chunk = chunk_for(g->b);
+  if (nbr == 0) {
+    g->nitems = 0;
+    g->nsplit = 0;
+    g->nslots = 0;
+    return GBO_OK;
+  }
+  int *nchunk = nullptr, *nslot = nullptr, *issplit = nullptr;
+  int *item_off = nullptr, *slot_off = nullptr, *split_off = nullptr;
+  long long* tot = nullptr;
+  size_t n1 = (size_t)nbr + 1;
+  GBO_CUDA_TRY(cudaMallocAsync(&nchunk, sizeof(int) * n1 * 6, s));
+  nslot = nchunk + n1;
+  issplit = nslot + n1;
+  item_off = issplit + n1;
+  slot_off = item_off + n1;
+  split_off = slot_off + n1;
+  GBO_CUDA_TRY(cudaMallocAsync(&tot, sizeof(long long) * 3, s));
+  k_sched_counts<<<blocks_for(nbr, 256), 256, 0, s>>>(g->rowptr, nbr, g->chunk, nchunk, nslot,
+                                                      issplit);
+  GBO_TRY(exclusive_scan_i32(nchunk, item_off, nbr, tot + 0, s));
+  GBO_TRY(exclusive_scan_i32(nslot, slot_off, nbr, tot + 1, s));
+  GBO_TRY(exclusive_scan_i32(issplit, split_off, nbr, tot + 2, s));
+  long long h[3];
+  GBO_CUDA_TRY(cudaMemcpyAsync(h, tot, sizeof(h), cudaMemcpyDeviceToHost, s));
+  GBO_CUDA_TRY(cudaStreamSynchronize(s));
+  g->nitems = (int)h[0];
+  g->nslots = (int)h[1];
+  g->nsplit = (int)h[2];
+  GBO_CUDA_TRY(cudaMalloc(&g->items, sizeof(gbo_item) * (size_t)(g->nitems > 0 ? g->nitems : 1)));
+  GBO_CUDA_TRY(cudaMalloc(&g->splits, sizeof(gbo_split) * (size_t)(g->nsplit > 0 ? g->nsplit : 1)));
+  g->device_bytes += sizeof(gbo_item) * (long long)g->nitems + sizeof(gbo_split) * (long long)g->nsplit;
+  k_sched_fill<<<blocks_for(nbr, 256), 256, 0, s>>>(g->rowptr, nbr, g->chunk, item_off, slot_off,
+                                                    split_off, g->items, g->splits);
+  GBO_CUDA_TRY(cudaGetLastError());
+  cudaFreeAsync(nchunk, s);
+  cudaFreeAsync(tot, s);
+  return GBO_OK;
+}
+
+int ensure_workspace(gbo_graph* g, size_t bytes, cudaStream_t s) {
+  if (g->ws_bytes >= bytes) return GBO_OK;
+  if (g->ws) {
+    GBO_CUDA_TRY(cudaStreamSynchronize(s));
+    GBO_CUDA_TRY(cudaFree(g->ws));
+    g->device_bytes -= (long long)g->ws_bytes;
+    g->ws = nullptr;
+    g->ws_bytes = 0;
+  }
+  size_t want = bytes + (bytes >> 3) + 256;
+  GBO_CUDA_TRY(cudaMalloc(&g->ws, want));
+  g->ws_bytes = want;
+  g->device_bytes += (long long)want;
+  return GBO_OK;
+}
+
+}  // namespace gbo
+
+// ------------------------------------------------------------------ C ABI
+using namespace gbo;
+
+extern "C" int gbo_b2sr_nnzb(const int* d_csrRowPtr, const int* d_csrColInd, int nrows,
+                             int ncols, int nnz, int tile_bits, int* d_bsrRowPtr, int* h_nblocks,
+                             gbo_stream_t stream) {
+  clear_error();
+  if (!valid_tile_bits(tile_bits)) return fail(GBO_ERR_INVALID, "tile_bits must be 4, 8, 16, 32 or 64");
+  if (nrows < 0 || ncols < 0 || nnz < 0 || !d_csrRowPtr || !d_bsrRowPtr || !h_nblocks ||
+      (nnz > 0 && !d_csrColInd))
+    return fail(GBO_ERR_INVALID, "gbo_b2sr_nnzb: bad argument");
+  long long tot = 0;
+  GBO_TRY(nnzb_impl(d_csrRowPtr, d_csrColInd, nrows, ncols, nnz, tile_bits, d_bsrRowPtr, &tot,
+                    as_stream(stream)));
+  *h_nblocks = (int)tot;
+  return GBO_OK;
+}
+
+extern "C" int gbo_b2sr_pack(const int* d_csrRowPtr, const int* d_csrColInd, int nrows,
+                             int ncols, int nnz, int tile_bits, int layout,
+                             const int* d_bsrRowPtr, int* d_bsrColInd, void* d_bsrVal,
+                             gbo_stream_t stream) {
+  clear_error();
+  if (!valid_tile_bits(tile_bits)) return fail(GBO_ERR_INVALID, "tile_bits must be 4, 8, 16, 32 or 64");
+  if (layout != GBO_LAYOUT_ROW && layout != GBO_LAYOUT_COL)
+    return fail(GBO_ERR_INVALID, "layout must be GBO_LAYOUT_ROW or GBO_LAYOUT_COL");
+  if (nrows < 0 || ncols < 0 || nnz < 0 || !d_csrRowPtr || !d_bsrRowPtr ||
+      (nnz > 0 && (!d_csrColInd || !d_bsrColInd || !d_bsrVal)))
+    return fail(GBO_ERR_INVALID, "gbo_b2sr_pack: bad argument");
+  return fill_impl(d_csrRowPtr, d_csrColInd, nrows, ncols, nnz, tile_bits, layout, d_bsrRowPtr,
+                   d_bsrColInd, d_bsrVal, as_stream(stream), true);
+}
+
+template <int B>
+static int pack_vec_impl(const float* xf, const int32_t* xi, int n, void* bits, cudaStream_t s) {
+  long long nw = ((long long)n + B - 1) / B;
+  if (B == 64) GBO_CUDA_TRY(cudaMemsetAsync(bits, 0, sizeof(unsigned long long) * nw, s));
+  long long threads = ((long long)n + 31) / 32 * 32;
+  if (B == 64) threads = nw * 64;  // whole 64-element words
+  if (threads == 0) return GBO_OK;
+  k_pack_vec<B><<<blocks_for(threads, 256), 256, 0, s>>>(
+      xf, xi, n, reinterpret_cast<typename Word<B>::T*>(bits), nw);
+  GBO_CUDA_TRY(cudaGetLastError());
+  return GBO_OK;
+}
+
+static int pack_vec_dispatch(const float* xf, const int32_t* xi, int n, int b, void* bits,
+                             gbo_stream_t stream) {
+  clear_error();
+  if (!valid_tile_bits(b)) return fail(GBO_ERR_INVALID, "tile_bits must be 4, 8, 16, 32 or 64");
+  if (n < 0 || (n > 0 && (!bits || (!xf && !xi)))) return fail(GBO_ERR_INVALID, "pack_vector: bad argument");
+  cudaStream_t s = as_stream(stream);
+  switch (b) {
+    case 4: return pack_vec_impl<4>(xf, xi, n, bits, s);
+    case 8: return pack_vec_impl<8>(xf, xi, n, bits, s);
+    case 16: return pack_vec_impl<16>(xf, xi, n, bits, s);
+    case 32: return pack_vec_impl<32>(xf, xi, n, bits, s);
+    default: return pack_vec_impl<64>(xf, xi, n, bits, s);
+  }
+}
+
+extern "C" int gbo_pack_vector_f32(const float* d_x, int n, int tile_bits, void* d_bits,
+                                   gbo_stream_t stream) {
+  return pack_vec_dispatch(d_x, nullptr, n, tile_bits, d_bits, stream);
+}
+extern "C" int gbo_pack_vector_i32(const int32_t* d_x, int n, int tile_bits, void* d_bits,
+                                   gbo_stream_t stream) {
+  return pack_vec_dispatch(nullptr, d_x, n, tile_bits, d_bits, stream);
+}
+
+extern "C" int gbo_unpack_vector(const void* d_bits, int n, int tile_bits, int32_t* d_out,
+                                 gbo_stream_t stream) {
+  clear_error();
+  if (!valid_tile_bits(tile_bits)) return fail(GBO_ERR_INVALID, "tile_bits must be 4, 8, 16, 32 or 64");
+  if (n < 0 || (n > 0 && (!d_bits || !d_out))) return fail(GBO_ERR_INVALID, "unpack_vector: bad argument");
+  if (n == 0) return GBO_OK;
+  cudaStream_t s = as_stream(stream);
+  unsigned grid = blocks_for(n, 256);
+  switch (tile_bits) {
+    case 4: k_unpack_vec<4><<<grid, 256, 0, s>>>((const uint8_t*)d_bits, n, d_out); break;
+    case 8: k_unpack_vec<8><<<grid, 256, 0, s>>>((const uint8_t*)d_bits, n, d_out); break;
+    case 16: k_unpack_vec<16><<<grid, 256, 0, s>>>((const uint16_t*)d_bits, n, d_out); break;
+    case 32: k_unpack_vec<32><<<grid, 256, 0, s>>>((const uint32_t*)d_bits, n, d_out); break;
+    default: k_unpack_vec<64><<<grid, 256, 0, s>>>((const unsigned long long*)d_bits, n, d_out); break;
+  }
+  GBO_CUDA_TRY(cudaGetLastError());
+  return GBO_OK;
+}

@@ -1,0 +1,177 @@
+// Triangle counting by masked binary SpGEMM on B2SR tiles.
+//
+// Reference: bmm32_sparse_masked_v5 (bsrbmm/bsrbmm.cu:1214-1265) computes
+// sum over mask tiles (I,K) of L of sum_r sum_c M[r][c] * (L L^T)[I*b+r][K*b+c],
+// looking up B = L^T tiles (col layout) by binary search, and reduces into an
+// int32 (overflows past 2^31 triangles, bsrbmm/tc.cu:861-863).
+//
+// Here the L^T operand is never built: the col-layout tile (J,K) of L^T has
+// the same words as the row-layout tile (K,J) of L, so the intersection of
+// block rows I and K of L (restricted to block columns <= K) gives every
+// contributing pair.  One warp per mask tile probes the shorter of the two
+// sorted column lists into the longer with binary searches (32 probes per
+// step), and for each hit computes
+//   sum_r sum_{c in M_r} popc(A_(I,J)[r] & A_(K,J)[c])
+// with the K-tile rows broadcast by warp shuffles.  The count is uint64.
+#include "bmv.cuh"
+
+namespace gbo {
+
+namespace {
+
+constexpr int kTPB = 256;
+
+__device__ __forceinline__ int lower_bound_dev(const int* __restrict__ a, int lo, int hi, int key) {
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (a[mid] < key) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Block row of tile m: largest I with rowptr[I] <= m.
+__device__ __forceinline__ int row_of_tile(const int* __restrict__ rowptr, int nbr, int m) {
+  int lo = 0, hi = nbr;  // rowptr[0] = 0 <= m < rowptr[nbr]
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (rowptr[mid] <= m) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+template <int B>
+__global__ void __launch_bounds__(kTPB) k_tc(GView v, long long nblk,
+                                             unsigned long long* __restrict__ count) {
+  using WT = typename Word<B>::T;
+  constexpr int RPL = B > 32 ? 2 : 1;
+  const unsigned lane = threadIdx.x & 31;
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
+  unsigned long long acc = 0;
+  for (long long m = warp; m < nblk; m += nwarps) {
+    const int I = row_of_tile(v.rowptr, v.nbr, (int)m);
+    const int K = v.colind[m];
+    // mask rows of tile (I,K)
+    WT M0 = 0, M1 = 0;
+    if (lane < (unsigned)(B < 32 ? B : 32)) M0 = val[(size_t)m * B + lane];
+    if (RPL == 2) M1 = val[(size_t)m * B + 32 + lane];
+    // union of the mask columns over the tile's rows
+    unsigned long long U = (unsigned long long)M0 | (unsigned long long)M1;
+    {
+      unsigned lo = __reduce_or_sync(0xffffffffu, (unsigned)U);
+      unsigned hi = __reduce_or_sync(0xffffffffu, (unsigned)(U >> 32));
+      U = ((unsigned long long)hi << 32) | lo;
+    }
+    // list A: row I, tiles with block column <= K  -> [rowptr[I], m]
+    // list B: row K, all tiles (block columns <= K in a lower triangle)
+    const int a0 = v.rowptr[I], a1 = (int)m + 1;
+    const int b0 = v.rowptr[K], b1 = v.rowptr[K + 1];
+    const bool probe_a = (a1 - a0) <= (b1 - b0);
+    const int p0 = probe_a ? a0 : b0, p1 = probe_a ? a1 : b1;
+    const int s0 = probe_a ? b0 : a0, s1 = probe_a ? b1 : a1;
+    for (int base = p0; base < p1; base += 32) {
+      const int p = base + (int)lane;
+      int hit = -1;
+      if (p < p1) {
+        const int J = v.colind[p];
+        const int q = lower_bound_dev(v.colind, s0, s1, J);
+        if (q < s1 && v.colind[q] == J) hit = q;
+      }
+      unsigned found = __ballot_sync(0xffffffffu, hit >= 0);
+      while (found) {
+        const int src = __ffs(found) - 1;
+        found &= found - 1;
+        const int ph = __shfl_sync(0xffffffffu, p, src);
+        const int qh = __shfl_sync(0xffffffffu, hit, src);
+        const int ia = probe_a ? ph : qh;  // tile (I,J)
+        const int ib = probe_a ? qh : ph;  // tile (K,J)
+        WT A0 = 0, A1 = 0, Bw0 = 0, Bw1 = 0;
+        if (lane < (unsigned)(B < 32 ? B : 32)) {
+          A0 = val[(size_t)ia * B + lane];
+          Bw0 = val[(size_t)ib * B + lane];
+        }
+        if (RPL == 2) {
+          A1 = val[(size_t)ia * B + 32 + lane];
+          Bw1 = val[(size_t)ib * B + 32 + lane];
+        }
+        unsigned long long u = U << (64 - B);  // column c at bit 63-c
+        while (u) {
+          const int c = __clzll(u);
+          u &= ~(0x8000000000000000ull >> c);
+          WT bc;
+          if (RPL == 2)
+            bc = c < 32 ? (WT)__shfl_sync(0xffffffffu, (unsigned long long)Bw0, c)
+                        : (WT)__shfl_sync(0xffffffffu, (unsigned long long)Bw1, c - 32);
+          else
+            bc = (WT)__shfl_sync(0xffffffffu, (unsigned)Bw0, c);
+          if ((M0 >> (B - 1 - c)) & 1) acc += popc_w((WT)(A0 & bc));
+          if (RPL == 2 && ((M1 >> (B - 1 - c)) & 1)) acc += popc_w((WT)(A1 & bc));
+        }
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0 && acc) atomicAdd(count, acc);
+}
+
+}  // namespace
+
+int tc_launch(const gbo_graph* g, unsigned long long* d_count, cudaStream_t s) {
+  GBO_CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s));
+  if (g->nblk == 0) return GBO_OK;
+  GView v = view_of(g);
+  long long warps = g->nblk;
+  long long cap = (long long)num_sms() * 64;  // 64 resident warps per SM
+  if (warps > cap * 8) warps = cap * 8;
+  const unsigned grid = blocks_for_warps(warps, kTPB / 32);
+  switch (g->b) {
+    case 4: k_tc<4><<<grid, kTPB, 0, s>>>(v, g->nblk, d_count); break;
+    case 8: k_tc<8><<<grid, kTPB, 0, s>>>(v, g->nblk, d_count); break;
+    case 16: k_tc<16><<<grid, kTPB, 0, s>>>(v, g->nblk, d_count); break;
+    case 32: k_tc<32><<<grid, kTPB, 0, s>>>(v, g->nblk, d_count); break;
+    default: k_tc<64><<<grid, kTPB, 0, s>>>(v, g->nblk, d_count); break;
+  }
+  GBO_CUDA_TRY(cudaGetLastError());
+  return GBO_OK;
+}
+
+}  // namespace gbo
+
+using namespace gbo;
+
+static int check_tc_graph(const gbo_graph* g) {
+  if (!g) return fail(GBO_ERR_INVALID, "graph is NULL");
+  if (g->layout != GBO_LAYOUT_ROW) return fail(GBO_ERR_UNSUPPORTED, "TC needs the ROW tile layout");
+  if (g->nrows != g->ncols) return fail(GBO_ERR_INVALID, "TC needs a square matrix");
+  return GBO_OK;
+}
+
+extern "C" int gbo_tc_device(const gbo_graph* lower, unsigned long long* d_count,
+                             gbo_stream_t stream) {
+  clear_error();
+  GBO_TRY(check_tc_graph(lower));
+  if (!d_count) return fail(GBO_ERR_INVALID, "count is NULL");
+  return tc_launch(lower, d_count, as_stream(stream));
+}
+
+extern "C" int gbo_tc(const gbo_graph* lower, uint64_t* h_count, gbo_stream_t stream) {
+  clear_error();
+  GBO_TRY(check_tc_graph(lower));
+  if (!h_count) return fail(GBO_ERR_INVALID, "count is NULL");
+  cudaStream_t s = as_stream(stream);
+  unsigned long long* d = nullptr;
+  GBO_CUDA_TRY(cudaMallocAsync(&d, sizeof(unsigned long long), s));
+  int st = tc_launch(lower, d, s);
+  unsigned long long h = 0;
+  if (st == GBO_OK) {
+    cudaError_t e = cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = fail_cuda(e, "tc readback");
+  }
+  cudaFreeAsync(d, s);
+  if (st == GBO_OK) *h_count = h;
+  return st;
+}

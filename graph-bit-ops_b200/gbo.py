@@ -1,0 +1,560 @@
+"""ctypes binding of libgbo (the C ABI in include/gbo.h) for Python callers.
+
+This module is a thin host-side mirror of the C ABI: device buffers, the
+graph handle, the B2SR primitives and the algorithms.  It contains no
+computation of its own; every call goes to libgbo.so, and importing it on a
+machine where libgbo.so is missing raises instead of falling back.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgbo.so")
+
+GBO_OK = 0
+GBO_ERR_INVALID = 1
+GBO_ERR_CUDA = 2
+GBO_ERR_NOMEM = 3
+GBO_ERR_UNSORTED = 4
+GBO_ERR_BOUNDS = 5
+GBO_ERR_TIMEOUT = 6
+GBO_ERR_IO = 7
+GBO_ERR_UNSUPPORTED = 8
+GBO_ERR_OVERFLOW = 9
+GBO_ERR_NOTREADY = 10
+
+LAYOUT_ROW = 0
+LAYOUT_COL = 1
+FLAG_DEVICE_PTRS = 1
+FLAG_TRANSPOSE = 2
+FLAG_LAYOUT_COL = 4
+FLAG_LOWER = 8
+OUT_I32 = 0
+OUT_F32 = 1
+MTX_READMTX = 0
+MTX_MMIO = 1
+
+WORD_DTYPE = {4: np.uint8, 8: np.uint8, 16: np.uint16, 32: np.uint32, 64: np.uint64}
+
+
+class GboError(RuntimeError):
+    def __init__(self, status: int, where: str, message: str):
+        super().__init__(f"{where}: {_status_name(status)}: {message}")
+        self.status = status
+
+
+class GraphInfo(C.Structure):
+    _fields_ = [
+        ("nrows", C.c_int), ("ncols", C.c_int), ("tile_bits", C.c_int), ("layout", C.c_int),
+        ("nblockrows", C.c_int), ("nblockcols", C.c_int), ("nblocks", C.c_int64),
+        ("nnz", C.c_int64), ("b2sr_bytes", C.c_int64), ("device_bytes", C.c_int64),
+        ("nsplit_rows", C.c_int), ("nitems", C.c_int),
+    ]
+
+
+MAX_STEP_TIMES = 256
+
+
+class RunStats(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("graph_replays", C.c_int),
+                ("kernel_launches", C.c_longlong), ("nsteps", C.c_int),
+                ("step_ms", C.c_float * MAX_STEP_TIMES)]
+
+
+class CsrStruct(C.Structure):
+    _fields_ = [("nrows", C.c_int), ("ncols", C.c_int), ("nnz", C.c_int64),
+                ("rowptr", C.POINTER(C.c_int)), ("colind", C.POINTER(C.c_int))]
+
+
+_P = C.c_void_p
+_I = C.c_int
+_SIGS = {
+    "gbo_status_string": (C.c_char_p, [_I]),
+    "gbo_last_error": (C.c_char_p, []),
+    "gbo_version": (_I, []),
+    "gbo_device_count": (_I, [C.POINTER(_I)]),
+    "gbo_set_device": (_I, [_I]),
+    "gbo_malloc": (_I, [C.POINTER(_P), C.c_size_t]),
+    "gbo_free": (_I, [_P]),
+    "gbo_host_alloc": (_I, [C.POINTER(_P), C.c_size_t]),
+    "gbo_host_free": (_I, [_P]),
+    "gbo_memset": (_I, [_P, _I, C.c_size_t, _P]),
+    "gbo_memcpy_h2d": (_I, [_P, _P, C.c_size_t, _P]),
+    "gbo_memcpy_d2h": (_I, [_P, _P, C.c_size_t, _P]),
+    "gbo_memcpy_d2d": (_I, [_P, _P, C.c_size_t, _P]),
+    "gbo_stream_create": (_I, [C.POINTER(_P)]),
+    "gbo_stream_destroy": (_I, [_P]),
+    "gbo_stream_sync": (_I, [_P]),
+    "gbo_device_sync": (_I, []),
+    "gbo_event_create": (_I, [C.POINTER(_P)]),
+    "gbo_event_destroy": (_I, [_P]),
+    "gbo_event_record": (_I, [_P, _P]),
+    "gbo_event_elapsed_ms": (_I, [_P, _P, C.POINTER(C.c_float)]),
+    "gbo_flush_l2": (_I, [_P]),
+    "gbo_b2sr_nnzb": (_I, [_P, _P, _I, _I, _I, _I, _P, C.POINTER(_I), _P]),
+    "gbo_b2sr_pack": (_I, [_P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P]),
+    "gbo_pack_vector_f32": (_I, [_P, _I, _I, _P, _P]),
+    "gbo_pack_vector_i32": (_I, [_P, _I, _I, _P, _P]),
+    "gbo_unpack_vector": (_I, [_P, _I, _I, _P, _P]),
+    "gbo_graph_from_csr": (_I, [_P, _P, _I, _I, _I, _I, _I, _P, C.POINTER(_P)]),
+    "gbo_graph_wrap_b2sr": (_I, [_I, _I, _I, _I, _I, _P, _P, _P, _P, _P, C.POINTER(_P)]),
+    "gbo_graph_free": (_I, [_P]),
+    "gbo_graph_get_info": (_I, [_P, C.POINTER(GraphInfo)]),
+    "gbo_graph_b2sr": (_I, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
+    "gbo_graph_outdeg": (_I, [_P, C.POINTER(_P)]),
+    "gbo_bmv_count": (_I, [_P, _P, _P, _I, _I, _P]),
+    "gbo_bmv_masked": (_I, [_P, _P, _P, _P, _P]),
+    "gbo_bmv_minplus": (_I, [_P, _P, _P, _P]),
+    "gbo_bmv_float": (_I, [_P, _P, _P, C.c_float, _P, C.c_float, _P]),
+    "gbo_bmv_minselect": (_I, [_P, _P, _P, _P]),
+    "gbo_bmv_float_transposed": (_I, [_P, _P, _P, C.c_float, _P, C.c_float, _P]),
+    "gbo_bfs": (_I, [_P, _I, _P, C.POINTER(_I), _P]),
+    "gbo_sssp_unit": (_I, [_P, _I, _P, C.POINTER(_I), _P]),
+    "gbo_pagerank": (_I, [_P, C.c_float, _I, C.c_float, _P, C.POINTER(_I), _P]),
+    "gbo_cc": (_I, [_P, _P, C.POINTER(_I), _P]),
+    "gbo_tc": (_I, [_P, C.POINTER(C.c_uint64), _P]),
+    "gbo_tc_device": (_I, [_P, _P, _P]),
+    "gbo_ppr_forward": (_I, [_P, _P, C.c_float, C.c_float, _I, _P, C.POINTER(_I), _P]),
+    "gbo_ppr_backward": (_I, [_P, _P, C.c_float, C.c_float, _I, _P, C.POINTER(_I), _P]),
+    "gbo_graph_last_run": (_I, [_P, C.POINTER(RunStats)]),
+    "gbo_read_mtx": (_I, [C.c_char_p, _I, _I, C.POINTER(C.POINTER(CsrStruct))]),
+    "gbo_csr_free": (_I, [C.POINTER(CsrStruct)]),
+    "gbo_csr_transpose": (_I, [C.POINTER(CsrStruct), C.POINTER(C.POINTER(CsrStruct))]),
+    "gbo_csr_tril": (_I, [C.POINTER(CsrStruct), C.POINTER(C.POINTER(CsrStruct))]),
+    "gbo_csr_from_edges": (_I, [_P, _P, C.c_int64, _I, _I, _I, C.POINTER(C.POINTER(CsrStruct))]),
+    "gbo_gen_rmat": (_I, [_I, _I, C.c_double, C.c_double, C.c_double, C.c_uint64,
+                          C.POINTER(C.POINTER(CsrStruct))]),
+    "gbo_gen_er": (_I, [_I, C.c_double, C.c_uint64, C.POINTER(C.POINTER(CsrStruct))]),
+    "gbo_gen_er_avgdeg": (_I, [_I, C.c_double, C.c_uint64, C.POINTER(C.POINTER(CsrStruct))]),
+    "gbo_gen_king_mesh": (_I, [_I, C.POINTER(C.POINTER(CsrStruct))]),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libgbo.so (built by __graft_entry__.build() / make); raise if absent."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"libgbo.so not found at {LIB_PATH}; run make in {_HERE}")
+        l = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(l, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = l
+    return _lib
+
+
+def exported_symbols():
+    return list(_SIGS)
+
+
+def _status_name(st: int) -> str:
+    try:
+        return lib().gbo_status_string(st).decode()
+    except Exception:  # pragma: no cover - only while the library is unavailable
+        return str(st)
+
+
+def check(st: int, where: str = "gbo"):
+    if st != GBO_OK:
+        raise GboError(st, where, lib().gbo_last_error().decode())
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+# ------------------------------------------------------------ device memory
+class DeviceBuffer:
+    """Owned device allocation (gbo_malloc / gbo_free)."""
+
+    def __init__(self, nbytes: int):
+        self.nbytes = int(nbytes)
+        p = C.c_void_p()
+        check(lib().gbo_malloc(C.byref(p), max(1, self.nbytes)), "gbo_malloc")
+        self.ptr = p.value
+
+    @classmethod
+    def from_numpy(cls, a: np.ndarray, stream=None) -> "DeviceBuffer":
+        a = np.ascontiguousarray(a)
+        buf = cls(a.nbytes)
+        if a.nbytes:
+            check(lib().gbo_memcpy_h2d(buf.ptr, _ptr(a), a.nbytes, stream), "h2d")
+            check(lib().gbo_stream_sync(stream), "sync")
+        return buf
+
+    @classmethod
+    def zeros(cls, nbytes: int, stream=None) -> "DeviceBuffer":
+        buf = cls(nbytes)
+        check(lib().gbo_memset(buf.ptr, 0, max(1, nbytes), stream), "memset")
+        return buf
+
+    def fill_bytes(self, value: int, stream=None):
+        check(lib().gbo_memset(self.ptr, value, max(1, self.nbytes), stream), "memset")
+
+    def upload(self, a: np.ndarray, stream=None):
+        a = np.ascontiguousarray(a)
+        assert a.nbytes <= self.nbytes
+        if a.nbytes:
+            check(lib().gbo_memcpy_h2d(self.ptr, _ptr(a), a.nbytes, stream), "h2d")
+
+    def to_numpy(self, dtype, count: int | None = None, stream=None) -> np.ndarray:
+        dtype = np.dtype(dtype)
+        if count is None:
+            count = self.nbytes // dtype.itemsize
+        out = np.empty(count, dtype=dtype)
+        if out.nbytes:
+            check(lib().gbo_memcpy_d2h(_ptr(out), self.ptr, out.nbytes, stream), "d2h")
+        check(lib().gbo_stream_sync(stream), "sync")
+        return out
+
+    def free(self):
+        if self.ptr:
+            lib().gbo_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def device_to_numpy(ptr: int, dtype, count: int, stream=None) -> np.ndarray:
+    out = np.empty(count, dtype=np.dtype(dtype))
+    if out.nbytes:
+        check(lib().gbo_memcpy_d2h(_ptr(out), ptr, out.nbytes, stream), "d2h")
+    check(lib().gbo_stream_sync(stream), "sync")
+    return out
+
+
+def device_count() -> int:
+    n = C.c_int(0)
+    st = lib().gbo_device_count(C.byref(n))
+    return n.value if st == GBO_OK else 0
+
+
+def sync(stream=None):
+    check(lib().gbo_stream_sync(stream), "sync")
+
+
+class Stream:
+    def __init__(self):
+        p = C.c_void_p()
+        check(lib().gbo_stream_create(C.byref(p)), "stream_create")
+        self.ptr = p.value
+
+    def sync(self):
+        check(lib().gbo_stream_sync(self.ptr), "stream_sync")
+
+    def __del__(self):
+        try:
+            if self.ptr:
+                lib().gbo_stream_destroy(self.ptr)
+        except Exception:
+            pass
+
+
+class Event:
+    def __init__(self):
+        p = C.c_void_p()
+        check(lib().gbo_event_create(C.byref(p)), "event_create")
+        self.ptr = p.value
+
+    def record(self, stream=None):
+        check(lib().gbo_event_record(self.ptr, stream), "event_record")
+
+    def elapsed_ms(self, later: "Event") -> float:
+        ms = C.c_float(0)
+        check(lib().gbo_event_elapsed_ms(self.ptr, later.ptr, C.byref(ms)), "event_elapsed")
+        return ms.value
+
+    def __del__(self):
+        try:
+            if self.ptr:
+                lib().gbo_event_destroy(self.ptr)
+        except Exception:
+            pass
+
+
+# --------------------------------------------------------------- host CSR
+class Csr:
+    """Host CSR produced by libgbo (reader / generators); arrays are copied out."""
+
+    def __init__(self, rowptr: np.ndarray, colind: np.ndarray, nrows: int, ncols: int):
+        self.rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
+        self.colind = np.ascontiguousarray(colind, dtype=np.int32)
+        self.nrows = int(nrows)
+        self.ncols = int(ncols)
+
+    @property
+    def nnz(self) -> int:
+        return int(self.rowptr[-1]) if len(self.rowptr) else 0
+
+    @classmethod
+    def _take(cls, p) -> "Csr":
+        s = p.contents
+        n = s.nrows
+        rp = np.ctypeslib.as_array(s.rowptr, shape=(n + 1,)).copy()
+        ci = (np.ctypeslib.as_array(s.colind, shape=(int(s.nnz),)).copy()
+              if s.nnz > 0 else np.zeros(0, np.int32))
+        out = cls(rp, ci, n, s.ncols)
+        lib().gbo_csr_free(p)
+        return out
+
+    def _struct(self):
+        s = CsrStruct()
+        s.nrows, s.ncols, s.nnz = self.nrows, self.ncols, self.nnz
+        s.rowptr = self.rowptr.ctypes.data_as(C.POINTER(C.c_int))
+        s.colind = self.colind.ctypes.data_as(C.POINTER(C.c_int))
+        return s
+
+    def transpose(self) -> "Csr":
+        s = self._struct()
+        out = C.POINTER(CsrStruct)()
+        check(lib().gbo_csr_transpose(C.byref(s), C.byref(out)), "csr_transpose")
+        return Csr._take(out)
+
+    def tril(self) -> "Csr":
+        s = self._struct()
+        out = C.POINTER(CsrStruct)()
+        check(lib().gbo_csr_tril(C.byref(s), C.byref(out)), "csr_tril")
+        return Csr._take(out)
+
+    def degrees(self) -> np.ndarray:
+        return np.diff(self.rowptr)
+
+
+def read_mtx(path: str, mode: int = MTX_READMTX, directed: int = 0) -> Csr:
+    out = C.POINTER(CsrStruct)()
+    check(lib().gbo_read_mtx(path.encode(), mode, directed, C.byref(out)), "read_mtx")
+    return Csr._take(out)
+
+
+def csr_from_edges(src, dst, nvertices: int, symmetrize=True, drop_self_loops=True) -> Csr:
+    src = np.ascontiguousarray(src, dtype=np.int32)
+    dst = np.ascontiguousarray(dst, dtype=np.int32)
+    out = C.POINTER(CsrStruct)()
+    check(lib().gbo_csr_from_edges(_ptr(src), _ptr(dst), len(src), nvertices, int(symmetrize),
+                                   int(drop_self_loops), C.byref(out)), "csr_from_edges")
+    return Csr._take(out)
+
+
+def gen_rmat(scale: int, edge_factor: int = 16, a=0.57, b=0.19, c=0.19, seed: int = 0) -> Csr:
+    out = C.POINTER(CsrStruct)()
+    check(lib().gbo_gen_rmat(scale, edge_factor, a, b, c, seed, C.byref(out)), "gen_rmat")
+    return Csr._take(out)
+
+
+def gen_er(n: int, p: float, seed: int = 0) -> Csr:
+    out = C.POINTER(CsrStruct)()
+    check(lib().gbo_gen_er(n, p, seed, C.byref(out)), "gen_er")
+    return Csr._take(out)
+
+
+def gen_er_avgdeg(n: int, avg_degree: float, seed: int = 0) -> Csr:
+    out = C.POINTER(CsrStruct)()
+    check(lib().gbo_gen_er_avgdeg(n, avg_degree, seed, C.byref(out)), "gen_er_avgdeg")
+    return Csr._take(out)
+
+
+def gen_king_mesh(side: int) -> Csr:
+    out = C.POINTER(CsrStruct)()
+    check(lib().gbo_gen_king_mesh(side, C.byref(out)), "gen_king_mesh")
+    return Csr._take(out)
+
+
+# ------------------------------------------------------------ graph handle
+class Graph:
+    """Device-resident B2SR graph (gbo_graph_from_csr)."""
+
+    def __init__(self, handle: int, keep=()):
+        self.h = handle
+        self._keep = keep  # buffers a wrapped graph points into
+
+    @classmethod
+    def from_csr(cls, csr: Csr, tile_bits: int = 32, flags: int = 0, stream=None) -> "Graph":
+        p = C.c_void_p()
+        check(lib().gbo_graph_from_csr(_ptr(csr.rowptr), _ptr(csr.colind), csr.nrows, csr.ncols,
+                                       csr.nnz, tile_bits, flags, stream, C.byref(p)),
+              "graph_from_csr")
+        return cls(p.value)
+
+    @classmethod
+    def wrap_b2sr(cls, nrows, ncols, tile_bits, layout, nblocks, rowptr: DeviceBuffer,
+                  colind: DeviceBuffer, val: DeviceBuffer, outdeg: DeviceBuffer | None = None,
+                  stream=None) -> "Graph":
+        p = C.c_void_p()
+        check(lib().gbo_graph_wrap_b2sr(nrows, ncols, tile_bits, layout, nblocks, rowptr.ptr,
+                                        colind.ptr, val.ptr, outdeg.ptr if outdeg else None,
+                                        stream, C.byref(p)), "graph_wrap_b2sr")
+        return cls(p.value, keep=(rowptr, colind, val, outdeg))
+
+    def info(self) -> GraphInfo:
+        inf = GraphInfo()
+        check(lib().gbo_graph_get_info(self.h, C.byref(inf)), "graph_get_info")
+        return inf
+
+    def b2sr(self):
+        """Copy the B2SR arrays back: (bsrRowPtr, bsrColInd, words)."""
+        inf = self.info()
+        r, c, v = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        check(lib().gbo_graph_b2sr(self.h, C.byref(r), C.byref(c), C.byref(v)), "graph_b2sr")
+        nb = int(inf.nblocks)
+        rp = device_to_numpy(r.value, np.int32, inf.nblockrows + 1)
+        ci = device_to_numpy(c.value, np.int32, nb) if nb else np.zeros(0, np.int32)
+        wd = WORD_DTYPE[inf.tile_bits]
+        w = device_to_numpy(v.value, wd, nb * inf.tile_bits) if nb else np.zeros(0, wd)
+        return rp, ci, w
+
+    def outdeg(self) -> np.ndarray:
+        p = C.c_void_p()
+        check(lib().gbo_graph_outdeg(self.h, C.byref(p)), "graph_outdeg")
+        return device_to_numpy(p.value, np.int32, self.info().ncols)
+
+    def last_run(self) -> dict:
+        st = RunStats()
+        check(lib().gbo_graph_last_run(self.h, C.byref(st)), "graph_last_run")
+        return {"iterations": st.iterations, "graph_replays": st.graph_replays,
+                "kernel_launches": int(st.kernel_launches),
+                "step_ms": [float(st.step_ms[i]) for i in range(st.nsteps)]}
+
+    def free(self):
+        if self.h:
+            lib().gbo_graph_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    # ---- primitives on device buffers
+    def bmv_count(self, x_bits: DeviceBuffer, y: DeviceBuffer, out_type=OUT_I32, accumulate=False,
+                  stream=None):
+        check(lib().gbo_bmv_count(self.h, x_bits.ptr, y.ptr, out_type, int(accumulate), stream),
+              "bmv_count")
+
+    def bmv_masked(self, x_bits: DeviceBuffer, mask_bits: DeviceBuffer | None, out_bits: DeviceBuffer,
+                   stream=None):
+        check(lib().gbo_bmv_masked(self.h, x_bits.ptr, mask_bits.ptr if mask_bits else None,
+                                   out_bits.ptr, stream), "bmv_masked")
+
+    def bmv_minplus(self, x: DeviceBuffer, y: DeviceBuffer, stream=None):
+        check(lib().gbo_bmv_minplus(self.h, x.ptr, y.ptr, stream), "bmv_minplus")
+
+    def bmv_float(self, x: DeviceBuffer, y: DeviceBuffer, alpha=1.0, scale: DeviceBuffer | None = None,
+                  add=0.0, stream=None):
+        check(lib().gbo_bmv_float(self.h, x.ptr, y.ptr, alpha, scale.ptr if scale else None, add,
+                                  stream), "bmv_float")
+
+    def bmv_minselect(self, x: DeviceBuffer, y: DeviceBuffer, stream=None):
+        check(lib().gbo_bmv_minselect(self.h, x.ptr, y.ptr, stream), "bmv_minselect")
+
+    def bmv_float_transposed(self, x: DeviceBuffer, y: DeviceBuffer, alpha=1.0,
+                             scale: DeviceBuffer | None = None, add=0.0, stream=None):
+        check(lib().gbo_bmv_float_transposed(self.h, x.ptr, y.ptr, alpha,
+                                             scale.ptr if scale else None, add, stream),
+              "bmv_float_transposed")
+
+    # ---- algorithms (numpy in / numpy out helpers)
+    def bfs(self, src: int, out: DeviceBuffer | None = None, stream=None):
+        n = self.info().nrows
+        buf = out or DeviceBuffer(4 * n)
+        depth = C.c_int(0)
+        check(lib().gbo_bfs(self.h, src, buf.ptr, C.byref(depth), stream), "bfs")
+        if out is not None:
+            return depth.value
+        return buf.to_numpy(np.int32, n, stream), depth.value
+
+    def sssp(self, src: int, stream=None):
+        n = self.info().nrows
+        buf = DeviceBuffer(4 * n)
+        it = C.c_int(0)
+        check(lib().gbo_sssp_unit(self.h, src, buf.ptr, C.byref(it), stream), "sssp_unit")
+        return buf.to_numpy(np.uint32, n, stream), it.value
+
+    def pagerank(self, alpha=0.85, max_iter=20, tol=-1.0, stream=None):
+        n = self.info().nrows
+        buf = DeviceBuffer(4 * n)
+        it = C.c_int(0)
+        check(lib().gbo_pagerank(self.h, alpha, max_iter, tol, buf.ptr, C.byref(it), stream),
+              "pagerank")
+        return buf.to_numpy(np.float32, n, stream), it.value
+
+    def cc(self, stream=None):
+        n = self.info().nrows
+        buf = DeviceBuffer(4 * n)
+        it = C.c_int(0)
+        check(lib().gbo_cc(self.h, buf.ptr, C.byref(it), stream), "cc")
+        return buf.to_numpy(np.int32, n, stream), it.value
+
+    def tc(self, stream=None) -> int:
+        c = C.c_uint64(0)
+        check(lib().gbo_tc(self.h, C.byref(c), stream), "tc")
+        return int(c.value)
+
+    def ppr_forward(self, v: np.ndarray, alpha=0.85, tol=1e-7, max_iter=1000, stream=None):
+        n = self.info().nrows
+        dv = DeviceBuffer.from_numpy(np.asarray(v, np.float32), stream)
+        buf = DeviceBuffer(4 * n)
+        it = C.c_int(0)
+        check(lib().gbo_ppr_forward(self.h, dv.ptr, alpha, tol, max_iter, buf.ptr, C.byref(it),
+                                    stream), "ppr_forward")
+        return buf.to_numpy(np.float32, n, stream), it.value
+
+    def ppr_backward(self, w: np.ndarray, alpha=0.85, tol=1e-7, max_iter=1000, stream=None):
+        n = self.info().nrows
+        dw = DeviceBuffer.from_numpy(np.asarray(w, np.float32), stream)
+        buf = DeviceBuffer(4 * n)
+        it = C.c_int(0)
+        check(lib().gbo_ppr_backward(self.h, dw.ptr, alpha, tol, max_iter, buf.ptr, C.byref(it),
+                                     stream), "ppr_backward")
+        return buf.to_numpy(np.float32, n, stream), it.value
+
+
+# ------------------------------------------------------------- raw B2SR
+def b2sr_pack_raw(rowptr: DeviceBuffer, colind: DeviceBuffer, nrows, ncols, nnz, tile_bits,
+                  layout=LAYOUT_ROW, stream=None):
+    """gbo_b2sr_nnzb + gbo_b2sr_pack on caller-owned buffers; returns device buffers."""
+    nbr = (nrows + tile_bits - 1) // tile_bits
+    brp = DeviceBuffer(4 * (nbr + 1))
+    nb = C.c_int(0)
+    check(lib().gbo_b2sr_nnzb(rowptr.ptr, colind.ptr, nrows, ncols, nnz, tile_bits, brp.ptr,
+                              C.byref(nb), stream), "b2sr_nnzb")
+    wb = np.dtype(WORD_DTYPE[tile_bits]).itemsize
+    bci = DeviceBuffer(4 * max(1, nb.value))
+    val = DeviceBuffer(wb * tile_bits * max(1, nb.value))
+    check(lib().gbo_b2sr_pack(rowptr.ptr, colind.ptr, nrows, ncols, nnz, tile_bits, layout, brp.ptr,
+                              bci.ptr, val.ptr, stream), "b2sr_pack")
+    return brp, bci, val, nb.value
+
+
+def pack_vector(x: DeviceBuffer, n: int, tile_bits: int, dtype="f32", stream=None) -> DeviceBuffer:
+    nw = (n + tile_bits - 1) // tile_bits
+    wb = np.dtype(WORD_DTYPE[tile_bits]).itemsize
+    out = DeviceBuffer(max(1, nw * wb))
+    f = lib().gbo_pack_vector_f32 if dtype == "f32" else lib().gbo_pack_vector_i32
+    check(f(x.ptr, n, tile_bits, out.ptr, stream), "pack_vector")
+    return out
+
+
+def bits_from_numpy(x01: np.ndarray, tile_bits: int) -> np.ndarray:
+    """Host helper: 0/1 vector -> B2SR bit words (same layout as ToBit*Row)."""
+    x01 = np.asarray(x01).astype(bool)
+    n = len(x01)
+    nw = (n + tile_bits - 1) // tile_bits
+    pad = np.zeros(nw * tile_bits, dtype=bool)
+    pad[:n] = x01
+    bits = pad.reshape(nw, tile_bits).astype(np.uint64)
+    weights = (np.uint64(1) << np.arange(tile_bits - 1, -1, -1, dtype=np.uint64))
+    words = (bits * weights).sum(axis=1, dtype=np.uint64)
+    return words.astype(WORD_DTYPE[tile_bits])

@@ -1,0 +1,298 @@
+/*
+ * gbo.h -- C ABI of graph-bit-ops on B200 (sm_100a).
+ *
+ * The reference (carolc0708/graph-bit-ops) has no library: its drivers include
+ * the kernel files textually and launch templated __global__ kernels on the
+ * default stream.  This header is the drop-in boundary that replaces those
+ * call sites.  Every entry point:
+ *   - is extern "C", takes plain pointers and sizes, returns an int status;
+ *   - is stream-ordered on the gbo_stream_t it is given (a cudaStream_t;
+ *     NULL means the legacy default stream, as in the reference);
+ *   - never calls exit(); on failure gbo_last_error() describes the cause.
+ *
+ * B2SR ("bit-packed BSR") layout, identical to the reference's:
+ *   bsrRowPtr  int32[nblockrows+1]           ascending block-row offsets
+ *   bsrColInd  int32[nblocks]                block columns, ascending per row
+ *   bsrVal     nblocks * b words of b bits   word type per tile width b:
+ *                b=4  uint8  (low nibble)    b=8  uint8
+ *                b=16 uint16                 b=32 uint32     b=64 uint64
+ *   ROW layout (GBO_LAYOUT_ROW): word r of a tile is tile row r and column c
+ *     sits at bit (b-1-c)  -- cusparse DIRECTION_ROW + ToBit*Col
+ *     (algorithm/bsrbmv.cu:31-235).
+ *   COL layout (GBO_LAYOUT_COL): word c is tile column c and row r sits at
+ *     bit (b-1-r)  -- the _col packers (bsrbmm/csr2bsr_batch.cu:1208).
+ * Bit vectors use one word of the same type per block row; element
+ * i = R*b + r is bit (b-1-r) of word R (ToBit*Row, algorithm/bsrbmv.cu:62-255).
+ */
+#ifndef GBO_H_
+#define GBO_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+enum gbo_status {
+  GBO_OK = 0,
+  GBO_ERR_INVALID = 1,       /* bad argument (null pointer, size, tile width) */
+  GBO_ERR_CUDA = 2,          /* a CUDA runtime call failed */
+  GBO_ERR_NOMEM = 3,         /* device or host allocation failed */
+  GBO_ERR_UNSORTED = 4,      /* CSR columns not ascending inside a row */
+  GBO_ERR_BOUNDS = 5,        /* an index outside its range (device-checked) */
+  GBO_ERR_TIMEOUT = 6,       /* a bounded device wait gave up */
+  GBO_ERR_IO = 7,            /* file missing or malformed */
+  GBO_ERR_UNSUPPORTED = 8,   /* combination not provided (e.g. layout) */
+  GBO_ERR_OVERFLOW = 9,      /* a count does not fit the int32 B2SR indices */
+  GBO_ERR_NOTREADY = 10      /* server: result not yet available */
+};
+
+#if defined(__GNUC__)
+#define GBO_API __attribute__((visibility("default")))
+#else
+#define GBO_API
+#endif
+
+typedef void* gbo_stream_t; /* cudaStream_t */
+
+GBO_API const char* gbo_status_string(int status);
+/* Message of the last failure on the calling host thread ("" if none). */
+GBO_API const char* gbo_last_error(void);
+GBO_API int gbo_version(void); /* major*10000 + minor*100 + patch */
+
+enum { GBO_LAYOUT_ROW = 0, GBO_LAYOUT_COL = 1 };
+
+/* ------------------------------------------- device plumbing for FFI users */
+/* Thin wrappers so that callers without CUDA bindings (ctypes, cgo, JNI)
+ * can own device buffers, streams and events.                              */
+GBO_API int gbo_device_count(int* count);
+GBO_API int gbo_set_device(int device);
+GBO_API int gbo_malloc(void** d_ptr, size_t bytes);
+GBO_API int gbo_free(void* d_ptr);
+GBO_API int gbo_host_alloc(void** h_ptr, size_t bytes); /* pinned host memory */
+GBO_API int gbo_host_free(void* h_ptr);
+GBO_API int gbo_memset(void* d_ptr, int value, size_t bytes, gbo_stream_t stream);
+GBO_API int gbo_memcpy_h2d(void* d_dst, const void* h_src, size_t bytes, gbo_stream_t stream);
+GBO_API int gbo_memcpy_d2h(void* h_dst, const void* d_src, size_t bytes, gbo_stream_t stream);
+GBO_API int gbo_memcpy_d2d(void* d_dst, const void* d_src, size_t bytes, gbo_stream_t stream);
+GBO_API int gbo_stream_create(gbo_stream_t* stream);
+GBO_API int gbo_stream_destroy(gbo_stream_t stream);
+GBO_API int gbo_stream_sync(gbo_stream_t stream);
+GBO_API int gbo_device_sync(void);
+typedef void* gbo_event_t;
+GBO_API int gbo_event_create(gbo_event_t* ev);
+GBO_API int gbo_event_destroy(gbo_event_t ev);
+GBO_API int gbo_event_record(gbo_event_t ev, gbo_stream_t stream);
+GBO_API int gbo_event_elapsed_ms(gbo_event_t start, gbo_event_t stop, float* ms);
+/* Write bytes >= the L2 size so the next timed launch starts cold. */
+GBO_API int gbo_flush_l2(gbo_stream_t stream);
+
+/* ------------------------------------------------ raw B2SR packing (A1, A2) */
+/* Number of non-empty b x b tiles per block row of a CSR matrix.
+ * Replaces cusparseXcsr2bsrNnz as used by the drivers (algorithm/bfs.cu:383).
+ * d_bsrRowPtr gets nblockrows+1 offsets, *h_nblocks the total.
+ * CSR column indices must be ascending inside each row (duplicates allowed);
+ * otherwise GBO_ERR_UNSORTED.  All pointers are device pointers except
+ * h_nblocks.  Synchronises the stream (the count sizes the next buffers). */
+GBO_API int gbo_b2sr_nnzb(const int* d_csrRowPtr, const int* d_csrColInd, int nrows,
+                  int ncols, int nnz, int tile_bits, int* d_bsrRowPtr,
+                  int* h_nblocks, gbo_stream_t stream);
+
+/* Fill bsrColInd / bsrVal for the offsets produced by gbo_b2sr_nnzb.
+ * Replaces csr2bsr_batch_{4,8,16,32,64} (algorithm/csr2bsr_batch_bsrbmv.cu:
+ * 9,180,406,621,786) and their _row/_col forms (bsrbmm/csr2bsr_batch.cu). */
+GBO_API int gbo_b2sr_pack(const int* d_csrRowPtr, const int* d_csrColInd, int nrows,
+                  int ncols, int nnz, int tile_bits, int layout,
+                  const int* d_bsrRowPtr, int* d_bsrColInd, void* d_bsrVal,
+                  gbo_stream_t stream);
+
+/* Dense vector -> bit vector (element > 0 sets the bit); n_words words.
+ * Replaces ToBit{4,8,16,32,64}Row (algorithm/bsrbmv.cu:62,110,154,195,239). */
+GBO_API int gbo_pack_vector_f32(const float* d_x, int n, int tile_bits, void* d_bits,
+                        gbo_stream_t stream);
+GBO_API int gbo_pack_vector_i32(const int32_t* d_x, int n, int tile_bits, void* d_bits,
+                        gbo_stream_t stream);
+/* Bit vector -> int32 0/1 per element (n elements). */
+GBO_API int gbo_unpack_vector(const void* d_bits, int n, int tile_bits, int32_t* d_out,
+                      gbo_stream_t stream);
+
+/* ----------------------------------------------------------- graph handle */
+typedef struct gbo_graph gbo_graph;
+
+enum gbo_graph_flags {
+  GBO_FLAG_DEVICE_PTRS = 1, /* rowptr/colind are device pointers (else host) */
+  GBO_FLAG_TRANSPOSE = 2,   /* pack the transpose of the given CSR (CSC) */
+  GBO_FLAG_LAYOUT_COL = 4,  /* COL tile layout instead of ROW */
+  GBO_FLAG_LOWER = 8        /* keep only row >= col entries (tril_csr) */
+};
+
+/* Pack a CSR matrix M into a device-resident B2SR graph owned by the handle.
+ * The algorithms below treat the packed matrix P as a pull operator:
+ * y[i] = (+)_{j : P[i][j] = 1} x[j].  The reference packs the CSC of A
+ * (algorithm/bfs.cu:398-423) so that BFS pulls along A's edges; pass
+ * GBO_FLAG_TRANSPOSE to get the same.  out-degrees (column counts of P
+ * including duplicate CSR entries, i.e. the reference's csrRowPtr deltas
+ * used at algorithm/bsrbmv.cu:1277) are kept for PageRank. */
+GBO_API int gbo_graph_from_csr(const int* rowptr, const int* colind, int nrows,
+                       int ncols, int nnz, int tile_bits, int flags,
+                       gbo_stream_t stream, gbo_graph** out);
+/* Wrap caller-owned device B2SR buffers (not copied, not freed).  d_outdeg
+ * may be NULL (then PageRank entry points return GBO_ERR_INVALID). */
+GBO_API int gbo_graph_wrap_b2sr(int nrows, int ncols, int tile_bits, int layout,
+                        int nblocks, const int* d_bsrRowPtr,
+                        const int* d_bsrColInd, const void* d_bsrVal,
+                        const int* d_outdeg, gbo_stream_t stream,
+                        gbo_graph** out);
+GBO_API int gbo_graph_free(gbo_graph* g);
+
+typedef struct gbo_graph_info {
+  int nrows, ncols, tile_bits, layout;
+  int nblockrows, nblockcols;
+  int64_t nblocks;
+  int64_t nnz;          /* CSR entries the graph was packed from (-1 if wrapped) */
+  int64_t b2sr_bytes;   /* rowptr + colind + tile words */
+  int64_t device_bytes; /* everything the handle owns on the device */
+  int nsplit_rows;      /* block rows split across warps for load balance */
+  int nitems;           /* warp work items of the balanced schedule */
+} gbo_graph_info;
+GBO_API int gbo_graph_get_info(const gbo_graph* g, gbo_graph_info* info);
+GBO_API int gbo_graph_b2sr(const gbo_graph* g, const int** d_bsrRowPtr,
+                   const int** d_bsrColInd, const void** d_bsrVal);
+/* Device array of out-degrees (ncols ints) or NULL. */
+GBO_API int gbo_graph_outdeg(const gbo_graph* g, const int** d_outdeg);
+
+/* ------------------------------------------------ BMV primitives (A3-A8) */
+enum { GBO_OUT_I32 = 0, GBO_OUT_F32 = 1 };
+/* y[i] (+)= popc over tiles of (P_row_i & x) = sum_j P[i][j]*x[j]  (exact).
+ * y has nrows entries of type out_type; accumulate=1 adds to y like the
+ * reference's "+=" (bsrbmv.cu:432), 0 overwrites.
+ * Replaces bmv{4,8,16,32,64}_sparse and *_sparse_new (bsrbmv.cu:262-474,
+ * 2434-3094).  Unlike the reference b=64 kernel (16-bit halves,
+ * bsrbmv.cu:464-471) counts are exact 32-bit. */
+GBO_API int gbo_bmv_count(const gbo_graph* g, const void* d_x_bits, void* d_y,
+                  int out_type, int accumulate, gbo_stream_t stream);
+/* out_bits[R] = bits (sum_j P[i][j] x[j] > 0) & ~mask[R]  (Boolean OR.AND with
+ * a complement mask).  Replaces bmv32_sparse_bin_masked_v4 and
+ * bmv4_sparse_bin_masked_v4 (bsrbmv.cu:637-783).  d_mask_bits may be NULL. */
+GBO_API int gbo_bmv_masked(const gbo_graph* g, const void* d_x_bits,
+                   const void* d_mask_bits, void* d_out_bits,
+                   gbo_stream_t stream);
+/* y[i] = min(x[i], min_{j: P[i][j]} x[j] (+) 1) over uint32 with
+ * 2147483647 as infinity (saturating).  The min-plus product of (P + I),
+ * bmv{4,32}_sparse_full_minplus (bsrbmv.cu:989-1138). */
+GBO_API int gbo_bmv_minplus(const gbo_graph* g, const uint32_t* d_x, uint32_t* d_y,
+                    gbo_stream_t stream);
+/* y[i] = alpha * sum_{j: P[i][j]} x[j] * scale[j] + add   (fp32).
+ * scale may be NULL (1).  bmv{4,32}_sparse_full (bsrbmv.cu:1156-1286) is
+ * scale = 1/outdeg, add = 0. */
+GBO_API int gbo_bmv_float(const gbo_graph* g, const float* d_x, float* d_y,
+                  float alpha, const float* d_scale, float add,
+                  gbo_stream_t stream);
+/* y[i] = min_{j: P[i][j]} x[j], INT32_MAX when row i is empty.
+ * bmv{4,8,16,32}_sparse_full_cc* (bsrbmv.cu:1367-2099). */
+GBO_API int gbo_bmv_minselect(const gbo_graph* g, const int32_t* d_x, int32_t* d_y,
+                      gbo_stream_t stream);
+/* y[j] = alpha * sum_{i: P[i][j]} x[i] * scale[i] + add  (y = alpha P^T x):
+ * the transposed bit-packed BMV used by the PageRank adjoint.  No reference
+ * counterpart; fp32 with atomics, ncols outputs. */
+GBO_API int gbo_bmv_float_transposed(const gbo_graph* g, const float* d_x, float* d_y,
+                             float alpha, const float* d_scale, float add,
+                             gbo_stream_t stream);
+
+/* --------------------------------------------------- algorithms (A5-A11) */
+/* Level-synchronous pull BFS on P from src: level[i] = hops, -1 unreachable.
+ * Rewrites algorithm/bfs.cu:508-564 with all state on the device and
+ * termination decided on the device (no per-level host copy).
+ * h_depth (nullable) receives the number of levels (max level + 1). */
+GBO_API int gbo_bfs(const gbo_graph* g, int src, int32_t* d_level, int* h_depth,
+            gbo_stream_t stream);
+/* Unit-weight SSSP by min-plus relaxation (algorithm/sssp.cu:420-470):
+ * dist[i] in uint32, 2147483647 = unreachable. */
+GBO_API int gbo_sssp_unit(const gbo_graph* g, int src, uint32_t* d_dist, int* h_iters,
+                  gbo_stream_t stream);
+/* PageRank p = alpha * P D^-1 p + (1-alpha)/n from p0 = 1/n, as in
+ * algorithm/pr.cu:449-513 (no dangling redistribution; D = out-degrees).
+ * Runs until ||p - p_prev||_2 <= tol or max_iter iterations (tol < 0 runs
+ * exactly max_iter).  *h_iters gets the iterations done. */
+GBO_API int gbo_pagerank(const gbo_graph* g, float alpha, int max_iter, float tol,
+                 float* d_p, int* h_iters, gbo_stream_t stream);
+/* Connected components (P symmetric): label[i] = smallest vertex id in the
+ * component of i -- the fixed point of the reference's FastSV loop
+ * (algorithm/cc.cu:223-287). */
+GBO_API int gbo_cc(const gbo_graph* g, int32_t* d_label, int* h_iters,
+           gbo_stream_t stream);
+/* Triangles of an undirected simple graph given its lower triangle L
+ * (graph built with GBO_FLAG_LOWER, ROW layout): sum over (i,k) in L of
+ * (L L^T)[i][k].  Replaces tril_csr + bmm*_sparse_masked_v5 with a uint64
+ * result (bsrbmm/bsrbmm.cu:1214-1265, 1416; bsrbmm/tc.cu:767-951). */
+GBO_API int gbo_tc(const gbo_graph* lower, uint64_t* h_count, gbo_stream_t stream);
+/* Same, result left in device memory (*d_count is overwritten). */
+GBO_API int gbo_tc_device(const gbo_graph* lower, unsigned long long* d_count,
+                  gbo_stream_t stream);
+
+/* Personalized PageRank p = alpha * P D^-1 p + (1-alpha) v  (fp32) and its
+ * adjoint: for loss L = dot(w, p), grad_v = (1-alpha) u with
+ * u = alpha * D^-1 P^T u + w.  Iterate until the L1 change <= tol or
+ * max_iter.  No reference counterpart (built from A7). */
+GBO_API int gbo_ppr_forward(const gbo_graph* g, const float* d_v, float alpha,
+                    float tol, int max_iter, float* d_p, int* h_iters,
+                    gbo_stream_t stream);
+GBO_API int gbo_ppr_backward(const gbo_graph* g, const float* d_w, float alpha,
+                     float tol, int max_iter, float* d_grad_v, int* h_iters,
+                     gbo_stream_t stream);
+
+/* Statistics of the last algorithm call on a graph (per-iteration device
+ * time of the main BMV kernel, measured with CUDA events recorded inside the
+ * captured iteration graph).  No reference counterpart (the reference's
+ * GpuTimer brackets whole loops, algorithm/utility.cu:38). */
+#define GBO_MAX_STEP_TIMES 256
+typedef struct gbo_run_stats {
+  int iterations;        /* iterations executed */
+  int graph_replays;     /* CUDA graph launches (one host sync each) */
+  long long kernel_launches;
+  int nsteps;            /* entries of step_ms */
+  float step_ms[GBO_MAX_STEP_TIMES];
+} gbo_run_stats;
+GBO_API int gbo_graph_last_run(const gbo_graph* g, gbo_run_stats* stats);
+
+/* ------------------------------------------------ host CSR + I/O (A13) */
+typedef struct gbo_csr {
+  int nrows, ncols;
+  int64_t nnz;
+  int* rowptr; /* host, nrows+1 */
+  int* colind; /* host, nnz     */
+} gbo_csr;
+enum { GBO_MTX_READMTX = 0, GBO_MTX_MMIO = 1 };
+/* mode GBO_MTX_READMTX: readMtx + coo2csr semantics (readMtx.hpp:351-423,
+ * 246-304): directed 0 = symmetrise iff the banner says symmetric, 1 = never,
+ * 2 = always; self-loops and duplicates removed; rows sorted.
+ * mode GBO_MTX_MMIO: mmio_data semantics (mmio_highlevel.h:139-309): banner
+ * symmetry mirrors off-diagonal entries, self-loops and duplicates kept;
+ * columns are sorted inside each row (order inside a row carries no meaning
+ * for a binary matrix). */
+GBO_API int gbo_read_mtx(const char* path, int mode, int directed, gbo_csr** out);
+GBO_API int gbo_csr_free(gbo_csr* csr);
+/* CSC of a host CSR (readMtx.hpp:319-345), rows of the result sorted. */
+GBO_API int gbo_csr_transpose(const gbo_csr* in, gbo_csr** out);
+/* Keep entries with row >= col (tril_csr, bsrbmm/bsrbmm.cu:1416). */
+GBO_API int gbo_csr_tril(const gbo_csr* in, gbo_csr** out);
+/* Host CSR from an edge list: symmetrise (optional), drop self-loops
+ * (optional), sort and deduplicate. */
+GBO_API int gbo_csr_from_edges(const int* src, const int* dst, int64_t nedges,
+                       int nvertices, int symmetrize, int drop_self_loops,
+                       gbo_csr** out);
+
+/* Seeded synthetic graphs (splitmix64 -> xoshiro256**; one stream per edge
+ * draw, so the result does not depend on the thread count). */
+GBO_API int gbo_gen_rmat(int scale, int edge_factor, double a, double b, double c,
+                 uint64_t seed, gbo_csr** out);
+GBO_API int gbo_gen_er(int n, double p, uint64_t seed, gbo_csr** out);
+GBO_API int gbo_gen_er_avgdeg(int n, double avg_degree, uint64_t seed, gbo_csr** out);
+GBO_API int gbo_gen_king_mesh(int side, gbo_csr** out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GBO_H_ */

@@ -1,0 +1,134 @@
+"""Graph algorithms on the GPU vs the oracle: BFS levels, unit SSSP, CC labels
+and triangle counts bit-exact; PageRank / PPR / PPR gradient within 1e-5
+relative L1 of fp64."""
+import numpy as np
+import pytest
+
+from conftest import sha
+from gpu_cases import cases
+
+pytestmark = pytest.mark.gpu
+WIDTHS = [4, 8, 16, 32, 64]
+INF = 2147483647
+
+
+@pytest.fixture(scope="module")
+def graphs(gbo):
+    return cases(gbo)
+
+
+def rel_l1(a, b):
+    return float(np.abs(np.asarray(a, np.float64) - b).sum() / max(1e-300, np.abs(b).sum()))
+
+
+@pytest.mark.parametrize("b", WIDTHS)
+def test_bfs_and_sssp(gbo, orc, gpu, graphs, b):
+    for name, csr in graphs.items():
+        g = gbo.Graph.from_csr(csr, b)
+        for src in (0, csr.nrows // 2, csr.nrows - 1):
+            lv_ref, d_ref = orc.bfs_csr(csr.rowptr, csr.colind, csr.nrows, src)
+            lv, depth = g.bfs(src)
+            assert np.array_equal(lv, lv_ref), (name, b, src)
+            assert depth == d_ref
+            dist, _ = g.sssp(src)
+            assert np.array_equal(dist, np.where(lv_ref < 0, INF, lv_ref).astype(np.uint32)), (name, b)
+
+
+def test_bfs_golden(gbo, gpu, golden):
+    for key, csr in (("er1000", gbo.gen_er(1000, 0.02002, 0)), ("rmat12", gbo.gen_rmat(12, 16, seed=0)),
+                     ("mesh33", gbo.gen_king_mesh(33))):
+        g = gbo.Graph.from_csr(csr, 32)
+        lv, depth = g.bfs(0)
+        assert sha(lv) == golden[key]["bfs_levels_sha"] and depth == golden[key]["bfs_depth"]
+
+
+def test_bfs_transpose_directed(gbo, orc, gpu, graphs):
+    """Directed graph: the reference packs the CSC so BFS follows A's edges."""
+    a = graphs["ragged1001"]
+    at = a.transpose()
+    g = gbo.Graph.from_csr(a, 32, gbo.FLAG_TRANSPOSE)
+    lv, _ = g.bfs(3)
+    ref, _ = orc.bfs_csr(at.rowptr, at.colind, at.nrows, 3)
+    assert np.array_equal(lv, ref)
+
+
+@pytest.mark.parametrize("b", WIDTHS)
+def test_cc_min_label(gbo, orc, gpu, graphs, b):
+    for name, csr in graphs.items():
+        if name == "ragged1001":
+            continue  # CC needs a symmetric matrix
+        g = gbo.Graph.from_csr(csr, b)
+        lab, _ = g.cc()
+        want = orc.cc(csr.rowptr, csr.colind, csr.nrows)
+        assert np.array_equal(lab, want), (name, b)
+        assert orc.verify_cc(csr.rowptr, csr.colind, csr.nrows, lab)[0] == 0
+
+
+def test_cc_disconnected(gbo, orc, gpu):
+    rng = np.random.default_rng(9)
+    n = 5000
+    src = rng.integers(0, n, 2500)
+    dst = rng.integers(0, n, 2500)
+    csr = gbo.csr_from_edges(src, dst, n, True, True)
+    for b in WIDTHS:
+        lab, _ = gbo.Graph.from_csr(csr, b).cc()
+        assert np.array_equal(lab, orc.cc(csr.rowptr, csr.colind, n))
+
+
+@pytest.mark.parametrize("b", WIDTHS)
+def test_triangle_count(gbo, orc, gpu, graphs, b):
+    for name, csr in graphs.items():
+        rows = np.repeat(np.arange(csr.nrows), np.diff(csr.rowptr))
+        if name == "ragged1001" or np.any(rows == csr.colind):
+            continue  # TC is defined on simple undirected graphs
+        g = gbo.Graph.from_csr(csr, b, gbo.FLAG_LOWER)
+        assert g.tc() == orc.tc_csr(csr.rowptr, csr.colind, csr.nrows), (name, b)
+
+
+def test_triangle_mesh_closed_form(gbo, gpu):
+    for side in (2, 3, 64, 257):
+        m = gbo.gen_king_mesh(side)
+        for b in (8, 16, 32, 64):
+            assert gbo.Graph.from_csr(m, b, gbo.FLAG_LOWER).tc() == 4 * (side - 1) ** 2
+
+
+@pytest.mark.parametrize("b", WIDTHS)
+def test_pagerank(gbo, orc, gpu, graphs, b):
+    for name, csr in graphs.items():
+        g = gbo.Graph.from_csr(csr, b)
+        outdeg = np.bincount(csr.colind, minlength=csr.ncols).astype(np.int32)
+        p, it = g.pagerank(0.85, 20, -1.0)
+        assert it == 20
+        p64, _ = orc.pagerank_f64(csr.rowptr, csr.colind, csr.nrows, outdeg, 0.85, 20, -1.0)
+        assert rel_l1(p, p64) <= 1e-5, (name, b, rel_l1(p, p64))
+        # tolerance mode stops like the reference loop (pr.cu:449)
+        p2, it2 = g.pagerank(0.85, 1000, 1e-6)
+        p64b, it64 = orc.pagerank_f64(csr.rowptr, csr.colind, csr.nrows, outdeg, 0.85, 1000, 1e-6)
+        assert abs(it2 - it64) <= 1 and rel_l1(p2, p64b) <= 1e-5
+
+
+@pytest.mark.parametrize("b", [8, 32, 64])
+def test_ppr_forward_backward(gbo, orc, gpu, b):
+    csr = gbo.gen_rmat(12, 16, seed=1)
+    n = csr.nrows
+    outdeg = np.bincount(csr.colind, minlength=n).astype(np.int32)
+    rng = np.random.default_rng(4)
+    v = np.zeros(n)
+    idx = rng.choice(n, max(1, n // 100), replace=False)
+    v[idx] = rng.dirichlet(np.ones(len(idx)))
+    w = rng.standard_normal(n)
+    g = gbo.Graph.from_csr(csr, b)
+    p, _ = g.ppr_forward(v.astype(np.float32), 0.85, 1e-7, 1000)
+    p64, _ = orc.ppr_f64(csr.rowptr, csr.colind, n, outdeg, v, 0.85, 1e-13)
+    assert rel_l1(p, p64) <= 1e-5
+    grad, _ = g.ppr_backward(w.astype(np.float32), 0.85, 1e-7, 1000)
+    g64, _ = orc.ppr_adjoint_f64(csr.rowptr, csr.colind, n, outdeg, w, 0.85, 1e-13)
+    assert rel_l1(grad, g64) <= 1e-5
+    # central finite differences of L = w . p(v) through the GPU forward pass
+    for _ in range(8):
+        d = np.zeros(n)
+        d[idx] = rng.standard_normal(len(idx))
+        pp, _ = g.ppr_forward((v + 1e-3 * d).astype(np.float32), 0.85, 1e-9, 2000)
+        pm, _ = g.ppr_forward((v - 1e-3 * d).astype(np.float32), 0.85, 1e-9, 2000)
+        fd = (w @ pp.astype(np.float64) - w @ pm.astype(np.float64)) / 2e-3
+        assert abs(fd - grad @ d) <= 2e-3 * max(1.0, abs(fd)) + 1e-4
