@@ -766,8 +766,8 @@ struct StepTimer {
   AlgoState* a;
   cudaStream_t s;
   int k;
-  void begin() const { cudaEventRecord(a->ev[2 * k], s); }
-  void end() const { cudaEventRecord(a->ev[2 * k + 1], s); }
+  void begin() const { cudaEventRecordWithFlags(a->ev[2 * k], s, cudaEventRecordExternal); }
+  void end() const { cudaEventRecordWithFlags(a->ev[2 * k + 1], s, cudaEventRecordExternal); }
 };
 
 // Replay the captured iterations until the device sets `done`.
@@ -786,7 +786,10 @@ int run_until_done(AlgoState* a, int id, cudaStream_t s, int max_iter, int* iter
     const int it1 = a->h_ctrl->iter;
     for (int q = 0; q < it1 - it0 && q < kStepsPerGraph; ++q) {
       float ms = 0.f;
-      if (cudaEventElapsedTime(&ms, a->ev[2 * q], a->ev[2 * q + 1]) != cudaSuccess) ms = -1.f;
+      if (cudaEventElapsedTime(&ms, a->ev[2 * q], a->ev[2 * q + 1]) != cudaSuccess) {
+        ms = -1.f;
+        (void)cudaGetLastError();
+      }
       a->step_ms.push_back(ms);
     }
     it0 = it1;

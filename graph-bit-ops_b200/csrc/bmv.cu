@@ -234,7 +234,16 @@ __device__ __forceinline__ typename SRT<SR>::A sr_term(const typename SRT<SR>::V
 struct SrParams {
   float alpha, add;
   const float* scale;
+  const int* degptr;  // when set: x[j] / (degptr[j+1] - degptr[j]) (the reference's form)
 };
+
+// Float term with the per-column degree read from a CSR row pointer at every
+// set bit, as bmv32_sparse_full does (algorithm/bsrbmv.cu:1277).
+__device__ __forceinline__ double float_term_deg(const float* __restrict__ x,
+                                                 const int* __restrict__ degptr, long long j) {
+  const int d = degptr[j + 1] - degptr[j];
+  return d > 0 ? (double)(x[j] / (float)d) : 0.0;
+}
 
 template <int SR>
 __device__ __forceinline__ typename SRT<SR>::V sr_finish(typename SRT<SR>::A acc,
@@ -266,6 +275,14 @@ __global__ void __launch_bounds__(kTPB) k_semiring(GView v, const typename SRT<S
   for (int t = it.t0; t < it.t1; ++t) {
     const long long base = (long long)v.colind[t] * B;
     const WT w0 = val[(size_t)t * B + r];
+    if (SR == SR_FLOAT && p.degptr) {
+      for_each_col<B>(w0, [&](int j) { acc0 += (A)float_term_deg((const float*)x, p.degptr, base + j); });
+      if (L::RPL == 2) {
+        const WT w1 = val[(size_t)t * B + 32 + r];
+        for_each_col<B>(w1, [&](int j) { acc1 += (A)float_term_deg((const float*)x, p.degptr, base + j); });
+      }
+      continue;
+    }
     for_each_col<B>(w0, [&](int j) { sr_combine<SR>(acc0, sr_term<SR>(x, p.scale, base + j)); });
     if (L::RPL == 2) {
       const WT w1 = val[(size_t)t * B + 32 + r];
@@ -453,7 +470,7 @@ int bmv_masked(const gbo_graph* g, const void* x, const void* mask, void* out, v
 
 int bmv_minplus(const gbo_graph* g, const uint32_t* x, uint32_t* y, void* scratch, cudaStream_t s) {
   GView v = view_of(g);
-  SrParams p{1.f, 0.f, nullptr};
+  SrParams p{1.f, 0.f, nullptr, nullptr};
   int st = GBO_OK;
   GBO_DISPATCH_B(g->b, st = (semiring_impl<B, SR_MINPLUS>(v, x, y, p, scratch, s)));
   return st;
@@ -461,16 +478,16 @@ int bmv_minplus(const gbo_graph* g, const uint32_t* x, uint32_t* y, void* scratc
 
 int bmv_minselect(const gbo_graph* g, const int32_t* x, int32_t* y, void* scratch, cudaStream_t s) {
   GView v = view_of(g);
-  SrParams p{1.f, 0.f, nullptr};
+  SrParams p{1.f, 0.f, nullptr, nullptr};
   int st = GBO_OK;
   GBO_DISPATCH_B(g->b, st = (semiring_impl<B, SR_MINSEL>(v, x, y, p, scratch, s)));
   return st;
 }
 
 int bmv_float(const gbo_graph* g, const float* x, float* y, float alpha, const float* scale,
-              float add, void* scratch, cudaStream_t s) {
+              float add, void* scratch, cudaStream_t s, const int* degptr) {
   GView v = view_of(g);
-  SrParams p{alpha, add, scale};
+  SrParams p{alpha, add, scale, degptr};
   int st = GBO_OK;
   GBO_DISPATCH_B(g->b, st = (semiring_impl<B, SR_FLOAT>(v, x, y, p, scratch, s)));
   return st;

@@ -30,7 +30,7 @@ int bmv_masked(const gbo_graph* g, const void* x, const void* mask, void* out, v
 int bmv_minplus(const gbo_graph* g, const uint32_t* x, uint32_t* y, void* scratch, cudaStream_t s);
 int bmv_minselect(const gbo_graph* g, const int32_t* x, int32_t* y, void* scratch, cudaStream_t s);
 int bmv_float(const gbo_graph* g, const float* x, float* y, float alpha, const float* scale,
-              float add, void* scratch, cudaStream_t s);
+              float add, void* scratch, cudaStream_t s, const int* degptr = nullptr);
 int bmv_float_transposed(const gbo_graph* g, const float* x, float* y, float alpha,
                          const float* scale, float add, cudaStream_t s);
 

@@ -27,7 +27,12 @@ int fail_cuda(cudaError_t err, const char* what) {
   return GBO_ERR_CUDA;
 }
 
-void clear_error() { g_last_error.clear(); }
+// Also drops a stale non-sticky CUDA error left by an earlier call, so that
+// the cudaGetLastError() checks after our launches report our own launches.
+void clear_error() {
+  g_last_error.clear();
+  (void)cudaGetLastError();
+}
 
 int num_sms() {
   static thread_local int cached = 0;

@@ -316,6 +316,7 @@ extern "C" int gbo_bmv_minplus(const gbo_graph* g, const uint32_t* d_x, uint32_t
   if (g->nrows > 0 && (!d_x || !d_y)) return fail(GBO_ERR_INVALID, "NULL vector");
   if (g->layout != GBO_LAYOUT_ROW) return fail(GBO_ERR_UNSUPPORTED, "BMV needs the ROW tile layout");
   if (d_x == d_y) return fail(GBO_ERR_INVALID, "x and y must not alias");
+  if (g->nrows > g->ncols) return fail(GBO_ERR_INVALID, "min-plus over (P + I) needs nrows <= ncols");
   return bmv_minplus(g, d_x, d_y, g->ws, as_stream(stream));
 }
 
@@ -327,6 +328,16 @@ extern "C" int gbo_bmv_float(const gbo_graph* g, const float* d_x, float* d_y, f
   if (g->layout != GBO_LAYOUT_ROW) return fail(GBO_ERR_UNSUPPORTED, "BMV needs the ROW tile layout");
   if (d_x == d_y) return fail(GBO_ERR_INVALID, "x and y must not alias");
   return bmv_float(g, d_x, d_y, alpha, d_scale, add, g->ws, as_stream(stream));
+}
+
+extern "C" int gbo_bmv_float_degptr(const gbo_graph* g, const float* d_x, float* d_y, float alpha,
+                                    const int* d_csrRowPtr, gbo_stream_t stream) {
+  clear_error();
+  GBO_TRY(check_graph(g));
+  if (g->nrows > 0 && (!d_x || !d_y || !d_csrRowPtr)) return fail(GBO_ERR_INVALID, "NULL vector");
+  if (g->layout != GBO_LAYOUT_ROW) return fail(GBO_ERR_UNSUPPORTED, "BMV needs the ROW tile layout");
+  if (d_x == d_y) return fail(GBO_ERR_INVALID, "x and y must not alias");
+  return bmv_float(g, d_x, d_y, alpha, nullptr, 0.f, g->ws, as_stream(stream), d_csrRowPtr);
 }
 
 extern "C" int gbo_bmv_minselect(const gbo_graph* g, const int32_t* d_x, int32_t* d_y,

@@ -691,3 +691,18 @@ extern "C" int gbo_unpack_vector(const void* d_bits, int n, int tile_bits, int32
   GBO_CUDA_TRY(cudaGetLastError());
   return GBO_OK;
 }
+
+extern "C" int gbo_invdeg_from_rowptr(const int* d_rowptr, int n, float* d_inv, gbo_stream_t stream) {
+  clear_error();
+  if (n < 0 || (n > 0 && (!d_rowptr || !d_inv))) return fail(GBO_ERR_INVALID, "invdeg: bad argument");
+  if (n == 0) return GBO_OK;
+  cudaStream_t s = as_stream(stream);
+  int* deg = nullptr;
+  GBO_CUDA_TRY(cudaMallocAsync(&deg, sizeof(int) * (size_t)n, s));
+  k_row_len<<<blocks_for(n, 256), 256, 0, s>>>(d_rowptr, n, deg);
+  k_inv<<<blocks_for(n, 256), 256, 0, s>>>(deg, n, d_inv);
+  cudaError_t e = cudaGetLastError();
+  cudaFreeAsync(deg, s);
+  if (e != cudaSuccess) return fail_cuda(e, "invdeg kernels");
+  return GBO_OK;
+}

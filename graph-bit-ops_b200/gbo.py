@@ -100,6 +100,7 @@ _SIGS = {
     "gbo_pack_vector_f32": (_I, [_P, _I, _I, _P, _P]),
     "gbo_pack_vector_i32": (_I, [_P, _I, _I, _P, _P]),
     "gbo_unpack_vector": (_I, [_P, _I, _I, _P, _P]),
+    "gbo_invdeg_from_rowptr": (_I, [_P, _I, _P, _P]),
     "gbo_graph_from_csr": (_I, [_P, _P, _I, _I, _I, _I, _I, _P, C.POINTER(_P)]),
     "gbo_graph_wrap_b2sr": (_I, [_I, _I, _I, _I, _I, _P, _P, _P, _P, _P, C.POINTER(_P)]),
     "gbo_graph_free": (_I, [_P]),
@@ -110,6 +111,7 @@ _SIGS = {
     "gbo_bmv_masked": (_I, [_P, _P, _P, _P, _P]),
     "gbo_bmv_minplus": (_I, [_P, _P, _P, _P]),
     "gbo_bmv_float": (_I, [_P, _P, _P, C.c_float, _P, C.c_float, _P]),
+    "gbo_bmv_float_degptr": (_I, [_P, _P, _P, C.c_float, _P, _P]),
     "gbo_bmv_minselect": (_I, [_P, _P, _P, _P]),
     "gbo_bmv_float_transposed": (_I, [_P, _P, _P, C.c_float, _P, C.c_float, _P]),
     "gbo_bfs": (_I, [_P, _I, _P, C.POINTER(_I), _P]),

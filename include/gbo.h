@@ -114,6 +114,11 @@ GBO_API int gbo_pack_vector_f32(const float* d_x, int n, int tile_bits, void* d_
                         gbo_stream_t stream);
 GBO_API int gbo_pack_vector_i32(const int32_t* d_x, int n, int tile_bits, void* d_bits,
                         gbo_stream_t stream);
+/* inv[i] = 1 / (rowptr[i+1] - rowptr[i]) (0 for empty rows), n entries: the
+ * per-column scale the reference recomputes at every set bit
+ * (algorithm/bsrbmv.cu:1277) precomputed once.  Device pointers. */
+GBO_API int gbo_invdeg_from_rowptr(const int* d_rowptr, int n, float* d_inv,
+                           gbo_stream_t stream);
 /* Bit vector -> int32 0/1 per element (n elements). */
 GBO_API int gbo_unpack_vector(const void* d_bits, int n, int tile_bits, int32_t* d_out,
                       gbo_stream_t stream);
@@ -190,6 +195,13 @@ GBO_API int gbo_bmv_minplus(const gbo_graph* g, const uint32_t* d_x, uint32_t* d
 GBO_API int gbo_bmv_float(const gbo_graph* g, const float* d_x, float* d_y,
                   float alpha, const float* d_scale, float add,
                   gbo_stream_t stream);
+/* The reference's own form of the fp32 BMV: y[i] = alpha * sum_{j: P[i][j]}
+ * x[j] / (csrRowPtr[j+1] - csrRowPtr[j]), the degree read from a CSR row
+ * pointer only at set bits (bmv32_sparse_full, algorithm/bsrbmv.cu:1239-1286,
+ * which writes C = sum; the caller adds (1-alpha)/n, pr.cu:486). */
+GBO_API int gbo_bmv_float_degptr(const gbo_graph* g, const float* d_x, float* d_y,
+                         float alpha, const int* d_csrRowPtr,
+                         gbo_stream_t stream);
 /* y[i] = min_{j: P[i][j]} x[j], INT32_MAX when row i is empty.
  * bmv{4,8,16,32}_sparse_full_cc* (bsrbmv.cu:1367-2099). */
 GBO_API int gbo_bmv_minselect(const gbo_graph* g, const int32_t* d_x, int32_t* d_y,

@@ -40,6 +40,9 @@ def test_bfs_golden(gbo, gpu, golden):
         g = gbo.Graph.from_csr(csr, 32)
         lv, depth = g.bfs(0)
         assert sha(lv) == golden[key]["bfs_levels_sha"] and depth == golden[key]["bfs_depth"]
+        st = g.last_run()  # per-level kernel times from events inside the loop graph
+        assert st["iterations"] == depth and len(st["step_ms"]) == depth
+        assert all(ms >= 0 for ms in st["step_ms"]) and st["kernel_launches"] > depth
 
 
 def test_bfs_transpose_directed(gbo, orc, gpu, graphs):
