@@ -14,7 +14,7 @@
 #include <algorithm>
 #include <vector>
 
-#include "bmv.cuh"
+#include "scan.cuh"
 
 namespace gbo {
 
@@ -75,13 +75,6 @@ constexpr int kTPB = 256;
 constexpr int kStepsPerGraph = 8;
 
 enum AlgoId { A_BFS = 0, A_SSSP = 1, A_PR = 2, A_CC = 3, A_PPR_F = 4, A_PPR_B = 5 };
-
-template <int B>
-struct Lay {
-  static constexpr int W = B >= 32 ? 32 : B;
-  static constexpr int G = 32 / W;
-  static constexpr int RPL = B > 32 ? 2 : 1;
-};
 
 template <int B>
 __device__ __forceinline__ typename Word<B>::T full_word() {
@@ -193,17 +186,11 @@ __global__ void __launch_bounds__(kTPB) k_bfs_step(GView v, typename Word<B>::T*
   const WT full = full_word<B>();
   const WT vis = active ? visited[it.row] : full;
   bool p0 = false, p1 = false;
-  if (active && (vis & full) != full) {
-    const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
-    const bool need0 = !bit_of<B>(vis, r);
-    const bool need1 = L::RPL == 2 && !bit_of<B>(vis, r + 32);
-    for (int t = it.t0; t < it.t1; ++t) {
-      const WT xs = x[v.colind[t]];
-      if (xs) {
-        if (need0 && !p0) p0 = (val[(size_t)t * B + r] & xs) != 0;
-        if (need1 && !p1) p1 = (val[(size_t)t * B + 32 + r] & xs) != 0;
-      }
-    }
+  if (active && (vis & full) != full) {  // uniform inside the item's lane group
+    const long long row0 = (long long)it.row * B + r;
+    const bool need0 = !bit_of<B>(vis, r) && row0 < v.nrows;
+    const bool need1 = L::RPL == 2 && !bit_of<B>(vis, r + 32) && row0 + 32 < v.nrows;
+    pull_or_scan<B>(v, it.t0, it.t1, x, need0, need1, p0, p1, lane);
   }
   const WT word = gather_bits<B>(p0, p1, lane);
   unsigned long long cnt = 0;
@@ -305,24 +292,52 @@ __global__ void __launch_bounds__(kTPB) k_sssp_step(GView v, typename Word<B>::T
   const WT full = full_word<B>();
   const WT vis = active ? visited[it.row] : full;
   uint32_t a0 = (uint32_t)kINF, a1 = (uint32_t)kINF;
-  if (active && (vis & full) != full) {
+  if (active && (vis & full) != full) {  // uniform inside the item's lane group
+    constexpr int W = L::W;
+    const unsigned gmask = group_mask<B>(lane);
+    const unsigned gshift = (lane / W) * W;
     const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
-    for (int t = it.t0; t < it.t1; ++t) {
-      const int c = v.colind[t];
-      const WT xs = x[c];
-      if (xs) {
-        const long long base = (long long)c * B;
-        const WT m0 = val[(size_t)t * B + r] & xs;
-        for_each_col<B>(m0, [&](int j) {
-          uint32_t d = dist[base + j];
-          a0 = min(a0, d >= (uint32_t)kINF ? (uint32_t)kINF : d + 1u);
-        });
-        if (L::RPL == 2) {
-          const WT m1 = val[(size_t)t * B + 32 + r] & xs;
-          for_each_col<B>(m1, [&](int j) {
-            uint32_t d = dist[base + j];
-            a1 = min(a1, d >= (uint32_t)kINF ? (uint32_t)kINF : d + 1u);
-          });
+    auto relax = [&](uint32_t& acc, WT m, long long base) {
+      for_each_col<B>(m, [&](int j) {
+        uint32_t d = dist[base + j];
+        acc = min(acc, d >= (uint32_t)kINF ? (uint32_t)kINF : d + 1u);
+      });
+    };
+    // block-column indices W at a time, x gathered in parallel, tile words
+    // fetched only for tiles with a non-empty frontier segment
+    for (int b0 = it.t0; b0 < it.t1; b0 += W) {
+      const int t = b0 + r;
+      int c = 0;
+      WT xs = 0;
+      if (t < it.t1) {
+        c = v.colind[t];
+        xs = x[c];
+      }
+      unsigned nz = (__ballot_sync(gmask, xs != 0) >> gshift) & seg_mask<W>();
+      while (nz) {
+        int j[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          j[q] = nz ? __ffs(nz) - 1 : -1;
+          nz &= nz - 1;
+        }
+        WT xv[4], w0[4] = {0, 0, 0, 0}, w1[4] = {0, 0, 0, 0};
+        int cv[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          xv[q] = shfl_word<WT>(gmask, xs, j[q] < 0 ? 0 : j[q], W);
+          cv[q] = __shfl_sync(gmask, c, j[q] < 0 ? 0 : j[q], W);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (j[q] >= 0) {
+            w0[q] = val[(size_t)(b0 + j[q]) * B + r];
+            if (L::RPL == 2) w1[q] = val[(size_t)(b0 + j[q]) * B + 32 + r];
+          }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          relax(a0, (WT)(w0[q] & xv[q]), (long long)cv[q] * B);
+          if (L::RPL == 2) relax(a1, (WT)(w1[q] & xv[q]), (long long)cv[q] * B);
         }
       }
     }

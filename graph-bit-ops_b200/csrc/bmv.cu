@@ -13,20 +13,13 @@
 // loads of one tile are contiguous) and combines it with the x segment of
 // the tile's block column.  Items that cover a chunk of a split row write
 // partial results to scratch; k_reduce_* combines them in slot order.
-#include "bmv.cuh"
+#include "scan.cuh"
 
 namespace gbo {
 
 namespace {
 
 constexpr int kTPB = 256;
-
-template <int B>
-struct Lay {
-  static constexpr int W = B >= 32 ? 32 : B;  // lanes per item
-  static constexpr int G = 32 / W;            // items per warp
-  static constexpr int RPL = B > 32 ? 2 : 1;  // rows per lane
-};
 
 // Left-align a b-bit word in 32 or 64 bits so that column 0 is the MSB.
 template <int B>
@@ -160,15 +153,12 @@ __global__ void __launch_bounds__(kTPB) k_masked(GView v, const typename Word<B>
   WT mk = 0;
   if (active && mask) mk = mask[it.row];
   bool p0 = false, p1 = false;
-  if (active && (mk & full) != full) {
-    const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
-    for (int t = it.t0; t < it.t1; ++t) {
-      const WT xs = x[v.colind[t]];
-      if (xs) {  // tiles whose x segment is empty contribute nothing
-        p0 |= (val[(size_t)t * B + r] & xs) != 0;
-        if (L::RPL == 2) p1 |= (val[(size_t)t * B + 32 + r] & xs) != 0;
-      }
-    }
+  if (active && (mk & full) != full) {  // uniform inside the item's lane group
+    // masked-out rows need no answer: their output bit is cleared anyway;
+    // tiles whose x segment is empty contribute nothing and are not read
+    const bool need0 = !((mk >> (B - 1 - r)) & 1);
+    const bool need1 = L::RPL == 2 && !((mk >> (B - 1 - (r + 32) % B)) & 1);
+    pull_or_scan<B>(v, it.t0, it.t1, x, need0, need1, p0, p1, lane);
   }
   const WT word = gather_bits<B>(p0, p1, lane);
   if (!active || r != 0) return;
