@@ -53,6 +53,8 @@ struct AlgoState {
   int* f = nullptr;
   int* gf = nullptr;
   int* mngf = nullptr;
+  int* seeds = nullptr;  // multi-seed BFS sources
+  int nseeds_cap = 0;
   double* acc64 = nullptr;  // PPR adjoint scatter accumulator
   void* scratch = nullptr;  // split partials (nslots * b * 8 bytes)
   cudaGraphExec_t exec[8] = {};
@@ -246,6 +248,21 @@ __global__ void k_bfs_finish(GView v, typename Word<B>::T* __restrict__ front,
   });
 }
 
+// Level-0 vertices of a multi-seed BFS (one thread: seeds may share words).
+template <int B>
+__global__ void k_bfs_seed(const int* __restrict__ seeds, int nseeds, typename Word<B>::T* front,
+                           typename Word<B>::T* visited, int* level) {
+  using WT = typename Word<B>::T;
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  for (int q = 0; q < nseeds; ++q) {
+    const int v0 = seeds[q];
+    const WT bit = (WT)((WT)1 << (B - 1 - v0 % B));
+    front[v0 / B] = (WT)(front[v0 / B] | bit);
+    visited[v0 / B] = (WT)(visited[v0 / B] | bit);
+    level[v0] = 0;
+  }
+}
+
 template <int B>
 __global__ void k_bfs_init(typename Word<B>::T* front, typename Word<B>::T* visited, int* level,
                            int nbr, int n, int src, Ctrl* ctrl, int max_iter) {
@@ -254,7 +271,7 @@ __global__ void k_bfs_init(typename Word<B>::T* front, typename Word<B>::T* visi
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long k = i; k < n; k += stride) level[k] = (k == src) ? 0 : -1;
   for (long long k = i; k < nbr; k += stride) {
-    WT w = (k == src / B) ? (WT)((WT)1 << (B - 1 - src % B)) : (WT)0;
+    WT w = (src >= 0 && k == src / B) ? (WT)((WT)1 << (B - 1 - src % B)) : (WT)0;
     front[k] = w;
     front[nbr + k] = 0;
     visited[k] = w;
@@ -824,8 +841,10 @@ int run_until_done(AlgoState* a, int id, cudaStream_t s, int max_iter, int* iter
     default: { constexpr int B = 64; CALL; } break; \
   }
 
+// src >= 0: one source passed by value; otherwise nseeds seeds from h_seeds.
 template <int B>
-int bfs_impl(gbo_graph* g, int src, int32_t* d_level, int* h_depth, cudaStream_t s) {
+int bfs_impl(gbo_graph* g, int src, const int* h_seeds, int nseeds, int32_t* d_level, int* h_depth,
+             cudaStream_t s) {
   using WT = typename Word<B>::T;
   AlgoState* a = nullptr;
   GBO_TRY(get_state(g, &a));
@@ -852,6 +871,17 @@ int bfs_impl(gbo_graph* g, int src, int32_t* d_level, int* h_depth, cudaStream_t
   const int max_iter = g->nrows + 1;
   k_bfs_init<B><<<grid_vertex(std::max(g->nrows, g->nbr)), kTPB, 0, s>>>(front, vis, level, g->nbr,
                                                                        g->nrows, src, ctrl, max_iter);
+  if (src < 0) {
+    if (a->nseeds_cap < nseeds) {
+      cudaFree(a->seeds);
+      a->seeds = nullptr;
+      GBO_CUDA_TRY(cudaMalloc(&a->seeds, sizeof(int) * (size_t)nseeds));
+      a->nseeds_cap = nseeds;
+    }
+    GBO_CUDA_TRY(cudaMemcpyAsync(a->seeds, h_seeds, sizeof(int) * (size_t)nseeds,
+                                 cudaMemcpyHostToDevice, s));
+    k_bfs_seed<B><<<1, 32, 0, s>>>(a->seeds, nseeds, front, vis, level);
+  }
   GBO_CUDA_TRY(cudaGetLastError());
   int iters = 0;
   GBO_TRY(run_until_done(a, A_BFS, s, max_iter, &iters));
@@ -1048,6 +1078,7 @@ void free_algo_state(gbo_graph* g) {
   cudaFree(a->gf);
   cudaFree(a->mngf);
   cudaFree(a->acc64);
+  cudaFree(a->seeds);
   cudaFree(a->scratch);
   if (a->cap) cudaStreamDestroy(a->cap);
   delete a;
@@ -1066,9 +1097,18 @@ extern "C" int gbo_bfs(const gbo_graph* gc, int src, int32_t* d_level, int* h_de
   if (src < 0 || src >= g->nrows) return fail(GBO_ERR_INVALID, "source vertex out of range");
   if (!d_level) return fail(GBO_ERR_INVALID, "level is NULL");
   int st = GBO_OK;
-  ALGO_DISPATCH_B(g->b, st = bfs_impl<B>(g, src, d_level, h_depth, as_stream(stream)));
+  ALGO_DISPATCH_B(g->b, st = bfs_impl<B>(g, src, nullptr, 0, d_level, h_depth, as_stream(stream)));
   return st;
 }
+
+namespace gbo {
+int bfs_seeded(gbo_graph* g, const int* h_seeds, int nseeds, int32_t* d_level, int* h_depth,
+               cudaStream_t s) {
+  int st = GBO_OK;
+  ALGO_DISPATCH_B(g->b, st = bfs_impl<B>(g, -1, h_seeds, nseeds, d_level, h_depth, s));
+  return st;
+}
+}  // namespace gbo
 
 extern "C" int gbo_sssp_unit(const gbo_graph* gc, int src, uint32_t* d_dist, int* h_iters,
                              gbo_stream_t stream) {

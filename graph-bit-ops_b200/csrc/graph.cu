@@ -110,6 +110,7 @@ void destroy(gbo_graph* g) {
   cudaFree(g->splits);
   cudaFree(g->ws);
   free_algo_state(g);
+  free_ms_state(g);
   delete g;
 }
 

@@ -40,6 +40,7 @@ struct gbo_graph {
   long long device_bytes = 0;
   // device state and captured CUDA graphs of the iteration loops
   struct AlgoState* algo = nullptr;
+  void* ms = nullptr;  // multi-source BFS state
 };
 
 namespace gbo {
@@ -79,5 +80,6 @@ int upload_outdeg(gbo_graph* g, const int* h_deg, int n, cudaStream_t stream);
 void launch_invdeg(const int* d_deg, int n, float* d_inv, cudaStream_t stream);
 // Release the algorithm state of g (called by gbo_graph_free).
 void free_algo_state(gbo_graph* g);
+void free_ms_state(gbo_graph* g);
 
 }  // namespace gbo

@@ -504,3 +504,70 @@ extern "C" int gbo_gen_king_mesh(int side, gbo_csr** out) {
   *out = g;
   return GBO_OK;
 }
+
+// A batch of independent G(n, m) graphs as one block-diagonal CSR: graph i
+// has n_i vertices, log-uniform in [nmin, nmax] (drawn from stream i of
+// `seed`), and round(n_i * avg_degree / 2) uniformly drawn pairs from its own
+// seed `seed + 1000 + i`.  offsets (count+1 entries) receives the first vertex
+// of every graph.
+extern "C" int gbo_gen_er_batch(int count, int nmin, int nmax, double avg_degree, uint64_t seed,
+                                gbo_csr** out, int* offsets) {
+  clear_error();
+  if (!out || !offsets || count < 1 || nmin < 1 || nmax < nmin || avg_degree < 0)
+    return fail(GBO_ERR_INVALID, "bad batch parameters");
+  std::vector<long long> off((size_t)count + 1, 0);
+  const double l0 = std::log((double)nmin), l1 = std::log((double)nmax + 1.0);
+  for (int i = 0; i < count; ++i) {
+    Xoshiro rng(seed, (uint64_t)i);
+    long long n = (long long)std::floor(std::exp(l0 + (l1 - l0) * rng.uniform()));
+    if (n < nmin) n = nmin;
+    if (n > nmax) n = nmax;
+    off[(size_t)i + 1] = off[(size_t)i] + n;
+  }
+  if (off[(size_t)count] > 2147483647LL) return fail(GBO_ERR_OVERFLOW, "batch has more than 2^31-1 vertices");
+  const int N = (int)off[(size_t)count];
+  std::vector<std::vector<int>> adj_ptr((size_t)count), adj_col((size_t)count);
+  long long total = 0;
+  int st_all = GBO_OK;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : total)
+  for (int i = 0; i < count; ++i) {
+    const int n = (int)(off[(size_t)i + 1] - off[(size_t)i]);
+    const long long m = (long long)std::llround((double)n * avg_degree / 2.0);
+    std::vector<int> rows((size_t)m * 2), cols((size_t)m * 2);
+    for (long long k = 0; k < m; ++k) {
+      Xoshiro rng(seed + 1000 + (uint64_t)i, (uint64_t)k);
+      int u = (int)rng.below((uint64_t)n), v = (int)rng.below((uint64_t)n);
+      rows[(size_t)(2 * k)] = u;
+      cols[(size_t)(2 * k)] = v;
+      rows[(size_t)(2 * k + 1)] = v;
+      cols[(size_t)(2 * k + 1)] = u;
+    }
+    gbo_csr* c = nullptr;
+    if (csr_from_pairs(rows, cols, n, n, true, true, &c) != GBO_OK) {
+      st_all = GBO_ERR_NOMEM;
+      continue;
+    }
+    adj_ptr[(size_t)i].assign(c->rowptr, c->rowptr + n + 1);
+    adj_col[(size_t)i].assign(c->colind, c->colind + c->nnz);
+    total += c->nnz;
+    gbo_csr_free(c);
+  }
+  if (st_all != GBO_OK) return fail(st_all, "batch generation");
+  if (total > 2147483647LL) return fail(GBO_ERR_OVERFLOW, "batch has more than 2^31-1 entries");
+  gbo_csr* g = new_csr(N, N, total);
+  if (!g) return fail(GBO_ERR_NOMEM, "host CSR allocation");
+  std::vector<long long> eoff((size_t)count + 1, 0);
+  for (int i = 0; i < count; ++i) eoff[(size_t)i + 1] = eoff[(size_t)i] + (long long)adj_col[(size_t)i].size();
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int i = 0; i < count; ++i) {
+    const int base = (int)off[(size_t)i];
+    const int n = (int)(off[(size_t)i + 1] - off[(size_t)i]);
+    for (int r = 0; r < n; ++r) g->rowptr[base + r] = (int)(eoff[(size_t)i] + adj_ptr[(size_t)i][(size_t)r]);
+    const std::vector<int>& cc = adj_col[(size_t)i];
+    for (size_t k = 0; k < cc.size(); ++k) g->colind[eoff[(size_t)i] + (long long)k] = cc[k] + base;
+  }
+  g->rowptr[N] = (int)total;
+  for (int i = 0; i <= count; ++i) offsets[i] = (int)off[(size_t)i];
+  *out = g;
+  return GBO_OK;
+}

@@ -49,26 +49,31 @@ __device__ __forceinline__ void pull_or_scan(const GView& v, int t0, int t1,
   const int r = lane % W;
   const unsigned gshift = (lane / W) * W;
   const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
+  constexpr int U = 8;  // tile words in flight per lane
+  // the next batch's block-column indices are loaded while this batch runs
+  int cnext = (t0 + r < t1) ? v.colind[t0 + r] : -1;
   for (int base = t0; base < t1; base += W) {
-    const int t = base + r;
-    WT xs = 0;
-    if (t < t1) xs = x[v.colind[t]];
+    const int cb = cnext;
+    cnext = (base + W + r < t1) ? v.colind[base + W + r] : -1;
+    const WT xs = cb >= 0 ? x[cb] : (WT)0;
     unsigned nz = (__ballot_sync(gmask, xs != 0) >> gshift) & seg_mask<W>();
     while (nz) {
-      int j[4];
+      int j[U];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < U; ++q) {
         j[q] = nz ? __ffs(nz) - 1 : -1;
         nz &= nz - 1;
       }
-      WT xv[4];
+      WT xv[U];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) xv[q] = shfl_word<WT>(gmask, xs, j[q] < 0 ? 0 : j[q], W);
+      for (int q = 0; q < U; ++q) xv[q] = shfl_word<WT>(gmask, xs, j[q] < 0 ? 0 : j[q], W);
       const bool l0 = need0 && !p0;
       const bool l1 = L::RPL == 2 && need1 && !p1;
-      WT a[4] = {0, 0, 0, 0}, c[4] = {0, 0, 0, 0};
+      WT a[U], c[U];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < U; ++q) {
+        a[q] = 0;
+        c[q] = 0;
         if (j[q] >= 0) {
           const size_t off = (size_t)(base + j[q]) * B;
           if (l0) a[q] = val[off + r];
@@ -76,7 +81,7 @@ __device__ __forceinline__ void pull_or_scan(const GView& v, int t0, int t1,
         }
       }
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < U; ++q) {
         p0 |= (a[q] & xv[q]) != 0;
         if (L::RPL == 2) p1 |= (c[q] & xv[q]) != 0;
       }

@@ -123,6 +123,8 @@ _SIGS = {
     "gbo_ppr_forward": (_I, [_P, _P, C.c_float, C.c_float, _I, _P, C.POINTER(_I), _P]),
     "gbo_ppr_backward": (_I, [_P, _P, C.c_float, C.c_float, _I, _P, C.POINTER(_I), _P]),
     "gbo_graph_last_run": (_I, [_P, C.POINTER(RunStats)]),
+    "gbo_msbfs": (_I, [_P, _P, _I, _P, C.POINTER(_I), _P]),
+    "gbo_bfs_multi": (_I, [_P, _P, _I, _P, C.POINTER(_I), _P]),
     "gbo_read_mtx": (_I, [C.c_char_p, _I, _I, C.POINTER(C.POINTER(CsrStruct))]),
     "gbo_csr_free": (_I, [C.POINTER(CsrStruct)]),
     "gbo_csr_transpose": (_I, [C.POINTER(CsrStruct), C.POINTER(C.POINTER(CsrStruct))]),
@@ -133,6 +135,7 @@ _SIGS = {
     "gbo_gen_er": (_I, [_I, C.c_double, C.c_uint64, C.POINTER(C.POINTER(CsrStruct))]),
     "gbo_gen_er_avgdeg": (_I, [_I, C.c_double, C.c_uint64, C.POINTER(C.POINTER(CsrStruct))]),
     "gbo_gen_king_mesh": (_I, [_I, C.POINTER(C.POINTER(CsrStruct))]),
+    "gbo_gen_er_batch": (_I, [_I, _I, _I, C.c_double, C.c_uint64, C.POINTER(C.POINTER(CsrStruct)), _P]),
 }
 
 _lib = None
@@ -367,6 +370,15 @@ def gen_er_avgdeg(n: int, avg_degree: float, seed: int = 0) -> Csr:
     return Csr._take(out)
 
 
+def gen_er_batch(count: int, nmin: int, nmax: int, avg_degree: float = 8.0, seed: int = 0):
+    """Block-diagonal union of `count` ER graphs; returns (Csr, offsets)."""
+    out = C.POINTER(CsrStruct)()
+    off = np.zeros(count + 1, np.int32)
+    check(lib().gbo_gen_er_batch(count, nmin, nmax, avg_degree, seed, C.byref(out), _ptr(off)),
+          "gen_er_batch")
+    return Csr._take(out), off
+
+
 def gen_king_mesh(side: int) -> Csr:
     out = C.POINTER(CsrStruct)()
     check(lib().gbo_gen_king_mesh(side, C.byref(out)), "gen_king_mesh")
@@ -473,6 +485,29 @@ class Graph:
         buf = out or DeviceBuffer(4 * n)
         depth = C.c_int(0)
         check(lib().gbo_bfs(self.h, src, buf.ptr, C.byref(depth), stream), "bfs")
+        if out is not None:
+            return depth.value
+        return buf.to_numpy(np.int32, n, stream), depth.value
+
+    def msbfs(self, srcs, out: DeviceBuffer | None = None, stream=None):
+        """Multi-source BFS; returns levels as an (n, k) int32 array (or the depth
+        when `out` is given)."""
+        srcs = np.ascontiguousarray(srcs, np.int32)
+        n, k = self.info().nrows, len(srcs)
+        buf = out or DeviceBuffer(4 * n * k)
+        depth = C.c_int(0)
+        check(lib().gbo_msbfs(self.h, _ptr(srcs), k, buf.ptr, C.byref(depth), stream), "msbfs")
+        if out is not None:
+            return depth.value
+        return buf.to_numpy(np.int32, n * k, stream).reshape(n, k), depth.value
+
+    def bfs_multi(self, seeds, out: DeviceBuffer | None = None, stream=None):
+        seeds = np.ascontiguousarray(seeds, np.int32)
+        n = self.info().nrows
+        buf = out or DeviceBuffer(4 * n)
+        depth = C.c_int(0)
+        check(lib().gbo_bfs_multi(self.h, _ptr(seeds), len(seeds), buf.ptr, C.byref(depth), stream),
+              "bfs_multi")
         if out is not None:
             return depth.value
         return buf.to_numpy(np.int32, n, stream), depth.value

@@ -244,6 +244,20 @@ GBO_API int gbo_tc(const gbo_graph* lower, uint64_t* h_count, gbo_stream_t strea
 GBO_API int gbo_tc_device(const gbo_graph* lower, unsigned long long* d_count,
                   gbo_stream_t stream);
 
+/* Multi-source BFS (batching): k sources (1 <= k <= 1024) traversed at once.
+ * The frontier is an n x k bit matrix, so every level is one B2SR x bit
+ * matrix product (OR.AND semiring).  d_levels: int32[n * k], vertex-major:
+ * d_levels[v * k + s] = hops from h_srcs[s] to v, -1 if unreachable.  Needs a
+ * square ROW-layout graph with 32x32 tiles.  No reference counterpart (the
+ * reference runs one source per traversal, algorithm/bfs.cu:445). */
+GBO_API int gbo_msbfs(const gbo_graph* g, const int* h_srcs, int k,
+              int32_t* d_levels, int* h_depth, gbo_stream_t stream);
+/* Multi-seed BFS: every vertex in h_seeds starts at level 0 of one frontier.
+ * On a block-diagonal union of independent graphs (gbo_gen_er_batch) with one
+ * seed per graph this is each graph's own BFS in one traversal. */
+GBO_API int gbo_bfs_multi(const gbo_graph* g, const int* h_seeds, int nseeds,
+                  int32_t* d_level, int* h_depth, gbo_stream_t stream);
+
 /* Personalized PageRank p = alpha * P D^-1 p + (1-alpha) v  (fp32) and its
  * adjoint: for loss L = dot(w, p), grad_v = (1-alpha) u with
  * u = alpha * D^-1 P^T u + w.  Iterate until the L1 change <= tol or
@@ -303,6 +317,11 @@ GBO_API int gbo_gen_rmat(int scale, int edge_factor, double a, double b, double 
 GBO_API int gbo_gen_er(int n, double p, uint64_t seed, gbo_csr** out);
 GBO_API int gbo_gen_er_avgdeg(int n, double avg_degree, uint64_t seed, gbo_csr** out);
 GBO_API int gbo_gen_king_mesh(int side, gbo_csr** out);
+/* count independent G(n, m) graphs as one block-diagonal CSR: n log-uniform in
+ * [nmin, nmax], average degree avg_degree, graph i seeded with seed+1000+i;
+ * offsets[count+1] receives each graph's first vertex. */
+GBO_API int gbo_gen_er_batch(int count, int nmin, int nmax, double avg_degree,
+                     uint64_t seed, gbo_csr** out, int* offsets);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,67 @@
+"""Batched traversals vs the oracle: multi-source BFS (bit frontier matrix)
+and the multi-seed BFS over a block-diagonal batch of small graphs."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_levels(orc, csr, srcs):
+    return np.stack([orc.bfs_csr(csr.rowptr, csr.colind, csr.nrows, int(s))[0] for s in srcs], axis=1)
+
+
+@pytest.mark.parametrize("k", [1, 5, 32, 64, 100, 256, 1024])
+def test_msbfs_matches_per_source_bfs(gbo, orc, gpu, k):
+    rng = np.random.default_rng(k)
+    for csr in (gbo.gen_rmat(12, 16, seed=0), gbo.gen_er(1000, 0.02002, 0), gbo.gen_king_mesh(33)):
+        g = gbo.Graph.from_csr(csr, 32)
+        srcs = rng.integers(0, csr.nrows, k).astype(np.int32)
+        lv, depth = g.msbfs(srcs)
+        want = oracle_levels(orc, csr, srcs)
+        assert np.array_equal(lv, want), (csr.nrows, k)
+        assert depth == int(want.max()) + 1
+
+
+def test_msbfs_split_rows_and_duplicates(gbo, orc, gpu):
+    # a hub vertex makes block row 0 long enough to be split across warps
+    n = 20000
+    src = np.zeros(n - 1, np.int32)
+    dst = np.arange(1, n, dtype=np.int32)
+    rng = np.random.default_rng(1)
+    src = np.concatenate([src, rng.integers(0, n, 30000)]).astype(np.int32)
+    dst = np.concatenate([dst, rng.integers(0, n, 30000)]).astype(np.int32)
+    csr = gbo.csr_from_edges(src, dst, n, True, True)
+    g = gbo.Graph.from_csr(csr, 32)
+    assert g.info().nsplit_rows > 0
+    srcs = np.array([5, 5, 0, 19999, 123] * 13, np.int32)  # duplicates allowed
+    lv, _ = g.msbfs(srcs)
+    assert np.array_equal(lv, oracle_levels(orc, csr, srcs))
+
+
+def test_msbfs_rejects_other_tiles(gbo, gpu):
+    g = gbo.Graph.from_csr(gbo.gen_er(200, 0.05, 1), 16)
+    with pytest.raises(gbo.GboError) as e:
+        g.msbfs([0, 1])
+    assert e.value.status == gbo.GBO_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("b", [4, 8, 32])
+def test_batch_of_small_graphs_one_traversal(gbo, orc, gpu, b):
+    csr, off = gbo.gen_er_batch(300, 32, 4096, 8.0, seed=7)
+    seeds = off[:-1].copy()  # vertex 0 of every graph
+    g = gbo.Graph.from_csr(csr, b)
+    lv, _ = g.bfs_multi(seeds)
+    for i in range(0, 300, 7):
+        a, e = off[i], off[i + 1]
+        sub_rp = csr.rowptr[a:e + 1] - csr.rowptr[a]
+        sub_ci = csr.colind[csr.rowptr[a]:csr.rowptr[e]] - a
+        want, _ = orc.bfs_csr(sub_rp, sub_ci, e - a, 0)
+        assert np.array_equal(lv[a:e], want), i
+    # whole batch against a multi-seed CPU BFS: per-graph levels never mix
+    ref = np.full(csr.nrows, -1, np.int64)
+    for i in range(300):
+        a, e = off[i], off[i + 1]
+        sub_rp = csr.rowptr[a:e + 1] - csr.rowptr[a]
+        sub_ci = csr.colind[csr.rowptr[a]:csr.rowptr[e]] - a
+        ref[a:e] = orc.bfs_csr(sub_rp, sub_ci, e - a, 0)[0]
+    assert np.array_equal(lv, ref)

@@ -124,16 +124,19 @@ def test_reference_minplus_and_float_on_our_packing(gbo, refbmv, graphs):
         rows = np.repeat(diag, 32)[:n]
         ours = dy.to_numpy(np.uint32, n)
         assert np.array_equal(ours[rows], dref.to_numpy(np.uint32, n)[rows]), name
-        # fp32 PageRank BMV with the degree read from the CSR row pointer
+        # fp32 PageRank BMV as pr.cu uses it: P = A^T (CSC packing) and the
+        # degree of column j read from A's CSR row pointer
+        gt = gbo.Graph.from_csr(csr, 32, gbo.FLAG_TRANSPOSE)
+        tr, tc, tv = _dev_b2sr(gbo, gt)
         p = rng.random(n).astype(np.float32)
         dp = gbo.DeviceBuffer.from_numpy(_pad(p, npad, np.float32(0)))
         rpp = _pad(csr.rowptr, npad + 1, csr.rowptr[-1])  # reads every column of a tile
         drp = gbo.DeviceBuffer.from_numpy(rpp)
         dref = gbo.DeviceBuffer.zeros(4 * npad)
-        assert ffl(v, dp.ptr, dref.ptr, r, c, inf.nblockrows, drp.ptr, 0.85) == 0
+        assert ffl(tv, dp.ptr, dref.ptr, tr, tc, inf.nblockrows, drp.ptr, 0.85) == 0
         assert refbmv.ref_sync() == 0
         dy = gbo.DeviceBuffer(4 * n)
-        gbo.check(gbo.lib().gbo_bmv_float_degptr(g.h, dp.ptr, dy.ptr, 0.85, drp.ptr, None))
+        gbo.check(gbo.lib().gbo_bmv_float_degptr(gt.h, dp.ptr, dy.ptr, 0.85, drp.ptr, None))
         np.testing.assert_allclose(dy.to_numpy(np.float32, n), dref.to_numpy(np.float32, n),
                                    rtol=2e-5, atol=1e-7, err_msg=name)
 
