@@ -46,7 +46,8 @@ __device__ __forceinline__ void ms_epilogue_row(int i, int w, uint32_t a, const 
                                                 uint32_t* __restrict__ Fn,
                                                 uint32_t* __restrict__ V,
                                                 int* __restrict__ levels, int k, int lvl,
-                                                unsigned long long& cnt, bool& any) {
+                                                unsigned long long& cnt, bool& any,
+                                                uint32_t* __restrict__ slot_any) {
   if (i >= v.nrows) return;
   const size_t o = (size_t)i * KW + w;
   const uint32_t vo = V[o];
@@ -55,6 +56,7 @@ __device__ __forceinline__ void ms_epilogue_row(int i, int w, uint32_t a, const 
   if (nw) {
     V[o] = vo | nw;
     any = true;
+    if (slot_any) atomicOr(slot_any + w, nw);
     cnt += __popc(nw);
     uint32_t m = nw;
     while (m) {
@@ -70,7 +72,8 @@ __global__ void __launch_bounds__(kTPB) k_ms_step(GView v, uint32_t* __restrict_
                                                   size_t fstride, uint32_t* __restrict__ V,
                                                   uint8_t* __restrict__ anyb, int* __restrict__ levels,
                                                   int k, int* __restrict__ ctl,
-                                                  uint32_t* __restrict__ scratch) {
+                                                  uint32_t* __restrict__ scratch,
+                                                  uint32_t* __restrict__ slot_any) {
   constexpr int S = 32 / KW;  // set bits processed at once
   __shared__ uint32_t acc_sh[kWarps][32 * KW];
   volatile int* c = ctl;
@@ -137,7 +140,8 @@ __global__ void __launch_bounds__(kTPB) k_ms_step(GView v, uint32_t* __restrict_
       bool any = false;
       for (int rr = 0; rr < 32; rr += S) {
         const int r = rr + s;
-        ms_epilogue_row<KW>(it.row * 32 + r, w, acc[r * KW + w], v, Fn, V, levels, k, lvl, cnt, any);
+        ms_epilogue_row<KW>(it.row * 32 + r, w, acc[r * KW + w], v, Fn, V, levels, k, lvl, cnt, any,
+                            slot_any);
       }
       const bool a = __any_sync(0xffffffffu, any);
       if (lane == 0) fany_n[it.row] = a ? 1 : 0;
@@ -161,7 +165,8 @@ __global__ void __launch_bounds__(kTPB) k_ms_finish(GView v, uint32_t* __restric
                                                     uint8_t* __restrict__ anyb,
                                                     int* __restrict__ levels, int k,
                                                     int* __restrict__ ctl,
-                                                    const uint32_t* __restrict__ scratch) {
+                                                    const uint32_t* __restrict__ scratch,
+                                                    uint32_t* __restrict__ slot_any) {
   constexpr int S = 32 / KW;
   volatile int* c = ctl;
   if (c[1]) return;
@@ -180,7 +185,7 @@ __global__ void __launch_bounds__(kTPB) k_ms_finish(GView v, uint32_t* __restric
       const int r = rr + s;
       uint32_t a = 0;
       for (int q = 0; q < sp.nslots; ++q) a |= scratch[(size_t)(sp.slot0 + q) * 32 * KW + r * KW + w];
-      ms_epilogue_row<KW>(sp.row * 32 + r, w, a, v, Fn, V, levels, k, lvl, cnt, any);
+      ms_epilogue_row<KW>(sp.row * 32 + r, w, a, v, Fn, V, levels, k, lvl, cnt, any, slot_any);
     }
     const bool a = __any_sync(0xffffffffu, any);
     if (lane == 0) fany_n[sp.row] = a ? 1 : 0;
@@ -306,9 +311,11 @@ int ms_capture(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
   for (int q = 0; q < 8; ++q) {
     cudaEventRecordWithFlags(m.ev[2 * q], m.cap, cudaEventRecordExternal);
     if (g->nitems > 0)
-      k_ms_step<KW><<<gi, kTPB, 0, m.cap>>>(v, m.F, fstride, m.V, m.anyb, d_levels, k, m.ctl, m.scratch);
+      k_ms_step<KW><<<gi, kTPB, 0, m.cap>>>(v, m.F, fstride, m.V, m.anyb, d_levels, k, m.ctl, m.scratch,
+                                            nullptr);
     cudaEventRecordWithFlags(m.ev[2 * q + 1], m.cap, cudaEventRecordExternal);
-    k_ms_finish<KW><<<gs, kTPB, 0, m.cap>>>(v, m.F, fstride, m.V, m.anyb, d_levels, k, m.ctl, m.scratch);
+    k_ms_finish<KW><<<gs, kTPB, 0, m.cap>>>(v, m.F, fstride, m.V, m.anyb, d_levels, k, m.ctl, m.scratch,
+                                              nullptr);
   }
   cudaError_t e = cudaStreamEndCapture(m.cap, &graph);
   if (e != cudaSuccess) return fail_cuda(e, "msbfs capture");
