@@ -1,0 +1,292 @@
+// Device code of the multi-source (bit frontier matrix) BFS, shared by the
+// batched API (msbfs.cu) and the query server (server.cu).
+//
+// State for k sources, KW = k/32 words per vertex (vertex-major):
+//   F[2][n*KW]  frontier rows (double-buffered by level parity); a row is
+//               valid only where its frontier bit (fbits) is set
+//   V[n*KW]     visited rows
+//   fbits[2][nbr+1]  per-vertex "frontier row non-empty" bits, b=32 word per
+//               block row, row r at bit 31-r (the B2SR vector layout)
+//   vfull[nbr]  per-vertex "all k sources visited" bits (padding rows set)
+//   levels[n*k] hops per (vertex, source), -1 unreachable
+// A level is the OR.AND product of the B2SR matrix with the frontier matrix.
+// One warp per work item; only tiles whose block column has frontier rows,
+// only set bits whose frontier row is non-empty, and only tile rows that are
+// not fully visited are touched.  The epilogue writes new frontier rows,
+// visited rows, levels and both bit vectors.
+#pragma once
+
+#include "scan.cuh"
+
+namespace gbo {
+namespace ms {
+
+constexpr int kTPB = 256;
+constexpr int kWarps = kTPB / 32;
+
+struct Args {
+  GView v;
+  uint32_t* F;
+  size_t fstride;
+  uint32_t* V;
+  uint32_t* fbits;  // 2 * (nbr + 1)
+  uint32_t* vfull;  // nbr + 1
+  int* levels;
+  int k;
+  int* ctl;  // iter, done, ticket, max_iter, count (u64 at ctl + 4)
+  uint32_t* scratch;
+  uint32_t* slot_any;  // optional: OR of the new bits of every source word
+};
+
+__device__ __forceinline__ unsigned nth_set_bit(unsigned m, int nth) {
+  return __fns(m, 0, nth);  // position of the nth (1-based) set bit from bit 0
+}
+
+// Bits of word w that are real sources (k need not be a multiple of 32).
+__device__ __forceinline__ unsigned src_mask(int w, int k) {
+  const int lo = w * 32;
+  if (k >= lo + 32) return 0xffffffffu;
+  if (k <= lo) return 0u;
+  return (1u << (k - lo)) - 1u;
+}
+
+// Epilogue of one block row R: acc(r, w) is the OR of the frontier rows of
+// row r's neighbours (word w), read through `get`.  Lane = (slot s, word w).
+template <int KW, typename Get>
+__device__ __forceinline__ void block_row_epilogue(const Args& a, int R, int lvl, uint32_t vrow,
+                                                   unsigned lane, Get get,
+                                                   unsigned long long& cnt) {
+  constexpr int S = 32 / KW;
+  const int w = lane % KW;
+  const int s = lane / KW;
+  const unsigned wmask = seg_mask<KW>();
+  uint32_t* Fn = a.F + (size_t)((lvl + 1) & 1) * a.fstride;
+  uint32_t fword = 0, vword = vrow;
+  for (int rr = 0; rr < 32; rr += S) {
+    const int r = rr + s;
+    const int i = R * 32 + r;
+    const bool open = !((vrow >> (31 - r)) & 1u);  // padding rows are marked full
+    uint32_t nw = 0, vn = 0;
+    size_t o = 0;
+    if (open) {
+      o = (size_t)i * KW + w;
+      const uint32_t vo = a.V[o];
+      nw = get(r, w) & ~vo & src_mask(w, a.k);
+      vn = vo | nw;
+    }
+    const unsigned bnew = __ballot_sync(0xffffffffu, nw != 0);
+    const unsigned bfull = __ballot_sync(0xffffffffu, !open || vn == src_mask(w, a.k));
+    const bool rowany = ((bnew >> (s * KW)) & wmask) != 0;
+    if (open && rowany) Fn[o] = nw;  // only rows marked in fbits are ever read
+    if (nw) {
+      a.V[o] = vn;
+      cnt += __popc(nw);
+      if (a.slot_any) atomicOr(a.slot_any + w, nw);
+      uint32_t m = nw;
+      while (m) {
+        const int p = __ffs(m) - 1;
+        m &= m - 1;
+        a.levels[(size_t)i * a.k + w * 32 + p] = lvl + 1;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < S; ++q) {
+      const unsigned rowbit = 1u << (31 - (rr + q));
+      if ((bnew >> (q * KW)) & wmask) fword |= rowbit;
+      if (((bfull >> (q * KW)) & wmask) == wmask) vword |= rowbit;
+    }
+  }
+  if (lane == 0) {
+    a.fbits[(size_t)((lvl + 1) & 1) * (a.v.nbr + 1) + R] = fword;
+    a.vfull[R] = vword;
+  }
+}
+
+template <int KW>
+__global__ void __launch_bounds__(kTPB) k_step(Args a) {
+  constexpr int S = 32 / KW;
+  __shared__ uint32_t acc_sh[kWarps][32 * KW];
+  volatile int* c = a.ctl;
+  if (c[1]) return;  // done
+  const int lvl = c[0];
+  const GView& v = a.v;
+  const uint32_t* __restrict__ F = a.F + (size_t)(lvl & 1) * a.fstride;
+  const uint32_t* __restrict__ fb = a.fbits + (size_t)(lvl & 1) * (v.nbr + 1);
+  const unsigned lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const long long item = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  uint32_t* acc = acc_sh[wib];
+  const int w = lane % KW;
+  const int s = lane / KW;
+  unsigned long long cnt = 0;
+  if (item < v.nitems) {
+    const gbo_item it = v.items[item];
+    const uint32_t vrow = a.vfull[it.row];
+    if (vrow != 0xffffffffu) {
+      for (int q = lane; q < 32 * KW; q += 32) acc[q] = 0u;
+      __syncwarp();
+      const unsigned need_rows = ~__brev(vrow);  // lane-bit r = row r still open
+      const uint32_t* __restrict__ val = reinterpret_cast<const uint32_t*>(v.val);
+      for (int b0 = it.t0; b0 < it.t1; b0 += 32) {
+        const int t = b0 + (int)lane;
+        int cb = 0;
+        uint32_t fw = 0;
+        if (t < it.t1) {
+          cb = v.colind[t];
+          fw = fb[cb];
+        }
+        unsigned tiles = __ballot_sync(0xffffffffu, fw != 0);
+        while (tiles) {
+          const int jt = __ffs(tiles) - 1;
+          tiles &= tiles - 1;
+          const int C = __shfl_sync(0xffffffffu, cb, jt);
+          const uint32_t fcol = __shfl_sync(0xffffffffu, fw, jt);
+          const uint32_t eff = val[(size_t)(b0 + jt) * 32 + lane] & fcol;  // lane r: row r
+          unsigned rows = __ballot_sync(0xffffffffu, eff != 0) & need_rows;
+          while (rows) {
+            const int r = __ffs(rows) - 1;
+            rows &= rows - 1;
+            unsigned bits = __shfl_sync(0xffffffffu, eff, r);
+            uint32_t racc = 0;
+            while (bits) {
+              const unsigned pos = nth_set_bit(bits, s + 1);
+              uint32_t f = 0;
+              if (pos != 0xffffffffu) f = F[((size_t)C * 32 + (31 - (int)pos)) * KW + w];
+#pragma unroll
+              for (int o = KW; o < 32; o <<= 1) f |= __shfl_xor_sync(0xffffffffu, f, o);
+              racc |= f;
+              const unsigned last = nth_set_bit(bits, S);
+              bits = last == 0xffffffffu ? 0u : (bits & ~(0xffffffffu >> (31 - last)));
+            }
+            if (s == 0) acc[r * KW + w] |= racc;
+          }
+        }
+      }
+      __syncwarp();
+      if (it.slot >= 0) {
+        uint32_t* dst = a.scratch + (size_t)it.slot * 32 * KW;
+        for (int q = lane; q < 32 * KW; q += 32) dst[q] = acc[q];
+      } else {
+        block_row_epilogue<KW>(a, it.row, lvl, vrow, lane,
+                               [&](int r, int ww) { return acc[r * KW + ww]; }, cnt);
+      }
+    } else if (it.slot < 0 && lane == 0) {
+      a.fbits[(size_t)((lvl + 1) & 1) * (v.nbr + 1) + it.row] = 0u;
+    } else if (it.slot >= 0) {
+      uint32_t* dst = a.scratch + (size_t)it.slot * 32 * KW;
+      for (int q = lane; q < 32 * KW; q += 32) dst[q] = 0u;
+    }
+  }
+  __shared__ unsigned long long sh;
+  if (threadIdx.x == 0) sh = 0;
+  __syncthreads();
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  if (lane == 0 && cnt) atomicAdd(&sh, cnt);
+  __syncthreads();
+  if (threadIdx.x == 0 && sh) atomicAdd(reinterpret_cast<unsigned long long*>(a.ctl + 4), sh);
+}
+
+// Split block rows (one warp each): OR the slot accumulators and run the
+// epilogue.  The last block closes the level (arrival ticket, no waiting).
+template <int KW>
+__global__ void __launch_bounds__(kTPB) k_finish(Args a) {
+  volatile int* c = a.ctl;
+  if (c[1]) return;
+  const int lvl = c[0];
+  const GView& v = a.v;
+  const unsigned lane = threadIdx.x & 31;
+  const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  unsigned long long cnt = 0;
+  if (wid < v.nsplit) {
+    const gbo_split sp = v.splits[wid];
+    const uint32_t vrow = a.vfull[sp.row];
+    if (vrow != 0xffffffffu) {
+      const uint32_t* sc = a.scratch;
+      block_row_epilogue<KW>(
+          a, sp.row, lvl, vrow, lane,
+          [&](int r, int ww) {
+            uint32_t x = 0;
+            for (int q = 0; q < sp.nslots; ++q) x |= sc[(size_t)(sp.slot0 + q) * 32 * KW + r * KW + ww];
+            return x;
+          },
+          cnt);
+    } else if (lane == 0) {
+      a.fbits[(size_t)((lvl + 1) & 1) * (v.nbr + 1) + sp.row] = 0u;
+    }
+  }
+  __shared__ unsigned long long sh;
+  __shared__ bool last;
+  if (threadIdx.x == 0) sh = 0;
+  __syncthreads();
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  if (lane == 0 && cnt) atomicAdd(&sh, cnt);
+  __syncthreads();
+  unsigned long long* count = reinterpret_cast<unsigned long long*>(a.ctl + 4);
+  if (threadIdx.x == 0) {
+    if (sh) atomicAdd(count, sh);
+    __threadfence();
+    last = atomicAdd(reinterpret_cast<unsigned*>(a.ctl + 2), 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    volatile unsigned long long* vc = count;
+    const int it = c[0] + 1;
+    const bool stop = *vc == 0ull || it >= c[3];
+    c[0] = it;
+    *vc = 0ull;
+    a.ctl[2] = 0;
+    if (stop) c[1] = 1;
+    __threadfence();
+  }
+}
+
+// Reset: levels -1, V 0, F[0] 0, frontier bits 0, padding rows marked full.
+static __global__ void k_init(Args a, int kw, int max_iter) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const int n = a.v.nrows, nbr = a.v.nbr;
+  for (long long q = i; q < (long long)n * a.k; q += stride) a.levels[q] = -1;
+  for (long long q = i; q < (long long)n * kw; q += stride) {
+    a.F[q] = 0u;
+    a.V[q] = 0u;
+  }
+  for (long long q = i; q < 2LL * (nbr + 1); q += stride) a.fbits[q] = 0u;
+  for (long long q = i; q <= nbr; q += stride) {
+    const long long lo = q * 32;
+    uint32_t pad = 0;
+    for (int r = 0; r < 32; ++r)
+      if (lo + r >= n) pad |= 1u << (31 - r);
+    a.vfull[q] = pad;
+  }
+  if (i == 0) {
+    a.ctl[0] = 0;
+    a.ctl[1] = 0;
+    a.ctl[2] = 0;
+    a.ctl[3] = max_iter;
+    reinterpret_cast<unsigned long long*>(a.ctl + 4)[0] = 0ull;
+  }
+}
+
+// Sources of the level-0 frontier (one thread: sources may share words).
+static __global__ void k_seed(Args a, const int* __restrict__ srcs, const int* __restrict__ slots,
+                              int nsrc, int kw, int lvl) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  uint32_t* F = a.F + (size_t)(lvl & 1) * a.fstride;
+  uint32_t* fb = a.fbits + (size_t)(lvl & 1) * (a.v.nbr + 1);
+  for (int q = 0; q < nsrc; ++q) {
+    const int v0 = srcs[q];
+    const int s = slots ? slots[q] : q;
+    if (v0 < 0 || v0 >= a.v.nrows) continue;
+    if (!((fb[v0 / 32] >> (31 - v0 % 32)) & 1u))  // first time this row enters: clear it
+      for (int w = 0; w < kw; ++w) F[(size_t)v0 * kw + w] = 0u;
+    F[(size_t)v0 * kw + s / 32] |= 1u << (s % 32);
+    a.V[(size_t)v0 * kw + s / 32] |= 1u << (s % 32);
+    a.levels[(size_t)v0 * a.k + s] = lvl;
+    fb[v0 / 32] |= 1u << (31 - v0 % 32);
+    a.vfull[v0 / 32] &= ~(1u << (31 - v0 % 32));
+  }
+}
+
+}  // namespace ms
+}  // namespace gbo

@@ -1,0 +1,743 @@
+// Query server with continuous batching over a resident graph.
+//
+// BFS queries occupy columns ("slots") of the multi-source BFS state (bit
+// frontier matrix, ms_kernels.cuh); PPR queries occupy columns of a 32-wide
+// fp32 value matrix.  One worker thread drives the GPU in rounds: it admits
+// waiting queries into free slots (a BFS query joins at the next level
+// boundary, a PPR query at the next iteration boundary), runs one BFS level
+// and/or one PPR iteration for every occupied slot, retires the slots that
+// finished (BFS: no new vertex this level; PPR: L1 change <= tol or the
+// iteration cap), copies their results into pinned host buffers and frees the
+// slots for the next queries.  A query's result does not depend on the other
+// queries in flight: every column is computed independently and in the same
+// order (BFS bit-exact; PPR identical arithmetic per column).
+#include <string.h>
+
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "ms_kernels.cuh"
+
+namespace gbo {
+namespace {
+
+constexpr int kPprSlots = 32;
+constexpr int kPprTPB = 128;
+constexpr int kPprWarps = kPprTPB / 32;
+
+double now_ms() {
+  using namespace std::chrono;
+  return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+// ------------------------------------------------------------ PPR kernels
+struct PprArgs {
+  GView v;
+  const float* inv;
+  float* X;       // 2 * n * 32, vertex-major
+  size_t xstride;
+  const float* P;  // (1 - alpha) * personalization, n * 32
+  float alpha;
+  int parity;      // X half holding the current iterate
+  double* err;     // 32 slot L1 changes
+  double* scratch; // split slots: 32 rows x 32 slots doubles each
+};
+
+// One iteration for all 32 slots: X'[i][s] = alpha * sum_{j: P[i][j]} X[j][s]
+// inv[j] + P[i][s]; lane = slot; fp64 accumulators in shared memory.
+__global__ void __launch_bounds__(kPprTPB) k_ppr_step(PprArgs a) {
+  __shared__ double acc_sh[kPprWarps][32 * kPprSlots];
+  const GView& v = a.v;
+  const unsigned lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const long long item = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  double* acc = acc_sh[wib];
+  const float* __restrict__ X = a.X + (size_t)a.parity * a.xstride;
+  float* __restrict__ Xn = a.X + (size_t)(a.parity ^ 1) * a.xstride;
+  double e = 0.0;
+  if (item < v.nitems) {
+    for (int q = lane; q < 32 * kPprSlots; q += 32) acc[q] = 0.0;
+    __syncwarp();
+    const gbo_item it = v.items[item];
+    const uint32_t* __restrict__ val = reinterpret_cast<const uint32_t*>(v.val);
+    for (int b0 = it.t0; b0 < it.t1; b0 += 32) {
+      const int t = b0 + (int)lane;
+      const int cb = t < it.t1 ? v.colind[t] : 0;
+      const int ntile = min(32, it.t1 - b0);
+      for (int jt = 0; jt < ntile; ++jt) {
+        const int C = __shfl_sync(0xffffffffu, cb, jt);
+        const uint32_t wr = val[(size_t)(b0 + jt) * 32 + lane];
+        unsigned rows = __ballot_sync(0xffffffffu, wr != 0);
+        while (rows) {
+          const int r = __ffs(rows) - 1;
+          rows &= rows - 1;
+          unsigned bits = __shfl_sync(0xffffffffu, wr, r);
+          double sum = 0.0;
+          while (bits) {
+            const int col = __clz(bits);
+            bits &= ~(0x80000000u >> col);
+            const size_t j = (size_t)C * 32 + col;
+            sum += (double)(X[j * kPprSlots + lane] * a.inv[j]);
+          }
+          acc[r * kPprSlots + lane] += sum;
+        }
+      }
+    }
+    __syncwarp();
+    if (it.slot >= 0) {
+      double* dst = a.scratch + (size_t)it.slot * 32 * kPprSlots;
+      for (int q = lane; q < 32 * kPprSlots; q += 32) dst[q] = acc[q];
+    } else {
+      for (int r = 0; r < 32; ++r) {
+        const long long i = (long long)it.row * 32 + r;
+        if (i >= v.nrows) break;
+        const size_t o = (size_t)i * kPprSlots + lane;
+        const float y = (float)((double)a.alpha * acc[r * kPprSlots + lane] + (double)a.P[o]);
+        e += fabs((double)y - (double)X[o]);
+        Xn[o] = y;
+      }
+    }
+  }
+  __shared__ double es[kPprWarps][32];
+  es[wib][lane] = e;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double t = 0.0;
+    for (int q = 0; q < kPprWarps; ++q) t += es[q][threadIdx.x];
+    if (t != 0.0) atomicAdd(a.err + threadIdx.x, t);
+  }
+}
+
+__global__ void __launch_bounds__(kPprTPB) k_ppr_finish(PprArgs a) {
+  const GView& v = a.v;
+  const unsigned lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const float* __restrict__ X = a.X + (size_t)a.parity * a.xstride;
+  float* __restrict__ Xn = a.X + (size_t)(a.parity ^ 1) * a.xstride;
+  double e = 0.0;
+  if (wid < v.nsplit) {
+    const gbo_split sp = v.splits[wid];
+    for (int r = 0; r < 32; ++r) {
+      const long long i = (long long)sp.row * 32 + r;
+      if (i >= v.nrows) break;
+      double s = 0.0;
+      for (int q = 0; q < sp.nslots; ++q) s += a.scratch[((size_t)(sp.slot0 + q) * 32 + r) * kPprSlots + lane];
+      const size_t o = (size_t)i * kPprSlots + lane;
+      const float y = (float)((double)a.alpha * s + (double)a.P[o]);
+      e += fabs((double)y - (double)X[o]);
+      Xn[o] = y;
+    }
+  }
+  __shared__ double es[kPprWarps][32];
+  es[wib][lane] = e;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double t = 0.0;
+    for (int q = 0; q < kPprWarps; ++q) t += es[q][threadIdx.x];
+    if (t != 0.0) atomicAdd(a.err + threadIdx.x, t);
+  }
+}
+
+// Admit PPR queries: column s of P = (1-alpha) v, X (current half) = P.
+__global__ void k_ppr_admit(float* X, size_t xstride, int parity, float* P, int n,
+                            const int* __restrict__ slots, int nslots_adm,
+                            const int* __restrict__ verts, const float* __restrict__ wts,
+                            const int* __restrict__ off, float one_minus_alpha) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  float* Xc = X + (size_t)parity * xstride;
+  // clear the admitted columns
+  for (long long q = i; q < (long long)n * nslots_adm; q += stride) {
+    const int a = (int)(q % nslots_adm);
+    const long long v0 = q / nslots_adm;
+    const size_t o = (size_t)v0 * kPprSlots + slots[a];
+    P[o] = 0.f;
+    Xc[o] = 0.f;
+  }
+}
+
+__global__ void k_ppr_admit_set(float* X, size_t xstride, int parity, float* P, int n,
+                                const int* __restrict__ slots, int nslots_adm,
+                                const int* __restrict__ verts, const float* __restrict__ wts,
+                                const int* __restrict__ off, float one_minus_alpha) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  float* Xc = X + (size_t)parity * xstride;
+  for (int a = 0; a < nslots_adm; ++a)
+    for (int q = off[a]; q < off[a + 1]; ++q) {
+      const int v0 = verts[q];
+      if (v0 < 0 || v0 >= n) continue;
+      const size_t o = (size_t)v0 * kPprSlots + slots[a];
+      P[o] += one_minus_alpha * wts[q];
+      Xc[o] = P[o];
+    }
+}
+
+// Copy column s of the current iterate out (and leave the column as is; a
+// new admission clears it).
+__global__ void k_ppr_extract(const float* X, size_t xstride, int parity, int n, int s, float* out) {
+  const float* Xc = X + (size_t)parity * xstride;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = Xc[(size_t)i * kPprSlots + s];
+}
+
+// ------------------------------------------------------ BFS slot kernels
+// Result of slot s: levels relative to its start level; then clear the
+// slot's column (levels -1, visited bit 0) for the next query.
+__global__ void k_bfs_extract(int* levels, uint32_t* V, int n, int kb, int kw, int s, int start,
+                              int* out) {
+  const uint32_t bit = 1u << (s % 32);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const size_t o = (size_t)i * kb + s;
+    const int lv = levels[o];
+    out[i] = lv >= 0 ? lv - start : -1;
+    levels[o] = -1;
+    V[(size_t)i * kw + s / 32] &= ~bit;
+  }
+}
+
+// After a visited column was cleared no row is "all sources visited" any
+// more: keep only the padding rows marked.
+__global__ void k_vfull_reset(uint32_t* vfull, int nbr, int n) {
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q <= nbr;
+       q += (long long)gridDim.x * blockDim.x) {
+    const long long lo = q * 32;
+    uint32_t pad = 0;
+    for (int r = 0; r < 32; ++r)
+      if (lo + r >= n) pad |= 1u << (31 - r);
+    vfull[q] = pad;
+  }
+}
+
+struct Query {
+  long long ticket;
+  int kind;  // 0 BFS, 1 PPR
+  int src;
+  std::vector<int> verts;
+  std::vector<float> wts;
+  double t_submit;
+};
+
+struct Result {
+  int kind;
+  std::vector<char> data;  // n int32 (BFS) or n float32 (PPR)
+  double t_submit, t_done;
+  int iters;
+};
+
+}  // namespace
+}  // namespace gbo
+
+struct gbo_server {
+  gbo_graph* g = nullptr;
+  int n = 0, nbr = 0;
+  float alpha = 0.85f, tol = 1e-7f;
+  int ppr_max_iter = 1000;
+  cudaStream_t s = nullptr;
+  int dev = 0;
+  // BFS engine
+  int kb = 0, kw = 0;
+  uint32_t *F = nullptr, *V = nullptr, *fbits = nullptr, *vfull = nullptr, *scratch = nullptr;
+  int* levels = nullptr;
+  int* ctl = nullptr;
+  int* h_ctl = nullptr;
+  uint32_t* slot_any = nullptr;
+  uint32_t* h_slot_any = nullptr;
+  int *d_adm_src = nullptr, *d_adm_slot = nullptr;
+  int level = 0;
+  std::vector<long long> bslot_ticket;
+  std::vector<int> bslot_start;
+  // PPR engine
+  float *X = nullptr, *P = nullptr;
+  double* err = nullptr;
+  double* h_err = nullptr;
+  double* pscratch = nullptr;
+  int *d_pslots = nullptr, *d_pverts = nullptr, *d_poff = nullptr;
+  float* d_pwts = nullptr;
+  int parity = 0;
+  std::vector<long long> pslot_ticket;
+  std::vector<int> pslot_iters;
+  std::vector<double> pslot_submit;
+  // extraction
+  void* d_out = nullptr;
+  void* h_stage = nullptr;
+  // host side
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<gbo::Query> pending;
+  std::map<long long, gbo::Result> results;
+  std::map<long long, double> submit_time;
+  long long next_ticket = 1;
+  bool stop = false;
+  int worker_status = GBO_OK;
+  std::string worker_error;
+  std::thread worker;
+  // statistics
+  long long rounds = 0, bfs_done = 0, ppr_done = 0, launches = 0;
+};
+
+namespace gbo {
+namespace {
+
+template <int KW>
+int bfs_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm, std::vector<int>& finished) {
+  ms::Args a;
+  a.v = view_of(S->g);
+  a.F = S->F;
+  a.fstride = (size_t)S->n * S->kw;
+  a.V = S->V;
+  a.fbits = S->fbits;
+  a.vfull = S->vfull;
+  a.levels = S->levels;
+  a.k = S->kb;
+  a.ctl = S->ctl;
+  a.scratch = S->scratch;
+  a.slot_any = S->slot_any;
+  cudaStream_t st = S->s;
+  if (!adm.empty()) {
+    std::vector<int> src, slot;
+    for (auto& q : adm) {
+      slot.push_back(q.first);
+      src.push_back(q.second.src);
+    }
+    GBO_CUDA_TRY(cudaMemcpyAsync(S->d_adm_src, src.data(), sizeof(int) * src.size(), cudaMemcpyHostToDevice, st));
+    GBO_CUDA_TRY(cudaMemcpyAsync(S->d_adm_slot, slot.data(), sizeof(int) * slot.size(), cudaMemcpyHostToDevice, st));
+    ms::k_seed<<<1, 32, 0, st>>>(a, S->d_adm_src, S->d_adm_slot, (int)src.size(), S->kw, S->level);
+    S->launches++;
+  }
+  // one level: iter = current level, not done, count 0
+  int h[4] = {S->level, 0, 0, 0x7fffffff};
+  GBO_CUDA_TRY(cudaMemcpyAsync(S->ctl, h, sizeof(h), cudaMemcpyHostToDevice, st));
+  GBO_CUDA_TRY(cudaMemsetAsync(S->ctl + 4, 0, 8, st));
+  GBO_CUDA_TRY(cudaMemsetAsync(S->slot_any, 0, sizeof(uint32_t) * S->kw, st));
+  const unsigned gi = blocks_for_warps(S->g->nitems, ms::kWarps);
+  const unsigned gs = blocks_for_warps(S->g->nsplit > 0 ? S->g->nsplit : 1, ms::kWarps);
+  if (S->g->nitems > 0) ms::k_step<KW><<<gi, ms::kTPB, 0, st>>>(a);
+  ms::k_finish<KW><<<gs, ms::kTPB, 0, st>>>(a);
+  S->launches += 2;
+  GBO_CUDA_TRY(cudaGetLastError());
+  GBO_CUDA_TRY(cudaMemcpyAsync(S->h_slot_any, S->slot_any, sizeof(uint32_t) * S->kw, cudaMemcpyDeviceToHost, st));
+  GBO_CUDA_TRY(cudaStreamSynchronize(st));
+  S->level += 1;
+  for (int q = 0; q < S->kb; ++q)
+    if (S->bslot_ticket[q] > 0 && !((S->h_slot_any[q / 32] >> (q % 32)) & 1u)) finished.push_back(q);
+  return GBO_OK;
+}
+
+int ppr_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm, std::vector<int>& finished) {
+  cudaStream_t st = S->s;
+  const size_t xstride = (size_t)S->n * kPprSlots;
+  if (!adm.empty()) {
+    std::vector<int> slots, verts, off(1, 0);
+    std::vector<float> wts;
+    for (auto& q : adm) {
+      slots.push_back(q.first);
+      for (size_t k = 0; k < q.second.verts.size(); ++k) {
+        verts.push_back(q.second.verts[k]);
+        wts.push_back(q.second.wts[k]);
+      }
+      off.push_back((int)verts.size());
+    }
+    GBO_CUDA_TRY(cudaMemcpyAsync(S->d_pslots, slots.data(), sizeof(int) * slots.size(), cudaMemcpyHostToDevice, st));
+    GBO_CUDA_TRY(cudaMemcpyAsync(S->d_pverts, verts.data(), sizeof(int) * verts.size(), cudaMemcpyHostToDevice, st));
+    GBO_CUDA_TRY(cudaMemcpyAsync(S->d_pwts, wts.data(), sizeof(float) * wts.size(), cudaMemcpyHostToDevice, st));
+    GBO_CUDA_TRY(cudaMemcpyAsync(S->d_poff, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, st));
+    unsigned gv = blocks_for((long long)S->n * (long long)slots.size(), 256);
+    if (gv > 4096u) gv = 4096u;
+    k_ppr_admit<<<gv, 256, 0, st>>>(S->X, xstride, S->parity, S->P, S->n, S->d_pslots, (int)slots.size(),
+                                    S->d_pverts, S->d_pwts, S->d_poff, 1.f - S->alpha);
+    k_ppr_admit_set<<<1, 32, 0, st>>>(S->X, xstride, S->parity, S->P, S->n, S->d_pslots,
+                                      (int)slots.size(), S->d_pverts, S->d_pwts, S->d_poff,
+                                      1.f - S->alpha);
+    S->launches += 2;
+  }
+  PprArgs a;
+  a.v = view_of(S->g);
+  a.inv = S->g->invdeg;
+  a.X = S->X;
+  a.xstride = xstride;
+  a.P = S->P;
+  a.alpha = S->alpha;
+  a.parity = S->parity;
+  a.err = S->err;
+  a.scratch = S->pscratch;
+  GBO_CUDA_TRY(cudaMemsetAsync(S->err, 0, sizeof(double) * kPprSlots, st));
+  const unsigned gi = blocks_for_warps(S->g->nitems, kPprWarps);
+  if (S->g->nitems > 0) k_ppr_step<<<gi, kPprTPB, 0, st>>>(a);
+  if (S->g->nsplit > 0) k_ppr_finish<<<blocks_for_warps(S->g->nsplit, kPprWarps), kPprTPB, 0, st>>>(a);
+  S->launches += 2;
+  GBO_CUDA_TRY(cudaGetLastError());
+  GBO_CUDA_TRY(cudaMemcpyAsync(S->h_err, S->err, sizeof(double) * kPprSlots, cudaMemcpyDeviceToHost, st));
+  GBO_CUDA_TRY(cudaStreamSynchronize(st));
+  S->parity ^= 1;
+  for (int q = 0; q < kPprSlots; ++q) {
+    if (S->pslot_ticket[q] <= 0) continue;
+    S->pslot_iters[q] += 1;
+    if ((S->tol >= 0 && S->h_err[q] <= (double)S->tol) || S->pslot_iters[q] >= S->ppr_max_iter)
+      finished.push_back(q);
+  }
+  return GBO_OK;
+}
+
+void worker_main(gbo_server* S) {
+  cudaSetDevice(S->dev);
+  auto failw = [&](int st) {
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->worker_status = st;
+    S->worker_error = gbo_last_error();
+    S->cv_done.notify_all();
+  };
+  const size_t rbytes = sizeof(int) * (size_t)S->n;
+  while (true) {
+    std::vector<std::pair<int, Query>> badm, padm;
+    {
+      std::unique_lock<std::mutex> lk(S->mu);
+      auto busy = [&] {
+        for (long long t : S->bslot_ticket)
+          if (t > 0) return true;
+        for (long long t : S->pslot_ticket)
+          if (t > 0) return true;
+        return false;
+      };
+      S->cv_work.wait(lk, [&] { return S->stop || !S->pending.empty() || busy(); });
+      if (S->stop) return;
+      // admission into free slots, arrival order, per engine
+      std::deque<Query> keep;
+      while (!S->pending.empty()) {
+        Query q = std::move(S->pending.front());
+        S->pending.pop_front();
+        std::vector<long long>& tab = q.kind == 0 ? S->bslot_ticket : S->pslot_ticket;
+        int slot = -1;
+        for (size_t z = 0; z < tab.size(); ++z)
+          if (tab[z] == 0) {
+            bool taken = false;
+            for (auto& p : (q.kind == 0 ? badm : padm))
+              if (p.first == (int)z) taken = true;
+            if (!taken) {
+              slot = (int)z;
+              break;
+            }
+          }
+        if (slot < 0) {
+          keep.push_back(std::move(q));
+          continue;
+        }
+        tab[(size_t)slot] = q.ticket;
+        if (q.kind == 0) {
+          S->bslot_start[(size_t)slot] = S->level;
+          badm.emplace_back(slot, std::move(q));
+        } else {
+          S->pslot_iters[(size_t)slot] = 0;
+          S->pslot_submit[(size_t)slot] = q.t_submit;
+          padm.emplace_back(slot, std::move(q));
+        }
+      }
+      S->pending.swap(keep);
+    }
+    bool bfs_busy = !badm.empty(), ppr_busy = !padm.empty();
+    for (long long t : S->bslot_ticket) bfs_busy |= t > 0;
+    for (long long t : S->pslot_ticket) ppr_busy |= t > 0;
+    std::vector<int> bfin, pfin;
+    int st = GBO_OK;
+    if (bfs_busy && S->kb > 0) {
+      switch (S->kw) {
+        case 1: st = bfs_round<1>(S, badm, bfin); break;
+        case 2: st = bfs_round<2>(S, badm, bfin); break;
+        case 4: st = bfs_round<4>(S, badm, bfin); break;
+        case 8: st = bfs_round<8>(S, badm, bfin); break;
+        case 16: st = bfs_round<16>(S, badm, bfin); break;
+        default: st = bfs_round<32>(S, badm, bfin); break;
+      }
+    }
+    if (st == GBO_OK && ppr_busy && S->g->invdeg) st = ppr_round(S, padm, pfin);
+    if (st != GBO_OK) {
+      failw(st);
+      return;
+    }
+    S->rounds++;
+    // retire finished slots: extract, copy to host, free the slot
+    for (int q : bfin) {
+      const unsigned gv = blocks_for(S->n, 256) > 2048u ? 2048u : blocks_for(S->n, 256);
+      k_bfs_extract<<<gv, 256, 0, S->s>>>(S->levels, S->V, S->n, S->kb, S->kw, q,
+                                          S->bslot_start[(size_t)q], (int*)S->d_out);
+      cudaMemcpyAsync(S->h_stage, S->d_out, rbytes, cudaMemcpyDeviceToHost, S->s);
+      if (cudaStreamSynchronize(S->s) != cudaSuccess) {
+        failw(fail(GBO_ERR_CUDA, "server BFS extraction"));
+        return;
+      }
+      S->launches++;
+      Result r;
+      r.kind = 0;
+      r.data.assign((char*)S->h_stage, (char*)S->h_stage + rbytes);
+      r.t_done = now_ms();
+      r.iters = S->level - S->bslot_start[(size_t)q];
+      std::lock_guard<std::mutex> lk(S->mu);
+      const long long t = S->bslot_ticket[(size_t)q];
+      r.t_submit = S->submit_time[t];
+      S->results[t] = std::move(r);
+      S->bslot_ticket[(size_t)q] = 0;
+      S->bfs_done++;
+    }
+    if (!bfin.empty()) {
+      k_vfull_reset<<<blocks_for(S->nbr + 1, 256), 256, 0, S->s>>>(S->vfull, S->nbr, S->n);
+      S->launches++;
+    }
+    for (int q : pfin) {
+      const unsigned gv = blocks_for(S->n, 256) > 2048u ? 2048u : blocks_for(S->n, 256);
+      k_ppr_extract<<<gv, 256, 0, S->s>>>(S->X, (size_t)S->n * kPprSlots, S->parity, S->n, q,
+                                          (float*)S->d_out);
+      cudaMemcpyAsync(S->h_stage, S->d_out, rbytes, cudaMemcpyDeviceToHost, S->s);
+      if (cudaStreamSynchronize(S->s) != cudaSuccess) {
+        failw(fail(GBO_ERR_CUDA, "server PPR extraction"));
+        return;
+      }
+      S->launches++;
+      Result r;
+      r.kind = 1;
+      r.data.assign((char*)S->h_stage, (char*)S->h_stage + rbytes);
+      r.t_done = now_ms();
+      r.iters = S->pslot_iters[(size_t)q];
+      std::lock_guard<std::mutex> lk(S->mu);
+      const long long t = S->pslot_ticket[(size_t)q];
+      r.t_submit = S->submit_time[t];
+      S->results[t] = std::move(r);
+      S->pslot_ticket[(size_t)q] = 0;
+      S->ppr_done++;
+    }
+    if (!bfin.empty() || !pfin.empty()) {
+      std::lock_guard<std::mutex> lk(S->mu);
+      S->cv_done.notify_all();
+    }
+  }
+}
+
+void destroy_server(gbo_server* S) {
+  if (!S) return;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->stop = true;
+  }
+  S->cv_work.notify_all();
+  if (S->worker.joinable()) S->worker.join();
+  cudaFree(S->F);
+  cudaFree(S->V);
+  cudaFree(S->fbits);
+  cudaFree(S->vfull);
+  cudaFree(S->scratch);
+  cudaFree(S->levels);
+  cudaFree(S->ctl);
+  cudaFreeHost(S->h_ctl);
+  cudaFree(S->slot_any);
+  cudaFreeHost(S->h_slot_any);
+  cudaFree(S->d_adm_src);
+  cudaFree(S->d_adm_slot);
+  cudaFree(S->X);
+  cudaFree(S->P);
+  cudaFree(S->err);
+  cudaFreeHost(S->h_err);
+  cudaFree(S->pscratch);
+  cudaFree(S->d_pslots);
+  cudaFree(S->d_pverts);
+  cudaFree(S->d_poff);
+  cudaFree(S->d_pwts);
+  cudaFree(S->d_out);
+  cudaFreeHost(S->h_stage);
+  if (S->s) cudaStreamDestroy(S->s);
+  delete S;
+}
+
+}  // namespace
+}  // namespace gbo
+
+using namespace gbo;
+
+extern "C" int gbo_server_create(const gbo_graph* gc, int bfs_slots, int ppr_slots, float alpha,
+                                 float tol, int ppr_max_iter, gbo_server** out) {
+  clear_error();
+  if (!gc || !out) return fail(GBO_ERR_INVALID, "NULL argument");
+  *out = nullptr;
+  gbo_graph* g = const_cast<gbo_graph*>(gc);
+  if (g->b != 32 || g->layout != GBO_LAYOUT_ROW || g->nrows != g->ncols)
+    return fail(GBO_ERR_UNSUPPORTED, "the server needs a square ROW-layout graph with 32x32 tiles");
+  if (bfs_slots < 0 || bfs_slots > 1024 || (ppr_slots != 0 && ppr_slots != kPprSlots))
+    return fail(GBO_ERR_INVALID, "bfs_slots in [0,1024]; ppr_slots 0 or 32");
+  if (ppr_slots && !g->invdeg) return fail(GBO_ERR_INVALID, "PPR needs out-degrees");
+  gbo_server* S = new gbo_server();
+  cudaGetDevice(&S->dev);
+  S->g = g;
+  S->n = g->nrows;
+  S->nbr = g->nbr;
+  S->alpha = alpha;
+  S->tol = tol;
+  S->ppr_max_iter = ppr_max_iter > 0 ? ppr_max_iter : 1000;
+  int kw = 1;
+  while (kw * 32 < bfs_slots) kw <<= 1;
+  S->kb = bfs_slots > 0 ? kw * 32 : 0;  // slots rounded up to whole words
+  S->kw = kw;
+  auto cu = [&](cudaError_t e, const char* w) {
+    if (e != cudaSuccess) throw fail_cuda(e, w);
+  };
+  try {
+    cu(cudaStreamCreateWithFlags(&S->s, cudaStreamNonBlocking), "stream");
+    const size_t n = (size_t)S->n;
+    if (S->kb) {
+      cu(cudaMalloc(&S->F, sizeof(uint32_t) * 2 * n * kw + 16), "F");
+      cu(cudaMalloc(&S->V, sizeof(uint32_t) * n * kw + 16), "V");
+      cu(cudaMalloc(&S->fbits, sizeof(uint32_t) * 2 * (size_t)(g->nbr + 1)), "fbits");
+      cu(cudaMalloc(&S->vfull, sizeof(uint32_t) * (size_t)(g->nbr + 1)), "vfull");
+      cu(cudaMalloc(&S->scratch, sizeof(uint32_t) * (size_t)(g->nslots > 0 ? g->nslots : 1) * 32 * kw), "scratch");
+      cu(cudaMalloc(&S->levels, sizeof(int) * n * S->kb + 16), "levels");
+      cu(cudaMalloc(&S->ctl, 64), "ctl");
+      cu(cudaHostAlloc(&S->h_ctl, 64, cudaHostAllocDefault), "h_ctl");
+      cu(cudaMalloc(&S->slot_any, sizeof(uint32_t) * kw), "slot_any");
+      cu(cudaHostAlloc(&S->h_slot_any, sizeof(uint32_t) * kw, cudaHostAllocDefault), "h_slot_any");
+      cu(cudaMalloc(&S->d_adm_src, sizeof(int) * S->kb), "adm");
+      cu(cudaMalloc(&S->d_adm_slot, sizeof(int) * S->kb), "adm");
+      ms::Args a;
+      a.v = view_of(g);
+      a.F = S->F;
+      a.fstride = n * kw;
+      a.V = S->V;
+      a.fbits = S->fbits;
+      a.vfull = S->vfull;
+      a.levels = S->levels;
+      a.k = S->kb;
+      a.ctl = S->ctl;
+      a.scratch = S->scratch;
+      a.slot_any = S->slot_any;
+      unsigned gv = blocks_for((long long)n * S->kb, 256);
+      if (gv > (unsigned)num_sms() * 16u) gv = (unsigned)num_sms() * 16u;
+      ms::k_init<<<gv, 256, 0, S->s>>>(a, kw, 0x7fffffff);
+    }
+    S->bslot_ticket.assign((size_t)S->kb, 0);
+    S->bslot_start.assign((size_t)S->kb, 0);
+    if (ppr_slots) {
+      cu(cudaMalloc(&S->X, sizeof(float) * 2 * n * kPprSlots), "X");
+      cu(cudaMemsetAsync(S->X, 0, sizeof(float) * 2 * n * kPprSlots, S->s), "X");
+      cu(cudaMalloc(&S->P, sizeof(float) * n * kPprSlots), "P");
+      cu(cudaMemsetAsync(S->P, 0, sizeof(float) * n * kPprSlots, S->s), "P");
+      cu(cudaMalloc(&S->err, sizeof(double) * kPprSlots), "err");
+      cu(cudaHostAlloc(&S->h_err, sizeof(double) * kPprSlots, cudaHostAllocDefault), "h_err");
+      cu(cudaMalloc(&S->pscratch, sizeof(double) * (size_t)(g->nslots > 0 ? g->nslots : 1) * 32 * kPprSlots), "pscratch");
+      cu(cudaMalloc(&S->d_pslots, sizeof(int) * kPprSlots), "pslots");
+      cu(cudaMalloc(&S->d_pverts, sizeof(int) * 64 * kPprSlots), "pverts");
+      cu(cudaMalloc(&S->d_pwts, sizeof(float) * 64 * kPprSlots), "pwts");
+      cu(cudaMalloc(&S->d_poff, sizeof(int) * (kPprSlots + 1)), "poff");
+    }
+    S->pslot_ticket.assign(ppr_slots ? (size_t)kPprSlots : 0, 0);
+    S->pslot_iters.assign((size_t)kPprSlots, 0);
+    S->pslot_submit.assign((size_t)kPprSlots, 0.0);
+    cu(cudaMalloc(&S->d_out, sizeof(int) * n + 16), "out");
+    cu(cudaHostAlloc(&S->h_stage, sizeof(int) * n + 16, cudaHostAllocDefault), "stage");
+    cu(cudaStreamSynchronize(S->s), "sync");
+  } catch (int st) {
+    destroy_server(S);
+    return st;
+  }
+  S->worker = std::thread(worker_main, S);
+  *out = S;
+  return GBO_OK;
+}
+
+static int submit(gbo_server* S, Query&& q, int64_t* ticket) {
+  std::lock_guard<std::mutex> lk(S->mu);
+  if (S->worker_status != GBO_OK) return fail(S->worker_status, S->worker_error);
+  q.ticket = S->next_ticket++;
+  q.t_submit = now_ms();
+  S->submit_time[q.ticket] = q.t_submit;
+  *ticket = q.ticket;
+  S->pending.push_back(std::move(q));
+  S->cv_work.notify_one();
+  return GBO_OK;
+}
+
+extern "C" int gbo_server_submit_bfs(gbo_server* S, int src, int64_t* ticket) {
+  clear_error();
+  if (!S || !ticket) return fail(GBO_ERR_INVALID, "NULL argument");
+  if (S->kb == 0) return fail(GBO_ERR_INVALID, "server has no BFS slots");
+  if (src < 0 || src >= S->n) return fail(GBO_ERR_INVALID, "source out of range");
+  Query q;
+  q.kind = 0;
+  q.src = src;
+  return submit(S, std::move(q), ticket);
+}
+
+extern "C" int gbo_server_submit_ppr(gbo_server* S, const int* verts, const float* weights, int count,
+                                     int64_t* ticket) {
+  clear_error();
+  if (!S || !ticket || !verts || !weights) return fail(GBO_ERR_INVALID, "NULL argument");
+  if (S->pslot_ticket.empty()) return fail(GBO_ERR_INVALID, "server has no PPR slots");
+  if (count < 1 || count > 64) return fail(GBO_ERR_INVALID, "a PPR set has 1..64 vertices");
+  for (int k = 0; k < count; ++k)
+    if (verts[k] < 0 || verts[k] >= S->n) return fail(GBO_ERR_INVALID, "vertex out of range");
+  Query q;
+  q.kind = 1;
+  q.src = -1;
+  q.verts.assign(verts, verts + count);
+  q.wts.assign(weights, weights + count);
+  return submit(S, std::move(q), ticket);
+}
+
+extern "C" int gbo_server_poll(gbo_server* S, int64_t ticket, void* h_out, double* latency_ms,
+                               int* iterations) {
+  clear_error();
+  if (!S) return fail(GBO_ERR_INVALID, "NULL server");
+  std::lock_guard<std::mutex> lk(S->mu);
+  if (S->worker_status != GBO_OK) return fail(S->worker_status, S->worker_error);
+  auto it = S->results.find(ticket);
+  if (it == S->results.end()) return GBO_ERR_NOTREADY;
+  if (h_out) memcpy(h_out, it->second.data.data(), it->second.data.size());
+  if (latency_ms) *latency_ms = it->second.t_done - it->second.t_submit;
+  if (iterations) *iterations = it->second.iters;
+  S->results.erase(it);
+  S->submit_time.erase(ticket);
+  return GBO_OK;
+}
+
+extern "C" int gbo_server_wait(gbo_server* S, int64_t ticket, void* h_out, double* latency_ms,
+                               int* iterations, double timeout_s) {
+  clear_error();
+  if (!S) return fail(GBO_ERR_INVALID, "NULL server");
+  std::unique_lock<std::mutex> lk(S->mu);
+  const bool ok = S->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] {
+    return S->worker_status != GBO_OK || S->results.count(ticket) > 0;
+  });
+  if (S->worker_status != GBO_OK) return fail(S->worker_status, S->worker_error);
+  if (!ok) return fail(GBO_ERR_TIMEOUT, "query not finished within the timeout");
+  auto it = S->results.find(ticket);
+  if (h_out) memcpy(h_out, it->second.data.data(), it->second.data.size());
+  if (latency_ms) *latency_ms = it->second.t_done - it->second.t_submit;
+  if (iterations) *iterations = it->second.iters;
+  S->results.erase(it);
+  S->submit_time.erase(ticket);
+  return GBO_OK;
+}
+
+extern "C" int gbo_server_get_stats(gbo_server* S, gbo_server_stats* st) {
+  clear_error();
+  if (!S || !st) return fail(GBO_ERR_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> lk(S->mu);
+  st->rounds = S->rounds;
+  st->bfs_completed = S->bfs_done;
+  st->ppr_completed = S->ppr_done;
+  st->kernel_launches = S->launches;
+  st->pending = (long long)S->pending.size();
+  long long a = 0;
+  for (long long t : S->bslot_ticket) a += t > 0;
+  for (long long t : S->pslot_ticket) a += t > 0;
+  st->in_flight = a;
+  return GBO_OK;
+}
+
+extern "C" int gbo_server_destroy(gbo_server* S) {
+  clear_error();
+  destroy_server(S);
+  return GBO_OK;
+}

@@ -65,6 +65,12 @@ class RunStats(C.Structure):
                 ("step_ms", C.c_float * MAX_STEP_TIMES)]
 
 
+class ServerStats(C.Structure):
+    _fields_ = [("rounds", C.c_longlong), ("bfs_completed", C.c_longlong),
+                ("ppr_completed", C.c_longlong), ("kernel_launches", C.c_longlong),
+                ("pending", C.c_longlong), ("in_flight", C.c_longlong)]
+
+
 class CsrStruct(C.Structure):
     _fields_ = [("nrows", C.c_int), ("ncols", C.c_int), ("nnz", C.c_int64),
                 ("rowptr", C.POINTER(C.c_int)), ("colind", C.POINTER(C.c_int))]
@@ -125,6 +131,13 @@ _SIGS = {
     "gbo_graph_last_run": (_I, [_P, C.POINTER(RunStats)]),
     "gbo_msbfs": (_I, [_P, _P, _I, _P, C.POINTER(_I), _P]),
     "gbo_bfs_multi": (_I, [_P, _P, _I, _P, C.POINTER(_I), _P]),
+    "gbo_server_create": (_I, [_P, _I, _I, C.c_float, C.c_float, _I, C.POINTER(_P)]),
+    "gbo_server_submit_bfs": (_I, [_P, _I, C.POINTER(C.c_int64)]),
+    "gbo_server_submit_ppr": (_I, [_P, _P, _P, _I, C.POINTER(C.c_int64)]),
+    "gbo_server_poll": (_I, [_P, C.c_int64, _P, C.POINTER(C.c_double), C.POINTER(_I)]),
+    "gbo_server_wait": (_I, [_P, C.c_int64, _P, C.POINTER(C.c_double), C.POINTER(_I), C.c_double]),
+    "gbo_server_get_stats": (_I, [_P, C.POINTER(ServerStats)]),
+    "gbo_server_destroy": (_I, [_P]),
     "gbo_read_mtx": (_I, [C.c_char_p, _I, _I, C.POINTER(C.POINTER(CsrStruct))]),
     "gbo_csr_free": (_I, [C.POINTER(CsrStruct)]),
     "gbo_csr_transpose": (_I, [C.POINTER(CsrStruct), C.POINTER(C.POINTER(CsrStruct))]),
@@ -595,3 +608,63 @@ def bits_from_numpy(x01: np.ndarray, tile_bits: int) -> np.ndarray:
     weights = (np.uint64(1) << np.arange(tile_bits - 1, -1, -1, dtype=np.uint64))
     words = (bits * weights).sum(axis=1, dtype=np.uint64)
     return words.astype(WORD_DTYPE[tile_bits])
+
+
+# ------------------------------------------------------------------ server
+class Server:
+    """Continuous-batching BFS / PPR query server over a resident graph."""
+
+    def __init__(self, graph: Graph, bfs_slots=256, ppr_slots=32, alpha=0.85, tol=1e-7,
+                 ppr_max_iter=1000):
+        p = C.c_void_p()
+        check(lib().gbo_server_create(graph.h, bfs_slots, ppr_slots, alpha, tol, ppr_max_iter,
+                                      C.byref(p)), "server_create")
+        self.h = p.value
+        self.graph = graph
+        self.n = graph.info().nrows
+
+    def submit_bfs(self, src: int) -> int:
+        t = C.c_int64(0)
+        check(lib().gbo_server_submit_bfs(self.h, int(src), C.byref(t)), "server_submit_bfs")
+        return t.value
+
+    def submit_ppr(self, verts, weights) -> int:
+        v = np.ascontiguousarray(verts, np.int32)
+        w = np.ascontiguousarray(weights, np.float32)
+        t = C.c_int64(0)
+        check(lib().gbo_server_submit_ppr(self.h, _ptr(v), _ptr(w), len(v), C.byref(t)),
+              "server_submit_ppr")
+        return t.value
+
+    def wait(self, ticket: int, kind: str = "bfs", timeout=600.0):
+        out = np.empty(self.n, np.int32 if kind == "bfs" else np.float32)
+        lat, it = C.c_double(0), C.c_int(0)
+        check(lib().gbo_server_wait(self.h, ticket, _ptr(out), C.byref(lat), C.byref(it), timeout),
+              "server_wait")
+        return out, lat.value, it.value
+
+    def poll(self, ticket: int, kind: str = "bfs"):
+        """(result, latency_ms, iterations) or None while the query runs."""
+        out = np.empty(self.n, np.int32 if kind == "bfs" else np.float32)
+        lat, it = C.c_double(0), C.c_int(0)
+        st = lib().gbo_server_poll(self.h, ticket, _ptr(out), C.byref(lat), C.byref(it))
+        if st == GBO_ERR_NOTREADY:
+            return None
+        check(st, "server_poll")
+        return out, lat.value, it.value
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        check(lib().gbo_server_get_stats(self.h, C.byref(s)), "server_get_stats")
+        return {f: getattr(s, f) for f, _ in ServerStats._fields_}
+
+    def close(self):
+        if self.h:
+            lib().gbo_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -258,6 +258,37 @@ GBO_API int gbo_msbfs(const gbo_graph* g, const int* h_srcs, int k,
 GBO_API int gbo_bfs_multi(const gbo_graph* g, const int* h_seeds, int nseeds,
                   int32_t* d_level, int* h_depth, gbo_stream_t stream);
 
+/* Query server with continuous batching (no reference counterpart).  BFS
+ * queries occupy columns of a multi-source BFS state (bfs_slots <= 1024,
+ * rounded up to a multiple of 32) and join or leave at level boundaries;
+ * PPR queries (1..64 weighted vertices, p = alpha P D^-1 p + (1-alpha) v,
+ * stop at L1 change <= tol) occupy columns of a 32-wide fp32 matrix
+ * (ppr_slots 0 or 32) and join or leave at iteration boundaries.  A worker
+ * thread drives the GPU; submit/poll/wait are thread-safe.  Results: BFS
+ * int32[n] levels (hops, -1 unreachable), PPR float[n].  A query's result
+ * is the same whatever else is in flight.  Needs a square ROW-layout graph
+ * with 32x32 tiles (and out-degrees for PPR). */
+typedef struct gbo_server gbo_server;
+typedef struct gbo_server_stats {
+  long long rounds;          /* worker rounds (one BFS level and/or PPR iteration) */
+  long long bfs_completed, ppr_completed;
+  long long kernel_launches;
+  long long pending, in_flight;
+} gbo_server_stats;
+GBO_API int gbo_server_create(const gbo_graph* g, int bfs_slots, int ppr_slots,
+                      float alpha, float tol, int ppr_max_iter,
+                      gbo_server** out);
+GBO_API int gbo_server_submit_bfs(gbo_server* s, int src, int64_t* ticket);
+GBO_API int gbo_server_submit_ppr(gbo_server* s, const int* verts,
+                          const float* weights, int count, int64_t* ticket);
+/* GBO_OK and the result copied to h_out (may be NULL), or GBO_ERR_NOTREADY. */
+GBO_API int gbo_server_poll(gbo_server* s, int64_t ticket, void* h_out,
+                    double* latency_ms, int* iterations);
+GBO_API int gbo_server_wait(gbo_server* s, int64_t ticket, void* h_out,
+                    double* latency_ms, int* iterations, double timeout_s);
+GBO_API int gbo_server_get_stats(gbo_server* s, gbo_server_stats* stats);
+GBO_API int gbo_server_destroy(gbo_server* s);
+
 /* Personalized PageRank p = alpha * P D^-1 p + (1-alpha) v  (fp32) and its
  * adjoint: for loss L = dot(w, p), grad_v = (1-alpha) u with
  * u = alpha * D^-1 P^T u + w.  Iterate until the L1 change <= tol or

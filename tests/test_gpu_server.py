@@ -1,0 +1,95 @@
+"""Continuous-batching query server: results vs the oracle, and each result
+identical alone and in the mix of concurrently running queries."""
+import threading
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l1(a, b):
+    return float(np.abs(np.asarray(a, np.float64) - b).sum() / np.abs(b).sum())
+
+
+def make_queries(n, nb, np_, seed):
+    rng = np.random.default_rng(seed)
+    qs = []
+    for _ in range(nb):
+        qs.append(("bfs", int(rng.integers(0, n))))
+    for _ in range(np_):
+        m = int(rng.integers(1, 65))
+        verts = rng.choice(n, m, replace=False).astype(np.int32)
+        wts = rng.dirichlet(np.ones(m)).astype(np.float32)
+        qs.append(("ppr", (verts, wts)))
+    order = rng.permutation(len(qs))
+    return [qs[i] for i in order]
+
+
+def submit_all(srv, qs, threads=2):
+    tickets = [None] * len(qs)
+
+    def run(part):
+        for i in part:
+            kind, arg = qs[i]
+            tickets[i] = srv.submit_bfs(arg) if kind == "bfs" else srv.submit_ppr(*arg)
+
+    parts = [range(t, len(qs), threads) for t in range(threads)]
+    ths = [threading.Thread(target=run, args=(p,)) for p in parts]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    return tickets
+
+
+def test_server_results_match_oracle_and_are_mix_independent(gbo, orc, gpu):
+    csr = gbo.gen_rmat(12, 16, seed=0)
+    n = csr.nrows
+    outdeg = np.bincount(csr.colind, minlength=n).astype(np.int32)
+    g = gbo.Graph.from_csr(csr, 32)
+    qs = make_queries(n, 150, 40, seed=11)
+    srv = gbo.Server(g, bfs_slots=64, ppr_slots=32, alpha=0.85, tol=1e-7)
+    tickets = submit_all(srv, qs)
+    mixed = []
+    for (kind, arg), t in zip(qs, tickets):
+        res, lat, it = srv.wait(t, kind)
+        assert lat >= 0 and it >= 1
+        mixed.append(res)
+    st = srv.stats()
+    assert st["bfs_completed"] == 150 and st["ppr_completed"] == 40 and st["in_flight"] == 0
+    srv.close()
+    for (kind, arg), res in zip(qs, mixed):
+        if kind == "bfs":
+            want, _ = orc.bfs_csr(csr.rowptr, csr.colind, n, arg)
+            assert np.array_equal(res, want), arg
+        else:
+            v = np.zeros(n)
+            v[arg[0]] = arg[1]
+            want, _ = orc.ppr_f64(csr.rowptr, csr.colind, n, outdeg, v, 0.85, 1e-13)
+            assert rel_l1(res, want) <= 1e-5
+    # each query alone on a fresh server gives the same bits as in the mix
+    srv1 = gbo.Server(g, bfs_slots=64, ppr_slots=32, alpha=0.85, tol=1e-7)
+    for idx in [i for i, q in enumerate(qs) if q[0] == "ppr"][:5] + [i for i, q in enumerate(qs) if q[0] == "bfs"][:5]:
+        kind, arg = qs[idx]
+        t = srv1.submit_bfs(arg) if kind == "bfs" else srv1.submit_ppr(*arg)
+        alone, _, _ = srv1.wait(t, kind)
+        assert np.array_equal(alone, mixed[idx]), (kind, idx)
+    srv1.close()
+
+
+def test_server_poll_and_errors(gbo, gpu):
+    g = gbo.Graph.from_csr(gbo.gen_er(1000, 0.02002, 0), 32)
+    srv = gbo.Server(g, bfs_slots=32, ppr_slots=0)
+    t = srv.submit_bfs(0)
+    got = None
+    for _ in range(100000):
+        got = srv.poll(t, "bfs")
+        if got is not None:
+            break
+    assert got is not None and got[0][0] == 0
+    with pytest.raises(gbo.GboError):
+        srv.submit_ppr([1], [1.0])  # no PPR slots
+    with pytest.raises(gbo.GboError):
+        srv.submit_bfs(10**6)
+    srv.close()
