@@ -39,6 +39,9 @@ def parse():
     ap.add_argument("--tile", type=int, default=TILE)
     ap.add_argument("--cpu-samples", type=int, default=3, help="BFS runs timed for cpu_baseline")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving streams")
+    ap.add_argument("--serve-qps", type=float, default=4000.0, help="offered BFS query rate")
+    ap.add_argument("--serve-s", type=float, default=1.5, help="seconds of arrivals per stream")
     return ap.parse_args()
 
 
@@ -250,6 +253,60 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------- serving
+def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed):
+    """Poisson arrivals of BFS sources and PPR sets (1..64 vertices, Dirichlet
+    weights) into the continuous-batching server; returns achieved qps and
+    p50/p99 latencies (submit to result in host memory)."""
+    import threading
+
+    rng = np.random.default_rng(seed)
+    nq = max(1, int(rate_qps * duration_s))
+    gaps = rng.exponential(1.0 / rate_qps, nq)
+    kinds = rng.random(nq) < ppr_frac
+    qs = []
+    for i in range(nq):
+        if kinds[i]:
+            m = int(rng.integers(1, 65))
+            qs.append(("ppr", (rng.choice(n, m, replace=False).astype(np.int32),
+                               rng.dirichlet(np.ones(m)).astype(np.float32))))
+        else:
+            qs.append(("bfs", int(rng.integers(0, n))))
+    srv = gbo.Server(g, bfs_slots=1024, ppr_slots=32 if ppr_frac > 0 else 0, alpha=0.85, tol=1e-7)
+    tickets = [None] * nq
+    t0 = time.perf_counter()
+
+    def producer():
+        t = t0
+        for i in range(nq):
+            t += gaps[i]
+            d = t - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            kind, arg = qs[i]
+            tickets[i] = srv.submit_bfs(arg) if kind == "bfs" else srv.submit_ppr(*arg)
+
+    th = threading.Thread(target=producer)
+    th.start()
+    th.join()
+    lat = {"bfs": [], "ppr": []}
+    for i in range(nq):
+        kind = qs[i][0]
+        _, ms, _ = srv.wait(tickets[i], kind, timeout=600.0)
+        lat[kind].append(ms)
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    out = {"offered_qps": rate_qps, "queries": nq, "achieved_qps": nq / wall, "wall_s": wall,
+           "rounds": st["rounds"]}
+    for k, v in lat.items():
+        if v:
+            out[f"{k}_p50_ms"] = float(np.percentile(v, 50))
+            out[f"{k}_p99_ms"] = float(np.percentile(v, 99))
+            out[f"{k}_count"] = len(v)
+    return out
+
+
 # ------------------------------------------------------------- our arm
 def run_ours(args, ws, rank, local):
     import gbo
@@ -354,6 +411,13 @@ def run_ours(args, ws, rank, local):
         batched[f"k{kq}"] = {"ms": mms, "qps": kq / (mms / 1e3),
                             "qps_vs_plain": (kq / mms) / (1.0 / ms)}
         d_lv.free()
+
+    # served: Poisson query streams into the continuous-batching server
+    served = {}
+    if not args.no_serve:
+        served["bfs_only"] = serve_stream(gbo, g, n, args.serve_qps, args.serve_s, 0.0, 5)
+        served["bfs_only"]["vs_plain_bfs_qps"] = served["bfs_only"]["achieved_qps"] / (1e3 / ms)
+        served["mixed_10pct_ppr"] = serve_stream(gbo, g, n, args.serve_qps / 4, args.serve_s, 0.1, 6)
     wb = max(1, args.tile // 8)
     bmv_bytes = (int(info.nblocks) * (args.tile * args.tile // 8 + 4) + 4 * (info.nblockrows + 1)
                  + wb * info.nblockcols + 4 * n)
@@ -383,6 +447,7 @@ def run_ours(args, ws, rank, local):
         "bmv_count": {"achieved_gbs": bmv_gbs, "frac": bmv_gbs / peak, "ms": bmv_ms,
                       "algorithmic_bytes": bmv_bytes, "gteps": csr.nnz / (bmv_ms / 1e3) / 1e9},
         "batched_bfs": dict(batched, plain_qps=1e3 / ms),
+        "served": served,
         "levels_ms": [float(v) for v in lvl_ms[:k]],
         "levels_gb": [b / 1e9 for b in lvl_bytes[:k]],
         "graph_build_s": build_s,

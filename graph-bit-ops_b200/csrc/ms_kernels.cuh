@@ -102,10 +102,16 @@ __device__ __forceinline__ void block_row_epilogue(const Args& a, int R, int lvl
   }
 }
 
+// Bit pairs (tile row r, frontier vertex j) queued per warp before their
+// frontier rows are gathered: S pairs per round, U rounds in flight.
+constexpr int kList = 192;
+
 template <int KW>
 __global__ void __launch_bounds__(kTPB) k_step(Args a) {
   constexpr int S = 32 / KW;
+  constexpr int U = S >= 8 ? 1 : 8 / S;
   __shared__ uint32_t acc_sh[kWarps][32 * KW];
+  __shared__ int2 list_sh[kWarps][kList];
   volatile int* c = a.ctl;
   if (c[1]) return;  // done
   const int lvl = c[0];
@@ -125,8 +131,34 @@ __global__ void __launch_bounds__(kTPB) k_step(Args a) {
     if (vrow != 0xffffffffu) {
       for (int q = lane; q < 32 * KW; q += 32) acc[q] = 0u;
       __syncwarp();
-      const unsigned need_rows = ~__brev(vrow);  // lane-bit r = row r still open
+      const bool row_open = !((vrow >> (31 - lane)) & 1u);  // lane r: row r still open
       const uint32_t* __restrict__ val = reinterpret_cast<const uint32_t*>(v.val);
+      int2* list = list_sh[wib];
+      int nlist = 0;  // warp-uniform
+      // gather the queued frontier rows, S pairs per round, U rounds in flight
+      auto flush = [&]() {
+        __syncwarp();
+        for (int base = 0; base < nlist; base += S * U) {
+          uint32_t f[U];
+          int rr[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int e = base + s + S * u;
+            rr[u] = -1;
+            f[u] = 0;
+            if (e < nlist) {
+              const int2 ent = list[e];
+              rr[u] = ent.x;
+              f[u] = F[(size_t)ent.y * KW + w];
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < U; ++u)
+            if (rr[u] >= 0 && f[u]) atomicOr(acc + rr[u] * KW + w, f[u]);
+        }
+        nlist = 0;
+        __syncwarp();
+      };
       for (int b0 = it.t0; b0 < it.t1; b0 += 32) {
         const int t = b0 + (int)lane;
         int cb = 0;
@@ -141,28 +173,53 @@ __global__ void __launch_bounds__(kTPB) k_step(Args a) {
           tiles &= tiles - 1;
           const int C = __shfl_sync(0xffffffffu, cb, jt);
           const uint32_t fcol = __shfl_sync(0xffffffffu, fw, jt);
-          const uint32_t eff = val[(size_t)(b0 + jt) * 32 + lane] & fcol;  // lane r: row r
-          unsigned rows = __ballot_sync(0xffffffffu, eff != 0) & need_rows;
-          while (rows) {
-            const int r = __ffs(rows) - 1;
-            rows &= rows - 1;
-            unsigned bits = __shfl_sync(0xffffffffu, eff, r);
-            uint32_t racc = 0;
-            while (bits) {
-              const unsigned pos = nth_set_bit(bits, s + 1);
-              uint32_t f = 0;
-              if (pos != 0xffffffffu) f = F[((size_t)C * 32 + (31 - (int)pos)) * KW + w];
+          uint32_t eff = val[(size_t)(b0 + jt) * 32 + lane] & fcol;  // lane r: row r
+          if (!row_open) eff = 0u;
+          // queue this lane's pairs (lane, C*32+c) at its prefix offset
+          const int cnt_l = __popc(eff);
+          int pre = cnt_l;
 #pragma unroll
-              for (int o = KW; o < 32; o <<= 1) f |= __shfl_xor_sync(0xffffffffu, f, o);
-              racc |= f;
-              const unsigned last = nth_set_bit(bits, S);
-              bits = last == 0xffffffffu ? 0u : (bits & ~(0xffffffffu >> (31 - last)));
-            }
-            if (s == 0) acc[r * KW + w] |= racc;
+          for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, pre, o);
+            if ((int)lane >= o) pre += y;
           }
+          const int total = __shfl_sync(0xffffffffu, pre, 31);
+          pre -= cnt_l;
+          if (total == 0) continue;
+          if (nlist + total > kList) flush();
+          if (total > kList) {
+            // dense tile: OR its rows straight from the row words
+            unsigned rows = __ballot_sync(0xffffffffu, eff != 0);
+            while (rows) {
+              const int r = __ffs(rows) - 1;
+              rows &= rows - 1;
+              unsigned bits = __shfl_sync(0xffffffffu, eff, r);
+              uint32_t racc = 0;
+              while (bits) {
+                const unsigned pos = nth_set_bit(bits, s + 1);
+                uint32_t f = 0;
+                if (pos != 0xffffffffu) f = F[((size_t)C * 32 + (31 - (int)pos)) * KW + w];
+#pragma unroll
+                for (int o = KW; o < 32; o <<= 1) f |= __shfl_xor_sync(0xffffffffu, f, o);
+                racc |= f;
+                const unsigned last = nth_set_bit(bits, S);
+                bits = last == 0xffffffffu ? 0u : (bits & ~(0xffffffffu >> (31 - last)));
+              }
+              if (s == 0) acc[r * KW + w] |= racc;
+            }
+            continue;
+          }
+          int pos = nlist + pre;
+          uint32_t m = eff;
+          while (m) {
+            const int col = __clz(m);
+            m &= ~(0x80000000u >> col);
+            list[pos++] = make_int2((int)lane, C * 32 + col);
+          }
+          nlist += total;
         }
       }
-      __syncwarp();
+      flush();
       if (it.slot >= 0) {
         uint32_t* dst = a.scratch + (size_t)it.slot * 32 * KW;
         for (int q = lane; q < 32 * KW; q += 32) dst[q] = acc[q];
