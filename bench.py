@@ -273,7 +273,11 @@ def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed):
         else:
             qs.append(("bfs", int(rng.integers(0, n))))
     srv = gbo.Server(g, bfs_slots=1024, ppr_slots=32 if ppr_frac > 0 else 0, alpha=0.85, tol=1e-7)
-    tickets = [None] * nq
+    import queue
+
+    tq = queue.Queue()
+    lat = {"bfs": [], "ppr": []}
+    lock = threading.Lock()
     t0 = time.perf_counter()
 
     def producer():
@@ -284,16 +288,26 @@ def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed):
             if d > 0:
                 time.sleep(d)
             kind, arg = qs[i]
-            tickets[i] = srv.submit_bfs(arg) if kind == "bfs" else srv.submit_ppr(*arg)
+            tq.put((kind, srv.submit_bfs(arg) if kind == "bfs" else srv.submit_ppr(*arg)))
+        for _ in range(consumers):
+            tq.put(None)
 
-    th = threading.Thread(target=producer)
-    th.start()
-    th.join()
-    lat = {"bfs": [], "ppr": []}
-    for i in range(nq):
-        kind = qs[i][0]
-        _, ms, _ = srv.wait(tickets[i], kind, timeout=600.0)
-        lat[kind].append(ms)
+    def consumer():
+        while True:
+            item = tq.get()
+            if item is None:
+                return
+            kind, ticket = item
+            _, ms, _ = srv.wait(ticket, kind, timeout=600.0)
+            with lock:
+                lat[kind].append(ms)
+
+    consumers = 8
+    ths = [threading.Thread(target=producer)] + [threading.Thread(target=consumer) for _ in range(consumers)]
+    for th in ths:
+        th.start()
+    for th in ths:
+        th.join()
     wall = time.perf_counter() - t0
     st = srv.stats()
     srv.close()
@@ -417,7 +431,7 @@ def run_ours(args, ws, rank, local):
     if not args.no_serve:
         served["bfs_only"] = serve_stream(gbo, g, n, args.serve_qps, args.serve_s, 0.0, 5)
         served["bfs_only"]["vs_plain_bfs_qps"] = served["bfs_only"]["achieved_qps"] / (1e3 / ms)
-        served["mixed_10pct_ppr"] = serve_stream(gbo, g, n, args.serve_qps / 4, args.serve_s, 0.1, 6)
+        served["mixed_10pct_ppr"] = serve_stream(gbo, g, n, args.serve_qps / 8, args.serve_s, 0.1, 6)
     wb = max(1, args.tile // 8)
     bmv_bytes = (int(info.nblocks) * (args.tile * args.tile // 8 + 4) + 4 * (info.nblockrows + 1)
                  + wb * info.nblockcols + 4 * n)

@@ -36,7 +36,15 @@ struct Args {
   int* ctl;  // iter, done, ticket, max_iter, count (u64 at ctl + 4)
   uint32_t* scratch;
   uint32_t* slot_any;  // optional: OR of the new bits of every source word
+  int level_group;     // 0: levels[i*k + s]; g > 0: levels[((s/g)*n + i)*g + s%g]
 };
+
+// Address of the level of (vertex i, source s) in either layout.
+__device__ __forceinline__ size_t level_index(const Args& a, long long i, int s) {
+  if (a.level_group == 0) return (size_t)i * a.k + s;
+  const int g = a.level_group;
+  return ((size_t)(s / g) * a.v.nrows + i) * g + s % g;
+}
 
 __device__ __forceinline__ unsigned nth_set_bit(unsigned m, int nth) {
   return __fns(m, 0, nth);  // position of the nth (1-based) set bit from bit 0
@@ -86,7 +94,7 @@ __device__ __forceinline__ void block_row_epilogue(const Args& a, int R, int lvl
       while (m) {
         const int p = __ffs(m) - 1;
         m &= m - 1;
-        a.levels[(size_t)i * a.k + w * 32 + p] = lvl + 1;
+        a.levels[level_index(a, i, w * 32 + p)] = lvl + 1;
       }
     }
 #pragma unroll
@@ -339,7 +347,7 @@ static __global__ void k_seed(Args a, const int* __restrict__ srcs, const int* _
       for (int w = 0; w < kw; ++w) F[(size_t)v0 * kw + w] = 0u;
     F[(size_t)v0 * kw + s / 32] |= 1u << (s % 32);
     a.V[(size_t)v0 * kw + s / 32] |= 1u << (s % 32);
-    a.levels[(size_t)v0 * a.k + s] = lvl;
+    a.levels[level_index(a, v0, s)] = lvl;
     fb[v0 / 32] |= 1u << (31 - v0 % 32);
     a.vfull[v0 / 32] &= ~(1u << (31 - v0 % 32));
   }

@@ -55,6 +55,7 @@ ms::Args make_args(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
   a.ctl = m.ctl;
   a.scratch = m.scratch;
   a.slot_any = nullptr;
+  a.level_group = 0;  // the API's vertex-major levels[v * k + s]
   return a;
 }
 

@@ -44,6 +44,7 @@ struct PprArgs {
   const float* P;  // (1 - alpha) * personalization, n * 32
   float alpha;
   int parity;      // X half holding the current iterate
+  uint32_t active; // slots still iterating; the others keep their column
   double* err;     // 32 slot L1 changes
   double* scratch; // split slots: 32 rows x 32 slots doubles each
 };
@@ -97,6 +98,10 @@ __global__ void __launch_bounds__(kPprTPB) k_ppr_step(PprArgs a) {
         const long long i = (long long)it.row * 32 + r;
         if (i >= v.nrows) break;
         const size_t o = (size_t)i * kPprSlots + lane;
+        if (!((a.active >> lane) & 1u)) {
+          Xn[o] = X[o];
+          continue;
+        }
         const float y = (float)((double)a.alpha * acc[r * kPprSlots + lane] + (double)a.P[o]);
         e += fabs((double)y - (double)X[o]);
         Xn[o] = y;
@@ -129,6 +134,10 @@ __global__ void __launch_bounds__(kPprTPB) k_ppr_finish(PprArgs a) {
       double s = 0.0;
       for (int q = 0; q < sp.nslots; ++q) s += a.scratch[((size_t)(sp.slot0 + q) * 32 + r) * kPprSlots + lane];
       const size_t o = (size_t)i * kPprSlots + lane;
+      if (!((a.active >> lane) & 1u)) {
+        Xn[o] = X[o];
+        continue;
+      }
       const float y = (float)((double)a.alpha * s + (double)a.P[o]);
       e += fabs((double)y - (double)X[o]);
       Xn[o] = y;
@@ -178,32 +187,71 @@ __global__ void k_ppr_admit_set(float* X, size_t xstride, int parity, float* P, 
     }
 }
 
-// Copy column s of the current iterate out (and leave the column as is; a
-// new admission clears it).
-__global__ void k_ppr_extract(const float* X, size_t xstride, int parity, int n, int s, float* out) {
-  const float* Xc = X + (size_t)parity * xstride;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x)
-    out[i] = Xc[(size_t)i * kPprSlots + s];
-}
+// ------------------------------------------------------------- retirement
+// Up to kRetire finished slots leave per round.  Their results are written
+// to a device staging area (one n-vector per slot) by a transposing kernel
+// that reads the slots' values row by row and writes each result
+// contiguously; the staging area then goes to pinned host buffers with
+// asynchronous copies on a second stream, so the next round overlaps them.
+constexpr int kRetire = 64;
+constexpr int kRetRows = 64;  // rows per block of the transposing kernels
 
-// ------------------------------------------------------ BFS slot kernels
-// Result of slot s: levels relative to its start level; then clear the
-// slot's column (levels -1, visited bit 0) for the next query.
-__global__ void k_bfs_extract(int* levels, uint32_t* V, int n, int kb, int kw, int s, int start,
-                              int* out) {
-  const uint32_t bit = 1u << (s % 32);
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const size_t o = (size_t)i * kb + s;
-    const int lv = levels[o];
-    out[i] = lv >= 0 ? lv - start : -1;
-    levels[o] = -1;
-    V[(size_t)i * kw + s / 32] &= ~bit;
+struct RetireList {
+  int count;
+  int slot[kRetire];
+  int start[kRetire];
+  uint32_t clr[32];  // visited bits to clear, per source word
+};
+
+// BFS: out[f][i] = level of (i, slot f) relative to its start level, -1 if
+// unreachable; the slot's levels become -1 and its visited bits 0.
+__global__ void __launch_bounds__(256) k_bfs_retire(int* levels, int g, uint32_t* V, int n, int kw,
+                                                    RetireList rl, int* out) {
+  __shared__ int sm[kRetire][kRetRows + 1];
+  const long long i0 = (long long)blockIdx.x * kRetRows;
+  const int R = rl.count;
+  for (int q = threadIdx.x; q < kRetRows * R; q += blockDim.x) {
+    const int ii = q / R, f = q % R;
+    const long long i = i0 + ii;
+    if (i >= n) continue;
+    const int s = rl.slot[f];
+    const size_t idx = ((size_t)(s / g) * n + i) * g + s % g;
+    const int lv = levels[idx];
+    sm[f][ii] = lv >= 0 ? lv - rl.start[f] : -1;
+    levels[idx] = -1;
+  }
+  for (int q = threadIdx.x; q < kRetRows * kw; q += blockDim.x) {
+    const int ii = q / kw, w = q % kw;
+    const long long i = i0 + ii;
+    if (i < n && rl.clr[w]) V[(size_t)i * kw + w] &= ~rl.clr[w];
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < kRetRows * R; q += blockDim.x) {
+    const int f = q / kRetRows, ii = q % kRetRows;
+    const long long i = i0 + ii;
+    if (i < n) out[(size_t)f * n + i] = sm[f][ii];
   }
 }
 
-// After a visited column was cleared no row is "all sources visited" any
+// PPR: out[f][i] = X[i][slot f] of the current iterate.
+__global__ void __launch_bounds__(256) k_ppr_retire(const float* X, int n, RetireList rl, float* out) {
+  __shared__ float sm[kRetire][kRetRows + 1];
+  const long long i0 = (long long)blockIdx.x * kRetRows;
+  const int R = rl.count;
+  for (int q = threadIdx.x; q < kRetRows * R; q += blockDim.x) {
+    const int ii = q / R, f = q % R;
+    const long long i = i0 + ii;
+    if (i < n) sm[f][ii] = X[(size_t)i * kPprSlots + rl.slot[f]];
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < kRetRows * R; q += blockDim.x) {
+    const int f = q / kRetRows, ii = q % kRetRows;
+    const long long i = i0 + ii;
+    if (i < n) out[(size_t)f * n + i] = sm[f][ii];
+  }
+}
+
+// After visited columns were cleared no row is "all sources visited" any
 // more: keep only the padding rows marked.
 __global__ void k_vfull_reset(uint32_t* vfull, int nbr, int n) {
   for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q <= nbr;
@@ -227,7 +275,9 @@ struct Query {
 
 struct Result {
   int kind;
-  std::vector<char> data;  // n int32 (BFS) or n float32 (PPR)
+  int buf;          // pinned pool buffer holding the result
+  cudaEvent_t ev;   // its copy has landed when this event completes
+  bool landed;
   double t_submit, t_done;
   int iters;
 };
@@ -240,20 +290,21 @@ struct gbo_server {
   int n = 0, nbr = 0;
   float alpha = 0.85f, tol = 1e-7f;
   int ppr_max_iter = 1000;
-  cudaStream_t s = nullptr;
+  cudaStream_t s = nullptr;   // compute
+  cudaStream_t cs = nullptr;  // result copies
   int dev = 0;
-  // BFS engine
+  // BFS engine (levels grouped 8 sources per 32-byte sector)
   int kb = 0, kw = 0;
   uint32_t *F = nullptr, *V = nullptr, *fbits = nullptr, *vfull = nullptr, *scratch = nullptr;
   int* levels = nullptr;
   int* ctl = nullptr;
-  int* h_ctl = nullptr;
   uint32_t* slot_any = nullptr;
   uint32_t* h_slot_any = nullptr;
   int *d_adm_src = nullptr, *d_adm_slot = nullptr;
   int level = 0;
   std::vector<long long> bslot_ticket;
   std::vector<int> bslot_start;
+  std::vector<char> bslot_finished;
   // PPR engine
   float *X = nullptr, *P = nullptr;
   double* err = nullptr;
@@ -264,16 +315,21 @@ struct gbo_server {
   int parity = 0;
   std::vector<long long> pslot_ticket;
   std::vector<int> pslot_iters;
-  std::vector<double> pslot_submit;
-  // extraction
-  void* d_out = nullptr;
-  void* h_stage = nullptr;
+  std::vector<char> pslot_finished;
+  // results: device staging (double-buffered), pinned host pool
+  void* d_stage[2] = {nullptr, nullptr};
+  cudaEvent_t stage_free[2] = {nullptr, nullptr};
+  int stage_next = 0;
+  std::vector<void*> pool;
+  std::vector<int> pool_free;
+  std::vector<cudaEvent_t> pool_ev;
   // host side
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<gbo::Query> pending;
   std::map<long long, gbo::Result> results;
   std::map<long long, double> submit_time;
+  int copies_in_flight = 0;
   long long next_ticket = 1;
   bool stop = false;
   int worker_status = GBO_OK;
@@ -286,8 +342,7 @@ struct gbo_server {
 namespace gbo {
 namespace {
 
-template <int KW>
-int bfs_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm, std::vector<int>& finished) {
+ms::Args bfs_args(gbo_server* S) {
   ms::Args a;
   a.v = view_of(S->g);
   a.F = S->F;
@@ -300,6 +355,13 @@ int bfs_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm, std::
   a.ctl = S->ctl;
   a.scratch = S->scratch;
   a.slot_any = S->slot_any;
+  a.level_group = 8;
+  return a;
+}
+
+template <int KW>
+int bfs_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
+  const ms::Args a = bfs_args(S);
   cudaStream_t st = S->s;
   if (!adm.empty()) {
     std::vector<int> src, slot;
@@ -312,8 +374,7 @@ int bfs_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm, std::
     ms::k_seed<<<1, 32, 0, st>>>(a, S->d_adm_src, S->d_adm_slot, (int)src.size(), S->kw, S->level);
     S->launches++;
   }
-  // one level: iter = current level, not done, count 0
-  int h[4] = {S->level, 0, 0, 0x7fffffff};
+  int h[4] = {S->level, 0, 0, 0x7fffffff};  // level, not done, ticket 0, no iteration cap
   GBO_CUDA_TRY(cudaMemcpyAsync(S->ctl, h, sizeof(h), cudaMemcpyHostToDevice, st));
   GBO_CUDA_TRY(cudaMemsetAsync(S->ctl + 4, 0, 8, st));
   GBO_CUDA_TRY(cudaMemsetAsync(S->slot_any, 0, sizeof(uint32_t) * S->kw, st));
@@ -327,11 +388,12 @@ int bfs_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm, std::
   GBO_CUDA_TRY(cudaStreamSynchronize(st));
   S->level += 1;
   for (int q = 0; q < S->kb; ++q)
-    if (S->bslot_ticket[q] > 0 && !((S->h_slot_any[q / 32] >> (q % 32)) & 1u)) finished.push_back(q);
+    if (S->bslot_ticket[q] > 0 && !S->bslot_finished[q] && !((S->h_slot_any[q / 32] >> (q % 32)) & 1u))
+      S->bslot_finished[q] = 1;
   return GBO_OK;
 }
 
-int ppr_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm, std::vector<int>& finished) {
+int ppr_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
   cudaStream_t st = S->s;
   const size_t xstride = (size_t)S->n * kPprSlots;
   if (!adm.empty()) {
@@ -366,6 +428,9 @@ int ppr_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm, std::
   a.P = S->P;
   a.alpha = S->alpha;
   a.parity = S->parity;
+  a.active = 0u;
+  for (int q = 0; q < kPprSlots; ++q)
+    if (S->pslot_ticket[(size_t)q] > 0 && !S->pslot_finished[(size_t)q]) a.active |= 1u << q;
   a.err = S->err;
   a.scratch = S->pscratch;
   GBO_CUDA_TRY(cudaMemsetAsync(S->err, 0, sizeof(double) * kPprSlots, st));
@@ -378,12 +443,101 @@ int ppr_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm, std::
   GBO_CUDA_TRY(cudaStreamSynchronize(st));
   S->parity ^= 1;
   for (int q = 0; q < kPprSlots; ++q) {
-    if (S->pslot_ticket[q] <= 0) continue;
+    if (S->pslot_ticket[q] <= 0 || S->pslot_finished[q]) continue;
     S->pslot_iters[q] += 1;
     if ((S->tol >= 0 && S->h_err[q] <= (double)S->tol) || S->pslot_iters[q] >= S->ppr_max_iter)
-      finished.push_back(q);
+      S->pslot_finished[q] = 1;
   }
   return GBO_OK;
+}
+
+// Retire finished slots of one engine (kind 0 BFS, 1 PPR) while pinned
+// buffers are free.  Called without the lock.
+int retire(gbo_server* S, int kind) {
+  std::vector<long long>& tick = kind == 0 ? S->bslot_ticket : S->pslot_ticket;
+  std::vector<char>& fin = kind == 0 ? S->bslot_finished : S->pslot_finished;
+  RetireList rl;
+  memset(&rl, 0, sizeof(rl));
+  std::vector<int> bufs;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    for (size_t q = 0; q < tick.size() && rl.count < kRetire; ++q) {
+      if (tick[q] <= 0 || !fin[q] || S->pool_free.empty()) continue;
+      rl.slot[rl.count] = (int)q;
+      rl.start[rl.count] = kind == 0 ? S->bslot_start[q] : 0;
+      if (kind == 0) rl.clr[q / 32] |= 1u << (q % 32);
+      bufs.push_back(S->pool_free.back());
+      S->pool_free.pop_back();
+      rl.count++;
+    }
+  }
+  if (rl.count == 0) return GBO_OK;
+  const int sb = S->stage_next;
+  S->stage_next ^= 1;
+  GBO_CUDA_TRY(cudaStreamWaitEvent(S->s, S->stage_free[sb], 0));  // its previous copies are done
+  const unsigned grid = blocks_for(S->n, kRetRows);
+  if (kind == 0) {
+    k_bfs_retire<<<grid, 256, 0, S->s>>>(S->levels, 8, S->V, S->n, S->kw, rl, (int*)S->d_stage[sb]);
+    k_vfull_reset<<<blocks_for(S->nbr + 1, 256), 256, 0, S->s>>>(S->vfull, S->nbr, S->n);
+    S->launches += 2;
+  } else {
+    k_ppr_retire<<<grid, 256, 0, S->s>>>(S->X + (size_t)S->parity * S->n * kPprSlots, S->n, rl,
+                                         (float*)S->d_stage[sb]);
+    S->launches += 1;
+  }
+  GBO_CUDA_TRY(cudaGetLastError());
+  cudaEvent_t ready;
+  GBO_CUDA_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+  GBO_CUDA_TRY(cudaEventRecord(ready, S->s));
+  GBO_CUDA_TRY(cudaStreamWaitEvent(S->cs, ready, 0));
+  cudaEventDestroy(ready);
+  const size_t rbytes = sizeof(int) * (size_t)S->n;
+  const double t_now = now_ms();
+  std::lock_guard<std::mutex> lk(S->mu);
+  for (int f = 0; f < rl.count; ++f) {
+    const int b = bufs[(size_t)f];
+    GBO_CUDA_TRY(cudaMemcpyAsync(S->pool[(size_t)b], (char*)S->d_stage[sb] + (size_t)f * rbytes, rbytes,
+                                 cudaMemcpyDeviceToHost, S->cs));
+    GBO_CUDA_TRY(cudaEventRecord(S->pool_ev[(size_t)b], S->cs));
+    const int q = rl.slot[f];
+    const long long t = tick[(size_t)q];
+    Result r;
+    r.kind = kind;
+    r.buf = b;
+    r.ev = S->pool_ev[(size_t)b];
+    r.landed = false;
+    r.t_submit = S->submit_time[t];
+    r.t_done = t_now;
+    r.iters = kind == 0 ? S->level - S->bslot_start[(size_t)q] : S->pslot_iters[(size_t)q];
+    S->results[t] = r;
+    S->copies_in_flight++;
+    tick[(size_t)q] = 0;
+    fin[(size_t)q] = 0;
+    if (kind == 0) S->bfs_done++;
+    else S->ppr_done++;
+  }
+  GBO_CUDA_TRY(cudaEventRecord(S->stage_free[sb], S->cs));
+  return GBO_OK;
+}
+
+// Mark results whose copies have landed (caller holds the lock).
+bool collect_landed(gbo_server* S) {
+  bool any = false;
+  if (S->copies_in_flight == 0) return false;
+  const double t = now_ms();
+  for (auto& kv : S->results) {
+    Result& r = kv.second;
+    if (r.landed) continue;
+    if (cudaEventQuery(r.ev) == cudaSuccess) {
+      r.landed = true;
+      r.t_done = t;
+      S->copies_in_flight--;
+      any = true;
+    } else {
+      (void)cudaGetLastError();  // cudaErrorNotReady is not an error here
+    }
+  }
+  return any;
 }
 
 void worker_main(gbo_server* S) {
@@ -394,127 +548,81 @@ void worker_main(gbo_server* S) {
     S->worker_error = gbo_last_error();
     S->cv_done.notify_all();
   };
-  const size_t rbytes = sizeof(int) * (size_t)S->n;
+  auto occupied = [&](const std::vector<long long>& tab) {
+    for (long long t : tab)
+      if (t > 0) return true;
+    return false;
+  };
+  auto unfinished = [&](const std::vector<long long>& tab, const std::vector<char>& fin) {
+    for (size_t q = 0; q < tab.size(); ++q)
+      if (tab[q] > 0 && !fin[q]) return true;
+    return false;
+  };
   while (true) {
     std::vector<std::pair<int, Query>> badm, padm;
     {
       std::unique_lock<std::mutex> lk(S->mu);
-      auto busy = [&] {
-        for (long long t : S->bslot_ticket)
-          if (t > 0) return true;
-        for (long long t : S->pslot_ticket)
-          if (t > 0) return true;
-        return false;
-      };
-      S->cv_work.wait(lk, [&] { return S->stop || !S->pending.empty() || busy(); });
-      if (S->stop) return;
+      for (;;) {
+        if (collect_landed(S)) S->cv_done.notify_all();
+        if (S->stop) return;
+        const bool work = !S->pending.empty() || unfinished(S->bslot_ticket, S->bslot_finished) ||
+                          unfinished(S->pslot_ticket, S->pslot_finished) ||
+                          ((occupied(S->bslot_ticket) || occupied(S->pslot_ticket)) && !S->pool_free.empty());
+        if (work) break;
+        if (S->copies_in_flight > 0)
+          S->cv_work.wait_for(lk, std::chrono::microseconds(200));
+        else
+          S->cv_work.wait(lk);
+      }
       // admission into free slots, arrival order, per engine
       std::deque<Query> keep;
+      std::vector<char> btaken(S->bslot_ticket.size(), 0), ptaken(S->pslot_ticket.size(), 0);
+      size_t bnext = 0, pnext = 0;
       while (!S->pending.empty()) {
         Query q = std::move(S->pending.front());
         S->pending.pop_front();
         std::vector<long long>& tab = q.kind == 0 ? S->bslot_ticket : S->pslot_ticket;
-        int slot = -1;
-        for (size_t z = 0; z < tab.size(); ++z)
-          if (tab[z] == 0) {
-            bool taken = false;
-            for (auto& p : (q.kind == 0 ? badm : padm))
-              if (p.first == (int)z) taken = true;
-            if (!taken) {
-              slot = (int)z;
-              break;
-            }
-          }
-        if (slot < 0) {
+        size_t& nx = q.kind == 0 ? bnext : pnext;
+        while (nx < tab.size() && tab[nx] != 0) ++nx;
+        if (nx >= tab.size()) {
           keep.push_back(std::move(q));
           continue;
         }
+        const int slot = (int)nx++;
         tab[(size_t)slot] = q.ticket;
         if (q.kind == 0) {
           S->bslot_start[(size_t)slot] = S->level;
+          S->bslot_finished[(size_t)slot] = 0;
           badm.emplace_back(slot, std::move(q));
         } else {
           S->pslot_iters[(size_t)slot] = 0;
-          S->pslot_submit[(size_t)slot] = q.t_submit;
+          S->pslot_finished[(size_t)slot] = 0;
           padm.emplace_back(slot, std::move(q));
         }
       }
       S->pending.swap(keep);
     }
-    bool bfs_busy = !badm.empty(), ppr_busy = !padm.empty();
-    for (long long t : S->bslot_ticket) bfs_busy |= t > 0;
-    for (long long t : S->pslot_ticket) ppr_busy |= t > 0;
-    std::vector<int> bfin, pfin;
     int st = GBO_OK;
+    const bool bfs_busy = !badm.empty() || unfinished(S->bslot_ticket, S->bslot_finished);
+    const bool ppr_busy = !padm.empty() || unfinished(S->pslot_ticket, S->pslot_finished);
     if (bfs_busy && S->kb > 0) {
       switch (S->kw) {
-        case 1: st = bfs_round<1>(S, badm, bfin); break;
-        case 2: st = bfs_round<2>(S, badm, bfin); break;
-        case 4: st = bfs_round<4>(S, badm, bfin); break;
-        case 8: st = bfs_round<8>(S, badm, bfin); break;
-        case 16: st = bfs_round<16>(S, badm, bfin); break;
-        default: st = bfs_round<32>(S, badm, bfin); break;
+        case 1: st = bfs_round<1>(S, badm); break;
+        case 2: st = bfs_round<2>(S, badm); break;
+        case 4: st = bfs_round<4>(S, badm); break;
+        case 8: st = bfs_round<8>(S, badm); break;
+        case 16: st = bfs_round<16>(S, badm); break;
+        default: st = bfs_round<32>(S, badm); break;
       }
     }
-    if (st == GBO_OK && ppr_busy && S->g->invdeg) st = ppr_round(S, padm, pfin);
+    if (st == GBO_OK && ppr_busy && S->g->invdeg) st = ppr_round(S, padm);
+    if (st == GBO_OK && S->kb > 0) st = retire(S, 0);
+    if (st == GBO_OK && !S->pslot_ticket.empty()) st = retire(S, 1);
     if (st != GBO_OK) {
       failw(st);
       return;
     }
     S->rounds++;
-    // retire finished slots: extract, copy to host, free the slot
-    for (int q : bfin) {
-      const unsigned gv = blocks_for(S->n, 256) > 2048u ? 2048u : blocks_for(S->n, 256);
-      k_bfs_extract<<<gv, 256, 0, S->s>>>(S->levels, S->V, S->n, S->kb, S->kw, q,
-                                          S->bslot_start[(size_t)q], (int*)S->d_out);
-      cudaMemcpyAsync(S->h_stage, S->d_out, rbytes, cudaMemcpyDeviceToHost, S->s);
-      if (cudaStreamSynchronize(S->s) != cudaSuccess) {
-        failw(fail(GBO_ERR_CUDA, "server BFS extraction"));
-        return;
-      }
-      S->launches++;
-      Result r;
-      r.kind = 0;
-      r.data.assign((char*)S->h_stage, (char*)S->h_stage + rbytes);
-      r.t_done = now_ms();
-      r.iters = S->level - S->bslot_start[(size_t)q];
-      std::lock_guard<std::mutex> lk(S->mu);
-      const long long t = S->bslot_ticket[(size_t)q];
-      r.t_submit = S->submit_time[t];
-      S->results[t] = std::move(r);
-      S->bslot_ticket[(size_t)q] = 0;
-      S->bfs_done++;
-    }
-    if (!bfin.empty()) {
-      k_vfull_reset<<<blocks_for(S->nbr + 1, 256), 256, 0, S->s>>>(S->vfull, S->nbr, S->n);
-      S->launches++;
-    }
-    for (int q : pfin) {
-      const unsigned gv = blocks_for(S->n, 256) > 2048u ? 2048u : blocks_for(S->n, 256);
-      k_ppr_extract<<<gv, 256, 0, S->s>>>(S->X, (size_t)S->n * kPprSlots, S->parity, S->n, q,
-                                          (float*)S->d_out);
-      cudaMemcpyAsync(S->h_stage, S->d_out, rbytes, cudaMemcpyDeviceToHost, S->s);
-      if (cudaStreamSynchronize(S->s) != cudaSuccess) {
-        failw(fail(GBO_ERR_CUDA, "server PPR extraction"));
-        return;
-      }
-      S->launches++;
-      Result r;
-      r.kind = 1;
-      r.data.assign((char*)S->h_stage, (char*)S->h_stage + rbytes);
-      r.t_done = now_ms();
-      r.iters = S->pslot_iters[(size_t)q];
-      std::lock_guard<std::mutex> lk(S->mu);
-      const long long t = S->pslot_ticket[(size_t)q];
-      r.t_submit = S->submit_time[t];
-      S->results[t] = std::move(r);
-      S->pslot_ticket[(size_t)q] = 0;
-      S->ppr_done++;
-    }
-    if (!bfin.empty() || !pfin.empty()) {
-      std::lock_guard<std::mutex> lk(S->mu);
-      S->cv_done.notify_all();
-    }
   }
 }
 
@@ -526,6 +634,8 @@ void destroy_server(gbo_server* S) {
   }
   S->cv_work.notify_all();
   if (S->worker.joinable()) S->worker.join();
+  if (S->s) cudaStreamSynchronize(S->s);
+  if (S->cs) cudaStreamSynchronize(S->cs);
   cudaFree(S->F);
   cudaFree(S->V);
   cudaFree(S->fbits);
@@ -533,7 +643,6 @@ void destroy_server(gbo_server* S) {
   cudaFree(S->scratch);
   cudaFree(S->levels);
   cudaFree(S->ctl);
-  cudaFreeHost(S->h_ctl);
   cudaFree(S->slot_any);
   cudaFreeHost(S->h_slot_any);
   cudaFree(S->d_adm_src);
@@ -547,9 +656,14 @@ void destroy_server(gbo_server* S) {
   cudaFree(S->d_pverts);
   cudaFree(S->d_poff);
   cudaFree(S->d_pwts);
-  cudaFree(S->d_out);
-  cudaFreeHost(S->h_stage);
+  for (int b = 0; b < 2; ++b) {
+    cudaFree(S->d_stage[b]);
+    if (S->stage_free[b]) cudaEventDestroy(S->stage_free[b]);
+  }
+  for (void* p : S->pool) cudaFreeHost(p);
+  for (cudaEvent_t e : S->pool_ev) cudaEventDestroy(e);
   if (S->s) cudaStreamDestroy(S->s);
+  if (S->cs) cudaStreamDestroy(S->cs);
   delete S;
 }
 
@@ -568,6 +682,7 @@ extern "C" int gbo_server_create(const gbo_graph* gc, int bfs_slots, int ppr_slo
     return fail(GBO_ERR_UNSUPPORTED, "the server needs a square ROW-layout graph with 32x32 tiles");
   if (bfs_slots < 0 || bfs_slots > 1024 || (ppr_slots != 0 && ppr_slots != kPprSlots))
     return fail(GBO_ERR_INVALID, "bfs_slots in [0,1024]; ppr_slots 0 or 32");
+  if (bfs_slots == 0 && ppr_slots == 0) return fail(GBO_ERR_INVALID, "no slots");
   if (ppr_slots && !g->invdeg) return fail(GBO_ERR_INVALID, "PPR needs out-degrees");
   gbo_server* S = new gbo_server();
   cudaGetDevice(&S->dev);
@@ -586,6 +701,7 @@ extern "C" int gbo_server_create(const gbo_graph* gc, int bfs_slots, int ppr_slo
   };
   try {
     cu(cudaStreamCreateWithFlags(&S->s, cudaStreamNonBlocking), "stream");
+    cu(cudaStreamCreateWithFlags(&S->cs, cudaStreamNonBlocking), "stream");
     const size_t n = (size_t)S->n;
     if (S->kb) {
       cu(cudaMalloc(&S->F, sizeof(uint32_t) * 2 * n * kw + 16), "F");
@@ -595,29 +711,19 @@ extern "C" int gbo_server_create(const gbo_graph* gc, int bfs_slots, int ppr_slo
       cu(cudaMalloc(&S->scratch, sizeof(uint32_t) * (size_t)(g->nslots > 0 ? g->nslots : 1) * 32 * kw), "scratch");
       cu(cudaMalloc(&S->levels, sizeof(int) * n * S->kb + 16), "levels");
       cu(cudaMalloc(&S->ctl, 64), "ctl");
-      cu(cudaHostAlloc(&S->h_ctl, 64, cudaHostAllocDefault), "h_ctl");
       cu(cudaMalloc(&S->slot_any, sizeof(uint32_t) * kw), "slot_any");
       cu(cudaHostAlloc(&S->h_slot_any, sizeof(uint32_t) * kw, cudaHostAllocDefault), "h_slot_any");
       cu(cudaMalloc(&S->d_adm_src, sizeof(int) * S->kb), "adm");
       cu(cudaMalloc(&S->d_adm_slot, sizeof(int) * S->kb), "adm");
-      ms::Args a;
-      a.v = view_of(g);
-      a.F = S->F;
-      a.fstride = n * kw;
-      a.V = S->V;
-      a.fbits = S->fbits;
-      a.vfull = S->vfull;
-      a.levels = S->levels;
-      a.k = S->kb;
-      a.ctl = S->ctl;
-      a.scratch = S->scratch;
-      a.slot_any = S->slot_any;
+      ms::Args a = bfs_args(S);
       unsigned gv = blocks_for((long long)n * S->kb, 256);
       if (gv > (unsigned)num_sms() * 16u) gv = (unsigned)num_sms() * 16u;
       ms::k_init<<<gv, 256, 0, S->s>>>(a, kw, 0x7fffffff);
+      cu(cudaGetLastError(), "init");
     }
     S->bslot_ticket.assign((size_t)S->kb, 0);
     S->bslot_start.assign((size_t)S->kb, 0);
+    S->bslot_finished.assign((size_t)S->kb, 0);
     if (ppr_slots) {
       cu(cudaMalloc(&S->X, sizeof(float) * 2 * n * kPprSlots), "X");
       cu(cudaMemsetAsync(S->X, 0, sizeof(float) * 2 * n * kPprSlots, S->s), "X");
@@ -633,9 +739,23 @@ extern "C" int gbo_server_create(const gbo_graph* gc, int bfs_slots, int ppr_slo
     }
     S->pslot_ticket.assign(ppr_slots ? (size_t)kPprSlots : 0, 0);
     S->pslot_iters.assign((size_t)kPprSlots, 0);
-    S->pslot_submit.assign((size_t)kPprSlots, 0.0);
-    cu(cudaMalloc(&S->d_out, sizeof(int) * n + 16), "out");
-    cu(cudaHostAlloc(&S->h_stage, sizeof(int) * n + 16, cudaHostAllocDefault), "stage");
+    S->pslot_finished.assign((size_t)kPprSlots, 0);
+    for (int b = 0; b < 2; ++b) {
+      cu(cudaMalloc(&S->d_stage[b], sizeof(int) * n * kRetire + 16), "stage");
+      cu(cudaEventCreateWithFlags(&S->stage_free[b], cudaEventDisableTiming), "event");
+      cu(cudaEventRecord(S->stage_free[b], S->cs), "event");
+    }
+    // pinned result buffers: enough for two rounds of retirements
+    const int npool = 2 * kRetire;
+    for (int b = 0; b < npool; ++b) {
+      void* p = nullptr;
+      cudaEvent_t e = nullptr;
+      cu(cudaHostAlloc(&p, sizeof(int) * n + 16, cudaHostAllocDefault), "pinned pool");
+      cu(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+      S->pool.push_back(p);
+      S->pool_ev.push_back(e);
+      S->pool_free.push_back(b);
+    }
     cu(cudaStreamSynchronize(S->s), "sync");
   } catch (int st) {
     destroy_server(S);
@@ -685,20 +805,34 @@ extern "C" int gbo_server_submit_ppr(gbo_server* S, const int* verts, const floa
   return submit(S, std::move(q), ticket);
 }
 
+// Hand a landed result to the caller: copy out of the pinned buffer outside
+// the lock, then give the buffer back to the pool.
+static int take_result(gbo_server* S, std::unique_lock<std::mutex>& lk, int64_t ticket, void* h_out,
+                       double* latency_ms, int* iterations) {
+  auto it = S->results.find(ticket);
+  const Result r = it->second;
+  S->results.erase(it);
+  S->submit_time.erase(ticket);
+  lk.unlock();
+  if (h_out) memcpy(h_out, S->pool[(size_t)r.buf], sizeof(int) * (size_t)S->n);
+  if (latency_ms) *latency_ms = r.t_done - r.t_submit;
+  if (iterations) *iterations = r.iters;
+  lk.lock();
+  S->pool_free.push_back(r.buf);
+  S->cv_work.notify_one();
+  return GBO_OK;
+}
+
 extern "C" int gbo_server_poll(gbo_server* S, int64_t ticket, void* h_out, double* latency_ms,
                                int* iterations) {
   clear_error();
   if (!S) return fail(GBO_ERR_INVALID, "NULL server");
-  std::lock_guard<std::mutex> lk(S->mu);
+  std::unique_lock<std::mutex> lk(S->mu);
   if (S->worker_status != GBO_OK) return fail(S->worker_status, S->worker_error);
+  collect_landed(S);
   auto it = S->results.find(ticket);
-  if (it == S->results.end()) return GBO_ERR_NOTREADY;
-  if (h_out) memcpy(h_out, it->second.data.data(), it->second.data.size());
-  if (latency_ms) *latency_ms = it->second.t_done - it->second.t_submit;
-  if (iterations) *iterations = it->second.iters;
-  S->results.erase(it);
-  S->submit_time.erase(ticket);
-  return GBO_OK;
+  if (it == S->results.end() || !it->second.landed) return GBO_ERR_NOTREADY;
+  return take_result(S, lk, ticket, h_out, latency_ms, iterations);
 }
 
 extern "C" int gbo_server_wait(gbo_server* S, int64_t ticket, void* h_out, double* latency_ms,
@@ -707,17 +841,14 @@ extern "C" int gbo_server_wait(gbo_server* S, int64_t ticket, void* h_out, doubl
   if (!S) return fail(GBO_ERR_INVALID, "NULL server");
   std::unique_lock<std::mutex> lk(S->mu);
   const bool ok = S->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] {
-    return S->worker_status != GBO_OK || S->results.count(ticket) > 0;
+    if (S->worker_status != GBO_OK) return true;
+    collect_landed(S);
+    auto it = S->results.find(ticket);
+    return it != S->results.end() && it->second.landed;
   });
   if (S->worker_status != GBO_OK) return fail(S->worker_status, S->worker_error);
   if (!ok) return fail(GBO_ERR_TIMEOUT, "query not finished within the timeout");
-  auto it = S->results.find(ticket);
-  if (h_out) memcpy(h_out, it->second.data.data(), it->second.data.size());
-  if (latency_ms) *latency_ms = it->second.t_done - it->second.t_submit;
-  if (iterations) *iterations = it->second.iters;
-  S->results.erase(it);
-  S->submit_time.erase(ticket);
-  return GBO_OK;
+  return take_result(S, lk, ticket, h_out, latency_ms, iterations);
 }
 
 extern "C" int gbo_server_get_stats(gbo_server* S, gbo_server_stats* st) {
