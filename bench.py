@@ -38,10 +38,16 @@ def parse():
     ap.add_argument("--scale", type=int, default=SCALE)
     ap.add_argument("--tile", type=int, default=TILE)
     ap.add_argument("--cpu-samples", type=int, default=3, help="BFS runs timed for cpu_baseline")
+    ap.add_argument("--direction", default="auto", choices=["auto", "pull"],
+                    help="auto: top-down steps while the frontier is small (graph is symmetric)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving streams")
     ap.add_argument("--serve-qps", type=float, default=4000.0, help="offered BFS query rate")
     ap.add_argument("--serve-s", type=float, default=1.5, help="seconds of arrivals per stream")
+    ap.add_argument("--workload", default="bfs", choices=["bfs"] + list(SUITE),
+                    help="bfs: the headline line; the others print one line each for the "
+                         "remaining workloads (SSSP/CC/PR on R-MAT 22, TC, MS-BFS, many-graph "
+                         "batch, PPR forward/adjoint, served streams)")
     return ap.parse_args()
 
 
@@ -95,26 +101,29 @@ def traversed_edges(csr, levels):
 
 
 # --------------------------------------------------------------- roofline
-def bfs_level_bytes(rowptr_b, colind_b, levels, nrows, b):
+def bfs_level_bytes(rowptr_b, colind_b, levels, nrows, b, row_live):
     """Algorithmic bytes of each BFS pull step (the words the step must touch).
 
     Step L reads the block-row offsets, the visited and frontier words, the
     block-column index of every tile in a block row that still has an
-    unvisited vertex, and -- only for tiles whose frontier segment is non-empty
-    -- one b-bit row word per unvisited row; it writes the next frontier
-    words, visited words of changed rows and one int32 level per new vertex.
+    unvisited vertex that can be reached (its row of P has an entry), and --
+    only for tiles whose frontier segment is non-empty -- one b-bit row word
+    per such row; it writes the next frontier words, visited words of changed
+    rows and one int32 level per new vertex.
     """
     nbr = len(rowptr_b) - 1
     wb = max(1, b // 8)
     pad = np.full(nbr * b, -2, np.int64)
     pad[:nrows] = levels
     lv = pad.reshape(nbr, b)
+    live = np.zeros(nbr * b, bool)
+    live[:nrows] = row_live
+    live = live.reshape(nbr, b)
     depth = int(levels.max()) + 1
     row_of = np.repeat(np.arange(nbr, dtype=np.int64), np.diff(rowptr_b))
     out = []
     for L in range(depth):
-        visited = (lv >= 0) & (lv <= L)
-        unvis = ((lv == -1) | (lv > L)).sum(axis=1)  # real unvisited rows
+        unvis = (((lv == -1) | (lv > L)) & live).sum(axis=1)  # reachable unvisited rows
         front_nz = (lv == L).any(axis=1)
         open_row = unvis > 0
         t_open = open_row[row_of]
@@ -125,7 +134,6 @@ def bfs_level_bytes(rowptr_b, colind_b, levels, nrows, b):
         by += 4 * int(t_open.sum())
         by += wb * int(unvis[row_of[t_need]].sum())
         out.append(by)
-        del visited
     return out
 
 
@@ -298,7 +306,7 @@ def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed):
             if item is None:
                 return
             kind, ticket = item
-            _, ms, _ = srv.wait(ticket, kind, timeout=600.0)
+            _, ms, _ = srv.wait(ticket, kind, timeout=120.0)
             with lock:
                 lat[kind].append(ms)
 
@@ -329,7 +337,9 @@ def run_ours(args, ws, rank, local):
     dist = Dist(ws)
     csr = gbo.gen_rmat(args.scale, EDGE_FACTOR, seed=SEED, **RMAT)
     t0 = time.perf_counter()
-    g = gbo.Graph.from_csr(csr, args.tile)
+    # the symmetrised R-MAT graph may take top-down steps on small frontiers
+    flags = gbo.FLAG_SYMMETRIC if args.direction == "auto" else 0
+    g = gbo.Graph.from_csr(csr, args.tile, flags)
     build_s = time.perf_counter() - t0
     info = g.info()
     n = csr.nrows
@@ -374,14 +384,28 @@ def run_ours(args, ws, rank, local):
     e2e_ms = dist.max(ev0.elapsed_ms(ev1) / args.steps)
 
     # roofline of the BFS pull kernel: algorithmic bytes per level / its
-    # event-timed duration inside the timed runs
+    # event-timed duration, from pull-only runs of the same BFS (every level
+    # a bottom-up step, so each level's bytes are known exactly)
+    g.set_bfs_direction(False)
+    for _ in range(2):
+        g.bfs(0, out=d_level)
+    auto_step_ms, step_ms_all = step_ms_all, []
+    ev0.record()
+    for _ in range(args.steps):
+        g.bfs(0, out=d_level)
+        step_ms_all.extend(g.last_run()["step_ms"])
+    ev1.record()
+    gbo.sync()
+    pull_ms = ev0.elapsed_ms(ev1) / args.steps
+    if args.direction == "auto":
+        g.set_bfs_direction(True)
     rp, ci, _ = None, None, None
     r = C_void()
     c = C_void()
     gbo.check(gbo.lib().gbo_graph_b2sr(g.h, r.ref(), c.ref(), None), "graph_b2sr")
     rowptr_b = gbo.device_to_numpy(r.value, np.int32, info.nblockrows + 1)
     colind_b = gbo.device_to_numpy(c.value, np.int32, int(info.nblocks))
-    lvl_bytes = bfs_level_bytes(rowptr_b, colind_b, levels, n, args.tile)
+    lvl_bytes = bfs_level_bytes(rowptr_b, colind_b, levels, n, args.tile, np.diff(csr.rowptr) > 0)
     per_level_ms = np.array(step_ms_all, np.float64).reshape(args.steps, -1)
     lvl_ms = per_level_ms.mean(axis=0)
     k = min(len(lvl_bytes), len(lvl_ms))
@@ -462,8 +486,11 @@ def run_ours(args, ws, rank, local):
                       "algorithmic_bytes": bmv_bytes, "gteps": csr.nnz / (bmv_ms / 1e3) / 1e9},
         "batched_bfs": dict(batched, plain_qps=1e3 / ms),
         "served": served,
-        "levels_ms": [float(v) for v in lvl_ms[:k]],
-        "levels_gb": [b / 1e9 for b in lvl_bytes[:k]],
+        "direction": args.direction,
+        "levels_ms": [float(v) for v in np.array(auto_step_ms).reshape(args.steps, -1).mean(axis=0)],
+        "pull_only": {"ms_per_bfs": pull_ms, "gteps": edges / (pull_ms / 1e3) / 1e9,
+                      "levels_ms": [float(v) for v in lvl_ms[:k]],
+                      "levels_gb": [b / 1e9 for b in lvl_bytes[:k]]},
         "graph_build_s": build_s,
     }
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -512,11 +539,327 @@ class C_pinned:
             pass
 
 
+# ----------------------------------------------------------------- suite
+# One JSON line per workload, same keys as the headline where they apply.
+# Device time by CUDA events around the public C-ABI calls (outputs in
+# preallocated device buffers; each call ends with its host-visible result
+# such as the iteration count, as a user sees it).  CPU figures are the
+# oracle's OpenMP restatement on one bounded sample.
+
+
+def _timed(gbo, fn, steps, warmup):
+    for _ in range(warmup):
+        fn()
+    gbo.sync()
+    e0, e1 = gbo.Event(), gbo.Event()
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    gbo.sync()
+    return e0.elapsed_ms(e1) / steps
+
+
+def _cpu(fn, samples=1):
+    ts = []
+    for _ in range(samples):
+        t0 = time.perf_counter()
+        fn()
+        ts.append(time.perf_counter() - t0)
+    return float(np.median(ts))
+
+
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    return oracle
+
+
+def _line(metric, value, unit, hib, ms, args, config, **extra):
+    d = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": hib, "scaling": "weak",
+         "vs_baseline": None, "data": "synthetic", "config": config}
+    d.update(extra)
+    print(json.dumps(d), flush=True)
+
+
+def _bmv_bytes(info, b, n, vec_bytes):
+    wb = max(1, b // 8)
+    return info.nblocks * (b * wb + 4) + 4 * (info.nblockrows + 1) + vec_bytes
+
+
+def suite_config2(args, which):
+    """SSSP, CC and PageRank (20 iterations) on the headline R-MAT 22 graph."""
+    import ctypes as C
+
+    import gbo
+
+    orc = _oracle()
+    csr = gbo.gen_rmat(args.scale, EDGE_FACTOR, seed=SEED, **RMAT)
+    g = gbo.Graph.from_csr(csr, args.tile)
+    info = g.info()
+    n = csr.nrows
+    lv, depth = g.bfs(0)
+    edges = traversed_edges(csr, lv)
+    cfg = {"workload": "", "scale": args.scale, "tile_bits": args.tile, "nvertices": n,
+           "nnz": csr.nnz, "nblocks": int(info.nblocks),
+           "l2": "inputs larger than L2 (B2SR tiles far above 126 MB)"}
+    buf = gbo.DeviceBuffer(4 * n)
+    it = C.c_int(0)
+    peak, psrc = load_peaks()
+    bs = orc.pack(csr.rowptr, csr.colind, n, n, args.tile) if not args.no_cpu else None
+    if which == "sssp":
+        ms = _timed(gbo, lambda: gbo.check(gbo.lib().gbo_sssp_unit(g.h, 0, buf.ptr, C.byref(it), None)),
+                    args.steps, args.warmup)
+        cfg["workload"] = f"unit-weight SSSP from vertex 0 (min-plus BMV), R-MAT scale {args.scale}"
+        extra = {"iterations": it.value, "traversed_edges": edges, "dtype": "u32"}
+        if bs is not None:
+            t = _cpu(lambda: orc.sssp_b2sr(bs, 0))
+            extra["cpu_baseline"] = {"value": edges / t / 1e9, "unit": "GTEPS", "cores": orc.max_threads(),
+                                     "kind": "port", "sample": "1 SSSP from vertex 0 (sssp.cu:420-470 port)"}
+        _line("GTEPS", edges / (ms / 1e3) / 1e9, "GTEPS", True, ms, args, cfg, **extra)
+    elif which == "cc":
+        ms = _timed(gbo, lambda: gbo.check(gbo.lib().gbo_cc(g.h, buf.ptr, C.byref(it), None)),
+                    args.steps, args.warmup)
+        und = csr.nnz // 2
+        cfg["workload"] = f"connected components (FastSV, min label), R-MAT scale {args.scale}"
+        extra = {"iterations": it.value, "undirected_edges": und, "dtype": "i32"}
+        if bs is not None:
+            t = _cpu(lambda: orc.cc(csr.rowptr, csr.colind, n))
+            extra["cpu_baseline"] = {"value": und / t / 1e9, "unit": "GTEPS", "cores": orc.max_threads(),
+                                     "kind": "port", "sample": "1 CC run (label propagation, min id)"}
+        _line("GTEPS", und / (ms / 1e3) / 1e9, "GTEPS", True, ms, args, cfg, **extra)
+    else:
+        iters = 20
+        ms = _timed(gbo, lambda: gbo.check(gbo.lib().gbo_pagerank(g.h, C.c_float(0.85), iters, C.c_float(-1.0),
+                                                                   buf.ptr, C.byref(it), None)),
+                    args.steps, args.warmup)
+        st = g.last_run()
+        step = float(np.mean(st["step_ms"])) if st["step_ms"] else ms / iters
+        by = _bmv_bytes(info, args.tile, n, 4 * n * 3)  # p read, D^-1 read, p' write
+        cfg["workload"] = f"PageRank alpha 0.85, 20 iterations, fp32 values / fp64 sums, R-MAT scale {args.scale}"
+        extra = {"iterations": it.value, "dtype": "f32",
+                 "roofline": {"bound": "hbm", "achieved": by / (step / 1e3) / 1e9, "peak": peak,
+                              "unit": "GB/s", "frac": by / (step / 1e3) / 1e9 / peak, "traffic": None,
+                              "kernel": "PageRank iteration (semiring BMV + update)", "peak_source": psrc,
+                              "algorithmic_bytes_per_launch": by, "ms_per_launch": step}}
+        if bs is not None:
+            outdeg = np.bincount(csr.colind, minlength=n).astype(np.int32)
+            t = _cpu(lambda: orc.pagerank_b2sr_f32(bs, outdeg, 0.85, iters, -1.0))
+            extra["cpu_baseline"] = {"value": iters * csr.nnz / t / 1e9, "unit": "GTEPS",
+                                     "cores": orc.max_threads(), "kind": "port",
+                                     "sample": "20 PageRank iterations (pr.cu:449-513 port)"}
+        _line("GTEPS", iters * csr.nnz / (ms / 1e3) / 1e9, "GTEPS", True, ms, args, cfg, **extra)
+    g.free()
+
+
+def suite_tc(args):
+    """Triangle counting: king mesh 4096^2 and R-MAT 20 (seed 1), every tile
+    width timed and the fastest kept (the autotuned choice)."""
+    import gbo
+
+    orc = _oracle()
+    for name, csr, known in (("king mesh 4096x4096", gbo.gen_king_mesh(4096), 4 * 4095 ** 2),
+                             ("R-MAT scale 20 ef16 seed 1", gbo.gen_rmat(20, 16, seed=1, **RMAT), None)):
+        table = {}
+        count = None
+        for b in (8, 16, 32, 64):
+            g = gbo.Graph.from_csr(csr, b, gbo.FLAG_LOWER)
+            count = g.tc()
+            if known is not None and count != known:
+                raise SystemExit(f"TC mismatch on {name}: {count} != {known}")
+            table[b] = _timed(gbo, g.tc, args.steps, args.warmup)
+            nblk = int(g.info().nblocks)
+            g.free()
+            table[b] = {"ms": table[b], "nblocks_L": nblk}
+        best = min(table, key=lambda k: table[k]["ms"])
+        model_best, _ = gbo.tune_tile_width(csr, gbo.TUNE_TC, gbo.TUNE_MODEL)
+        ms = table[best]["ms"]
+        lower_edges = (csr.nnz + 0) // 2
+        extra = {"triangles": count, "tile_table": table, "best_tile": best, "model_tile": model_best,
+                 "dtype": "u64"}
+        if not args.no_cpu:
+            t = _cpu(lambda: orc.tc_csr(csr.rowptr, csr.colind, csr.nrows))
+            extra["cpu_baseline"] = {"value": lower_edges / t / 1e9, "unit": "G lower edges/s",
+                                     "cores": orc.max_threads(), "kind": "port",
+                                     "sample": "1 full count (sorted-adjacency intersection on L)"}
+        _line("G lower edges/s", lower_edges / (ms / 1e3) / 1e9, "G lower edges/s", True, ms, args,
+              {"workload": f"triangle count (masked B2SR SpGEMM on L), {name}", "nvertices": csr.nrows,
+               "nnz": csr.nnz}, **extra)
+
+
+def _ms_edges(gbo, out, deg, n, k, rows=65536):
+    """Traversed undirected edges summed over the k columns of an (n, k)
+    int32 level matrix on the device, read back in row chunks."""
+    tot = np.zeros(k, np.float64)
+    degf = deg.astype(np.float64)
+    for r0 in range(0, n, rows):
+        m = min(rows, n - r0)
+        chunk = np.empty((m, k), np.int32)
+        gbo.check(gbo.lib().gbo_memcpy_d2h(chunk.ctypes.data, out.ptr + 4 * r0 * k, chunk.nbytes, None), "d2h")
+        gbo.check(gbo.lib().gbo_stream_sync(None), "sync")
+        tot += degf[r0:r0 + m] @ (chunk >= 0)
+    return int(tot.sum()) // 2
+
+
+def suite_msbfs(args):
+    """Multi-source BFS on R-MAT 21 (seed 2), k = 64/256/1024 sources (seed 3),
+    queries per second against one plain BFS per source."""
+    import gbo
+
+    csr = gbo.gen_rmat(21, 16, seed=2, **RMAT)
+    g = gbo.Graph.from_csr(csr, 32, gbo.FLAG_SYMMETRIC)
+    n = csr.nrows
+    rng = np.random.default_rng(3)
+    d_level = gbo.DeviceBuffer(4 * n)
+    srcs_plain = rng.integers(0, n, 16).astype(np.int32)
+    plain_ms = np.mean([_timed(gbo, lambda s=int(s): g.bfs(s, out=d_level), 1, 1) for s in srcs_plain])
+    res = {}
+    deg = np.diff(csr.rowptr).astype(np.int64)
+    for k in (64, 256, 1024):
+        srcs = rng.integers(0, n, k).astype(np.int32)
+        out = gbo.DeviceBuffer(4 * n * k)
+        ms = _timed(gbo, lambda: g.msbfs(srcs, out=out), max(1, args.steps // 2), args.warmup)
+        edges = _ms_edges(gbo, out, deg, n, k)
+        res[k] = {"ms": ms, "qps": k / (ms / 1e3), "gteps_x_k": edges / (ms / 1e3) / 1e9,
+                  "speedup_vs_plain": (k / (ms / 1e3)) / (1e3 / plain_ms)}
+        del out
+    best = res[1024]
+    _line("qps", best["qps"], "queries/s", True, best["ms"], args,
+          {"workload": "multi-source BFS, R-MAT scale 21 ef16 seed 2, k random sources (seed 3), B2SR 32",
+           "nvertices": n, "nnz": csr.nnz},
+          dtype="u32", by_k=res, plain_qps=1e3 / plain_ms)
+    g.free()
+
+
+def suite_batch(args):
+    """10,000 ER graphs (n log-uniform in [32, 65536], average degree 8,
+    seeds 1000+i) as one block-diagonal B2SR: one multi-seed BFS (vertex 0 of
+    every graph) against one BFS per graph on its own handle."""
+    import gbo
+
+    count = 10000
+    t0 = time.perf_counter()
+    csr, off = gbo.gen_er_batch(count, 32, 65536, 8.0, 1000)
+    gen_s = time.perf_counter() - t0
+    b, tune_cost = gbo.tune_tile_width(csr, gbo.TUNE_BFS, gbo.TUNE_MODEL)  # bytes model
+    g = gbo.Graph.from_csr(csr, b, gbo.FLAG_SYMMETRIC)
+    n = csr.nrows
+    seeds = off[:-1].astype(np.int32)
+    d_level = gbo.DeviceBuffer(4 * n)
+    ms = _timed(gbo, lambda: g.bfs_multi(seeds, out=d_level), args.steps, args.warmup)
+    info = g.info()
+    g.free()
+    # one graph per handle and per BFS call, on a sample of 100 graphs
+    rp = csr.rowptr
+    ci = csr.colind
+    per = []
+    rng = np.random.default_rng(7)
+    for i in rng.choice(count, 100, replace=False):
+        lo, hi = int(off[i]), int(off[i + 1])
+        sub_rp = (rp[lo:hi + 1] - rp[lo]).astype(np.int32)
+        sub_ci = (ci[rp[lo]:rp[hi]] - lo).astype(np.int32)
+        sub = gbo.Csr(sub_rp, sub_ci, hi - lo, hi - lo)
+        gs = gbo.Graph.from_csr(sub, b)
+        buf = gbo.DeviceBuffer(4 * (hi - lo))
+        per.append(_timed(gbo, lambda: gs.bfs(0, out=buf), 3, 1))
+        gs.free()
+    one_ms = float(np.mean(per))
+    _line("graphs/s", count / (ms / 1e3), "graphs/s", True, ms, args,
+          {"workload": "BFS from vertex 0 of each of 10000 ER graphs (n log-uniform 32..65536, avg degree 8, "
+                       "seeds 1000+i) packed block-diagonally as one B2SR graph, tile width from the tuner",
+           "tile_bits": b, "tuner_bytes": {k: (v if np.isfinite(v) else None) for k, v in tune_cost.items()},
+           "nvertices": n, "nnz": csr.nnz, "nblocks": int(info.nblocks), "generate_s": gen_s},
+          dtype="bits", one_by_one_graphs_per_s=1e3 / one_ms, speedup=(count / (ms / 1e3)) / (1e3 / one_ms))
+
+
+def suite_ppr(args):
+    """PPR forward and adjoint on R-MAT 20: v Dirichlet over a random 1 % of
+    vertices (seed 4), w ~ N(0,1) (seed 5), alpha 0.85, tol 1e-7; gradient
+    checked by central differences along 64 random directions."""
+    import ctypes as C
+
+    import gbo
+
+    csr = gbo.gen_rmat(20, 16, seed=1, **RMAT)
+    n = csr.nrows
+    g = gbo.Graph.from_csr(csr, 32)
+    rng = np.random.default_rng(4)
+    idx = rng.choice(n, n // 100, replace=False)
+    v = np.zeros(n)
+    v[idx] = rng.dirichlet(np.ones(len(idx)))
+    w = np.random.default_rng(5).standard_normal(n)
+    dv = gbo.DeviceBuffer.from_numpy(v.astype(np.float32))
+    dw = gbo.DeviceBuffer.from_numpy(w.astype(np.float32))
+    dp = gbo.DeviceBuffer(4 * n)
+    dg = gbo.DeviceBuffer(4 * n)
+    it_f, it_b = C.c_int(0), C.c_int(0)
+    fwd = _timed(gbo, lambda: gbo.check(gbo.lib().gbo_ppr_forward(g.h, dv.ptr, C.c_float(0.85), C.c_float(1e-7),
+                                                                   1000, dp.ptr, C.byref(it_f), None)),
+                 args.steps, args.warmup)
+    bwd = _timed(gbo, lambda: gbo.check(gbo.lib().gbo_ppr_backward(g.h, dw.ptr, C.c_float(0.85), C.c_float(1e-7),
+                                                                    1000, dg.ptr, C.byref(it_b), None)),
+                 args.steps, args.warmup)
+    grad = dg.to_numpy(np.float32, n).astype(np.float64)
+    errs = []
+    for _ in range(64):
+        d = np.zeros(n)
+        d[idx] = rng.standard_normal(len(idx))
+        pp, _ = g.ppr_forward((v + 1e-3 * d).astype(np.float32), 0.85, 1e-9, 2000)
+        pm, _ = g.ppr_forward((v - 1e-3 * d).astype(np.float32), 0.85, 1e-9, 2000)
+        fd = (w @ pp.astype(np.float64) - w @ pm.astype(np.float64)) / 2e-3
+        errs.append(abs(fd - grad @ d) / max(1.0, abs(fd)))
+    _line("ms", fwd + bwd, "ms per forward+adjoint", False, fwd + bwd, args,
+          {"workload": "PPR forward + adjoint, R-MAT scale 20 seed 1, v on 1% of vertices, alpha 0.85, tol 1e-7",
+           "nvertices": n, "nnz": csr.nnz},
+          dtype="f32", forward_ms=fwd, forward_iters=it_f.value, backward_ms=bwd, backward_iters=it_b.value,
+          fd_directions=64, fd_max_rel_err=float(max(errs)))
+    g.free()
+
+
+def suite_serve(args):
+    """Poisson arrivals at 1k, 10k and 100k queries/s into the continuous
+    batching server (R-MAT 21 seed 2, B2SR 32): 90 % BFS sources, 10 % PPR
+    sets of 1-64 vertices; achieved rate and p50/p99 latency."""
+    import gbo
+
+    csr = gbo.gen_rmat(21, 16, seed=2, **RMAT)
+    g = gbo.Graph.from_csr(csr, 32)
+    out = {}
+    for rate in (1000.0, 10000.0, 100000.0):
+        out[int(rate)] = serve_stream(gbo, g, csr.nrows, rate, min(args.serve_s, 2e4 / rate), 0.1, 11)
+    top = out[10000]
+    _line("qps", top["achieved_qps"], "queries/s", True, 1e3 / max(top["achieved_qps"], 1e-9), args,
+          {"workload": "served BFS + PPR queries, Poisson arrivals, R-MAT scale 21 seed 2, B2SR 32",
+           "nvertices": csr.nrows, "nnz": csr.nnz}, dtype="u32", by_rate=out)
+    g.free()
+
+
+SUITE = {
+    "sssp": lambda a: suite_config2(a, "sssp"),
+    "cc": lambda a: suite_config2(a, "cc"),
+    "pr": lambda a: suite_config2(a, "pr"),
+    "tc": suite_tc,
+    "msbfs": suite_msbfs,
+    "batch": suite_batch,
+    "ppr": suite_ppr,
+    "serve": suite_serve,
+}
+
+
 def main():
     args = parse()
     ws, rank, local = dist_env()
     if args.impl == "reference":
         run_reference(args, ws, rank)
+        return
+    if args.workload != "bfs":
+        import gbo
+
+        gbo.check(gbo.lib().gbo_set_device(local), "set_device")
+        if rank == 0:
+            SUITE[args.workload](args)
         return
     run_ours(args, ws, rank, local)
 

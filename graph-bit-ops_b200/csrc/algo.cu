@@ -33,6 +33,8 @@ struct Ctrl {
   float add_scale;  // PPR: add_scale * v[i] added as well
   int norm;       // 1 = L1, 2 = L2 error
   int n;
+  int mode;       // BFS: 0 = pull (bottom-up) step, 1 = push (top-down) step
+  int push_thr;   // BFS: push while the frontier has fewer vertices (0 = never)
 };
 
 }  // namespace gbo
@@ -45,6 +47,7 @@ struct AlgoState {
   // BFS / SSSP
   void* front = nullptr;   // 2 * nbr words (8 bytes each max)
   void* visited = nullptr; // nbr words
+  void* live = nullptr;    // nbr words: bit set where the row of P has an entry
   int* level = nullptr;    // n
   uint32_t* dist = nullptr;
   // PR / PPR / CC vectors
@@ -176,7 +179,7 @@ __global__ void __launch_bounds__(kTPB) k_bfs_step(GView v, typename Word<B>::T*
                                                    typename Word<B>::T* __restrict__ scratch) {
   using WT = typename Word<B>::T;
   using L = Lay<B>;
-  if (((volatile Ctrl*)ctrl)->done) return;
+  if (((volatile Ctrl*)ctrl)->done || ((volatile Ctrl*)ctrl)->mode) return;
   const int lvl = ((volatile Ctrl*)ctrl)->iter;
   const WT* __restrict__ x = front + (size_t)(lvl & 1) * v.nbr;
   WT* __restrict__ out = front + (size_t)((lvl + 1) & 1) * v.nbr;
@@ -214,6 +217,87 @@ __global__ void __launch_bounds__(kTPB) k_bfs_step(GView v, typename Word<B>::T*
   block_add_u64(cnt, &ctrl->count);
 }
 
+// OR `val` into word idx of a b-bit word array with a 32- or 64-bit atomic
+// (words narrower than 32 bits are OR-ed inside their enclosing 32-bit word;
+// the other bytes receive zero bits and do not change).
+template <int B>
+__device__ __forceinline__ void atomic_or_word(typename Word<B>::T* base, long long idx,
+                                               typename Word<B>::T val) {
+  if (B == 64) {
+    atomicOr(reinterpret_cast<unsigned long long*>(base) + idx, (unsigned long long)val);
+  } else if (B == 32) {
+    atomicOr(reinterpret_cast<unsigned*>(base) + idx, (unsigned)val);
+  } else {
+    const uintptr_t p = reinterpret_cast<uintptr_t>(base) + (uintptr_t)idx * sizeof(typename Word<B>::T);
+    unsigned* w = reinterpret_cast<unsigned*>(p & ~(uintptr_t)3);
+    atomicOr(w, (unsigned)val << ((p & 3) * 8));
+  }
+}
+
+// Rows of P with at least one entry (bit b-1-r of word R for row R*b+r).
+// A row without entries can never be reached, so BFS and SSSP start with it
+// marked visited: block rows whose other rows are done are then skipped
+// instead of being scanned to the end for a parent that does not exist.
+template <int B>
+__global__ void __launch_bounds__(kTPB) k_live(GView v, typename Word<B>::T* __restrict__ live) {
+  using WT = typename Word<B>::T;
+  using L = Lay<B>;
+  const unsigned lane = threadIdx.x & 31;
+  const long long item = item_index(lane, L::W, L::G);
+  const bool active = item < v.nitems;
+  const int r = lane % L::W;
+  const gbo_item it = active ? v.items[item] : gbo_item{0, 0, 0, -2};
+  const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
+  WT a0 = 0, a1 = 0;
+  for (int t = it.t0; t < it.t1; ++t) {
+    a0 = (WT)(a0 | val[(size_t)t * B + r]);
+    if (L::RPL == 2) a1 = (WT)(a1 | val[(size_t)t * B + 32 + r]);
+  }
+  const WT word = gather_bits<B>(a0 != 0, a1 != 0, lane);
+  if (active && r == 0 && word) atomic_or_word<B>(live, it.row, word);
+}
+
+// Next-frontier words start empty in a push step.
+template <int B>
+__global__ void k_bfs_push_clear(typename Word<B>::T* __restrict__ front, int nbr, Ctrl* __restrict__ ctrl) {
+  if (((volatile Ctrl*)ctrl)->done || !((volatile Ctrl*)ctrl)->mode) return;
+  const int lvl = ((volatile Ctrl*)ctrl)->iter;
+  typename Word<B>::T* out = front + (size_t)((lvl + 1) & 1) * nbr;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nbr;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = 0;
+}
+
+// Top-down (push) step for symmetric P, used while the frontier is small:
+// for every frontier row r of block row J and every tile (J, C), the row
+// word (the neighbours of vertex J*b+r in block C) is OR-ed into the next
+// frontier, minus vertices already visited.  One warp per work item, one
+// lane per tile; k_bfs_finish then keeps the unvisited bits.
+template <int B>
+__global__ void __launch_bounds__(kTPB) k_bfs_push(GView v, typename Word<B>::T* __restrict__ front,
+                                                   const typename Word<B>::T* __restrict__ visited,
+                                                   Ctrl* __restrict__ ctrl) {
+  using WT = typename Word<B>::T;
+  if (((volatile Ctrl*)ctrl)->done || !((volatile Ctrl*)ctrl)->mode) return;
+  const int lvl = ((volatile Ctrl*)ctrl)->iter;
+  const WT* __restrict__ x = front + (size_t)(lvl & 1) * v.nbr;
+  WT* out = front + (size_t)((lvl + 1) & 1) * v.nbr;
+  const unsigned lane = threadIdx.x & 31;
+  const long long item = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (item >= v.nitems) return;
+  const gbo_item it = v.items[item];
+  const WT xs = x[it.row];
+  if (!xs) return;
+  const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
+  for (int t = it.t0 + (int)lane; t < it.t1; t += 32) {
+    const int C = v.colind[t];
+    WT acc = 0;
+    for_each_col<B>(xs, [&](int r) { acc = (WT)(acc | val[(size_t)t * B + r]); });
+    const WT cand = (WT)(acc & ~visited[C]);
+    if (cand) atomic_or_word<B>(out, C, cand);
+  }
+}
+
 template <int B>
 __global__ void k_bfs_finish(GView v, typename Word<B>::T* __restrict__ front,
                              typename Word<B>::T* __restrict__ visited, int* __restrict__ level,
@@ -221,10 +305,27 @@ __global__ void k_bfs_finish(GView v, typename Word<B>::T* __restrict__ front,
   using WT = typename Word<B>::T;
   if (((volatile Ctrl*)ctrl)->done) return;
   const int lvl = ((volatile Ctrl*)ctrl)->iter;
+  const int push = ((volatile Ctrl*)ctrl)->mode;
   WT* __restrict__ out = front + (size_t)((lvl + 1) & 1) * v.nbr;
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long cnt = 0;
-  if (i < v.nsplit) {
+  if (push) {
+    // keep the unvisited bits of every next-frontier word
+    if (i < v.nbr) {
+      const WT full = full_word<B>();
+      const WT vis = visited[i];
+      const WT nw = (WT)(out[i] & ~vis & full);
+      out[i] = nw;
+      if (nw) {
+        visited[i] = (WT)(vis | nw);
+        for (int r = 0; r < B; ++r) {
+          const long long row = i * B + r;
+          if (bit_of<B>(nw, r) && row < v.nrows) level[row] = lvl + 1;
+        }
+        cnt = popc_w(nw);
+      }
+    }
+  } else if (i < v.nsplit) {
     const gbo_split sp = v.splits[i];
     const WT full = full_word<B>();
     const WT vis = visited[sp.row];
@@ -244,7 +345,10 @@ __global__ void k_bfs_finish(GView v, typename Word<B>::T* __restrict__ front,
   }
   block_add_u64(cnt, &ctrl->count);
   close_iteration(ctrl, [](volatile Ctrl* c, int it) {
-    return c->count == 0ull || it >= c->max_iter;
+    // direction of the next level: push while the new frontier is small
+    const unsigned long long nf = c->count;
+    c->mode = (c->push_thr > 0 && nf > 0ull && nf < (unsigned long long)c->push_thr) ? 1 : 0;
+    return nf == 0ull || it >= c->max_iter;
   });
 }
 
@@ -265,7 +369,8 @@ __global__ void k_bfs_seed(const int* __restrict__ seeds, int nseeds, typename W
 
 template <int B>
 __global__ void k_bfs_init(typename Word<B>::T* front, typename Word<B>::T* visited, int* level,
-                           int nbr, int n, int src, Ctrl* ctrl, int max_iter) {
+                           const typename Word<B>::T* __restrict__ live, int nbr, int n, int src,
+                           Ctrl* ctrl, int max_iter, int push_thr, int mode0) {
   using WT = typename Word<B>::T;
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -274,7 +379,7 @@ __global__ void k_bfs_init(typename Word<B>::T* front, typename Word<B>::T* visi
     WT w = (src >= 0 && k == src / B) ? (WT)((WT)1 << (B - 1 - src % B)) : (WT)0;
     front[k] = w;
     front[nbr + k] = 0;
-    visited[k] = w;
+    visited[k] = (WT)(w | (~live[k] & full_word<B>()));
   }
   if (i == 0) {
     ctrl->iter = 0;
@@ -284,6 +389,8 @@ __global__ void k_bfs_init(typename Word<B>::T* front, typename Word<B>::T* visi
     ctrl->count = 0;
     ctrl->err = 0;
     ctrl->last_err = 0;
+    ctrl->push_thr = push_thr;
+    ctrl->mode = mode0;
   }
 }
 
@@ -415,7 +522,8 @@ __global__ void k_sssp_finish(GView v, typename Word<B>::T* __restrict__ front,
 
 template <int B>
 __global__ void k_sssp_init(typename Word<B>::T* front, typename Word<B>::T* visited,
-                            uint32_t* dist, int nbr, int n, int src, Ctrl* ctrl, int max_iter) {
+                            const typename Word<B>::T* __restrict__ live, uint32_t* dist, int nbr,
+                            int n, int src, Ctrl* ctrl, int max_iter) {
   using WT = typename Word<B>::T;
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -424,7 +532,7 @@ __global__ void k_sssp_init(typename Word<B>::T* front, typename Word<B>::T* vis
     WT w = (k == src / B) ? (WT)((WT)1 << (B - 1 - src % B)) : (WT)0;
     front[k] = w;
     front[nbr + k] = 0;
-    visited[k] = w;
+    visited[k] = (WT)(w | (~live[k] & full_word<B>()));
   }
   if (i == 0) {
     ctrl->iter = 0;
@@ -747,12 +855,26 @@ int get_state(gbo_graph* g, AlgoState** out) {
   return GBO_OK;
 }
 
-int ensure_frontier(gbo_graph* g, AlgoState* a) {
+int ensure_frontier(gbo_graph* g, AlgoState* a, cudaStream_t s) {
   if (!a->front) {
     const size_t wb = 8;  // widest word
     GBO_CUDA_TRY(cudaMalloc(&a->front, wb * 2 * (size_t)(g->nbr + 1)));
     GBO_CUDA_TRY(cudaMalloc(&a->visited, wb * (size_t)(g->nbr + 1)));
-    g->device_bytes += (long long)(wb * 3 * (g->nbr + 1));
+    GBO_CUDA_TRY(cudaMalloc(&a->live, wb * (size_t)(g->nbr + 1)));
+    g->device_bytes += (long long)(wb * 4 * (g->nbr + 1));
+    GBO_CUDA_TRY(cudaMemsetAsync(a->live, 0, wb * (size_t)(g->nbr + 1), s));
+    if (g->nitems > 0) {
+      const GView v = view_of(g);
+      const unsigned grid = grid_for_items(g->nitems, g->b);
+      switch (g->b) {
+        case 4: k_live<4><<<grid, kTPB, 0, s>>>(v, (Word<4>::T*)a->live); break;
+        case 8: k_live<8><<<grid, kTPB, 0, s>>>(v, (Word<8>::T*)a->live); break;
+        case 16: k_live<16><<<grid, kTPB, 0, s>>>(v, (Word<16>::T*)a->live); break;
+        case 32: k_live<32><<<grid, kTPB, 0, s>>>(v, (Word<32>::T*)a->live); break;
+        default: k_live<64><<<grid, kTPB, 0, s>>>(v, (Word<64>::T*)a->live); break;
+      }
+      GBO_CUDA_TRY(cudaGetLastError());
+    }
   }
   return GBO_OK;
 }
@@ -848,7 +970,7 @@ int bfs_impl(gbo_graph* g, int src, const int* h_seeds, int nseeds, int32_t* d_l
   using WT = typename Word<B>::T;
   AlgoState* a = nullptr;
   GBO_TRY(get_state(g, &a));
-  GBO_TRY(ensure_frontier(g, a));
+  GBO_TRY(ensure_frontier(g, a, s));
   GBO_TRY(ensure_vec_i32(g, &a->level));
   GView v = view_of(g);
   WT* front = (WT*)a->front;
@@ -857,20 +979,30 @@ int bfs_impl(gbo_graph* g, int src, const int* h_seeds, int nseeds, int32_t* d_l
   int* level = a->level;
   WT* scratch = (WT*)a->scratch;
   const unsigned gi = grid_for_items(g->nitems, B);
-  const unsigned gs = blocks_for(g->nsplit, kTPB);
+  // push steps (symmetric graphs) finalise every block row in k_bfs_finish
+  const bool push_ok = g->symmetric;
+  const unsigned gs = blocks_for(std::max<long long>(g->nsplit, push_ok ? g->nbr : 0), kTPB);
+  const unsigned gp = blocks_for_warps(g->nitems, kTPB / 32);
+  const unsigned gc = grid_vertex(g->nbr);
   GBO_TRY(get_exec(a, A_BFS, nullptr, [&](cudaStream_t cs, int k, int* nl) -> int {
     StepTimer tm{a, cs, k};
     tm.begin();
+    if (push_ok) k_bfs_push_clear<B><<<gc, kTPB, 0, cs>>>(front, g->nbr, ctrl);
     if (g->nitems > 0) k_bfs_step<B><<<gi, kTPB, 0, cs>>>(v, front, vis, level, ctrl, scratch);
+    if (push_ok && g->nitems > 0) k_bfs_push<B><<<gp, kTPB, 0, cs>>>(v, front, vis, ctrl);
     tm.end();
     k_bfs_finish<B><<<gs, kTPB, 0, cs>>>(v, front, vis, level, ctrl, scratch);
-    *nl += (g->nitems > 0) + 1;
+    *nl += (g->nitems > 0) + 1 + (push_ok ? 1 + (g->nitems > 0) : 0);
     GBO_CUDA_TRY(cudaGetLastError());
     return GBO_OK;
   }));
   const int max_iter = g->nrows + 1;
-  k_bfs_init<B><<<grid_vertex(std::max(g->nrows, g->nbr)), kTPB, 0, s>>>(front, vis, level, g->nbr,
-                                                                       g->nrows, src, ctrl, max_iter);
+  // push while the frontier holds fewer than n/64 vertices (symmetric only)
+  const int push_thr = !push_ok ? 0 : g->bfs_push_thr >= 0 ? g->bfs_push_thr : std::max(1, g->nrows / 64);
+  const int nstart = src >= 0 ? 1 : nseeds;
+  k_bfs_init<B><<<grid_vertex(std::max(g->nrows, g->nbr)), kTPB, 0, s>>>(
+      front, vis, level, (const WT*)a->live, g->nbr, g->nrows, src, ctrl, max_iter, push_thr,
+      push_ok && nstart < push_thr ? 1 : 0);
   if (src < 0) {
     if (a->nseeds_cap < nseeds) {
       cudaFree(a->seeds);
@@ -897,7 +1029,7 @@ int sssp_impl(gbo_graph* g, int src, uint32_t* d_dist, int* h_iters, cudaStream_
   using WT = typename Word<B>::T;
   AlgoState* a = nullptr;
   GBO_TRY(get_state(g, &a));
-  GBO_TRY(ensure_frontier(g, a));
+  GBO_TRY(ensure_frontier(g, a, s));
   if (!a->dist) {
     GBO_CUDA_TRY(cudaMalloc(&a->dist, sizeof(uint32_t) * (size_t)(g->nrows > 0 ? g->nrows : 1)));
     g->device_bytes += 4LL * g->nrows;
@@ -921,8 +1053,8 @@ int sssp_impl(gbo_graph* g, int src, uint32_t* d_dist, int* h_iters, cudaStream_
     return GBO_OK;
   }));
   const int max_iter = g->nrows + 1;
-  k_sssp_init<B><<<grid_vertex(std::max(g->nrows, g->nbr)), kTPB, 0, s>>>(front, vis, dist, g->nbr,
-                                                                        g->nrows, src, ctrl, max_iter);
+  k_sssp_init<B><<<grid_vertex(std::max(g->nrows, g->nbr)), kTPB, 0, s>>>(
+      front, vis, (const WT*)a->live, dist, g->nbr, g->nrows, src, ctrl, max_iter);
   GBO_CUDA_TRY(cudaGetLastError());
   GBO_TRY(run_until_done(a, A_SSSP, s, max_iter, h_iters));
   if (g->nrows > 0)
@@ -1071,6 +1203,7 @@ void free_algo_state(gbo_graph* g) {
   cudaFreeHost(a->h_ctrl);
   cudaFree(a->front);
   cudaFree(a->visited);
+  cudaFree(a->live);
   cudaFree(a->level);
   cudaFree(a->dist);
   cudaFree(a->pr);

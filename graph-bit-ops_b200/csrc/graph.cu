@@ -1,5 +1,6 @@
 // Graph handle construction and the C ABI of the BMV primitives.
 #include <algorithm>
+#include <cmath>
 #include <vector>
 
 #include "bmv.cuh"
@@ -167,6 +168,7 @@ extern "C" int gbo_graph_from_csr(const int* rowptr, const int* colind, int nrow
   }
 
   gbo_graph* g = new gbo_graph();
+  g->symmetric = (flags & GBO_FLAG_SYMMETRIC) && !lower && nrows == ncols;
   DevCsr csr, low;
   int st = upload_csr(src_ptr, src_col, prow, nnz, src_device, s, &csr);
   const DevCsr* use = &csr;
@@ -285,6 +287,17 @@ extern "C" int gbo_graph_outdeg(const gbo_graph* g, const int** d) {
   return GBO_OK;
 }
 
+extern "C" int gbo_graph_set_bfs_direction(gbo_graph* g, int symmetric, int push_threshold) {
+  clear_error();
+  if (!g) return fail(GBO_ERR_INVALID, "NULL graph");
+  if (push_threshold < -1) return fail(GBO_ERR_INVALID, "push_threshold must be >= -1");
+  if (symmetric && (g->nrows != g->ncols || g->layout != GBO_LAYOUT_ROW))
+    return fail(GBO_ERR_UNSUPPORTED, "push steps need a square ROW-layout graph");
+  g->symmetric = symmetric != 0;
+  g->bfs_push_thr = push_threshold;
+  return GBO_OK;
+}
+
 // ------------------------------------------------------------ BMV C ABI
 static int check_graph(const gbo_graph* g) {
   if (!g) return fail(GBO_ERR_INVALID, "graph is NULL");
@@ -360,4 +373,114 @@ extern "C" int gbo_bmv_float_transposed(const gbo_graph* g, const float* d_x, fl
   if (g->layout != GBO_LAYOUT_ROW) return fail(GBO_ERR_UNSUPPORTED, "BMV needs the ROW tile layout");
   if ((const void*)d_x == (const void*)d_y) return fail(GBO_ERR_INVALID, "x and y must not alias");
   return bmv_float_transposed(g, d_x, d_y, alpha, d_scale, add, as_stream(stream));
+}
+
+// ------------------------------------------------------------ tile tuner
+// Pick the tile width for a matrix and an operation.  MODEL ranks the widths
+// by the algorithmic bytes of one sweep over the packing (tile words +
+// column indices + block-row offsets), from the packer's count pass alone;
+// TIMED packs the matrix at every width and times the operation with CUDA
+// events (one warm-up, three timed runs), keeping the fastest.
+extern "C" int gbo_tune_tile_width(const int* rowptr, const int* colind, int nrows, int ncols,
+                                   int nnz, int flags, int op, int mode, gbo_stream_t stream,
+                                   int* best_bits, double* cost) {
+  clear_error();
+  static const int kWidths[5] = {4, 8, 16, 32, 64};
+  if (!best_bits) return fail(GBO_ERR_INVALID, "best_bits is NULL");
+  if (op != GBO_TUNE_BMV && op != GBO_TUNE_BFS && op != GBO_TUNE_TC) return fail(GBO_ERR_INVALID, "bad op");
+  if (mode != GBO_TUNE_MODEL && mode != GBO_TUNE_TIMED) return fail(GBO_ERR_INVALID, "bad mode");
+  if (nrows < 0 || ncols < 0 || nnz < 0 || !rowptr || (nnz > 0 && !colind))
+    return fail(GBO_ERR_INVALID, "gbo_tune_tile_width: bad CSR argument");
+  if (op == GBO_TUNE_TC) flags |= GBO_FLAG_LOWER;
+  if ((flags & GBO_FLAG_LOWER) && nrows != ncols) return fail(GBO_ERR_INVALID, "TC needs a square matrix");
+  cudaStream_t s = as_stream(stream);
+  double c[5];
+  if (mode == GBO_TUNE_MODEL) {
+    // tile counts of P and P^T are equal, so the transpose is never built
+    DevCsr csr, low;
+    int st = upload_csr(rowptr, colind, nrows, nnz, flags & GBO_FLAG_DEVICE_PTRS, s, &csr);
+    const DevCsr* use = &csr;
+    if (st == GBO_OK && (flags & GBO_FLAG_LOWER)) {
+      st = tril_device(csr, nrows, s, &low);
+      use = &low;
+    }
+    for (int k = 0; k < 5 && st == GBO_OK; ++k) {
+      const int b = kWidths[k];
+      long long nblk = 0;
+      st = count_tiles(use->rowptr, use->colind, nrows, ncols, use->nnz, b, &nblk, s);
+      if (st == GBO_OK) {
+        const double wb = b >= 8 ? b / 8 : 1;
+        c[k] = (double)nblk * (b * wb + 4.0) + 4.0 * ((nrows + b - 1) / b + 1);
+      } else if (st == GBO_ERR_OVERFLOW) {
+        c[k] = INFINITY;
+        st = GBO_OK;
+        clear_error();
+      }
+    }
+    if (st == GBO_OK) st = cudaStreamSynchronize(s) == cudaSuccess ? GBO_OK : fail(GBO_ERR_CUDA, "tuner sync");
+    low.release();
+    csr.release();
+    if (st != GBO_OK) return st;
+  } else {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    GBO_CUDA_TRY(cudaEventCreate(&e0));
+    GBO_CUDA_TRY(cudaEventCreate(&e1));
+    int st = GBO_OK;
+    for (int k = 0; k < 5 && st == GBO_OK; ++k) {
+      const int b = kWidths[k];
+      gbo_graph* g = nullptr;
+      st = gbo_graph_from_csr(rowptr, colind, nrows, ncols, nnz, b, flags, stream, &g);
+      if (st == GBO_ERR_OVERFLOW) {  // too many tiles at this width
+        c[k] = INFINITY;
+        st = GBO_OK;
+        clear_error();
+        continue;
+      }
+      if (st != GBO_OK) break;
+      void* buf = nullptr;
+      const size_t xb = (size_t)(g->nbc + 1) * 8;
+      const size_t yb = sizeof(int) * (size_t)(g->nrows > 0 ? g->nrows : 1) + 8;
+      if (cudaMalloc(&buf, xb + yb) != cudaSuccess) {
+        gbo_graph_free(g);
+        st = fail(GBO_ERR_NOMEM, "tuner buffers");
+        break;
+      }
+      char* x = static_cast<char*>(buf);
+      char* y = x + xb;
+      cudaMemsetAsync(x, 0x55, xb, s);  // every other vertex set
+      auto run = [&]() -> int {
+        int d = 0;
+        switch (op) {
+          case GBO_TUNE_BMV: return gbo_bmv_count(g, x, y, GBO_OUT_I32, 0, stream);
+          case GBO_TUNE_BFS: return gbo_bfs(g, 0, reinterpret_cast<int32_t*>(y), &d, stream);
+          default: return gbo_tc_device(g, reinterpret_cast<unsigned long long*>(y), stream);
+        }
+      };
+      st = run();
+      float ms = 0.f;
+      if (st == GBO_OK) {
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < 3 && st == GBO_OK; ++r) st = run();
+        cudaEventRecord(e1, s);
+        const cudaError_t e = cudaEventSynchronize(e1);
+        if (st == GBO_OK && e != cudaSuccess) st = fail_cuda(e, "tuner timing");
+        if (st == GBO_OK) cudaEventElapsedTime(&ms, e0, e1);
+      }
+      c[k] = ms / 3.0;
+      cudaStreamSynchronize(s);
+      cudaFree(buf);
+      gbo_graph_free(g);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != GBO_OK) return st;
+  }
+  int best = -1;
+  for (int k = 0; k < 5; ++k)
+    if (c[k] < INFINITY && (op != GBO_TUNE_TC || kWidths[k] >= 8) && (best < 0 || c[k] < c[best])) best = k;
+  if (cost)
+    for (int k = 0; k < 5; ++k) cost[k] = c[k];
+  if (best < 0) return fail(GBO_ERR_OVERFLOW, "no tile width packs this matrix");
+  *best_bits = kWidths[best];
+  return GBO_OK;
 }

@@ -26,6 +26,8 @@ struct gbo_graph {
   int* outdeg = nullptr;   // ncols (column counts of P), may be null
   float* invdeg = nullptr; // 1/outdeg (0 where outdeg == 0), may be null
   bool owns_b2sr = true;
+  bool symmetric = false;  // caller asserts P == P^T (enables push BFS steps)
+  int bfs_push_thr = -1;   // push below this frontier size (-1: nrows / 64)
   bool owns_outdeg = true;
   // balanced schedule
   int chunk = 0;
@@ -67,6 +69,8 @@ int ensure_workspace(gbo_graph* g, size_t bytes, cudaStream_t stream);
 
 // Pack CSR (device pointers) into B2SR owned by g.  Sets nblk, rowptr, colind,
 // val.  Synchronises the stream once (to size the tile arrays).
+int count_tiles(const int* d_rowptr, const int* d_colind, int nrows, int ncols, long long nnz, int b,
+                long long* nblk, cudaStream_t s);
 int pack_into(gbo_graph* g, const int* d_rowptr, const int* d_colind, int nrows, int ncols,
               long long nnz, int b, int layout, cudaStream_t stream);
 

@@ -456,6 +456,18 @@ static int nnzb_impl(const int* rowptr, const int* colind, int nrows, int ncols,
   return GBO_OK;
 }
 
+// Tile count of the B2SR packing of a device CSR at tile width b (the
+// count pass of the packer alone; used by the tile-width tuner).
+int count_tiles(const int* d_rowptr, const int* d_colind, int nrows, int ncols, long long nnz, int b,
+                long long* nblk, cudaStream_t s) {
+  const int nbr = (nrows + b - 1) / b;
+  int* tmp = nullptr;
+  GBO_CUDA_TRY(cudaMallocAsync(&tmp, sizeof(int) * ((size_t)nbr + 1), s));
+  const int st = nnzb_impl(d_rowptr, d_colind, nrows, ncols, nnz, b, tmp, nblk, s);
+  cudaFreeAsync(tmp, s);
+  return st;
+}
+
 static int fill_impl(const int* rowptr, const int* colind, int nrows, int ncols, long long nnz,
                      int b, int layout, const int* bsr_rowptr, int* bsr_colind, void* bsr_val,
                      cudaStream_t s, bool check) {

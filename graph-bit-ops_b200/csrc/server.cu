@@ -275,11 +275,12 @@ struct Query {
 
 struct Result {
   int kind;
-  int buf;          // pinned pool buffer holding the result
+  int buf;          // pinned pool buffer holding the result (-1: moved to heap)
   cudaEvent_t ev;   // its copy has landed when this event completes
   bool landed;
   double t_submit, t_done;
   int iters;
+  std::vector<int> heap;  // the result once moved out of the pinned pool
 };
 
 }  // namespace
@@ -540,6 +541,30 @@ bool collect_landed(gbo_server* S) {
   return any;
 }
 
+// Results that nobody has taken yet keep their pinned buffers; when every
+// buffer is held that way and finished slots wait for one, move landed
+// results to heap memory (oldest tickets first) so that retirement never
+// waits on the order in which clients collect (caller holds the lock).
+bool spill_landed(gbo_server* S) {
+  bool waiting = false;
+  for (size_t q = 0; q < S->bslot_ticket.size() && !waiting; ++q)
+    waiting = S->bslot_ticket[q] > 0 && S->bslot_finished[q];
+  for (size_t q = 0; q < S->pslot_ticket.size() && !waiting; ++q)
+    waiting = S->pslot_ticket[q] > 0 && S->pslot_finished[q];
+  if (!waiting || !S->pool_free.empty()) return false;
+  int moved = 0;
+  for (auto& kv : S->results) {
+    Result& r = kv.second;
+    if (!r.landed || r.buf < 0) continue;
+    const int* src = static_cast<const int*>(S->pool[(size_t)r.buf]);
+    r.heap.assign(src, src + S->n);
+    S->pool_free.push_back(r.buf);
+    r.buf = -1;
+    if (++moved == kRetire) break;
+  }
+  return moved > 0;
+}
+
 void worker_main(gbo_server* S) {
   cudaSetDevice(S->dev);
   auto failw = [&](int st) {
@@ -565,6 +590,7 @@ void worker_main(gbo_server* S) {
       for (;;) {
         if (collect_landed(S)) S->cv_done.notify_all();
         if (S->stop) return;
+        spill_landed(S);
         const bool work = !S->pending.empty() || unfinished(S->bslot_ticket, S->bslot_finished) ||
                           unfinished(S->pslot_ticket, S->pslot_finished) ||
                           ((occupied(S->bslot_ticket) || occupied(S->pslot_ticket)) && !S->pool_free.empty());
@@ -810,15 +836,16 @@ extern "C" int gbo_server_submit_ppr(gbo_server* S, const int* verts, const floa
 static int take_result(gbo_server* S, std::unique_lock<std::mutex>& lk, int64_t ticket, void* h_out,
                        double* latency_ms, int* iterations) {
   auto it = S->results.find(ticket);
-  const Result r = it->second;
+  const Result r = std::move(it->second);
   S->results.erase(it);
   S->submit_time.erase(ticket);
   lk.unlock();
-  if (h_out) memcpy(h_out, S->pool[(size_t)r.buf], sizeof(int) * (size_t)S->n);
+  if (h_out) memcpy(h_out, r.buf >= 0 ? S->pool[(size_t)r.buf] : (const void*)r.heap.data(),
+                    sizeof(int) * (size_t)S->n);
   if (latency_ms) *latency_ms = r.t_done - r.t_submit;
   if (iterations) *iterations = r.iters;
   lk.lock();
-  S->pool_free.push_back(r.buf);
+  if (r.buf >= 0) S->pool_free.push_back(r.buf);
   S->cv_work.notify_one();
   return GBO_OK;
 }

@@ -33,6 +33,7 @@ FLAG_DEVICE_PTRS = 1
 FLAG_TRANSPOSE = 2
 FLAG_LAYOUT_COL = 4
 FLAG_LOWER = 8
+FLAG_SYMMETRIC = 16
 OUT_I32 = 0
 OUT_F32 = 1
 MTX_READMTX = 0
@@ -113,6 +114,8 @@ _SIGS = {
     "gbo_graph_get_info": (_I, [_P, C.POINTER(GraphInfo)]),
     "gbo_graph_b2sr": (_I, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
     "gbo_graph_outdeg": (_I, [_P, C.POINTER(_P)]),
+    "gbo_graph_set_bfs_direction": (_I, [_P, _I, _I]),
+    "gbo_tune_tile_width": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _P, C.POINTER(_I), _P]),
     "gbo_bmv_count": (_I, [_P, _P, _P, _I, _I, _P]),
     "gbo_bmv_masked": (_I, [_P, _P, _P, _P, _P]),
     "gbo_bmv_minplus": (_I, [_P, _P, _P, _P]),
@@ -392,6 +395,20 @@ def gen_er_batch(count: int, nmin: int, nmax: int, avg_degree: float = 8.0, seed
     return Csr._take(out), off
 
 
+TUNE_BMV, TUNE_BFS, TUNE_TC = 0, 1, 2
+TUNE_MODEL, TUNE_TIMED = 0, 1
+
+
+def tune_tile_width(csr: "Csr", op: int = TUNE_BMV, mode: int = TUNE_MODEL, flags: int = 0, stream=None):
+    """gbo_tune_tile_width: returns (best b, {b: bytes or ms})."""
+    best = C.c_int(0)
+    cost = np.zeros(5, np.float64)
+    check(lib().gbo_tune_tile_width(_ptr(csr.rowptr), _ptr(csr.colind), csr.nrows, csr.ncols, csr.nnz,
+                                    flags, op, mode, stream, C.byref(best), _ptr(cost)),
+          "tune_tile_width")
+    return best.value, dict(zip((4, 8, 16, 32, 64), cost.tolist()))
+
+
 def gen_king_mesh(side: int) -> Csr:
     out = C.POINTER(CsrStruct)()
     check(lib().gbo_gen_king_mesh(side, C.byref(out)), "gen_king_mesh")
@@ -445,6 +462,12 @@ class Graph:
         p = C.c_void_p()
         check(lib().gbo_graph_outdeg(self.h, C.byref(p)), "graph_outdeg")
         return device_to_numpy(p.value, np.int32, self.info().ncols)
+
+    def set_bfs_direction(self, symmetric: bool, push_threshold: int = -1) -> None:
+        """Allow top-down BFS steps on a symmetric graph below push_threshold
+        frontier vertices (-1: nrows / 64; 0: pull only)."""
+        check(lib().gbo_graph_set_bfs_direction(self.h, int(bool(symmetric)), push_threshold),
+              "graph_set_bfs_direction")
 
     def last_run(self) -> dict:
         st = RunStats()
@@ -636,7 +659,7 @@ class Server:
               "server_submit_ppr")
         return t.value
 
-    def wait(self, ticket: int, kind: str = "bfs", timeout=600.0):
+    def wait(self, ticket: int, kind: str = "bfs", timeout=120.0):
         out = np.empty(self.n, np.int32 if kind == "bfs" else np.float32)
         lat, it = C.c_double(0), C.c_int(0)
         check(lib().gbo_server_wait(self.h, ticket, _ptr(out), C.byref(lat), C.byref(it), timeout),

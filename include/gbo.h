@@ -130,7 +130,10 @@ enum gbo_graph_flags {
   GBO_FLAG_DEVICE_PTRS = 1, /* rowptr/colind are device pointers (else host) */
   GBO_FLAG_TRANSPOSE = 2,   /* pack the transpose of the given CSR (CSC) */
   GBO_FLAG_LAYOUT_COL = 4,  /* COL tile layout instead of ROW */
-  GBO_FLAG_LOWER = 8        /* keep only row >= col entries (tril_csr) */
+  GBO_FLAG_LOWER = 8,       /* keep only row >= col entries (tril_csr) */
+  GBO_FLAG_SYMMETRIC = 16   /* caller asserts the packed matrix is symmetric:
+                               BFS may then take top-down (push) steps while
+                               the frontier is small (direction-optimising) */
 };
 
 /* Pack a CSR matrix M into a device-resident B2SR graph owned by the handle.
@@ -167,6 +170,31 @@ GBO_API int gbo_graph_b2sr(const gbo_graph* g, const int** d_bsrRowPtr,
                    const int** d_bsrColInd, const void** d_bsrVal);
 /* Device array of out-degrees (ncols ints) or NULL. */
 GBO_API int gbo_graph_outdeg(const gbo_graph* g, const int** d_outdeg);
+/* Direction-optimising BFS control (no counterpart in the reference, whose
+ * BFS only pulls).  symmetric = 1 asserts P == P^T (what GBO_FLAG_SYMMETRIC
+ * does for gbo_graph_from_csr; needed for wrapped graphs), 0 restores
+ * pull-only BFS.  A level whose frontier holds fewer than push_threshold
+ * vertices is expanded top-down; -1 selects the default nrows / 64.
+ * Rejected (GBO_ERR_UNSUPPORTED) for a non-square or COL-layout graph. */
+GBO_API int gbo_graph_set_bfs_direction(gbo_graph* g, int symmetric, int push_threshold);
+
+/* Tile-width tuner (no counterpart in the reference, whose drivers take b
+ * from the command line).  Ranks b = 4, 8, 16, 32, 64 for the CSR matrix
+ * (same arguments and flags as gbo_graph_from_csr) and an operation:
+ *   mode GBO_TUNE_MODEL: algorithmic bytes of one sweep over the packing
+ *     (nblocks(b) * (b words + 4-byte column index) + block-row offsets),
+ *     from the packer's count pass only -- nothing is packed;
+ *   mode GBO_TUNE_TIMED: packs at every width and times the operation
+ *     (one warm-up, mean of three runs, CUDA events on `stream`).
+ * op GBO_TUNE_TC packs the lower triangle and never picks b = 4.
+ * *best_bits gets the cheapest width; cost (nullable, 5 doubles, widths in
+ * the order above) gets bytes or milliseconds (INFINITY where a width
+ * overflows the int32 tile count). */
+enum { GBO_TUNE_BMV = 0, GBO_TUNE_BFS = 1, GBO_TUNE_TC = 2 };
+enum { GBO_TUNE_MODEL = 0, GBO_TUNE_TIMED = 1 };
+GBO_API int gbo_tune_tile_width(const int* rowptr, const int* colind, int nrows, int ncols,
+                                int nnz, int flags, int op, int mode, gbo_stream_t stream,
+                                int* best_bits, double* cost);
 
 /* ------------------------------------------------ BMV primitives (A3-A8) */
 enum { GBO_OUT_I32 = 0, GBO_OUT_F32 = 1 };

@@ -135,3 +135,42 @@ def test_ppr_forward_backward(gbo, orc, gpu, b):
         pm, _ = g.ppr_forward((v - 1e-3 * d).astype(np.float32), 0.85, 1e-9, 2000)
         fd = (w @ pp.astype(np.float64) - w @ pm.astype(np.float64)) / 2e-3
         assert abs(fd - grad @ d) <= 2e-3 * max(1.0, abs(fd)) + 1e-4
+
+
+@pytest.mark.parametrize("b", WIDTHS)
+def test_bfs_direction_optimizing(gbo, orc, gpu, graphs, b):
+    """Symmetric graphs may take top-down (push) steps: same levels."""
+    for name, csr in graphs.items():
+        if name == "ragged1001":
+            continue  # not symmetric
+        g = gbo.Graph.from_csr(csr, b, gbo.FLAG_SYMMETRIC)
+        for src in (0, csr.nrows // 3, csr.nrows - 1):
+            lv, depth = g.bfs(src)
+            want, d = orc.bfs_csr(csr.rowptr, csr.colind, csr.nrows, src)
+            assert np.array_equal(lv, want), (name, b, src)
+            assert depth == d
+        # many seeds at once (block-diagonal batches) start in push mode too
+        seeds = np.arange(0, csr.nrows, max(1, csr.nrows // 7), dtype=np.int32)
+        lv, _ = g.bfs_multi(seeds)
+        ref = np.full(csr.nrows, -1, np.int64)
+        for s in seeds:
+            x, _ = orc.bfs_csr(csr.rowptr, csr.colind, csr.nrows, int(s))
+            ref = np.where((ref < 0) | ((x >= 0) & (x < ref)), x, ref)
+        assert np.array_equal(lv, ref), (name, b)
+
+
+@pytest.mark.parametrize("b", WIDTHS)
+def test_bfs_push_every_level(gbo, orc, gpu, graphs, b):
+    """Threshold above n: every level is a top-down step (atomics into the
+    next frontier), including the dense middle levels."""
+    for name in ("rmat14", "mesh33", "star20000", "er1000"):
+        csr = graphs[name]
+        g = gbo.Graph.from_csr(csr, b)
+        g.set_bfs_direction(True, csr.nrows + 1)
+        for src in (1, csr.nrows - 2):
+            lv, depth = g.bfs(src)
+            want, d = orc.bfs_csr(csr.rowptr, csr.colind, csr.nrows, src)
+            assert np.array_equal(lv, want) and depth == d, (name, b, src)
+        g.set_bfs_direction(False)
+        lv, _ = g.bfs(1)
+        assert np.array_equal(lv, orc.bfs_csr(csr.rowptr, csr.colind, csr.nrows, 1)[0])

@@ -93,3 +93,21 @@ def test_server_poll_and_errors(gbo, gpu):
     with pytest.raises(gbo.GboError):
         srv.submit_bfs(10**6)
     srv.close()
+
+
+def test_server_results_collected_in_any_order(gbo, orc, gpu):
+    """More finished queries than pinned result buffers, collected newest
+    first: results left uncollected move to heap memory instead of blocking
+    retirement, and every result is still exact."""
+    csr = gbo.gen_er(3000, 0.003, 5)
+    g = gbo.Graph.from_csr(csr, 32)
+    srv = gbo.Server(g, bfs_slots=64, ppr_slots=0)
+    srcs = np.random.default_rng(12).integers(0, csr.nrows, 400)
+    tickets = [srv.submit_bfs(int(s)) for s in srcs]
+    out = {}
+    for s, t in reversed(list(zip(srcs, tickets))):
+        out[t] = (s, srv.wait(t, "bfs", timeout=60.0)[0])
+    assert srv.stats()["bfs_completed"] == 400
+    srv.close()
+    for s, lv in out.values():
+        assert np.array_equal(lv, orc.bfs_csr(csr.rowptr, csr.colind, csr.nrows, int(s))[0])
