@@ -117,6 +117,7 @@ _SIGS = {
     "gbo_graph_set_bfs_direction": (_I, [_P, _I, _I]),
     "gbo_tune_tile_width": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _P, C.POINTER(_I), _P]),
     "gbo_bmv_count": (_I, [_P, _P, _P, _I, _I, _P]),
+    "gbo_bmv_count_noalloc": (_I, [_I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _I, _P]),
     "gbo_bmv_masked": (_I, [_P, _P, _P, _P, _P]),
     "gbo_bmv_minplus": (_I, [_P, _P, _P, _P]),
     "gbo_bmv_float": (_I, [_P, _P, _P, C.c_float, _P, C.c_float, _P]),

@@ -206,6 +206,26 @@ enum { GBO_OUT_I32 = 0, GBO_OUT_F32 = 1 };
  * bsrbmv.cu:464-471) counts are exact 32-bit. */
 GBO_API int gbo_bmv_count(const gbo_graph* g, const void* d_x_bits, void* d_y,
                   int out_type, int accumulate, gbo_stream_t stream);
+/* The same y as gbo_bmv_count, computed straight from caller-owned ROW-layout
+ * B2SR arrays (bsrRowPtr: ceil(nrows/b)+1 ints ending at nblocks; bsrColInd,
+ * bsrVal as gbo_b2sr_pack writes them) without a graph handle, and without
+ * allocating any device or host memory at any call.  No counterpart in the
+ * reference.  For callers that may not allocate: a framework that owns all
+ * device memory through its own pool, or a thread that must not let
+ * cudaMalloc / cudaFree synchronise a device shared with other streams.
+ * Row partials of long block rows go to one fixed 8 MiB device array inside
+ * this library, shared by every call on a device:
+ *   - at most 2^35 / b^2 tiles per call (33,554,432 at b = 32, 8,388,608 at
+ *     b = 64); more returns GBO_ERR_UNSUPPORTED before any launch;
+ *   - calls whose kernels may overlap (other streams, unordered threads)
+ *     race on that array and can return wrong counts: order them;
+ *   - the first call on each device looks up the array's device address
+ *     (cudaGetSymbolAddress, which may load this library's device code):
+ *     make that first call before any stream capture begins. */
+GBO_API int gbo_bmv_count_noalloc(int nrows, int ncols, int tile_bits, int nblocks,
+                                  const int* d_bsrRowPtr, const int* d_bsrColInd,
+                                  const void* d_bsrVal, const void* d_x_bits, void* d_y,
+                                  int out_type, int accumulate, gbo_stream_t stream);
 /* out_bits[R] = bits (sum_j P[i][j] x[j] > 0) & ~mask[R]  (Boolean OR.AND with
  * a complement mask).  Replaces bmv32_sparse_bin_masked_v4 and
  * bmv4_sparse_bin_masked_v4 (bsrbmv.cu:637-783).  d_mask_bits may be NULL. */
