@@ -320,7 +320,9 @@ def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed):
     st = srv.stats()
     srv.close()
     out = {"offered_qps": rate_qps, "queries": nq, "achieved_qps": nq / wall, "wall_s": wall,
-           "rounds": st["rounds"]}
+           "rounds": st["rounds"], "kernel_launches": st["kernel_launches"],
+           "phase_ms": {k: round(st[k], 1) for k in ("bfs_round_ms", "ppr_round_ms", "retire_ms", "spill_ms")},
+           "spilled": st["spilled"]}
     for k, v in lat.items():
         if v:
             out[f"{k}_p50_ms"] = float(np.percentile(v, 50))
@@ -454,7 +456,10 @@ def run_ours(args, ws, rank, local):
     served = {}
     if not args.no_serve:
         served["bfs_only"] = serve_stream(gbo, g, n, args.serve_qps, args.serve_s, 0.0, 5)
+        # against one plain BFS per query on the device, and against the same
+        # call with its levels read back to host memory (what a served query delivers)
         served["bfs_only"]["vs_plain_bfs_qps"] = served["bfs_only"]["achieved_qps"] / (1e3 / ms)
+        served["bfs_only"]["vs_plain_e2e_qps"] = served["bfs_only"]["achieved_qps"] / (1e3 / e2e_ms)
         served["mixed_10pct_ppr"] = serve_stream(gbo, g, n, args.serve_qps / 8, args.serve_s, 0.1, 6)
     wb = max(1, args.tile // 8)
     bmv_bytes = (int(info.nblocks) * (args.tile * args.tile // 8 + 4) + 4 * (info.nblockrows + 1)
@@ -597,7 +602,7 @@ def suite_config2(args, which):
 
     orc = _oracle()
     csr = gbo.gen_rmat(args.scale, EDGE_FACTOR, seed=SEED, **RMAT)
-    g = gbo.Graph.from_csr(csr, args.tile)
+    g = gbo.Graph.from_csr(csr, args.tile, gbo.FLAG_SYMMETRIC)  # symmetrised R-MAT
     info = g.info()
     n = csr.nrows
     lv, depth = g.bfs(0)
@@ -637,7 +642,7 @@ def suite_config2(args, which):
                     args.steps, args.warmup)
         st = g.last_run()
         step = float(np.mean(st["step_ms"])) if st["step_ms"] else ms / iters
-        by = _bmv_bytes(info, args.tile, n, 4 * n * 3)  # p read, D^-1 read, p' write
+        by = _bmv_bytes(info, args.tile, n, 4 * n * 5)  # p/deg gathered, p, D^-1 read; p', p'/deg written
         cfg["workload"] = f"PageRank alpha 0.85, 20 iterations, fp32 values / fp64 sums, R-MAT scale {args.scale}"
         extra = {"iterations": it.value, "dtype": "f32",
                  "roofline": {"bound": "hbm", "achieved": by / (step / 1e3) / 1e9, "peak": peak,
@@ -784,7 +789,7 @@ def suite_ppr(args):
 
     csr = gbo.gen_rmat(20, 16, seed=1, **RMAT)
     n = csr.nrows
-    g = gbo.Graph.from_csr(csr, 32)
+    g = gbo.Graph.from_csr(csr, 32, gbo.FLAG_SYMMETRIC)  # adjoint gathers over P = P^T
     rng = np.random.default_rng(4)
     idx = rng.choice(n, n // 100, replace=False)
     v = np.zeros(n)

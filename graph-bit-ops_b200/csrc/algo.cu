@@ -33,6 +33,9 @@ struct Ctrl {
   float add_scale;  // PPR: add_scale * v[i] added as well
   int norm;       // 1 = L1, 2 = L2 error
   int n;
+  double ref;     // PPR adjoint: ||w||_1, the scale of its stopping test
+  unsigned long long work;  // BFS pull step: warp work units handed out this iteration
+  int row_scale;  // PR-type step: 0 = columns scaled (PageRank), 1 = rows (adjoint on P = P^T)
   int mode;       // BFS: 0 = pull (bottom-up) step, 1 = push (top-down) step
   int push_thr;   // BFS: push while the frontier has fewer vertices (0 = never)
 };
@@ -52,6 +55,7 @@ struct AlgoState {
   uint32_t* dist = nullptr;
   // PR / PPR / CC vectors
   float* pr = nullptr;     // 2 * n
+  float* prs = nullptr;    // 2 * n: the iterate scaled by D^-1 (PageRank gathers it)
   const float* ppr_v = nullptr;
   int* f = nullptr;
   int* gf = nullptr;
@@ -79,7 +83,7 @@ namespace {
 constexpr int kTPB = 256;
 constexpr int kStepsPerGraph = 8;
 
-enum AlgoId { A_BFS = 0, A_SSSP = 1, A_PR = 2, A_CC = 3, A_PPR_F = 4, A_PPR_B = 5 };
+enum AlgoId { A_BFS = 0, A_SSSP = 1, A_PR = 2, A_CC = 3, A_PPR_F = 4, A_PPR_B = 5, A_PPR_BG = 6 };
 
 template <int B>
 __device__ __forceinline__ typename Word<B>::T full_word() {
@@ -121,6 +125,15 @@ __device__ __forceinline__ long long item_index(unsigned lane, int W, int G) {
   const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   return warp * G + lane / W;
 }
+
+// The iteration kernels visit work items in a warp-uniform grid-stride loop
+// and run on a persistent grid (a few blocks per SM): an iteration with
+// nothing to do (the loop has finished, or the other BFS direction is
+// active) then costs microseconds instead of a launch over every item.
+__device__ __forceinline__ long long warp_global() {
+  return ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+}
+__device__ __forceinline__ long long warps_total() { return ((long long)gridDim.x * blockDim.x) >> 5; }
 
 // Block-wide sum of `v` added to *dst once per block.
 __device__ __forceinline__ void block_add_u64(unsigned long long v, unsigned long long* dst) {
@@ -165,6 +178,7 @@ __device__ __forceinline__ void close_iteration(Ctrl* ctrl, Decide decide) {
     c->last_err = c->err;
     c->err = 0.0;
     c->count = 0ull;
+    c->work = 0ull;
     c->ticket = 0u;
     if (stop) c->done = 1;
     __threadfence();
@@ -184,33 +198,47 @@ __global__ void __launch_bounds__(kTPB) k_bfs_step(GView v, typename Word<B>::T*
   const WT* __restrict__ x = front + (size_t)(lvl & 1) * v.nbr;
   WT* __restrict__ out = front + (size_t)((lvl + 1) & 1) * v.nbr;
   const unsigned lane = threadIdx.x & 31;
-  const long long item = item_index(lane, L::W, L::G);
-  const bool active = item < v.nitems;
   const int r = lane % L::W;
-  gbo_item it = active ? v.items[item] : gbo_item{0, 0, 0, -2};
   const WT full = full_word<B>();
-  const WT vis = active ? visited[it.row] : full;
-  bool p0 = false, p1 = false;
-  if (active && (vis & full) != full) {  // uniform inside the item's lane group
-    const long long row0 = (long long)it.row * B + r;
-    const bool need0 = !bit_of<B>(vis, r) && row0 < v.nrows;
-    const bool need1 = L::RPL == 2 && !bit_of<B>(vis, r + 32) && row0 + 32 < v.nrows;
-    pull_or_scan<B>(v, it.t0, it.t1, x, need0, need1, p0, p1, lane);
-  }
-  const WT word = gather_bits<B>(p0, p1, lane);
   unsigned long long cnt = 0;
-  if (active) {
-    if (it.slot >= 0) {
-      if (r == 0) scratch[it.slot] = word;
-    } else {
-      const WT nw = (WT)(word & ~vis & full);
+  // warps take work units (L::G items each) kGrab at a time from a counter:
+  // rows that stop early and rows scanned to the end even out dynamically
+  constexpr long long kGrab = 4;
+  long long w = 0, wend = 0;
+  for (;;) {
+    if (w == wend) {
+      unsigned long long g0 = 0;
+      if (lane == 0) g0 = atomicAdd(&ctrl->work, (unsigned long long)kGrab);
+      w = (long long)__shfl_sync(0xffffffffu, g0, 0);
+      wend = w + kGrab;
+    }
+    if (w * L::G >= v.nitems) break;
+    const long long item = w * L::G + lane / L::W;
+    ++w;
+    const bool active = item < v.nitems;
+    gbo_item it = active ? v.items[item] : gbo_item{0, 0, 0, -2};
+    const WT vis = active ? visited[it.row] : full;
+    bool p0 = false, p1 = false;
+    if (active && (vis & full) != full) {  // uniform inside the item's lane group
       const long long row0 = (long long)it.row * B + r;
-      if (bit_of<B>(nw, r) && row0 < v.nrows) level[row0] = lvl + 1;
-      if (L::RPL == 2 && bit_of<B>(nw, r + 32) && row0 + 32 < v.nrows) level[row0 + 32] = lvl + 1;
-      if (r == 0) {
-        out[it.row] = nw;
-        if (nw) visited[it.row] = (WT)(vis | nw);
-        cnt = popc_w(nw);
+      const bool need0 = !bit_of<B>(vis, r) && row0 < v.nrows;
+      const bool need1 = L::RPL == 2 && !bit_of<B>(vis, r + 32) && row0 + 32 < v.nrows;
+      pull_or_scan<B>(v, it.t0, it.t1, x, need0, need1, p0, p1, lane);
+    }
+    const WT word = gather_bits<B>(p0, p1, lane);
+    if (active) {
+      if (it.slot >= 0) {
+        if (r == 0) scratch[it.slot] = word;
+      } else {
+        const WT nw = (WT)(word & ~vis & full);
+        const long long row0 = (long long)it.row * B + r;
+        if (bit_of<B>(nw, r) && row0 < v.nrows) level[row0] = lvl + 1;
+        if (L::RPL == 2 && bit_of<B>(nw, r + 32) && row0 + 32 < v.nrows) level[row0 + 32] = lvl + 1;
+        if (r == 0) {
+          out[it.row] = nw;
+          if (nw) visited[it.row] = (WT)(vis | nw);
+          cnt += popc_w(nw);
+        }
       }
     }
   }
@@ -283,18 +311,19 @@ __global__ void __launch_bounds__(kTPB) k_bfs_push(GView v, typename Word<B>::T*
   const WT* __restrict__ x = front + (size_t)(lvl & 1) * v.nbr;
   WT* out = front + (size_t)((lvl + 1) & 1) * v.nbr;
   const unsigned lane = threadIdx.x & 31;
-  const long long item = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (item >= v.nitems) return;
-  const gbo_item it = v.items[item];
-  const WT xs = x[it.row];
-  if (!xs) return;
   const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
-  for (int t = it.t0 + (int)lane; t < it.t1; t += 32) {
-    const int C = v.colind[t];
-    WT acc = 0;
-    for_each_col<B>(xs, [&](int r) { acc = (WT)(acc | val[(size_t)t * B + r]); });
-    const WT cand = (WT)(acc & ~visited[C]);
-    if (cand) atomic_or_word<B>(out, C, cand);
+  const long long nwarps = warps_total();
+  for (long long item = warp_global(); item < v.nitems; item += nwarps) {
+    const gbo_item it = v.items[item];
+    const WT xs = x[it.row];
+    if (!xs) continue;
+    for (int t = it.t0 + (int)lane; t < it.t1; t += 32) {
+      const int C = v.colind[t];
+      WT acc = 0;
+      for_each_col<B>(xs, [&](int r) { acc = (WT)(acc | val[(size_t)t * B + r]); });
+      const WT cand = (WT)(acc & ~visited[C]);
+      if (cand) atomic_or_word<B>(out, C, cand);
+    }
   }
 }
 
@@ -391,209 +420,79 @@ __global__ void k_bfs_init(typename Word<B>::T* front, typename Word<B>::T* visi
     ctrl->last_err = 0;
     ctrl->push_thr = push_thr;
     ctrl->mode = mode0;
+    ctrl->work = 0ull;
   }
 }
 
 // ============================================================= SSSP
-// Min-plus relaxation from the frontier: d'[i] = min over frontier
-// neighbours j of d[j] + 1, kept where it improves d[i].
-template <int B>
-__global__ void __launch_bounds__(kTPB) k_sssp_step(GView v, typename Word<B>::T* __restrict__ front,
-                                                    typename Word<B>::T* __restrict__ visited,
-                                                    uint32_t* __restrict__ dist, Ctrl* __restrict__ ctrl,
-                                                    uint32_t* __restrict__ scratch) {
-  using WT = typename Word<B>::T;
-  using L = Lay<B>;
-  if (((volatile Ctrl*)ctrl)->done) return;
-  const int lvl = ((volatile Ctrl*)ctrl)->iter;
-  const WT* __restrict__ x = front + (size_t)(lvl & 1) * v.nbr;
-  WT* __restrict__ out = front + (size_t)((lvl + 1) & 1) * v.nbr;
-  const unsigned lane = threadIdx.x & 31;
-  const long long item = item_index(lane, L::W, L::G);
-  const bool active = item < v.nitems;
-  const int r = lane % L::W;
-  gbo_item it = active ? v.items[item] : gbo_item{0, 0, 0, -2};
-  const WT full = full_word<B>();
-  const WT vis = active ? visited[it.row] : full;
-  uint32_t a0 = (uint32_t)kINF, a1 = (uint32_t)kINF;
-  if (active && (vis & full) != full) {  // uniform inside the item's lane group
-    constexpr int W = L::W;
-    const unsigned gmask = group_mask<B>(lane);
-    const unsigned gshift = (lane / W) * W;
-    const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
-    auto relax = [&](uint32_t& acc, WT m, long long base) {
-      for_each_col<B>(m, [&](int j) {
-        uint32_t d = dist[base + j];
-        acc = min(acc, d >= (uint32_t)kINF ? (uint32_t)kINF : d + 1u);
-      });
-    };
-    // block-column indices W at a time, x gathered in parallel, tile words
-    // fetched only for tiles with a non-empty frontier segment
-    for (int b0 = it.t0; b0 < it.t1; b0 += W) {
-      const int t = b0 + r;
-      int c = 0;
-      WT xs = 0;
-      if (t < it.t1) {
-        c = v.colind[t];
-        xs = x[c];
-      }
-      unsigned nz = (__ballot_sync(gmask, xs != 0) >> gshift) & seg_mask<W>();
-      while (nz) {
-        int j[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          j[q] = nz ? __ffs(nz) - 1 : -1;
-          nz &= nz - 1;
-        }
-        WT xv[4], w0[4] = {0, 0, 0, 0}, w1[4] = {0, 0, 0, 0};
-        int cv[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          xv[q] = shfl_word<WT>(gmask, xs, j[q] < 0 ? 0 : j[q], W);
-          cv[q] = __shfl_sync(gmask, c, j[q] < 0 ? 0 : j[q], W);
-        }
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-          if (j[q] >= 0) {
-            w0[q] = val[(size_t)(b0 + j[q]) * B + r];
-            if (L::RPL == 2) w1[q] = val[(size_t)(b0 + j[q]) * B + 32 + r];
-          }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          relax(a0, (WT)(w0[q] & xv[q]), (long long)cv[q] * B);
-          if (L::RPL == 2) relax(a1, (WT)(w1[q] & xv[q]), (long long)cv[q] * B);
-        }
-      }
-    }
-  }
-  const long long row0 = (long long)it.row * B + r;
-  bool n0 = false, n1 = false;
-  if (active && it.slot < 0) {
-    if (row0 < v.nrows && a0 < dist[row0]) { dist[row0] = a0; n0 = true; }
-    if (L::RPL == 2 && row0 + 32 < v.nrows && a1 < dist[row0 + 32]) { dist[row0 + 32] = a1; n1 = true; }
-  }
-  const WT word = gather_bits<B>(n0, n1, lane);
-  unsigned long long cnt = 0;
-  if (active) {
-    if (it.slot >= 0) {
-      scratch[(size_t)it.slot * B + r] = a0;
-      if (L::RPL == 2) scratch[(size_t)it.slot * B + 32 + r] = a1;
-    } else if (r == 0) {
-      out[it.row] = word;
-      if (word) visited[it.row] = (WT)(vis | word);
-      cnt = popc_w(word);
-    }
-  }
-  block_add_u64(cnt, &ctrl->count);
-}
-
-template <int B>
-__global__ void k_sssp_finish(GView v, typename Word<B>::T* __restrict__ front,
-                              typename Word<B>::T* __restrict__ visited, uint32_t* __restrict__ dist,
-                              Ctrl* __restrict__ ctrl, const uint32_t* __restrict__ scratch) {
-  using WT = typename Word<B>::T;
-  if (((volatile Ctrl*)ctrl)->done) return;
-  const int lvl = ((volatile Ctrl*)ctrl)->iter;
-  WT* __restrict__ out = front + (size_t)((lvl + 1) & 1) * v.nbr;
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned long long cnt = 0;
-  if (i < v.nsplit) {
-    const gbo_split sp = v.splits[i];
-    const WT vis = visited[sp.row];
-    WT nw = 0;
-    for (int r = 0; r < B; ++r) {
-      uint32_t a = (uint32_t)kINF;
-      for (int q = 0; q < sp.nslots; ++q) a = min(a, scratch[(size_t)(sp.slot0 + q) * B + r]);
-      const long long row = (long long)sp.row * B + r;
-      if (row < v.nrows && a < dist[row]) {
-        dist[row] = a;
-        nw |= (WT)((WT)1 << (B - 1 - r));
-      }
-    }
-    out[sp.row] = nw;
-    if (nw) visited[sp.row] = (WT)(vis | nw);
-    cnt = popc_w(nw);
-  }
-  block_add_u64(cnt, &ctrl->count);
-  close_iteration(ctrl, [](volatile Ctrl* c, int it) {
-    return c->count == 0ull || it >= c->max_iter;
-  });
-}
-
-template <int B>
-__global__ void k_sssp_init(typename Word<B>::T* front, typename Word<B>::T* visited,
-                            const typename Word<B>::T* __restrict__ live, uint32_t* dist, int nbr,
-                            int n, int src, Ctrl* ctrl, int max_iter) {
-  using WT = typename Word<B>::T;
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long k = i; k < n; k += stride) dist[k] = (k == src) ? 0u : (uint32_t)kINF;
-  for (long long k = i; k < nbr; k += stride) {
-    WT w = (k == src / B) ? (WT)((WT)1 << (B - 1 - src % B)) : (WT)0;
-    front[k] = w;
-    front[nbr + k] = 0;
-    visited[k] = (WT)(w | (~live[k] & full_word<B>()));
-  }
-  if (i == 0) {
-    ctrl->iter = 0;
-    ctrl->done = 0;
-    ctrl->ticket = 0;
-    ctrl->max_iter = max_iter;
-    ctrl->count = 0;
-    ctrl->err = 0;
-    ctrl->last_err = 0;
+// Unit weights: every frontier vertex at iteration k has distance k, so the
+// min-plus relaxation min_j (d[j] + 1) over a row's frontier neighbours is
+// k + 1 as soon as one such neighbour exists.  The SSSP step is therefore
+// the BFS step (pull with early exit, push on small frontiers of symmetric
+// graphs); distances are the levels in uint32 with 2147483647 unreachable.
+__global__ void k_level_to_dist(uint32_t* __restrict__ d, int n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int lv = (int)d[i];
+    d[i] = lv < 0 ? (uint32_t)kINF : (uint32_t)lv;
   }
 }
 
 // ============================================================ PageRank
 // p'[i] = alpha * sum_{j: P[i][j]} p[j] * inv[j] + add + add_scale * v[i].
+// New value of row i from its gathered sum a (fp64): PageRank / PPR forward
+// y = alpha * a + add + add_scale * pv[i], with a = sum of x[j] / deg(j);
+// adjoint on a symmetric P (row_scale) y = pv[i] + alpha * inv[i] * a with
+// a = sum of u[j].  Writes y (and y * inv[i], the next gathered operand, for
+// PageRank) and returns the |change| (or its square for the L2 norm).
+__device__ __forceinline__ double pr_row_update(long long i, double a, const float* __restrict__ x,
+                                                float* __restrict__ y, float* __restrict__ ys,
+                                                const float* __restrict__ inv, const float* __restrict__ pv,
+                                                double alpha, double add, double adds, int norm,
+                                                int row_scale) {
+  const double base = pv ? adds * (double)pv[i] : 0.0;
+  const float yn = row_scale ? (float)(base + alpha * (double)inv[i] * a) : (float)(alpha * a + add + base);
+  y[i] = yn;
+  if (!row_scale) ys[i] = yn * inv[i];
+  const double d = (double)yn - (double)x[i];
+  return norm == 1 ? fabs(d) : d * d;
+}
+
 template <int B>
-__global__ void __launch_bounds__(kTPB) k_pr_step(GView v, float* __restrict__ pr,
+__global__ void __launch_bounds__(kTPB) k_pr_step(GView v, float* __restrict__ pr, float* __restrict__ prs,
                                                   const float* __restrict__ inv,
                                                   const float* __restrict__ pv,
                                                   Ctrl* __restrict__ ctrl, double* __restrict__ scratch) {
-  using WT = typename Word<B>::T;
   using L = Lay<B>;
   if (((volatile Ctrl*)ctrl)->done) return;
   const int itn = ((volatile Ctrl*)ctrl)->iter;
   const double alpha = ctrl->alpha, add = ctrl->add, adds = ctrl->add_scale;
-  const int norm = ctrl->norm;
+  const int norm = ctrl->norm, row_scale = ctrl->row_scale;
   const int n = v.nrows;
   const float* __restrict__ x = pr + (size_t)(itn & 1) * n;
   float* __restrict__ y = pr + (size_t)((itn + 1) & 1) * n;
+  float* __restrict__ ys = prs + (size_t)((itn + 1) & 1) * n;
+  // gathered operand: x / deg (kept up to date by the previous iteration) or x
+  const float* __restrict__ xg = row_scale ? x : prs + (size_t)(itn & 1) * n;
   const unsigned lane = threadIdx.x & 31;
-  const long long item = item_index(lane, L::W, L::G);
   double e = 0.0;
-  if (item < v.nitems) {
-    const int r = lane % L::W;
-    const gbo_item it = v.items[item];
-    const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
-    double a0 = 0.0, a1 = 0.0;
-    for (int t = it.t0; t < it.t1; ++t) {
-      const long long base = (long long)v.colind[t] * B;
-      const WT w0 = val[(size_t)t * B + r];
-      for_each_col<B>(w0, [&](int j) { a0 += (double)(x[base + j] * inv[base + j]); });
-      if (L::RPL == 2) {
-        const WT w1 = val[(size_t)t * B + 32 + r];
-        for_each_col<B>(w1, [&](int j) { a1 += (double)(x[base + j] * inv[base + j]); });
-      }
-    }
-    if (it.slot >= 0) {
-      scratch[(size_t)it.slot * B + r] = a0;
-      if (L::RPL == 2) scratch[(size_t)it.slot * B + 32 + r] = a1;
-    } else {
-      const long long row0 = (long long)it.row * B + r;
-      if (row0 < n) {
-        float yn = (float)(alpha * a0 + add + (pv ? adds * (double)pv[row0] : 0.0));
-        y[row0] = yn;
-        double d = (double)yn - (double)x[row0];
-        e += norm == 1 ? fabs(d) : d * d;
-      }
-      if (L::RPL == 2 && row0 + 32 < n) {
-        float yn = (float)(alpha * a1 + add + (pv ? adds * (double)pv[row0 + 32] : 0.0));
-        y[row0 + 32] = yn;
-        double d = (double)yn - (double)x[row0 + 32];
-        e += norm == 1 ? fabs(d) : d * d;
+  const long long nwarps = warps_total();
+  for (long long w = warp_global(); w * L::G < v.nitems; w += nwarps) {
+    const long long item = w * L::G + lane / L::W;
+    if (item < v.nitems) {
+      const int r = lane % L::W;
+      const gbo_item it = v.items[item];
+      double a0 = 0.0, a1 = 0.0;
+      fold_row_cols<B, 8>(v, it.t0, it.t1, r, [&](long long j) { return (double)xg[j]; },
+                          [](double& a, double b) { a += b; }, a0, a1);
+      if (it.slot >= 0) {
+        scratch[(size_t)it.slot * B + r] = a0;
+        if (L::RPL == 2) scratch[(size_t)it.slot * B + 32 + r] = a1;
+      } else {
+        const long long row0 = (long long)it.row * B + r;
+        if (row0 < n) e += pr_row_update(row0, a0, x, y, ys, inv, pv, alpha, add, adds, norm, row_scale);
+        if (L::RPL == 2 && row0 + 32 < n)
+          e += pr_row_update(row0 + 32, a1, x, y, ys, inv, pv, alpha, add, adds, norm, row_scale);
       }
     }
   }
@@ -601,15 +500,17 @@ __global__ void __launch_bounds__(kTPB) k_pr_step(GView v, float* __restrict__ p
 }
 
 template <int B>
-__global__ void k_pr_finish(GView v, float* __restrict__ pr, const float* __restrict__ pv,
+__global__ void k_pr_finish(GView v, float* __restrict__ pr, float* __restrict__ prs,
+                            const float* __restrict__ inv, const float* __restrict__ pv,
                             Ctrl* __restrict__ ctrl, const double* __restrict__ scratch) {
   if (((volatile Ctrl*)ctrl)->done) return;
   const int itn = ((volatile Ctrl*)ctrl)->iter;
   const double alpha = ctrl->alpha, add = ctrl->add, adds = ctrl->add_scale;
-  const int norm = ctrl->norm;
+  const int norm = ctrl->norm, row_scale = ctrl->row_scale;
   const int n = v.nrows;
   const float* __restrict__ x = pr + (size_t)(itn & 1) * n;
   float* __restrict__ y = pr + (size_t)((itn + 1) & 1) * n;
+  float* __restrict__ ys = prs + (size_t)((itn + 1) & 1) * n;
   const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   double e = 0.0;
   if (gid < (long long)v.nsplit * B) {
@@ -618,28 +519,29 @@ __global__ void k_pr_finish(GView v, float* __restrict__ pr, const float* __rest
     double a = 0.0;
     for (int q = 0; q < sp.nslots; ++q) a += scratch[(size_t)(sp.slot0 + q) * B + r];
     const long long row = (long long)sp.row * B + r;
-    if (row < n) {
-      float yn = (float)(alpha * a + add + (pv ? adds * (double)pv[row] : 0.0));
-      y[row] = yn;
-      double d = (double)yn - (double)x[row];
-      e += norm == 1 ? fabs(d) : d * d;
-    }
+    if (row < n) e += pr_row_update(row, a, x, y, ys, inv, pv, alpha, add, adds, norm, row_scale);
   }
   block_add_f64(e, &ctrl->err);
   close_iteration(ctrl, [](volatile Ctrl* c, int it) {
-    double m = c->norm == 2 ? sqrt(c->err) : c->err;
-    return it >= c->max_iter || (c->tol >= 0.f && m <= (double)c->tol);
+    const double m = c->norm == 2 ? sqrt(c->err) : c->err;
+    const double ref = c->ref > 0.0 ? c->ref : 1.0;  // ||w||_1 for the adjoint, else 1
+    return it >= c->max_iter || (c->tol >= 0.f && m <= (double)c->tol * ref);
   });
 }
 
-__global__ void k_pr_init(float* pr, const float* pv, int n, float init_const, float init_scale,
-                          Ctrl* ctrl, int max_iter, float tol, float alpha, float add,
-                          float add_scale, int norm) {
+__global__ void k_pr_init(float* pr, float* prs, const float* inv, const float* pv, int n,
+                          float init_const, float init_scale, Ctrl* ctrl, int max_iter, float tol,
+                          float alpha, float add, float add_scale, int norm, int row_scale) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long k = i; k < n; k += stride) {
-    pr[k] = init_const + (pv ? init_scale * pv[k] : 0.f);
+    const float x0 = init_const + (pv ? init_scale * pv[k] : 0.f);
+    pr[k] = x0;
     pr[n + k] = 0.f;
+    if (prs) {
+      prs[k] = inv ? x0 * inv[k] : 0.f;
+      prs[n + k] = 0.f;
+    }
   }
   if (i == 0) {
     ctrl->iter = 0;
@@ -655,6 +557,8 @@ __global__ void k_pr_init(float* pr, const float* pv, int n, float init_const, f
     ctrl->add_scale = add_scale;
     ctrl->norm = norm;
     ctrl->n = n;
+    ctrl->ref = 0.0;
+    ctrl->row_scale = row_scale;
   }
 }
 
@@ -678,21 +582,24 @@ __global__ void __launch_bounds__(kTPB) k_adj_scatter(GView v, const float* __re
   const int n = v.nrows;
   const float* __restrict__ u = pr + (size_t)(itn & 1) * n;
   const unsigned lane = threadIdx.x & 31;
-  const long long item = item_index(lane, L::W, L::G);
-  if (item >= v.nitems) return;
-  const int r = lane % L::W;
-  const gbo_item it = v.items[item];
-  const long long row0 = (long long)it.row * B + r;
-  const float u0 = row0 < n ? u[row0] : 0.f;
-  const float u1 = (L::RPL == 2 && row0 + 32 < n) ? u[row0 + 32] : 0.f;
-  if (u0 == 0.f && u1 == 0.f) return;
-  const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
-  for (int t = it.t0; t < it.t1; ++t) {
-    const long long base = (long long)v.colind[t] * B;
-    if (u0 != 0.f)
-      for_each_col<B>(val[(size_t)t * B + r], [&](int j) { atomicAdd(acc + base + j, (double)u0); });
-    if (L::RPL == 2 && u1 != 0.f)
-      for_each_col<B>(val[(size_t)t * B + 32 + r], [&](int j) { atomicAdd(acc + base + j, (double)u1); });
+  const long long nwarps = warps_total();
+  for (long long w = warp_global(); w * L::G < v.nitems; w += nwarps) {
+    const long long item = w * L::G + lane / L::W;
+    if (item >= v.nitems) continue;
+    const int r = lane % L::W;
+    const gbo_item it = v.items[item];
+    const long long row0 = (long long)it.row * B + r;
+    const float u0 = row0 < n ? u[row0] : 0.f;
+    const float u1 = (L::RPL == 2 && row0 + 32 < n) ? u[row0 + 32] : 0.f;
+    if (u0 == 0.f && u1 == 0.f) continue;
+    const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
+    for (int t = it.t0; t < it.t1; ++t) {
+      const long long base = (long long)v.colind[t] * B;
+      if (u0 != 0.f)
+        for_each_col<B>(val[(size_t)t * B + r], [&](int j) { atomicAdd(acc + base + j, (double)u0); });
+      if (L::RPL == 2 && u1 != 0.f)
+        for_each_col<B>(val[(size_t)t * B + 32 + r], [&](int j) { atomicAdd(acc + base + j, (double)u1); });
+    }
   }
 }
 
@@ -713,8 +620,19 @@ __global__ void k_adj_apply(float* __restrict__ pr, const float* __restrict__ w,
   }
   block_add_f64(e, &ctrl->err);
   close_iteration(ctrl, [](volatile Ctrl* c, int it) {
-    return it >= c->max_iter || (c->tol >= 0.f && c->err <= (double)c->tol);
+    // relative test: w is any real vector, not a distribution
+    const double ref = c->ref > 0.0 ? c->ref : 1.0;
+    return it >= c->max_iter || (c->tol >= 0.f && c->err <= (double)c->tol * ref);
   });
+}
+
+// ||w||_1 into ctrl->ref (after k_pr_init zeroed it).
+__global__ void k_l1_ref(const float* __restrict__ w, int n, Ctrl* __restrict__ ctrl) {
+  double e = 0.0;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x)
+    e += fabs((double)w[k]);
+  block_add_f64(e, &ctrl->ref);
 }
 
 __global__ void k_scale_copy(const float* __restrict__ src, float* __restrict__ dst, int n, float s) {
@@ -734,25 +652,24 @@ __global__ void __launch_bounds__(kTPB) k_cc_mngf(GView v, const int* __restrict
   using L = Lay<B>;
   if (((volatile Ctrl*)ctrl)->done) return;
   const unsigned lane = threadIdx.x & 31;
-  const long long item = item_index(lane, L::W, L::G);
-  if (item >= v.nitems) return;
-  const int r = lane % L::W;
-  const gbo_item it = v.items[item];
-  const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
-  int a0 = kINF, a1 = kINF;
-  for (int t = it.t0; t < it.t1; ++t) {
-    const long long base = (long long)v.colind[t] * B;
-    for_each_col<B>(val[(size_t)t * B + r], [&](int j) { a0 = min(a0, gf[base + j]); });
-    if (L::RPL == 2) for_each_col<B>(val[(size_t)t * B + 32 + r], [&](int j) { a1 = min(a1, gf[base + j]); });
+  const long long nwarps = warps_total();
+  for (long long w = warp_global(); w * L::G < v.nitems; w += nwarps) {
+    const long long item = w * L::G + lane / L::W;
+    if (item >= v.nitems) continue;
+    const int r = lane % L::W;
+    const gbo_item it = v.items[item];
+    int a0 = kINF, a1 = kINF;
+    fold_row_cols<B, 4>(v, it.t0, it.t1, r, [&](long long j) { return gf[j]; },
+                        [](int& a, int b) { a = min(a, b); }, a0, a1);
+    if (it.slot >= 0) {
+      scratch[(size_t)it.slot * B + r] = a0;
+      if (L::RPL == 2) scratch[(size_t)it.slot * B + 32 + r] = a1;
+      continue;
+    }
+    const long long row0 = (long long)it.row * B + r;
+    if (row0 < v.nrows && a0 < mngf[row0]) mngf[row0] = a0;
+    if (L::RPL == 2 && row0 + 32 < v.nrows && a1 < mngf[row0 + 32]) mngf[row0 + 32] = a1;
   }
-  if (it.slot >= 0) {
-    scratch[(size_t)it.slot * B + r] = a0;
-    if (L::RPL == 2) scratch[(size_t)it.slot * B + 32 + r] = a1;
-    return;
-  }
-  const long long row0 = (long long)it.row * B + r;
-  if (row0 < v.nrows && a0 < mngf[row0]) mngf[row0] = a0;
-  if (L::RPL == 2 && row0 + 32 < v.nrows && a1 < mngf[row0 + 32]) mngf[row0 + 32] = a1;
 }
 
 template <int B>
@@ -832,6 +749,28 @@ unsigned grid_for_items(int nitems, int b) {
   return blocks_for_warps(warps, kTPB / 32);
 }
 
+// Persistent grid of an iteration kernel: enough warps for every item, and
+// no more blocks than stay resident together (the kernels loop over items,
+// so a second wave would only lengthen the tail).
+template <typename K>
+unsigned grid_persistent(K kernel, long long warps) {
+  const unsigned g = blocks_for_warps(warps, kTPB / 32);
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTPB, 0) != cudaSuccess || per_sm < 1) {
+    (void)cudaGetLastError();
+    per_sm = 1;
+  }
+  const unsigned cap = (unsigned)num_sms() * (unsigned)per_sm;
+  return g < cap ? g : cap;
+}
+
+// Same, for a kernel that gives each work item min(b, 32) lanes.
+template <typename K>
+unsigned grid_items_persistent(K kernel, int nitems, int b) {
+  const int G = b >= 32 ? 1 : 32 / b;
+  return grid_persistent(kernel, ((long long)nitems + G - 1) / G);
+}
+
 unsigned grid_vertex(long long n) {
   unsigned g = blocks_for(n, kTPB);
   unsigned cap = (unsigned)num_sms() * 8u;
@@ -875,6 +814,31 @@ int ensure_frontier(gbo_graph* g, AlgoState* a, cudaStream_t s) {
       }
       GBO_CUDA_TRY(cudaGetLastError());
     }
+  }
+  return GBO_OK;
+}
+
+}  // namespace
+
+int live_rows(gbo_graph* g, cudaStream_t s, const void** out) {
+  AlgoState* a = nullptr;
+  GBO_TRY(get_state(g, &a));
+  GBO_TRY(ensure_frontier(g, a, s));
+  *out = a->live;
+  return GBO_OK;
+}
+
+namespace {
+
+int ensure_pr_vectors(gbo_graph* g, AlgoState* a) {
+  const size_t n = (size_t)(g->nrows > 0 ? g->nrows : 1);
+  if (!a->pr) {
+    GBO_CUDA_TRY(cudaMalloc(&a->pr, sizeof(float) * 2 * n));
+    g->device_bytes += 8LL * g->nrows;
+  }
+  if (!a->prs) {
+    GBO_CUDA_TRY(cudaMalloc(&a->prs, sizeof(float) * 2 * n));
+    g->device_bytes += 8LL * g->nrows;
   }
   return GBO_OK;
 }
@@ -978,11 +942,11 @@ int bfs_impl(gbo_graph* g, int src, const int* h_seeds, int nseeds, int32_t* d_l
   Ctrl* ctrl = a->ctrl;
   int* level = a->level;
   WT* scratch = (WT*)a->scratch;
-  const unsigned gi = grid_for_items(g->nitems, B);
+  const unsigned gi = grid_items_persistent(k_bfs_step<B>, g->nitems, B);
   // push steps (symmetric graphs) finalise every block row in k_bfs_finish
   const bool push_ok = g->symmetric;
   const unsigned gs = blocks_for(std::max<long long>(g->nsplit, push_ok ? g->nbr : 0), kTPB);
-  const unsigned gp = blocks_for_warps(g->nitems, kTPB / 32);
+  const unsigned gp = grid_persistent(k_bfs_push<B>, g->nitems);
   const unsigned gc = grid_vertex(g->nbr);
   GBO_TRY(get_exec(a, A_BFS, nullptr, [&](cudaStream_t cs, int k, int* nl) -> int {
     StepTimer tm{a, cs, k};
@@ -1026,40 +990,9 @@ int bfs_impl(gbo_graph* g, int src, const int* h_seeds, int nseeds, int32_t* d_l
 
 template <int B>
 int sssp_impl(gbo_graph* g, int src, uint32_t* d_dist, int* h_iters, cudaStream_t s) {
-  using WT = typename Word<B>::T;
-  AlgoState* a = nullptr;
-  GBO_TRY(get_state(g, &a));
-  GBO_TRY(ensure_frontier(g, a, s));
-  if (!a->dist) {
-    GBO_CUDA_TRY(cudaMalloc(&a->dist, sizeof(uint32_t) * (size_t)(g->nrows > 0 ? g->nrows : 1)));
-    g->device_bytes += 4LL * g->nrows;
-  }
-  GView v = view_of(g);
-  WT* front = (WT*)a->front;
-  WT* vis = (WT*)a->visited;
-  Ctrl* ctrl = a->ctrl;
-  uint32_t* dist = a->dist;
-  uint32_t* scratch = (uint32_t*)a->scratch;
-  const unsigned gi = grid_for_items(g->nitems, B);
-  const unsigned gs = blocks_for(g->nsplit, kTPB);
-  GBO_TRY(get_exec(a, A_SSSP, nullptr, [&](cudaStream_t cs, int k, int* nl) -> int {
-    StepTimer tm{a, cs, k};
-    tm.begin();
-    if (g->nitems > 0) k_sssp_step<B><<<gi, kTPB, 0, cs>>>(v, front, vis, dist, ctrl, scratch);
-    tm.end();
-    k_sssp_finish<B><<<gs, kTPB, 0, cs>>>(v, front, vis, dist, ctrl, scratch);
-    *nl += (g->nitems > 0) + 1;
-    GBO_CUDA_TRY(cudaGetLastError());
-    return GBO_OK;
-  }));
-  const int max_iter = g->nrows + 1;
-  k_sssp_init<B><<<grid_vertex(std::max(g->nrows, g->nbr)), kTPB, 0, s>>>(
-      front, vis, (const WT*)a->live, dist, g->nbr, g->nrows, src, ctrl, max_iter);
+  GBO_TRY(bfs_impl<B>(g, src, nullptr, 0, reinterpret_cast<int32_t*>(d_dist), h_iters, s));
+  if (g->nrows > 0) k_level_to_dist<<<grid_vertex(g->nrows), kTPB, 0, s>>>(d_dist, g->nrows);
   GBO_CUDA_TRY(cudaGetLastError());
-  GBO_TRY(run_until_done(a, A_SSSP, s, max_iter, h_iters));
-  if (g->nrows > 0)
-    GBO_CUDA_TRY(cudaMemcpyAsync(d_dist, dist, sizeof(uint32_t) * (size_t)g->nrows,
-                                 cudaMemcpyDeviceToDevice, s));
   return GBO_OK;
 }
 
@@ -1070,29 +1003,27 @@ int pr_impl(gbo_graph* g, const float* d_v, float alpha, int max_iter, float tol
             int id, cudaStream_t s) {
   AlgoState* a = nullptr;
   GBO_TRY(get_state(g, &a));
-  if (!a->pr) {
-    GBO_CUDA_TRY(cudaMalloc(&a->pr, sizeof(float) * 2 * (size_t)(g->nrows > 0 ? g->nrows : 1)));
-    g->device_bytes += 8LL * g->nrows;
-  }
+  GBO_TRY(ensure_pr_vectors(g, a));
   GView v = view_of(g);
   float* pr = a->pr;
+  float* prs = a->prs;
   const float* inv = g->invdeg;
   Ctrl* ctrl = a->ctrl;
   double* scratch = (double*)a->scratch;
-  const unsigned gi = grid_for_items(g->nitems, B);
+  const unsigned gi = grid_items_persistent(k_pr_step<B>, g->nitems, B);
   const unsigned gs = blocks_for((long long)g->nsplit * B, kTPB);
   GBO_TRY(get_exec(a, id, d_v, [&](cudaStream_t cs, int k, int* nl) -> int {
     StepTimer tm{a, cs, k};
     tm.begin();
-    if (g->nitems > 0) k_pr_step<B><<<gi, kTPB, 0, cs>>>(v, pr, inv, d_v, ctrl, scratch);
+    if (g->nitems > 0) k_pr_step<B><<<gi, kTPB, 0, cs>>>(v, pr, prs, inv, d_v, ctrl, scratch);
     tm.end();
-    k_pr_finish<B><<<gs, kTPB, 0, cs>>>(v, pr, d_v, ctrl, scratch);
+    k_pr_finish<B><<<gs, kTPB, 0, cs>>>(v, pr, prs, inv, d_v, ctrl, scratch);
     *nl += (g->nitems > 0) + 1;
     GBO_CUDA_TRY(cudaGetLastError());
     return GBO_OK;
   }));
-  k_pr_init<<<grid_vertex(g->nrows), kTPB, 0, s>>>(pr, d_v, g->nrows, init_const, init_scale, ctrl,
-                                                  max_iter, tol, alpha, add, add_scale, norm);
+  k_pr_init<<<grid_vertex(g->nrows), kTPB, 0, s>>>(pr, prs, inv, d_v, g->nrows, init_const, init_scale,
+                                                  ctrl, max_iter, tol, alpha, add, add_scale, norm, 0);
   GBO_CUDA_TRY(cudaGetLastError());
   int iters = 0;
   if (max_iter > 0) GBO_TRY(run_until_done(a, id, s, max_iter, &iters));
@@ -1108,9 +1039,41 @@ int ppr_backward_impl(gbo_graph* g, const float* d_w, float alpha, float tol, in
                       float* d_grad, int* h_iters, cudaStream_t s) {
   AlgoState* a = nullptr;
   GBO_TRY(get_state(g, &a));
-  if (!a->pr) {
-    GBO_CUDA_TRY(cudaMalloc(&a->pr, sizeof(float) * 2 * (size_t)(g->nrows > 0 ? g->nrows : 1)));
-    g->device_bytes += 8LL * g->nrows;
+  GBO_TRY(ensure_pr_vectors(g, a));
+  const int n = g->nrows;
+  const unsigned gv = grid_vertex(n);
+  int iters = 0;
+  if (g->symmetric) {
+    // P^T = P: u' = w + alpha * D^-1 P u is a gather over P's rows (the
+    // PageRank step with the scale on rows), no scatter atomics
+    float* pr = a->pr;
+    float* prs = a->prs;
+    const float* inv = g->invdeg;
+    Ctrl* ctrl = a->ctrl;
+    double* scratch = (double*)a->scratch;
+    GView v = view_of(g);
+    const unsigned gi = grid_items_persistent(k_pr_step<B>, g->nitems, B);
+    const unsigned gs = blocks_for((long long)g->nsplit * B, kTPB);
+    GBO_TRY(get_exec(a, A_PPR_BG, d_w, [&](cudaStream_t cs, int k, int* nl) -> int {
+      StepTimer tm{a, cs, k};
+      tm.begin();
+      if (g->nitems > 0) k_pr_step<B><<<gi, kTPB, 0, cs>>>(v, pr, prs, inv, d_w, ctrl, scratch);
+      tm.end();
+      k_pr_finish<B><<<gs, kTPB, 0, cs>>>(v, pr, prs, inv, d_w, ctrl, scratch);
+      *nl += (g->nitems > 0) + 1;
+      GBO_CUDA_TRY(cudaGetLastError());
+      return GBO_OK;
+    }));
+    // u0 = w; y = w + alpha * inv * (P u)
+    k_pr_init<<<gv, kTPB, 0, s>>>(pr, nullptr, nullptr, d_w, n, 0.f, 1.f, ctrl, max_iter, tol, alpha,
+                                  0.f, 1.f, 1, 1);
+    k_l1_ref<<<gv, kTPB, 0, s>>>(d_w, n, ctrl);
+    GBO_CUDA_TRY(cudaGetLastError());
+    if (max_iter > 0) GBO_TRY(run_until_done(a, A_PPR_BG, s, max_iter, &iters));
+    if (n > 0) k_scale_copy<<<gv, kTPB, 0, s>>>(pr + (size_t)(iters & 1) * n, d_grad, n, 1.f - alpha);
+    GBO_CUDA_TRY(cudaGetLastError());
+    if (h_iters) *h_iters = iters;
+    return GBO_OK;
   }
   if (!a->acc64) {
     GBO_CUDA_TRY(cudaMalloc(&a->acc64, sizeof(double) * (size_t)(g->nrows > 0 ? g->nrows : 1)));
@@ -1121,9 +1084,7 @@ int ppr_backward_impl(gbo_graph* g, const float* d_w, float alpha, float tol, in
   double* acc = a->acc64;
   const float* inv = g->invdeg;
   Ctrl* ctrl = a->ctrl;
-  const int n = g->nrows;
-  const unsigned gi = grid_for_items(g->nitems, B);
-  const unsigned gv = grid_vertex(n);
+  const unsigned gi = grid_items_persistent(k_adj_scatter<B>, g->nitems, B);
   GBO_TRY(get_exec(a, A_PPR_B, d_w, [&](cudaStream_t cs, int k, int* nl) -> int {
     StepTimer tm{a, cs, k};
     k_adj_prep<<<gv, kTPB, 0, cs>>>(pr, d_w, n, ctrl, acc);
@@ -1136,9 +1097,10 @@ int ppr_backward_impl(gbo_graph* g, const float* d_w, float alpha, float tol, in
     return GBO_OK;
   }));
   // u0 = w
-  k_pr_init<<<gv, kTPB, 0, s>>>(pr, d_w, n, 0.f, 1.f, ctrl, max_iter, tol, alpha, 0.f, 0.f, 1);
+  k_pr_init<<<gv, kTPB, 0, s>>>(pr, nullptr, nullptr, d_w, n, 0.f, 1.f, ctrl, max_iter, tol, alpha, 0.f,
+                                0.f, 1, 0);
+  k_l1_ref<<<gv, kTPB, 0, s>>>(d_w, n, ctrl);
   GBO_CUDA_TRY(cudaGetLastError());
-  int iters = 0;
   if (max_iter > 0) GBO_TRY(run_until_done(a, A_PPR_B, s, max_iter, &iters));
   if (n > 0) k_scale_copy<<<gv, kTPB, 0, s>>>(pr + (size_t)(iters & 1) * n, d_grad, n, 1.f - alpha);
   GBO_CUDA_TRY(cudaGetLastError());
@@ -1158,7 +1120,7 @@ int cc_impl(gbo_graph* g, int32_t* d_label, int* h_iters, cudaStream_t s) {
   Ctrl* ctrl = a->ctrl;
   int* scratch = (int*)a->scratch;
   const int n = g->nrows;
-  const unsigned gi = grid_for_items(g->nitems, B);
+  const unsigned gi = grid_items_persistent(k_cc_mngf<B>, g->nitems, B);
   const unsigned gs = blocks_for((long long)g->nsplit * B, kTPB);
   const unsigned gv = grid_vertex(n);
   GBO_TRY(get_exec(a, A_CC, nullptr, [&](cudaStream_t cs, int k, int* nl) -> int {
@@ -1207,6 +1169,7 @@ void free_algo_state(gbo_graph* g) {
   cudaFree(a->level);
   cudaFree(a->dist);
   cudaFree(a->pr);
+  cudaFree(a->prs);
   cudaFree(a->f);
   cudaFree(a->gf);
   cudaFree(a->mngf);

@@ -260,25 +260,15 @@ __global__ void __launch_bounds__(kTPB) k_semiring(GView v, const typename SRT<S
   if (item >= v.nitems) return;
   const int r = lane % L::W;
   const gbo_item it = v.items[item];
-  const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
   A acc0 = sr_identity<SR>(), acc1 = sr_identity<SR>();
-  for (int t = it.t0; t < it.t1; ++t) {
-    const long long base = (long long)v.colind[t] * B;
-    const WT w0 = val[(size_t)t * B + r];
-    if (SR == SR_FLOAT && p.degptr) {
-      for_each_col<B>(w0, [&](int j) { acc0 += (A)float_term_deg((const float*)x, p.degptr, base + j); });
-      if (L::RPL == 2) {
-        const WT w1 = val[(size_t)t * B + 32 + r];
-        for_each_col<B>(w1, [&](int j) { acc1 += (A)float_term_deg((const float*)x, p.degptr, base + j); });
-      }
-      continue;
-    }
-    for_each_col<B>(w0, [&](int j) { sr_combine<SR>(acc0, sr_term<SR>(x, p.scale, base + j)); });
-    if (L::RPL == 2) {
-      const WT w1 = val[(size_t)t * B + 32 + r];
-      for_each_col<B>(w1, [&](int j) { sr_combine<SR>(acc1, sr_term<SR>(x, p.scale, base + j)); });
-    }
-  }
+  auto comb = [](A& a, A b) { sr_combine<SR>(a, b); };
+  if (SR == SR_FLOAT && p.degptr)
+    fold_row_cols<B, 4>(v, it.t0, it.t1, r,
+                        [&](long long j) { return (A)float_term_deg((const float*)x, p.degptr, j); },
+                        comb, acc0, acc1);
+  else
+    fold_row_cols<B, 4>(v, it.t0, it.t1, r, [&](long long j) { return sr_term<SR>(x, p.scale, j); },
+                        comb, acc0, acc1);
   if (it.slot >= 0) {
     scratch[(size_t)it.slot * B + r] = acc0;
     if (L::RPL == 2) scratch[(size_t)it.slot * B + 32 + r] = acc1;

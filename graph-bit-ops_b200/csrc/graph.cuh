@@ -69,6 +69,9 @@ int ensure_workspace(gbo_graph* g, size_t bytes, cudaStream_t stream);
 
 // Pack CSR (device pointers) into B2SR owned by g.  Sets nblk, rowptr, colind,
 // val.  Synchronises the stream once (to size the tile arrays).
+// Per block row, the rows of P that have an entry (bit b-1-r of word R),
+// computed once per graph on `s` and owned by the graph's algorithm state.
+int live_rows(gbo_graph* g, cudaStream_t s, const void** out);
 int count_tiles(const int* d_rowptr, const int* d_colind, int nrows, int ncols, long long nnz, int b,
                 long long* nblk, cudaStream_t s);
 int pack_into(gbo_graph* g, const int* d_rowptr, const int* d_colind, int nrows, int ncols,

@@ -36,6 +36,9 @@ struct Args {
   int* ctl;  // iter, done, ticket, max_iter, count (u64 at ctl + 4)
   uint32_t* scratch;
   uint32_t* slot_any;  // optional: OR of the new bits of every source word
+  const uint32_t* live;  // optional: rows of P with an entry (others can never be reached)
+  const uint32_t* active;  // optional: source columns still traversing (kw words); a row
+                           // counts as finished once every active column reached it
   int level_group;     // 0: levels[i*k + s]; g > 0: levels[((s/g)*n + i)*g + s%g]
 };
 
@@ -70,6 +73,7 @@ __device__ __forceinline__ void block_row_epilogue(const Args& a, int R, int lvl
   const unsigned wmask = seg_mask<KW>();
   uint32_t* Fn = a.F + (size_t)((lvl + 1) & 1) * a.fstride;
   uint32_t fword = 0, vword = vrow;
+  const uint32_t need = src_mask(w, a.k) & (a.active ? a.active[w] : 0xffffffffu);
   for (int rr = 0; rr < 32; rr += S) {
     const int r = rr + s;
     const int i = R * 32 + r;
@@ -83,7 +87,7 @@ __device__ __forceinline__ void block_row_epilogue(const Args& a, int R, int lvl
       vn = vo | nw;
     }
     const unsigned bnew = __ballot_sync(0xffffffffu, nw != 0);
-    const unsigned bfull = __ballot_sync(0xffffffffu, !open || vn == src_mask(w, a.k));
+    const unsigned bfull = __ballot_sync(0xffffffffu, !open || (vn & need) == need);
     const bool rowany = ((bnew >> (s * KW)) & wmask) != 0;
     if (open && rowany) Fn[o] = nw;  // only rows marked in fbits are ever read
     if (nw) {
@@ -306,7 +310,9 @@ __global__ void __launch_bounds__(kTPB) k_finish(Args a) {
   }
 }
 
-// Reset: levels -1, V 0, F[0] 0, frontier bits 0, padding rows marked full.
+// Reset: levels -1, V 0, F[0] 0, frontier bits 0, padding rows and rows
+// without entries marked full (no source can reach them).  A source in such
+// a row reopens it in k_seed.
 static __global__ void k_init(Args a, int kw, int max_iter) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -322,6 +328,7 @@ static __global__ void k_init(Args a, int kw, int max_iter) {
     uint32_t pad = 0;
     for (int r = 0; r < 32; ++r)
       if (lo + r >= n) pad |= 1u << (31 - r);
+    if (a.live && q < nbr) pad |= ~a.live[q];
     a.vfull[q] = pad;
   }
   if (i == 0) {
@@ -333,24 +340,43 @@ static __global__ void k_init(Args a, int kw, int max_iter) {
   }
 }
 
-// Sources of the level-0 frontier (one thread: sources may share words).
-static __global__ void k_seed(Args a, const int* __restrict__ srcs, const int* __restrict__ slots,
-                              int nsrc, int kw, int lvl) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+// Sources entering the frontier of level lvl, one thread per source (two
+// kernels, so that every row is cleared before any source bit is set):
+// a row that is not in the frontier yet has stale words, cleared first.
+static __global__ void k_seed_clear(Args a, const int* __restrict__ srcs, int nsrc, int kw, int lvl) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nsrc) return;
+  const int v0 = srcs[q];
+  if (v0 < 0 || v0 >= a.v.nrows) return;
+  const uint32_t* fb = a.fbits + (size_t)(lvl & 1) * (a.v.nbr + 1);
+  uint32_t* F = a.F + (size_t)(lvl & 1) * a.fstride;
+  if (!((fb[v0 / 32] >> (31 - v0 % 32)) & 1u))
+    for (int w = 0; w < kw; ++w) F[(size_t)v0 * kw + w] = 0u;
+}
+
+static __global__ void k_seed_set(Args a, const int* __restrict__ srcs, const int* __restrict__ slots,
+                                  int nsrc, int kw, int lvl) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nsrc) return;
+  const int v0 = srcs[q];
+  const int s = slots ? slots[q] : q;
+  if (v0 < 0 || v0 >= a.v.nrows) return;
   uint32_t* F = a.F + (size_t)(lvl & 1) * a.fstride;
   uint32_t* fb = a.fbits + (size_t)(lvl & 1) * (a.v.nbr + 1);
-  for (int q = 0; q < nsrc; ++q) {
-    const int v0 = srcs[q];
-    const int s = slots ? slots[q] : q;
-    if (v0 < 0 || v0 >= a.v.nrows) continue;
-    if (!((fb[v0 / 32] >> (31 - v0 % 32)) & 1u))  // first time this row enters: clear it
-      for (int w = 0; w < kw; ++w) F[(size_t)v0 * kw + w] = 0u;
-    F[(size_t)v0 * kw + s / 32] |= 1u << (s % 32);
-    a.V[(size_t)v0 * kw + s / 32] |= 1u << (s % 32);
-    a.levels[level_index(a, v0, s)] = lvl;
-    fb[v0 / 32] |= 1u << (31 - v0 % 32);
-    a.vfull[v0 / 32] &= ~(1u << (31 - v0 % 32));
-  }
+  atomicOr(F + (size_t)v0 * kw + s / 32, 1u << (s % 32));
+  atomicOr(a.V + (size_t)v0 * kw + s / 32, 1u << (s % 32));
+  a.levels[level_index(a, v0, s)] = lvl;
+  atomicOr(fb + v0 / 32, 1u << (31 - v0 % 32));
+  atomicAnd(a.vfull + v0 / 32, ~(1u << (31 - v0 % 32)));
+}
+
+// Both seeding kernels on stream st.
+static inline void seed_sources(const Args& a, const int* srcs, const int* slots, int nsrc, int kw, int lvl,
+                                cudaStream_t st) {
+  if (nsrc <= 0) return;
+  const unsigned g = (unsigned)((nsrc + 255) / 256);
+  k_seed_clear<<<g, 256, 0, st>>>(a, srcs, nsrc, kw, lvl);
+  k_seed_set<<<g, 256, 0, st>>>(a, srcs, slots, nsrc, kw, lvl);
 }
 
 }  // namespace ms

@@ -30,6 +30,7 @@ struct MsState {
   int* srcs = nullptr;
   int* ctl = nullptr;
   int* h_ctl = nullptr;
+  const uint32_t* live = nullptr;  // owned by the graph's algorithm state
   int kw = 0;
   int ksrc = 0;
   cudaStream_t cap = nullptr;
@@ -55,6 +56,8 @@ ms::Args make_args(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
   a.ctl = m.ctl;
   a.scratch = m.scratch;
   a.slot_any = nullptr;
+  a.active = nullptr;
+  a.live = m.live;
   a.level_group = 0;  // the API's vertex-major levels[v * k + s]
   return a;
 }
@@ -98,6 +101,11 @@ int msbfs_impl(gbo_graph* g, const int* h_srcs, int k, int32_t* d_levels, int* h
     GBO_CUDA_TRY(cudaMalloc(&m.vfull, sizeof(uint32_t) * (size_t)(g->nbr + 1)));
     for (auto& e : m.ev) GBO_CUDA_TRY(cudaEventCreate(&e));
   }
+  if (!m.live) {
+    const void* lv = nullptr;
+    GBO_TRY(live_rows(g, s, &lv));
+    m.live = static_cast<const uint32_t*>(lv);
+  }
   if (kw != m.kw) {  // state sized for exactly kw words per vertex
     if (m.exec) cudaGraphExecDestroy(m.exec);
     m.exec = nullptr;
@@ -138,10 +146,10 @@ int msbfs_impl(gbo_graph* g, const int* h_srcs, int k, int32_t* d_levels, int* h
   unsigned gv = blocks_for((long long)n * k, 256);
   if (gv > (unsigned)num_sms() * 16u) gv = (unsigned)num_sms() * 16u;
   ms::k_init<<<gv, 256, 0, s>>>(a, kw, max_iter);
-  ms::k_seed<<<1, 32, 0, s>>>(a, m.srcs, nullptr, k, kw, 0);
+  ms::seed_sources(a, m.srcs, nullptr, k, kw, 0, s);
   GBO_CUDA_TRY(cudaGetLastError());
   m.step_ms.clear();
-  m.launches = 2;
+  m.launches = 3;
   int it0 = 0;
   const long long max_launch = (long long)max_iter / kLevelsPerGraph + 2;
   bool done = false;

@@ -2,6 +2,8 @@
 // work item and the batched Boolean (OR.AND) scan of a block row.
 #pragma once
 
+#include <type_traits>
+
 #include "bmv.cuh"
 
 namespace gbo {
@@ -36,7 +38,7 @@ __device__ __forceinline__ WT shfl_word(unsigned mask, WT v, int src, int width)
 // once it has one, and the group leaves the row as soon as all its rows are
 // answered.  Block-column indices are read W at a time (one coalesced load),
 // their x words gathered in parallel, and only tiles with a non-empty x
-// segment are fetched, four tile words in flight per lane.
+// segment are fetched, U tile words in flight per lane.
 template <int B>
 __device__ __forceinline__ void pull_or_scan(const GView& v, int t0, int t1,
                                              const typename Word<B>::T* __restrict__ x,
@@ -50,12 +52,16 @@ __device__ __forceinline__ void pull_or_scan(const GView& v, int t0, int t1,
   const unsigned gshift = (lane / W) * W;
   const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
   constexpr int U = 8;  // tile words in flight per lane
-  // the next batch's block-column indices are loaded while this batch runs
-  int cnext = (t0 + r < t1) ? v.colind[t0 + r] : -1;
+  // Software pipeline over batches of W tiles: while batch i's tile words
+  // load, batch i+1's x words and batch i+2's block-column indices are in
+  // flight, so only the tile loads sit on the critical path.
+  int c1 = (t0 + r < t1) ? v.colind[t0 + r] : -1;
+  int c2 = (t0 + W + r < t1) ? v.colind[t0 + W + r] : -1;
+  WT x1 = c1 >= 0 ? x[c1] : (WT)0;
   for (int base = t0; base < t1; base += W) {
-    const int cb = cnext;
-    cnext = (base + W + r < t1) ? v.colind[base + W + r] : -1;
-    const WT xs = cb >= 0 ? x[cb] : (WT)0;
+    const WT xs = x1;
+    x1 = c2 >= 0 ? x[c2] : (WT)0;
+    c2 = (base + 2 * W + r < t1) ? v.colind[base + 2 * W + r] : -1;
     unsigned nz = (__ballot_sync(gmask, xs != 0) >> gshift) & seg_mask<W>();
     while (nz) {
       int j[U];
@@ -88,6 +94,78 @@ __device__ __forceinline__ void pull_or_scan(const GView& v, int t0, int t1,
     }
     const bool open = (need0 && !p0) || (L::RPL == 2 && need1 && !p1);
     if (!__any_sync(gmask, open)) break;
+  }
+}
+
+// Fold term(column) over the set columns of this lane's row words in tiles
+// [t0, t1) (row r, and r + 32 for b = 64), for semirings whose value comes
+// from a gather at the column (x[j], dist[j], labels[j] ...).  U tiles per
+// step: their block-column indices and row words are loaded together, then
+// the first set column of every word is gathered together (U or 2U
+// independent loads in flight); further set columns of a word (rare in
+// sparse tiles) follow one at a time.  term(idx) returns the value at global
+// column idx; comb(acc, value) folds it into acc.  Words are left-aligned
+// in 32 bits for b <= 32 (64 for b = 64) so that column 0 is the top bit.
+template <int B, int U, typename Acc, typename Term, typename Comb>
+__device__ __forceinline__ void fold_row_cols(const GView& v, int t0, int t1, int r, Term term,
+                                              Comb comb, Acc& acc0, Acc& acc1) {
+  using WT = typename Word<B>::T;
+  using L = Lay<B>;
+  using T = decltype(term(0ll));
+  using AW = typename std::conditional<(B > 32), unsigned long long, unsigned>::type;
+  constexpr int kBits = sizeof(AW) * 8;
+  constexpr AW kTop = (AW)1 << (kBits - 1);
+  const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
+  auto lead = [](AW a) -> int { return kBits == 64 ? __clzll((long long)a) : __clz((int)a); };
+  auto rest = [&](AW a, long long base, Acc& acc) {
+    while (a) {
+      const int j = lead(a);
+      a &= ~(kTop >> j);
+      comb(acc, term(base + j));
+    }
+  };
+  int t = t0;
+  for (; t + U <= t1; t += U) {
+    long long base[U];
+    AW a0[U], a1[U];
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      base[k] = (long long)v.colind[t + k] * B;
+      a0[k] = (AW)val[(size_t)(t + k) * B + r] << (kBits - B);
+      a1[k] = L::RPL == 2 ? (AW)val[(size_t)(t + k) * B + 32 + r] << (kBits - B) : (AW)0;
+    }
+    T g0[U], g1[U];
+    bool h0[U], h1[U];
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      h0[k] = a0[k] != 0;
+      h1[k] = L::RPL == 2 && a1[k] != 0;
+      if (h0[k]) {
+        const int j = lead(a0[k]);
+        a0[k] &= ~(kTop >> j);
+        g0[k] = term(base[k] + j);
+      }
+      if (h1[k]) {
+        const int j = lead(a1[k]);
+        a1[k] &= ~(kTop >> j);
+        g1[k] = term(base[k] + j);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      if (h0[k]) comb(acc0, g0[k]);
+      if (h1[k]) comb(acc1, g1[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      rest(a0[k], base[k], acc0);
+      if (L::RPL == 2) rest(a1[k], base[k], acc1);
+    }
+  }
+  for (; t < t1; ++t) {
+    const long long base = (long long)v.colind[t] * B;
+    rest((AW)val[(size_t)t * B + r] << (kBits - B), base, acc0);
+    if (L::RPL == 2) rest((AW)val[(size_t)t * B + 32 + r] << (kBits - B), base, acc1);
   }
 }
 

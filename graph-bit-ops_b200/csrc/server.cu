@@ -15,6 +15,8 @@
 
 #include <chrono>
 #include <condition_variable>
+#include <algorithm>
+#include <atomic>
 #include <deque>
 #include <map>
 #include <mutex>
@@ -66,26 +68,77 @@ __global__ void __launch_bounds__(kPprTPB) k_ppr_step(PprArgs a) {
     __syncwarp();
     const gbo_item it = v.items[item];
     const uint32_t* __restrict__ val = reinterpret_cast<const uint32_t*>(v.val);
+    // kU tile words per lane (lane = tile row) load together; the set bits
+    // (tile row r, column j) of those tiles are then walked in order and
+    // their X rows (lane = slot) gathered kP at a time.
+    constexpr int kU = 8, kP = 8;
     for (int b0 = it.t0; b0 < it.t1; b0 += 32) {
       const int t = b0 + (int)lane;
       const int cb = t < it.t1 ? v.colind[t] : 0;
       const int ntile = min(32, it.t1 - b0);
-      for (int jt = 0; jt < ntile; ++jt) {
-        const int C = __shfl_sync(0xffffffffu, cb, jt);
-        const uint32_t wr = val[(size_t)(b0 + jt) * 32 + lane];
-        unsigned rows = __ballot_sync(0xffffffffu, wr != 0);
-        while (rows) {
-          const int r = __ffs(rows) - 1;
-          rows &= rows - 1;
-          unsigned bits = __shfl_sync(0xffffffffu, wr, r);
-          double sum = 0.0;
-          while (bits) {
-            const int col = __clz(bits);
-            bits &= ~(0x80000000u >> col);
-            const size_t j = (size_t)C * 32 + col;
-            sum += (double)(X[j * kPprSlots + lane] * a.inv[j]);
+      for (int g0 = 0; g0 < ntile; g0 += kU) {
+        uint32_t wr[kU];
+        unsigned rowsk[kU];
+        int ck[kU];
+#pragma unroll
+        for (int k = 0; k < kU; ++k) wr[k] = g0 + k < ntile ? val[(size_t)(b0 + g0 + k) * 32 + lane] : 0u;
+#pragma unroll
+        for (int k = 0; k < kU; ++k) {
+          rowsk[k] = __ballot_sync(0xffffffffu, wr[k] != 0);
+          ck[k] = __shfl_sync(0xffffffffu, cb, (g0 + k) & 31);
+        }
+        auto sel_w = [&](int k) {
+          uint32_t x = wr[0];
+#pragma unroll
+          for (int q = 1; q < kU; ++q) x = k == q ? wr[q] : x;
+          return x;
+        };
+        auto sel_i = [&](const int* arr, int k) {
+          int x = arr[0];
+#pragma unroll
+          for (int q = 1; q < kU; ++q) x = k == q ? arr[q] : x;
+          return x;
+        };
+        int kk = 0;
+        unsigned rows = rowsk[0], cur = 0;
+        int cr = 0;
+        for (;;) {
+          int pr[kP];
+          size_t pj[kP];
+#pragma unroll
+          for (int q = 0; q < kP; ++q) {
+            while (!cur) {  // warp-uniform: rows and cur come from ballots and shuffles
+              if (rows) {
+                cr = __ffs(rows) - 1;
+                rows &= rows - 1;
+                cur = __shfl_sync(0xffffffffu, sel_w(kk), cr);
+              } else if (kk + 1 < kU) {
+                ++kk;
+                rows = (unsigned)sel_i(reinterpret_cast<const int*>(rowsk), kk);
+              } else {
+                break;
+              }
+            }
+            pr[q] = -1;
+            pj[q] = 0;
+            if (cur) {
+              const int col = __clz(cur);
+              cur &= ~(0x80000000u >> col);
+              pr[q] = cr;
+              pj[q] = (size_t)sel_i(ck, kk) * 32 + col;
+            }
           }
-          acc[r * kPprSlots + lane] += sum;
+          if (pr[0] < 0) break;
+          float xv[kP], iv[kP];
+#pragma unroll
+          for (int q = 0; q < kP; ++q)
+            if (pr[q] >= 0) {
+              xv[q] = X[pj[q] * kPprSlots + lane];
+              iv[q] = a.inv[pj[q]];
+            }
+#pragma unroll
+          for (int q = 0; q < kP; ++q)
+            if (pr[q] >= 0) acc[pr[q] * kPprSlots + lane] += (double)(xv[q] * iv[q]);
         }
       }
     }
@@ -204,9 +257,12 @@ struct RetireList {
 };
 
 // BFS: out[f][i] = level of (i, slot f) relative to its start level, -1 if
-// unreachable; the slot's levels become -1 and its visited bits 0.
+// unreachable; the slot's levels become -1 and its visited bits 0.  When
+// every retired query is shallower than 255 levels (u8), the results leave
+// as one byte per vertex (255 = unreachable), a quarter of the bytes to
+// copy to the host; the client widens them to int32.
 __global__ void __launch_bounds__(256) k_bfs_retire(int* levels, int g, uint32_t* V, int n, int kw,
-                                                    RetireList rl, int* out) {
+                                                    RetireList rl, void* out, int u8) {
   __shared__ int sm[kRetire][kRetRows + 1];
   const long long i0 = (long long)blockIdx.x * kRetRows;
   const int R = rl.count;
@@ -229,7 +285,11 @@ __global__ void __launch_bounds__(256) k_bfs_retire(int* levels, int g, uint32_t
   for (int q = threadIdx.x; q < kRetRows * R; q += blockDim.x) {
     const int f = q / kRetRows, ii = q % kRetRows;
     const long long i = i0 + ii;
-    if (i < n) out[(size_t)f * n + i] = sm[f][ii];
+    if (i >= n) continue;
+    if (u8)
+      static_cast<uint8_t*>(out)[(size_t)f * n + i] = sm[f][ii] < 0 ? (uint8_t)255 : (uint8_t)sm[f][ii];
+    else
+      static_cast<int*>(out)[(size_t)f * n + i] = sm[f][ii];
   }
 }
 
@@ -253,13 +313,14 @@ __global__ void __launch_bounds__(256) k_ppr_retire(const float* X, int n, Retir
 
 // After visited columns were cleared no row is "all sources visited" any
 // more: keep only the padding rows marked.
-__global__ void k_vfull_reset(uint32_t* vfull, int nbr, int n) {
+__global__ void k_vfull_reset(uint32_t* vfull, const uint32_t* __restrict__ live, int nbr, int n) {
   for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q <= nbr;
        q += (long long)gridDim.x * blockDim.x) {
     const long long lo = q * 32;
     uint32_t pad = 0;
     for (int r = 0; r < 32; ++r)
       if (lo + r >= n) pad |= 1u << (31 - r);
+    if (q < nbr) pad |= ~live[q];  // rows without entries stay closed
     vfull[q] = pad;
   }
 }
@@ -276,11 +337,12 @@ struct Query {
 struct Result {
   int kind;
   int buf;          // pinned pool buffer holding the result (-1: moved to heap)
+  int u8;           // BFS levels stored one byte per vertex (255 = unreachable)
   cudaEvent_t ev;   // its copy has landed when this event completes
   bool landed;
   double t_submit, t_done;
   int iters;
-  std::vector<int> heap;  // the result once moved out of the pinned pool
+  std::vector<unsigned char> heap;  // the result once moved out of the pinned pool
 };
 
 }  // namespace
@@ -291,8 +353,10 @@ struct gbo_server {
   int n = 0, nbr = 0;
   float alpha = 0.85f, tol = 1e-7f;
   int ppr_max_iter = 1000;
-  cudaStream_t s = nullptr;   // compute
-  cudaStream_t cs = nullptr;  // result copies
+  // one worker thread per engine (0 BFS, 1 PPR), each with its own compute
+  // stream and result-copy stream, so the engines overlap on the GPU
+  cudaStream_t s[2] = {nullptr, nullptr};
+  cudaStream_t cs[2] = {nullptr, nullptr};
   int dev = 0;
   // BFS engine (levels grouped 8 sources per 32-byte sector)
   int kb = 0, kw = 0;
@@ -301,6 +365,10 @@ struct gbo_server {
   int* ctl = nullptr;
   uint32_t* slot_any = nullptr;
   uint32_t* h_slot_any = nullptr;
+  uint32_t* d_active = nullptr;  // columns still traversing (kw words)
+  std::vector<uint32_t> h_active;
+  bool reopen = false;           // active set grew: rows marked finished reopen
+  const uint32_t* live = nullptr;  // rows of P with an entry (owned by the graph)
   int *d_adm_src = nullptr, *d_adm_slot = nullptr;
   int level = 0;
   std::vector<long long> bslot_ticket;
@@ -317,17 +385,17 @@ struct gbo_server {
   std::vector<long long> pslot_ticket;
   std::vector<int> pslot_iters;
   std::vector<char> pslot_finished;
-  // results: device staging (double-buffered), pinned host pool
-  void* d_stage[2] = {nullptr, nullptr};
-  cudaEvent_t stage_free[2] = {nullptr, nullptr};
-  int stage_next = 0;
+  // results: device staging (double-buffered per engine), pinned host pool
+  void* d_stage[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  cudaEvent_t stage_free[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  int stage_next[2] = {0, 0};
   std::vector<void*> pool;
   std::vector<int> pool_free;
   std::vector<cudaEvent_t> pool_ev;
   // host side
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
-  std::deque<gbo::Query> pending;
+  std::deque<gbo::Query> pending[2];
   std::map<long long, gbo::Result> results;
   std::map<long long, double> submit_time;
   int copies_in_flight = 0;
@@ -335,9 +403,12 @@ struct gbo_server {
   bool stop = false;
   int worker_status = GBO_OK;
   std::string worker_error;
-  std::thread worker;
+  std::thread worker[2];
   // statistics
-  long long rounds = 0, bfs_done = 0, ppr_done = 0, launches = 0;
+  std::atomic<long long> rounds{0}, launches{0};
+  long long bfs_done = 0, ppr_done = 0;
+  double phase_ms[4] = {0, 0, 0, 0};  // BFS round, PPR round, retire, spill (under mu)
+  long long spilled = 0;
 };
 
 namespace gbo {
@@ -356,6 +427,8 @@ ms::Args bfs_args(gbo_server* S) {
   a.ctl = S->ctl;
   a.scratch = S->scratch;
   a.slot_any = S->slot_any;
+  a.live = S->live;
+  a.active = S->d_active;
   a.level_group = 8;
   return a;
 }
@@ -363,7 +436,17 @@ ms::Args bfs_args(gbo_server* S) {
 template <int KW>
 int bfs_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
   const ms::Args a = bfs_args(S);
-  cudaStream_t st = S->s;
+  cudaStream_t st = S->s[0];
+  // columns still traversing; rows marked finished for the old set reopen
+  // when the set grows
+  for (int w = 0; w < S->kw; ++w) S->h_active[(size_t)w] = 0u;
+  for (int q = 0; q < S->kb; ++q)
+    if (S->bslot_ticket[(size_t)q] > 0 && !S->bslot_finished[(size_t)q]) S->h_active[(size_t)(q / 32)] |= 1u << (q % 32);
+  GBO_CUDA_TRY(cudaMemcpyAsync(S->d_active, S->h_active.data(), sizeof(uint32_t) * S->kw, cudaMemcpyHostToDevice, st));
+  if (!adm.empty()) {
+    k_vfull_reset<<<blocks_for(S->nbr + 1, 256), 256, 0, st>>>(S->vfull, S->live, S->nbr, S->n);
+    S->launches++;
+  }
   if (!adm.empty()) {
     std::vector<int> src, slot;
     for (auto& q : adm) {
@@ -372,8 +455,8 @@ int bfs_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
     }
     GBO_CUDA_TRY(cudaMemcpyAsync(S->d_adm_src, src.data(), sizeof(int) * src.size(), cudaMemcpyHostToDevice, st));
     GBO_CUDA_TRY(cudaMemcpyAsync(S->d_adm_slot, slot.data(), sizeof(int) * slot.size(), cudaMemcpyHostToDevice, st));
-    ms::k_seed<<<1, 32, 0, st>>>(a, S->d_adm_src, S->d_adm_slot, (int)src.size(), S->kw, S->level);
-    S->launches++;
+    ms::seed_sources(a, S->d_adm_src, S->d_adm_slot, (int)src.size(), S->kw, S->level, st);
+    S->launches += 2;
   }
   int h[4] = {S->level, 0, 0, 0x7fffffff};  // level, not done, ticket 0, no iteration cap
   GBO_CUDA_TRY(cudaMemcpyAsync(S->ctl, h, sizeof(h), cudaMemcpyHostToDevice, st));
@@ -388,6 +471,7 @@ int bfs_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
   GBO_CUDA_TRY(cudaMemcpyAsync(S->h_slot_any, S->slot_any, sizeof(uint32_t) * S->kw, cudaMemcpyDeviceToHost, st));
   GBO_CUDA_TRY(cudaStreamSynchronize(st));
   S->level += 1;
+  std::lock_guard<std::mutex> lk(S->mu);  // finished flags are read by the other worker
   for (int q = 0; q < S->kb; ++q)
     if (S->bslot_ticket[q] > 0 && !S->bslot_finished[q] && !((S->h_slot_any[q / 32] >> (q % 32)) & 1u))
       S->bslot_finished[q] = 1;
@@ -395,7 +479,7 @@ int bfs_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
 }
 
 int ppr_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
-  cudaStream_t st = S->s;
+  cudaStream_t st = S->s[1];
   const size_t xstride = (size_t)S->n * kPprSlots;
   if (!adm.empty()) {
     std::vector<int> slots, verts, off(1, 0);
@@ -443,6 +527,7 @@ int ppr_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
   GBO_CUDA_TRY(cudaMemcpyAsync(S->h_err, S->err, sizeof(double) * kPprSlots, cudaMemcpyDeviceToHost, st));
   GBO_CUDA_TRY(cudaStreamSynchronize(st));
   S->parity ^= 1;
+  std::lock_guard<std::mutex> lk(S->mu);  // finished flags are read by the other worker
   for (int q = 0; q < kPprSlots; ++q) {
     if (S->pslot_ticket[q] <= 0 || S->pslot_finished[q]) continue;
     S->pslot_iters[q] += 1;
@@ -473,38 +558,45 @@ int retire(gbo_server* S, int kind) {
     }
   }
   if (rl.count == 0) return GBO_OK;
-  const int sb = S->stage_next;
-  S->stage_next ^= 1;
-  GBO_CUDA_TRY(cudaStreamWaitEvent(S->s, S->stage_free[sb], 0));  // its previous copies are done
+  cudaStream_t st = S->s[kind], cst = S->cs[kind];
+  const int sb = S->stage_next[kind];
+  S->stage_next[kind] ^= 1;
+  void* stage = S->d_stage[kind][sb];
+  GBO_CUDA_TRY(cudaStreamWaitEvent(st, S->stage_free[kind][sb], 0));  // its previous copies are done
   const unsigned grid = blocks_for(S->n, kRetRows);
+  int u8 = 0;
   if (kind == 0) {
-    k_bfs_retire<<<grid, 256, 0, S->s>>>(S->levels, 8, S->V, S->n, S->kw, rl, (int*)S->d_stage[sb]);
-    k_vfull_reset<<<blocks_for(S->nbr + 1, 256), 256, 0, S->s>>>(S->vfull, S->nbr, S->n);
-    S->launches += 2;
+    int deepest = 0;
+    for (int f = 0; f < rl.count; ++f) deepest = std::max(deepest, S->level - rl.start[f]);
+    u8 = deepest < 255;
+    // retired columns were already out of the active set: rows marked
+    // finished stay finished
+    k_bfs_retire<<<grid, 256, 0, st>>>(S->levels, 8, S->V, S->n, S->kw, rl, stage, u8);
+    S->launches += 1;
   } else {
-    k_ppr_retire<<<grid, 256, 0, S->s>>>(S->X + (size_t)S->parity * S->n * kPprSlots, S->n, rl,
-                                         (float*)S->d_stage[sb]);
+    k_ppr_retire<<<grid, 256, 0, st>>>(S->X + (size_t)S->parity * S->n * kPprSlots, S->n, rl, (float*)stage);
     S->launches += 1;
   }
   GBO_CUDA_TRY(cudaGetLastError());
   cudaEvent_t ready;
   GBO_CUDA_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
-  GBO_CUDA_TRY(cudaEventRecord(ready, S->s));
-  GBO_CUDA_TRY(cudaStreamWaitEvent(S->cs, ready, 0));
+  GBO_CUDA_TRY(cudaEventRecord(ready, st));
+  GBO_CUDA_TRY(cudaStreamWaitEvent(cst, ready, 0));
   cudaEventDestroy(ready);
-  const size_t rbytes = sizeof(int) * (size_t)S->n;
+  const size_t rbytes = (u8 ? 1 : sizeof(int)) * (size_t)S->n;
   const double t_now = now_ms();
   std::lock_guard<std::mutex> lk(S->mu);
   for (int f = 0; f < rl.count; ++f) {
     const int b = bufs[(size_t)f];
-    GBO_CUDA_TRY(cudaMemcpyAsync(S->pool[(size_t)b], (char*)S->d_stage[sb] + (size_t)f * rbytes, rbytes,
-                                 cudaMemcpyDeviceToHost, S->cs));
-    GBO_CUDA_TRY(cudaEventRecord(S->pool_ev[(size_t)b], S->cs));
+    GBO_CUDA_TRY(cudaMemcpyAsync(S->pool[(size_t)b], (char*)stage + (size_t)f * rbytes, rbytes,
+                                 cudaMemcpyDeviceToHost, cst));
+    GBO_CUDA_TRY(cudaEventRecord(S->pool_ev[(size_t)b], cst));
     const int q = rl.slot[f];
     const long long t = tick[(size_t)q];
     Result r;
     r.kind = kind;
     r.buf = b;
+    r.u8 = u8;
     r.ev = S->pool_ev[(size_t)b];
     r.landed = false;
     r.t_submit = S->submit_time[t];
@@ -517,7 +609,7 @@ int retire(gbo_server* S, int kind) {
     if (kind == 0) S->bfs_done++;
     else S->ppr_done++;
   }
-  GBO_CUDA_TRY(cudaEventRecord(S->stage_free[sb], S->cs));
+  GBO_CUDA_TRY(cudaEventRecord(S->stage_free[kind][sb], cst));
   return GBO_OK;
 }
 
@@ -552,20 +644,23 @@ bool spill_landed(gbo_server* S) {
   for (size_t q = 0; q < S->pslot_ticket.size() && !waiting; ++q)
     waiting = S->pslot_ticket[q] > 0 && S->pslot_finished[q];
   if (!waiting || !S->pool_free.empty()) return false;
+  const double t0 = now_ms();
   int moved = 0;
   for (auto& kv : S->results) {
     Result& r = kv.second;
     if (!r.landed || r.buf < 0) continue;
-    const int* src = static_cast<const int*>(S->pool[(size_t)r.buf]);
-    r.heap.assign(src, src + S->n);
+    const unsigned char* src = static_cast<const unsigned char*>(S->pool[(size_t)r.buf]);
+    r.heap.assign(src, src + (r.u8 ? 1 : 4) * (size_t)S->n);
     S->pool_free.push_back(r.buf);
     r.buf = -1;
     if (++moved == kRetire) break;
   }
+  S->spilled += moved;
+  S->phase_ms[3] += now_ms() - t0;
   return moved > 0;
 }
 
-void worker_main(gbo_server* S) {
+void worker_main(gbo_server* S, int kind) {
   cudaSetDevice(S->dev);
   auto failw = [&](int st) {
     std::lock_guard<std::mutex> lk(S->mu);
@@ -573,80 +668,77 @@ void worker_main(gbo_server* S) {
     S->worker_error = gbo_last_error();
     S->cv_done.notify_all();
   };
-  auto occupied = [&](const std::vector<long long>& tab) {
+  std::vector<long long>& tab = kind == 0 ? S->bslot_ticket : S->pslot_ticket;
+  std::vector<char>& fin = kind == 0 ? S->bslot_finished : S->pslot_finished;
+  auto occupied = [&]() {
     for (long long t : tab)
       if (t > 0) return true;
     return false;
   };
-  auto unfinished = [&](const std::vector<long long>& tab, const std::vector<char>& fin) {
+  auto unfinished = [&]() {
     for (size_t q = 0; q < tab.size(); ++q)
       if (tab[q] > 0 && !fin[q]) return true;
     return false;
   };
   while (true) {
-    std::vector<std::pair<int, Query>> badm, padm;
+    std::vector<std::pair<int, Query>> adm;
     {
       std::unique_lock<std::mutex> lk(S->mu);
       for (;;) {
         if (collect_landed(S)) S->cv_done.notify_all();
         if (S->stop) return;
         spill_landed(S);
-        const bool work = !S->pending.empty() || unfinished(S->bslot_ticket, S->bslot_finished) ||
-                          unfinished(S->pslot_ticket, S->pslot_finished) ||
-                          ((occupied(S->bslot_ticket) || occupied(S->pslot_ticket)) && !S->pool_free.empty());
+        const bool work = !S->pending[kind].empty() || unfinished() || (occupied() && !S->pool_free.empty());
         if (work) break;
         if (S->copies_in_flight > 0)
           S->cv_work.wait_for(lk, std::chrono::microseconds(200));
         else
           S->cv_work.wait(lk);
       }
-      // admission into free slots, arrival order, per engine
-      std::deque<Query> keep;
-      std::vector<char> btaken(S->bslot_ticket.size(), 0), ptaken(S->pslot_ticket.size(), 0);
-      size_t bnext = 0, pnext = 0;
-      while (!S->pending.empty()) {
-        Query q = std::move(S->pending.front());
-        S->pending.pop_front();
-        std::vector<long long>& tab = q.kind == 0 ? S->bslot_ticket : S->pslot_ticket;
-        size_t& nx = q.kind == 0 ? bnext : pnext;
+      // admission into free slots, arrival order
+      size_t nx = 0;
+      std::deque<Query>& pend = S->pending[kind];
+      while (!pend.empty()) {
         while (nx < tab.size() && tab[nx] != 0) ++nx;
-        if (nx >= tab.size()) {
-          keep.push_back(std::move(q));
-          continue;
-        }
+        if (nx >= tab.size()) break;
+        Query q = std::move(pend.front());
+        pend.pop_front();
         const int slot = (int)nx++;
         tab[(size_t)slot] = q.ticket;
-        if (q.kind == 0) {
-          S->bslot_start[(size_t)slot] = S->level;
-          S->bslot_finished[(size_t)slot] = 0;
-          badm.emplace_back(slot, std::move(q));
-        } else {
-          S->pslot_iters[(size_t)slot] = 0;
-          S->pslot_finished[(size_t)slot] = 0;
-          padm.emplace_back(slot, std::move(q));
-        }
+        fin[(size_t)slot] = 0;
+        if (kind == 0) S->bslot_start[(size_t)slot] = S->level;
+        else S->pslot_iters[(size_t)slot] = 0;
+        adm.emplace_back(slot, std::move(q));
       }
-      S->pending.swap(keep);
     }
     int st = GBO_OK;
-    const bool bfs_busy = !badm.empty() || unfinished(S->bslot_ticket, S->bslot_finished);
-    const bool ppr_busy = !padm.empty() || unfinished(S->pslot_ticket, S->pslot_finished);
-    if (bfs_busy && S->kb > 0) {
-      switch (S->kw) {
-        case 1: st = bfs_round<1>(S, badm); break;
-        case 2: st = bfs_round<2>(S, badm); break;
-        case 4: st = bfs_round<4>(S, badm); break;
-        case 8: st = bfs_round<8>(S, badm); break;
-        case 16: st = bfs_round<16>(S, badm); break;
-        default: st = bfs_round<32>(S, badm); break;
+    const bool busy = !adm.empty() || unfinished();
+    const double t0 = now_ms();
+    if (busy) {
+      if (kind == 0) {
+        switch (S->kw) {
+          case 1: st = bfs_round<1>(S, adm); break;
+          case 2: st = bfs_round<2>(S, adm); break;
+          case 4: st = bfs_round<4>(S, adm); break;
+          case 8: st = bfs_round<8>(S, adm); break;
+          case 16: st = bfs_round<16>(S, adm); break;
+          default: st = bfs_round<32>(S, adm); break;
+        }
+      } else {
+        st = ppr_round(S, adm);
       }
     }
-    if (st == GBO_OK && ppr_busy && S->g->invdeg) st = ppr_round(S, padm);
-    if (st == GBO_OK && S->kb > 0) st = retire(S, 0);
-    if (st == GBO_OK && !S->pslot_ticket.empty()) st = retire(S, 1);
+    const double t1 = now_ms();
+    if (st == GBO_OK) st = retire(S, kind);
+    const double t2 = now_ms();
     if (st != GBO_OK) {
       failw(st);
       return;
+    }
+    {
+      std::lock_guard<std::mutex> lk(S->mu);
+      S->phase_ms[kind] += t1 - t0;
+      S->phase_ms[2] += t2 - t1;
     }
     S->rounds++;
   }
@@ -659,9 +751,11 @@ void destroy_server(gbo_server* S) {
     S->stop = true;
   }
   S->cv_work.notify_all();
-  if (S->worker.joinable()) S->worker.join();
-  if (S->s) cudaStreamSynchronize(S->s);
-  if (S->cs) cudaStreamSynchronize(S->cs);
+  for (int e = 0; e < 2; ++e) {
+    if (S->worker[e].joinable()) S->worker[e].join();
+    if (S->s[e]) cudaStreamSynchronize(S->s[e]);
+    if (S->cs[e]) cudaStreamSynchronize(S->cs[e]);
+  }
   cudaFree(S->F);
   cudaFree(S->V);
   cudaFree(S->fbits);
@@ -671,6 +765,7 @@ void destroy_server(gbo_server* S) {
   cudaFree(S->ctl);
   cudaFree(S->slot_any);
   cudaFreeHost(S->h_slot_any);
+  cudaFree(S->d_active);
   cudaFree(S->d_adm_src);
   cudaFree(S->d_adm_slot);
   cudaFree(S->X);
@@ -682,14 +777,17 @@ void destroy_server(gbo_server* S) {
   cudaFree(S->d_pverts);
   cudaFree(S->d_poff);
   cudaFree(S->d_pwts);
-  for (int b = 0; b < 2; ++b) {
-    cudaFree(S->d_stage[b]);
-    if (S->stage_free[b]) cudaEventDestroy(S->stage_free[b]);
-  }
+  for (int e = 0; e < 2; ++e)
+    for (int b = 0; b < 2; ++b) {
+      cudaFree(S->d_stage[e][b]);
+      if (S->stage_free[e][b]) cudaEventDestroy(S->stage_free[e][b]);
+    }
   for (void* p : S->pool) cudaFreeHost(p);
   for (cudaEvent_t e : S->pool_ev) cudaEventDestroy(e);
-  if (S->s) cudaStreamDestroy(S->s);
-  if (S->cs) cudaStreamDestroy(S->cs);
+  for (int e = 0; e < 2; ++e) {
+    if (S->s[e]) cudaStreamDestroy(S->s[e]);
+    if (S->cs[e]) cudaStreamDestroy(S->cs[e]);
+  }
   delete S;
 }
 
@@ -726,8 +824,10 @@ extern "C" int gbo_server_create(const gbo_graph* gc, int bfs_slots, int ppr_slo
     if (e != cudaSuccess) throw fail_cuda(e, w);
   };
   try {
-    cu(cudaStreamCreateWithFlags(&S->s, cudaStreamNonBlocking), "stream");
-    cu(cudaStreamCreateWithFlags(&S->cs, cudaStreamNonBlocking), "stream");
+    for (int e = 0; e < 2; ++e) {
+      cu(cudaStreamCreateWithFlags(&S->s[e], cudaStreamNonBlocking), "stream");
+      cu(cudaStreamCreateWithFlags(&S->cs[e], cudaStreamNonBlocking), "stream");
+    }
     const size_t n = (size_t)S->n;
     if (S->kb) {
       cu(cudaMalloc(&S->F, sizeof(uint32_t) * 2 * n * kw + 16), "F");
@@ -741,10 +841,20 @@ extern "C" int gbo_server_create(const gbo_graph* gc, int bfs_slots, int ppr_slo
       cu(cudaHostAlloc(&S->h_slot_any, sizeof(uint32_t) * kw, cudaHostAllocDefault), "h_slot_any");
       cu(cudaMalloc(&S->d_adm_src, sizeof(int) * S->kb), "adm");
       cu(cudaMalloc(&S->d_adm_slot, sizeof(int) * S->kb), "adm");
+      {
+        const void* lv = nullptr;
+        const int st = live_rows(g, S->s[0], &lv);
+        if (st != GBO_OK) throw st;
+        S->live = static_cast<const uint32_t*>(lv);
+      }
       ms::Args a = bfs_args(S);
       unsigned gv = blocks_for((long long)n * S->kb, 256);
       if (gv > (unsigned)num_sms() * 16u) gv = (unsigned)num_sms() * 16u;
-      ms::k_init<<<gv, 256, 0, S->s>>>(a, kw, 0x7fffffff);
+      cu(cudaMalloc(&S->d_active, sizeof(uint32_t) * kw), "active");
+      cu(cudaMemsetAsync(S->d_active, 0, sizeof(uint32_t) * kw, S->s[0]), "active");
+      S->h_active.assign((size_t)kw, 0u);
+      a.active = S->d_active;
+      ms::k_init<<<gv, 256, 0, S->s[0]>>>(a, kw, 0x7fffffff);
       cu(cudaGetLastError(), "init");
     }
     S->bslot_ticket.assign((size_t)S->kb, 0);
@@ -752,9 +862,9 @@ extern "C" int gbo_server_create(const gbo_graph* gc, int bfs_slots, int ppr_slo
     S->bslot_finished.assign((size_t)S->kb, 0);
     if (ppr_slots) {
       cu(cudaMalloc(&S->X, sizeof(float) * 2 * n * kPprSlots), "X");
-      cu(cudaMemsetAsync(S->X, 0, sizeof(float) * 2 * n * kPprSlots, S->s), "X");
+      cu(cudaMemsetAsync(S->X, 0, sizeof(float) * 2 * n * kPprSlots, S->s[1]), "X");
       cu(cudaMalloc(&S->P, sizeof(float) * n * kPprSlots), "P");
-      cu(cudaMemsetAsync(S->P, 0, sizeof(float) * n * kPprSlots, S->s), "P");
+      cu(cudaMemsetAsync(S->P, 0, sizeof(float) * n * kPprSlots, S->s[1]), "P");
       cu(cudaMalloc(&S->err, sizeof(double) * kPprSlots), "err");
       cu(cudaHostAlloc(&S->h_err, sizeof(double) * kPprSlots, cudaHostAllocDefault), "h_err");
       cu(cudaMalloc(&S->pscratch, sizeof(double) * (size_t)(g->nslots > 0 ? g->nslots : 1) * 32 * kPprSlots), "pscratch");
@@ -766,10 +876,13 @@ extern "C" int gbo_server_create(const gbo_graph* gc, int bfs_slots, int ppr_slo
     S->pslot_ticket.assign(ppr_slots ? (size_t)kPprSlots : 0, 0);
     S->pslot_iters.assign((size_t)kPprSlots, 0);
     S->pslot_finished.assign((size_t)kPprSlots, 0);
-    for (int b = 0; b < 2; ++b) {
-      cu(cudaMalloc(&S->d_stage[b], sizeof(int) * n * kRetire + 16), "stage");
-      cu(cudaEventCreateWithFlags(&S->stage_free[b], cudaEventDisableTiming), "event");
-      cu(cudaEventRecord(S->stage_free[b], S->cs), "event");
+    for (int e = 0; e < 2; ++e) {
+      if (e == 0 ? S->kb == 0 : ppr_slots == 0) continue;
+      for (int b = 0; b < 2; ++b) {
+        cu(cudaMalloc(&S->d_stage[e][b], sizeof(int) * n * kRetire + 16), "stage");
+        cu(cudaEventCreateWithFlags(&S->stage_free[e][b], cudaEventDisableTiming), "event");
+        cu(cudaEventRecord(S->stage_free[e][b], S->cs[e]), "event");
+      }
     }
     // pinned result buffers: enough for two rounds of retirements
     const int npool = 2 * kRetire;
@@ -782,12 +895,14 @@ extern "C" int gbo_server_create(const gbo_graph* gc, int bfs_slots, int ppr_slo
       S->pool_ev.push_back(e);
       S->pool_free.push_back(b);
     }
-    cu(cudaStreamSynchronize(S->s), "sync");
+    cu(cudaStreamSynchronize(S->s[0]), "sync");
+    cu(cudaStreamSynchronize(S->s[1]), "sync");
   } catch (int st) {
     destroy_server(S);
     return st;
   }
-  S->worker = std::thread(worker_main, S);
+  if (S->kb > 0) S->worker[0] = std::thread(worker_main, S, 0);
+  if (ppr_slots) S->worker[1] = std::thread(worker_main, S, 1);
   *out = S;
   return GBO_OK;
 }
@@ -799,8 +914,9 @@ static int submit(gbo_server* S, Query&& q, int64_t* ticket) {
   q.t_submit = now_ms();
   S->submit_time[q.ticket] = q.t_submit;
   *ticket = q.ticket;
-  S->pending.push_back(std::move(q));
-  S->cv_work.notify_one();
+  const int kind = q.kind;
+  S->pending[kind].push_back(std::move(q));
+  S->cv_work.notify_all();
   return GBO_OK;
 }
 
@@ -840,13 +956,19 @@ static int take_result(gbo_server* S, std::unique_lock<std::mutex>& lk, int64_t 
   S->results.erase(it);
   S->submit_time.erase(ticket);
   lk.unlock();
-  if (h_out) memcpy(h_out, r.buf >= 0 ? S->pool[(size_t)r.buf] : (const void*)r.heap.data(),
-                    sizeof(int) * (size_t)S->n);
+  const void* src = r.buf >= 0 ? S->pool[(size_t)r.buf] : (const void*)r.heap.data();
+  if (h_out && r.u8) {
+    const unsigned char* b8 = static_cast<const unsigned char*>(src);
+    int* o = static_cast<int*>(h_out);
+    for (int i = 0; i < S->n; ++i) o[i] = b8[i] == 255 ? -1 : (int)b8[i];
+  } else if (h_out) {
+    memcpy(h_out, src, sizeof(int) * (size_t)S->n);
+  }
   if (latency_ms) *latency_ms = r.t_done - r.t_submit;
   if (iterations) *iterations = r.iters;
   lk.lock();
   if (r.buf >= 0) S->pool_free.push_back(r.buf);
-  S->cv_work.notify_one();
+  S->cv_work.notify_all();
   return GBO_OK;
 }
 
@@ -886,11 +1008,16 @@ extern "C" int gbo_server_get_stats(gbo_server* S, gbo_server_stats* st) {
   st->bfs_completed = S->bfs_done;
   st->ppr_completed = S->ppr_done;
   st->kernel_launches = S->launches;
-  st->pending = (long long)S->pending.size();
+  st->pending = (long long)(S->pending[0].size() + S->pending[1].size());
   long long a = 0;
   for (long long t : S->bslot_ticket) a += t > 0;
   for (long long t : S->pslot_ticket) a += t > 0;
   st->in_flight = a;
+  st->bfs_round_ms = S->phase_ms[0];
+  st->ppr_round_ms = S->phase_ms[1];
+  st->retire_ms = S->phase_ms[2];
+  st->spill_ms = S->phase_ms[3];
+  st->spilled = S->spilled;
   return GBO_OK;
 }
 

@@ -69,7 +69,9 @@ class RunStats(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [("rounds", C.c_longlong), ("bfs_completed", C.c_longlong),
                 ("ppr_completed", C.c_longlong), ("kernel_launches", C.c_longlong),
-                ("pending", C.c_longlong), ("in_flight", C.c_longlong)]
+                ("pending", C.c_longlong), ("in_flight", C.c_longlong),
+                ("bfs_round_ms", C.c_double), ("ppr_round_ms", C.c_double),
+                ("retire_ms", C.c_double), ("spill_ms", C.c_double), ("spilled", C.c_longlong)]
 
 
 class CsrStruct(C.Structure):

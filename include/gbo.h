@@ -268,8 +268,13 @@ GBO_API int gbo_bmv_float_transposed(const gbo_graph* g, const float* d_x, float
  * h_depth (nullable) receives the number of levels (max level + 1). */
 GBO_API int gbo_bfs(const gbo_graph* g, int src, int32_t* d_level, int* h_depth,
             gbo_stream_t stream);
-/* Unit-weight SSSP by min-plus relaxation (algorithm/sssp.cu:420-470):
- * dist[i] in uint32, 2147483647 = unreachable. */
+/* Unit-weight SSSP with the distances of the reference's min-plus loop
+ * (algorithm/sssp.cu:420-470): dist[i] in uint32, 2147483647 = unreachable.
+ * With unit weights every frontier vertex at iteration k has distance k, so
+ * a row's relaxation min_j (d[j] + 1) is k + 1 at its first frontier
+ * neighbour: the step runs as the BFS step (early exit; push on small
+ * frontiers of symmetric graphs).  The general min-plus product is
+ * gbo_bmv_minplus. */
 GBO_API int gbo_sssp_unit(const gbo_graph* g, int src, uint32_t* d_dist, int* h_iters,
                   gbo_stream_t stream);
 /* PageRank p = alpha * P D^-1 p + (1-alpha)/n from p0 = 1/n, as in
@@ -315,13 +320,21 @@ GBO_API int gbo_bfs_multi(const gbo_graph* g, const int* h_seeds, int nseeds,
  * thread drives the GPU; submit/poll/wait are thread-safe.  Results: BFS
  * int32[n] levels (hops, -1 unreachable), PPR float[n].  A query's result
  * is the same whatever else is in flight.  Needs a square ROW-layout graph
- * with 32x32 tiles (and out-degrees for PPR). */
+ * with 32x32 tiles (and out-degrees for PPR).  A finished result waits in
+ * host memory (a pinned buffer, or heap memory once the pinned pool is all
+ * held by uncollected results) until wait/poll takes it, in any order. */
 typedef struct gbo_server gbo_server;
 typedef struct gbo_server_stats {
-  long long rounds;          /* worker rounds (one BFS level and/or PPR iteration) */
+  long long rounds;          /* worker rounds (one BFS level or one PPR iteration) */
   long long bfs_completed, ppr_completed;
   long long kernel_launches;
   long long pending, in_flight;
+  /* wall time the workers spent per phase (ms, summed over rounds):
+   * BFS levels and PPR iterations (kernels and the completion read-back),
+   * retirement (extraction kernels and copy issue), and moving uncollected
+   * results out of the pinned pool */
+  double bfs_round_ms, ppr_round_ms, retire_ms, spill_ms;
+  long long spilled;         /* results moved to heap memory */
 } gbo_server_stats;
 GBO_API int gbo_server_create(const gbo_graph* g, int bfs_slots, int ppr_slots,
                       float alpha, float tol, int ppr_max_iter,
@@ -339,8 +352,9 @@ GBO_API int gbo_server_destroy(gbo_server* s);
 
 /* Personalized PageRank p = alpha * P D^-1 p + (1-alpha) v  (fp32) and its
  * adjoint: for loss L = dot(w, p), grad_v = (1-alpha) u with
- * u = alpha * D^-1 P^T u + w.  Iterate until the L1 change <= tol or
- * max_iter.  No reference counterpart (built from A7). */
+ * u = alpha * D^-1 P^T u + w.  Iterate until the L1 change <= tol (forward:
+ * v is a distribution) or <= tol * ||w||_1 (adjoint), or max_iter.  No
+ * reference counterpart (built from A7). */
 GBO_API int gbo_ppr_forward(const gbo_graph* g, const float* d_v, float alpha,
                     float tol, int max_iter, float* d_p, int* h_iters,
                     gbo_stream_t stream);

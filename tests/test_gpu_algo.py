@@ -111,7 +111,10 @@ def test_pagerank(gbo, orc, gpu, graphs, b):
 
 
 @pytest.mark.parametrize("b", [8, 32, 64])
-def test_ppr_forward_backward(gbo, orc, gpu, b):
+@pytest.mark.parametrize("sym", [False, True])
+def test_ppr_forward_backward(gbo, orc, gpu, b, sym):
+    """sym: the graph is flagged symmetric, so the adjoint gathers over P's
+    rows instead of scattering with atomics."""
     csr = gbo.gen_rmat(12, 16, seed=1)
     n = csr.nrows
     outdeg = np.bincount(csr.colind, minlength=n).astype(np.int32)
@@ -120,7 +123,7 @@ def test_ppr_forward_backward(gbo, orc, gpu, b):
     idx = rng.choice(n, max(1, n // 100), replace=False)
     v[idx] = rng.dirichlet(np.ones(len(idx)))
     w = rng.standard_normal(n)
-    g = gbo.Graph.from_csr(csr, b)
+    g = gbo.Graph.from_csr(csr, b, gbo.FLAG_SYMMETRIC if sym else 0)
     p, _ = g.ppr_forward(v.astype(np.float32), 0.85, 1e-7, 1000)
     p64, _ = orc.ppr_f64(csr.rowptr, csr.colind, n, outdeg, v, 0.85, 1e-13)
     assert rel_l1(p, p64) <= 1e-5
