@@ -38,12 +38,19 @@ def parse():
     ap.add_argument("--scale", type=int, default=SCALE)
     ap.add_argument("--tile", type=int, default=TILE)
     ap.add_argument("--cpu-samples", type=int, default=3, help="BFS runs timed for cpu_baseline")
+    ap.add_argument("--layout", default="row", choices=["row", "col"],
+                    help="tile layout of the BFS graph (COL: pull steps read only the frontier's column words)")
     ap.add_argument("--direction", default="auto", choices=["auto", "pull"],
                     help="auto: top-down steps while the frontier is small (graph is symmetric)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving streams")
     ap.add_argument("--serve-qps", type=float, default=4000.0, help="offered BFS query rate")
     ap.add_argument("--serve-s", type=float, default=1.5, help="seconds of arrivals per stream")
+    ap.add_argument("--tc-graphs", default="mesh,rmat", help="graphs of --workload tc (mesh, rmat)")
+    ap.add_argument("--tc-variants", default="input,degree", help="vertex orders of --workload tc")
+    ap.add_argument("--tc-tiles", default="8,16,32,64", help="tile widths of --workload tc")
+    ap.add_argument("--serve-rates", default="1000,10000,100000",
+                    help="offered rates of --workload serve (queries/s, comma-separated)")
     ap.add_argument("--workload", default="bfs", choices=["bfs"] + list(SUITE),
                     help="bfs: the headline line; the others print one line each for the "
                          "remaining workloads (SSSP/CC/PR on R-MAT 22, TC, MS-BFS, many-graph "
@@ -90,9 +97,10 @@ class Dist:
             self.dist.destroy_process_group()
 
 
-def workload_name(scale, tile):
+def workload_name(scale, tile, layout="row"):
     return (f"BFS from vertex 0, R-MAT scale {scale} edge factor {EDGE_FACTOR} "
-            f"(a=0.57,b=0.19,c=0.19, seed {SEED}, symmetrised, deduplicated), B2SR {tile}x{tile}")
+            f"(a=0.57,b=0.19,c=0.19, seed {SEED}, symmetrised, deduplicated), B2SR {tile}x{tile}, "
+            f"{'column' if layout == 'col' else 'row'}-word tiles")
 
 
 def traversed_edges(csr, levels):
@@ -101,15 +109,17 @@ def traversed_edges(csr, levels):
 
 
 # --------------------------------------------------------------- roofline
-def bfs_level_bytes(rowptr_b, colind_b, levels, nrows, b, row_live):
+def bfs_level_bytes(rowptr_b, colind_b, levels, nrows, b, row_live, layout="row"):
     """Algorithmic bytes of each BFS pull step (the words the step must touch).
 
     Step L reads the block-row offsets, the visited and frontier words, the
     block-column index of every tile in a block row that still has an
     unvisited vertex that can be reached (its row of P has an entry), and --
-    only for tiles whose frontier segment is non-empty -- one b-bit row word
-    per such row; it writes the next frontier words, visited words of changed
-    rows and one int32 level per new vertex.
+    only for tiles whose frontier segment is non-empty -- the tile words that
+    decide the step: with ROW tiles one b-bit row word per such row, with COL
+    tiles one column word per frontier vertex of the segment; it writes the
+    next frontier words, visited words of changed rows and one int32 level
+    per new vertex.
     """
     nbr = len(rowptr_b) - 1
     wb = max(1, b // 8)
@@ -132,7 +142,11 @@ def bfs_level_bytes(rowptr_b, colind_b, levels, nrows, b, row_live):
         changed = int(((lv == L + 1).any(axis=1)).sum())
         by = 4 * (nbr + 1) + 2 * wb * nbr + wb * changed + 4 * newv
         by += 4 * int(t_open.sum())
-        by += wb * int(unvis[row_of[t_need]].sum())
+        if layout == "col":
+            fcount = (lv == L).sum(axis=1)  # frontier vertices per block column
+            by += wb * int(fcount[colind_b[t_need]].sum())
+        else:
+            by += wb * int(unvis[row_of[t_need]].sum())
         out.append(by)
     return out
 
@@ -251,7 +265,7 @@ def run_reference(args, ws, rank):
         "impl": "reference", "metric": "GTEPS", "value": v, "unit": "GTEPS", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": workload_name(args.scale, args.tile), "scale": args.scale,
+        "config": {"workload": workload_name(args.scale, args.tile, args.layout), "scale": args.scale,
                    "tile_bits": args.tile, "traversed_edges": edges},
         "cpu_baseline": {"value": v, "unit": "GTEPS", "cores": oracle.max_threads(), "kind": "port",
                          "sample": f"{args.steps} full BFS runs from vertex 0 (oracle port of "
@@ -301,16 +315,17 @@ def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed):
             tq.put(None)
 
     def consumer():
+        bufs = {"bfs": np.empty(n, np.int32), "ppr": np.empty(n, np.float32)}  # reused per thread
         while True:
             item = tq.get()
             if item is None:
                 return
             kind, ticket = item
-            _, ms, _ = srv.wait(ticket, kind, timeout=120.0)
+            _, ms, _ = srv.wait(ticket, kind, timeout=120.0, out=bufs[kind])
             with lock:
                 lat[kind].append(ms)
 
-    consumers = 8
+    consumers = 12
     ths = [threading.Thread(target=producer)] + [threading.Thread(target=consumer) for _ in range(consumers)]
     for th in ths:
         th.start()
@@ -321,8 +336,7 @@ def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed):
     srv.close()
     out = {"offered_qps": rate_qps, "queries": nq, "achieved_qps": nq / wall, "wall_s": wall,
            "rounds": st["rounds"], "kernel_launches": st["kernel_launches"],
-           "phase_ms": {k: round(st[k], 1) for k in ("bfs_round_ms", "ppr_round_ms", "retire_ms", "spill_ms")},
-           "spilled": st["spilled"]}
+           "phase_ms": {k: round(st[k], 1) for k in ("bfs_round_ms", "ppr_round_ms", "retire_ms", "copy_ms")}}
     for k, v in lat.items():
         if v:
             out[f"{k}_p50_ms"] = float(np.percentile(v, 50))
@@ -341,6 +355,8 @@ def run_ours(args, ws, rank, local):
     t0 = time.perf_counter()
     # the symmetrised R-MAT graph may take top-down steps on small frontiers
     flags = gbo.FLAG_SYMMETRIC if args.direction == "auto" else 0
+    if args.layout == "col":
+        flags |= gbo.FLAG_LAYOUT_COL
     g = gbo.Graph.from_csr(csr, args.tile, flags)
     build_s = time.perf_counter() - t0
     info = g.info()
@@ -407,13 +423,16 @@ def run_ours(args, ws, rank, local):
     gbo.check(gbo.lib().gbo_graph_b2sr(g.h, r.ref(), c.ref(), None), "graph_b2sr")
     rowptr_b = gbo.device_to_numpy(r.value, np.int32, info.nblockrows + 1)
     colind_b = gbo.device_to_numpy(c.value, np.int32, int(info.nblocks))
-    lvl_bytes = bfs_level_bytes(rowptr_b, colind_b, levels, n, args.tile, np.diff(csr.rowptr) > 0)
+    lvl_bytes = bfs_level_bytes(rowptr_b, colind_b, levels, n, args.tile, np.diff(csr.rowptr) > 0, args.layout)
     per_level_ms = np.array(step_ms_all, np.float64).reshape(args.steps, -1)
     lvl_ms = per_level_ms.mean(axis=0)
     k = min(len(lvl_bytes), len(lvl_ms))
     peak, peak_src = load_peaks()
     achieved = sum(lvl_bytes[:k]) / (sum(lvl_ms[:k]) / 1e3) / 1e9
-    traffic = load_traffic("bfs_step_rmat22_b32.md")
+    traffic = load_traffic("k_bfs_step_rmat20_b32_ncu.md") if args.layout == "row" else None
+
+    # the BMV primitives, multi-source BFS and the server run on ROW tiles
+    g_row = g if args.layout == "row" else gbo.Graph.from_csr(csr, args.tile, gbo.FLAG_SYMMETRIC)
 
     # plain BSR-BMV count roofline on the same graph (random x, density 0.5)
     x = (np.random.default_rng(0).random(n) < 0.5).astype(np.int32)
@@ -421,12 +440,12 @@ def run_ours(args, ws, rank, local):
     dx = gbo.DeviceBuffer.from_numpy(xw)
     dy = gbo.DeviceBuffer(4 * n)
     for _ in range(3):
-        g.bmv_count(dx, dy)
+        g_row.bmv_count(dx, dy)
     gbo.sync()
     ev0.record()
     nb = 20
     for _ in range(nb):
-        g.bmv_count(dx, dy)
+        g_row.bmv_count(dx, dy)
     ev1.record()
     gbo.sync()
     bmv_ms = ev0.elapsed_ms(ev1) / nb
@@ -439,12 +458,12 @@ def run_ours(args, ws, rank, local):
     for kq in (64, 1024):
         srcs = rng.integers(0, n, kq).astype(np.int32)
         d_lv = gbo.DeviceBuffer(4 * n * kq)
-        g.msbfs(srcs, out=d_lv)
+        g_row.msbfs(srcs, out=d_lv)
         gbo.sync()
         reps = 3
         ev0.record()
         for _ in range(reps):
-            g.msbfs(srcs, out=d_lv)
+            g_row.msbfs(srcs, out=d_lv)
         ev1.record()
         gbo.sync()
         mms = ev0.elapsed_ms(ev1) / reps
@@ -455,12 +474,12 @@ def run_ours(args, ws, rank, local):
     # served: Poisson query streams into the continuous-batching server
     served = {}
     if not args.no_serve:
-        served["bfs_only"] = serve_stream(gbo, g, n, args.serve_qps, args.serve_s, 0.0, 5)
+        served["bfs_only"] = serve_stream(gbo, g_row, n, args.serve_qps, args.serve_s, 0.0, 5)
         # against one plain BFS per query on the device, and against the same
         # call with its levels read back to host memory (what a served query delivers)
         served["bfs_only"]["vs_plain_bfs_qps"] = served["bfs_only"]["achieved_qps"] / (1e3 / ms)
         served["bfs_only"]["vs_plain_e2e_qps"] = served["bfs_only"]["achieved_qps"] / (1e3 / e2e_ms)
-        served["mixed_10pct_ppr"] = serve_stream(gbo, g, n, args.serve_qps / 8, args.serve_s, 0.1, 6)
+        served["mixed_10pct_ppr"] = serve_stream(gbo, g_row, n, args.serve_qps / 8, args.serve_s, 0.1, 6)
     wb = max(1, args.tile // 8)
     bmv_bytes = (int(info.nblocks) * (args.tile * args.tile // 8 + 4) + 4 * (info.nblockrows + 1)
                  + wb * info.nblockcols + 4 * n)
@@ -471,8 +490,8 @@ def run_ours(args, ws, rank, local):
         "metric": "GTEPS", "value": gteps, "unit": "GTEPS", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": workload_name(args.scale, args.tile), "scale": args.scale,
-                   "tile_bits": args.tile, "nvertices": n, "nnz": csr.nnz,
+        "config": {"workload": workload_name(args.scale, args.tile, args.layout), "scale": args.scale,
+                   "tile_bits": args.tile, "layout": args.layout, "nvertices": n, "nnz": csr.nnz,
                    "nblocks": int(info.nblocks), "b2sr_gb": info.b2sr_bytes / 1e9,
                    "traversed_edges": edges, "bfs_depth": depth,
                    "l2": "inputs larger than L2 (B2SR tiles far above 126 MB)",
@@ -505,6 +524,8 @@ def run_ours(args, ws, rank, local):
                                           f"(median {t:.2f} s), oracle port of algorithm/bfs.cu:508-564"}
     if rank == 0:
         print(json.dumps(line), flush=True)
+    if g_row is not g:
+        g_row.free()
     g.free()
     dist.close()
 
@@ -661,28 +682,37 @@ def suite_config2(args, which):
 
 def suite_tc(args):
     """Triangle counting: king mesh 4096^2 and R-MAT 20 (seed 1), every tile
-    width timed and the fastest kept (the autotuned choice)."""
+    width timed in input vertex order and relabelled by descending degree
+    (the count is the same); the fastest combination is the tuned choice."""
     import gbo
 
     orc = _oracle()
-    for name, csr, known in (("king mesh 4096x4096", gbo.gen_king_mesh(4096), 4 * 4095 ** 2),
-                             ("R-MAT scale 20 ef16 seed 1", gbo.gen_rmat(20, 16, seed=1, **RMAT), None)):
+    graphs = {"mesh": lambda: ("king mesh 4096x4096", gbo.gen_king_mesh(4096), 4 * 4095 ** 2),
+              "rmat": lambda: ("R-MAT scale 20 ef16 seed 1", gbo.gen_rmat(20, 16, seed=1, **RMAT), None)}
+    orders = {"input": gbo.FLAG_LOWER, "degree": gbo.FLAG_LOWER | gbo.FLAG_DEGREE_ORDER}
+    for key in args.tc_graphs.split(","):
+        name, csr, known = graphs[key]()
         table = {}
         count = None
-        for b in (8, 16, 32, 64):
-            g = gbo.Graph.from_csr(csr, b, gbo.FLAG_LOWER)
-            count = g.tc()
-            if known is not None and count != known:
-                raise SystemExit(f"TC mismatch on {name}: {count} != {known}")
-            table[b] = _timed(gbo, g.tc, args.steps, args.warmup)
-            nblk = int(g.info().nblocks)
-            g.free()
-            table[b] = {"ms": table[b], "nblocks_L": nblk}
+        for order in args.tc_variants.split(","):
+            flags = orders[order]
+            for b in (int(t) for t in args.tc_tiles.split(",")):
+                t0 = time.perf_counter()
+                g = gbo.Graph.from_csr(csr, b, flags)
+                build_s = time.perf_counter() - t0
+                c = g.tc()
+                if count is None:
+                    count = c
+                if c != count or (known is not None and c != known):
+                    raise SystemExit(f"TC mismatch on {name} ({order}, b={b}): {c}")
+                ms = _timed(gbo, g.tc, args.steps, args.warmup)
+                table[f"{order}/b{b}"] = {"ms": ms, "nblocks_L": int(g.info().nblocks), "build_s": build_s}
+                g.free()
         best = min(table, key=lambda k: table[k]["ms"])
-        model_best, _ = gbo.tune_tile_width(csr, gbo.TUNE_TC, gbo.TUNE_MODEL)
         ms = table[best]["ms"]
-        lower_edges = (csr.nnz + 0) // 2
-        extra = {"triangles": count, "tile_table": table, "best_tile": best, "model_tile": model_best,
+        model_best, _ = gbo.tune_tile_width(csr, gbo.TUNE_TC, gbo.TUNE_MODEL)
+        lower_edges = csr.nnz // 2
+        extra = {"triangles": count, "tile_table": table, "best": best, "model_tile_input_order": model_best,
                  "dtype": "u64"}
         if not args.no_cpu:
             t = _cpu(lambda: orc.tc_csr(csr.rowptr, csr.colind, csr.nrows))
@@ -832,9 +862,10 @@ def suite_serve(args):
     csr = gbo.gen_rmat(21, 16, seed=2, **RMAT)
     g = gbo.Graph.from_csr(csr, 32)
     out = {}
-    for rate in (1000.0, 10000.0, 100000.0):
+    rates = [float(r) for r in args.serve_rates.split(",")]
+    for rate in rates:
         out[int(rate)] = serve_stream(gbo, g, csr.nrows, rate, min(args.serve_s, 2e4 / rate), 0.1, 11)
-    top = out[10000]
+    top = out[int(rates[len(rates) // 2])]
     _line("qps", top["achieved_qps"], "queries/s", True, 1e3 / max(top["achieved_qps"], 1e-9), args,
           {"workload": "served BFS + PPR queries, Poisson arrivals, R-MAT scale 21 seed 2, B2SR 32",
            "nvertices": csr.nrows, "nnz": csr.nnz}, dtype="u32", by_rate=out)

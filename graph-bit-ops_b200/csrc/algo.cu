@@ -327,6 +327,159 @@ __global__ void __launch_bounds__(kTPB) k_bfs_push(GView v, typename Word<B>::T*
   }
 }
 
+// ------------------------------------------------ COL tile layout (BFS)
+// With column words (word c of a tile = column c, row r at bit b-1-r) a pull
+// step needs, per tile, only the words of the columns whose frontier bit is
+// set: rows(I) |= OR_{c in x[C]} word_c(I, C).  Sparse frontier segments then
+// cost a word or two per tile instead of one word per unvisited row.
+
+// OR of a word across the warp.
+template <int B>
+__device__ __forceinline__ typename Word<B>::T warp_or(typename Word<B>::T w) {
+  if (B == 64) {
+    const unsigned long long u = (unsigned long long)w;
+    const unsigned lo = __reduce_or_sync(0xffffffffu, (unsigned)u);
+    const unsigned hi = __reduce_or_sync(0xffffffffu, (unsigned)(u >> 32));
+    return (typename Word<B>::T)(((unsigned long long)hi << 32) | lo);
+  }
+  return (typename Word<B>::T)__reduce_or_sync(0xffffffffu, (unsigned)w);
+}
+
+// OR of the column words of tile t selected by the set bits of sel (bit
+// b-1-c selects column c), four loads in flight.
+template <int B>
+__device__ __forceinline__ typename Word<B>::T or_selected_cols(const typename Word<B>::T* __restrict__ val,
+                                                                long long t, typename Word<B>::T sel) {
+  using WT = typename Word<B>::T;
+  unsigned long long a = (unsigned long long)sel << (64 - B);
+  WT acc = 0;
+  while (a) {
+    int c[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      c[q] = a ? __clzll((long long)a) : -1;
+      if (a) a &= ~(0x8000000000000000ull >> c[q]);
+    }
+    WT w[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) w[q] = c[q] >= 0 ? val[(size_t)t * B + c[q]] : (WT)0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc = (WT)(acc | w[q]);
+  }
+  return acc;
+}
+
+// Rows with an entry, COL layout: OR of every column word of the block row.
+template <int B>
+__global__ void __launch_bounds__(kTPB) k_live_col(GView v, typename Word<B>::T* __restrict__ live) {
+  using WT = typename Word<B>::T;
+  const unsigned lane = threadIdx.x & 31;
+  const long long item = warp_global();
+  if (item >= v.nitems) return;
+  const gbo_item it = v.items[item];
+  const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
+  WT acc = 0;
+  for (long long q = (long long)it.t0 * B + lane; q < (long long)it.t1 * B; q += 32) acc = (WT)(acc | val[q]);
+  acc = warp_or<B>(acc);
+  if (lane == 0 && acc) atomic_or_word<B>(live, it.row, acc);
+}
+
+// Pull step on COL tiles: a warp per work item, a lane per tile, 32 tiles
+// per batch; the block row leaves once its rows are all visited or found.
+template <int B>
+__global__ void __launch_bounds__(kTPB) k_bfs_step_col(GView v, typename Word<B>::T* __restrict__ front,
+                                                       typename Word<B>::T* __restrict__ visited,
+                                                       int* __restrict__ level, Ctrl* __restrict__ ctrl,
+                                                       typename Word<B>::T* __restrict__ scratch) {
+  using WT = typename Word<B>::T;
+  if (((volatile Ctrl*)ctrl)->done || ((volatile Ctrl*)ctrl)->mode) return;
+  const int lvl = ((volatile Ctrl*)ctrl)->iter;
+  const WT* __restrict__ x = front + (size_t)(lvl & 1) * v.nbr;
+  WT* __restrict__ out = front + (size_t)((lvl + 1) & 1) * v.nbr;
+  const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
+  const unsigned lane = threadIdx.x & 31;
+  const WT full = full_word<B>();
+  unsigned long long cnt = 0;
+  constexpr long long kGrab = 16;
+  long long w = 0, wend = 0;
+  for (;;) {
+    if (w == wend) {
+      unsigned long long g0 = 0;
+      if (lane == 0) g0 = atomicAdd(&ctrl->work, (unsigned long long)kGrab);
+      w = (long long)__shfl_sync(0xffffffffu, g0, 0);
+      wend = w + kGrab;
+    }
+    if (w >= v.nitems) break;
+    const gbo_item it = v.items[w];
+    ++w;
+    const WT vis = visited[it.row];
+    WT found = 0;
+    if ((vis & full) != full) {
+      // batch i's tiles are ORed while batch i+1's x words and batch i+2's
+      // block-column indices load
+      int c2 = (it.t0 + 32 + (int)lane < it.t1) ? v.colind[it.t0 + 32 + lane] : -1;
+      const int c1 = (it.t0 + (int)lane < it.t1) ? v.colind[it.t0 + lane] : -1;
+      WT x1 = c1 >= 0 ? x[c1] : (WT)0;
+      for (int base = it.t0; base < it.t1; base += 32) {
+        const WT xs = x1;
+        x1 = c2 >= 0 ? x[c2] : (WT)0;
+        c2 = (base + 64 + (int)lane < it.t1) ? v.colind[base + 64 + lane] : -1;
+        const WT acc = xs ? or_selected_cols<B>(val, base + lane, xs) : (WT)0;
+        found = (WT)(found | warp_or<B>(acc));
+        if ((WT)((found | vis) & full) == full) break;
+      }
+    }
+    if (it.slot >= 0) {
+      if (lane == 0) scratch[it.slot] = found;
+      continue;
+    }
+    const WT nw = (WT)(found & ~vis & full);
+    if (nw) {
+      for (int r = (int)lane; r < B; r += 32) {
+        const long long row = (long long)it.row * B + r;
+        if (bit_of<B>(nw, r) && row < v.nrows) level[row] = lvl + 1;
+      }
+      if (lane == 0) visited[it.row] = (WT)(vis | nw);
+    }
+    if (lane == 0) {
+      out[it.row] = nw;
+      cnt += popc_w(nw);
+    }
+  }
+  block_add_u64(cnt, &ctrl->count);
+}
+
+// Push step on COL tiles of a symmetric P: the neighbours of frontier row r
+// in block C are bit r of every column word of tile (J, C), so the lane of a
+// tile reads all its words and keeps the columns that meet the frontier rows.
+template <int B>
+__global__ void __launch_bounds__(kTPB) k_bfs_push_col(GView v, typename Word<B>::T* __restrict__ front,
+                                                       const typename Word<B>::T* __restrict__ visited,
+                                                       Ctrl* __restrict__ ctrl) {
+  using WT = typename Word<B>::T;
+  if (((volatile Ctrl*)ctrl)->done || !((volatile Ctrl*)ctrl)->mode) return;
+  const int lvl = ((volatile Ctrl*)ctrl)->iter;
+  const WT* __restrict__ x = front + (size_t)(lvl & 1) * v.nbr;
+  WT* out = front + (size_t)((lvl + 1) & 1) * v.nbr;
+  const unsigned lane = threadIdx.x & 31;
+  const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
+  const long long nwarps = warps_total();
+  for (long long item = warp_global(); item < v.nitems; item += nwarps) {
+    const gbo_item it = v.items[item];
+    const WT xs = x[it.row];
+    if (!xs) continue;
+    for (int t = it.t0 + (int)lane; t < it.t1; t += 32) {
+      const int C = v.colind[t];
+      WT cand = 0;
+#pragma unroll 8
+      for (int c = 0; c < B; ++c)
+        if ((WT)(val[(size_t)t * B + c] & xs)) cand = (WT)(cand | ((WT)1 << (B - 1 - c)));
+      cand = (WT)(cand & ~visited[C]);
+      if (cand) atomic_or_word<B>(out, C, cand);
+    }
+  }
+}
+
 template <int B>
 __global__ void k_bfs_finish(GView v, typename Word<B>::T* __restrict__ front,
                              typename Word<B>::T* __restrict__ visited, int* __restrict__ level,
@@ -802,7 +955,18 @@ int ensure_frontier(gbo_graph* g, AlgoState* a, cudaStream_t s) {
     GBO_CUDA_TRY(cudaMalloc(&a->live, wb * (size_t)(g->nbr + 1)));
     g->device_bytes += (long long)(wb * 4 * (g->nbr + 1));
     GBO_CUDA_TRY(cudaMemsetAsync(a->live, 0, wb * (size_t)(g->nbr + 1), s));
-    if (g->nitems > 0) {
+    if (g->nitems > 0 && g->layout == GBO_LAYOUT_COL) {
+      const GView v = view_of(g);
+      const unsigned grid = blocks_for_warps(g->nitems, kTPB / 32);
+      switch (g->b) {
+        case 4: k_live_col<4><<<grid, kTPB, 0, s>>>(v, (Word<4>::T*)a->live); break;
+        case 8: k_live_col<8><<<grid, kTPB, 0, s>>>(v, (Word<8>::T*)a->live); break;
+        case 16: k_live_col<16><<<grid, kTPB, 0, s>>>(v, (Word<16>::T*)a->live); break;
+        case 32: k_live_col<32><<<grid, kTPB, 0, s>>>(v, (Word<32>::T*)a->live); break;
+        default: k_live_col<64><<<grid, kTPB, 0, s>>>(v, (Word<64>::T*)a->live); break;
+      }
+      GBO_CUDA_TRY(cudaGetLastError());
+    } else if (g->nitems > 0) {
       const GView v = view_of(g);
       const unsigned grid = grid_for_items(g->nitems, g->b);
       switch (g->b) {
@@ -942,18 +1106,27 @@ int bfs_impl(gbo_graph* g, int src, const int* h_seeds, int nseeds, int32_t* d_l
   Ctrl* ctrl = a->ctrl;
   int* level = a->level;
   WT* scratch = (WT*)a->scratch;
-  const unsigned gi = grid_items_persistent(k_bfs_step<B>, g->nitems, B);
+  // the COL tile layout has its own pull and push kernels (column words)
+  const bool col = g->layout == GBO_LAYOUT_COL;
+  const unsigned gi = col ? grid_persistent(k_bfs_step_col<B>, g->nitems)
+                          : grid_items_persistent(k_bfs_step<B>, g->nitems, B);
   // push steps (symmetric graphs) finalise every block row in k_bfs_finish
   const bool push_ok = g->symmetric;
   const unsigned gs = blocks_for(std::max<long long>(g->nsplit, push_ok ? g->nbr : 0), kTPB);
-  const unsigned gp = grid_persistent(k_bfs_push<B>, g->nitems);
+  const unsigned gp = col ? grid_persistent(k_bfs_push_col<B>, g->nitems) : grid_persistent(k_bfs_push<B>, g->nitems);
   const unsigned gc = grid_vertex(g->nbr);
   GBO_TRY(get_exec(a, A_BFS, nullptr, [&](cudaStream_t cs, int k, int* nl) -> int {
     StepTimer tm{a, cs, k};
     tm.begin();
     if (push_ok) k_bfs_push_clear<B><<<gc, kTPB, 0, cs>>>(front, g->nbr, ctrl);
-    if (g->nitems > 0) k_bfs_step<B><<<gi, kTPB, 0, cs>>>(v, front, vis, level, ctrl, scratch);
-    if (push_ok && g->nitems > 0) k_bfs_push<B><<<gp, kTPB, 0, cs>>>(v, front, vis, ctrl);
+    if (g->nitems > 0) {
+      if (col) k_bfs_step_col<B><<<gi, kTPB, 0, cs>>>(v, front, vis, level, ctrl, scratch);
+      else k_bfs_step<B><<<gi, kTPB, 0, cs>>>(v, front, vis, level, ctrl, scratch);
+    }
+    if (push_ok && g->nitems > 0) {
+      if (col) k_bfs_push_col<B><<<gp, kTPB, 0, cs>>>(v, front, vis, ctrl);
+      else k_bfs_push<B><<<gp, kTPB, 0, cs>>>(v, front, vis, ctrl);
+    }
     tm.end();
     k_bfs_finish<B><<<gs, kTPB, 0, cs>>>(v, front, vis, level, ctrl, scratch);
     *nl += (g->nitems > 0) + 1 + (push_ok ? 1 + (g->nitems > 0) : 0);
@@ -1145,9 +1318,10 @@ int cc_impl(gbo_graph* g, int32_t* d_label, int* h_iters, cudaStream_t s) {
   return GBO_OK;
 }
 
-int check_algo_graph(const gbo_graph* g) {
+int check_algo_graph(const gbo_graph* g, bool col_ok = false) {
   if (!g) return fail(GBO_ERR_INVALID, "graph is NULL");
-  if (g->layout != GBO_LAYOUT_ROW) return fail(GBO_ERR_UNSUPPORTED, "algorithms need the ROW tile layout");
+  if (g->layout != GBO_LAYOUT_ROW && !col_ok)
+    return fail(GBO_ERR_UNSUPPORTED, "this algorithm needs the ROW tile layout (BFS and SSSP also take COL)");
   if (g->nrows != g->ncols) return fail(GBO_ERR_INVALID, "algorithms need a square matrix");
   return GBO_OK;
 }
@@ -1188,7 +1362,7 @@ using namespace gbo;
 extern "C" int gbo_bfs(const gbo_graph* gc, int src, int32_t* d_level, int* h_depth,
                        gbo_stream_t stream) {
   clear_error();
-  GBO_TRY(check_algo_graph(gc));
+  GBO_TRY(check_algo_graph(gc, true));
   gbo_graph* g = const_cast<gbo_graph*>(gc);
   if (src < 0 || src >= g->nrows) return fail(GBO_ERR_INVALID, "source vertex out of range");
   if (!d_level) return fail(GBO_ERR_INVALID, "level is NULL");
@@ -1209,7 +1383,7 @@ int bfs_seeded(gbo_graph* g, const int* h_seeds, int nseeds, int32_t* d_level, i
 extern "C" int gbo_sssp_unit(const gbo_graph* gc, int src, uint32_t* d_dist, int* h_iters,
                              gbo_stream_t stream) {
   clear_error();
-  GBO_TRY(check_algo_graph(gc));
+  GBO_TRY(check_algo_graph(gc, true));
   gbo_graph* g = const_cast<gbo_graph*>(gc);
   if (src < 0 || src >= g->nrows) return fail(GBO_ERR_INVALID, "source vertex out of range");
   if (!d_dist) return fail(GBO_ERR_INVALID, "dist is NULL");

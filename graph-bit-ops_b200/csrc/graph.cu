@@ -106,6 +106,7 @@ void destroy(gbo_graph* g) {
     cudaFree(g->val);
   }
   if (g->owns_outdeg) cudaFree(g->outdeg);
+  cudaFree(g->perm);
   cudaFree(g->invdeg);
   cudaFree(g->items);
   cudaFree(g->splits);
@@ -120,6 +121,9 @@ void destroy(gbo_graph* g) {
 // Host CSR transpose used when GBO_FLAG_TRANSPOSE is given with host pointers.
 int host_transpose(const int* rowptr, const int* colind, int nrows, int ncols, long long nnz,
                    std::vector<int>* tptr, std::vector<int>* tcol);
+// Host relabelling by descending degree (GBO_FLAG_DEGREE_ORDER).
+int host_degree_relabel(const int* rowptr, const int* colind, int n, long long nnz,
+                        std::vector<int>* new_of_old, std::vector<int>* nptr, std::vector<int>* ncol);
 
 }  // namespace gbo
 
@@ -166,9 +170,38 @@ extern "C" int gbo_graph_from_csr(const int* rowptr, const int* colind, int nrow
     pcol = nrows;
     src_device = false;
   }
+  // Relabel by descending degree: the packed matrix is P' = Q P Q^T.  Row
+  // lengths of the lower triangle are then bounded by the number of
+  // higher-degree neighbours, which keeps hub rows short for TC.
+  std::vector<int> perm, rptr, rcol;
+  if (flags & GBO_FLAG_DEGREE_ORDER) {
+    if (prow != pcol) return fail(GBO_ERR_INVALID, "GBO_FLAG_DEGREE_ORDER needs a square matrix");
+    if (transpose) return fail(GBO_ERR_UNSUPPORTED, "GBO_FLAG_DEGREE_ORDER does not combine with GBO_FLAG_TRANSPOSE");
+    if (src_device) {
+      hptr.resize((size_t)prow + 1);
+      hcol.resize((size_t)nnz);
+      GBO_CUDA_TRY(cudaMemcpyAsync(hptr.data(), src_ptr, sizeof(int) * hptr.size(), cudaMemcpyDeviceToHost, s));
+      if (nnz) GBO_CUDA_TRY(cudaMemcpyAsync(hcol.data(), src_col, sizeof(int) * hcol.size(), cudaMemcpyDeviceToHost, s));
+      GBO_CUDA_TRY(cudaStreamSynchronize(s));
+      src_ptr = hptr.data();
+      src_col = hcol.data();
+      src_device = false;
+    }
+    GBO_TRY(host_degree_relabel(src_ptr, src_col, prow, nnz, &perm, &rptr, &rcol));
+    src_ptr = rptr.data();
+    src_col = rcol.data();
+  }
 
   gbo_graph* g = new gbo_graph();
   g->symmetric = (flags & GBO_FLAG_SYMMETRIC) && !lower && nrows == ncols;
+  if (!perm.empty()) {
+    if (cudaMalloc(&g->perm, sizeof(int) * perm.size()) != cudaSuccess ||
+        cudaMemcpy(g->perm, perm.data(), sizeof(int) * perm.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+      destroy(g);
+      return fail(GBO_ERR_NOMEM, "permutation upload");
+    }
+    g->device_bytes += 4LL * (long long)perm.size();
+  }
   DevCsr csr, low;
   int st = upload_csr(src_ptr, src_col, prow, nnz, src_device, s, &csr);
   const DevCsr* use = &csr;
@@ -287,12 +320,18 @@ extern "C" int gbo_graph_outdeg(const gbo_graph* g, const int** d) {
   return GBO_OK;
 }
 
+extern "C" int gbo_graph_permutation(const gbo_graph* g, const int** d_new_of_old) {
+  clear_error();
+  if (!g || !d_new_of_old) return fail(GBO_ERR_INVALID, "NULL argument");
+  *d_new_of_old = g->perm;
+  return GBO_OK;
+}
+
 extern "C" int gbo_graph_set_bfs_direction(gbo_graph* g, int symmetric, int push_threshold) {
   clear_error();
   if (!g) return fail(GBO_ERR_INVALID, "NULL graph");
   if (push_threshold < -1) return fail(GBO_ERR_INVALID, "push_threshold must be >= -1");
-  if (symmetric && (g->nrows != g->ncols || g->layout != GBO_LAYOUT_ROW))
-    return fail(GBO_ERR_UNSUPPORTED, "push steps need a square ROW-layout graph");
+  if (symmetric && g->nrows != g->ncols) return fail(GBO_ERR_UNSUPPORTED, "push steps need a square graph");
   g->symmetric = symmetric != 0;
   g->bfs_push_thr = push_threshold;
   return GBO_OK;

@@ -28,6 +28,7 @@ struct gbo_graph {
   bool owns_b2sr = true;
   bool symmetric = false;  // caller asserts P == P^T (enables push BFS steps)
   int bfs_push_thr = -1;   // push below this frontier size (-1: nrows / 64)
+  int* perm = nullptr;     // GBO_FLAG_DEGREE_ORDER: new label of every input vertex
   bool owns_outdeg = true;
   // balanced schedule
   int chunk = 0;

@@ -25,6 +25,8 @@ namespace gbo {
 
 int host_transpose(const int* rowptr, const int* colind, int nrows, int ncols, long long nnz,
                    std::vector<int>* tptr, std::vector<int>* tcol);
+int host_degree_relabel(const int* rowptr, const int* colind, int n, long long nnz,
+                        std::vector<int>* new_of_old, std::vector<int>* nptr, std::vector<int>* ncol);
 
 namespace {
 
@@ -222,6 +224,45 @@ int host_transpose(const int* rowptr, const int* colind, int nrows, int ncols, l
   // rows visited in ascending order: every column's row list comes out sorted
   for (int r = 0; r < nrows; ++r)
     for (int k = rowptr[r]; k < rowptr[r + 1]; ++k) (*tcol)[(size_t)pos[colind[k]]++] = r;
+  return GBO_OK;
+}
+
+// Relabel the vertices of a square CSR by descending degree (ties by id):
+// (*new_of_old)[v] is the new label of v; the relabelled CSR comes out with
+// every row's columns ascending.
+int host_degree_relabel(const int* rowptr, const int* colind, int n, long long nnz,
+                        std::vector<int>* new_of_old, std::vector<int>* nptr, std::vector<int>* ncol) {
+  std::vector<int> order((size_t)n);
+  for (int v = 0; v < n; ++v) order[(size_t)v] = v;
+  std::sort(order.begin(), order.end(), [&](int a, int b) {
+    const int da = rowptr[a + 1] - rowptr[a], db = rowptr[b + 1] - rowptr[b];
+    return da != db ? da > db : a < b;
+  });
+  new_of_old->resize((size_t)n);
+  for (int k = 0; k < n; ++k) (*new_of_old)[(size_t)order[(size_t)k]] = k;
+  nptr->assign((size_t)n + 1, 0);
+  for (int k = 0; k < n; ++k) {
+    const int v = order[(size_t)k];
+    (*nptr)[(size_t)k + 1] = (*nptr)[(size_t)k] + (rowptr[v + 1] - rowptr[v]);
+  }
+  ncol->resize((size_t)nnz);
+  std::atomic<int> bad{0};
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (int k = 0; k < n; ++k) {
+    const int v = order[(size_t)k];
+    int* dst = ncol->data() + (*nptr)[(size_t)k];
+    for (int j = rowptr[v]; j < rowptr[v + 1]; ++j) {
+      const int c = colind[j];
+      if (c < 0 || c >= n) {
+        bad = 1;
+        *dst++ = 0;
+      } else {
+        *dst++ = (*new_of_old)[(size_t)c];
+      }
+    }
+    std::sort(ncol->data() + (*nptr)[(size_t)k], dst);
+  }
+  if (bad) return fail(GBO_ERR_BOUNDS, "CSR column index outside [0, n)");
   return GBO_OK;
 }
 

@@ -223,8 +223,7 @@ extern "C" int gbo_bfs_multi(const gbo_graph* gc, const int* h_seeds, int nseeds
   clear_error();
   if (!gc) return fail(GBO_ERR_INVALID, "graph is NULL");
   gbo_graph* g = const_cast<gbo_graph*>(gc);
-  if (g->layout != GBO_LAYOUT_ROW || g->nrows != g->ncols)
-    return fail(GBO_ERR_INVALID, "BFS needs a square ROW-layout graph");
+  if (g->nrows != g->ncols) return fail(GBO_ERR_INVALID, "BFS needs a square graph");
   if (nseeds < 1 || !h_seeds || !d_level) return fail(GBO_ERR_INVALID, "bad argument");
   for (int s = 0; s < nseeds; ++s)
     if (h_seeds[s] < 0 || h_seeds[s] >= g->nrows) return fail(GBO_ERR_INVALID, "seed out of range");

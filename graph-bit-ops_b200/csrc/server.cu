@@ -32,6 +32,15 @@ constexpr int kPprSlots = 32;
 constexpr int kPprTPB = 128;
 constexpr int kPprWarps = kPprTPB / 32;
 
+// Wait for the work queued on st with a blocking-sync event: the calling
+// thread sleeps instead of spinning, so client threads, the two workers and
+// the caller's own threads do not starve each other of host cores.
+cudaError_t wait_stream(cudaStream_t st, cudaEvent_t ev) {
+  cudaError_t e = cudaEventRecord(ev, st);
+  if (e == cudaSuccess) e = cudaEventSynchronize(ev);
+  return e;
+}
+
 double now_ms() {
   using namespace std::chrono;
   return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
@@ -53,13 +62,26 @@ struct PprArgs {
 
 // One iteration for all 32 slots: X'[i][s] = alpha * sum_{j: P[i][j]} X[j][s]
 // inv[j] + P[i][s]; lane = slot; fp64 accumulators in shared memory.
+// A warp walks its item's tiles kU at a time (lane = tile row: one word per
+// lane per tile, loaded together); each set bit (row r, column j) goes to a
+// per-warp list in shared memory at the position a warp prefix sum of the
+// lanes' bit counts gives it; the list is then consumed with lane = slot,
+// kP X-row gathers in flight.  Tiles with more bits than the list holds are
+// walked directly.  The (row, column) order is the tiles' own, so every
+// column's sum has a fixed order whatever the other slots hold.
+constexpr int kPprList = 256;
+
 __global__ void __launch_bounds__(kPprTPB) k_ppr_step(PprArgs a) {
   __shared__ double acc_sh[kPprWarps][32 * kPprSlots];
+  __shared__ int lj_sh[kPprWarps][kPprList];
+  __shared__ unsigned char lr_sh[kPprWarps][kPprList];
   const GView& v = a.v;
   const unsigned lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const long long item = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   double* acc = acc_sh[wib];
+  int* lj = lj_sh[wib];
+  unsigned char* lr = lr_sh[wib];
   const float* __restrict__ X = a.X + (size_t)a.parity * a.xstride;
   float* __restrict__ Xn = a.X + (size_t)(a.parity ^ 1) * a.xstride;
   double e = 0.0;
@@ -68,81 +90,80 @@ __global__ void __launch_bounds__(kPprTPB) k_ppr_step(PprArgs a) {
     __syncwarp();
     const gbo_item it = v.items[item];
     const uint32_t* __restrict__ val = reinterpret_cast<const uint32_t*>(v.val);
-    // kU tile words per lane (lane = tile row) load together; the set bits
-    // (tile row r, column j) of those tiles are then walked in order and
-    // their X rows (lane = slot) gathered kP at a time.
+    const bool lane_active = (a.active >> lane) & 1u;
     constexpr int kU = 8, kP = 8;
+    int nl = 0;  // list length (warp-uniform)
+    auto flush = [&]() {
+      for (int q0 = 0; q0 < nl; q0 += kP) {
+        int rq[kP];
+        float xv[kP], iv[kP];
+#pragma unroll
+        for (int q = 0; q < kP; ++q) {
+          rq[q] = q0 + q < nl ? (int)lr[q0 + q] : -1;
+          if (rq[q] >= 0 && lane_active) {
+            const size_t jj = (size_t)lj[q0 + q];
+            xv[q] = X[jj * kPprSlots + lane];
+            iv[q] = a.inv[jj];
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < kP; ++q)
+          if (rq[q] >= 0 && lane_active) acc[rq[q] * kPprSlots + lane] += (double)(xv[q] * iv[q]);
+      }
+      nl = 0;
+      __syncwarp();
+    };
     for (int b0 = it.t0; b0 < it.t1; b0 += 32) {
       const int t = b0 + (int)lane;
       const int cb = t < it.t1 ? v.colind[t] : 0;
       const int ntile = min(32, it.t1 - b0);
       for (int g0 = 0; g0 < ntile; g0 += kU) {
         uint32_t wr[kU];
-        unsigned rowsk[kU];
-        int ck[kU];
 #pragma unroll
         for (int k = 0; k < kU; ++k) wr[k] = g0 + k < ntile ? val[(size_t)(b0 + g0 + k) * 32 + lane] : 0u;
 #pragma unroll
         for (int k = 0; k < kU; ++k) {
-          rowsk[k] = __ballot_sync(0xffffffffu, wr[k] != 0);
-          ck[k] = __shfl_sync(0xffffffffu, cb, (g0 + k) & 31);
-        }
-        auto sel_w = [&](int k) {
-          uint32_t x = wr[0];
+          const int cnt = __popc(wr[k]);
+          int incl = cnt;
 #pragma unroll
-          for (int q = 1; q < kU; ++q) x = k == q ? wr[q] : x;
-          return x;
-        };
-        auto sel_i = [&](const int* arr, int k) {
-          int x = arr[0];
-#pragma unroll
-          for (int q = 1; q < kU; ++q) x = k == q ? arr[q] : x;
-          return x;
-        };
-        int kk = 0;
-        unsigned rows = rowsk[0], cur = 0;
-        int cr = 0;
-        for (;;) {
-          int pr[kP];
-          size_t pj[kP];
-#pragma unroll
-          for (int q = 0; q < kP; ++q) {
-            while (!cur) {  // warp-uniform: rows and cur come from ballots and shuffles
-              if (rows) {
-                cr = __ffs(rows) - 1;
-                rows &= rows - 1;
-                cur = __shfl_sync(0xffffffffu, sel_w(kk), cr);
-              } else if (kk + 1 < kU) {
-                ++kk;
-                rows = (unsigned)sel_i(reinterpret_cast<const int*>(rowsk), kk);
-              } else {
-                break;
+          for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if ((int)lane >= o) incl += y;
+          }
+          const int total = __shfl_sync(0xffffffffu, incl, 31);
+          if (total == 0) continue;
+          const int C = __shfl_sync(0xffffffffu, cb, (g0 + k) & 31);
+          if (nl + total > kPprList) flush();
+          if (total > kPprList) {  // a dense tile: walk its bits directly
+            unsigned rows = __ballot_sync(0xffffffffu, wr[k] != 0);
+            while (rows) {
+              const int r = __ffs(rows) - 1;
+              rows &= rows - 1;
+              unsigned bits = __shfl_sync(0xffffffffu, wr[k], r);
+              while (bits) {
+                const int col = __clz(bits);
+                bits &= ~(0x80000000u >> col);
+                const size_t jj = (size_t)C * 32 + col;
+                if (lane_active) acc[r * kPprSlots + lane] += (double)(X[jj * kPprSlots + lane] * a.inv[jj]);
               }
             }
-            pr[q] = -1;
-            pj[q] = 0;
-            if (cur) {
-              const int col = __clz(cur);
-              cur &= ~(0x80000000u >> col);
-              pr[q] = cr;
-              pj[q] = (size_t)sel_i(ck, kk) * 32 + col;
-            }
+            continue;
           }
-          if (pr[0] < 0) break;
-          float xv[kP], iv[kP];
-#pragma unroll
-          for (int q = 0; q < kP; ++q)
-            if (pr[q] >= 0) {
-              xv[q] = X[pj[q] * kPprSlots + lane];
-              iv[q] = a.inv[pj[q]];
-            }
-#pragma unroll
-          for (int q = 0; q < kP; ++q)
-            if (pr[q] >= 0) acc[pr[q] * kPprSlots + lane] += (double)(xv[q] * iv[q]);
+          int pos = nl + incl - cnt;
+          unsigned bits = wr[k];
+          while (bits) {
+            const int col = __clz(bits);
+            bits &= ~(0x80000000u >> col);
+            lj[pos] = C * 32 + col;
+            lr[pos] = (unsigned char)lane;
+            ++pos;
+          }
+          nl += total;
+          __syncwarp();
         }
       }
     }
-    __syncwarp();
+    flush();
     if (it.slot >= 0) {
       double* dst = a.scratch + (size_t)it.slot * 32 * kPprSlots;
       for (int q = lane; q < 32 * kPprSlots; q += 32) dst[q] = acc[q];
@@ -241,28 +262,29 @@ __global__ void k_ppr_admit_set(float* X, size_t xstride, int parity, float* P, 
 }
 
 // ------------------------------------------------------------- retirement
-// Up to kRetire finished slots leave per round.  Their results are written
-// to a device staging area (one n-vector per slot) by a transposing kernel
-// that reads the slots' values row by row and writes each result
-// contiguously; the staging area then goes to pinned host buffers with
-// asynchronous copies on a second stream, so the next round overlaps them.
-constexpr int kRetire = 64;
-constexpr int kRetRows = 64;  // rows per block of the transposing kernels
+// Up to kRetire finished slots of an engine leave per round.  A transposing
+// kernel reads their values row by row and writes each result contiguously
+// into its own buffer of a device result pool; the result stays there until
+// a client takes it (wait/poll copy it to the host), so the engines never
+// wait on host copies or on the order in which clients collect.
+constexpr int kRetire = 128;
+constexpr int kRetRows = 32;  // rows per block of the transposing kernels
 
 struct RetireList {
   int count;
   int slot[kRetire];
   int start[kRetire];
-  uint32_t clr[32];  // visited bits to clear, per source word
+  uint32_t clr[32];     // visited bits to clear, per source word
+  void* out[kRetire];   // destination buffer of each retired slot
 };
 
 // BFS: out[f][i] = level of (i, slot f) relative to its start level, -1 if
 // unreachable; the slot's levels become -1 and its visited bits 0.  When
-// every retired query is shallower than 255 levels (u8), the results leave
-// as one byte per vertex (255 = unreachable), a quarter of the bytes to
-// copy to the host; the client widens them to int32.
+// every retired query is shallower than 255 levels (u8), a result is one
+// byte per vertex (255 = unreachable), a quarter of the bytes the client
+// copies; the client widens them to int32.
 __global__ void __launch_bounds__(256) k_bfs_retire(int* levels, int g, uint32_t* V, int n, int kw,
-                                                    RetireList rl, void* out, int u8) {
+                                                    RetireList rl, int u8) {
   __shared__ int sm[kRetire][kRetRows + 1];
   const long long i0 = (long long)blockIdx.x * kRetRows;
   const int R = rl.count;
@@ -287,14 +309,14 @@ __global__ void __launch_bounds__(256) k_bfs_retire(int* levels, int g, uint32_t
     const long long i = i0 + ii;
     if (i >= n) continue;
     if (u8)
-      static_cast<uint8_t*>(out)[(size_t)f * n + i] = sm[f][ii] < 0 ? (uint8_t)255 : (uint8_t)sm[f][ii];
+      static_cast<uint8_t*>(rl.out[f])[i] = sm[f][ii] < 0 ? (uint8_t)255 : (uint8_t)sm[f][ii];
     else
-      static_cast<int*>(out)[(size_t)f * n + i] = sm[f][ii];
+      static_cast<int*>(rl.out[f])[i] = sm[f][ii];
   }
 }
 
 // PPR: out[f][i] = X[i][slot f] of the current iterate.
-__global__ void __launch_bounds__(256) k_ppr_retire(const float* X, int n, RetireList rl, float* out) {
+__global__ void __launch_bounds__(256) k_ppr_retire(const float* X, int n, RetireList rl) {
   __shared__ float sm[kRetire][kRetRows + 1];
   const long long i0 = (long long)blockIdx.x * kRetRows;
   const int R = rl.count;
@@ -307,7 +329,7 @@ __global__ void __launch_bounds__(256) k_ppr_retire(const float* X, int n, Retir
   for (int q = threadIdx.x; q < kRetRows * R; q += blockDim.x) {
     const int f = q / kRetRows, ii = q % kRetRows;
     const long long i = i0 + ii;
-    if (i < n) out[(size_t)f * n + i] = sm[f][ii];
+    if (i < n) static_cast<float*>(rl.out[f])[i] = sm[f][ii];
   }
 }
 
@@ -336,13 +358,14 @@ struct Query {
 
 struct Result {
   int kind;
-  int buf;          // pinned pool buffer holding the result (-1: moved to heap)
+  int pool;         // 0: byte pool (BFS levels < 255), 1: word pool (PPR, deep BFS)
+  int buf;          // buffer index in that pool (-1: moved to host memory)
   int u8;           // BFS levels stored one byte per vertex (255 = unreachable)
-  cudaEvent_t ev;   // its copy has landed when this event completes
-  bool landed;
+  cudaEvent_t ev;   // the result is in its buffer once this event completes
   double t_submit, t_done;
   int iters;
-  std::vector<unsigned char> heap;  // the result once moved out of the pinned pool
+  bool moving = false;             // being copied to host memory by a worker
+  std::vector<unsigned char> host;  // the result once moved out of the pool
 };
 
 }  // namespace
@@ -353,10 +376,10 @@ struct gbo_server {
   int n = 0, nbr = 0;
   float alpha = 0.85f, tol = 1e-7f;
   int ppr_max_iter = 1000;
-  // one worker thread per engine (0 BFS, 1 PPR), each with its own compute
-  // stream and result-copy stream, so the engines overlap on the GPU
+  // one worker thread per engine (0 BFS, 1 PPR), each with its own stream,
+  // so the engines overlap on the GPU
   cudaStream_t s[2] = {nullptr, nullptr};
-  cudaStream_t cs[2] = {nullptr, nullptr};
+  cudaEvent_t sync_ev[2] = {nullptr, nullptr};  // blocking-sync events of the workers
   int dev = 0;
   // BFS engine (levels grouped 8 sources per 32-byte sector)
   int kb = 0, kw = 0;
@@ -385,20 +408,18 @@ struct gbo_server {
   std::vector<long long> pslot_ticket;
   std::vector<int> pslot_iters;
   std::vector<char> pslot_finished;
-  // results: device staging (double-buffered per engine), pinned host pool
-  void* d_stage[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
-  cudaEvent_t stage_free[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
-  int stage_next[2] = {0, 0};
-  std::vector<void*> pool;
-  std::vector<int> pool_free;
-  std::vector<cudaEvent_t> pool_ev;
+  // results wait on the device: pool 0 holds n-byte buffers (BFS levels),
+  // pool 1 n-word buffers (PPR values, BFS levels of deep queries)
+  char* dpool[2] = {nullptr, nullptr};
+  size_t dbytes[2] = {0, 0};       // bytes per buffer
+  std::vector<int> pool_free[2];
+  std::vector<cudaEvent_t> pool_ev[2];
   // host side
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<gbo::Query> pending[2];
   std::map<long long, gbo::Result> results;
   std::map<long long, double> submit_time;
-  int copies_in_flight = 0;
   long long next_ticket = 1;
   bool stop = false;
   int worker_status = GBO_OK;
@@ -407,8 +428,7 @@ struct gbo_server {
   // statistics
   std::atomic<long long> rounds{0}, launches{0};
   long long bfs_done = 0, ppr_done = 0;
-  double phase_ms[4] = {0, 0, 0, 0};  // BFS round, PPR round, retire, spill (under mu)
-  long long spilled = 0;
+  double phase_ms[4] = {0, 0, 0, 0};  // BFS round, PPR round, retire, client copies (under mu)
 };
 
 namespace gbo {
@@ -469,7 +489,7 @@ int bfs_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
   S->launches += 2;
   GBO_CUDA_TRY(cudaGetLastError());
   GBO_CUDA_TRY(cudaMemcpyAsync(S->h_slot_any, S->slot_any, sizeof(uint32_t) * S->kw, cudaMemcpyDeviceToHost, st));
-  GBO_CUDA_TRY(cudaStreamSynchronize(st));
+  GBO_CUDA_TRY(wait_stream(st, S->sync_ev[0]));
   S->level += 1;
   std::lock_guard<std::mutex> lk(S->mu);  // finished flags are read by the other worker
   for (int q = 0; q < S->kb; ++q)
@@ -525,7 +545,7 @@ int ppr_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
   S->launches += 2;
   GBO_CUDA_TRY(cudaGetLastError());
   GBO_CUDA_TRY(cudaMemcpyAsync(S->h_err, S->err, sizeof(double) * kPprSlots, cudaMemcpyDeviceToHost, st));
-  GBO_CUDA_TRY(cudaStreamSynchronize(st));
+  GBO_CUDA_TRY(wait_stream(st, S->sync_ev[1]));
   S->parity ^= 1;
   std::lock_guard<std::mutex> lk(S->mu);  // finished flags are read by the other worker
   for (int q = 0; q < kPprSlots; ++q) {
@@ -537,127 +557,120 @@ int ppr_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
   return GBO_OK;
 }
 
-// Retire finished slots of one engine (kind 0 BFS, 1 PPR) while pinned
-// buffers are free.  Called without the lock.
+// Retire finished slots of one engine (kind 0 BFS, 1 PPR) into free device
+// result buffers.  Called without the lock.
 int retire(gbo_server* S, int kind) {
   std::vector<long long>& tick = kind == 0 ? S->bslot_ticket : S->pslot_ticket;
   std::vector<char>& fin = kind == 0 ? S->bslot_finished : S->pslot_finished;
-  RetireList rl;
-  memset(&rl, 0, sizeof(rl));
-  std::vector<int> bufs;
+  // BFS results of queries shallower than 255 levels go to the byte pool,
+  // the others to the word pool; one launch per pool
+  RetireList rl[2];
+  std::vector<int> bufs[2];
+  for (int p = 0; p < 2; ++p) memset(&rl[p], 0, sizeof(RetireList));
   {
     std::lock_guard<std::mutex> lk(S->mu);
-    for (size_t q = 0; q < tick.size() && rl.count < kRetire; ++q) {
-      if (tick[q] <= 0 || !fin[q] || S->pool_free.empty()) continue;
-      rl.slot[rl.count] = (int)q;
-      rl.start[rl.count] = kind == 0 ? S->bslot_start[q] : 0;
-      if (kind == 0) rl.clr[q / 32] |= 1u << (q % 32);
-      bufs.push_back(S->pool_free.back());
-      S->pool_free.pop_back();
-      rl.count++;
+    for (size_t q = 0; q < tick.size(); ++q) {
+      if (tick[q] <= 0 || !fin[q]) continue;
+      const int p = kind == 0 && S->level - S->bslot_start[q] < 255 ? 0 : 1;
+      if (rl[p].count >= kRetire || S->pool_free[p].empty()) continue;
+      const int b = S->pool_free[p].back();
+      S->pool_free[p].pop_back();
+      RetireList& r = rl[p];
+      r.slot[r.count] = (int)q;
+      r.start[r.count] = kind == 0 ? S->bslot_start[q] : 0;
+      r.out[r.count] = S->dpool[p] + (size_t)b * S->dbytes[p];
+      if (kind == 0) r.clr[q / 32] |= 1u << (q % 32);
+      bufs[p].push_back(b);
+      r.count++;
     }
   }
-  if (rl.count == 0) return GBO_OK;
-  cudaStream_t st = S->s[kind], cst = S->cs[kind];
-  const int sb = S->stage_next[kind];
-  S->stage_next[kind] ^= 1;
-  void* stage = S->d_stage[kind][sb];
-  GBO_CUDA_TRY(cudaStreamWaitEvent(st, S->stage_free[kind][sb], 0));  // its previous copies are done
+  cudaStream_t st = S->s[kind];
   const unsigned grid = blocks_for(S->n, kRetRows);
-  int u8 = 0;
-  if (kind == 0) {
-    int deepest = 0;
-    for (int f = 0; f < rl.count; ++f) deepest = std::max(deepest, S->level - rl.start[f]);
-    u8 = deepest < 255;
+  const double t_now = now_ms();
+  for (int p = 0; p < 2; ++p) {
+    if (rl[p].count == 0) continue;
     // retired columns were already out of the active set: rows marked
     // finished stay finished
-    k_bfs_retire<<<grid, 256, 0, st>>>(S->levels, 8, S->V, S->n, S->kw, rl, stage, u8);
+    if (kind == 0) k_bfs_retire<<<grid, 256, 0, st>>>(S->levels, 8, S->V, S->n, S->kw, rl[p], p == 0);
+    else k_ppr_retire<<<grid, 256, 0, st>>>(S->X + (size_t)S->parity * S->n * kPprSlots, S->n, rl[p]);
     S->launches += 1;
-  } else {
-    k_ppr_retire<<<grid, 256, 0, st>>>(S->X + (size_t)S->parity * S->n * kPprSlots, S->n, rl, (float*)stage);
-    S->launches += 1;
+    GBO_CUDA_TRY(cudaGetLastError());
+    for (int b : bufs[p]) GBO_CUDA_TRY(cudaEventRecord(S->pool_ev[p][(size_t)b], st));
+    std::lock_guard<std::mutex> lk(S->mu);
+    for (int f = 0; f < rl[p].count; ++f) {
+      const int q = rl[p].slot[f];
+      const long long t = tick[(size_t)q];
+      Result r;
+      r.kind = kind;
+      r.pool = p;
+      r.buf = bufs[p][(size_t)f];
+      r.u8 = kind == 0 && p == 0;
+      r.ev = S->pool_ev[p][(size_t)r.buf];
+      r.t_submit = S->submit_time[t];
+      r.t_done = t_now;
+      r.iters = kind == 0 ? S->level - S->bslot_start[(size_t)q] : S->pslot_iters[(size_t)q];
+      S->results[t] = r;
+      tick[(size_t)q] = 0;
+      fin[(size_t)q] = 0;
+      if (kind == 0) S->bfs_done++;
+      else S->ppr_done++;
+    }
+    S->cv_done.notify_all();
   }
-  GBO_CUDA_TRY(cudaGetLastError());
-  cudaEvent_t ready;
-  GBO_CUDA_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
-  GBO_CUDA_TRY(cudaEventRecord(ready, st));
-  GBO_CUDA_TRY(cudaStreamWaitEvent(cst, ready, 0));
-  cudaEventDestroy(ready);
-  const size_t rbytes = (u8 ? 1 : sizeof(int)) * (size_t)S->n;
-  const double t_now = now_ms();
-  std::lock_guard<std::mutex> lk(S->mu);
-  for (int f = 0; f < rl.count; ++f) {
-    const int b = bufs[(size_t)f];
-    GBO_CUDA_TRY(cudaMemcpyAsync(S->pool[(size_t)b], (char*)stage + (size_t)f * rbytes, rbytes,
-                                 cudaMemcpyDeviceToHost, cst));
-    GBO_CUDA_TRY(cudaEventRecord(S->pool_ev[(size_t)b], cst));
-    const int q = rl.slot[f];
-    const long long t = tick[(size_t)q];
-    Result r;
-    r.kind = kind;
-    r.buf = b;
-    r.u8 = u8;
-    r.ev = S->pool_ev[(size_t)b];
-    r.landed = false;
-    r.t_submit = S->submit_time[t];
-    r.t_done = t_now;
-    r.iters = kind == 0 ? S->level - S->bslot_start[(size_t)q] : S->pslot_iters[(size_t)q];
-    S->results[t] = r;
-    S->copies_in_flight++;
-    tick[(size_t)q] = 0;
-    fin[(size_t)q] = 0;
-    if (kind == 0) S->bfs_done++;
-    else S->ppr_done++;
-  }
-  GBO_CUDA_TRY(cudaEventRecord(S->stage_free[kind][sb], cst));
   return GBO_OK;
 }
 
-// Mark results whose copies have landed (caller holds the lock).
-bool collect_landed(gbo_server* S) {
-  bool any = false;
-  if (S->copies_in_flight == 0) return false;
-  const double t = now_ms();
-  for (auto& kv : S->results) {
-    Result& r = kv.second;
-    if (r.landed) continue;
-    if (cudaEventQuery(r.ev) == cudaSuccess) {
-      r.landed = true;
-      r.t_done = t;
-      S->copies_in_flight--;
-      any = true;
-    } else {
-      (void)cudaGetLastError();  // cudaErrorNotReady is not an error here
-    }
+// Pool that finished slots of this engine wait for while it has no free
+// buffer, or -1 (caller holds the lock).
+int blocked_pool(gbo_server* S, int kind) {
+  const std::vector<long long>& tab = kind == 0 ? S->bslot_ticket : S->pslot_ticket;
+  const std::vector<char>& fin = kind == 0 ? S->bslot_finished : S->pslot_finished;
+  for (size_t q = 0; q < tab.size(); ++q) {
+    if (tab[q] <= 0 || !fin[q]) continue;
+    const int p = kind == 0 && S->level - S->bslot_start[q] < 255 ? 0 : 1;
+    if (S->pool_free[p].empty()) return p;
   }
-  return any;
+  return -1;
 }
 
-// Results that nobody has taken yet keep their pinned buffers; when every
-// buffer is held that way and finished slots wait for one, move landed
-// results to heap memory (oldest tickets first) so that retirement never
-// waits on the order in which clients collect (caller holds the lock).
-bool spill_landed(gbo_server* S) {
-  bool waiting = false;
-  for (size_t q = 0; q < S->bslot_ticket.size() && !waiting; ++q)
-    waiting = S->bslot_ticket[q] > 0 && S->bslot_finished[q];
-  for (size_t q = 0; q < S->pslot_ticket.size() && !waiting; ++q)
-    waiting = S->pslot_ticket[q] > 0 && S->pslot_finished[q];
-  if (!waiting || !S->pool_free.empty()) return false;
-  const double t0 = now_ms();
-  int moved = 0;
+// Clients may collect in any order, so uncollected results can hold every
+// buffer of a pool while finished queries wait for one: then the oldest
+// results of that pool move to host memory (the copies run without the
+// lock; clients wait until a result has moved).  Called and returns with lk
+// held.
+bool move_results_to_host(gbo_server* S, int p, std::unique_lock<std::mutex>& lk) {
+  std::vector<std::pair<long long, Result*>> jobs;
   for (auto& kv : S->results) {
     Result& r = kv.second;
-    if (!r.landed || r.buf < 0) continue;
-    const unsigned char* src = static_cast<const unsigned char*>(S->pool[(size_t)r.buf]);
-    r.heap.assign(src, src + (r.u8 ? 1 : 4) * (size_t)S->n);
-    S->pool_free.push_back(r.buf);
-    r.buf = -1;
-    if (++moved == kRetire) break;
+    if (r.pool != p || r.buf < 0 || r.moving) continue;
+    r.moving = true;
+    jobs.emplace_back(kv.first, &r);  // map nodes stay put while others change
+    if ((int)jobs.size() == kRetire) break;
   }
-  S->spilled += moved;
-  S->phase_ms[3] += now_ms() - t0;
-  return moved > 0;
+  if (jobs.empty()) return false;
+  lk.unlock();
+  cudaError_t e = cudaSuccess;
+  for (auto& j : jobs) {
+    Result& r = *j.second;
+    r.host.resize(r.u8 ? (size_t)S->n : sizeof(int) * (size_t)S->n);
+    if (e == cudaSuccess) e = cudaEventSynchronize(r.ev);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(r.host.data(), S->dpool[p] + (size_t)r.buf * S->dbytes[p], r.host.size(),
+                     cudaMemcpyDeviceToHost);
+  }
+  lk.lock();
+  for (auto& j : jobs) {
+    Result& r = *j.second;
+    S->pool_free[p].push_back(r.buf);
+    r.buf = -1;
+    r.moving = false;
+  }
+  S->cv_done.notify_all();
+  if (e != cudaSuccess) {
+    S->worker_status = fail_cuda(e, "server result move");
+    S->worker_error = gbo_last_error();
+  }
+  return true;
 }
 
 void worker_main(gbo_server* S, int kind) {
@@ -685,15 +698,13 @@ void worker_main(gbo_server* S, int kind) {
     {
       std::unique_lock<std::mutex> lk(S->mu);
       for (;;) {
-        if (collect_landed(S)) S->cv_done.notify_all();
-        if (S->stop) return;
-        spill_landed(S);
-        const bool work = !S->pending[kind].empty() || unfinished() || (occupied() && !S->pool_free.empty());
+        if (S->stop || S->worker_status != GBO_OK) return;
+        const int bp = blocked_pool(S, kind);
+        if (bp >= 0) move_results_to_host(S, bp, lk);
+        const bool work = !S->pending[kind].empty() || unfinished() || (occupied() && blocked_pool(S, kind) < 0);
         if (work) break;
-        if (S->copies_in_flight > 0)
-          S->cv_work.wait_for(lk, std::chrono::microseconds(200));
-        else
-          S->cv_work.wait(lk);
+        // submit, take and destroy notify; the timeout bounds a missed wake-up
+        S->cv_work.wait_for(lk, std::chrono::milliseconds(20));
       }
       // admission into free slots, arrival order
       size_t nx = 0;
@@ -754,7 +765,6 @@ void destroy_server(gbo_server* S) {
   for (int e = 0; e < 2; ++e) {
     if (S->worker[e].joinable()) S->worker[e].join();
     if (S->s[e]) cudaStreamSynchronize(S->s[e]);
-    if (S->cs[e]) cudaStreamSynchronize(S->cs[e]);
   }
   cudaFree(S->F);
   cudaFree(S->V);
@@ -777,16 +787,13 @@ void destroy_server(gbo_server* S) {
   cudaFree(S->d_pverts);
   cudaFree(S->d_poff);
   cudaFree(S->d_pwts);
-  for (int e = 0; e < 2; ++e)
-    for (int b = 0; b < 2; ++b) {
-      cudaFree(S->d_stage[e][b]);
-      if (S->stage_free[e][b]) cudaEventDestroy(S->stage_free[e][b]);
-    }
-  for (void* p : S->pool) cudaFreeHost(p);
-  for (cudaEvent_t e : S->pool_ev) cudaEventDestroy(e);
+  for (int p = 0; p < 2; ++p) {
+    cudaFree(S->dpool[p]);
+    for (cudaEvent_t e : S->pool_ev[p]) cudaEventDestroy(e);
+  }
   for (int e = 0; e < 2; ++e) {
     if (S->s[e]) cudaStreamDestroy(S->s[e]);
-    if (S->cs[e]) cudaStreamDestroy(S->cs[e]);
+    if (S->sync_ev[e]) cudaEventDestroy(S->sync_ev[e]);
   }
   delete S;
 }
@@ -826,7 +833,7 @@ extern "C" int gbo_server_create(const gbo_graph* gc, int bfs_slots, int ppr_slo
   try {
     for (int e = 0; e < 2; ++e) {
       cu(cudaStreamCreateWithFlags(&S->s[e], cudaStreamNonBlocking), "stream");
-      cu(cudaStreamCreateWithFlags(&S->cs[e], cudaStreamNonBlocking), "stream");
+      cu(cudaEventCreateWithFlags(&S->sync_ev[e], cudaEventBlockingSync | cudaEventDisableTiming), "event");
     }
     const size_t n = (size_t)S->n;
     if (S->kb) {
@@ -876,24 +883,20 @@ extern "C" int gbo_server_create(const gbo_graph* gc, int bfs_slots, int ppr_slo
     S->pslot_ticket.assign(ppr_slots ? (size_t)kPprSlots : 0, 0);
     S->pslot_iters.assign((size_t)kPprSlots, 0);
     S->pslot_finished.assign((size_t)kPprSlots, 0);
-    for (int e = 0; e < 2; ++e) {
-      if (e == 0 ? S->kb == 0 : ppr_slots == 0) continue;
-      for (int b = 0; b < 2; ++b) {
-        cu(cudaMalloc(&S->d_stage[e][b], sizeof(int) * n * kRetire + 16), "stage");
-        cu(cudaEventCreateWithFlags(&S->stage_free[e][b], cudaEventDisableTiming), "event");
-        cu(cudaEventRecord(S->stage_free[e][b], S->cs[e]), "event");
+    // device result pools: every slot can hold a finished result plus two
+    // rounds of retirements waiting for their clients
+    const int nbuf[2] = {S->kb > 0 ? S->kb + 2 * kRetire : 0, (ppr_slots ? kPprSlots : 0) + 2 * kRetire};
+    S->dbytes[0] = (n + 255) / 256 * 256;
+    S->dbytes[1] = (sizeof(int) * n + 255) / 256 * 256;
+    for (int p = 0; p < 2; ++p) {
+      if (nbuf[p] == 0) continue;
+      cu(cudaMalloc(&S->dpool[p], S->dbytes[p] * (size_t)nbuf[p]), "result pool");
+      for (int b = 0; b < nbuf[p]; ++b) {
+        cudaEvent_t e = nullptr;
+        cu(cudaEventCreateWithFlags(&e, cudaEventBlockingSync | cudaEventDisableTiming), "event");
+        S->pool_ev[p].push_back(e);
+        S->pool_free[p].push_back(nbuf[p] - 1 - b);
       }
-    }
-    // pinned result buffers: enough for two rounds of retirements
-    const int npool = 2 * kRetire;
-    for (int b = 0; b < npool; ++b) {
-      void* p = nullptr;
-      cudaEvent_t e = nullptr;
-      cu(cudaHostAlloc(&p, sizeof(int) * n + 16, cudaHostAllocDefault), "pinned pool");
-      cu(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
-      S->pool.push_back(p);
-      S->pool_ev.push_back(e);
-      S->pool_free.push_back(b);
     }
     cu(cudaStreamSynchronize(S->s[0]), "sync");
     cu(cudaStreamSynchronize(S->s[1]), "sync");
@@ -947,8 +950,39 @@ extern "C" int gbo_server_submit_ppr(gbo_server* S, const int* verts, const floa
   return submit(S, std::move(q), ticket);
 }
 
-// Hand a landed result to the caller: copy out of the pinned buffer outside
-// the lock, then give the buffer back to the pool.
+// Per client thread: a pinned bounce buffer and a stream, so that result
+// copies from many client threads run at full link speed side by side
+// (copies into pageable memory would serialise on the driver's staging).
+struct ClientCopy {
+  void* pinned = nullptr;
+  size_t bytes = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t done = nullptr;
+  ~ClientCopy() {
+    if (pinned) cudaFreeHost(pinned);
+    if (st) cudaStreamDestroy(st);
+    if (done) cudaEventDestroy(done);
+  }
+  // Copy `bytes` from device memory into the bounce buffer; returns it.
+  const void* fetch(const void* src, size_t n, cudaError_t* err) {
+    if (!st) *err = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (*err == cudaSuccess && !done) *err = cudaEventCreateWithFlags(&done, cudaEventBlockingSync | cudaEventDisableTiming);
+    if (*err == cudaSuccess && bytes < n) {
+      if (pinned) cudaFreeHost(pinned);
+      pinned = nullptr;
+      bytes = 0;
+      *err = cudaHostAlloc(&pinned, n, cudaHostAllocDefault);
+      if (*err == cudaSuccess) bytes = n;
+    }
+    if (*err == cudaSuccess) *err = cudaMemcpyAsync(pinned, src, n, cudaMemcpyDeviceToHost, st);
+    if (*err == cudaSuccess) *err = wait_stream(st, done);
+    return pinned;
+  }
+};
+
+// Hand a finished result to the caller: wait for its retirement kernel,
+// copy it from the device buffer (widening byte levels to int32) outside the
+// lock, then give the buffer back to the pool.
 static int take_result(gbo_server* S, std::unique_lock<std::mutex>& lk, int64_t ticket, void* h_out,
                        double* latency_ms, int* iterations) {
   auto it = S->results.find(ticket);
@@ -956,19 +990,38 @@ static int take_result(gbo_server* S, std::unique_lock<std::mutex>& lk, int64_t 
   S->results.erase(it);
   S->submit_time.erase(ticket);
   lk.unlock();
-  const void* src = r.buf >= 0 ? S->pool[(size_t)r.buf] : (const void*)r.heap.data();
-  if (h_out && r.u8) {
-    const unsigned char* b8 = static_cast<const unsigned char*>(src);
-    int* o = static_cast<int*>(h_out);
-    for (int i = 0; i < S->n; ++i) o[i] = b8[i] == 255 ? -1 : (int)b8[i];
-  } else if (h_out) {
-    memcpy(h_out, src, sizeof(int) * (size_t)S->n);
+  const double t0 = now_ms();
+  cudaError_t e = cudaSuccess;
+  if (r.buf < 0) {  // already in host memory
+    if (h_out && r.u8) {
+      int* o = static_cast<int*>(h_out);
+      for (int i = 0; i < S->n; ++i) o[i] = r.host[(size_t)i] == 255 ? -1 : (int)r.host[(size_t)i];
+    } else if (h_out) {
+      memcpy(h_out, r.host.data(), sizeof(int) * (size_t)S->n);
+    }
+  } else {
+    const char* src = S->dpool[r.pool] + (size_t)r.buf * S->dbytes[r.pool];
+    e = cudaEventSynchronize(r.ev);
+    if (e == cudaSuccess && h_out) {
+      thread_local ClientCopy cc;
+      const size_t nb = (r.u8 ? 1 : sizeof(int)) * (size_t)S->n;
+      const void* h = cc.fetch(src, nb, &e);
+      if (e == cudaSuccess && r.u8) {
+        const unsigned char* b8 = static_cast<const unsigned char*>(h);
+        int* o = static_cast<int*>(h_out);
+        for (int i = 0; i < S->n; ++i) o[i] = b8[i] == 255 ? -1 : (int)b8[i];
+      } else if (e == cudaSuccess) {
+        memcpy(h_out, h, nb);
+      }
+    }
   }
-  if (latency_ms) *latency_ms = r.t_done - r.t_submit;
+  if (latency_ms) *latency_ms = now_ms() - r.t_submit;
   if (iterations) *iterations = r.iters;
   lk.lock();
-  if (r.buf >= 0) S->pool_free.push_back(r.buf);
+  if (r.buf >= 0) S->pool_free[r.pool].push_back(r.buf);
+  S->phase_ms[3] += now_ms() - t0;
   S->cv_work.notify_all();
+  if (e != cudaSuccess) return fail_cuda(e, "server result copy");
   return GBO_OK;
 }
 
@@ -978,9 +1031,12 @@ extern "C" int gbo_server_poll(gbo_server* S, int64_t ticket, void* h_out, doubl
   if (!S) return fail(GBO_ERR_INVALID, "NULL server");
   std::unique_lock<std::mutex> lk(S->mu);
   if (S->worker_status != GBO_OK) return fail(S->worker_status, S->worker_error);
-  collect_landed(S);
   auto it = S->results.find(ticket);
-  if (it == S->results.end() || !it->second.landed) return GBO_ERR_NOTREADY;
+  if (it == S->results.end() || it->second.moving) return GBO_ERR_NOTREADY;
+  if (it->second.buf >= 0 && cudaEventQuery(it->second.ev) == cudaErrorNotReady) {
+    (void)cudaGetLastError();
+    return GBO_ERR_NOTREADY;
+  }
   return take_result(S, lk, ticket, h_out, latency_ms, iterations);
 }
 
@@ -991,9 +1047,8 @@ extern "C" int gbo_server_wait(gbo_server* S, int64_t ticket, void* h_out, doubl
   std::unique_lock<std::mutex> lk(S->mu);
   const bool ok = S->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] {
     if (S->worker_status != GBO_OK) return true;
-    collect_landed(S);
     auto it = S->results.find(ticket);
-    return it != S->results.end() && it->second.landed;
+    return it != S->results.end() && !it->second.moving;
   });
   if (S->worker_status != GBO_OK) return fail(S->worker_status, S->worker_error);
   if (!ok) return fail(GBO_ERR_TIMEOUT, "query not finished within the timeout");
@@ -1016,8 +1071,7 @@ extern "C" int gbo_server_get_stats(gbo_server* S, gbo_server_stats* st) {
   st->bfs_round_ms = S->phase_ms[0];
   st->ppr_round_ms = S->phase_ms[1];
   st->retire_ms = S->phase_ms[2];
-  st->spill_ms = S->phase_ms[3];
-  st->spilled = S->spilled;
+  st->copy_ms = S->phase_ms[3];
   return GBO_OK;
 }
 

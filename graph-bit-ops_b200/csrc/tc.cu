@@ -30,17 +30,6 @@ __device__ __forceinline__ int lower_bound_dev(const int* __restrict__ a, int lo
   return lo;
 }
 
-// Block row of tile m: largest I with rowptr[I] <= m.
-__device__ __forceinline__ int row_of_tile(const int* __restrict__ rowptr, int nbr, int m) {
-  int lo = 0, hi = nbr;  // rowptr[0] = 0 <= m < rowptr[nbr]
-  while (hi - lo > 1) {
-    int mid = (lo + hi) >> 1;
-    if (rowptr[mid] <= m) lo = mid;
-    else hi = mid;
-  }
-  return lo;
-}
-
 template <int B>
 __global__ void __launch_bounds__(kTPB) k_tc(GView v, long long nblk,
                                              unsigned long long* __restrict__ count) {
@@ -51,8 +40,9 @@ __global__ void __launch_bounds__(kTPB) k_tc(GView v, long long nblk,
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
   const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
   unsigned long long acc = 0;
-  for (long long m = warp; m < nblk; m += nwarps) {
-    const int I = row_of_tile(v.rowptr, v.nbr, (int)m);
+  // mask tiles in block-row order through the work items (no search for I)
+  for (long long item = warp; item < v.nitems; item += nwarps)
+  for (int m = v.items[item].t0, mend = v.items[item].t1, I = v.items[item].row; m < mend; ++m) {
     const int K = v.colind[m];
     // mask rows of tile (I,K)
     WT M0 = 0, M1 = 0;
@@ -123,7 +113,7 @@ int tc_launch(const gbo_graph* g, unsigned long long* d_count, cudaStream_t s) {
   GBO_CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s));
   if (g->nblk == 0) return GBO_OK;
   GView v = view_of(g);
-  long long warps = g->nblk;
+  long long warps = g->nitems;
   long long cap = (long long)num_sms() * 64;  // 64 resident warps per SM
   if (warps > cap * 8) warps = cap * 8;
   const unsigned grid = blocks_for_warps(warps, kTPB / 32);

@@ -34,6 +34,7 @@ FLAG_TRANSPOSE = 2
 FLAG_LAYOUT_COL = 4
 FLAG_LOWER = 8
 FLAG_SYMMETRIC = 16
+FLAG_DEGREE_ORDER = 32
 OUT_I32 = 0
 OUT_F32 = 1
 MTX_READMTX = 0
@@ -71,7 +72,7 @@ class ServerStats(C.Structure):
                 ("ppr_completed", C.c_longlong), ("kernel_launches", C.c_longlong),
                 ("pending", C.c_longlong), ("in_flight", C.c_longlong),
                 ("bfs_round_ms", C.c_double), ("ppr_round_ms", C.c_double),
-                ("retire_ms", C.c_double), ("spill_ms", C.c_double), ("spilled", C.c_longlong)]
+                ("retire_ms", C.c_double), ("copy_ms", C.c_double)]
 
 
 class CsrStruct(C.Structure):
@@ -117,6 +118,7 @@ _SIGS = {
     "gbo_graph_b2sr": (_I, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
     "gbo_graph_outdeg": (_I, [_P, C.POINTER(_P)]),
     "gbo_graph_set_bfs_direction": (_I, [_P, _I, _I]),
+    "gbo_graph_permutation": (_I, [_P, C.POINTER(_P)]),
     "gbo_tune_tile_width": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _P, C.POINTER(_I), _P]),
     "gbo_bmv_count": (_I, [_P, _P, _P, _I, _I, _P]),
     "gbo_bmv_count_noalloc": (_I, [_I, _I, _I, _I, _P, _P, _P, _P, _P, _I, _I, _P]),
@@ -466,6 +468,12 @@ class Graph:
         check(lib().gbo_graph_outdeg(self.h, C.byref(p)), "graph_outdeg")
         return device_to_numpy(p.value, np.int32, self.info().ncols)
 
+    def permutation(self):
+        """new_of_old labels of a graph packed with FLAG_DEGREE_ORDER, else None."""
+        p = C.c_void_p()
+        check(lib().gbo_graph_permutation(self.h, C.byref(p)), "graph_permutation")
+        return None if not p.value else device_to_numpy(p.value, np.int32, self.info().nrows)
+
     def set_bfs_direction(self, symmetric: bool, push_threshold: int = -1) -> None:
         """Allow top-down BFS steps on a symmetric graph below push_threshold
         frontier vertices (-1: nrows / 64; 0: pull only)."""
@@ -662,8 +670,11 @@ class Server:
               "server_submit_ppr")
         return t.value
 
-    def wait(self, ticket: int, kind: str = "bfs", timeout=120.0):
-        out = np.empty(self.n, np.int32 if kind == "bfs" else np.float32)
+    def wait(self, ticket: int, kind: str = "bfs", timeout=120.0, out: np.ndarray | None = None):
+        """Block until the query's result is in host memory; `out` (n int32
+        for BFS, n float32 for PPR) is reused when given."""
+        if out is None:
+            out = np.empty(self.n, np.int32 if kind == "bfs" else np.float32)
         lat, it = C.c_double(0), C.c_int(0)
         check(lib().gbo_server_wait(self.h, ticket, _ptr(out), C.byref(lat), C.byref(it), timeout),
               "server_wait")

@@ -131,9 +131,16 @@ enum gbo_graph_flags {
   GBO_FLAG_TRANSPOSE = 2,   /* pack the transpose of the given CSR (CSC) */
   GBO_FLAG_LAYOUT_COL = 4,  /* COL tile layout instead of ROW */
   GBO_FLAG_LOWER = 8,       /* keep only row >= col entries (tril_csr) */
-  GBO_FLAG_SYMMETRIC = 16   /* caller asserts the packed matrix is symmetric:
+  GBO_FLAG_SYMMETRIC = 16,  /* caller asserts the packed matrix is symmetric:
                                BFS may then take top-down (push) steps while
                                the frontier is small (direction-optimising) */
+  GBO_FLAG_DEGREE_ORDER = 32 /* relabel vertices by descending degree before
+                               packing (P' = Q P Q^T; gbo_graph_permutation
+                               gives the labels).  For permutation-invariant
+                               results such as the triangle count: with
+                               GBO_FLAG_LOWER every row then holds only
+                               higher-degree neighbours, so hub rows stay
+                               short.  No reference counterpart. */
 };
 
 /* Pack a CSR matrix M into a device-resident B2SR graph owned by the handle.
@@ -170,12 +177,15 @@ GBO_API int gbo_graph_b2sr(const gbo_graph* g, const int** d_bsrRowPtr,
                    const int** d_bsrColInd, const void** d_bsrVal);
 /* Device array of out-degrees (ncols ints) or NULL. */
 GBO_API int gbo_graph_outdeg(const gbo_graph* g, const int** d_outdeg);
+/* Device array new_of_old[v] (nrows ints) of a graph packed with
+ * GBO_FLAG_DEGREE_ORDER, else NULL. */
+GBO_API int gbo_graph_permutation(const gbo_graph* g, const int** d_new_of_old);
 /* Direction-optimising BFS control (no counterpart in the reference, whose
  * BFS only pulls).  symmetric = 1 asserts P == P^T (what GBO_FLAG_SYMMETRIC
  * does for gbo_graph_from_csr; needed for wrapped graphs), 0 restores
  * pull-only BFS.  A level whose frontier holds fewer than push_threshold
  * vertices is expanded top-down; -1 selects the default nrows / 64.
- * Rejected (GBO_ERR_UNSUPPORTED) for a non-square or COL-layout graph. */
+ * Rejected (GBO_ERR_UNSUPPORTED) for a non-square graph. */
 GBO_API int gbo_graph_set_bfs_direction(gbo_graph* g, int symmetric, int push_threshold);
 
 /* Tile-width tuner (no counterpart in the reference, whose drivers take b
@@ -265,7 +275,12 @@ GBO_API int gbo_bmv_float_transposed(const gbo_graph* g, const float* d_x, float
 /* Level-synchronous pull BFS on P from src: level[i] = hops, -1 unreachable.
  * Rewrites algorithm/bfs.cu:508-564 with all state on the device and
  * termination decided on the device (no per-level host copy).
- * h_depth (nullable) receives the number of levels (max level + 1). */
+ * h_depth (nullable) receives the number of levels (max level + 1).
+ * Takes ROW- and COL-layout graphs (the other algorithms need ROW): with
+ * column words a pull step reads, per tile, only the words of the
+ * frontier's columns, which pays off where frontier segments are sparse in
+ * dense tiles; on sparse tiles (R-MAT) the 32-byte DRAM sectors make both
+ * layouts read about the same bytes and ROW is faster. */
 GBO_API int gbo_bfs(const gbo_graph* g, int src, int32_t* d_level, int* h_depth,
             gbo_stream_t stream);
 /* Unit-weight SSSP with the distances of the reference's min-plus loop
@@ -321,20 +336,20 @@ GBO_API int gbo_bfs_multi(const gbo_graph* g, const int* h_seeds, int nseeds,
  * int32[n] levels (hops, -1 unreachable), PPR float[n].  A query's result
  * is the same whatever else is in flight.  Needs a square ROW-layout graph
  * with 32x32 tiles (and out-degrees for PPR).  A finished result waits in
- * host memory (a pinned buffer, or heap memory once the pinned pool is all
- * held by uncollected results) until wait/poll takes it, in any order. */
+ * a device buffer until wait/poll copies it to the caller, in any order;
+ * while every buffer holds an uncollected result, finished queries keep
+ * their slots until a client takes one. */
 typedef struct gbo_server gbo_server;
 typedef struct gbo_server_stats {
   long long rounds;          /* worker rounds (one BFS level or one PPR iteration) */
   long long bfs_completed, ppr_completed;
   long long kernel_launches;
   long long pending, in_flight;
-  /* wall time the workers spent per phase (ms, summed over rounds):
-   * BFS levels and PPR iterations (kernels and the completion read-back),
-   * retirement (extraction kernels and copy issue), and moving uncollected
-   * results out of the pinned pool */
-  double bfs_round_ms, ppr_round_ms, retire_ms, spill_ms;
-  long long spilled;         /* results moved to heap memory */
+  /* wall time per phase (ms, summed): the workers' BFS levels and PPR
+   * iterations (kernels and the completion read-back) and retirements
+   * (extraction into device result buffers), and the clients' result
+   * copies (device to host, inside wait/poll) */
+  double bfs_round_ms, ppr_round_ms, retire_ms, copy_ms;
 } gbo_server_stats;
 GBO_API int gbo_server_create(const gbo_graph* g, int bfs_slots, int ppr_slots,
                       float alpha, float tol, int ppr_max_iter,

@@ -177,3 +177,47 @@ def test_bfs_push_every_level(gbo, orc, gpu, graphs, b):
         g.set_bfs_direction(False)
         lv, _ = g.bfs(1)
         assert np.array_equal(lv, orc.bfs_csr(csr.rowptr, csr.colind, csr.nrows, 1)[0])
+
+
+@pytest.mark.parametrize("b", WIDTHS)
+def test_bfs_col_layout(gbo, orc, gpu, graphs, b):
+    """BFS and SSSP on column-word tiles: pull-only, direction-optimising,
+    every level pushed, and many seeds, all equal to the oracle."""
+    for name, csr in graphs.items():
+        sym = name != "ragged1001"
+        g = gbo.Graph.from_csr(csr, b, gbo.FLAG_LAYOUT_COL | (gbo.FLAG_SYMMETRIC if sym else 0))
+        for thr in ((-1, csr.nrows + 1, 0) if sym else (0,)):
+            g.set_bfs_direction(sym and thr != 0, thr)
+            for src in (0, csr.nrows // 2, csr.nrows - 1):
+                want, d = orc.bfs_csr(csr.rowptr, csr.colind, csr.nrows, src)
+                lv, depth = g.bfs(src)
+                assert np.array_equal(lv, want) and depth == d, (name, b, thr, src)
+        dist, _ = g.sssp(1 % csr.nrows)
+        want, _ = orc.bfs_csr(csr.rowptr, csr.colind, csr.nrows, 1 % csr.nrows)
+        assert np.array_equal(dist, np.where(want < 0, INF, want).astype(np.uint32)), (name, b)
+        seeds = np.arange(0, csr.nrows, max(1, csr.nrows // 5), dtype=np.int32)
+        lv, _ = g.bfs_multi(seeds)
+        ref = np.full(csr.nrows, -1, np.int64)
+        for s in seeds:
+            x, _ = orc.bfs_csr(csr.rowptr, csr.colind, csr.nrows, int(s))
+            ref = np.where((ref < 0) | ((x >= 0) & (x < ref)), x, ref)
+        assert np.array_equal(lv, ref), (name, b)
+
+
+@pytest.mark.parametrize("b", [8, 16, 32, 64])
+def test_degree_order(gbo, orc, gpu, graphs, b):
+    """Relabelling by descending degree: the triangle count is unchanged and
+    BFS levels are the original ones under the returned labels."""
+    for name in ("rmat12", "rmat14", "er1000", "mesh33", "star20000"):
+        csr = graphs[name]
+        g = gbo.Graph.from_csr(csr, b, gbo.FLAG_LOWER | gbo.FLAG_DEGREE_ORDER)
+        assert g.tc() == orc.tc_csr(csr.rowptr, csr.colind, csr.nrows), (name, b)
+        perm = g.permutation()
+        assert np.array_equal(np.sort(perm), np.arange(csr.nrows))
+        deg = np.diff(csr.rowptr)
+        assert np.all(np.diff(deg[np.argsort(perm)]) <= 0)  # labels by descending degree
+        h = gbo.Graph.from_csr(csr, b, gbo.FLAG_DEGREE_ORDER | gbo.FLAG_SYMMETRIC)
+        lv, _ = h.bfs(int(perm[3]))
+        want, _ = orc.bfs_csr(csr.rowptr, csr.colind, csr.nrows, 3)
+        assert np.array_equal(lv[perm], want), (name, b)
+    assert gbo.Graph.from_csr(graphs["mesh33"], 8).permutation() is None
