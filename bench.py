@@ -336,7 +336,8 @@ def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed):
     srv.close()
     out = {"offered_qps": rate_qps, "queries": nq, "achieved_qps": nq / wall, "wall_s": wall,
            "rounds": st["rounds"], "kernel_launches": st["kernel_launches"],
-           "phase_ms": {k: round(st[k], 1) for k in ("bfs_round_ms", "ppr_round_ms", "retire_ms", "copy_ms")}}
+           "phase_ms": {k: round(st[k], 1) for k in ("bfs_round_ms", "ppr_round_ms", "retire_ms", "copy_ms",
+                                                     "copy_wait_ms", "copy_d2h_ms", "copy_widen_ms")}}
     for k, v in lat.items():
         if v:
             out[f"{k}_p50_ms"] = float(np.percentile(v, 50))

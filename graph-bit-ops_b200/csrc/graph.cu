@@ -107,6 +107,7 @@ void destroy(gbo_graph* g) {
   }
   if (g->owns_outdeg) cudaFree(g->outdeg);
   cudaFree(g->perm);
+  cudaFree(g->tile_row);
   cudaFree(g->invdeg);
   cudaFree(g->items);
   cudaFree(g->splits);

@@ -29,6 +29,7 @@ struct gbo_graph {
   bool symmetric = false;  // caller asserts P == P^T (enables push BFS steps)
   int bfs_push_thr = -1;   // push below this frontier size (-1: nrows / 64)
   int* perm = nullptr;     // GBO_FLAG_DEGREE_ORDER: new label of every input vertex
+  int* tile_row = nullptr; // block row of every tile (triangle counting)
   bool owns_outdeg = true;
   // balanced schedule
   int chunk = 0;

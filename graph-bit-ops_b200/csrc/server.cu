@@ -272,31 +272,46 @@ constexpr int kRetRows = 32;  // rows per block of the transposing kernels
 
 struct RetireList {
   int count;
-  int slot[kRetire];
+  int slot[kRetire];    // ascending, so the slots of one level group are adjacent
   int start[kRetire];
   uint32_t clr[32];     // visited bits to clear, per source word
   void* out[kRetire];   // destination buffer of each retired slot
+  // BFS: the level groups (8 slots per 32-byte sector) holding retired slots:
+  // group id, index of its first retired slot, which of its 8 slots retire
+  int ngroups;
+  int group[kRetire];
+  short fbeg[kRetire];
+  unsigned char mask8[kRetire];
 };
 
 // BFS: out[f][i] = level of (i, slot f) relative to its start level, -1 if
-// unreachable; the slot's levels become -1 and its visited bits 0.  When
-// every retired query is shallower than 255 levels (u8), a result is one
-// byte per vertex (255 = unreachable), a quarter of the bytes the client
-// copies; the client widens them to int32.
-__global__ void __launch_bounds__(256) k_bfs_retire(int* levels, int g, uint32_t* V, int n, int kw,
-                                                    RetireList rl, int u8) {
+// unreachable, and the slot's visited bits become 0.  Levels are absolute
+// (the server's level counter), so a slot's column never needs clearing: a
+// value older than the query's start level was left by an earlier query of
+// the slot and reads as unreachable.  Each thread loads the 32-byte sector of
+// one (row, level group) and keeps the group's retiring slots; results go
+// out through shared memory row-contiguous.  When every retired query is
+// shallower than 255 levels (u8), a result is one byte per vertex (255 =
+// unreachable), a quarter of the bytes the client copies.
+__global__ void __launch_bounds__(256) k_bfs_retire(const int* __restrict__ levels, uint32_t* V, int n,
+                                                    int kw, RetireList rl, int u8) {
   __shared__ int sm[kRetire][kRetRows + 1];
   const long long i0 = (long long)blockIdx.x * kRetRows;
-  const int R = rl.count;
-  for (int q = threadIdx.x; q < kRetRows * R; q += blockDim.x) {
-    const int ii = q / R, f = q % R;
+  for (int q = threadIdx.x; q < kRetRows * rl.ngroups; q += blockDim.x) {
+    const int gi = q / kRetRows, ii = q % kRetRows;
     const long long i = i0 + ii;
     if (i >= n) continue;
-    const int s = rl.slot[f];
-    const size_t idx = ((size_t)(s / g) * n + i) * g + s % g;
-    const int lv = levels[idx];
-    sm[f][ii] = lv >= 0 ? lv - rl.start[f] : -1;
-    levels[idx] = -1;
+    const int4* p = reinterpret_cast<const int4*>(levels + ((size_t)rl.group[gi] * n + i) * 8);
+    const int4 a = p[0], b = p[1];
+    const int lv[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    const unsigned m = rl.mask8[gi];
+    int f = rl.fbeg[gi];
+#pragma unroll
+    for (int w = 0; w < 8; ++w)
+      if ((m >> w) & 1u) {
+        sm[f][ii] = lv[w] >= rl.start[f] ? lv[w] - rl.start[f] : -1;
+        ++f;
+      }
   }
   for (int q = threadIdx.x; q < kRetRows * kw; q += blockDim.x) {
     const int ii = q / kw, w = q % kw;
@@ -304,7 +319,7 @@ __global__ void __launch_bounds__(256) k_bfs_retire(int* levels, int g, uint32_t
     if (i < n && rl.clr[w]) V[(size_t)i * kw + w] &= ~rl.clr[w];
   }
   __syncthreads();
-  for (int q = threadIdx.x; q < kRetRows * R; q += blockDim.x) {
+  for (int q = threadIdx.x; q < kRetRows * rl.count; q += blockDim.x) {
     const int f = q / kRetRows, ii = q % kRetRows;
     const long long i = i0 + ii;
     if (i >= n) continue;
@@ -429,6 +444,7 @@ struct gbo_server {
   std::atomic<long long> rounds{0}, launches{0};
   long long bfs_done = 0, ppr_done = 0;
   double phase_ms[4] = {0, 0, 0, 0};  // BFS round, PPR round, retire, client copies (under mu)
+  double copy_parts[3] = {0, 0, 0};   // client copies: event wait, device-to-host, widening
 };
 
 namespace gbo {
@@ -589,9 +605,21 @@ int retire(gbo_server* S, int kind) {
   const double t_now = now_ms();
   for (int p = 0; p < 2; ++p) {
     if (rl[p].count == 0) continue;
+    RetireList& r = rl[p];
+    r.ngroups = 0;
+    for (int f = 0; f < r.count; ++f) {  // slots ascend: a group's slots are adjacent
+      const int gid = r.slot[f] / 8;
+      if (r.ngroups == 0 || r.group[r.ngroups - 1] != gid) {
+        r.group[r.ngroups] = gid;
+        r.fbeg[r.ngroups] = (short)f;
+        r.mask8[r.ngroups] = 0;
+        r.ngroups++;
+      }
+      r.mask8[r.ngroups - 1] |= (unsigned char)(1u << (r.slot[f] % 8));
+    }
     // retired columns were already out of the active set: rows marked
     // finished stay finished
-    if (kind == 0) k_bfs_retire<<<grid, 256, 0, st>>>(S->levels, 8, S->V, S->n, S->kw, rl[p], p == 0);
+    if (kind == 0) k_bfs_retire<<<grid, 256, 0, st>>>(S->levels, S->V, S->n, S->kw, rl[p], p == 0);
     else k_ppr_retire<<<grid, 256, 0, st>>>(S->X + (size_t)S->parity * S->n * kPprSlots, S->n, rl[p]);
     S->launches += 1;
     GBO_CUDA_TRY(cudaGetLastError());
@@ -950,6 +978,12 @@ extern "C" int gbo_server_submit_ppr(gbo_server* S, const int* verts, const floa
   return submit(S, std::move(q), ticket);
 }
 
+// Byte levels to int32, 255 (unreachable) to -1; branch-free so that the
+// compiler vectorises it.
+static void widen_levels(const unsigned char* __restrict__ b8, int* __restrict__ o, int n) {
+  for (int i = 0; i < n; ++i) o[i] = (int)b8[i] | -(int)(b8[i] == 255);
+}
+
 // Per client thread: a pinned bounce buffer and a stream, so that result
 // copies from many client threads run at full link speed side by side
 // (copies into pageable memory would serialise on the driver's staging).
@@ -991,35 +1025,44 @@ static int take_result(gbo_server* S, std::unique_lock<std::mutex>& lk, int64_t 
   S->submit_time.erase(ticket);
   lk.unlock();
   const double t0 = now_ms();
+  double t1 = t0, t2 = t0;
   cudaError_t e = cudaSuccess;
   if (r.buf < 0) {  // already in host memory
     if (h_out && r.u8) {
       int* o = static_cast<int*>(h_out);
-      for (int i = 0; i < S->n; ++i) o[i] = r.host[(size_t)i] == 255 ? -1 : (int)r.host[(size_t)i];
+      widen_levels(r.host.data(), o, S->n);
     } else if (h_out) {
       memcpy(h_out, r.host.data(), sizeof(int) * (size_t)S->n);
     }
   } else {
     const char* src = S->dpool[r.pool] + (size_t)r.buf * S->dbytes[r.pool];
     e = cudaEventSynchronize(r.ev);
+    t1 = now_ms();
     if (e == cudaSuccess && h_out) {
       thread_local ClientCopy cc;
       const size_t nb = (r.u8 ? 1 : sizeof(int)) * (size_t)S->n;
       const void* h = cc.fetch(src, nb, &e);
+      t2 = now_ms();
       if (e == cudaSuccess && r.u8) {
         const unsigned char* b8 = static_cast<const unsigned char*>(h);
         int* o = static_cast<int*>(h_out);
-        for (int i = 0; i < S->n; ++i) o[i] = b8[i] == 255 ? -1 : (int)b8[i];
+        widen_levels(b8, o, S->n);
       } else if (e == cudaSuccess) {
         memcpy(h_out, h, nb);
       }
     }
   }
-  if (latency_ms) *latency_ms = now_ms() - r.t_submit;
+  const double t3 = now_ms();
+  if (latency_ms) *latency_ms = t3 - r.t_submit;
   if (iterations) *iterations = r.iters;
   lk.lock();
   if (r.buf >= 0) S->pool_free[r.pool].push_back(r.buf);
-  S->phase_ms[3] += now_ms() - t0;
+  S->phase_ms[3] += t3 - t0;
+  if (r.buf >= 0) {
+    S->copy_parts[0] += t1 - t0;
+    S->copy_parts[1] += t2 - t1;
+    S->copy_parts[2] += t3 - t2;
+  }
   S->cv_work.notify_all();
   if (e != cudaSuccess) return fail_cuda(e, "server result copy");
   return GBO_OK;
@@ -1072,6 +1115,9 @@ extern "C" int gbo_server_get_stats(gbo_server* S, gbo_server_stats* st) {
   st->ppr_round_ms = S->phase_ms[1];
   st->retire_ms = S->phase_ms[2];
   st->copy_ms = S->phase_ms[3];
+  st->copy_wait_ms = S->copy_parts[0];
+  st->copy_d2h_ms = S->copy_parts[1];
+  st->copy_widen_ms = S->copy_parts[2];
   return GBO_OK;
 }
 

@@ -30,8 +30,16 @@ __device__ __forceinline__ int lower_bound_dev(const int* __restrict__ a, int lo
   return lo;
 }
 
+// Block row of every tile (computed once per graph, from the work items).
+__global__ void k_tile_row(GView v, int* __restrict__ tile_row) {
+  const long long item = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (item >= v.nitems) return;
+  const gbo_item it = v.items[item];
+  for (int t = it.t0 + (int)(threadIdx.x & 31); t < it.t1; t += 32) tile_row[t] = it.row;
+}
+
 template <int B>
-__global__ void __launch_bounds__(kTPB) k_tc(GView v, long long nblk,
+__global__ void __launch_bounds__(kTPB) k_tc(GView v, long long nblk, const int* __restrict__ tile_row,
                                              unsigned long long* __restrict__ count) {
   using WT = typename Word<B>::T;
   constexpr int RPL = B > 32 ? 2 : 1;
@@ -40,9 +48,9 @@ __global__ void __launch_bounds__(kTPB) k_tc(GView v, long long nblk,
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
   const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
   unsigned long long acc = 0;
-  // mask tiles in block-row order through the work items (no search for I)
-  for (long long item = warp; item < v.nitems; item += nwarps)
-  for (int m = v.items[item].t0, mend = v.items[item].t1, I = v.items[item].row; m < mend; ++m) {
+  // mask tiles strided over the warps (hub rows spread out)
+  for (long long m = warp; m < nblk; m += nwarps) {
+    const int I = tile_row[m];
     const int K = v.colind[m];
     // mask rows of tile (I,K)
     WT M0 = 0, M1 = 0;
@@ -78,14 +86,16 @@ __global__ void __launch_bounds__(kTPB) k_tc(GView v, long long nblk,
         const int qh = __shfl_sync(0xffffffffu, hit, src);
         const int ia = probe_a ? ph : qh;  // tile (I,J)
         const int ib = probe_a ? qh : ph;  // tile (K,J)
+        // only the rows that matter are loaded: A rows with mask bits, B
+        // rows of the mask's columns (sparse tiles touch one or two sectors)
         WT A0 = 0, A1 = 0, Bw0 = 0, Bw1 = 0;
         if (lane < (unsigned)(B < 32 ? B : 32)) {
-          A0 = val[(size_t)ia * B + lane];
-          Bw0 = val[(size_t)ib * B + lane];
+          if (M0) A0 = val[(size_t)ia * B + lane];
+          if ((U >> (B - 1 - lane)) & 1ull) Bw0 = val[(size_t)ib * B + lane];
         }
         if (RPL == 2) {
-          A1 = val[(size_t)ia * B + 32 + lane];
-          Bw1 = val[(size_t)ib * B + 32 + lane];
+          if (M1) A1 = val[(size_t)ia * B + 32 + lane];
+          if ((U >> (31 - lane)) & 1ull) Bw1 = val[(size_t)ib * B + 32 + lane];
         }
         unsigned long long u = U << (64 - B);  // column c at bit 63-c
         while (u) {
@@ -109,20 +119,25 @@ __global__ void __launch_bounds__(kTPB) k_tc(GView v, long long nblk,
 
 }  // namespace
 
-int tc_launch(const gbo_graph* g, unsigned long long* d_count, cudaStream_t s) {
+int tc_launch(gbo_graph* g, unsigned long long* d_count, cudaStream_t s) {
   GBO_CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s));
   if (g->nblk == 0) return GBO_OK;
   GView v = view_of(g);
-  long long warps = g->nitems;
+  if (!g->tile_row) {  // block row of every tile, kept with the graph
+    GBO_CUDA_TRY(cudaMalloc(&g->tile_row, sizeof(int) * (size_t)g->nblk));
+    g->device_bytes += 4LL * g->nblk;
+    k_tile_row<<<blocks_for_warps(g->nitems, kTPB / 32), kTPB, 0, s>>>(v, g->tile_row);
+  }
+  long long warps = g->nblk;
   long long cap = (long long)num_sms() * 64;  // 64 resident warps per SM
   if (warps > cap * 8) warps = cap * 8;
   const unsigned grid = blocks_for_warps(warps, kTPB / 32);
   switch (g->b) {
-    case 4: k_tc<4><<<grid, kTPB, 0, s>>>(v, g->nblk, d_count); break;
-    case 8: k_tc<8><<<grid, kTPB, 0, s>>>(v, g->nblk, d_count); break;
-    case 16: k_tc<16><<<grid, kTPB, 0, s>>>(v, g->nblk, d_count); break;
-    case 32: k_tc<32><<<grid, kTPB, 0, s>>>(v, g->nblk, d_count); break;
-    default: k_tc<64><<<grid, kTPB, 0, s>>>(v, g->nblk, d_count); break;
+    case 4: k_tc<4><<<grid, kTPB, 0, s>>>(v, g->nblk, g->tile_row, d_count); break;
+    case 8: k_tc<8><<<grid, kTPB, 0, s>>>(v, g->nblk, g->tile_row, d_count); break;
+    case 16: k_tc<16><<<grid, kTPB, 0, s>>>(v, g->nblk, g->tile_row, d_count); break;
+    case 32: k_tc<32><<<grid, kTPB, 0, s>>>(v, g->nblk, g->tile_row, d_count); break;
+    default: k_tc<64><<<grid, kTPB, 0, s>>>(v, g->nblk, g->tile_row, d_count); break;
   }
   GBO_CUDA_TRY(cudaGetLastError());
   return GBO_OK;
@@ -144,7 +159,7 @@ extern "C" int gbo_tc_device(const gbo_graph* lower, unsigned long long* d_count
   clear_error();
   GBO_TRY(check_tc_graph(lower));
   if (!d_count) return fail(GBO_ERR_INVALID, "count is NULL");
-  return tc_launch(lower, d_count, as_stream(stream));
+  return tc_launch(const_cast<gbo_graph*>(lower), d_count, as_stream(stream));
 }
 
 extern "C" int gbo_tc(const gbo_graph* lower, uint64_t* h_count, gbo_stream_t stream) {
@@ -154,7 +169,7 @@ extern "C" int gbo_tc(const gbo_graph* lower, uint64_t* h_count, gbo_stream_t st
   cudaStream_t s = as_stream(stream);
   unsigned long long* d = nullptr;
   GBO_CUDA_TRY(cudaMallocAsync(&d, sizeof(unsigned long long), s));
-  int st = tc_launch(lower, d, s);
+  int st = tc_launch(const_cast<gbo_graph*>(lower), d, s);
   unsigned long long h = 0;
   if (st == GBO_OK) {
     cudaError_t e = cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, s);

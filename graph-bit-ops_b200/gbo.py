@@ -72,7 +72,8 @@ class ServerStats(C.Structure):
                 ("ppr_completed", C.c_longlong), ("kernel_launches", C.c_longlong),
                 ("pending", C.c_longlong), ("in_flight", C.c_longlong),
                 ("bfs_round_ms", C.c_double), ("ppr_round_ms", C.c_double),
-                ("retire_ms", C.c_double), ("copy_ms", C.c_double)]
+                ("retire_ms", C.c_double), ("copy_ms", C.c_double), ("copy_wait_ms", C.c_double),
+                ("copy_d2h_ms", C.c_double), ("copy_widen_ms", C.c_double)]
 
 
 class CsrStruct(C.Structure):

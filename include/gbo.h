@@ -350,6 +350,9 @@ typedef struct gbo_server_stats {
    * (extraction into device result buffers), and the clients' result
    * copies (device to host, inside wait/poll) */
   double bfs_round_ms, ppr_round_ms, retire_ms, copy_ms;
+  /* copy_ms split: waiting for the retirement kernel, the device-to-host
+   * copy, and widening byte levels into the caller's int32 buffer */
+  double copy_wait_ms, copy_d2h_ms, copy_widen_ms;
 } gbo_server_stats;
 GBO_API int gbo_server_create(const gbo_graph* g, int bfs_slots, int ppr_slots,
                       float alpha, float tol, int ppr_max_iter,
