@@ -38,12 +38,21 @@ __global__ void k_tile_row(GView v, int* __restrict__ tile_row) {
   for (int t = it.t0 + (int)(threadIdx.x & 31); t < it.t1; t += 32) tile_row[t] = it.row;
 }
 
+// Mask tiles with at most kSparsePairs set bits take the lane-per-hit path:
+// the (row, column) bits of the mask go to a per-warp list, and every lane
+// with a hit sums popc(A[r] & B[c]) over the list for its own tile pair,
+// loading just those rows -- hits of a probe round proceed side by side
+// instead of one after another.  Denser masks broadcast the K-tile rows.
+constexpr int kSparsePairs = 16;
+
 template <int B>
 __global__ void __launch_bounds__(kTPB) k_tc(GView v, long long nblk, const int* __restrict__ tile_row,
                                              unsigned long long* __restrict__ count) {
   using WT = typename Word<B>::T;
   constexpr int RPL = B > 32 ? 2 : 1;
+  __shared__ short pairs_sh[kTPB / 32][kSparsePairs];  // (r << 7) | c
   const unsigned lane = threadIdx.x & 31;
+  short* pairs = pairs_sh[threadIdx.x >> 5];
   const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
   const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
@@ -63,6 +72,32 @@ __global__ void __launch_bounds__(kTPB) k_tc(GView v, long long nblk, const int*
       unsigned hi = __reduce_or_sync(0xffffffffu, (unsigned)(U >> 32));
       U = ((unsigned long long)hi << 32) | lo;
     }
+    // mask bits as a list when the mask is sparse (lane order = row order)
+    int npairs = -1;
+    {
+      const int c0 = popc_w(M0) + (RPL == 2 ? popc_w(M1) : 0);
+      int incl = c0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if ((int)lane >= o) incl += y;
+      }
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      if (total <= kSparsePairs) {
+        int pos = incl - c0;
+        for (int h = 0; h < RPL; ++h) {
+          const int r = (int)lane + 32 * h;
+          unsigned long long w = (unsigned long long)(h ? M1 : M0) << (64 - B);
+          while (w) {
+            const int c = __clzll(w);
+            w &= ~(0x8000000000000000ull >> c);
+            pairs[pos++] = (short)((r << 7) | c);
+          }
+        }
+        npairs = total;
+      }
+      __syncwarp();
+    }
     // list A: row I, tiles with block column <= K  -> [rowptr[I], m]
     // list B: row K, all tiles (block columns <= K in a lower triangle)
     const int a0 = v.rowptr[I], a1 = (int)m + 1;
@@ -79,6 +114,17 @@ __global__ void __launch_bounds__(kTPB) k_tc(GView v, long long nblk, const int*
         if (q < s1 && v.colind[q] == J) hit = q;
       }
       unsigned found = __ballot_sync(0xffffffffu, hit >= 0);
+      if (npairs >= 0) {  // sparse mask: each lane handles its own hit
+        if (hit >= 0) {
+          const int ia = probe_a ? p : hit;  // tile (I,J)
+          const int ib = probe_a ? hit : p;  // tile (K,J)
+          for (int k = 0; k < npairs; ++k) {
+            const int pr = pairs[k];
+            acc += popc_w((WT)(val[(size_t)ia * B + (pr >> 7)] & val[(size_t)ib * B + (pr & 127)]));
+          }
+        }
+        continue;
+      }
       while (found) {
         const int src = __ffs(found) - 1;
         found &= found - 1;
