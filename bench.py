@@ -44,7 +44,7 @@ def parse():
                     help="auto: top-down steps while the frontier is small (graph is symmetric)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving streams")
-    ap.add_argument("--serve-qps", type=float, default=4000.0, help="offered BFS query rate")
+    ap.add_argument("--serve-qps", type=float, default=8000.0, help="offered BFS query rate")
     ap.add_argument("--serve-s", type=float, default=1.5, help="seconds of arrivals per stream")
     ap.add_argument("--tc-graphs", default="mesh,rmat", help="graphs of --workload tc (mesh, rmat)")
     ap.add_argument("--tc-variants", default="input,degree", help="vertex orders of --workload tc")
@@ -297,8 +297,12 @@ def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed):
     srv = gbo.Server(g, bfs_slots=1024, ppr_slots=32 if ppr_frac > 0 else 0, alpha=0.85, tol=1e-7)
     import queue
 
-    tq = queue.Queue()
+    # one queue and consumer pool per kind, so clients waiting on slow PPR
+    # results never hold BFS results back (each pool collects in order)
+    tq = {"bfs": queue.Queue(), "ppr": queue.Queue()}
+    consumers = {"bfs": 14, "ppr": 4 if ppr_frac > 0 else 0}
     lat = {"bfs": [], "ppr": []}
+    done_t = {"bfs": 0.0, "ppr": 0.0}
     lock = threading.Lock()
     t0 = time.perf_counter()
 
@@ -310,23 +314,25 @@ def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed):
             if d > 0:
                 time.sleep(d)
             kind, arg = qs[i]
-            tq.put((kind, srv.submit_bfs(arg) if kind == "bfs" else srv.submit_ppr(*arg)))
-        for _ in range(consumers):
-            tq.put(None)
+            tq[kind].put(srv.submit_bfs(arg) if kind == "bfs" else srv.submit_ppr(*arg))
+        for kind, c in consumers.items():
+            for _ in range(c):
+                tq[kind].put(None)
 
-    def consumer():
-        bufs = {"bfs": np.empty(n, np.int32), "ppr": np.empty(n, np.float32)}  # reused per thread
+    def consumer(kind):
+        buf = np.empty(n, np.int32 if kind == "bfs" else np.float32)  # reused per thread
         while True:
-            item = tq.get()
-            if item is None:
+            ticket = tq[kind].get()
+            if ticket is None:
                 return
-            kind, ticket = item
-            _, ms, _ = srv.wait(ticket, kind, timeout=120.0, out=bufs[kind])
+            _, ms, _ = srv.wait(ticket, kind, timeout=300.0, out=buf)
             with lock:
                 lat[kind].append(ms)
+                done_t[kind] = max(done_t[kind], time.perf_counter() - t0)
 
-    consumers = 12
-    ths = [threading.Thread(target=producer)] + [threading.Thread(target=consumer) for _ in range(consumers)]
+    ths = [threading.Thread(target=producer)]
+    for kind, c in consumers.items():
+        ths += [threading.Thread(target=consumer, args=(kind,)) for _ in range(c)]
     for th in ths:
         th.start()
     for th in ths:
@@ -335,6 +341,8 @@ def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed):
     st = srv.stats()
     srv.close()
     out = {"offered_qps": rate_qps, "queries": nq, "achieved_qps": nq / wall, "wall_s": wall,
+           "bfs_qps": len(lat["bfs"]) / max(done_t["bfs"], 1e-9),
+           "ppr_qps": len(lat["ppr"]) / max(done_t["ppr"], 1e-9) if lat["ppr"] else None,
            "rounds": st["rounds"], "kernel_launches": st["kernel_launches"],
            "phase_ms": {k: round(st[k], 1) for k in ("bfs_round_ms", "ppr_round_ms", "retire_ms", "copy_ms",
                                                      "copy_wait_ms", "copy_d2h_ms", "copy_widen_ms")}}
@@ -757,9 +765,10 @@ def suite_msbfs(args):
         srcs = rng.integers(0, n, k).astype(np.int32)
         out = gbo.DeviceBuffer(4 * n * k)
         ms = _timed(gbo, lambda: g.msbfs(srcs, out=out), max(1, args.steps // 2), args.warmup)
+        levels_ms = [round(x, 3) for x in g.last_run()["step_ms"]]
         edges = _ms_edges(gbo, out, deg, n, k)
         res[k] = {"ms": ms, "qps": k / (ms / 1e3), "gteps_x_k": edges / (ms / 1e3) / 1e9,
-                  "speedup_vs_plain": (k / (ms / 1e3)) / (1e3 / plain_ms)}
+                  "speedup_vs_plain": (k / (ms / 1e3)) / (1e3 / plain_ms), "levels_ms": levels_ms}
         del out
     best = res[1024]
     _line("qps", best["qps"], "queries/s", True, best["ms"], args,

@@ -636,7 +636,7 @@ __global__ void __launch_bounds__(kTPB) k_pr_step(GView v, float* __restrict__ p
       const int r = lane % L::W;
       const gbo_item it = v.items[item];
       double a0 = 0.0, a1 = 0.0;
-      fold_row_cols<B, 8>(v, it.t0, it.t1, r, [&](long long j) { return (double)xg[j]; },
+      fold_row_cols<B, 4>(v, it.t0, it.t1, r, [&](long long j) { return (double)xg[j]; },
                           [](double& a, double b) { a += b; }, a0, a1);
       if (it.slot >= 0) {
         scratch[(size_t)it.slot * B + r] = a0;
@@ -931,6 +931,7 @@ unsigned grid_vertex(long long n) {
 }
 
 int get_state(gbo_graph* g, AlgoState** out) {
+  g->last_run_ms = 0;  // statistics now describe this algorithm's run
   if (!g->algo) {
     AlgoState* a = new AlgoState();
     g->algo = a;
@@ -1450,6 +1451,7 @@ extern "C" int gbo_graph_last_run(const gbo_graph* g, gbo_run_stats* stats) {
   clear_error();
   if (!g || !stats) return fail(GBO_ERR_INVALID, "NULL argument");
   memset(stats, 0, sizeof(*stats));
+  if (g->last_run_ms) return ms_last_run(g, stats);
   const AlgoState* a = g->algo;
   if (!a) return GBO_OK;
   stats->iterations = a->h_ctrl ? a->h_ctrl->iter : 0;

@@ -30,6 +30,7 @@ struct gbo_graph {
   int bfs_push_thr = -1;   // push below this frontier size (-1: nrows / 64)
   int* perm = nullptr;     // GBO_FLAG_DEGREE_ORDER: new label of every input vertex
   int* tile_row = nullptr; // block row of every tile (triangle counting)
+  int last_run_ms = 0;     // 1: the last traversal was a multi-source BFS
   bool owns_outdeg = true;
   // balanced schedule
   int chunk = 0;
@@ -90,5 +91,7 @@ void launch_invdeg(const int* d_deg, int n, float* d_inv, cudaStream_t stream);
 // Release the algorithm state of g (called by gbo_graph_free).
 void free_algo_state(gbo_graph* g);
 void free_ms_state(gbo_graph* g);
+// Statistics of the last multi-source BFS (per-level times of its step kernel).
+int ms_last_run(const gbo_graph* g, gbo_run_stats* stats);
 
 }  // namespace gbo

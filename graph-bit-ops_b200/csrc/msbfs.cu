@@ -175,10 +175,23 @@ int msbfs_impl(gbo_graph* g, const int* h_srcs, int k, int32_t* d_levels, int* h
   }
   if (!done) return fail(GBO_ERR_TIMEOUT, "multi-source BFS did not terminate");
   if (h_depth) *h_depth = m.h_ctl[0];
+  g->last_run_ms = 1;
   return GBO_OK;
 }
 
 }  // namespace
+
+int ms_last_run(const gbo_graph* g, gbo_run_stats* st) {
+  const MsState* m = reinterpret_cast<const MsState*>(g->ms);
+  if (!m) return GBO_OK;
+  st->iterations = m->h_ctl ? m->h_ctl[0] : 0;
+  st->graph_replays = (int)((m->launches - 3) / (m->launches_per_replay > 0 ? m->launches_per_replay : 1));
+  st->kernel_launches = m->launches;
+  const int n = (int)m->step_ms.size();
+  st->nsteps = n < GBO_MAX_STEP_TIMES ? n : GBO_MAX_STEP_TIMES;
+  for (int i = 0; i < st->nsteps; ++i) st->step_ms[i] = m->step_ms[(size_t)i];
+  return GBO_OK;
+}
 
 void free_ms_state(gbo_graph* g) {
   MsState* m = reinterpret_cast<MsState*>(g->ms);

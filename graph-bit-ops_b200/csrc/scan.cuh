@@ -124,16 +124,27 @@ __device__ __forceinline__ void fold_row_cols(const GView& v, int t0, int t1, in
       comb(acc, term(base + j));
     }
   };
-  int t = t0;
-  for (; t + U <= t1; t += U) {
-    long long base[U];
-    AW a0[U], a1[U];
+  // software pipeline: batch i+1's column indices and row words load while
+  // batch i's gathers run
+  auto load = [&](int tb, long long (&base)[U], AW (&a0)[U], AW (&a1)[U]) {
 #pragma unroll
     for (int k = 0; k < U; ++k) {
-      base[k] = (long long)v.colind[t + k] * B;
-      a0[k] = (AW)val[(size_t)(t + k) * B + r] << (kBits - B);
-      a1[k] = L::RPL == 2 ? (AW)val[(size_t)(t + k) * B + 32 + r] << (kBits - B) : (AW)0;
+      base[k] = (long long)v.colind[tb + k] * B;
+      a0[k] = (AW)val[(size_t)(tb + k) * B + r] << (kBits - B);
+      a1[k] = L::RPL == 2 ? (AW)val[(size_t)(tb + k) * B + 32 + r] << (kBits - B) : (AW)0;
     }
+  };
+  int t = t0;
+  long long base[U];
+  AW a0[U], a1[U];
+  bool have = t + U <= t1;
+  if (have) load(t, base, a0, a1);
+  while (have) {
+    const int tn = t + U;
+    const bool next = tn + U <= t1;
+    long long nbase[U];
+    AW n0[U], n1[U];
+    if (next) load(tn, nbase, n0, n1);
     T g0[U], g1[U];
     bool h0[U], h1[U];
 #pragma unroll
@@ -160,6 +171,16 @@ __device__ __forceinline__ void fold_row_cols(const GView& v, int t0, int t1, in
     for (int k = 0; k < U; ++k) {
       rest(a0[k], base[k], acc0);
       if (L::RPL == 2) rest(a1[k], base[k], acc1);
+    }
+    t = tn;
+    have = next;
+    if (next) {
+#pragma unroll
+      for (int k = 0; k < U; ++k) {
+        base[k] = nbase[k];
+        a0[k] = n0[k];
+        a1[k] = n1[k];
+      }
     }
   }
   for (; t < t1; ++t) {
