@@ -44,6 +44,7 @@ def parse():
                     help="auto: top-down steps while the frontier is small (graph is symmetric)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving streams")
+    ap.add_argument("--no-permuted", action="store_true", help="skip the degree-ordered variant")
     ap.add_argument("--serve-qps", type=float, default=8000.0, help="offered BFS query rate")
     ap.add_argument("--serve-s", type=float, default=1.5, help="seconds of arrivals per stream")
     ap.add_argument("--tc-graphs", default="mesh,rmat", help="graphs of --workload tc (mesh, rmat)")
@@ -480,6 +481,36 @@ def run_ours(args, ws, rank, local):
                             "qps_vs_plain": (kq / mms) / (1.0 / ms)}
         d_lv.free()
 
+    # permuted variant (reported beside the headline, never as it): the same
+    # graph relabelled by descending degree, BFS from vertex 0's new label
+    permuted = None
+    if not args.no_permuted and args.layout == "row":
+        t0 = time.perf_counter()
+        gp = gbo.Graph.from_csr(csr, args.tile, gbo.FLAG_SYMMETRIC | gbo.FLAG_DEGREE_ORDER)
+        pbuild = time.perf_counter() - t0
+        perm = gp.permutation()
+        plv, _ = gp.bfs(int(perm[0]))
+        if not np.array_equal(plv[perm], levels):
+            raise SystemExit("degree-ordered BFS levels differ from the headline BFS")
+        pbuf = gbo.DeviceBuffer(4 * n)
+        for _ in range(args.warmup):
+            gp.bfs(int(perm[0]), out=pbuf)
+        gbo.sync()
+        pst = []
+        ev0.record()
+        for _ in range(args.steps):
+            gp.bfs(int(perm[0]), out=pbuf)
+            pst.append(gp.last_run()["step_ms"])
+        ev1.record()
+        gbo.sync()
+        pms = ev0.elapsed_ms(ev1) / args.steps
+        permuted = {"workload": "the same BFS on the graph relabelled by descending degree",
+                    "gteps": edges / (pms / 1e3) / 1e9, "ms_per_bfs": pms,
+                    "nblocks": int(gp.info().nblocks), "relabel_and_pack_s": pbuild,
+                    "levels_ms": [float(v) for v in np.array(pst).mean(axis=0)]}
+        pbuf.free()
+        gp.free()
+
     # served: Poisson query streams into the continuous-batching server
     served = {}
     if not args.no_serve:
@@ -525,6 +556,7 @@ def run_ours(args, ws, rank, local):
                       "levels_ms": [float(v) for v in lvl_ms[:k]],
                       "levels_gb": [b / 1e9 for b in lvl_bytes[:k]]},
         "graph_build_s": build_s,
+        "permuted_variant": permuted,
     }
     if rank == 0 and ws == 1 and not args.no_cpu:
         v, t, cores, _ = cpu_bfs(csr, args.tile, args.cpu_samples)

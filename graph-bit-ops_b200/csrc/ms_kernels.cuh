@@ -124,6 +124,7 @@ __global__ void __launch_bounds__(kTPB) k_step(Args a) {
   constexpr int U = S >= 8 ? 1 : 8 / S;
   __shared__ uint32_t acc_sh[kWarps][32 * KW];
   __shared__ int2 list_sh[kWarps][kList];
+  __shared__ int nl_sh[kWarps];  // pairs appended to the list by the current tile
   volatile int* c = a.ctl;
   if (c[1]) return;  // done
   const int lvl = c[0];
@@ -142,6 +143,7 @@ __global__ void __launch_bounds__(kTPB) k_step(Args a) {
     const uint32_t vrow = a.vfull[it.row];
     if (vrow != 0xffffffffu) {
       for (int q = lane; q < 32 * KW; q += 32) acc[q] = 0u;
+      if (lane == 0) nl_sh[wib] = 0;
       __syncwarp();
       const bool row_open = !((vrow >> (31 - lane)) & 1u);  // lane r: row r still open
       const uint32_t* __restrict__ val = reinterpret_cast<const uint32_t*>(v.val);
@@ -180,55 +182,67 @@ __global__ void __launch_bounds__(kTPB) k_step(Args a) {
           fw = fb[cb];
         }
         unsigned tiles = __ballot_sync(0xffffffffu, fw != 0);
+        // tiles with frontier columns, kT at a time: their row words load
+        // together (lane r: row r); pairs go to the list at positions taken
+        // with a shared-memory counter (the OR accumulation does not depend
+        // on the order)
+        constexpr int kT = 8;
         while (tiles) {
-          const int jt = __ffs(tiles) - 1;
-          tiles &= tiles - 1;
-          const int C = __shfl_sync(0xffffffffu, cb, jt);
-          const uint32_t fcol = __shfl_sync(0xffffffffu, fw, jt);
-          uint32_t eff = val[(size_t)(b0 + jt) * 32 + lane] & fcol;  // lane r: row r
-          if (!row_open) eff = 0u;
-          // queue this lane's pairs (lane, C*32+c) at its prefix offset
-          const int cnt_l = __popc(eff);
-          int pre = cnt_l;
+          int jt[kT];
 #pragma unroll
-          for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, pre, o);
-            if ((int)lane >= o) pre += y;
+          for (int k = 0; k < kT; ++k) {
+            jt[k] = tiles ? __ffs(tiles) - 1 : -1;
+            if (tiles) tiles &= tiles - 1;
           }
-          const int total = __shfl_sync(0xffffffffu, pre, 31);
-          pre -= cnt_l;
-          if (total == 0) continue;
-          if (nlist + total > kList) flush();
-          if (total > kList) {
-            // dense tile: OR its rows straight from the row words
-            unsigned rows = __ballot_sync(0xffffffffu, eff != 0);
-            while (rows) {
-              const int r = __ffs(rows) - 1;
-              rows &= rows - 1;
-              unsigned bits = __shfl_sync(0xffffffffu, eff, r);
-              uint32_t racc = 0;
-              while (bits) {
-                const unsigned pos = nth_set_bit(bits, s + 1);
-                uint32_t f = 0;
-                if (pos != 0xffffffffu) f = F[((size_t)C * 32 + (31 - (int)pos)) * KW + w];
+          uint32_t eff[kT];
+          int Ck[kT];
 #pragma unroll
-                for (int o = KW; o < 32; o <<= 1) f |= __shfl_xor_sync(0xffffffffu, f, o);
-                racc |= f;
-                const unsigned last = nth_set_bit(bits, S);
-                bits = last == 0xffffffffu ? 0u : (bits & ~(0xffffffffu >> (31 - last)));
+          for (int k = 0; k < kT; ++k) {
+            const int src = jt[k] < 0 ? 0 : jt[k];
+            Ck[k] = __shfl_sync(0xffffffffu, cb, src);
+            const uint32_t fcol = __shfl_sync(0xffffffffu, fw, src);
+            eff[k] = (jt[k] >= 0 && row_open) ? (val[(size_t)(b0 + jt[k]) * 32 + lane] & fcol) : 0u;
+          }
+#pragma unroll
+          for (int k = 0; k < kT; ++k) {
+            const int cnt_l = __popc(eff[k]);
+            const int total = (int)__reduce_add_sync(0xffffffffu, (unsigned)cnt_l);
+            if (total == 0) continue;
+            if (nlist + total > kList) flush();
+            if (total > kList) {
+              // dense tile: OR its rows straight from the row words
+              unsigned rows = __ballot_sync(0xffffffffu, eff[k] != 0);
+              while (rows) {
+                const int r = __ffs(rows) - 1;
+                rows &= rows - 1;
+                unsigned bits = __shfl_sync(0xffffffffu, eff[k], r);
+                uint32_t racc = 0;
+                while (bits) {
+                  const unsigned pos = nth_set_bit(bits, s + 1);
+                  uint32_t f = 0;
+                  if (pos != 0xffffffffu) f = F[((size_t)Ck[k] * 32 + (31 - (int)pos)) * KW + w];
+#pragma unroll
+                  for (int o = KW; o < 32; o <<= 1) f |= __shfl_xor_sync(0xffffffffu, f, o);
+                  racc |= f;
+                  const unsigned last = nth_set_bit(bits, S);
+                  bits = last == 0xffffffffu ? 0u : (bits & ~(0xffffffffu >> (31 - last)));
+                }
+                if (s == 0) acc[r * KW + w] |= racc;
               }
-              if (s == 0) acc[r * KW + w] |= racc;
+              continue;
             }
-            continue;
+            int pos = cnt_l ? nlist + atomicAdd(&nl_sh[wib], cnt_l) : 0;
+            uint32_t m = eff[k];
+            while (m) {
+              const int col = __clz(m);
+              m &= ~(0x80000000u >> col);
+              list[pos++] = make_int2((int)lane, Ck[k] * 32 + col);
+            }
+            nlist += total;
+            __syncwarp();
+            if (lane == 0) nl_sh[wib] = 0;
+            __syncwarp();
           }
-          int pos = nlist + pre;
-          uint32_t m = eff;
-          while (m) {
-            const int col = __clz(m);
-            m &= ~(0x80000000u >> col);
-            list[pos++] = make_int2((int)lane, C * 32 + col);
-          }
-          nlist += total;
         }
       }
       flush();

@@ -126,23 +126,23 @@ __device__ __forceinline__ void fold_row_cols(const GView& v, int t0, int t1, in
   };
   // software pipeline: batch i+1's column indices and row words load while
   // batch i's gathers run
-  auto load = [&](int tb, long long (&base)[U], AW (&a0)[U], AW (&a1)[U]) {
+  auto load = [&](int tb, unsigned (&base)[U], AW (&a0)[U], AW (&a1)[U]) {
 #pragma unroll
     for (int k = 0; k < U; ++k) {
-      base[k] = (long long)v.colind[tb + k] * B;
+      base[k] = (unsigned)v.colind[tb + k] * (unsigned)B;  // < 2^32: ncols is an int
       a0[k] = (AW)val[(size_t)(tb + k) * B + r] << (kBits - B);
       a1[k] = L::RPL == 2 ? (AW)val[(size_t)(tb + k) * B + 32 + r] << (kBits - B) : (AW)0;
     }
   };
   int t = t0;
-  long long base[U];
+  unsigned base[U];
   AW a0[U], a1[U];
   bool have = t + U <= t1;
   if (have) load(t, base, a0, a1);
   while (have) {
     const int tn = t + U;
     const bool next = tn + U <= t1;
-    long long nbase[U];
+    unsigned nbase[U];
     AW n0[U], n1[U];
     if (next) load(tn, nbase, n0, n1);
     T g0[U], g1[U];
@@ -154,12 +154,12 @@ __device__ __forceinline__ void fold_row_cols(const GView& v, int t0, int t1, in
       if (h0[k]) {
         const int j = lead(a0[k]);
         a0[k] &= ~(kTop >> j);
-        g0[k] = term(base[k] + j);
+        g0[k] = term((long long)base[k] + j);
       }
       if (h1[k]) {
         const int j = lead(a1[k]);
         a1[k] &= ~(kTop >> j);
-        g1[k] = term(base[k] + j);
+        g1[k] = term((long long)base[k] + j);
       }
     }
 #pragma unroll
@@ -169,8 +169,8 @@ __device__ __forceinline__ void fold_row_cols(const GView& v, int t0, int t1, in
     }
 #pragma unroll
     for (int k = 0; k < U; ++k) {
-      rest(a0[k], base[k], acc0);
-      if (L::RPL == 2) rest(a1[k], base[k], acc1);
+      rest(a0[k], (long long)base[k], acc0);
+      if (L::RPL == 2) rest(a1[k], (long long)base[k], acc1);
     }
     t = tn;
     have = next;

@@ -721,6 +721,17 @@ void worker_main(gbo_server* S, int kind) {
       if (tab[q] > 0 && !fin[q]) return true;
     return false;
   };
+  // Every query in flight keeps one result buffer of its pool in reserve
+  // (BFS: the byte pool, PPR: the word pool), so a finished query can always
+  // retire and the engines never wait on clients mid-traversal; queries past
+  // that budget stay pending.
+  const int rpool = kind == 0 ? 0 : 1;
+  auto budget = [&]() {
+    long long inflight = 0;
+    for (long long t : tab) inflight += t > 0;
+    return (long long)S->pool_free[rpool].size() - inflight;
+  };
+  double stall_since = -1.0;
   while (true) {
     std::vector<std::pair<int, Query>> adm;
     {
@@ -729,15 +740,32 @@ void worker_main(gbo_server* S, int kind) {
         if (S->stop || S->worker_status != GBO_OK) return;
         const int bp = blocked_pool(S, kind);
         if (bp >= 0) move_results_to_host(S, bp, lk);
-        const bool work = !S->pending[kind].empty() || unfinished() || (occupied() && blocked_pool(S, kind) < 0);
-        if (work) break;
+        const bool can_admit = !S->pending[kind].empty() && budget() > 0;
+        const bool work = can_admit || unfinished() || (occupied() && blocked_pool(S, kind) < 0);
+        if (work) {
+          stall_since = -1.0;
+          break;
+        }
+        if (!S->pending[kind].empty()) {
+          // every buffer of the pool holds a result nobody has taken: wait a
+          // little for clients, then move results to host memory (a client
+          // may be waiting for a query that is still pending)
+          const double now = now_ms();
+          if (stall_since < 0) stall_since = now;
+          if (now - stall_since > 100.0) {
+            move_results_to_host(S, rpool, lk);
+            stall_since = -1.0;
+            continue;
+          }
+        }
         // submit, take and destroy notify; the timeout bounds a missed wake-up
         S->cv_work.wait_for(lk, std::chrono::milliseconds(20));
       }
-      // admission into free slots, arrival order
+      // admission into free slots, arrival order, within the buffer budget
       size_t nx = 0;
       std::deque<Query>& pend = S->pending[kind];
-      while (!pend.empty()) {
+      long long room = budget();
+      while (!pend.empty() && room > 0) {
         while (nx < tab.size() && tab[nx] != 0) ++nx;
         if (nx >= tab.size()) break;
         Query q = std::move(pend.front());
@@ -748,6 +776,7 @@ void worker_main(gbo_server* S, int kind) {
         if (kind == 0) S->bslot_start[(size_t)slot] = S->level;
         else S->pslot_iters[(size_t)slot] = 0;
         adm.emplace_back(slot, std::move(q));
+        --room;
       }
     }
     int st = GBO_OK;
