@@ -902,15 +902,37 @@ def suite_serve(args):
     import gbo
 
     csr = gbo.gen_rmat(21, 16, seed=2, **RMAT)
+    n = csr.nrows
     g = gbo.Graph.from_csr(csr, 32)
+    # plain per-query kernels on the same graph and GPU: one BFS per source,
+    # one PPR forward solve per personalization set (same tolerance)
+    rng = np.random.default_rng(13)
+    buf = gbo.DeviceBuffer(4 * n)
+    bfs_ms = float(np.mean([_timed(gbo, lambda s=int(s): g.bfs(s, out=buf), 2, 1)
+                            for s in rng.integers(0, n, 8)]))
+    import ctypes as C
+
+    it = C.c_int(0)
+    ppr_ms = []
+    for _ in range(3):
+        m = int(rng.integers(1, 65))
+        v = np.zeros(n, np.float32)
+        v[rng.choice(n, m, replace=False)] = rng.dirichlet(np.ones(m))
+        dv = gbo.DeviceBuffer.from_numpy(v)
+        ppr_ms.append(_timed(gbo, lambda: gbo.check(gbo.lib().gbo_ppr_forward(
+            g.h, dv.ptr, C.c_float(0.85), C.c_float(1e-7), 1000, buf.ptr, C.byref(it), None)), 1, 1))
+    plain = {"bfs_qps": 1e3 / bfs_ms, "ppr_qps": 1e3 / float(np.mean(ppr_ms)), "ppr_iterations": it.value}
     out = {}
     rates = [float(r) for r in args.serve_rates.split(",")]
     for rate in rates:
-        out[int(rate)] = serve_stream(gbo, g, csr.nrows, rate, min(args.serve_s, 2e4 / rate), 0.1, 11)
+        r = serve_stream(gbo, g, n, rate, min(args.serve_s, 2e4 / rate), 0.1, 11)
+        r["bfs_vs_plain"] = r["bfs_qps"] / plain["bfs_qps"]
+        r["ppr_vs_plain"] = (r["ppr_qps"] or 0.0) / plain["ppr_qps"]
+        out[int(rate)] = r
     top = out[int(rates[len(rates) // 2])]
     _line("qps", top["achieved_qps"], "queries/s", True, 1e3 / max(top["achieved_qps"], 1e-9), args,
           {"workload": "served BFS + PPR queries, Poisson arrivals, R-MAT scale 21 seed 2, B2SR 32",
-           "nvertices": csr.nrows, "nnz": csr.nnz}, dtype="u32", by_rate=out)
+           "nvertices": n, "nnz": csr.nnz}, dtype="u32", plain=plain, by_rate=out)
     g.free()
 
 
