@@ -195,6 +195,7 @@ extern "C" int gbo_graph_from_csr(const int* rowptr, const int* colind, int nrow
 
   gbo_graph* g = new gbo_graph();
   g->symmetric = (flags & GBO_FLAG_SYMMETRIC) && !lower && nrows == ncols;
+  g->tc_mma = (flags & GBO_FLAG_TC_MMA) != 0;
   if (!perm.empty()) {
     if (cudaMalloc(&g->perm, sizeof(int) * perm.size()) != cudaSuccess ||
         cudaMemcpy(g->perm, perm.data(), sizeof(int) * perm.size(), cudaMemcpyHostToDevice) != cudaSuccess) {

@@ -31,6 +31,7 @@ struct gbo_graph {
   int* perm = nullptr;     // GBO_FLAG_DEGREE_ORDER: new label of every input vertex
   int* tile_row = nullptr; // block row of every tile (triangle counting)
   int last_run_ms = 0;     // 1: the last traversal was a multi-source BFS
+  bool tc_mma = false;     // GBO_FLAG_TC_MMA: dense 32x32 mask tiles on the 1-bit MMA
   bool owns_outdeg = true;
   // balanced schedule
   int chunk = 0;

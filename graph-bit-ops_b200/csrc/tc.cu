@@ -47,7 +47,7 @@ constexpr int kSparsePairs = 16;
 
 template <int B>
 __global__ void __launch_bounds__(kTPB) k_tc(GView v, long long nblk, const int* __restrict__ tile_row,
-                                             unsigned long long* __restrict__ count) {
+                                             int skip_dense, unsigned long long* __restrict__ count) {
   using WT = typename Word<B>::T;
   constexpr int RPL = B > 32 ? 2 : 1;
   __shared__ short pairs_sh[kTPB / 32][kSparsePairs];  // (r << 7) | c
@@ -98,6 +98,7 @@ __global__ void __launch_bounds__(kTPB) k_tc(GView v, long long nblk, const int*
       }
       __syncwarp();
     }
+    if (npairs < 0 && skip_dense) continue;  // dense masks go to the tensor-core kernel
     // list A: row I, tiles with block column <= K  -> [rowptr[I], m]
     // list B: row K, all tiles (block columns <= K in a lower triangle)
     const int a0 = v.rowptr[I], a1 = (int)m + 1;
@@ -163,6 +164,118 @@ __global__ void __launch_bounds__(kTPB) k_tc(GView v, long long nblk, const int*
   if (lane == 0 && acc) atomicAdd(count, acc);
 }
 
+// D += popc(A AND B) over 256-bit rows/columns: the 1-bit tensor-core MMA
+// (m16n8k256, A row-major 16x256, B column-major 256x8, s32 accumulators).
+// Fragments, with g = lane / 4 and q = lane % 4: a0 = A[g][32q..32q+31],
+// a1 = A[g+8][same], a2 = A[g][128+32q..], a3 = A[g+8][128+32q..];
+// b0 = B[32q..][g], b1 = B[128+32q..][g]; d0,d1 = D[g][2q, 2q+1],
+// d2,d3 = D[g+8][2q, 2q+1].
+__device__ __forceinline__ void mma_and_popc(int (&d)[4], unsigned a0, unsigned a1, unsigned a2,
+                                             unsigned a3, unsigned b0, unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k256.row.col.s32.b1.b1.s32.and.popc "
+      "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// Opt-in (GBO_FLAG_TC_MMA): on the configured graphs this path did not beat
+// the CUDA-core one (king mesh b=32: 3.3 vs 3.6 ms but b=16 without it 2.1 ms;
+// R-MAT 20 degree-ordered b=32: 25.8 vs 20.5 ms), so it is not the default.
+// Dense 32x32 mask tiles (more than kSparsePairs bits) on the tensor cores:
+// for a mask tile (I,K) the product P = sum_J A_IJ B_KJ^T over the hits J is
+// a 32x32 AND-popc product with the hits' 32-bit rows laid side by side
+// along k (8 hits per 256-bit step), then sum_{r,c} M[r][c] P[r][c].
+__global__ void __launch_bounds__(kTPB) k_tc32_mma(GView v, long long nblk, const int* __restrict__ tile_row,
+                                                   unsigned long long* __restrict__ count) {
+  __shared__ int2 hits_sh[kTPB / 32][32];
+  __shared__ uint32_t tiles_sh[kTPB / 32][2][8][32];  // A and B tiles of 8 hits
+  const unsigned lane = threadIdx.x & 31;
+  const int g = (int)(lane >> 2), q4 = (int)(lane & 3);
+  int2* hits = hits_sh[threadIdx.x >> 5];
+  uint32_t (*sA)[32] = tiles_sh[threadIdx.x >> 5][0];
+  uint32_t (*sB)[32] = tiles_sh[threadIdx.x >> 5][1];
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  const uint32_t* __restrict__ val = reinterpret_cast<const uint32_t*>(v.val);
+  unsigned long long acc = 0;
+  for (long long m = warp; m < nblk; m += nwarps) {
+    const uint32_t M0 = val[(size_t)m * 32 + lane];
+    const int total = (int)__reduce_add_sync(0xffffffffu, (unsigned)__popc(M0));
+    if (total <= kSparsePairs) continue;  // handled by k_tc
+    const int I = tile_row[m];
+    const int K = v.colind[m];
+    const int a0i = v.rowptr[I], a1i = (int)m + 1;
+    const int b0i = v.rowptr[K], b1i = v.rowptr[K + 1];
+    const bool probe_a = (a1i - a0i) <= (b1i - b0i);
+    const int p0 = probe_a ? a0i : b0i, p1 = probe_a ? a1i : b1i;
+    const int s0 = probe_a ? b0i : a0i, s1 = probe_a ? b1i : a1i;
+    int d[2][4][4];
+#pragma unroll
+    for (int mb = 0; mb < 2; ++mb)
+#pragma unroll
+      for (int nb = 0; nb < 4; ++nb)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) d[mb][nb][e] = 0;
+    for (int base = p0; base < p1; base += 32) {
+      const int p = base + (int)lane;
+      int hit = -1;
+      if (p < p1) {
+        const int J = v.colind[p];
+        const int qq = lower_bound_dev(v.colind, s0, s1, J);
+        if (qq < s1 && v.colind[qq] == J) hit = qq;
+      }
+      const unsigned found = __ballot_sync(0xffffffffu, hit >= 0);
+      const int nh = __popc(found);
+      if (hit >= 0)
+        hits[__popc(found & ((1u << lane) - 1u))] = probe_a ? make_int2(p, hit) : make_int2(hit, p);
+      __syncwarp();
+      for (int c0 = 0; c0 < nh; c0 += 8) {
+        // stage the 8 hits' A tiles (I,J) and B tiles (K,J), one coalesced
+        // 128-byte load per tile, then build the fragments from shared memory
+#pragma unroll
+        for (int h = 0; h < 8; ++h) {
+          const int2 hh = c0 + h < nh ? hits[c0 + h] : make_int2(-1, -1);
+          sA[h][lane] = hh.x >= 0 ? val[(size_t)hh.x * 32 + lane] : 0u;
+          sB[h][lane] = hh.y >= 0 ? val[(size_t)hh.y * 32 + lane] : 0u;
+        }
+        __syncwarp();
+        unsigned bq[4][2];
+#pragma unroll
+        for (int nb = 0; nb < 4; ++nb) {
+          bq[nb][0] = sB[q4][8 * nb + g];
+          bq[nb][1] = sB[q4 + 4][8 * nb + g];
+        }
+#pragma unroll
+        for (int mb = 0; mb < 2; ++mb) {
+          const unsigned a0 = sA[q4][16 * mb + g], a1 = sA[q4][16 * mb + g + 8];
+          const unsigned a2 = sA[q4 + 4][16 * mb + g], a3 = sA[q4 + 4][16 * mb + g + 8];
+#pragma unroll
+          for (int nb = 0; nb < 4; ++nb) mma_and_popc(d[mb][nb], a0, a1, a2, a3, bq[nb][0], bq[nb][1]);
+        }
+        __syncwarp();
+      }
+      __syncwarp();
+    }
+    // sum of P over the mask's bits: row r, column c at bit 31-c of M[r]
+#pragma unroll
+    for (int mb = 0; mb < 2; ++mb) {
+      const uint32_t mr0 = __shfl_sync(0xffffffffu, M0, 16 * mb + g);
+      const uint32_t mr1 = __shfl_sync(0xffffffffu, M0, 16 * mb + g + 8);
+#pragma unroll
+      for (int nb = 0; nb < 4; ++nb) {
+        const int col = 8 * nb + 2 * q4;
+        if ((mr0 >> (31 - col)) & 1u) acc += (unsigned)d[mb][nb][0];
+        if ((mr0 >> (30 - col)) & 1u) acc += (unsigned)d[mb][nb][1];
+        if ((mr1 >> (31 - col)) & 1u) acc += (unsigned)d[mb][nb][2];
+        if ((mr1 >> (30 - col)) & 1u) acc += (unsigned)d[mb][nb][3];
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0 && acc) atomicAdd(count, acc);
+}
+
 }  // namespace
 
 int tc_launch(gbo_graph* g, unsigned long long* d_count, cudaStream_t s) {
@@ -179,11 +292,16 @@ int tc_launch(gbo_graph* g, unsigned long long* d_count, cudaStream_t s) {
   if (warps > cap * 8) warps = cap * 8;
   const unsigned grid = blocks_for_warps(warps, kTPB / 32);
   switch (g->b) {
-    case 4: k_tc<4><<<grid, kTPB, 0, s>>>(v, g->nblk, g->tile_row, d_count); break;
-    case 8: k_tc<8><<<grid, kTPB, 0, s>>>(v, g->nblk, g->tile_row, d_count); break;
-    case 16: k_tc<16><<<grid, kTPB, 0, s>>>(v, g->nblk, g->tile_row, d_count); break;
-    case 32: k_tc<32><<<grid, kTPB, 0, s>>>(v, g->nblk, g->tile_row, d_count); break;
-    default: k_tc<64><<<grid, kTPB, 0, s>>>(v, g->nblk, g->tile_row, d_count); break;
+    case 4: k_tc<4><<<grid, kTPB, 0, s>>>(v, g->nblk, g->tile_row, 0, d_count); break;
+    case 8: k_tc<8><<<grid, kTPB, 0, s>>>(v, g->nblk, g->tile_row, 0, d_count); break;
+    case 16: k_tc<16><<<grid, kTPB, 0, s>>>(v, g->nblk, g->tile_row, 0, d_count); break;
+    case 32: if (g->tc_mma) {
+      k_tc<32><<<grid, kTPB, 0, s>>>(v, g->nblk, g->tile_row, 1, d_count);
+      k_tc32_mma<<<grid, kTPB, 0, s>>>(v, g->nblk, g->tile_row, d_count);
+    } else {
+      k_tc<32><<<grid, kTPB, 0, s>>>(v, g->nblk, g->tile_row, 0, d_count);
+    }; break;
+    default: k_tc<64><<<grid, kTPB, 0, s>>>(v, g->nblk, g->tile_row, 0, d_count); break;
   }
   GBO_CUDA_TRY(cudaGetLastError());
   return GBO_OK;

@@ -35,6 +35,7 @@ FLAG_LAYOUT_COL = 4
 FLAG_LOWER = 8
 FLAG_SYMMETRIC = 16
 FLAG_DEGREE_ORDER = 32
+FLAG_TC_MMA = 64
 OUT_I32 = 0
 OUT_F32 = 1
 MTX_READMTX = 0

@@ -134,13 +134,18 @@ enum gbo_graph_flags {
   GBO_FLAG_SYMMETRIC = 16,  /* caller asserts the packed matrix is symmetric:
                                BFS may then take top-down (push) steps while
                                the frontier is small (direction-optimising) */
-  GBO_FLAG_DEGREE_ORDER = 32 /* relabel vertices by descending degree before
+  GBO_FLAG_DEGREE_ORDER = 32, /* relabel vertices by descending degree before
                                packing (P' = Q P Q^T; gbo_graph_permutation
                                gives the labels).  For permutation-invariant
                                results such as the triangle count: with
                                GBO_FLAG_LOWER every row then holds only
                                higher-degree neighbours, so hub rows stay
                                short.  No reference counterpart. */
+  GBO_FLAG_TC_MMA = 64       /* b = 32: count the mask tiles with more than 16
+                               bits on the 1-bit tensor-core MMA
+                               (mma.sync m16n8k256 AND-popc, 8 hits per
+                               step).  Opt-in: on sparse-tile graphs the
+                               CUDA-core path is as fast or faster. */
 };
 
 /* Pack a CSR matrix M into a device-resident B2SR graph owned by the handle.

@@ -88,6 +88,18 @@ def test_triangle_count(gbo, orc, gpu, graphs, b):
         assert g.tc() == orc.tc_csr(csr.rowptr, csr.colind, csr.nrows), (name, b)
 
 
+def test_triangle_count_tensor_core_path(gbo, orc, gpu, graphs):
+    """b = 32 with GBO_FLAG_TC_MMA: dense mask tiles through the 1-bit MMA."""
+    for name in ("mesh33", "rmat12", "er1000", "star20000"):
+        csr = graphs[name]
+        for extra in (0, gbo.FLAG_DEGREE_ORDER):
+            g = gbo.Graph.from_csr(csr, 32, gbo.FLAG_LOWER | gbo.FLAG_TC_MMA | extra)
+            assert g.tc() == orc.tc_csr(csr.rowptr, csr.colind, csr.nrows), (name, extra)
+    for side in (64, 257):
+        m = gbo.gen_king_mesh(side)
+        assert gbo.Graph.from_csr(m, 32, gbo.FLAG_LOWER | gbo.FLAG_TC_MMA).tc() == 4 * (side - 1) ** 2
+
+
 def test_triangle_mesh_closed_form(gbo, gpu):
     for side in (2, 3, 64, 257):
         m = gbo.gen_king_mesh(side)
