@@ -110,7 +110,7 @@ def traversed_edges(csr, levels):
 
 
 # --------------------------------------------------------------- roofline
-def bfs_level_bytes(rowptr_b, colind_b, levels, nrows, b, row_live, layout="row"):
+def bfs_level_bytes(rowptr_b, colind_b, levels, nrows, b, row_live, layout="row", csr=None):
     """Algorithmic bytes of each BFS pull step (the words the step must touch).
 
     Step L reads the block-row offsets, the visited and frontier words, the
@@ -120,7 +120,10 @@ def bfs_level_bytes(rowptr_b, colind_b, levels, nrows, b, row_live, layout="row"
     decide the step: with ROW tiles one b-bit row word per such row, with COL
     tiles one column word per frontier vertex of the segment; it writes the
     next frontier words, visited words of changed rows and one int32 level
-    per new vertex.
+    per new vertex.  32x32 ROW tiles carry an occupancy word per tile (read
+    with the block-column index); there the step needs only the non-empty
+    row words of unvisited rows, counted from the CSR (`csr`) as the distinct
+    (row, block column) pairs.
     """
     nbr = len(rowptr_b) - 1
     wb = max(1, b // 8)
@@ -132,6 +135,15 @@ def bfs_level_bytes(rowptr_b, colind_b, levels, nrows, b, row_live, layout="row"
     live = live.reshape(nbr, b)
     depth = int(levels.max()) + 1
     row_of = np.repeat(np.arange(nbr, dtype=np.int64), np.diff(rowptr_b))
+    occ = csr is not None and b == 32 and layout == "row"
+    if occ:
+        # non-empty row words: distinct (row, block column) pairs of P
+        prow = np.repeat(np.arange(nrows, dtype=np.int32), np.diff(csr.rowptr))
+        pcol = (csr.colind // b).astype(np.int32)
+        first = np.ones(len(pcol), bool)
+        first[1:] = (pcol[1:] != pcol[:-1]) | (prow[1:] != prow[:-1])
+        prow, pcol = prow[first], pcol[first]
+        del first
     out = []
     for L in range(depth):
         unvis = (((lv == -1) | (lv > L)) & live).sum(axis=1)  # reachable unvisited rows
@@ -143,7 +155,12 @@ def bfs_level_bytes(rowptr_b, colind_b, levels, nrows, b, row_live, layout="row"
         changed = int(((lv == L + 1).any(axis=1)).sum())
         by = 4 * (nbr + 1) + 2 * wb * nbr + wb * changed + 4 * newv
         by += 4 * int(t_open.sum())
-        if layout == "col":
+        if occ:
+            unv_v = np.zeros(nrows, bool)
+            unv_v[:] = (levels == -1) | (levels > L)
+            by += 4 * int(t_open.sum())  # occupancy words
+            by += wb * int(np.count_nonzero(front_nz[pcol] & unv_v[prow]))
+        elif layout == "col":
             fcount = (lv == L).sum(axis=1)  # frontier vertices per block column
             by += wb * int(fcount[colind_b[t_need]].sum())
         else:
@@ -433,7 +450,8 @@ def run_ours(args, ws, rank, local):
     gbo.check(gbo.lib().gbo_graph_b2sr(g.h, r.ref(), c.ref(), None), "graph_b2sr")
     rowptr_b = gbo.device_to_numpy(r.value, np.int32, info.nblockrows + 1)
     colind_b = gbo.device_to_numpy(c.value, np.int32, int(info.nblocks))
-    lvl_bytes = bfs_level_bytes(rowptr_b, colind_b, levels, n, args.tile, np.diff(csr.rowptr) > 0, args.layout)
+    lvl_bytes = bfs_level_bytes(rowptr_b, colind_b, levels, n, args.tile, np.diff(csr.rowptr) > 0,
+                                args.layout, csr)
     per_level_ms = np.array(step_ms_all, np.float64).reshape(args.steps, -1)
     lvl_ms = per_level_ms.mean(axis=0)
     k = min(len(lvl_bytes), len(lvl_ms))

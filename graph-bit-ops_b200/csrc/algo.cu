@@ -320,7 +320,20 @@ __global__ void __launch_bounds__(kTPB) k_bfs_push(GView v, typename Word<B>::T*
     for (int t = it.t0 + (int)lane; t < it.t1; t += 32) {
       const int C = v.colind[t];
       WT acc = 0;
-      for_each_col<B>(xs, [&](int r) { acc = (WT)(acc | val[(size_t)t * B + r]); });
+      if constexpr (B == 32) {
+        if (v.rowmask) {  // frontier rows with a non-empty word only (bit r = row r)
+          unsigned sel = __brev((unsigned)xs) & v.rowmask[t];
+          while (sel) {
+            const int r = __ffs(sel) - 1;
+            sel &= sel - 1;
+            acc = (WT)(acc | val[(size_t)t * B + r]);
+          }
+        } else {
+          for_each_col<B>(xs, [&](int r) { acc = (WT)(acc | val[(size_t)t * B + r]); });
+        }
+      } else {
+        for_each_col<B>(xs, [&](int r) { acc = (WT)(acc | val[(size_t)t * B + r]); });
+      }
       const WT cand = (WT)(acc & ~visited[C]);
       if (cand) atomic_or_word<B>(out, C, cand);
     }

@@ -414,6 +414,7 @@ GView view_of(const gbo_graph* g) {
   v.nitems = g->nitems;
   v.splits = g->splits;
   v.nsplit = g->nsplit;
+  v.rowmask = g->rowmask;
   return v;
 }
 

@@ -16,6 +16,9 @@ struct GView {
   int nitems;
   const gbo_split* __restrict__ splits;
   int nsplit;
+  // b = 32 ROW tiles: bit r of rowmask[t] is set iff row word r of tile t is
+  // non-zero (null for other widths and layouts)
+  const unsigned* __restrict__ rowmask = nullptr;
 };
 
 GView view_of(const gbo_graph* g);

@@ -108,6 +108,7 @@ void destroy(gbo_graph* g) {
   if (g->owns_outdeg) cudaFree(g->outdeg);
   cudaFree(g->perm);
   cudaFree(g->tile_row);
+  cudaFree(g->rowmask);
   cudaFree(g->invdeg);
   cudaFree(g->items);
   cudaFree(g->splits);
@@ -227,6 +228,7 @@ extern "C" int gbo_graph_from_csr(const int* rowptr, const int* colind, int nrow
     }
   }
   if (st == GBO_OK) st = build_schedule(g, s);
+  if (st == GBO_OK) st = build_rowmask(g, s);
   if (st == GBO_OK) st = ensure_workspace(g, bmv_scratch_bytes(g), s);
   if (st == GBO_OK) st = cudaStreamSynchronize(s) == cudaSuccess ? GBO_OK : fail(GBO_ERR_CUDA, "graph build sync");
   low.release();
@@ -272,6 +274,7 @@ extern "C" int gbo_graph_wrap_b2sr(int nrows, int ncols, int tile_bits, int layo
     if (st == GBO_OK) launch_invdeg(d_outdeg, ncols, g->invdeg, s);
   }
   if (st == GBO_OK) st = build_schedule(g, s);
+  if (st == GBO_OK) st = build_rowmask(g, s);
   if (st == GBO_OK) st = ensure_workspace(g, bmv_scratch_bytes(g), s);
   if (st == GBO_OK) st = cudaStreamSynchronize(s) == cudaSuccess ? GBO_OK : fail(GBO_ERR_CUDA, "wrap sync");
   if (st != GBO_OK) {

@@ -30,6 +30,7 @@ struct gbo_graph {
   int bfs_push_thr = -1;   // push below this frontier size (-1: nrows / 64)
   int* perm = nullptr;     // GBO_FLAG_DEGREE_ORDER: new label of every input vertex
   int* tile_row = nullptr; // block row of every tile (triangle counting)
+  unsigned* rowmask = nullptr;  // b = 32 ROW: non-empty row words of every tile
   int last_run_ms = 0;     // 1: the last traversal was a multi-source BFS
   bool tc_mma = false;     // GBO_FLAG_TC_MMA: dense 32x32 mask tiles on the 1-bit MMA
   bool owns_outdeg = true;
@@ -67,6 +68,9 @@ inline int groups_per_warp(int b) { return b >= 32 ? 1 : 32 / b; }
 
 // Build items/splits for g (rowptr must be set).  Allocates g->items/splits.
 int build_schedule(gbo_graph* g, cudaStream_t stream);
+
+// Row-occupancy words of b = 32 ROW tiles -> g->rowmask (no-op otherwise).
+int build_rowmask(gbo_graph* g, cudaStream_t stream);
 
 // Ensure g->ws has at least `bytes` (contents undefined).
 int ensure_workspace(gbo_graph* g, size_t bytes, cudaStream_t stream);

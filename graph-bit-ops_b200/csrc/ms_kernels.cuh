@@ -173,15 +173,20 @@ __global__ void __launch_bounds__(kTPB) k_step(Args a) {
         nlist = 0;
         __syncwarp();
       };
+      // with occupancy words, tiles whose non-empty rows are all closed are
+      // skipped and only non-empty open rows load their word
+      const unsigned* __restrict__ rm = v.rowmask;
+      const unsigned openm = __ballot_sync(0xffffffffu, row_open);
       for (int b0 = it.t0; b0 < it.t1; b0 += 32) {
         const int t = b0 + (int)lane;
         int cb = 0;
-        uint32_t fw = 0;
+        uint32_t fw = 0, mw = ~0u;
         if (t < it.t1) {
           cb = v.colind[t];
+          if (rm) mw = rm[t];
           fw = fb[cb];
         }
-        unsigned tiles = __ballot_sync(0xffffffffu, fw != 0);
+        unsigned tiles = __ballot_sync(0xffffffffu, fw != 0 && (mw & openm) != 0u);
         // tiles with frontier columns, kT at a time: their row words load
         // together (lane r: row r); pairs go to the list at positions taken
         // with a shared-memory counter (the OR accumulation does not depend
@@ -201,7 +206,10 @@ __global__ void __launch_bounds__(kTPB) k_step(Args a) {
             const int src = jt[k] < 0 ? 0 : jt[k];
             Ck[k] = __shfl_sync(0xffffffffu, cb, src);
             const uint32_t fcol = __shfl_sync(0xffffffffu, fw, src);
-            eff[k] = (jt[k] >= 0 && row_open) ? (val[(size_t)(b0 + jt[k]) * 32 + lane] & fcol) : 0u;
+            const uint32_t mk = __shfl_sync(0xffffffffu, mw, src);
+            eff[k] = (jt[k] >= 0 && row_open && ((mk >> lane) & 1u))
+                         ? (val[(size_t)(b0 + jt[k]) * 32 + lane] & fcol)
+                         : 0u;
           }
 #pragma unroll
           for (int k = 0; k < kT; ++k) {

@@ -597,6 +597,37 @@ int build_schedule(gbo_graph* g, cudaStream_t s) {
   return GBO_OK;
 }
 
+// One warp per tile: bit r of the tile's occupancy word is set iff row word
+// r is non-zero.  A 32x32 tile spans four 32-byte sectors while R-MAT-like
+// graphs hold one or two set bits per tile, so pull kernels that read this
+// word first and load only the non-empty row words move about half the
+// bytes of a full tile read.
+__global__ void k_rowmask32(const unsigned* __restrict__ val, long long nblk,
+                            unsigned* __restrict__ mask) {
+  const unsigned lane = threadIdx.x & 31;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < nblk; t += nwarps) {
+    const unsigned m = __ballot_sync(0xffffffffu, val[t * 32 + lane] != 0u);
+    if (lane == 0) mask[t] = m;
+  }
+}
+
+int build_rowmask(gbo_graph* g, cudaStream_t s) {
+  if (g->b != 32 || g->layout != GBO_LAYOUT_ROW || g->rowmask) return GBO_OK;
+  GBO_CUDA_TRY(cudaMalloc(&g->rowmask, sizeof(unsigned) * (size_t)(g->nblk > 0 ? g->nblk : 1)));
+  g->device_bytes += 4LL * g->nblk;
+  if (g->nblk > 0) {
+    int nsm = 148;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const long long want = (g->nblk + 7) / 8;  // 8 warps per block
+    const int grid = (int)std::min<long long>(want, 8LL * nsm);
+    k_rowmask32<<<grid, 256, 0, s>>>(static_cast<const unsigned*>(g->val), g->nblk, g->rowmask);
+  }
+  GBO_CUDA_TRY(cudaGetLastError());
+  return GBO_OK;
+}
+
 int ensure_workspace(gbo_graph* g, size_t bytes, cudaStream_t s) {
   if (g->ws_bytes >= bytes) return GBO_OK;
   if (g->ws) {

@@ -32,6 +32,58 @@ __device__ __forceinline__ WT shfl_word(unsigned mask, WT v, int src, int width)
   return (WT)__shfl_sync(mask, (unsigned)v, src, width);
 }
 
+// The b = 32 form of pull_or_scan (below) for tiles with occupancy words
+// (v.rowmask): a tile is fetched only if one of the rows that still need an
+// answer has a non-empty word in it, and only those rows load their word, so
+// a tile with one or two set rows costs one or two 32-byte sectors instead
+// of four.
+__device__ __forceinline__ void pull_or_scan_rowmask32(const GView& v, int t0, int t1,
+                                                       const unsigned* __restrict__ x, bool need0,
+                                                       bool& p0, unsigned lane) {
+  const unsigned* __restrict__ val = reinterpret_cast<const unsigned*>(v.val);
+  const unsigned* __restrict__ rm = v.rowmask;
+  constexpr int U = 8;
+  // pipeline: batch i+1's x words and occupancy words and batch i+2's
+  // block-column indices are in flight while batch i's row words load
+  int c1 = (t0 + (int)lane < t1) ? v.colind[t0 + lane] : -1;
+  int c2 = (t0 + 32 + (int)lane < t1) ? v.colind[t0 + 32 + lane] : -1;
+  unsigned m1 = c1 >= 0 ? rm[t0 + lane] : 0u;
+  unsigned x1 = c1 >= 0 ? x[c1] : 0u;
+  unsigned needm = __ballot_sync(0xffffffffu, need0 && !p0);
+  for (int base = t0; base < t1 && needm; base += 32) {
+    const unsigned xs = x1, ms = m1;
+    m1 = c2 >= 0 ? rm[base + 32 + lane] : 0u;
+    x1 = c2 >= 0 ? x[c2] : 0u;
+    c2 = (base + 64 + (int)lane < t1) ? v.colind[base + 64 + lane] : -1;
+    unsigned nz = __ballot_sync(0xffffffffu, xs != 0u && (ms & needm) != 0u);
+    while (nz) {
+      int j[U];
+#pragma unroll
+      for (int q = 0; q < U; ++q) {
+        j[q] = nz ? __ffs(nz) - 1 : -1;
+        nz &= nz - 1;
+      }
+      unsigned xv[U], mv[U], a[U];
+#pragma unroll
+      for (int q = 0; q < U; ++q) {
+        xv[q] = __shfl_sync(0xffffffffu, xs, j[q] < 0 ? 0 : j[q]);
+        mv[q] = __shfl_sync(0xffffffffu, ms, j[q] < 0 ? 0 : j[q]);
+      }
+      const bool l0 = need0 && !p0;
+#pragma unroll
+      for (int q = 0; q < U; ++q) {
+        a[q] = 0u;
+        if (j[q] >= 0 && l0 && ((mv[q] >> lane) & 1u)) a[q] = val[(size_t)(base + j[q]) * 32 + lane];
+      }
+#pragma unroll
+      for (int q = 0; q < U; ++q) p0 |= (a[q] & xv[q]) != 0u;
+      needm = __ballot_sync(0xffffffffu, need0 && !p0);
+      // drop the remaining tiles that only rows answered meanwhile needed
+      nz &= __ballot_sync(0xffffffffu, (ms & needm) != 0u);
+    }
+  }
+}
+
 // Boolean pull over tiles [t0, t1) of one block row for the rows this lane
 // owns: p0 |= (row word & x[colind]) != 0 (p1 for row r+32 when b = 64).
 // need0/need1 say whether the row still needs an answer; a row stops loading
@@ -46,6 +98,12 @@ __device__ __forceinline__ void pull_or_scan(const GView& v, int t0, int t1,
                                              unsigned lane) {
   using WT = typename Word<B>::T;
   using L = Lay<B>;
+  if constexpr (B == 32) {
+    if (v.rowmask) {
+      pull_or_scan_rowmask32(v, t0, t1, reinterpret_cast<const unsigned*>(x), need0, p0, lane);
+      return;
+    }
+  }
   constexpr int W = L::W;
   const unsigned gmask = group_mask<B>(lane);
   const int r = lane % W;
@@ -124,27 +182,43 @@ __device__ __forceinline__ void fold_row_cols(const GView& v, int t0, int t1, in
       comb(acc, term(base + j));
     }
   };
+  // b = 32 tiles with occupancy words: a lane loads its row word only where
+  // it is non-empty (the others are zero and fold nothing), so a sparse
+  // tile costs the sectors of its non-empty rows.  The occupancy words run
+  // one batch ahead of the row words they predicate.
+  const unsigned* __restrict__ rm = B == 32 ? v.rowmask : nullptr;
+  auto masks = [&](int tb, unsigned (&m)[U]) {
+#pragma unroll
+    for (int k = 0; k < U; ++k) m[k] = rm ? rm[tb + k] : ~0u;
+  };
   // software pipeline: batch i+1's column indices and row words load while
   // batch i's gathers run
-  auto load = [&](int tb, unsigned (&base)[U], AW (&a0)[U], AW (&a1)[U]) {
+  auto load = [&](int tb, unsigned (&base)[U], AW (&a0)[U], AW (&a1)[U], const unsigned (&m)[U]) {
 #pragma unroll
     for (int k = 0; k < U; ++k) {
       base[k] = (unsigned)v.colind[tb + k] * (unsigned)B;  // < 2^32: ncols is an int
-      a0[k] = (AW)val[(size_t)(tb + k) * B + r] << (kBits - B);
+      a0[k] = (m[k] >> (r & 31)) & 1u ? (AW)val[(size_t)(tb + k) * B + r] << (kBits - B) : (AW)0;
       a1[k] = L::RPL == 2 ? (AW)val[(size_t)(tb + k) * B + 32 + r] << (kBits - B) : (AW)0;
     }
   };
   int t = t0;
-  unsigned base[U];
+  unsigned base[U], mk[U];
   AW a0[U], a1[U];
   bool have = t + U <= t1;
-  if (have) load(t, base, a0, a1);
+  if (have) {
+    masks(t, mk);
+    load(t, base, a0, a1, mk);
+    if (t + 2 * U <= t1) masks(t + U, mk);
+  }
   while (have) {
     const int tn = t + U;
     const bool next = tn + U <= t1;
     unsigned nbase[U];
     AW n0[U], n1[U];
-    if (next) load(tn, nbase, n0, n1);
+    if (next) {
+      load(tn, nbase, n0, n1, mk);
+      if (tn + 2 * U <= t1) masks(tn + U, mk);
+    }
     T g0[U], g1[U];
     bool h0[U], h1[U];
 #pragma unroll

@@ -113,14 +113,19 @@ __global__ void __launch_bounds__(kPprTPB) k_ppr_step(PprArgs a) {
       nl = 0;
       __syncwarp();
     };
+    const unsigned* __restrict__ rm = v.rowmask;  // occupancy words: skip empty row words
     for (int b0 = it.t0; b0 < it.t1; b0 += 32) {
       const int t = b0 + (int)lane;
       const int cb = t < it.t1 ? v.colind[t] : 0;
+      const unsigned mw = t < it.t1 && rm ? rm[t] : ~0u;
       const int ntile = min(32, it.t1 - b0);
       for (int g0 = 0; g0 < ntile; g0 += kU) {
         uint32_t wr[kU];
 #pragma unroll
-        for (int k = 0; k < kU; ++k) wr[k] = g0 + k < ntile ? val[(size_t)(b0 + g0 + k) * 32 + lane] : 0u;
+        for (int k = 0; k < kU; ++k) {
+          const unsigned mk = __shfl_sync(0xffffffffu, mw, (g0 + k) & 31);
+          wr[k] = g0 + k < ntile && ((mk >> lane) & 1u) ? val[(size_t)(b0 + g0 + k) * 32 + lane] : 0u;
+        }
 #pragma unroll
         for (int k = 0; k < kU; ++k) {
           const int cnt = __popc(wr[k]);
