@@ -49,10 +49,6 @@ __device__ __forceinline__ size_t level_index(const Args& a, long long i, int s)
   return ((size_t)(s / g) * a.v.nrows + i) * g + s % g;
 }
 
-__device__ __forceinline__ unsigned nth_set_bit(unsigned m, int nth) {
-  return __fns(m, 0, nth);  // position of the nth (1-based) set bit from bit 0
-}
-
 // Bits of word w that are real sources (k need not be a multiple of 32).
 __device__ __forceinline__ unsigned src_mask(int w, int k) {
   const int lo = w * 32;
@@ -114,17 +110,26 @@ __device__ __forceinline__ void block_row_epilogue(const Args& a, int R, int lvl
   }
 }
 
+// Inclusive warp prefix sum.
+__device__ __forceinline__ int warp_incl_sum(int x, unsigned lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if ((int)lane >= o) x += y;
+  }
+  return x;
+}
+
 // Bit pairs (tile row r, frontier vertex j) queued per warp before their
 // frontier rows are gathered: S pairs per round, U rounds in flight.
 constexpr int kList = 192;
 
 template <int KW>
-__global__ void __launch_bounds__(kTPB) k_step(Args a) {
+__global__ void __launch_bounds__(kTPB, 4) k_step(Args a) {
   constexpr int S = 32 / KW;
-  constexpr int U = S >= 8 ? 1 : 8 / S;
+  constexpr int U = S >= 64 ? 1 : (64 / S > 8 ? 8 : 64 / S);  // gathers in flight: S*U pairs
   __shared__ uint32_t acc_sh[kWarps][32 * KW];
   __shared__ int2 list_sh[kWarps][kList];
-  __shared__ int nl_sh[kWarps];  // pairs appended to the list by the current tile
   volatile int* c = a.ctl;
   if (c[1]) return;  // done
   const int lvl = c[0];
@@ -143,7 +148,6 @@ __global__ void __launch_bounds__(kTPB) k_step(Args a) {
     const uint32_t vrow = a.vfull[it.row];
     if (vrow != 0xffffffffu) {
       for (int q = lane; q < 32 * KW; q += 32) acc[q] = 0u;
-      if (lane == 0) nl_sh[wib] = 0;
       __syncwarp();
       const bool row_open = !((vrow >> (31 - lane)) & 1u);  // lane r: row r still open
       const uint32_t* __restrict__ val = reinterpret_cast<const uint32_t*>(v.val);
@@ -173,8 +177,17 @@ __global__ void __launch_bounds__(kTPB) k_step(Args a) {
         nlist = 0;
         __syncwarp();
       };
-      // with occupancy words, tiles whose non-empty rows are all closed are
-      // skipped and only non-empty open rows load their word
+      // Per batch of 32 tiles (lane j: tile j) the row words worth a load
+      // are the pairs (tile j, row r) with frontier columns at j and row r
+      // open and non-empty in tile j (all open rows without occupancy
+      // words).  They are dealt out to the lanes, 32 per round: lane p takes
+      // pair p (its tile by a binary search over the lanes' prefix counts,
+      // its row as the k-th candidate bit), loads the word and ANDs it with
+      // the tile's frontier columns.  Each set bit (row r, frontier vertex)
+      // then goes to the list, at most kPerPass per lane per pass, at
+      // positions from a warp prefix sum (the OR accumulation does not
+      // depend on the order).
+      constexpr int kPerPass = kList / 32;
       const unsigned* __restrict__ rm = v.rowmask;
       const unsigned openm = __ballot_sync(0xffffffffu, row_open);
       for (int b0 = it.t0; b0 < it.t1; b0 += 32) {
@@ -186,69 +199,41 @@ __global__ void __launch_bounds__(kTPB) k_step(Args a) {
           if (rm) mw = rm[t];
           fw = fb[cb];
         }
-        unsigned tiles = __ballot_sync(0xffffffffu, fw != 0 && (mw & openm) != 0u);
-        // tiles with frontier columns, kT at a time: their row words load
-        // together (lane r: row r); pairs go to the list at positions taken
-        // with a shared-memory counter (the OR accumulation does not depend
-        // on the order)
-        constexpr int kT = 8;
-        while (tiles) {
-          int jt[kT];
+        const unsigned cand = fw ? (mw & openm) : 0u;
+        const int cnt = __popc(cand);
+        const int incl = warp_incl_sum(cnt, lane);
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        const int excl = incl - cnt;
+        for (int pb = 0; pb < total; pb += 32) {
+          const int p = pb + (int)lane;
+          int j = 0;
 #pragma unroll
-          for (int k = 0; k < kT; ++k) {
-            jt[k] = tiles ? __ffs(tiles) - 1 : -1;
-            if (tiles) tiles &= tiles - 1;
+          for (int st = 16; st > 0; st >>= 1) {
+            const int q = __shfl_sync(0xffffffffu, incl, j + st - 1);
+            if (q <= p) j += st;
           }
-          uint32_t eff[kT];
-          int Ck[kT];
-#pragma unroll
-          for (int k = 0; k < kT; ++k) {
-            const int src = jt[k] < 0 ? 0 : jt[k];
-            Ck[k] = __shfl_sync(0xffffffffu, cb, src);
-            const uint32_t fcol = __shfl_sync(0xffffffffu, fw, src);
-            const uint32_t mk = __shfl_sync(0xffffffffu, mw, src);
-            eff[k] = (jt[k] >= 0 && row_open && ((mk >> lane) & 1u))
-                         ? (val[(size_t)(b0 + jt[k]) * 32 + lane] & fcol)
-                         : 0u;
+          const int ej = __shfl_sync(0xffffffffu, excl, j);
+          const unsigned cj = __shfl_sync(0xffffffffu, cand, j);
+          const uint32_t fj = __shfl_sync(0xffffffffu, fw, j);
+          const int vbase = __shfl_sync(0xffffffffu, cb, j) * 32;
+          int r = 0;
+          uint32_t eff = 0u;
+          if (p < total) {
+            r = (int)__fns(cj, 0, p - ej + 1);
+            eff = val[(size_t)(b0 + j) * 32 + r] & fj;
           }
-#pragma unroll
-          for (int k = 0; k < kT; ++k) {
-            const int cnt_l = __popc(eff[k]);
-            const int total = (int)__reduce_add_sync(0xffffffffu, (unsigned)cnt_l);
-            if (total == 0) continue;
-            if (nlist + total > kList) flush();
-            if (total > kList) {
-              // dense tile: OR its rows straight from the row words
-              unsigned rows = __ballot_sync(0xffffffffu, eff[k] != 0);
-              while (rows) {
-                const int r = __ffs(rows) - 1;
-                rows &= rows - 1;
-                unsigned bits = __shfl_sync(0xffffffffu, eff[k], r);
-                uint32_t racc = 0;
-                while (bits) {
-                  const unsigned pos = nth_set_bit(bits, s + 1);
-                  uint32_t f = 0;
-                  if (pos != 0xffffffffu) f = F[((size_t)Ck[k] * 32 + (31 - (int)pos)) * KW + w];
-#pragma unroll
-                  for (int o = KW; o < 32; o <<= 1) f |= __shfl_xor_sync(0xffffffffu, f, o);
-                  racc |= f;
-                  const unsigned last = nth_set_bit(bits, S);
-                  bits = last == 0xffffffffu ? 0u : (bits & ~(0xffffffffu >> (31 - last)));
-                }
-                if (s == 0) acc[r * KW + w] |= racc;
-              }
-              continue;
+          while (__any_sync(0xffffffffu, eff != 0u)) {
+            const int c = min(__popc(eff), kPerPass);
+            const int ic = warp_incl_sum(c, lane);
+            const int tc = __shfl_sync(0xffffffffu, ic, 31);
+            if (nlist + tc > kList) flush();
+            int pos = nlist + ic - c;
+            for (int q = 0; q < c; ++q) {
+              const int col = __clz(eff);
+              eff &= ~(0x80000000u >> col);
+              list[pos++] = make_int2(r, vbase + col);
             }
-            int pos = cnt_l ? nlist + atomicAdd(&nl_sh[wib], cnt_l) : 0;
-            uint32_t m = eff[k];
-            while (m) {
-              const int col = __clz(m);
-              m &= ~(0x80000000u >> col);
-              list[pos++] = make_int2((int)lane, Ck[k] * 32 + col);
-            }
-            nlist += total;
-            __syncwarp();
-            if (lane == 0) nl_sh[wib] = 0;
+            nlist += tc;
             __syncwarp();
           }
         }

@@ -33,55 +33,72 @@ __device__ __forceinline__ WT shfl_word(unsigned mask, WT v, int src, int width)
 }
 
 // The b = 32 form of pull_or_scan (below) for tiles with occupancy words
-// (v.rowmask): a tile is fetched only if one of the rows that still need an
-// answer has a non-empty word in it, and only those rows load their word, so
-// a tile with one or two set rows costs one or two 32-byte sectors instead
-// of four.
+// (v.rowmask).  Per batch of 32 tiles (lane j: tile j) the words that can
+// answer a row are the pairs (tile j, row r) with a non-empty frontier
+// segment at j and r both still open and non-empty in tile j: one or two per
+// tile on sparse graphs.  Those pairs are dealt out to the lanes (lane p
+// takes pair p of the batch: its tile by a binary search over the lanes'
+// prefix counts, its row as the k-th set bit of the tile's candidate rows),
+// so a batch costs a round or two of 32 independent word loads instead of a
+// pass over every tile with one or two lanes active.  A word that hits the
+// tile's frontier segment answers its row; the answers are OR-ed across the
+// warp after each pair of rounds, and rows answered meanwhile drop their
+// remaining pairs.
 __device__ __forceinline__ void pull_or_scan_rowmask32(const GView& v, int t0, int t1,
                                                        const unsigned* __restrict__ x, bool need0,
                                                        bool& p0, unsigned lane) {
   const unsigned* __restrict__ val = reinterpret_cast<const unsigned*>(v.val);
   const unsigned* __restrict__ rm = v.rowmask;
-  constexpr int U = 8;
   // pipeline: batch i+1's x words and occupancy words and batch i+2's
   // block-column indices are in flight while batch i's row words load
   int c1 = (t0 + (int)lane < t1) ? v.colind[t0 + lane] : -1;
   int c2 = (t0 + 32 + (int)lane < t1) ? v.colind[t0 + 32 + lane] : -1;
   unsigned m1 = c1 >= 0 ? rm[t0 + lane] : 0u;
   unsigned x1 = c1 >= 0 ? x[c1] : 0u;
-  unsigned needm = __ballot_sync(0xffffffffu, need0 && !p0);
+  unsigned needm = __ballot_sync(0xffffffffu, need0 && !p0);  // bit r: row r open
   for (int base = t0; base < t1 && needm; base += 32) {
     const unsigned xs = x1, ms = m1;
     m1 = c2 >= 0 ? rm[base + 32 + lane] : 0u;
     x1 = c2 >= 0 ? x[c2] : 0u;
     c2 = (base + 64 + (int)lane < t1) ? v.colind[base + 64 + lane] : -1;
-    unsigned nz = __ballot_sync(0xffffffffu, xs != 0u && (ms & needm) != 0u);
-    while (nz) {
-      int j[U];
+    const unsigned cand = xs ? (ms & needm) : 0u;  // this lane's tile: rows worth a load
+    const int cnt = __popc(cand);
+    int incl = cnt;
 #pragma unroll
-      for (int q = 0; q < U; ++q) {
-        j[q] = nz ? __ffs(nz) - 1 : -1;
-        nz &= nz - 1;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if ((int)lane >= o) incl += y;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    const int excl = incl - cnt;
+    for (int pb = 0; pb < total; pb += 64) {
+      unsigned hit = 0u;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int p = pb + h * 32 + (int)lane;
+        // tile of pair p: the number of lanes whose inclusive count is <= p
+        int j = 0;
+#pragma unroll
+        for (int st = 16; st > 0; st >>= 1) {
+          const int q = __shfl_sync(0xffffffffu, incl, j + st - 1);
+          if (q <= p) j += st;
+        }
+        const int ej = __shfl_sync(0xffffffffu, excl, j);
+        const unsigned cj = __shfl_sync(0xffffffffu, cand, j);
+        const unsigned xj = __shfl_sync(0xffffffffu, xs, j);
+        if (p < total) {
+          const int r = (int)__fns(cj, 0, p - ej + 1);
+          if ((needm >> r) & 1u) {
+            if (val[(size_t)(base + j) * 32 + r] & xj) hit |= 1u << r;
+          }
+        }
       }
-      unsigned xv[U], mv[U], a[U];
-#pragma unroll
-      for (int q = 0; q < U; ++q) {
-        xv[q] = __shfl_sync(0xffffffffu, xs, j[q] < 0 ? 0 : j[q]);
-        mv[q] = __shfl_sync(0xffffffffu, ms, j[q] < 0 ? 0 : j[q]);
-      }
-      const bool l0 = need0 && !p0;
-#pragma unroll
-      for (int q = 0; q < U; ++q) {
-        a[q] = 0u;
-        if (j[q] >= 0 && l0 && ((mv[q] >> lane) & 1u)) a[q] = val[(size_t)(base + j[q]) * 32 + lane];
-      }
-#pragma unroll
-      for (int q = 0; q < U; ++q) p0 |= (a[q] & xv[q]) != 0u;
-      needm = __ballot_sync(0xffffffffu, need0 && !p0);
-      // drop the remaining tiles that only rows answered meanwhile needed
-      nz &= __ballot_sync(0xffffffffu, (ms & needm) != 0u);
+      const unsigned found = __reduce_or_sync(0xffffffffu, hit);
+      needm &= ~found;
+      if (!needm) break;
     }
   }
+  p0 = p0 || (need0 && !((needm >> lane) & 1u));
 }
 
 // Boolean pull over tiles [t0, t1) of one block row for the rows this lane
