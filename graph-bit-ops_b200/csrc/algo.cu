@@ -317,23 +317,38 @@ __global__ void __launch_bounds__(kTPB) k_bfs_push(GView v, typename Word<B>::T*
     const gbo_item it = v.items[item];
     const WT xs = x[it.row];
     if (!xs) continue;
-    for (int t = it.t0 + (int)lane; t < it.t1; t += 32) {
-      const int C = v.colind[t];
-      WT acc = 0;
-      if constexpr (B == 32) {
-        if (v.rowmask) {  // frontier rows with a non-empty word only (bit r = row r)
-          unsigned sel = __brev((unsigned)xs) & v.rowmask[t];
+    if constexpr (B == 32) {
+      if (v.rowword) {
+        // frontier rows with a non-empty word only (bit r = row r), read from
+        // the packed row words; batches of 32 tiles give each tile's offset
+        long long wb = v.item_wbase[item];
+        const unsigned fr = __brev((unsigned)xs);
+        for (int b0 = it.t0; b0 < it.t1; b0 += 32) {
+          const int t = b0 + (int)lane;
+          const unsigned m = t < it.t1 ? v.rowmask[t] : 0u;
+          const int mc = __popc(m);
+          const int mi = warp_incl_sum(mc, lane);
+          const long long off = wb + (mi - mc);
+          wb += __shfl_sync(0xffffffffu, mi, 31);
+          unsigned sel = fr & m;
+          if (!sel) continue;
+          WT acc = 0;
           while (sel) {
             const int r = __ffs(sel) - 1;
             sel &= sel - 1;
-            acc = (WT)(acc | val[(size_t)t * B + r]);
+            acc = (WT)(acc | v.rowword[rowword_index(off, m, r)]);
           }
-        } else {
-          for_each_col<B>(xs, [&](int r) { acc = (WT)(acc | val[(size_t)t * B + r]); });
+          const int C = v.colind[t];
+          const WT cand = (WT)(acc & ~visited[C]);
+          if (cand) atomic_or_word<B>(out, C, cand);
         }
-      } else {
-        for_each_col<B>(xs, [&](int r) { acc = (WT)(acc | val[(size_t)t * B + r]); });
+        continue;
       }
+    }
+    for (int t = it.t0 + (int)lane; t < it.t1; t += 32) {
+      const int C = v.colind[t];
+      WT acc = 0;
+      for_each_col<B>(xs, [&](int r) { acc = (WT)(acc | val[(size_t)t * B + r]); });
       const WT cand = (WT)(acc & ~visited[C]);
       if (cand) atomic_or_word<B>(out, C, cand);
     }
@@ -649,7 +664,7 @@ __global__ void __launch_bounds__(kTPB) k_pr_step(GView v, float* __restrict__ p
       const int r = lane % L::W;
       const gbo_item it = v.items[item];
       double a0 = 0.0, a1 = 0.0;
-      fold_row_cols<B, 4>(v, it.t0, it.t1, r, [&](long long j) { return (double)xg[j]; },
+      fold_row_cols<B, 4>(v, it.t0, it.t1, v.item_wbase ? v.item_wbase[item] : 0ll, r, [&](long long j) { return (double)xg[j]; },
                           [](double& a, double b) { a += b; }, a0, a1);
       if (it.slot >= 0) {
         scratch[(size_t)it.slot * B + r] = a0;
@@ -825,7 +840,7 @@ __global__ void __launch_bounds__(kTPB) k_cc_mngf(GView v, const int* __restrict
     const int r = lane % L::W;
     const gbo_item it = v.items[item];
     int a0 = kINF, a1 = kINF;
-    fold_row_cols<B, 4>(v, it.t0, it.t1, r, [&](long long j) { return gf[j]; },
+    fold_row_cols<B, 4>(v, it.t0, it.t1, v.item_wbase ? v.item_wbase[item] : 0ll, r, [&](long long j) { return gf[j]; },
                         [](int& a, int b) { a = min(a, b); }, a0, a1);
     if (it.slot >= 0) {
       scratch[(size_t)it.slot * B + r] = a0;

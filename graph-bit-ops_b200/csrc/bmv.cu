@@ -263,11 +263,11 @@ __global__ void __launch_bounds__(kTPB) k_semiring(GView v, const typename SRT<S
   A acc0 = sr_identity<SR>(), acc1 = sr_identity<SR>();
   auto comb = [](A& a, A b) { sr_combine<SR>(a, b); };
   if (SR == SR_FLOAT && p.degptr)
-    fold_row_cols<B, 4>(v, it.t0, it.t1, r,
+    fold_row_cols<B, 4>(v, it.t0, it.t1, v.item_wbase ? v.item_wbase[item] : 0ll, r,
                         [&](long long j) { return (A)float_term_deg((const float*)x, p.degptr, j); },
                         comb, acc0, acc1);
   else
-    fold_row_cols<B, 4>(v, it.t0, it.t1, r, [&](long long j) { return sr_term<SR>(x, p.scale, j); },
+    fold_row_cols<B, 4>(v, it.t0, it.t1, v.item_wbase ? v.item_wbase[item] : 0ll, r, [&](long long j) { return sr_term<SR>(x, p.scale, j); },
                         comb, acc0, acc1);
   if (it.slot >= 0) {
     scratch[(size_t)it.slot * B + r] = acc0;
@@ -415,6 +415,8 @@ GView view_of(const gbo_graph* g) {
   v.splits = g->splits;
   v.nsplit = g->nsplit;
   v.rowmask = g->rowmask;
+  v.rowword = g->rowword;
+  v.item_wbase = g->item_wbase;
   return v;
 }
 

@@ -19,7 +19,17 @@ struct GView {
   // b = 32 ROW tiles: bit r of rowmask[t] is set iff row word r of tile t is
   // non-zero (null for other widths and layouts)
   const unsigned* __restrict__ rowmask = nullptr;
+  // with rowmask: the non-empty row words packed in tile order (row order
+  // inside a tile) and the index of every work item's first word
+  const unsigned* __restrict__ rowword = nullptr;
+  const long long* __restrict__ item_wbase = nullptr;
 };
+
+// Index in rowword of row r's word of a tile with occupancy word m whose
+// first word is at `off` (bit r of m must be set).
+__device__ __forceinline__ long long rowword_index(long long off, unsigned m, int r) {
+  return off + __popc(m & ((1u << r) - 1u));
+}
 
 GView view_of(const gbo_graph* g);
 

@@ -109,6 +109,8 @@ void destroy(gbo_graph* g) {
   cudaFree(g->perm);
   cudaFree(g->tile_row);
   cudaFree(g->rowmask);
+  cudaFree(g->rowword);
+  cudaFree(g->item_wbase);
   cudaFree(g->invdeg);
   cudaFree(g->items);
   cudaFree(g->splits);
@@ -229,6 +231,7 @@ extern "C" int gbo_graph_from_csr(const int* rowptr, const int* colind, int nrow
   }
   if (st == GBO_OK) st = build_schedule(g, s);
   if (st == GBO_OK) st = build_rowmask(g, s);
+  if (st == GBO_OK) st = build_rowwords(g, s);
   if (st == GBO_OK) st = ensure_workspace(g, bmv_scratch_bytes(g), s);
   if (st == GBO_OK) st = cudaStreamSynchronize(s) == cudaSuccess ? GBO_OK : fail(GBO_ERR_CUDA, "graph build sync");
   low.release();
@@ -275,6 +278,7 @@ extern "C" int gbo_graph_wrap_b2sr(int nrows, int ncols, int tile_bits, int layo
   }
   if (st == GBO_OK) st = build_schedule(g, s);
   if (st == GBO_OK) st = build_rowmask(g, s);
+  if (st == GBO_OK) st = build_rowwords(g, s);
   if (st == GBO_OK) st = ensure_workspace(g, bmv_scratch_bytes(g), s);
   if (st == GBO_OK) st = cudaStreamSynchronize(s) == cudaSuccess ? GBO_OK : fail(GBO_ERR_CUDA, "wrap sync");
   if (st != GBO_OK) {

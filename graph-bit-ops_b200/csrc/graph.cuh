@@ -31,6 +31,9 @@ struct gbo_graph {
   int* perm = nullptr;     // GBO_FLAG_DEGREE_ORDER: new label of every input vertex
   int* tile_row = nullptr; // block row of every tile (triangle counting)
   unsigned* rowmask = nullptr;  // b = 32 ROW: non-empty row words of every tile
+  unsigned* rowword = nullptr;  // b = 32 ROW: the non-empty row words, packed in tile order
+  long long* item_wbase = nullptr;  // index in rowword of every work item's first word
+  long long nrowword = 0;
   int last_run_ms = 0;     // 1: the last traversal was a multi-source BFS
   bool tc_mma = false;     // GBO_FLAG_TC_MMA: dense 32x32 mask tiles on the 1-bit MMA
   bool owns_outdeg = true;
@@ -71,6 +74,9 @@ int build_schedule(gbo_graph* g, cudaStream_t stream);
 
 // Row-occupancy words of b = 32 ROW tiles -> g->rowmask (no-op otherwise).
 int build_rowmask(gbo_graph* g, cudaStream_t stream);
+// Packed non-empty row words -> g->rowword, g->item_wbase (needs rowmask and
+// the schedule; no-op without them).
+int build_rowwords(gbo_graph* g, cudaStream_t stream);
 
 // Ensure g->ws has at least `bytes` (contents undefined).
 int ensure_workspace(gbo_graph* g, size_t bytes, cudaStream_t stream);

@@ -110,16 +110,6 @@ __device__ __forceinline__ void block_row_epilogue(const Args& a, int R, int lvl
   }
 }
 
-// Inclusive warp prefix sum.
-__device__ __forceinline__ int warp_incl_sum(int x, unsigned lane) {
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, x, o);
-    if ((int)lane >= o) x += y;
-  }
-  return x;
-}
-
 // Bit pairs (tile row r, frontier vertex j) queued per warp before their
 // frontier rows are gathered: S pairs per round, U rounds in flight.
 constexpr int kList = 192;
@@ -193,7 +183,7 @@ __global__ void __launch_bounds__(kTPB, 4) k_step(Args a) {
       for (int b0 = it.t0; b0 < it.t1; b0 += 32) {
         const int t = b0 + (int)lane;
         int cb = 0;
-        uint32_t fw = 0, mw = ~0u;
+        uint32_t fw = 0, mw = rm ? 0u : ~0u;
         if (t < it.t1) {
           cb = v.colind[t];
           if (rm) mw = rm[t];
@@ -201,8 +191,9 @@ __global__ void __launch_bounds__(kTPB, 4) k_step(Args a) {
         }
         const unsigned cand = fw ? (mw & openm) : 0u;
         const int cnt = __popc(cand);
+        const int total = (int)__reduce_add_sync(0xffffffffu, (unsigned)cnt);
+        if (total == 0) continue;
         const int incl = warp_incl_sum(cnt, lane);
-        const int total = __shfl_sync(0xffffffffu, incl, 31);
         const int excl = incl - cnt;
         for (int pb = 0; pb < total; pb += 32) {
           const int p = pb + (int)lane;

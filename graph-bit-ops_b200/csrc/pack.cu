@@ -230,8 +230,9 @@ __global__ void k_scan_sums(long long* __restrict__ sums, long long nb, long lon
   if (threadIdx.x == 0) *total = carry;
 }
 
+template <typename OutT>
 __global__ void k_scan_apply(const int* __restrict__ in, long long n,
-                             const long long* __restrict__ sums, int* __restrict__ out,
+                             const long long* __restrict__ sums, OutT* __restrict__ out,
                              const long long* __restrict__ total) {
   __shared__ long long sh[32];
   long long i = (long long)blockIdx.x * kScanTPB + threadIdx.x;
@@ -254,8 +255,13 @@ __global__ void k_scan_apply(const int* __restrict__ in, long long n,
   __syncthreads();
   long long warp_prefix = (threadIdx.x >> 5) ? sh[(threadIdx.x >> 5) - 1] : 0;
   long long excl = x - v + warp_prefix + sums[blockIdx.x];
-  if (i < n) out[i] = (int)(excl > 2147483647LL ? 2147483647LL : excl);
-  if (i == 0) out[n] = (int)(*total > 2147483647LL ? 2147483647LL : *total);
+  if (sizeof(OutT) == 8) {
+    if (i < n) out[i] = (OutT)excl;
+    if (i == 0) out[n] = (OutT)*total;
+  } else {
+    if (i < n) out[i] = (OutT)(excl > 2147483647LL ? 2147483647LL : excl);
+    if (i == 0) out[n] = (OutT)(*total > 2147483647LL ? 2147483647LL : *total);
+  }
 }
 
 // ------------------------------------------------------- vector packing
@@ -403,19 +409,26 @@ struct ScanScratch {
 
 }  // namespace
 
-int exclusive_scan_i32(const int* d_in, int* d_out, long long n, long long* d_total,
-                       cudaStream_t s) {
+namespace {
+template <typename OutT>
+int exclusive_scan(const int* d_in, OutT* d_out, long long n, long long* d_total, cudaStream_t s) {
   long long nb = (n + kScanTPB - 1) / kScanTPB;
   if (nb < 1) nb = 1;
   long long* sums = nullptr;
   GBO_CUDA_TRY(cudaMallocAsync(&sums, sizeof(long long) * nb, s));
   k_scan_block_sums<<<(unsigned)nb, kScanTPB, 0, s>>>(d_in, n, sums);
   k_scan_sums<<<1, kScanTPB, 0, s>>>(sums, nb, d_total);
-  k_scan_apply<<<(unsigned)nb, kScanTPB, 0, s>>>(d_in, n, sums, d_out, d_total);
+  k_scan_apply<OutT><<<(unsigned)nb, kScanTPB, 0, s>>>(d_in, n, sums, d_out, d_total);
   cudaError_t e = cudaGetLastError();
   cudaFreeAsync(sums, s);
   if (e != cudaSuccess) return fail_cuda(e, "scan kernels");
   return GBO_OK;
+}
+}  // namespace
+
+int exclusive_scan_i32(const int* d_in, int* d_out, long long n, long long* d_total,
+                       cudaStream_t s) {
+  return exclusive_scan<int>(d_in, d_out, n, d_total, s);
 }
 
 // nnzb per block row: counts -> bsr_rowptr (device) and total (host).
@@ -610,6 +623,88 @@ __global__ void k_rowmask32(const unsigned* __restrict__ val, long long nblk,
     const unsigned m = __ballot_sync(0xffffffffu, val[t * 32 + lane] != 0u);
     if (lane == 0) mask[t] = m;
   }
+}
+
+// Non-empty row words per work item (items cover the tiles in order).
+__global__ void k_item_words(const gbo_item* __restrict__ items, int nitems,
+                             const unsigned* __restrict__ mask, int* __restrict__ cnt) {
+  const unsigned lane = threadIdx.x & 31;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nitems; i += nwarps) {
+    const gbo_item it = items[i];
+    int c = 0;
+    for (int t = it.t0 + (int)lane; t < it.t1; t += 32) c += __popc(mask[t]);
+    c = (int)__reduce_add_sync(0xffffffffu, (unsigned)c);
+    if (lane == 0) cnt[i] = c;
+  }
+}
+
+// Copy the non-empty row words of every tile, in tile order and row order
+// inside a tile, to `out`; item i's words start at wbase[i].
+__global__ void k_pack_rowwords(const gbo_item* __restrict__ items, int nitems,
+                                const unsigned* __restrict__ val, const unsigned* __restrict__ mask,
+                                const long long* __restrict__ wbase, unsigned* __restrict__ out) {
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nitems; i += nwarps) {
+    const gbo_item it = items[i];
+    long long base = wbase[i];
+    for (int b0 = it.t0; b0 < it.t1; b0 += 32) {
+      const int t = b0 + (int)lane;
+      const unsigned m = t < it.t1 ? mask[t] : 0u;
+      const int c = __popc(m);
+      int incl = c;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if ((int)lane >= o) incl += y;
+      }
+      const int excl = incl - c;
+      const int ntile = min(32, it.t1 - b0);
+      for (int k0 = 0; k0 < ntile; k0 += 8) {  // eight tiles' words in flight
+        unsigned w[8], mk[8];
+        int ok[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          mk[u] = __shfl_sync(0xffffffffu, m, (k0 + u) & 31);
+          ok[u] = __shfl_sync(0xffffffffu, excl, (k0 + u) & 31);
+          if (k0 + u >= ntile) mk[u] = 0u;
+          w[u] = (mk[u] >> lane) & 1u ? val[(size_t)(b0 + k0 + u) * 32 + lane] : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+          if ((mk[u] >> lane) & 1u) out[base + ok[u] + __popc(mk[u] & below)] = w[u];
+      }
+      base += __shfl_sync(0xffffffffu, incl, 31);
+    }
+  }
+}
+
+int build_rowwords(gbo_graph* g, cudaStream_t s) {
+  if (!g->rowmask || g->rowword || g->nitems <= 0) return GBO_OK;
+  int* cnt = nullptr;
+  long long* tot = nullptr;
+  GBO_CUDA_TRY(cudaMallocAsync(&cnt, sizeof(int) * (size_t)g->nitems, s));
+  GBO_CUDA_TRY(cudaMallocAsync(&tot, sizeof(long long), s));
+  GBO_CUDA_TRY(cudaMalloc(&g->item_wbase, sizeof(long long) * ((size_t)g->nitems + 1)));
+  g->device_bytes += 8LL * (g->nitems + 1);
+  int nsm = 148, dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = (int)std::min<long long>(((long long)g->nitems + 7) / 8, 8LL * nsm);
+  k_item_words<<<grid, 256, 0, s>>>(g->items, g->nitems, g->rowmask, cnt);
+  GBO_TRY(exclusive_scan<long long>(cnt, g->item_wbase, g->nitems, tot, s));
+  long long nw = 0;
+  GBO_CUDA_TRY(cudaMemcpyAsync(&nw, tot, sizeof(nw), cudaMemcpyDeviceToHost, s));
+  GBO_CUDA_TRY(cudaStreamSynchronize(s));
+  cudaFreeAsync(cnt, s);
+  cudaFreeAsync(tot, s);
+  GBO_CUDA_TRY(cudaMalloc(&g->rowword, sizeof(unsigned) * (size_t)(nw > 0 ? nw : 1)));
+  g->nrowword = nw;
+  g->device_bytes += 4LL * nw;
+  k_pack_rowwords<<<grid, 256, 0, s>>>(g->items, g->nitems, static_cast<const unsigned*>(g->val),
+                                       g->rowmask, g->item_wbase, g->rowword);
+  GBO_CUDA_TRY(cudaGetLastError());
+  return GBO_OK;
 }
 
 int build_rowmask(gbo_graph* g, cudaStream_t s) {

@@ -32,6 +32,16 @@ __device__ __forceinline__ WT shfl_word(unsigned mask, WT v, int src, int width)
   return (WT)__shfl_sync(mask, (unsigned)v, src, width);
 }
 
+// Inclusive prefix sum over the lanes of a warp.
+__device__ __forceinline__ int warp_incl_sum(int x, unsigned lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if ((int)lane >= o) x += y;
+  }
+  return x;
+}
+
 // The b = 32 form of pull_or_scan (below) for tiles with occupancy words
 // (v.rowmask).  Per batch of 32 tiles (lane j: tile j) the words that can
 // answer a row are the pairs (tile j, row r) with a non-empty frontier
@@ -39,57 +49,73 @@ __device__ __forceinline__ WT shfl_word(unsigned mask, WT v, int src, int width)
 // tile on sparse graphs.  Those pairs are dealt out to the lanes (lane p
 // takes pair p of the batch: its tile by a binary search over the lanes'
 // prefix counts, its row as the k-th set bit of the tile's candidate rows),
-// so a batch costs a round or two of 32 independent word loads instead of a
-// pass over every tile with one or two lanes active.  A word that hits the
-// tile's frontier segment answers its row; the answers are OR-ed across the
-// warp after each pair of rounds, and rows answered meanwhile drop their
-// remaining pairs.
+// so a batch costs a round of 32 independent word loads instead of a pass
+// over every tile with one or two lanes active.  A word that hits the tile's
+// frontier segment answers its row; the answers are OR-ed across the warp
+// after each round, and rows answered meanwhile drop their remaining pairs.
+// NB batches are dealt side by side so that their word loads are in flight
+// together.
 __device__ __forceinline__ void pull_or_scan_rowmask32(const GView& v, int t0, int t1,
                                                        const unsigned* __restrict__ x, bool need0,
                                                        bool& p0, unsigned lane) {
+  constexpr int NB = 2;          // batches per step
+  constexpr int SPAN = 32 * NB;  // tiles per step
   const unsigned* __restrict__ val = reinterpret_cast<const unsigned*>(v.val);
   const unsigned* __restrict__ rm = v.rowmask;
-  // pipeline: batch i+1's x words and occupancy words and batch i+2's
-  // block-column indices are in flight while batch i's row words load
-  int c1 = (t0 + (int)lane < t1) ? v.colind[t0 + lane] : -1;
-  int c2 = (t0 + 32 + (int)lane < t1) ? v.colind[t0 + 32 + lane] : -1;
-  unsigned m1 = c1 >= 0 ? rm[t0 + lane] : 0u;
-  unsigned x1 = c1 >= 0 ? x[c1] : 0u;
-  unsigned needm = __ballot_sync(0xffffffffu, need0 && !p0);  // bit r: row r open
-  for (int base = t0; base < t1 && needm; base += 32) {
-    const unsigned xs = x1, ms = m1;
-    m1 = c2 >= 0 ? rm[base + 32 + lane] : 0u;
-    x1 = c2 >= 0 ? x[c2] : 0u;
-    c2 = (base + 64 + (int)lane < t1) ? v.colind[base + 64 + lane] : -1;
-    const unsigned cand = xs ? (ms & needm) : 0u;  // this lane's tile: rows worth a load
-    const int cnt = __popc(cand);
-    int incl = cnt;
+  // pipeline: step i+1's x words and occupancy words and step i+2's
+  // block-column indices are in flight while step i's row words load
+  int c2[NB];
+  unsigned m1[NB], x1[NB];
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, incl, o);
-      if ((int)lane >= o) incl += y;
+  for (int q = 0; q < NB; ++q) {
+    const int t = t0 + q * 32 + (int)lane;
+    const int c1 = t < t1 ? v.colind[t] : -1;
+    c2[q] = t + SPAN < t1 ? v.colind[t + SPAN] : -1;
+    m1[q] = c1 >= 0 ? rm[t] : 0u;
+    x1[q] = c1 >= 0 ? x[c1] : 0u;
+  }
+  unsigned needm = __ballot_sync(0xffffffffu, need0 && !p0);  // bit r: row r open
+  for (int base = t0; base < t1 && needm; base += SPAN) {
+    unsigned xs[NB], cand[NB];
+    int incl[NB], excl[NB], total[NB];
+    int most = 0;
+#pragma unroll
+    for (int q = 0; q < NB; ++q) {
+      const int t = base + q * 32 + (int)lane;
+      xs[q] = x1[q];
+      cand[q] = xs[q] ? (m1[q] & needm) : 0u;  // this lane's tile: rows worth a load
+      m1[q] = c2[q] >= 0 ? rm[t + SPAN] : 0u;
+      x1[q] = c2[q] >= 0 ? x[c2[q]] : 0u;
+      c2[q] = t + 2 * SPAN < t1 ? v.colind[t + 2 * SPAN] : -1;
+      // pair positions, only for batches with pairs
+      const int cnt = __popc(cand[q]);
+      total[q] = (int)__reduce_add_sync(0xffffffffu, (unsigned)cnt);
+      incl[q] = excl[q] = 0;
+      if (total[q]) {
+        incl[q] = warp_incl_sum(cnt, lane);
+        excl[q] = incl[q] - cnt;
+      }
+      most = max(most, total[q]);
     }
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
-    const int excl = incl - cnt;
-    for (int pb = 0; pb < total; pb += 64) {
+    for (int pb = 0; pb < most; pb += 32) {
       unsigned hit = 0u;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int p = pb + h * 32 + (int)lane;
+      for (int q = 0; q < NB; ++q) {
+        const int p = pb + (int)lane;
         // tile of pair p: the number of lanes whose inclusive count is <= p
         int j = 0;
 #pragma unroll
         for (int st = 16; st > 0; st >>= 1) {
-          const int q = __shfl_sync(0xffffffffu, incl, j + st - 1);
-          if (q <= p) j += st;
+          const int c = __shfl_sync(0xffffffffu, incl[q], j + st - 1);
+          if (c <= p) j += st;
         }
-        const int ej = __shfl_sync(0xffffffffu, excl, j);
-        const unsigned cj = __shfl_sync(0xffffffffu, cand, j);
-        const unsigned xj = __shfl_sync(0xffffffffu, xs, j);
-        if (p < total) {
+        const int ej = __shfl_sync(0xffffffffu, excl[q], j);
+        const unsigned cj = __shfl_sync(0xffffffffu, cand[q], j);
+        const unsigned xj = __shfl_sync(0xffffffffu, xs[q], j);
+        if (p < total[q]) {
           const int r = (int)__fns(cj, 0, p - ej + 1);
           if ((needm >> r) & 1u) {
-            if (val[(size_t)(base + j) * 32 + r] & xj) hit |= 1u << r;
+            if (val[(size_t)(base + q * 32 + j) * 32 + r] & xj) hit |= 1u << r;
           }
         }
       }
@@ -172,9 +198,99 @@ __device__ __forceinline__ void pull_or_scan(const GView& v, int t0, int t1,
   }
 }
 
+// 32x32 bit transpose across a warp: lane j holds word m_j; lane r gets the
+// word whose bit j is bit r of m_j (recursive swap of off-diagonal blocks).
+__device__ __forceinline__ unsigned warp_transpose32(unsigned x, unsigned lane) {
+  const unsigned lo_masks[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+#pragma unroll
+  for (int s = 0; s < 5; ++s) {
+    const int k = 16 >> s;
+    const unsigned lo = lo_masks[s];
+    const unsigned y = __shfl_xor_sync(0xffffffffu, x, k);
+    x = (lane & k) ? ((x & ~lo) | ((y & ~lo) >> k)) : ((x & lo) | ((y & lo) << k));
+  }
+  return x;
+}
+
+// fold_row_cols (below) for b = 32 tiles with packed row words.  Per batch
+// of 32 tiles the occupancy words are transposed, so lane r holds the set of
+// the batch's tiles in which row r is non-empty and visits only those, U at
+// a time (on sparse graphs a row is non-empty in one or two tiles of a
+// batch, where the per-tile walk would keep 30 of 32 lanes idle).  Per row
+// the terms come in tile order: the first set column of each of the U
+// tiles, then the other set columns of each.
+template <int U, typename Acc, typename Term, typename Comb>
+__device__ __forceinline__ void fold_row_cols_t32(const GView& v, int t0, int t1, long long wb,
+                                                  unsigned lane, Term term, Comb comb, Acc& acc) {
+  using T = decltype(term(0ll));
+  const unsigned* __restrict__ words = v.rowword;
+  const unsigned* __restrict__ rm = v.rowmask;
+  const unsigned below = (1u << lane) - 1u;
+  auto rest = [&](unsigned a, long long base) {
+    while (a) {
+      const int j = __clz((int)a);
+      a &= ~(0x80000000u >> j);
+      comb(acc, term(base + j));
+    }
+  };
+  int cn = t0 + (int)lane < t1 ? v.colind[t0 + lane] : 0;
+  unsigned mn = t0 + (int)lane < t1 ? rm[t0 + lane] : 0u;
+  for (int b0 = t0; b0 < t1; b0 += 32) {
+    const int cb = cn;
+    const unsigned m = mn;
+    if (b0 + 32 < t1) {
+      const int t = b0 + 32 + (int)lane;
+      cn = t < t1 ? v.colind[t] : 0;
+      mn = t < t1 ? rm[t] : 0u;
+    }
+    const int mc = __popc(m);
+    const int mi = warp_incl_sum(mc, lane);
+    const int off = mi - mc;  // lane j: tile j's first word, relative to wb
+    const long long wbat = wb;
+    wb += __shfl_sync(0xffffffffu, mi, 31);
+    unsigned tl = warp_transpose32(m, lane);  // lane r: tiles of the batch where row r is non-empty
+    while (__any_sync(0xffffffffu, tl != 0u)) {
+      int jj[U];
+#pragma unroll
+      for (int k = 0; k < U; ++k) {
+        jj[k] = tl ? __ffs(tl) - 1 : -1;
+        if (tl) tl &= tl - 1;
+      }
+      unsigned w[U];
+      long long base[U];
+#pragma unroll
+      for (int k = 0; k < U; ++k) {
+        const int src = jj[k] < 0 ? 0 : jj[k];
+        const unsigned mj = __shfl_sync(0xffffffffu, m, src);
+        const int oj = __shfl_sync(0xffffffffu, off, src);
+        base[k] = (long long)__shfl_sync(0xffffffffu, cb, src) * 32;
+        w[k] = jj[k] >= 0 ? words[wbat + oj + __popc(mj & below)] : 0u;
+      }
+      T g[U];
+      bool h[U];
+#pragma unroll
+      for (int k = 0; k < U; ++k) {
+        h[k] = w[k] != 0u;
+        if (h[k]) {
+          const int j = __clz((int)w[k]);
+          w[k] &= ~(0x80000000u >> j);
+          g[k] = term(base[k] + j);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < U; ++k)
+        if (h[k]) comb(acc, g[k]);
+#pragma unroll
+      for (int k = 0; k < U; ++k) rest(w[k], base[k]);
+    }
+  }
+}
+
 // Fold term(column) over the set columns of this lane's row words in tiles
 // [t0, t1) (row r, and r + 32 for b = 64), for semirings whose value comes
-// from a gather at the column (x[j], dist[j], labels[j] ...).  U tiles per
+// from a gather at the column (x[j], dist[j], labels[j] ...).  wb is the
+// packed-word index of tile t0's first word (b = 32 graphs with packed row
+// words take fold_row_cols_t32 above).  U tiles per
 // step: their block-column indices and row words are loaded together, then
 // the first set column of every word is gathered together (U or 2U
 // independent loads in flight); further set columns of a word (rare in
@@ -182,12 +298,18 @@ __device__ __forceinline__ void pull_or_scan(const GView& v, int t0, int t1,
 // column idx; comb(acc, value) folds it into acc.  Words are left-aligned
 // in 32 bits for b <= 32 (64 for b = 64) so that column 0 is the top bit.
 template <int B, int U, typename Acc, typename Term, typename Comb>
-__device__ __forceinline__ void fold_row_cols(const GView& v, int t0, int t1, int r, Term term,
-                                              Comb comb, Acc& acc0, Acc& acc1) {
+__device__ __forceinline__ void fold_row_cols(const GView& v, int t0, int t1, long long wb, int r,
+                                              Term term, Comb comb, Acc& acc0, Acc& acc1) {
   using WT = typename Word<B>::T;
   using L = Lay<B>;
   using T = decltype(term(0ll));
   using AW = typename std::conditional<(B > 32), unsigned long long, unsigned>::type;
+  if constexpr (B == 32) {
+    if (v.rowword) {
+      fold_row_cols_t32<U>(v, t0, t1, wb, (unsigned)r, term, comb, acc0);
+      return;
+    }
+  }
   constexpr int kBits = sizeof(AW) * 8;
   constexpr AW kTop = (AW)1 << (kBits - 1);
   const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
@@ -199,43 +321,27 @@ __device__ __forceinline__ void fold_row_cols(const GView& v, int t0, int t1, in
       comb(acc, term(base + j));
     }
   };
-  // b = 32 tiles with occupancy words: a lane loads its row word only where
-  // it is non-empty (the others are zero and fold nothing), so a sparse
-  // tile costs the sectors of its non-empty rows.  The occupancy words run
-  // one batch ahead of the row words they predicate.
-  const unsigned* __restrict__ rm = B == 32 ? v.rowmask : nullptr;
-  auto masks = [&](int tb, unsigned (&m)[U]) {
-#pragma unroll
-    for (int k = 0; k < U; ++k) m[k] = rm ? rm[tb + k] : ~0u;
-  };
   // software pipeline: batch i+1's column indices and row words load while
   // batch i's gathers run
-  auto load = [&](int tb, unsigned (&base)[U], AW (&a0)[U], AW (&a1)[U], const unsigned (&m)[U]) {
+  auto load = [&](int tb, unsigned (&base)[U], AW (&a0)[U], AW (&a1)[U]) {
 #pragma unroll
     for (int k = 0; k < U; ++k) {
       base[k] = (unsigned)v.colind[tb + k] * (unsigned)B;  // < 2^32: ncols is an int
-      a0[k] = (m[k] >> (r & 31)) & 1u ? (AW)val[(size_t)(tb + k) * B + r] << (kBits - B) : (AW)0;
+      a0[k] = (AW)val[(size_t)(tb + k) * B + r] << (kBits - B);
       a1[k] = L::RPL == 2 ? (AW)val[(size_t)(tb + k) * B + 32 + r] << (kBits - B) : (AW)0;
     }
   };
   int t = t0;
-  unsigned base[U], mk[U];
+  unsigned base[U];
   AW a0[U], a1[U];
   bool have = t + U <= t1;
-  if (have) {
-    masks(t, mk);
-    load(t, base, a0, a1, mk);
-    if (t + 2 * U <= t1) masks(t + U, mk);
-  }
+  if (have) load(t, base, a0, a1);
   while (have) {
     const int tn = t + U;
     const bool next = tn + U <= t1;
     unsigned nbase[U];
     AW n0[U], n1[U];
-    if (next) {
-      load(tn, nbase, n0, n1, mk);
-      if (tn + 2 * U <= t1) masks(tn + U, mk);
-    }
+    if (next) load(tn, nbase, n0, n1);
     T g0[U], g1[U];
     bool h0[U], h1[U];
 #pragma unroll

@@ -113,18 +113,34 @@ __global__ void __launch_bounds__(kPprTPB) k_ppr_step(PprArgs a) {
       nl = 0;
       __syncwarp();
     };
-    const unsigned* __restrict__ rm = v.rowmask;  // occupancy words: skip empty row words
+    // occupancy words: skip empty row words; packed row words: read the
+    // non-empty ones from there (offsets from a prefix over the batch)
+    const unsigned* __restrict__ rm = v.rowmask;
+    const unsigned* __restrict__ words = v.rowword;
+    long long wb = words ? v.item_wbase[item] : 0ll;
     for (int b0 = it.t0; b0 < it.t1; b0 += 32) {
       const int t = b0 + (int)lane;
       const int cb = t < it.t1 ? v.colind[t] : 0;
-      const unsigned mw = t < it.t1 && rm ? rm[t] : ~0u;
+      const unsigned mw = t < it.t1 ? (rm ? rm[t] : ~0u) : 0u;
+      int woff = 0;
+      const long long wbat = wb;
+      if (words) {
+        const int mc = __popc(mw);
+        const int mi = warp_incl_sum(mc, lane);
+        woff = mi - mc;
+        wb += __shfl_sync(0xffffffffu, mi, 31);
+      }
       const int ntile = min(32, it.t1 - b0);
       for (int g0 = 0; g0 < ntile; g0 += kU) {
         uint32_t wr[kU];
 #pragma unroll
         for (int k = 0; k < kU; ++k) {
           const unsigned mk = __shfl_sync(0xffffffffu, mw, (g0 + k) & 31);
-          wr[k] = g0 + k < ntile && ((mk >> lane) & 1u) ? val[(size_t)(b0 + g0 + k) * 32 + lane] : 0u;
+          const int ok = __shfl_sync(0xffffffffu, woff, (g0 + k) & 31);
+          wr[k] = 0u;
+          if (g0 + k < ntile && ((mk >> lane) & 1u))
+            wr[k] = words ? words[rowword_index(wbat + ok, mk, (int)lane)]
+                          : val[(size_t)(b0 + g0 + k) * 32 + lane];
         }
 #pragma unroll
         for (int k = 0; k < kU; ++k) {
