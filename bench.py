@@ -296,10 +296,11 @@ def run_reference(args, ws, rank):
 
 
 # --------------------------------------------------------------- serving
-def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed):
+def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed, device=False):
     """Poisson arrivals of BFS sources and PPR sets (1..64 vertices, Dirichlet
     weights) into the continuous-batching server; returns achieved qps and
-    p50/p99 latencies (submit to result in host memory)."""
+    p50/p99 latencies (submit to result in host memory, or with `device` in
+    a device buffer of the client's)."""
     import threading
 
     rng = np.random.default_rng(seed)
@@ -340,12 +341,16 @@ def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed):
                 tq[kind].put(None)
 
     def consumer(kind):
-        buf = np.empty(n, np.int32 if kind == "bfs" else np.float32)  # reused per thread
+        # result buffer reused per thread
+        buf = gbo.DeviceBuffer(4 * n) if device else np.empty(n, np.int32 if kind == "bfs" else np.float32)
         while True:
             ticket = tq[kind].get()
             if ticket is None:
                 return
-            _, ms, _ = srv.wait(ticket, kind, timeout=300.0, out=buf)
+            if device:
+                ms, _ = srv.wait_device(ticket, buf, timeout=300.0)
+            else:
+                _, ms, _ = srv.wait(ticket, kind, timeout=300.0, out=buf)
             with lock:
                 lat[kind].append(ms)
                 done_t[kind] = max(done_t[kind], time.perf_counter() - t0)
@@ -539,6 +544,11 @@ def run_ours(args, ws, rank, local):
         # call with its levels read back to host memory (what a served query delivers)
         served["bfs_only"]["vs_plain_bfs_qps"] = served["bfs_only"]["achieved_qps"] / (1e3 / ms)
         served["bfs_only"]["vs_plain_e2e_qps"] = served["bfs_only"]["achieved_qps"] / (1e3 / e2e_ms)
+        # the same stream with results handed over in device memory (clients
+        # that consume them on the GPU), offered at twice the rate
+        served["bfs_only_device"] = serve_stream(gbo, g_row, n, 2 * args.serve_qps, args.serve_s, 0.0, 7,
+                                                 device=True)
+        served["bfs_only_device"]["vs_plain_bfs_qps"] = served["bfs_only_device"]["achieved_qps"] / (1e3 / ms)
         served["mixed_10pct_ppr"] = serve_stream(gbo, g_row, n, args.serve_qps / 8, args.serve_s, 0.1, 6)
     wb = max(1, args.tile // 8)
     bmv_bytes = (int(info.nblocks) * (args.tile * args.tile // 8 + 4) + 4 * (info.nblockrows + 1)

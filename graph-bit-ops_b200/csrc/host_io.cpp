@@ -19,6 +19,8 @@
 #include <string>
 #include <vector>
 
+#include <immintrin.h>
+
 #include "host_common.h"
 
 namespace gbo {
@@ -612,3 +614,41 @@ extern "C" int gbo_gen_er_batch(int count, int nmin, int nmax, double avg_degree
   *out = g;
   return GBO_OK;
 }
+
+// ----------------------------------------------------- result widening
+// Served BFS results travel as byte levels (255 = unreachable) and are
+// widened to the caller's int32 levels (-1 = unreachable) on the client
+// thread.  That pass writes 16 bytes per 4 read per vertex, so it is written
+// with AVX2 and non-temporal stores (no read-for-ownership of the 4n-byte
+// destination) where the CPU has AVX2.
+namespace gbo {
+namespace {
+__attribute__((target("avx2"))) void widen_levels_avx2(const unsigned char* b8, int* o, long long n) {
+  long long i = 0;
+  for (; i < n && (reinterpret_cast<uintptr_t>(o + i) & 31); ++i) o[i] = b8[i] == 255 ? -1 : b8[i];
+  const __m256i ff = _mm256_set1_epi32(255);
+  for (; i + 32 <= n; i += 32) {
+    const __m256i v = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(b8 + i));
+    const __m128i lo = _mm256_castsi256_si128(v);
+    const __m128i hi = _mm256_extracti128_si256(v, 1);
+    __m256i q[4] = {_mm256_cvtepu8_epi32(lo), _mm256_cvtepu8_epi32(_mm_srli_si128(lo, 8)),
+                    _mm256_cvtepu8_epi32(hi), _mm256_cvtepu8_epi32(_mm_srli_si128(hi, 8))};
+    for (int k = 0; k < 4; ++k) {
+      q[k] = _mm256_or_si256(q[k], _mm256_cmpeq_epi32(q[k], ff));  // 255 -> all ones = -1
+      _mm256_stream_si256(reinterpret_cast<__m256i*>(o + i + 8 * k), q[k]);
+    }
+  }
+  for (; i < n; ++i) o[i] = b8[i] == 255 ? -1 : b8[i];
+  _mm_sfence();
+}
+}  // namespace
+
+void host_widen_levels(const unsigned char* b8, int* o, long long n) {
+  static const bool avx2 = __builtin_cpu_supports("avx2");
+  if (avx2) {
+    widen_levels_avx2(b8, o, n);
+    return;
+  }
+  for (long long i = 0; i < n; ++i) o[i] = (int)b8[i] | -(int)(b8[i] == 255);
+}
+}  // namespace gbo

@@ -120,8 +120,15 @@ __global__ void __launch_bounds__(kTPB, 4) k_step(Args a) {
   constexpr int U = S >= 64 ? 1 : (64 / S > 8 ? 8 : 64 / S);  // gathers in flight: S*U pairs
   __shared__ uint32_t acc_sh[kWarps][32 * KW];
   __shared__ int2 list_sh[kWarps][kList];
+  __shared__ unsigned long long cnt_sh;
+  __shared__ int arrived_sh;
   volatile int* c = a.ctl;
-  if (c[1]) return;  // done
+  if (c[1]) return;  // done (the same for every block)
+  if (threadIdx.x == 0) {
+    cnt_sh = 0ull;
+    arrived_sh = 0;
+  }
+  __syncthreads();
   const int lvl = c[0];
   const GView& v = a.v;
   const uint32_t* __restrict__ F = a.F + (size_t)(lvl & 1) * a.fstride;
@@ -213,19 +220,37 @@ __global__ void __launch_bounds__(kTPB, 4) k_step(Args a) {
             r = (int)__fns(cj, 0, p - ej + 1);
             eff = val[(size_t)(b0 + j) * 32 + r] & fj;
           }
-          while (__any_sync(0xffffffffu, eff != 0u)) {
-            const int c = min(__popc(eff), kPerPass);
-            const int ic = warp_incl_sum(c, lane);
-            const int tc = __shfl_sync(0xffffffffu, ic, 31);
-            if (nlist + tc > kList) flush();
-            int pos = nlist + ic - c;
-            for (int q = 0; q < c; ++q) {
+          if constexpr (KW <= 2) {
+            // narrow frontier rows (k <= 64): each lane ORs the rows of its
+            // word's frontier vertices straight into the accumulator
+            while (eff) {
               const int col = __clz(eff);
               eff &= ~(0x80000000u >> col);
-              list[pos++] = make_int2(r, vbase + col);
+              const size_t fo = (size_t)(vbase + col) * KW;
+              if (KW == 1) {
+                const uint32_t f = F[fo];
+                if (f) atomicOr(acc + r, f);
+              } else {
+                const uint2 f = *reinterpret_cast<const uint2*>(F + fo);
+                if (f.x) atomicOr(acc + r * KW, f.x);
+                if (f.y) atomicOr(acc + r * KW + 1, f.y);
+              }
             }
-            nlist += tc;
-            __syncwarp();
+          } else {
+            while (__any_sync(0xffffffffu, eff != 0u)) {
+              const int c = min(__popc(eff), kPerPass);
+              const int ic = warp_incl_sum(c, lane);
+              const int tc = __shfl_sync(0xffffffffu, ic, 31);
+              if (nlist + tc > kList) flush();
+              int pos = nlist + ic - c;
+              for (int q = 0; q < c; ++q) {
+                const int col = __clz(eff);
+                eff &= ~(0x80000000u >> col);
+                list[pos++] = make_int2(r, vbase + col);
+              }
+              nlist += tc;
+              __syncwarp();
+            }
           }
         }
       }
@@ -244,13 +269,18 @@ __global__ void __launch_bounds__(kTPB, 4) k_step(Args a) {
       for (int q = lane; q < 32 * KW; q += 32) dst[q] = 0u;
     }
   }
-  __shared__ unsigned long long sh;
-  if (threadIdx.x == 0) sh = 0;
-  __syncthreads();
+  // block count without a closing barrier: warps add and leave; the last
+  // warp of the block to arrive adds the block's count to the level total
   for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-  if (lane == 0 && cnt) atomicAdd(&sh, cnt);
-  __syncthreads();
-  if (threadIdx.x == 0 && sh) atomicAdd(reinterpret_cast<unsigned long long*>(a.ctl + 4), sh);
+  if (lane == 0) {
+    if (cnt) atomicAdd(&cnt_sh, cnt);
+    __threadfence_block();
+    if (atomicAdd(&arrived_sh, 1) == kWarps - 1) {
+      __threadfence_block();
+      const unsigned long long tot = atomicAdd(&cnt_sh, 0ull);
+      if (tot) atomicAdd(reinterpret_cast<unsigned long long*>(a.ctl + 4), tot);
+    }
+  }
 }
 
 // Split block rows (one warp each): OR the slot accumulators and run the

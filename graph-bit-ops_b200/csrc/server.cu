@@ -1028,10 +1028,37 @@ extern "C" int gbo_server_submit_ppr(gbo_server* S, const int* verts, const floa
   return submit(S, std::move(q), ticket);
 }
 
-// Byte levels to int32, 255 (unreachable) to -1; branch-free so that the
-// compiler vectorises it.
-static void widen_levels(const unsigned char* __restrict__ b8, int* __restrict__ o, int n) {
-  for (int i = 0; i < n; ++i) o[i] = (int)b8[i] | -(int)(b8[i] == 255);
+// Byte levels to int32, 255 (unreachable) to -1 (host_io.cpp).
+namespace gbo {
+void host_widen_levels(const unsigned char* b8, int* o, long long n);
+}
+static void widen_levels(const unsigned char* b8, int* o, int n) { gbo::host_widen_levels(b8, o, n); }
+
+// Byte levels to int32 on the device (device delivery), 16 per thread.
+__global__ void k_widen_levels(const unsigned char* __restrict__ b8, int* __restrict__ o, int n) {
+  const long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 16;
+  if (i >= n) return;
+  const bool vec = i + 16 <= n && ((reinterpret_cast<uintptr_t>(o) | reinterpret_cast<uintptr_t>(b8)) & 15) == 0;
+  if (vec) {
+    const uint4 v = *reinterpret_cast<const uint4*>(b8 + i);
+    const unsigned w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      int4 r;
+      const unsigned a = w[q];
+      r.x = (int)(a & 0xffu);
+      r.y = (int)((a >> 8) & 0xffu);
+      r.z = (int)((a >> 16) & 0xffu);
+      r.w = (int)(a >> 24);
+      r.x = r.x == 255 ? -1 : r.x;
+      r.y = r.y == 255 ? -1 : r.y;
+      r.z = r.z == 255 ? -1 : r.z;
+      r.w = r.w == 255 ? -1 : r.w;
+      reinterpret_cast<int4*>(o + i)[q] = r;
+    }
+  } else {
+    for (long long k = i; k < i + 16 && k < n; ++k) o[k] = b8[k] == 255 ? -1 : (int)b8[k];
+  }
 }
 
 // Per client thread: a pinned bounce buffer and a stream, so that result
@@ -1064,11 +1091,71 @@ struct ClientCopy {
   }
 };
 
+// Per client thread for device delivery: a stream (when the caller gives
+// none) and a blocking-sync event that says when the result buffer has been
+// read.
+struct ClientDeviceCopy {
+  cudaStream_t st = nullptr;
+  cudaEvent_t done = nullptr;
+  std::vector<int> widened;  // results already moved to host memory
+  ~ClientDeviceCopy() {
+    if (st) cudaStreamDestroy(st);
+    if (done) cudaEventDestroy(done);
+  }
+};
+
+// Copy result r into the caller's device buffer d_out on stream ds (0: the
+// thread's own stream), widening byte levels to int32, and wait until the
+// copy has read the result buffer.
+static cudaError_t deliver_device(gbo_server* S, const Result& r, void* d_out, cudaStream_t ds) {
+  thread_local ClientDeviceCopy cc;
+  cudaError_t e = cudaSuccess;
+  if (!ds) {
+    // the thread's own stream at the highest priority, so that the copy's
+    // blocks are scheduled ahead of the traversal kernels already queued
+    if (!cc.st) {
+      int least = 0, greatest = 0;
+      e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+      if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&cc.st, cudaStreamNonBlocking, greatest);
+    }
+    ds = cc.st;
+  }
+  if (e == cudaSuccess && !cc.done)
+    e = cudaEventCreateWithFlags(&cc.done, cudaEventBlockingSync | cudaEventDisableTiming);
+  if (e != cudaSuccess) return e;
+  const int n = S->n;
+  if (r.buf < 0) {  // already in host memory
+    const void* src = r.host.data();
+    if (r.u8) {
+      cc.widened.resize((size_t)n);
+      widen_levels(r.host.data(), cc.widened.data(), n);
+      src = cc.widened.data();
+    }
+    e = cudaMemcpyAsync(d_out, src, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, ds);
+  } else {
+    const char* src = S->dpool[r.pool] + (size_t)r.buf * S->dbytes[r.pool];
+    e = cudaStreamWaitEvent(ds, r.ev, 0);
+    if (e == cudaSuccess && r.u8) {
+      const long long th = ((long long)n + 15) / 16;
+      if (th > 0)
+        k_widen_levels<<<(unsigned)((th + 255) / 256), 256, 0, ds>>>(
+            reinterpret_cast<const unsigned char*>(src), static_cast<int*>(d_out), n);
+      e = cudaGetLastError();
+    } else if (e == cudaSuccess) {
+      e = cudaMemcpyAsync(d_out, src, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, ds);
+    }
+  }
+  if (e == cudaSuccess) e = wait_stream(ds, cc.done);
+  return e;
+}
+
 // Hand a finished result to the caller: wait for its retirement kernel,
 // copy it from the device buffer (widening byte levels to int32) outside the
-// lock, then give the buffer back to the pool.
+// lock -- to host memory (h_out) or, with `device`, to the caller's device
+// buffer d_out -- then give the buffer back to the pool.
 static int take_result(gbo_server* S, std::unique_lock<std::mutex>& lk, int64_t ticket, void* h_out,
-                       double* latency_ms, int* iterations) {
+                       double* latency_ms, int* iterations, bool device = false,
+                       cudaStream_t ds = nullptr) {
   auto it = S->results.find(ticket);
   const Result r = std::move(it->second);
   S->results.erase(it);
@@ -1077,7 +1164,10 @@ static int take_result(gbo_server* S, std::unique_lock<std::mutex>& lk, int64_t 
   const double t0 = now_ms();
   double t1 = t0, t2 = t0;
   cudaError_t e = cudaSuccess;
-  if (r.buf < 0) {  // already in host memory
+  if (device) {
+    if (h_out) e = deliver_device(S, r, h_out, ds);
+    t2 = t1 = now_ms();
+  } else if (r.buf < 0) {  // already in host memory
     if (h_out && r.u8) {
       int* o = static_cast<int*>(h_out);
       widen_levels(r.host.data(), o, S->n);
@@ -1146,6 +1236,22 @@ extern "C" int gbo_server_wait(gbo_server* S, int64_t ticket, void* h_out, doubl
   if (S->worker_status != GBO_OK) return fail(S->worker_status, S->worker_error);
   if (!ok) return fail(GBO_ERR_TIMEOUT, "query not finished within the timeout");
   return take_result(S, lk, ticket, h_out, latency_ms, iterations);
+}
+
+extern "C" int gbo_server_wait_device(gbo_server* S, int64_t ticket, void* d_out,
+                                      double* latency_ms, int* iterations, double timeout_s,
+                                      gbo_stream_t stream) {
+  clear_error();
+  if (!S) return fail(GBO_ERR_INVALID, "NULL server");
+  std::unique_lock<std::mutex> lk(S->mu);
+  const bool ok = S->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] {
+    if (S->worker_status != GBO_OK) return true;
+    auto it = S->results.find(ticket);
+    return it != S->results.end() && !it->second.moving;
+  });
+  if (S->worker_status != GBO_OK) return fail(S->worker_status, S->worker_error);
+  if (!ok) return fail(GBO_ERR_TIMEOUT, "query not finished within the timeout");
+  return take_result(S, lk, ticket, d_out, latency_ms, iterations, true, as_stream(stream));
 }
 
 extern "C" int gbo_server_get_stats(gbo_server* S, gbo_server_stats* st) {

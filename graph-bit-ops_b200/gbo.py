@@ -146,6 +146,8 @@ _SIGS = {
     "gbo_server_submit_ppr": (_I, [_P, _P, _P, _I, C.POINTER(C.c_int64)]),
     "gbo_server_poll": (_I, [_P, C.c_int64, _P, C.POINTER(C.c_double), C.POINTER(_I)]),
     "gbo_server_wait": (_I, [_P, C.c_int64, _P, C.POINTER(C.c_double), C.POINTER(_I), C.c_double]),
+    "gbo_server_wait_device": (_I, [_P, C.c_int64, _P, C.POINTER(C.c_double), C.POINTER(_I),
+                                    C.c_double, _P]),
     "gbo_server_get_stats": (_I, [_P, C.POINTER(ServerStats)]),
     "gbo_server_destroy": (_I, [_P]),
     "gbo_read_mtx": (_I, [C.c_char_p, _I, _I, C.POINTER(C.POINTER(CsrStruct))]),
@@ -681,6 +683,14 @@ class Server:
         check(lib().gbo_server_wait(self.h, ticket, _ptr(out), C.byref(lat), C.byref(it), timeout),
               "server_wait")
         return out, lat.value, it.value
+
+    def wait_device(self, ticket: int, out, timeout=120.0):
+        """Block until the query's result is in `out` (a DeviceBuffer of n
+        int32 levels or n float32 PPR values); (latency_ms, iterations)."""
+        lat, it = C.c_double(0), C.c_int(0)
+        check(lib().gbo_server_wait_device(self.h, ticket, out.ptr, C.byref(lat), C.byref(it),
+                                           timeout, None), "server_wait_device")
+        return lat.value, it.value
 
     def poll(self, ticket: int, kind: str = "bfs"):
         """(result, latency_ms, iterations) or None while the query runs."""

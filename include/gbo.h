@@ -355,7 +355,8 @@ typedef struct gbo_server_stats {
    * (extraction into device result buffers), and the clients' result
    * copies (device to host, inside wait/poll) */
   double bfs_round_ms, ppr_round_ms, retire_ms, copy_ms;
-  /* copy_ms split: waiting for the retirement kernel, the device-to-host
+  /* copy_ms split: waiting for the retirement kernel (with
+   * gbo_server_wait_device: the whole device-side copy), the device-to-host
    * copy, and widening byte levels into the caller's int32 buffer */
   double copy_wait_ms, copy_d2h_ms, copy_widen_ms;
 } gbo_server_stats;
@@ -370,6 +371,14 @@ GBO_API int gbo_server_poll(gbo_server* s, int64_t ticket, void* h_out,
                     double* latency_ms, int* iterations);
 GBO_API int gbo_server_wait(gbo_server* s, int64_t ticket, void* h_out,
                     double* latency_ms, int* iterations, double timeout_s);
+/* As gbo_server_wait, but the result goes to the caller's device buffer
+ * d_out (BFS int32[n] levels, PPR float[n]), for consumers that stay on the
+ * GPU: no host copy.  The copy runs on `stream` (0: a high-priority stream
+ * of the calling thread's own, so that it does not queue behind the
+ * server's traversal kernels) and is complete when the call returns. */
+GBO_API int gbo_server_wait_device(gbo_server* s, int64_t ticket, void* d_out,
+                           double* latency_ms, int* iterations, double timeout_s,
+                           gbo_stream_t stream);
 GBO_API int gbo_server_get_stats(gbo_server* s, gbo_server_stats* stats);
 GBO_API int gbo_server_destroy(gbo_server* s);
 

@@ -111,3 +111,27 @@ def test_server_results_collected_in_any_order(gbo, orc, gpu):
     srv.close()
     for s, lv in out.values():
         assert np.array_equal(lv, orc.bfs_csr(csr.rowptr, csr.colind, csr.nrows, int(s))[0])
+
+
+def test_server_device_delivery_matches_host_delivery(gbo, orc, gpu):
+    """gbo_server_wait_device writes the same result into a device buffer as
+    gbo_server_wait writes into host memory (BFS byte levels widened on the
+    GPU, PPR values copied)."""
+    csr = gbo.gen_rmat(12, 16, seed=1)
+    n = csr.nrows
+    g = gbo.Graph.from_csr(csr, 32)
+    qs = make_queries(n, 60, 12, seed=12)
+    srv = gbo.Server(g, bfs_slots=64, ppr_slots=32, alpha=0.85, tol=1e-7)
+    t_host = submit_all(srv, qs)
+    t_dev = submit_all(srv, qs)
+    dbuf = gbo.DeviceBuffer(4 * n)
+    for (kind, arg), th, td in zip(qs, t_host, t_dev):
+        host, _, _ = srv.wait(th, kind)
+        lat, it = srv.wait_device(td, dbuf)
+        assert lat >= 0 and it >= 1
+        dev = gbo.device_to_numpy(dbuf.ptr, np.int32 if kind == "bfs" else np.float32, n)
+        assert np.array_equal(dev, host), (kind, arg if kind == "bfs" else len(arg[0]))
+        if kind == "bfs":
+            want, _ = orc.bfs_csr(csr.rowptr, csr.colind, n, arg)
+            assert np.array_equal(dev, want)
+    srv.close()
