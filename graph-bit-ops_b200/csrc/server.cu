@@ -62,13 +62,11 @@ struct PprArgs {
 
 // One iteration for all 32 slots: X'[i][s] = alpha * sum_{j: P[i][j]} X[j][s]
 // inv[j] + P[i][s]; lane = slot; fp64 accumulators in shared memory.
-// A warp walks its item's tiles kU at a time (lane = tile row: one word per
-// lane per tile, loaded together); each set bit (row r, column j) goes to a
-// per-warp list in shared memory at the position a warp prefix sum of the
-// lanes' bit counts gives it; the list is then consumed with lane = slot,
-// kP X-row gathers in flight.  Tiles with more bits than the list holds are
-// walked directly.  The (row, column) order is the tiles' own, so every
-// column's sum has a fixed order whatever the other slots hold.
+// A warp deals its item's non-empty row words out to the lanes (below); each
+// set bit (row r, column j) goes to a per-warp list in shared memory, which
+// is then consumed with lane = slot, kP X-row gathers in flight.  The list
+// order depends on the graph only, so every column's sum has a fixed order
+// whatever the other slots hold.
 constexpr int kPprList = 256;
 
 __global__ void __launch_bounds__(kPprTPB) k_ppr_step(PprArgs a) {
@@ -91,7 +89,7 @@ __global__ void __launch_bounds__(kPprTPB) k_ppr_step(PprArgs a) {
     const gbo_item it = v.items[item];
     const uint32_t* __restrict__ val = reinterpret_cast<const uint32_t*>(v.val);
     const bool lane_active = (a.active >> lane) & 1u;
-    constexpr int kU = 8, kP = 8;
+    constexpr int kP = 8;  // X-row gathers in flight
     int nl = 0;  // list length (warp-uniform)
     auto flush = [&]() {
       for (int q0 = 0; q0 < nl; q0 += kP) {
@@ -113,73 +111,59 @@ __global__ void __launch_bounds__(kPprTPB) k_ppr_step(PprArgs a) {
       nl = 0;
       __syncwarp();
     };
-    // occupancy words: skip empty row words; packed row words: read the
-    // non-empty ones from there (offsets from a prefix over the batch)
+    // Per batch of 32 tiles (lane j: tile j) the non-empty row words -- all
+    // 32 rows of every tile without occupancy words -- are dealt out to the
+    // lanes in (tile, row) order, 32 per round: lane p takes word p (its
+    // tile by a binary search over the prefix counts; with packed row words
+    // word p of the batch is simply the next packed word).  Each word's set
+    // bits go to the list at positions from a warp prefix sum, at most
+    // kPprList / 32 per lane per pass, so the list order -- and with it every
+    // sum's order -- depends on the graph only.
     const unsigned* __restrict__ rm = v.rowmask;
     const unsigned* __restrict__ words = v.rowword;
     long long wb = words ? v.item_wbase[item] : 0ll;
+    constexpr int kPerPass = kPprList / 32;
     for (int b0 = it.t0; b0 < it.t1; b0 += 32) {
       const int t = b0 + (int)lane;
       const int cb = t < it.t1 ? v.colind[t] : 0;
       const unsigned mw = t < it.t1 ? (rm ? rm[t] : ~0u) : 0u;
-      int woff = 0;
+      const int mc = __popc(mw);
+      const int mi = warp_incl_sum(mc, lane);
+      const int mex = mi - mc;
+      const int total = __shfl_sync(0xffffffffu, mi, 31);
       const long long wbat = wb;
-      if (words) {
-        const int mc = __popc(mw);
-        const int mi = warp_incl_sum(mc, lane);
-        woff = mi - mc;
-        wb += __shfl_sync(0xffffffffu, mi, 31);
-      }
-      const int ntile = min(32, it.t1 - b0);
-      for (int g0 = 0; g0 < ntile; g0 += kU) {
-        uint32_t wr[kU];
+      wb += total;
+      for (int pb = 0; pb < total; pb += 32) {
+        const int p = pb + (int)lane;
+        int j = 0;
 #pragma unroll
-        for (int k = 0; k < kU; ++k) {
-          const unsigned mk = __shfl_sync(0xffffffffu, mw, (g0 + k) & 31);
-          const int ok = __shfl_sync(0xffffffffu, woff, (g0 + k) & 31);
-          wr[k] = 0u;
-          if (g0 + k < ntile && ((mk >> lane) & 1u))
-            wr[k] = words ? words[rowword_index(wbat + ok, mk, (int)lane)]
-                          : val[(size_t)(b0 + g0 + k) * 32 + lane];
+        for (int st = 16; st > 0; st >>= 1) {
+          const int q = __shfl_sync(0xffffffffu, mi, j + st - 1);
+          if (q <= p) j += st;
         }
-#pragma unroll
-        for (int k = 0; k < kU; ++k) {
-          const int cnt = __popc(wr[k]);
-          int incl = cnt;
-#pragma unroll
-          for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if ((int)lane >= o) incl += y;
-          }
-          const int total = __shfl_sync(0xffffffffu, incl, 31);
-          if (total == 0) continue;
-          const int C = __shfl_sync(0xffffffffu, cb, (g0 + k) & 31);
-          if (nl + total > kPprList) flush();
-          if (total > kPprList) {  // a dense tile: walk its bits directly
-            unsigned rows = __ballot_sync(0xffffffffu, wr[k] != 0);
-            while (rows) {
-              const int r = __ffs(rows) - 1;
-              rows &= rows - 1;
-              unsigned bits = __shfl_sync(0xffffffffu, wr[k], r);
-              while (bits) {
-                const int col = __clz(bits);
-                bits &= ~(0x80000000u >> col);
-                const size_t jj = (size_t)C * 32 + col;
-                if (lane_active) acc[r * kPprSlots + lane] += (double)(X[jj * kPprSlots + lane] * a.inv[jj]);
-              }
-            }
-            continue;
-          }
-          int pos = nl + incl - cnt;
-          unsigned bits = wr[k];
-          while (bits) {
-            const int col = __clz(bits);
-            bits &= ~(0x80000000u >> col);
+        const int ej = __shfl_sync(0xffffffffu, mex, j);
+        const unsigned mj = __shfl_sync(0xffffffffu, mw, j);
+        const int C = __shfl_sync(0xffffffffu, cb, j);
+        int r = 0;
+        unsigned w = 0u;
+        if (p < total) {
+          r = (int)__fns(mj, 0, p - ej + 1);
+          w = words ? words[wbat + p] : val[(size_t)(b0 + j) * 32 + r];
+        }
+        while (__any_sync(0xffffffffu, w != 0u)) {
+          const int c = min(__popc(w), kPerPass);
+          const int ic = warp_incl_sum(c, lane);
+          const int tc = __shfl_sync(0xffffffffu, ic, 31);
+          if (nl + tc > kPprList) flush();
+          int pos = nl + ic - c;
+          for (int q = 0; q < c; ++q) {
+            const int col = __clz(w);
+            w &= ~(0x80000000u >> col);
             lj[pos] = C * 32 + col;
-            lr[pos] = (unsigned char)lane;
+            lr[pos] = (unsigned char)r;
             ++pos;
           }
-          nl += total;
+          nl += tc;
           __syncwarp();
         }
       }
