@@ -79,7 +79,7 @@ class Dist:
             import torch.distributed as dist
 
             os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
             self.dist = dist
 
     def barrier(self):
