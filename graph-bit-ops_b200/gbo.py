@@ -116,6 +116,8 @@ _SIGS = {
     "gbo_graph_from_csr": (_I, [_P, _P, _I, _I, _I, _I, _I, _P, C.POINTER(_P)]),
     "gbo_graph_wrap_b2sr": (_I, [_I, _I, _I, _I, _I, _P, _P, _P, _P, _P, C.POINTER(_P)]),
     "gbo_graph_free": (_I, [_P]),
+    "gbo_graph_save": (_I, [_P, C.c_char_p]),
+    "gbo_graph_load": (_I, [C.c_char_p, _I, _P, C.POINTER(_P)]),
     "gbo_graph_get_info": (_I, [_P, C.POINTER(GraphInfo)]),
     "gbo_graph_b2sr": (_I, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
     "gbo_graph_outdeg": (_I, [_P, C.POINTER(_P)]),
@@ -449,6 +451,17 @@ class Graph:
                                         colind.ptr, val.ptr, outdeg.ptr if outdeg else None,
                                         stream, C.byref(p)), "graph_wrap_b2sr")
         return cls(p.value, keep=(rowptr, colind, val, outdeg))
+
+    @classmethod
+    def load(cls, path: str, flags: int = 0, stream=None) -> "Graph":
+        """Rebuild a graph from a B2SR cache file written by save()."""
+        p = C.c_void_p()
+        check(lib().gbo_graph_load(os.fsencode(path), flags, stream, C.byref(p)), "graph_load")
+        return cls(p.value)
+
+    def save(self, path: str) -> None:
+        """Write the B2SR arrays, out-degrees and permutation to a cache file."""
+        check(lib().gbo_graph_save(self.h, os.fsencode(path)), "graph_save")
 
     def info(self) -> GraphInfo:
         inf = GraphInfo()

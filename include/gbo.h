@@ -166,6 +166,17 @@ GBO_API int gbo_graph_wrap_b2sr(int nrows, int ncols, int tile_bits, int layout,
                         const int* d_outdeg, gbo_stream_t stream,
                         gbo_graph** out);
 GBO_API int gbo_graph_free(gbo_graph* g);
+/* Binary B2SR cache file.  gbo_graph_save writes g's B2SR arrays (the
+ * reference layout, byte for byte), its out-degrees and its vertex
+ * permutation (GBO_FLAG_DEGREE_ORDER) to `path`; gbo_graph_load rebuilds the
+ * graph from such a file without reparsing or repacking (flags:
+ * GBO_FLAG_SYMMETRIC, GBO_FLAG_TC_MMA as in gbo_graph_from_csr; a graph
+ * saved as symmetric stays symmetric).  Malformed files return GBO_ERR_IO.
+ * No reference counterpart: the reference reads the .mtx and repacks on
+ * every run (algorithm/bfs.cu:333-424). */
+GBO_API int gbo_graph_save(const gbo_graph* g, const char* path);
+GBO_API int gbo_graph_load(const char* path, int flags, gbo_stream_t stream,
+                   gbo_graph** out);
 
 typedef struct gbo_graph_info {
   int nrows, ncols, tile_bits, layout;
