@@ -85,5 +85,8 @@ int num_sms();
 // total also returned through d_total (int64).  No spin waits: three kernels.
 int exclusive_scan_i32(const int* d_in, int* d_out, long long n, long long* d_total,
                        cudaStream_t stream);
+// The same with int64 outputs.
+int exclusive_scan_i32_to_i64(const int* d_in, long long* d_out, long long n, long long* d_total,
+                              cudaStream_t stream);
 
 }  // namespace gbo

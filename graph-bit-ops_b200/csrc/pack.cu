@@ -431,6 +431,11 @@ int exclusive_scan_i32(const int* d_in, int* d_out, long long n, long long* d_to
   return exclusive_scan<int>(d_in, d_out, n, d_total, s);
 }
 
+int exclusive_scan_i32_to_i64(const int* d_in, long long* d_out, long long n, long long* d_total,
+                              cudaStream_t s) {
+  return exclusive_scan<long long>(d_in, d_out, n, d_total, s);
+}
+
 // nnzb per block row: counts -> bsr_rowptr (device) and total (host).
 static int nnzb_impl(const int* rowptr, const int* colind, int nrows, int ncols, long long nnz,
                      int b, int* bsr_rowptr, long long* h_total, cudaStream_t s) {

@@ -142,6 +142,9 @@ _SIGS = {
     "gbo_ppr_backward": (_I, [_P, _P, C.c_float, C.c_float, _I, _P, C.POINTER(_I), _P]),
     "gbo_graph_last_run": (_I, [_P, C.POINTER(RunStats)]),
     "gbo_msbfs": (_I, [_P, _P, _I, _P, C.POINTER(_I), _P]),
+    "gbo_bmm_sum": (_I, [_P, _P, C.POINTER(C.c_uint64), _P]),
+    "gbo_spgemm_nnz": (_I, [_P, _P, _P, C.POINTER(C.c_int64), _P]),
+    "gbo_spgemm_fill": (_I, [_P, _P, _P, _P, _P, _P]),
     "gbo_bfs_multi": (_I, [_P, _P, _I, _P, C.POINTER(_I), _P]),
     "gbo_server_create": (_I, [_P, _I, _I, C.c_float, C.c_float, _I, C.POINTER(_P)]),
     "gbo_server_submit_bfs": (_I, [_P, _I, C.POINTER(C.c_int64)]),
@@ -597,6 +600,27 @@ class Graph:
         it = C.c_int(0)
         check(lib().gbo_cc(self.h, buf.ptr, C.byref(it), stream), "cc")
         return buf.to_numpy(np.int32, n, stream), it.value
+
+    def bmm_sum(self, other: "Graph", stream=None) -> int:
+        """Sum of all entries of self @ other over the integers."""
+        out = C.c_uint64(0)
+        check(lib().gbo_bmm_sum(self.h, other.h, C.byref(out), stream), "bmm_sum")
+        return int(out.value)
+
+    def spgemm(self, other: "Graph", stream=None):
+        """self @ other (self: 32x32 ROW tiles, other: 32x32 COL tiles) as CSR:
+        (int64 rowptr, int32 colind, int32 counts)."""
+        n = self.info().nrows
+        drp = DeviceBuffer(8 * (n + 1))
+        nnz = C.c_int64(0)
+        check(lib().gbo_spgemm_nnz(self.h, other.h, drp.ptr, C.byref(nnz), stream), "spgemm_nnz")
+        m = int(nnz.value)
+        dci, dv = DeviceBuffer(4 * max(m, 1)), DeviceBuffer(4 * max(m, 1))
+        check(lib().gbo_spgemm_fill(self.h, other.h, drp.ptr, dci.ptr, dv.ptr, stream), "spgemm_fill")
+        rp = drp.to_numpy(np.int64, n + 1, stream)
+        if m == 0:
+            return rp, np.zeros(0, np.int32), np.zeros(0, np.int32)
+        return rp, dci.to_numpy(np.int32, m, stream), dv.to_numpy(np.int32, m, stream)
 
     def tc(self, stream=None) -> int:
         c = C.c_uint64(0)

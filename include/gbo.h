@@ -328,6 +328,24 @@ GBO_API int gbo_tc(const gbo_graph* lower, uint64_t* h_count, gbo_stream_t strea
 GBO_API int gbo_tc_device(const gbo_graph* lower, unsigned long long* d_count,
                   gbo_stream_t stream);
 
+/* Unmasked products (bsrbmm/bsrbmm.cu:244-555, bmm{4..64}_sparse): the sum
+ * of all entries of A B over the integers (A.ncols == B.nrows, same tile
+ * width, either layout), computed as sum_m colcount_A(m) * rowcount_B(m). */
+GBO_API int gbo_bmm_sum(const gbo_graph* a, const gbo_graph* b, uint64_t* h_sum,
+                gbo_stream_t stream);
+/* Sparse-output product C = A B over the integers (bsrbmm/bsrbmm.cu:
+ * 1273-1373, bmm32_sparse_symbolic/numeric): A with 32x32 ROW tiles, B with
+ * 32x32 COL tiles (as the reference packs it).  C is CSR with int64 row
+ * offsets, columns ascending in each row, and values C[i][j] = number of k
+ * with A[i][k] = B[k][j] = 1 (zeros not stored).  Two passes: gbo_spgemm_nnz
+ * writes d_rowptr[A.nrows + 1] and the entry count; the caller allocates
+ * d_colind and d_val (int32[nnz]) for gbo_spgemm_fill. */
+GBO_API int gbo_spgemm_nnz(const gbo_graph* a, const gbo_graph* b, int64_t* d_rowptr,
+                   int64_t* h_nnz, gbo_stream_t stream);
+GBO_API int gbo_spgemm_fill(const gbo_graph* a, const gbo_graph* b,
+                    const int64_t* d_rowptr, int32_t* d_colind, int32_t* d_val,
+                    gbo_stream_t stream);
+
 /* Multi-source BFS (batching): k sources (1 <= k <= 1024) traversed at once.
  * The frontier is an n x k bit matrix, so every level is one B2SR x bit
  * matrix product (OR.AND semiring).  d_levels: int32[n * k], vertex-major:

@@ -485,6 +485,64 @@ unsigned long long orc_tc_b2sr(const int* brp, const int* bci, const uint64_t* w
   return total;
 }
 
+// Sparse-output product C = A B over the integers on CSR (the math of
+// bmm32_sparse_symbolic/numeric, bsrbmm/bsrbmm.cu:1273-1373): row i of C is
+// the multiset union of B's rows m over A's row i, counted per column,
+// columns ascending.  Pass 1 (colind == NULL) writes the row lengths into
+// rowptr[1..n]; pass 2 fills colind/val at the caller's prefix rowptr.
+void orc_spgemm_csr(const int* arp, const int* aci, int n, const int* brp, const int* bci, int m,
+                    long long* rowptr, int* colind, int* val) {
+#pragma omp parallel
+  {
+    std::vector<int> acc((size_t)m, 0);
+    std::vector<int> touched;
+#pragma omp for schedule(dynamic, 64)
+    for (int i = 0; i < n; ++i) {
+      touched.clear();
+      for (int p = arp[i]; p < arp[i + 1]; ++p) {
+        const int k = aci[p];
+        for (int q = brp[k]; q < brp[k + 1]; ++q) {
+          const int j = bci[q];
+          if (acc[j]++ == 0) touched.push_back(j);
+        }
+      }
+      std::sort(touched.begin(), touched.end());
+      if (!colind) {
+        rowptr[i + 1] = (long long)touched.size();
+      } else {
+        long long o = rowptr[i];
+        for (int j : touched) {
+          colind[o] = j;
+          val[o] = acc[j];
+          ++o;
+        }
+      }
+      for (int j : touched) acc[j] = 0;
+    }
+  }
+}
+
+// bmm{4..64}_sparse (bsrbmm/bsrbmm.cu:244-555) restated on tiles: A with row
+// words, B with column words (word c = tile column c, row m at bit b-1-m);
+// the total over every block row I, A tile (I,K) and B tile (K,C) of
+// sum_r sum_c popc(A_IK[r] & B_KC[c]).
+unsigned long long orc_bmm_sum_b2sr(const int* arp, const int* aci, const uint64_t* aw, int anbr,
+                                    const int* brp, const int* bci, const uint64_t* bw, int b) {
+  unsigned long long total = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : total)
+  for (int I = 0; I < anbr; ++I)
+    for (int ta = arp[I]; ta < arp[I + 1]; ++ta) {
+      const int K = aci[ta];
+      for (int tb = brp[K]; tb < brp[K + 1]; ++tb)
+        for (int r = 0; r < b; ++r) {
+          const uint64_t A = aw[(long long)ta * b + r];
+          if (!A) continue;
+          for (int c = 0; c < b; ++c) total += popc64(A & bw[(long long)tb * b + c]);
+        }
+    }
+  return total;
+}
+
 int orc_max_threads(void) { return omp_get_max_threads(); }
 void orc_set_threads(int n) { omp_set_num_threads(n); }
 

@@ -51,6 +51,8 @@ def lib():
             "orc_verify_cc": (C.c_longlong, [_P, _P, _I, _P, C.POINTER(_I)]),
             "orc_tc_csr": (C.c_ulonglong, [_P, _P, _I]),
             "orc_tc_b2sr": (C.c_ulonglong, [_P, _P, _P, _I, _I]),
+            "orc_spgemm_csr": (None, [_P, _P, _I, _P, _P, _I, _P, _P, _P]),
+            "orc_bmm_sum_b2sr": (C.c_ulonglong, [_P, _P, _P, _I, _P, _P, _P, _I]),
             "orc_max_threads": (_I, []),
             "orc_set_threads": (None, [_I]),
         }
@@ -234,6 +236,26 @@ def tc_csr(rowptr, colind, n) -> int:
 
 def tc_b2sr(lower: B2SR) -> int:
     return int(lib().orc_tc_b2sr(*_g(lower)))
+
+
+def spgemm_csr(arp, aci, n, brp, bci, m):
+    """C = A B over the integers (CSR in, CSR out: int64 rowptr, colind, counts)."""
+    arp, aci, brp, bci = _i32(arp), _i32(aci), _i32(brp), _i32(bci)
+    rowptr = np.zeros(n + 1, np.int64)
+    lib().orc_spgemm_csr(_p(arp), _p(aci), n, _p(brp), _p(bci), m, _p(rowptr), None, None)
+    rowptr = np.cumsum(rowptr).astype(np.int64)
+    colind = np.zeros(max(1, int(rowptr[-1])), np.int32)
+    val = np.zeros_like(colind)
+    lib().orc_spgemm_csr(_p(arp), _p(aci), n, _p(brp), _p(bci), m, _p(rowptr), _p(colind), _p(val))
+    nnz = int(rowptr[-1])
+    return rowptr, colind[:nnz], val[:nnz]
+
+
+def bmm_sum_b2sr(a: B2SR, b_col: B2SR) -> int:
+    """Total of A B over tiles (A row words, B column words)."""
+    assert a.b == b_col.b and b_col.layout == 1
+    return int(lib().orc_bmm_sum_b2sr(_p(a.rowptr), _p(a.colind), _p(a.words), a.nbr,
+                                      _p(b_col.rowptr), _p(b_col.colind), _p(b_col.words), a.b))
 
 
 def set_threads(n: int):

@@ -137,3 +137,37 @@ def test_oracle_reference_fixture_readers(orc, gbo):
         nr, nc, rp, ci = orc.read_mtx_mmio(p)
         c = gbo.read_mtx(p, gbo.MTX_MMIO, 0)
         assert np.array_equal(c.rowptr, rp) and np.array_equal(c.colind, ci)
+
+
+def _rect_csr(n, m, p, seed):
+    rng = np.random.default_rng(seed)
+    d = rng.random((n, m)) < p
+    rowptr = np.concatenate([[0], np.cumsum(d.sum(1))]).astype(np.int32)
+    return rowptr, np.nonzero(d)[1].astype(np.int32), d
+
+
+def test_oracle_spgemm_and_bmm_sum_vs_scipy(gbo, orc):
+    """The oracle's sparse-output product and its tile-level total
+    (bsrbmm/bsrbmm.cu:244-555, 1273-1373) against scipy's product."""
+    import scipy.sparse as sp
+
+    cases = []
+    csr = gbo.gen_rmat(9, 8, seed=7)
+    low = csr.tril()
+    lt = low.transpose()
+    cases.append((low.rowptr, low.colind, low.nrows, low.ncols, lt.rowptr, lt.colind, lt.ncols))
+    arp, aci, _ = _rect_csr(150, 90, 0.05, 1)
+    brp, bci, _ = _rect_csr(90, 200, 0.08, 2)
+    cases.append((arp, aci, 150, 90, brp, bci, 200))
+    for arp, aci, n, k, brp, bci, m in cases:
+        A = sp.csr_matrix((np.ones(len(aci), np.int64), aci, arp), shape=(n, k))
+        B = sp.csr_matrix((np.ones(len(bci), np.int64), bci, brp), shape=(k, m))
+        Cm = (A @ B).tocsr()
+        Cm.sort_indices()
+        rp, ci, v = orc.spgemm_csr(arp, aci, n, brp, bci, m)
+        assert np.array_equal(rp, Cm.indptr) and np.array_equal(ci, Cm.indices)
+        assert np.array_equal(v, Cm.data)
+        for b in (8, 32):
+            a_t = orc.pack(arp, aci, n, k, b)
+            b_t = orc.pack(brp, bci, k, m, b, layout=1)
+            assert orc.bmm_sum_b2sr(a_t, b_t) == int(Cm.sum())
