@@ -969,6 +969,57 @@ def suite_serve(args):
     g.free()
 
 
+def suite_spgemm(args):
+    """Unmasked binary products: C = L L^T (benchmark-bsrbmm.cu's check) on
+    the king mesh 1024^2 and R-MAT 14 (seed 1): the sparse-output product
+    (both passes, int64 offsets, int32 columns and counts) and the total of
+    A B, against the oracle's CPU product on the same graphs."""
+    import ctypes as C
+
+    import gbo
+
+    oracle = _oracle()
+    res = {}
+    for name, csr in (("mesh1024", gbo.gen_king_mesh(1024)), ("rmat14", gbo.gen_rmat(14, 16, seed=1, **RMAT))):
+        low = csr.tril()
+        lt = low.transpose()
+        ga = gbo.Graph.from_csr(low, 32)
+        gb = gbo.Graph.from_csr(lt, 32, gbo.FLAG_LAYOUT_COL)
+        n = low.nrows
+        drp = gbo.DeviceBuffer(8 * (n + 1))
+        nnz = C.c_int64(0)
+        gbo.check(gbo.lib().gbo_spgemm_nnz(ga.h, gb.h, drp.ptr, C.byref(nnz), None), "spgemm_nnz")
+        m = int(nnz.value)
+        dci, dv = gbo.DeviceBuffer(4 * max(m, 1)), gbo.DeviceBuffer(4 * max(m, 1))
+
+        def run():
+            gbo.check(gbo.lib().gbo_spgemm_nnz(ga.h, gb.h, drp.ptr, C.byref(nnz), None), "spgemm_nnz")
+            gbo.check(gbo.lib().gbo_spgemm_fill(ga.h, gb.h, drp.ptr, dci.ptr, dv.ptr, None), "spgemm_fill")
+
+        ms = _timed(gbo, run, max(1, args.steps // 2), args.warmup)
+        total = ga.bmm_sum(gb)
+        sum_ms = _timed(gbo, lambda: ga.bmm_sum(gb), args.steps, args.warmup)
+        rp, ci, _ = ga.b2sr()
+        brp, _, _ = gb.b2sr()
+        pairs = int(np.diff(brp.astype(np.int64))[ci].sum())
+        t0 = time.perf_counter()
+        wrp, _, wv = oracle.spgemm_csr(low.rowptr, low.colind, n, lt.rowptr, lt.colind, lt.ncols)
+        cpu_ms = (time.perf_counter() - t0) * 1e3
+        res[name] = {"ms": ms, "nnz_c": m, "tile_pairs": pairs, "g_tile_pairs_per_s": pairs / (ms / 1e3) / 1e9,
+                     "sum": total, "sum_ms": sum_ms, "matches_oracle": bool(int(wrp[-1]) == m and int(wv.sum()) == total),
+                     "cpu_ms": cpu_ms, "cpu_threads": oracle.max_threads(), "vs_cpu": cpu_ms / ms,
+                     "nnz_l": low.nnz}
+        for x in (ga, gb):
+            x.free()
+    r = res["rmat14"]
+    _line("ms", r["ms"], "ms per product (count + fill)", False, r["ms"], args,
+          {"workload": "C = L L^T sparse output, R-MAT 14 ef16 seed 1 (lower triangle), B2SR 32 (L row words, "
+                       "L^T column words)", "nnz_l": r["nnz_l"], "nnz_c": r["nnz_c"]},
+          dtype="i32", by_graph=res,
+          cpu_baseline={"value": r["cpu_ms"], "unit": "ms", "cores": r["cpu_threads"], "kind": "port",
+                        "sample": "one oracle product (CSR Gustavson, bsrbmm/bsrbmm.cu:1273-1373 math)"})
+
+
 SUITE = {
     "sssp": lambda a: suite_config2(a, "sssp"),
     "cc": lambda a: suite_config2(a, "cc"),
@@ -978,6 +1029,7 @@ SUITE = {
     "batch": suite_batch,
     "ppr": suite_ppr,
     "serve": suite_serve,
+    "spgemm": suite_spgemm,
 }
 
 

@@ -15,13 +15,14 @@
 // row (a binary search per (block column, A tile)); here the tile pairs are
 // enumerated instead: every A tile (I, K) meets every B tile (K, C), the
 // pairs are sorted by output tile (I, C) (stable, so the K order of a tile
-// is kept), and one warp per block row walks its pairs in output-tile order,
-// summing 32x32 popcount dot products in registers (lane = row r, the B
-// tile's column words broadcast by shuffles) and emitting the non-zero
-// entries of each output tile in column order.  A count pass gives the row
-// lengths (scanned into the caller's int64 row offsets); a fill pass writes
-// column indices and counts.  Block rows are processed in ranges whose pair
-// lists fit a fixed budget.
+// is kept), and one warp per output tile sums its 32x32 popcount dot
+// products in registers (lane = row r, the B tile's column words broadcast
+// by shuffles).  The count pass adds each tile's non-zero entries per row
+// into the row lengths (scanned into the caller's int64 row offsets); the
+// fill pass gives every tile its position in each of its rows (a walk over
+// the block row's tiles in column order) and writes the entries, columns
+// ascending.  Block rows are processed in ranges whose pair lists fit a
+// fixed budget.
 #include <algorithm>
 #include <vector>
 
@@ -107,83 +108,140 @@ __global__ void k_pair_counts(const int* __restrict__ a_colind, long long nblk_a
   }
 }
 
-// Pairs of block rows [I0, I1): key (I, C), value (A tile, B tile); pair
-// positions from the per-A-tile prefix (relative to the range's first pair).
-__global__ void k_expand_pairs(const int* __restrict__ a_rowptr, const int* __restrict__ a_colind,
+// Block row of every A tile.
+__global__ void k_tile_rows(const int* __restrict__ rowptr, int nbr, int* __restrict__ trow) {
+  const unsigned lane = threadIdx.x & 31;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long I = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; I < nbr; I += nwarps)
+    for (int t = rowptr[I] + (int)lane; t < rowptr[I + 1]; t += 32) trow[t] = (int)I;
+}
+
+// Pairs of A tiles [ta0, ta1) (warp per A tile, lanes over its B tiles): key
+// (I, C), value (A tile, B tile); positions from the per-A-tile prefix,
+// relative to the range's first pair.
+__global__ void k_expand_pairs(const int* __restrict__ a_trow, const int* __restrict__ a_colind,
                                const int* __restrict__ b_rowptr, const int* __restrict__ b_colind,
-                               const long long* __restrict__ pfx, int I0, int I1, long long base,
-                               unsigned long long* __restrict__ keys,
+                               const long long* __restrict__ pfx, long long ta0, long long ta1,
+                               long long base, unsigned long long* __restrict__ keys,
                                unsigned long long* __restrict__ vals) {
   const unsigned lane = threadIdx.x & 31;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-  for (long long I = I0 + (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5); I < I1; I += nwarps) {
-    for (int ta = a_rowptr[I]; ta < a_rowptr[I + 1]; ++ta) {
-      const int K = a_colind[ta];
-      const int s0 = b_rowptr[K], s1 = b_rowptr[K + 1];
-      const long long o = pfx[ta] - base - s0;
-      for (int tb = s0 + (int)lane; tb < s1; tb += 32) {
-        keys[o + tb] = ((unsigned long long)I << 32) | (unsigned)b_colind[tb];
-        vals[o + tb] = ((unsigned long long)ta << 32) | (unsigned)tb;
-      }
+  for (long long ta = ta0 + (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5); ta < ta1; ta += nwarps) {
+    const unsigned long long I = (unsigned)a_trow[ta];
+    const int K = a_colind[ta];
+    const int s0 = b_rowptr[K], s1 = b_rowptr[K + 1];
+    const long long o = pfx[ta] - base - s0;
+    for (int tb = s0 + (int)lane; tb < s1; tb += 32) {
+      keys[o + tb] = (I << 32) | (unsigned)b_colind[tb];
+      vals[o + tb] = ((unsigned long long)ta << 32) | (unsigned)tb;
     }
   }
 }
 
-// One warp per block row of the range: walk its sorted pairs, one output
-// tile (equal keys) at a time; lane r sums row r of the tile's product.
-// FILL = false: per-row entry counts; FILL = true: entries at the row
-// offsets.
-template <bool FILL>
-__global__ void k_tile_products(const unsigned* __restrict__ a_val, const unsigned* __restrict__ b_val,
-                                const long long* __restrict__ pfx, const int* __restrict__ a_rowptr,
-                                int I0, int I1, long long base, int nrows,
-                                const unsigned long long* __restrict__ keys,
-                                const unsigned long long* __restrict__ vals,
-                                int* __restrict__ rowcnt, const long long* __restrict__ rowptr,
-                                int* __restrict__ colind_out, int* __restrict__ val_out) {
+// Output tiles of the sorted pairs: head[p] = 1 where a new key starts.
+__global__ void k_group_heads(const unsigned long long* __restrict__ keys, long long np,
+                              int* __restrict__ head) {
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < np;
+       p += (long long)gridDim.x * blockDim.x)
+    head[p] = p == 0 || keys[p] != keys[p - 1];
+}
+
+__global__ void k_group_starts(const int* __restrict__ head, const int* __restrict__ gid, long long np,
+                               int* __restrict__ gstart) {
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < np;
+       p += (long long)gridDim.x * blockDim.x)
+    if (head[p]) gstart[gid[p]] = (int)p;
+}
+
+// The 32x32 product of output tile g: lane r gets row r's 32 sums.
+__device__ __forceinline__ void tile_product(const unsigned* __restrict__ a_val, const unsigned* __restrict__ b_val,
+                                             const unsigned long long* __restrict__ vals, int p0, int p1,
+                                             unsigned lane, int (&acc)[32]) {
+#pragma unroll
+  for (int k = 0; k < 32; ++k) acc[k] = 0;
+  for (int q = p0; q < p1; ++q) {
+    const unsigned long long pv = vals[q];
+    const long long ta = (long long)(pv >> 32), tb = (long long)(pv & 0xffffffffull);
+    const unsigned a = a_val[ta * 32 + lane];   // row word r of A_IK
+    const unsigned bw = b_val[tb * 32 + lane];  // column word c = lane of B_KC
+#pragma unroll
+    for (int k = 0; k < 32; ++k) acc[k] += __popc(a & __shfl_sync(0xffffffffu, bw, k));
+  }
+}
+
+// Count kernel (warp per output tile): non-zero entries per row of the tile
+// (cnt[g][r]) and, added up, per row of C.
+__global__ void k_tile_counts(const unsigned* __restrict__ a_val, const unsigned* __restrict__ b_val,
+                              const unsigned long long* __restrict__ keys,
+                              const unsigned long long* __restrict__ vals, const int* __restrict__ gstart,
+                              int ngroups, int nrows, int* __restrict__ cnt, int* __restrict__ rowcnt) {
+  const unsigned lane = threadIdx.x & 31;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long g = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ngroups; g += nwarps) {
+    const int p0 = gstart[g], p1 = gstart[g + 1];
+    int acc[32];
+    tile_product(a_val, b_val, vals, p0, p1, lane, acc);
+    int c = 0;
+#pragma unroll
+    for (int k = 0; k < 32; ++k) c += acc[k] != 0;
+    const long long row = (long long)(keys[p0] >> 32) * 32 + lane;
+    if (row >= nrows) c = 0;
+    cnt[g * 32 + lane] = c;
+    if (rowcnt && c) atomicAdd(rowcnt + row, c);
+  }
+}
+
+// Per block row of the range (warp, lane = row): each output tile's first
+// position in its rows relative to the row's start, walking the block row's
+// tiles in column order; it replaces the tile's count in place.
+__global__ void k_tile_offsets(const long long* __restrict__ pfx, const int* __restrict__ a_rowptr,
+                               const int* __restrict__ gid, int I0, int I1, long long base,
+                               int* __restrict__ cnt) {
   const unsigned lane = threadIdx.x & 31;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
   for (long long I = I0 + (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5); I < I1; I += nwarps) {
     const long long p0 = pfx[a_rowptr[I]] - base, p1 = pfx[a_rowptr[I + 1]] - base;
-    const long long row = I * 32 + lane;
-    int cnt_row = 0;
-    long long pos = FILL && row < nrows ? rowptr[row] : 0;
-    long long p = p0;
-    while (p < p1) {
-      const unsigned C = (unsigned)(keys[p] & 0xffffffffull);
-      int acc[32];
-#pragma unroll
-      for (int k = 0; k < 32; ++k) acc[k] = 0;
-      long long q = p;
-      for (; q < p1 && (unsigned)(keys[q] & 0xffffffffull) == C; ++q) {
-        const unsigned long long pv = vals[q];
-        const long long ta = (long long)(pv >> 32), tb = (long long)(pv & 0xffffffffull);
-        const unsigned a = a_val[ta * 32 + lane];   // row word r of A_IK
-        const unsigned bw = b_val[tb * 32 + lane];  // column word c = lane of B_KC
-#pragma unroll
-        for (int k = 0; k < 32; ++k) acc[k] += __popc(a & __shfl_sync(0xffffffffu, bw, k));
-      }
-      if (row < nrows) {
-#pragma unroll
-        for (int k = 0; k < 32; ++k) {
-          if (acc[k]) {
-            if (FILL) {
-              colind_out[pos] = (int)(C * 32 + k);
-              val_out[pos] = acc[k];
-              ++pos;
-            } else {
-              ++cnt_row;
-            }
-          }
-        }
-      }
-      p = q;
+    if (p0 >= p1) continue;
+    const int g0 = gid[p0], g1 = gid[p1];  // gid: exclusive count of heads, gid[np] = G
+    int rel = 0;
+    for (int g = g0; g < g1; ++g) {
+      const int c = cnt[(long long)g * 32 + lane];
+      cnt[(long long)g * 32 + lane] = rel;
+      rel += c;
     }
-    if (!FILL && row < nrows) rowcnt[row] = cnt_row;
   }
 }
 
-// Stream-ordered device buffer freed on scope exit (alloc replaces it).
+// Fill kernel (warp per output tile): the non-zero entries of row r of the
+// tile at rowptr[row] + its offset, columns ascending.
+__global__ void k_tile_fill(const unsigned* __restrict__ a_val, const unsigned* __restrict__ b_val,
+                            const unsigned long long* __restrict__ keys,
+                            const unsigned long long* __restrict__ vals, const int* __restrict__ gstart,
+                            int ngroups, int nrows, const int* __restrict__ off,
+                            const long long* __restrict__ rowptr, int* __restrict__ colind_out,
+                            int* __restrict__ val_out) {
+  const unsigned lane = threadIdx.x & 31;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long g = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ngroups; g += nwarps) {
+    const int p0 = gstart[g], p1 = gstart[g + 1];
+    int acc[32];
+    tile_product(a_val, b_val, vals, p0, p1, lane, acc);
+    const unsigned long long key = keys[p0];
+    const long long row = (long long)(key >> 32) * 32 + lane;
+    if (row >= nrows) continue;
+    const int C = (int)(key & 0xffffffffull);
+    long long pos = rowptr[row] + off[g * 32 + lane];
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+      if (acc[k]) {
+        colind_out[pos] = C * 32 + k;
+        val_out[pos] = acc[k];
+        ++pos;
+      }
+    }
+  }
+}
+
 struct DevBuf {
   void* p = nullptr;
   cudaStream_t s = nullptr;
@@ -200,7 +258,7 @@ struct DevBuf {
   }
 };
 
-constexpr long long kPairBudget = 1ll << 25;  // tile pairs per range (512 MB of keys and values)
+constexpr long long kPairBudget = 1ll << 25;  // tile pairs per range (keys and values: 1 GB with the sort's second buffer)
 
 int check_pair(const gbo_graph* a, const gbo_graph* b) {
   if (!a || !b) return fail(GBO_ERR_INVALID, "NULL graph");
@@ -209,21 +267,26 @@ int check_pair(const gbo_graph* a, const gbo_graph* b) {
   return GBO_OK;
 }
 
-// Count (FILL = false) or fill pass of the sparse product.
+// Count (fill = false: per-row entry counts into rowcnt) or fill pass of
+// the sparse product.
 int spgemm_pass(const gbo_graph* a, const gbo_graph* b, bool fill, int* rowcnt, const long long* rowptr,
                 int* colind_out, int* val_out, cudaStream_t s) {
   if (a->b != 32 || a->layout != GBO_LAYOUT_ROW || b->layout != GBO_LAYOUT_COL)
     return fail(GBO_ERR_UNSUPPORTED, "sparse-output product: A with 32x32 ROW tiles, B with 32x32 COL tiles");
   const long long na = a->nblk;
-  DevBuf cnt, pfx, tot;
+  DevBuf cnt, pfx, tot, trow;
   GBO_TRY(cnt.alloc(sizeof(int) * (size_t)std::max(na, 1ll), s));
   GBO_TRY(pfx.alloc(sizeof(long long) * ((size_t)na + 1), s));
   GBO_TRY(tot.alloc(sizeof(long long), s));
+  GBO_TRY(trow.alloc(sizeof(int) * (size_t)std::max(na, 1ll), s));
   int* d_cnt = static_cast<int*>(cnt.p);
   long long* d_pfx = static_cast<long long*>(pfx.p);
+  int* d_trow = static_cast<int*>(trow.p);
+  const int wgrid = 8 * num_sms();  // blocks of 8 warps, grid-stride
   if (na > 0) {
     k_pair_counts<<<(unsigned)std::min<long long>((na + 255) / 256, 4096), 256, 0, s>>>(
         a->colind, na, b->rowptr, d_cnt);
+    k_tile_rows<<<wgrid, 256, 0, s>>>(a->rowptr, a->nbr, d_trow);
     GBO_CUDA_TRY(cudaGetLastError());
   }
   GBO_TRY(exclusive_scan_i32_to_i64(d_cnt, d_pfx, na, static_cast<long long*>(tot.p), s));
@@ -235,8 +298,10 @@ int spgemm_pass(const gbo_graph* a, const gbo_graph* b, bool fill, int* rowcnt, 
   GBO_CUDA_TRY(cudaStreamSynchronize(s));
   if (!fill && a->nrows > 0) GBO_CUDA_TRY(cudaMemsetAsync(rowcnt, 0, sizeof(int) * (size_t)a->nrows, s));
   long long cap = 0;
-  DevBuf kbuf[2], vbuf[2], temp;
+  DevBuf kbuf[2], vbuf[2], temp, head, gid, gstart, tcnt, ng;
   size_t temp_bytes = 0;
+  long long tcap = 0;  // output tiles the per-tile counts can hold
+  GBO_TRY(ng.alloc(sizeof(long long), s));
   for (int I0 = 0; I0 < a->nbr;) {
     int I1 = I0 + 1;
     while (I1 < a->nbr && hp[arp[I1 + 1]] - hp[arp[I0]] <= kPairBudget) ++I1;
@@ -247,6 +312,9 @@ int spgemm_pass(const gbo_graph* a, const gbo_graph* b, bool fill, int* rowcnt, 
           GBO_TRY(kbuf[k].alloc(sizeof(unsigned long long) * (size_t)np, s));
           GBO_TRY(vbuf[k].alloc(sizeof(unsigned long long) * (size_t)np, s));
         }
+        GBO_TRY(head.alloc(sizeof(int) * (size_t)np, s));
+        GBO_TRY(gid.alloc(sizeof(int) * ((size_t)np + 1), s));
+        GBO_TRY(gstart.alloc(sizeof(int) * ((size_t)np + 1), s));
         cap = np;
         size_t need = 0;
         GBO_CUDA_TRY(cub::DeviceRadixSort::SortPairs(
@@ -261,24 +329,41 @@ int spgemm_pass(const gbo_graph* a, const gbo_graph* b, bool fill, int* rowcnt, 
       auto* v0 = static_cast<unsigned long long*>(vbuf[0].p);
       auto* k1 = static_cast<unsigned long long*>(kbuf[1].p);
       auto* v1 = static_cast<unsigned long long*>(vbuf[1].p);
-      const int nrow = I1 - I0;
-      const int grid = (int)std::min<long long>(((long long)nrow + 7) / 8, 8LL * num_sms());
-      k_expand_pairs<<<grid, 256, 0, s>>>(a->rowptr, a->colind, b->rowptr, b->colind, d_pfx, I0, I1, base,
-                                          k0, v0);
+      int* d_head = static_cast<int*>(head.p);
+      int* d_gid = static_cast<int*>(gid.p);
+      int* d_gstart = static_cast<int*>(gstart.p);
+      k_expand_pairs<<<wgrid, 256, 0, s>>>(d_trow, a->colind, b->rowptr, b->colind, d_pfx, arp[I0], arp[I1],
+                                           base, k0, v0);
       GBO_CUDA_TRY(cudaGetLastError());
       size_t tb = temp_bytes;
       GBO_CUDA_TRY(cub::DeviceRadixSort::SortPairs(temp.p, tb, k0, k1, v0, v1, (int)np, 0, 64, s));
-      if (fill)
-        k_tile_products<true><<<grid, 256, 0, s>>>(static_cast<const unsigned*>(a->val),
-                                                   static_cast<const unsigned*>(b->val), d_pfx, a->rowptr,
-                                                   I0, I1, base, a->nrows, k1, v1, nullptr, rowptr,
-                                                   colind_out, val_out);
-      else
-        k_tile_products<false><<<grid, 256, 0, s>>>(static_cast<const unsigned*>(a->val),
-                                                    static_cast<const unsigned*>(b->val), d_pfx, a->rowptr,
-                                                    I0, I1, base, a->nrows, k1, v1, rowcnt, nullptr, nullptr,
-                                                    nullptr);
+      // output tiles: heads, their ids (exclusive scan) and first pairs
+      const unsigned eg = (unsigned)std::min<long long>((np + 255) / 256, 8192);
+      k_group_heads<<<eg, 256, 0, s>>>(k1, np, d_head);
+      GBO_TRY(exclusive_scan_i32(d_head, d_gid, np, static_cast<long long*>(ng.p), s));
+      k_group_starts<<<eg, 256, 0, s>>>(d_head, d_gid, np, d_gstart);
       GBO_CUDA_TRY(cudaGetLastError());
+      // d_gid[np] is the number of output tiles; gstart[G] = np
+      int G = 0;
+      GBO_CUDA_TRY(cudaMemcpyAsync(&G, d_gid + np, sizeof(int), cudaMemcpyDeviceToHost, s));
+      GBO_CUDA_TRY(cudaStreamSynchronize(s));
+      const int npi = (int)np;
+      GBO_CUDA_TRY(cudaMemcpyAsync(d_gstart + G, &npi, sizeof(int), cudaMemcpyHostToDevice, s));
+      if (G > tcap) {
+        GBO_TRY(tcnt.alloc(sizeof(int) * 32 * (size_t)G, s));
+        tcap = G;
+      }
+      int* d_tcnt = static_cast<int*>(tcnt.p);
+      const auto* av = static_cast<const unsigned*>(a->val);
+      const auto* bv = static_cast<const unsigned*>(b->val);
+      k_tile_counts<<<wgrid, 256, 0, s>>>(av, bv, k1, v1, d_gstart, G, a->nrows, d_tcnt, fill ? nullptr : rowcnt);
+      if (fill) {
+        k_tile_offsets<<<wgrid, 256, 0, s>>>(d_pfx, a->rowptr, d_gid, I0, I1, base, d_tcnt);
+        k_tile_fill<<<wgrid, 256, 0, s>>>(av, bv, k1, v1, d_gstart, G, a->nrows, d_tcnt, rowptr, colind_out,
+                                          val_out);
+      }
+      GBO_CUDA_TRY(cudaGetLastError());
+      GBO_CUDA_TRY(cudaStreamSynchronize(s));  // npi lives on this frame
     }
     I0 = I1;
   }
