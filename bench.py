@@ -1020,6 +1020,56 @@ def suite_spgemm(args):
                         "sample": "one oracle product (CSR Gustavson, bsrbmm/bsrbmm.cu:1273-1373 math)"})
 
 
+def suite_ingest(args):
+    """Matrix Market ingestion: R-MAT 20 (seed 0) written as a symmetric
+    pattern .mtx (one triangle, 1-based), read by the host reader
+    (gbo_read_mtx, readMtx semantics) and by the GPU reader
+    (gbo_read_mtx_device), and packed by gbo_graph_from_mtx."""
+    import tempfile
+
+    import pandas as pd
+
+    import gbo
+
+    csr = gbo.gen_rmat(20, 16, seed=0, **RMAT)
+    rows = np.repeat(np.arange(csr.nrows, dtype=np.int64), np.diff(csr.rowptr))
+    keep = rows >= csr.colind
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "rmat20.mtx")
+        with open(path, "w") as f:
+            f.write("%%MatrixMarket matrix coordinate pattern symmetric\n")
+            f.write(f"{csr.nrows} {csr.ncols} {int(keep.sum())}\n")
+        pd.DataFrame({"i": rows[keep] + 1, "j": csr.colind[keep].astype(np.int64) + 1}).to_csv(
+            path, sep=" ", header=False, index=False, mode="a")
+        size = os.path.getsize(path)
+        t0 = time.perf_counter()
+        host = gbo.read_mtx(path)
+        host_s = time.perf_counter() - t0
+        dev = gbo.read_mtx_device(path)  # warm-up (and the check below)
+        same = bool(np.array_equal(host.rowptr, dev.rowptr) and np.array_equal(host.colind, dev.colind))
+        ts = []
+        for _ in range(max(1, args.steps // 2)):
+            t0 = time.perf_counter()
+            gbo.read_mtx_device(path)
+            ts.append(time.perf_counter() - t0)
+        dev_s = float(np.median(ts))
+        gs = []
+        for _ in range(1 + max(1, args.steps // 2)):  # the first call is a warm-up
+            t0 = time.perf_counter()
+            g = gbo.Graph.from_mtx(path, gbo.MTX_READMTX, 0, 32, gbo.FLAG_SYMMETRIC)
+            gbo.sync()
+            gs.append(time.perf_counter() - t0)
+            g.free()
+        graph_s = float(np.median(gs[1:]))
+    _line("GB/s", size / dev_s / 1e9, "GB/s of .mtx text parsed into a device CSR", True, dev_s * 1e3, args,
+          {"workload": "R-MAT 20 ef16 seed 0, symmetric pattern .mtx (lower triangle), readMtx semantics",
+           "file_bytes": size, "lines": int(keep.sum()), "nnz": host.nnz},
+          dtype="u8", gpu_read_s=dev_s, host_read_s=host_s, speedup=host_s / dev_s, graph_from_mtx_s=graph_s,
+          same_csr_as_host=same,
+          cpu_baseline={"value": size / host_s / 1e9, "unit": "GB/s", "cores": 1, "kind": "port",
+                        "sample": "one gbo_read_mtx of the same file (host parser, readMtx.hpp:351-423 semantics)"})
+
+
 SUITE = {
     "sssp": lambda a: suite_config2(a, "sssp"),
     "cc": lambda a: suite_config2(a, "cc"),
@@ -1030,6 +1080,7 @@ SUITE = {
     "ppr": suite_ppr,
     "serve": suite_serve,
     "spgemm": suite_spgemm,
+    "ingest": suite_ingest,
 }
 
 

@@ -8,4 +8,23 @@
 namespace gbo {
 int fail(int status, const std::string& msg);
 void clear_error();
+
+#define GBO_HOST_TRY(call)          \
+  do {                              \
+    int s_ = (call);                \
+    if (s_ != GBO_OK) return s_;    \
+  } while (0)
+
+// Matrix Market banner and size line (host_io.cpp).
+struct MtxHeader {
+  bool symmetric = false;  // 'symmetric'
+  bool hermitian = false;
+  bool skew = false;
+  bool pattern = false, real = false, integer = false, complex_ = false;
+  int nrows = 0, ncols = 0;
+  long long nnz = 0;
+};
+int parse_mtx_header(const char* p, const char* end, MtxHeader* h, const char** entries);
+// GRB_UTIL_REMOVE_SELFLOOP (readMtx.hpp:155): drop self-loops unless set to 0.
+bool env_remove_self_loops();
 }  // namespace gbo

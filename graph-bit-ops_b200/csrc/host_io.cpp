@@ -123,15 +123,6 @@ int csr_from_pairs(const std::vector<int>& rows, const std::vector<int>& cols, i
 }
 
 // --------------------------------------------------------- Matrix Market
-struct MtxHeader {
-  bool symmetric = false;  // 'symmetric'
-  bool hermitian = false;
-  bool skew = false;
-  bool pattern = false, real = false, integer = false, complex_ = false;
-  int nrows = 0, ncols = 0;
-  long long nnz = 0;
-};
-
 bool read_file(const char* path, std::string* data) {
   FILE* f = fopen(path, "rb");
   if (!f) return false;
@@ -149,11 +140,11 @@ std::string lower(std::string s) {
   return s;
 }
 
-int parse_mtx(const char* path, MtxHeader* h, std::vector<int>* I, std::vector<int>* J) {
-  std::string data;
-  if (!read_file(path, &data)) return fail(GBO_ERR_IO, std::string("cannot read ") + path);
-  const char* p = data.c_str();
-  const char* end = p + data.size();
+}  // namespace
+
+// Banner, comments and size line of a Matrix Market text in [p, end);
+// *entries gets the position right after the size line's numbers.
+int parse_mtx_header(const char* p, const char* end, MtxHeader* h, const char** entries) {
   // banner
   const char* nl = (const char*)memchr(p, '\n', (size_t)(end - p));
   std::string banner(p, nl ? nl : end);
@@ -183,7 +174,26 @@ int parse_mtx(const char* path, MtxHeader* h, std::vector<int>* I, std::vector<i
   h->nrows = (int)r;
   h->ncols = (int)c;
   h->nnz = z;
-  p = e2;
+  *entries = e2;
+  return GBO_OK;
+}
+
+bool env_remove_self_loops() {
+  // GRB_UTIL_REMOVE_SELFLOOP, default true (readMtx.hpp:155).
+  const char* v = getenv("GRB_UTIL_REMOVE_SELFLOOP");
+  if (!v) return true;
+  return atoi(v) != 0;
+}
+
+namespace {
+
+int parse_mtx(const char* path, MtxHeader* h, std::vector<int>* I, std::vector<int>* J) {
+  std::string data;
+  if (!read_file(path, &data)) return fail(GBO_ERR_IO, std::string("cannot read ") + path);
+  const char* p = nullptr;
+  const char* end = data.c_str() + data.size();
+  GBO_HOST_TRY(parse_mtx_header(data.c_str(), end, h, &p));
+  const long long r = h->nrows, c = h->ncols, z = h->nnz;
   I->resize((size_t)z);
   J->resize((size_t)z);
   for (long long k = 0; k < z; ++k) {
@@ -201,13 +211,6 @@ int parse_mtx(const char* path, MtxHeader* h, std::vector<int>* I, std::vector<i
     p = eol ? eol + 1 : end;
   }
   return GBO_OK;
-}
-
-bool env_remove_self_loops() {
-  // GRB_UTIL_REMOVE_SELFLOOP, default true (readMtx.hpp:155).
-  const char* v = getenv("GRB_UTIL_REMOVE_SELFLOOP");
-  if (!v) return true;
-  return atoi(v) != 0;
 }
 
 }  // namespace

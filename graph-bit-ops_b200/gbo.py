@@ -157,6 +157,9 @@ _SIGS = {
     "gbo_server_destroy": (_I, [_P]),
     "gbo_read_mtx": (_I, [C.c_char_p, _I, _I, C.POINTER(C.POINTER(CsrStruct))]),
     "gbo_csr_free": (_I, [C.POINTER(CsrStruct)]),
+    "gbo_read_mtx_device": (_I, [C.c_char_p, _I, _I, C.POINTER(_P), C.POINTER(_P), C.POINTER(_I),
+                                 C.POINTER(_I), C.POINTER(C.c_int64), _P]),
+    "gbo_graph_from_mtx": (_I, [C.c_char_p, _I, _I, _I, _I, _P, C.POINTER(_P)]),
     "gbo_csr_transpose": (_I, [C.POINTER(CsrStruct), C.POINTER(C.POINTER(CsrStruct))]),
     "gbo_csr_tril": (_I, [C.POINTER(CsrStruct), C.POINTER(C.POINTER(CsrStruct))]),
     "gbo_csr_from_edges": (_I, [_P, _P, C.c_int64, _I, _I, _I, C.POINTER(C.POINTER(CsrStruct))]),
@@ -367,6 +370,21 @@ class Csr:
         return np.diff(self.rowptr)
 
 
+def read_mtx_device(path: str, mode: int = MTX_READMTX, directed: int = 0) -> Csr:
+    """gbo_read_mtx_device (parsed on the GPU); the CSR is copied back."""
+    rp, ci = C.c_void_p(), C.c_void_p()
+    nr, nc, nz = C.c_int(0), C.c_int(0), C.c_int64(0)
+    check(lib().gbo_read_mtx_device(os.fsencode(path), mode, directed, C.byref(rp), C.byref(ci), C.byref(nr),
+                                    C.byref(nc), C.byref(nz), None), "read_mtx_device")
+    try:
+        rowptr = device_to_numpy(rp.value, np.int32, nr.value + 1)
+        colind = device_to_numpy(ci.value, np.int32, nz.value) if nz.value else np.zeros(0, np.int32)
+    finally:
+        lib().gbo_free(rp.value)
+        lib().gbo_free(ci.value)
+    return Csr(rowptr, colind, nr.value, nc.value)
+
+
 def read_mtx(path: str, mode: int = MTX_READMTX, directed: int = 0) -> Csr:
     out = C.POINTER(CsrStruct)()
     check(lib().gbo_read_mtx(path.encode(), mode, directed, C.byref(out)), "read_mtx")
@@ -454,6 +472,15 @@ class Graph:
                                         colind.ptr, val.ptr, outdeg.ptr if outdeg else None,
                                         stream, C.byref(p)), "graph_wrap_b2sr")
         return cls(p.value, keep=(rowptr, colind, val, outdeg))
+
+    @classmethod
+    def from_mtx(cls, path: str, mode: int = MTX_READMTX, directed: int = 0, tile_bits: int = 32,
+                 flags: int = 0, stream=None) -> "Graph":
+        """Parse a Matrix Market file on the GPU and pack it (gbo_graph_from_mtx)."""
+        p = C.c_void_p()
+        check(lib().gbo_graph_from_mtx(os.fsencode(path), mode, directed, tile_bits, flags, stream, C.byref(p)),
+              "graph_from_mtx")
+        return cls(p.value)
 
     @classmethod
     def load(cls, path: str, flags: int = 0, stream=None) -> "Graph":

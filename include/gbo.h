@@ -454,6 +454,18 @@ enum { GBO_MTX_READMTX = 0, GBO_MTX_MMIO = 1 };
  * for a binary matrix). */
 GBO_API int gbo_read_mtx(const char* path, int mode, int directed, gbo_csr** out);
 GBO_API int gbo_csr_free(gbo_csr* csr);
+/* The same readers on the GPU (SURVEY next item: GPU ingestion): the entry
+ * lines are parsed in parallel and the CSR is built in device memory --
+ * identical to gbo_read_mtx's for well-formed files (each line is parsed on
+ * its own).  d_rowptr (int32[nrows+1]) and d_colind (int32[nnz]) are
+ * allocated here; free them with gbo_free.  gbo_graph_from_mtx packs the
+ * parsed CSR straight into a graph (flags as gbo_graph_from_csr). */
+GBO_API int gbo_read_mtx_device(const char* path, int mode, int directed,
+                        int** d_rowptr, int** d_colind, int* nrows, int* ncols,
+                        int64_t* nnz, gbo_stream_t stream);
+GBO_API int gbo_graph_from_mtx(const char* path, int mode, int directed,
+                       int tile_bits, int flags, gbo_stream_t stream,
+                       gbo_graph** out);
 /* CSC of a host CSR (readMtx.hpp:319-345), rows of the result sorted. */
 GBO_API int gbo_csr_transpose(const gbo_csr* in, gbo_csr** out);
 /* Keep entries with row >= col (tril_csr, bsrbmm/bsrbmm.cu:1416). */
