@@ -21,6 +21,10 @@
 namespace gbo {
 namespace ms {
 
+// Per-split-row accumulators (nsplit x 32 x kw words, zeroed) and the split
+// index of every slot, for the step/finish kernels (msbfs.cu).
+int split_state(const gbo_graph* g, int kw, uint32_t** acc, int** slot_split, cudaStream_t s);
+
 constexpr int kTPB = 256;
 constexpr int kWarps = kTPB / 32;
 
@@ -34,7 +38,9 @@ struct Args {
   int* levels;
   int k;
   int* ctl;  // iter, done, ticket, max_iter, count (u64 at ctl + 4)
-  uint32_t* scratch;
+  uint32_t* split_acc;     // per split block row: 32 x KW words OR-ed by its items, zero
+                           // between levels (the finish kernel reads and clears them)
+  const int* slot_split;   // split index of every work item's slot
   uint32_t* slot_any;  // optional: OR of the new bits of every source word
   const uint32_t* live;  // optional: rows of P with an entry (others can never be reached)
   const uint32_t* active;  // optional: source columns still traversing (kw words); a row
@@ -256,17 +262,17 @@ __global__ void __launch_bounds__(kTPB, 4) k_step(Args a) {
       }
       flush();
       if (it.slot >= 0) {
-        uint32_t* dst = a.scratch + (size_t)it.slot * 32 * KW;
-        for (int q = lane; q < 32 * KW; q += 32) dst[q] = acc[q];
+        // a piece of a split block row: OR its non-zero words into the row's
+        // accumulator (pieces of one row OR in any order)
+        uint32_t* dst = a.split_acc + (size_t)a.slot_split[it.slot] * 32 * KW;
+        for (int q = lane; q < 32 * KW; q += 32)
+          if (acc[q]) atomicOr(dst + q, acc[q]);
       } else {
         block_row_epilogue<KW>(a, it.row, lvl, vrow, lane,
                                [&](int r, int ww) { return acc[r * KW + ww]; }, cnt);
       }
     } else if (it.slot < 0 && lane == 0) {
       a.fbits[(size_t)((lvl + 1) & 1) * (v.nbr + 1) + it.row] = 0u;
-    } else if (it.slot >= 0) {
-      uint32_t* dst = a.scratch + (size_t)it.slot * 32 * KW;
-      for (int q = lane; q < 32 * KW; q += 32) dst[q] = 0u;
     }
   }
   // block count without a closing barrier: warps add and leave; the last
@@ -298,15 +304,11 @@ __global__ void __launch_bounds__(kTPB) k_finish(Args a) {
     const gbo_split sp = v.splits[wid];
     const uint32_t vrow = a.vfull[sp.row];
     if (vrow != 0xffffffffu) {
-      const uint32_t* sc = a.scratch;
-      block_row_epilogue<KW>(
-          a, sp.row, lvl, vrow, lane,
-          [&](int r, int ww) {
-            uint32_t x = 0;
-            for (int q = 0; q < sp.nslots; ++q) x |= sc[(size_t)(sp.slot0 + q) * 32 * KW + r * KW + ww];
-            return x;
-          },
-          cnt);
+      uint32_t* sacc = a.split_acc + (size_t)wid * 32 * KW;
+      block_row_epilogue<KW>(a, sp.row, lvl, vrow, lane, [&](int r, int ww) { return sacc[r * KW + ww]; },
+                             cnt);
+      __syncwarp();
+      for (int q = lane; q < 32 * KW; q += 32) sacc[q] = 0u;  // zero for the next level
     } else if (lane == 0) {
       a.fbits[(size_t)((lvl + 1) & 1) * (v.nbr + 1) + sp.row] = 0u;
     }

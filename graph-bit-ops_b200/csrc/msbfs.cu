@@ -26,7 +26,8 @@ struct MsState {
   uint32_t* V = nullptr;  // n * kw
   uint32_t* fbits = nullptr;
   uint32_t* vfull = nullptr;
-  uint32_t* scratch = nullptr;
+  uint32_t* split_acc = nullptr;
+  int* slot_split = nullptr;
   int* srcs = nullptr;
   int* ctl = nullptr;
   int* h_ctl = nullptr;
@@ -54,7 +55,8 @@ ms::Args make_args(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
   a.levels = d_levels;
   a.k = k;
   a.ctl = m.ctl;
-  a.scratch = m.scratch;
+  a.split_acc = m.split_acc;
+  a.slot_split = m.slot_split;
   a.slot_any = nullptr;
   a.active = nullptr;
   a.live = m.live;
@@ -111,13 +113,14 @@ int msbfs_impl(gbo_graph* g, const int* h_srcs, int k, int32_t* d_levels, int* h
     m.exec = nullptr;
     cudaFree(m.F);
     cudaFree(m.V);
-    cudaFree(m.scratch);
-    m.F = m.V = m.scratch = nullptr;
+    cudaFree(m.split_acc);
+    cudaFree(m.slot_split);
+    m.F = m.V = m.split_acc = nullptr;
+    m.slot_split = nullptr;
     m.kw = 0;
     GBO_CUDA_TRY(cudaMalloc(&m.F, sizeof(uint32_t) * 2 * (size_t)n * kw + 16));
     GBO_CUDA_TRY(cudaMalloc(&m.V, sizeof(uint32_t) * (size_t)n * kw + 16));
-    GBO_CUDA_TRY(cudaMalloc(&m.scratch,
-                            sizeof(uint32_t) * (size_t)(g->nslots > 0 ? g->nslots : 1) * 32 * kw));
+    GBO_TRY(ms::split_state(g, kw, &m.split_acc, &m.slot_split, s));
     m.kw = kw;
   }
   if (k > m.ksrc) {
@@ -193,6 +196,32 @@ int ms_last_run(const gbo_graph* g, gbo_run_stats* st) {
   return GBO_OK;
 }
 
+namespace ms {
+namespace {
+__global__ void k_slot_split(const gbo_split* __restrict__ splits, int nsplit, int* __restrict__ map) {
+  const unsigned lane = threadIdx.x & 31;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nsplit; w += nwarps) {
+    const gbo_split sp = splits[w];
+    for (int q = (int)lane; q < sp.nslots; q += 32) map[sp.slot0 + q] = (int)w;
+  }
+}
+}  // namespace
+
+int split_state(const gbo_graph* g, int kw, uint32_t** acc, int** slot_split, cudaStream_t s) {
+  const size_t accw = (size_t)(g->nsplit > 0 ? g->nsplit : 1) * 32 * (size_t)kw;
+  GBO_CUDA_TRY(cudaMalloc(acc, sizeof(uint32_t) * accw));
+  GBO_CUDA_TRY(cudaMemsetAsync(*acc, 0, sizeof(uint32_t) * accw, s));
+  GBO_CUDA_TRY(cudaMalloc(slot_split, sizeof(int) * (size_t)(g->nslots > 0 ? g->nslots : 1)));
+  if (g->nsplit > 0) {
+    const unsigned grid = (unsigned)std::min<long long>(((long long)g->nsplit + 7) / 8, 4096);
+    k_slot_split<<<grid, 256, 0, s>>>(g->splits, g->nsplit, *slot_split);
+    GBO_CUDA_TRY(cudaGetLastError());
+  }
+  return GBO_OK;
+}
+}  // namespace ms
+
 void free_ms_state(gbo_graph* g) {
   MsState* m = reinterpret_cast<MsState*>(g->ms);
   if (!m) return;
@@ -203,7 +232,8 @@ void free_ms_state(gbo_graph* g) {
   cudaFree(m->V);
   cudaFree(m->fbits);
   cudaFree(m->vfull);
-  cudaFree(m->scratch);
+  cudaFree(m->split_acc);
+  cudaFree(m->slot_split);
   cudaFree(m->srcs);
   cudaFree(m->ctl);
   cudaFreeHost(m->h_ctl);

@@ -403,7 +403,8 @@ struct gbo_server {
   int dev = 0;
   // BFS engine (levels grouped 8 sources per 32-byte sector)
   int kb = 0, kw = 0;
-  uint32_t *F = nullptr, *V = nullptr, *fbits = nullptr, *vfull = nullptr, *scratch = nullptr;
+  uint32_t *F = nullptr, *V = nullptr, *fbits = nullptr, *vfull = nullptr, *split_acc = nullptr;
+  int* slot_split = nullptr;
   int* levels = nullptr;
   int* ctl = nullptr;
   uint32_t* slot_any = nullptr;
@@ -466,7 +467,8 @@ ms::Args bfs_args(gbo_server* S) {
   a.levels = S->levels;
   a.k = S->kb;
   a.ctl = S->ctl;
-  a.scratch = S->scratch;
+  a.split_acc = S->split_acc;
+  a.slot_split = S->slot_split;
   a.slot_any = S->slot_any;
   a.live = S->live;
   a.active = S->d_active;
@@ -832,7 +834,8 @@ void destroy_server(gbo_server* S) {
   cudaFree(S->V);
   cudaFree(S->fbits);
   cudaFree(S->vfull);
-  cudaFree(S->scratch);
+  cudaFree(S->split_acc);
+  cudaFree(S->slot_split);
   cudaFree(S->levels);
   cudaFree(S->ctl);
   cudaFree(S->slot_any);
@@ -903,7 +906,10 @@ extern "C" int gbo_server_create(const gbo_graph* gc, int bfs_slots, int ppr_slo
       cu(cudaMalloc(&S->V, sizeof(uint32_t) * n * kw + 16), "V");
       cu(cudaMalloc(&S->fbits, sizeof(uint32_t) * 2 * (size_t)(g->nbr + 1)), "fbits");
       cu(cudaMalloc(&S->vfull, sizeof(uint32_t) * (size_t)(g->nbr + 1)), "vfull");
-      cu(cudaMalloc(&S->scratch, sizeof(uint32_t) * (size_t)(g->nslots > 0 ? g->nslots : 1) * 32 * kw), "scratch");
+      {
+        const int st = ms::split_state(g, kw, &S->split_acc, &S->slot_split, S->s[0]);
+        if (st != GBO_OK) throw st;
+      }
       cu(cudaMalloc(&S->levels, sizeof(int) * n * S->kb + 16), "levels");
       cu(cudaMalloc(&S->ctl, 64), "ctl");
       cu(cudaMalloc(&S->slot_any, sizeof(uint32_t) * kw), "slot_any");
