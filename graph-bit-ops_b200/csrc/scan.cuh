@@ -213,26 +213,21 @@ __device__ __forceinline__ unsigned warp_transpose32(unsigned x, unsigned lane) 
 }
 
 // fold_row_cols (below) for b = 32 tiles with packed row words.  Per batch
-// of 32 tiles the occupancy words are transposed, so lane r holds the set of
-// the batch's tiles in which row r is non-empty and visits only those, U at
-// a time (on sparse graphs a row is non-empty in one or two tiles of a
-// batch, where the per-tile walk would keep 30 of 32 lanes idle).  Per row
-// the terms come in tile order: the first set column of each of the U
-// tiles, then the other set columns of each.
+// of 32 tiles the occupancy words are transposed (lane r: the tiles where
+// row r is non-empty), and the batch's non-empty words are dealt out to the
+// lanes in row-major order, 32 per round: lane p takes word p (its row by a
+// binary search over the rows' prefix counts, its tile as the k-th tile of
+// that row), folds the word's columns (first set column, then the others in
+// order), and a segmented scan over the lanes of each row's run (the runs
+// are contiguous) leaves the run's fold in its last lane, which the row's
+// own lane folds into its accumulator.  Every lane does one word per round
+// whatever the rows' lengths, and the order of every fold is fixed by the
+// graph alone.
 template <int U, typename Acc, typename Term, typename Comb>
 __device__ __forceinline__ void fold_row_cols_t32(const GView& v, int t0, int t1, long long wb,
                                                   unsigned lane, Term term, Comb comb, Acc& acc) {
-  using T = decltype(term(0ll));
   const unsigned* __restrict__ words = v.rowword;
   const unsigned* __restrict__ rm = v.rowmask;
-  const unsigned below = (1u << lane) - 1u;
-  auto rest = [&](unsigned a, long long base) {
-    while (a) {
-      const int j = __clz((int)a);
-      a &= ~(0x80000000u >> j);
-      comb(acc, term(base + j));
-    }
-  };
   int cn = t0 + (int)lane < t1 ? v.colind[t0 + lane] : 0;
   unsigned mn = t0 + (int)lane < t1 ? rm[t0 + lane] : 0u;
   for (int b0 = t0; b0 < t1; b0 += 32) {
@@ -244,44 +239,58 @@ __device__ __forceinline__ void fold_row_cols_t32(const GView& v, int t0, int t1
       mn = t < t1 ? rm[t] : 0u;
     }
     const int mc = __popc(m);
-    const int mi = warp_incl_sum(mc, lane);
-    const int off = mi - mc;  // lane j: tile j's first word, relative to wb
+    const int off = warp_incl_sum(mc, lane) - mc;  // lane j: tile j's first word, relative to wb
     const long long wbat = wb;
-    wb += __shfl_sync(0xffffffffu, mi, 31);
-    unsigned tl = warp_transpose32(m, lane);  // lane r: tiles of the batch where row r is non-empty
-    while (__any_sync(0xffffffffu, tl != 0u)) {
-      int jj[U];
+    const unsigned tl = warp_transpose32(m, lane);  // lane r: tiles of the batch where row r is non-empty
+    const int rc = __popc(tl);
+    const int rincl = warp_incl_sum(rc, lane);
+    const int total = __shfl_sync(0xffffffffu, rincl, 31);
+    wb += total;
+    const int rexcl = rincl - rc;
+    for (int pb = 0; pb < total; pb += 32) {
+      const int p = pb + (int)lane;
+      // row of word p: the number of rows whose inclusive count is <= p
+      int r = 0;
 #pragma unroll
-      for (int k = 0; k < U; ++k) {
-        jj[k] = tl ? __ffs(tl) - 1 : -1;
-        if (tl) tl &= tl - 1;
+      for (int st = 16; st > 0; st >>= 1) {
+        const int c = __shfl_sync(0xffffffffu, rincl, r + st - 1);
+        if (c <= p) r += st;
       }
-      unsigned w[U];
-      long long base[U];
-#pragma unroll
-      for (int k = 0; k < U; ++k) {
-        const int src = jj[k] < 0 ? 0 : jj[k];
-        const unsigned mj = __shfl_sync(0xffffffffu, m, src);
-        const int oj = __shfl_sync(0xffffffffu, off, src);
-        base[k] = (long long)__shfl_sync(0xffffffffu, cb, src) * 32;
-        w[k] = jj[k] >= 0 ? words[wbat + oj + __popc(mj & below)] : 0u;
-      }
-      T g[U];
-      bool h[U];
-#pragma unroll
-      for (int k = 0; k < U; ++k) {
-        h[k] = w[k] != 0u;
-        if (h[k]) {
-          const int j = __clz((int)w[k]);
-          w[k] &= ~(0x80000000u >> j);
-          g[k] = term(base[k] + j);
+      const int er = __shfl_sync(0xffffffffu, rexcl, r);
+      const unsigned tr = __shfl_sync(0xffffffffu, tl, r);
+      const int j = p < total ? (int)__fns(tr, 0, p - er + 1) : 0;
+      const unsigned mj = __shfl_sync(0xffffffffu, m, j);
+      const int oj = __shfl_sync(0xffffffffu, off, j);
+      const long long base = (long long)__shfl_sync(0xffffffffu, cb, j) * 32;
+      const bool valid = p < total;
+      Acc x{};
+      if (valid) {
+        unsigned w = words[wbat + oj + __popc(mj & ((1u << r) - 1u))];
+        int col = __clz((int)w);
+        w &= ~(0x80000000u >> col);
+        x = term(base + col);
+        while (w) {
+          col = __clz((int)w);
+          w &= ~(0x80000000u >> col);
+          comb(x, term(base + col));
         }
       }
+      // segmented inclusive scan over each row's run of lanes
+      const int key = valid ? r : -1 - (int)lane;
 #pragma unroll
-      for (int k = 0; k < U; ++k)
-        if (h[k]) comb(acc, g[k]);
-#pragma unroll
-      for (int k = 0; k < U; ++k) rest(w[k], base[k]);
+      for (int d = 1; d < 32; d <<= 1) {
+        const Acc y = __shfl_up_sync(0xffffffffu, x, d);
+        const int ky = __shfl_up_sync(0xffffffffu, key, d);
+        if ((int)lane >= d && ky == key) {
+          Acc z = y;
+          comb(z, x);
+          x = z;
+        }
+      }
+      // row `lane`: the last lane of its run in this round, if any
+      const int lo = max(rexcl, pb), hi = min(rincl, pb + 32);
+      const Acc seg = __shfl_sync(0xffffffffu, x, hi > lo ? hi - 1 - pb : 0);
+      if (hi > lo) comb(acc, seg);
     }
   }
 }
