@@ -221,8 +221,8 @@ __device__ __forceinline__ unsigned warp_transpose32(unsigned x, unsigned lane) 
 // order), and a segmented scan over the lanes of each row's run (the runs
 // are contiguous) leaves the run's fold in its last lane, which the row's
 // own lane folds into its accumulator.  Every lane does one word per round
-// whatever the rows' lengths, and the order of every fold is fixed by the
-// graph alone.
+// whatever the rows' lengths (two rounds at a time, so that their loads
+// overlap), and the order of every fold is fixed by the graph alone.
 template <int U, typename Acc, typename Term, typename Comb>
 __device__ __forceinline__ void fold_row_cols_t32(const GView& v, int t0, int t1, long long wb,
                                                   unsigned lane, Term term, Comb comb, Acc& acc) {
@@ -247,50 +247,72 @@ __device__ __forceinline__ void fold_row_cols_t32(const GView& v, int t0, int t1
     const int total = __shfl_sync(0xffffffffu, rincl, 31);
     wb += total;
     const int rexcl = rincl - rc;
-    for (int pb = 0; pb < total; pb += 32) {
-      const int p = pb + (int)lane;
-      // row of word p: the number of rows whose inclusive count is <= p
-      int r = 0;
+    constexpr int H = 2;  // rounds dealt together (their loads overlap)
+    for (int pb = 0; pb < total; pb += 32 * H) {
+      Acc x[H];
+      int key[H];
+      unsigned w[H];
+      long long base[H];
 #pragma unroll
-      for (int st = 16; st > 0; st >>= 1) {
-        const int c = __shfl_sync(0xffffffffu, rincl, r + st - 1);
-        if (c <= p) r += st;
+      for (int h = 0; h < H; ++h) {
+        const int p = pb + 32 * h + (int)lane;
+        // row of word p: the number of rows whose inclusive count is <= p
+        int r = 0;
+#pragma unroll
+        for (int st = 16; st > 0; st >>= 1) {
+          const int c = __shfl_sync(0xffffffffu, rincl, r + st - 1);
+          if (c <= p) r += st;
+        }
+        const int er = __shfl_sync(0xffffffffu, rexcl, r);
+        const unsigned tr = __shfl_sync(0xffffffffu, tl, r);
+        const bool valid = p < total;
+        const int j = valid ? (int)__fns(tr, 0, p - er + 1) : 0;
+        const unsigned mj = __shfl_sync(0xffffffffu, m, j);
+        const int oj = __shfl_sync(0xffffffffu, off, j);
+        base[h] = (long long)__shfl_sync(0xffffffffu, cb, j) * 32;
+        w[h] = valid ? words[wbat + oj + __popc(mj & ((1u << r) - 1u))] : 0u;
+        key[h] = valid ? r : -1 - (int)lane;
       }
-      const int er = __shfl_sync(0xffffffffu, rexcl, r);
-      const unsigned tr = __shfl_sync(0xffffffffu, tl, r);
-      const int j = p < total ? (int)__fns(tr, 0, p - er + 1) : 0;
-      const unsigned mj = __shfl_sync(0xffffffffu, m, j);
-      const int oj = __shfl_sync(0xffffffffu, off, j);
-      const long long base = (long long)__shfl_sync(0xffffffffu, cb, j) * 32;
-      const bool valid = p < total;
-      Acc x{};
-      if (valid) {
-        unsigned w = words[wbat + oj + __popc(mj & ((1u << r) - 1u))];
-        int col = __clz((int)w);
-        w &= ~(0x80000000u >> col);
-        x = term(base + col);
-        while (w) {
-          col = __clz((int)w);
-          w &= ~(0x80000000u >> col);
-          comb(x, term(base + col));
+      // the first set column of each word gathered together, then the others
+#pragma unroll
+      for (int h = 0; h < H; ++h) {
+        x[h] = Acc{};
+        if (w[h]) {
+          const int col = __clz((int)w[h]);
+          w[h] &= ~(0x80000000u >> col);
+          x[h] = term(base[h] + col);
         }
       }
-      // segmented inclusive scan over each row's run of lanes
-      const int key = valid ? r : -1 - (int)lane;
+#pragma unroll
+      for (int h = 0; h < H; ++h) {
+        while (w[h]) {
+          const int col = __clz((int)w[h]);
+          w[h] &= ~(0x80000000u >> col);
+          comb(x[h], term(base[h] + col));
+        }
+      }
+      // segmented inclusive scan over each row's run of lanes, per round
 #pragma unroll
       for (int d = 1; d < 32; d <<= 1) {
-        const Acc y = __shfl_up_sync(0xffffffffu, x, d);
-        const int ky = __shfl_up_sync(0xffffffffu, key, d);
-        if ((int)lane >= d && ky == key) {
-          Acc z = y;
-          comb(z, x);
-          x = z;
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+          const Acc y = __shfl_up_sync(0xffffffffu, x[h], d);
+          const int ky = __shfl_up_sync(0xffffffffu, key[h], d);
+          if ((int)lane >= d && ky == key[h]) {
+            Acc z = y;
+            comb(z, x[h]);
+            x[h] = z;
+          }
         }
       }
-      // row `lane`: the last lane of its run in this round, if any
-      const int lo = max(rexcl, pb), hi = min(rincl, pb + 32);
-      const Acc seg = __shfl_sync(0xffffffffu, x, hi > lo ? hi - 1 - pb : 0);
-      if (hi > lo) comb(acc, seg);
+      // row `lane`: the last lane of its run in each round, rounds in order
+#pragma unroll
+      for (int h = 0; h < H; ++h) {
+        const int rb = pb + 32 * h;
+        const int lo = max(rexcl, rb), hi = min(rincl, rb + 32);
+        const Acc seg = __shfl_sync(0xffffffffu, x[h], hi > lo ? hi - 1 - rb : 0);
+        if (hi > lo) comb(acc, seg);
+      }
     }
   }
 }
