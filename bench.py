@@ -738,7 +738,9 @@ def suite_config2(args, which):
         cfg["workload"] = f"PageRank alpha 0.85, 20 iterations, fp32 values / fp64 sums, R-MAT scale {args.scale}"
         extra = {"iterations": it.value, "dtype": "f32",
                  "roofline": {"bound": "hbm", "achieved": by / (step / 1e3) / 1e9, "peak": peak,
-                              "unit": "GB/s", "frac": by / (step / 1e3) / 1e9 / peak, "traffic": None,
+                              "unit": "GB/s", "frac": by / (step / 1e3) / 1e9 / peak,
+                              "traffic": (load_traffic("k_pr_step_rmat20_b32_ncu.md")
+                                          if args.scale == SCALE and args.tile == 32 else None),
                               "kernel": "PageRank iteration (semiring BMV + update)", "peak_source": psrc,
                               "algorithmic_bytes_per_launch": by, "ms_per_launch": step}}
         if bs is not None:
