@@ -186,6 +186,18 @@ __device__ __forceinline__ void close_iteration(Ctrl* ctrl, Decide decide) {
 }
 
 // ============================================================== BFS
+// Frontier words rotate through three buffers of front_stride(nbr) words:
+// level L reads buffer L % 3 and writes buffer (L + 1) % 3, and its active
+// step kernel zeroes buffer (L + 2) % 3 -- read last at level L - 1 -- so
+// that a push step at level L + 1 finds its output empty without a clearing
+// launch.  The stride keeps every buffer on a 4-byte boundary, so the 32-bit
+// atomics that OR narrow words never reach into a neighbouring buffer.
+__host__ __device__ __forceinline__ size_t front_stride(int nbr) { return ((size_t)nbr + 4) & ~(size_t)3; }
+template <typename WT>
+__device__ __forceinline__ WT* front_buf(WT* front, int nbr, int lvl) {
+  return front + (size_t)(lvl % 3) * front_stride(nbr);
+}
+
 template <int B>
 __global__ void __launch_bounds__(kTPB) k_bfs_step(GView v, typename Word<B>::T* __restrict__ front,
                                                    typename Word<B>::T* __restrict__ visited,
@@ -195,8 +207,9 @@ __global__ void __launch_bounds__(kTPB) k_bfs_step(GView v, typename Word<B>::T*
   using L = Lay<B>;
   if (((volatile Ctrl*)ctrl)->done || ((volatile Ctrl*)ctrl)->mode) return;
   const int lvl = ((volatile Ctrl*)ctrl)->iter;
-  const WT* __restrict__ x = front + (size_t)(lvl & 1) * v.nbr;
-  WT* __restrict__ out = front + (size_t)((lvl + 1) & 1) * v.nbr;
+  const WT* __restrict__ x = front_buf(front, v.nbr, lvl);
+  WT* __restrict__ out = front_buf(front, v.nbr, lvl + 1);
+  WT* __restrict__ z = front_buf(front, v.nbr, lvl + 2);
   const unsigned lane = threadIdx.x & 31;
   const int r = lane % L::W;
   const WT full = full_word<B>();
@@ -227,6 +240,7 @@ __global__ void __launch_bounds__(kTPB) k_bfs_step(GView v, typename Word<B>::T*
     }
     const WT word = gather_bits<B>(p0, p1, lane);
     if (active) {
+      if (r == 0) z[it.row] = 0;
       if (it.slot >= 0) {
         if (r == 0) scratch[it.slot] = word;
       } else {
@@ -285,17 +299,6 @@ __global__ void __launch_bounds__(kTPB) k_live(GView v, typename Word<B>::T* __r
   if (active && r == 0 && word) atomic_or_word<B>(live, it.row, word);
 }
 
-// Next-frontier words start empty in a push step.
-template <int B>
-__global__ void k_bfs_push_clear(typename Word<B>::T* __restrict__ front, int nbr, Ctrl* __restrict__ ctrl) {
-  if (((volatile Ctrl*)ctrl)->done || !((volatile Ctrl*)ctrl)->mode) return;
-  const int lvl = ((volatile Ctrl*)ctrl)->iter;
-  typename Word<B>::T* out = front + (size_t)((lvl + 1) & 1) * nbr;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nbr;
-       i += (long long)gridDim.x * blockDim.x)
-    out[i] = 0;
-}
-
 // Top-down (push) step for symmetric P, used while the frontier is small:
 // for every frontier row r of block row J and every tile (J, C), the row
 // word (the neighbours of vertex J*b+r in block C) is OR-ed into the next
@@ -308,13 +311,15 @@ __global__ void __launch_bounds__(kTPB) k_bfs_push(GView v, typename Word<B>::T*
   using WT = typename Word<B>::T;
   if (((volatile Ctrl*)ctrl)->done || !((volatile Ctrl*)ctrl)->mode) return;
   const int lvl = ((volatile Ctrl*)ctrl)->iter;
-  const WT* __restrict__ x = front + (size_t)(lvl & 1) * v.nbr;
-  WT* out = front + (size_t)((lvl + 1) & 1) * v.nbr;
+  const WT* __restrict__ x = front_buf(front, v.nbr, lvl);
+  WT* out = front_buf(front, v.nbr, lvl + 1);
+  WT* __restrict__ z = front_buf(front, v.nbr, lvl + 2);
   const unsigned lane = threadIdx.x & 31;
   const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
   const long long nwarps = warps_total();
   for (long long item = warp_global(); item < v.nitems; item += nwarps) {
     const gbo_item it = v.items[item];
+    if (lane == 0) z[it.row] = 0;
     const WT xs = x[it.row];
     if (!xs) continue;
     if constexpr (B == 32) {
@@ -422,8 +427,9 @@ __global__ void __launch_bounds__(kTPB) k_bfs_step_col(GView v, typename Word<B>
   using WT = typename Word<B>::T;
   if (((volatile Ctrl*)ctrl)->done || ((volatile Ctrl*)ctrl)->mode) return;
   const int lvl = ((volatile Ctrl*)ctrl)->iter;
-  const WT* __restrict__ x = front + (size_t)(lvl & 1) * v.nbr;
-  WT* __restrict__ out = front + (size_t)((lvl + 1) & 1) * v.nbr;
+  const WT* __restrict__ x = front_buf(front, v.nbr, lvl);
+  WT* __restrict__ out = front_buf(front, v.nbr, lvl + 1);
+  WT* __restrict__ z = front_buf(front, v.nbr, lvl + 2);
   const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
   const unsigned lane = threadIdx.x & 31;
   const WT full = full_word<B>();
@@ -457,6 +463,7 @@ __global__ void __launch_bounds__(kTPB) k_bfs_step_col(GView v, typename Word<B>
         if ((WT)((found | vis) & full) == full) break;
       }
     }
+    if (lane == 0) z[it.row] = 0;
     if (it.slot >= 0) {
       if (lane == 0) scratch[it.slot] = found;
       continue;
@@ -487,13 +494,15 @@ __global__ void __launch_bounds__(kTPB) k_bfs_push_col(GView v, typename Word<B>
   using WT = typename Word<B>::T;
   if (((volatile Ctrl*)ctrl)->done || !((volatile Ctrl*)ctrl)->mode) return;
   const int lvl = ((volatile Ctrl*)ctrl)->iter;
-  const WT* __restrict__ x = front + (size_t)(lvl & 1) * v.nbr;
-  WT* out = front + (size_t)((lvl + 1) & 1) * v.nbr;
+  const WT* __restrict__ x = front_buf(front, v.nbr, lvl);
+  WT* out = front_buf(front, v.nbr, lvl + 1);
+  WT* __restrict__ z = front_buf(front, v.nbr, lvl + 2);
   const unsigned lane = threadIdx.x & 31;
   const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
   const long long nwarps = warps_total();
   for (long long item = warp_global(); item < v.nitems; item += nwarps) {
     const gbo_item it = v.items[item];
+    if (lane == 0) z[it.row] = 0;
     const WT xs = x[it.row];
     if (!xs) continue;
     for (int t = it.t0 + (int)lane; t < it.t1; t += 32) {
@@ -516,7 +525,7 @@ __global__ void k_bfs_finish(GView v, typename Word<B>::T* __restrict__ front,
   if (((volatile Ctrl*)ctrl)->done) return;
   const int lvl = ((volatile Ctrl*)ctrl)->iter;
   const int push = ((volatile Ctrl*)ctrl)->mode;
-  WT* __restrict__ out = front + (size_t)((lvl + 1) & 1) * v.nbr;
+  WT* __restrict__ out = front_buf(front, v.nbr, lvl + 1);
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long cnt = 0;
   if (push) {
@@ -588,7 +597,8 @@ __global__ void k_bfs_init(typename Word<B>::T* front, typename Word<B>::T* visi
   for (long long k = i; k < nbr; k += stride) {
     WT w = (src >= 0 && k == src / B) ? (WT)((WT)1 << (B - 1 - src % B)) : (WT)0;
     front[k] = w;
-    front[nbr + k] = 0;
+    front[front_stride(nbr) + k] = 0;
+    front[2 * front_stride(nbr) + k] = 0;
     visited[k] = (WT)(w | (~live[k] & full_word<B>()));
   }
   if (i == 0) {
@@ -979,10 +989,10 @@ int get_state(gbo_graph* g, AlgoState** out) {
 int ensure_frontier(gbo_graph* g, AlgoState* a, cudaStream_t s) {
   if (!a->front) {
     const size_t wb = 8;  // widest word
-    GBO_CUDA_TRY(cudaMalloc(&a->front, wb * 2 * (size_t)(g->nbr + 1)));
+    GBO_CUDA_TRY(cudaMalloc(&a->front, wb * 3 * front_stride(g->nbr)));
     GBO_CUDA_TRY(cudaMalloc(&a->visited, wb * (size_t)(g->nbr + 1)));
     GBO_CUDA_TRY(cudaMalloc(&a->live, wb * (size_t)(g->nbr + 1)));
-    g->device_bytes += (long long)(wb * 4 * (g->nbr + 1));
+    g->device_bytes += (long long)(wb * (3 * front_stride(g->nbr) + 2 * (g->nbr + 1)));
     GBO_CUDA_TRY(cudaMemsetAsync(a->live, 0, wb * (size_t)(g->nbr + 1), s));
     if (g->nitems > 0 && g->layout == GBO_LAYOUT_COL) {
       const GView v = view_of(g);
@@ -1143,11 +1153,9 @@ int bfs_impl(gbo_graph* g, int src, const int* h_seeds, int nseeds, int32_t* d_l
   const bool push_ok = g->symmetric;
   const unsigned gs = blocks_for(std::max<long long>(g->nsplit, push_ok ? g->nbr : 0), kTPB);
   const unsigned gp = col ? grid_persistent(k_bfs_push_col<B>, g->nitems) : grid_persistent(k_bfs_push<B>, g->nitems);
-  const unsigned gc = grid_vertex(g->nbr);
   GBO_TRY(get_exec(a, A_BFS, nullptr, [&](cudaStream_t cs, int k, int* nl) -> int {
     StepTimer tm{a, cs, k};
     tm.begin();
-    if (push_ok) k_bfs_push_clear<B><<<gc, kTPB, 0, cs>>>(front, g->nbr, ctrl);
     if (g->nitems > 0) {
       if (col) k_bfs_step_col<B><<<gi, kTPB, 0, cs>>>(v, front, vis, level, ctrl, scratch);
       else k_bfs_step<B><<<gi, kTPB, 0, cs>>>(v, front, vis, level, ctrl, scratch);
@@ -1158,7 +1166,7 @@ int bfs_impl(gbo_graph* g, int src, const int* h_seeds, int nseeds, int32_t* d_l
     }
     tm.end();
     k_bfs_finish<B><<<gs, kTPB, 0, cs>>>(v, front, vis, level, ctrl, scratch);
-    *nl += (g->nitems > 0) + 1 + (push_ok ? 1 + (g->nitems > 0) : 0);
+    *nl += (g->nitems > 0) + 1 + (push_ok ? (g->nitems > 0) : 0);
     GBO_CUDA_TRY(cudaGetLastError());
     return GBO_OK;
   }));
