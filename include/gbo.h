@@ -454,10 +454,9 @@ enum { GBO_MTX_READMTX = 0, GBO_MTX_MMIO = 1 };
  * for a binary matrix). */
 GBO_API int gbo_read_mtx(const char* path, int mode, int directed, gbo_csr** out);
 GBO_API int gbo_csr_free(gbo_csr* csr);
-/* The same readers on the GPU (SURVEY next item: GPU ingestion): the entry
- * lines are parsed in parallel and the CSR is built in device memory --
- * identical to gbo_read_mtx's for well-formed files (each line is parsed on
- * its own).  d_rowptr (int32[nrows+1]) and d_colind (int32[nnz]) are
+/* The same readers on the GPU: the entry lines are parsed in parallel and
+ * the CSR is built in device memory -- identical to gbo_read_mtx's for
+ * well-formed files (each line is parsed on its own).  d_rowptr (int32[nrows+1]) and d_colind (int32[nnz]) are
  * allocated here; free them with gbo_free.  gbo_graph_from_mtx packs the
  * parsed CSR straight into a graph (flags as gbo_graph_from_csr). */
 GBO_API int gbo_read_mtx_device(const char* path, int mode, int directed,
