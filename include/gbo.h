@@ -159,7 +159,10 @@ GBO_API int gbo_graph_from_csr(const int* rowptr, const int* colind, int nrows,
                        int ncols, int nnz, int tile_bits, int flags,
                        gbo_stream_t stream, gbo_graph** out);
 /* Wrap caller-owned device B2SR buffers (not copied, not freed).  d_outdeg
- * may be NULL (then PageRank entry points return GBO_ERR_INVALID). */
+ * may be NULL (then PageRank entry points return GBO_ERR_INVALID).  The
+ * work schedule and, for 32x32 ROW tiles, the per-tile occupancy words and
+ * packed non-empty row words are derived from the buffers here, so their
+ * contents must not change while the graph is in use. */
 GBO_API int gbo_graph_wrap_b2sr(int nrows, int ncols, int tile_bits, int layout,
                         int nblocks, const int* d_bsrRowPtr,
                         const int* d_bsrColInd, const void* d_bsrVal,
