@@ -192,6 +192,10 @@ __global__ void __launch_bounds__(kTPB, 4) k_step(Args a) {
       // depend on the order).
       constexpr int kPerPass = kList / 32;
       const unsigned* __restrict__ rm = v.rowmask;
+      // packed non-empty row words (32x32 ROW graphs): the words a batch
+      // loads sit together instead of one per 32-byte sector
+      const unsigned* __restrict__ words = v.rowword;
+      long long wb = words ? v.item_wbase[item] : 0ll;
       const unsigned openm = __ballot_sync(0xffffffffu, row_open);
       for (int b0 = it.t0; b0 < it.t1; b0 += 32) {
         const int t = b0 + (int)lane;
@@ -205,7 +209,11 @@ __global__ void __launch_bounds__(kTPB, 4) k_step(Args a) {
         const unsigned cand = fw ? (mw & openm) : 0u;
         const int cnt = __popc(cand);
         const int total = (int)__reduce_add_sync(0xffffffffu, (unsigned)cnt);
+        const long long wbat = wb;
+        const int mc = words ? __popc(mw) : 0;
+        if (words) wb += (long long)__reduce_add_sync(0xffffffffu, (unsigned)mc);
         if (total == 0) continue;
+        const int woff = words ? warp_incl_sum(mc, lane) - mc : 0;  // lane j: tile j's first word
         const int incl = warp_incl_sum(cnt, lane);
         const int excl = incl - cnt;
         for (int pb = 0; pb < total; pb += 32) {
@@ -220,11 +228,13 @@ __global__ void __launch_bounds__(kTPB, 4) k_step(Args a) {
           const unsigned cj = __shfl_sync(0xffffffffu, cand, j);
           const uint32_t fj = __shfl_sync(0xffffffffu, fw, j);
           const int vbase = __shfl_sync(0xffffffffu, cb, j) * 32;
+          const unsigned mj = __shfl_sync(0xffffffffu, mw, j);
+          const int oj = __shfl_sync(0xffffffffu, woff, j);
           int r = 0;
           uint32_t eff = 0u;
           if (p < total) {
             r = (int)__fns(cj, 0, p - ej + 1);
-            eff = val[(size_t)(b0 + j) * 32 + r] & fj;
+            eff = (words ? words[rowword_index(wbat + oj, mj, r)] : val[(size_t)(b0 + j) * 32 + r]) & fj;
           }
           if constexpr (KW <= 2) {
             // narrow frontier rows (k <= 64): each lane ORs the rows of its
