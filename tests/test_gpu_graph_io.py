@@ -58,3 +58,16 @@ def test_load_rejects_malformed_files(gbo, gpu, tmp_path):
         gbo.Graph.load(str(tmp_path / "missing.b2sr"))
     assert e.value.status == gbo.GBO_ERR_IO
     g.free()
+
+
+def test_save_load_empty_graph(gbo, gpu, tmp_path):
+    empty = gbo.Csr(np.zeros(101, np.int32), np.zeros(0, np.int32), 100, 100)
+    g = gbo.Graph.from_csr(empty, 32)
+    path = str(tmp_path / "empty.b2sr")
+    g.save(path)
+    h = gbo.Graph.load(path)
+    assert h.info().nblocks == 0 and h.info().nrows == 100
+    lv, depth = h.bfs(3)
+    assert lv[3] == 0 and (lv[np.arange(100) != 3] == -1).all()
+    g.free()
+    h.free()

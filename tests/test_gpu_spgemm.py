@@ -73,3 +73,16 @@ def test_spgemm_rejects_other_layouts(gbo, gpu):
     g16 = gbo.Graph.from_csr(a, 16)
     with pytest.raises(gbo.GboError):
         g16.bmm_sum(ga)  # tile widths differ
+
+
+def test_products_of_empty_matrices(gbo, gpu):
+    empty = gbo.Csr(np.zeros(65, np.int32), np.zeros(0, np.int32), 64, 64)
+    a = _rect(gbo, 64, 64, 0.1, 4)
+    for x, y in ((empty, a), (a, empty), (empty, empty)):
+        gx = gbo.Graph.from_csr(x, 32)
+        gy = gbo.Graph.from_csr(y, 32, gbo.FLAG_LAYOUT_COL)
+        rp, ci, v = gx.spgemm(gy)
+        assert rp.shape == (65,) and not rp.any() and len(ci) == 0 and len(v) == 0
+        assert gx.bmm_sum(gy) == 0
+        gx.free()
+        gy.free()
