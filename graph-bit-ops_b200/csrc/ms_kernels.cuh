@@ -121,7 +121,7 @@ __device__ __forceinline__ void block_row_epilogue(const Args& a, int R, int lvl
 constexpr int kList = 192;
 
 template <int KW>
-__global__ void __launch_bounds__(kTPB, 4) k_step(Args a) {
+__global__ void __launch_bounds__(kTPB, KW <= 2 ? 6 : 4) k_step(Args a) {
   constexpr int S = 32 / KW;
   constexpr int U = S >= 64 ? 1 : (64 / S > 8 ? 8 : 64 / S);  // gathers in flight: S*U pairs
   __shared__ uint32_t acc_sh[kWarps][32 * KW];
