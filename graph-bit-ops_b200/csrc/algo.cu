@@ -1355,6 +1355,109 @@ int cc_impl(gbo_graph* g, int32_t* d_label, int* h_iters, cudaStream_t s) {
   return GBO_OK;
 }
 
+// ------------------------------------------------ block-row shards (BFS)
+// One pull level over a shard -- the block rows of some of the vertices,
+// every column -- against the whole graph's frontier words x: the shard's
+// next-frontier words, visited words and levels.  A work group per item;
+// split rows leave their words in scratch slots for k_bfs_shard_finish.
+template <int B>
+__global__ void __launch_bounds__(kTPB) k_bfs_shard_step(GView v, const typename Word<B>::T* __restrict__ x,
+                                                         typename Word<B>::T* __restrict__ visited,
+                                                         int* __restrict__ level, int lvl,
+                                                         typename Word<B>::T* __restrict__ out,
+                                                         typename Word<B>::T* __restrict__ scratch,
+                                                         unsigned long long* __restrict__ count) {
+  using WT = typename Word<B>::T;
+  using L = Lay<B>;
+  const unsigned lane = threadIdx.x & 31;
+  const int r = lane % L::W;
+  const WT full = full_word<B>();
+  const long long item = item_index(lane, L::W, L::G);
+  const bool active = item < v.nitems;
+  const gbo_item it = active ? v.items[item] : gbo_item{0, 0, 0, -2};
+  const WT vis = active ? visited[it.row] : full;
+  bool p0 = false, p1 = false;
+  if (active && (vis & full) != full) {  // uniform inside the item's lane group
+    const long long row0 = (long long)it.row * B + r;
+    const bool need0 = !bit_of<B>(vis, r) && row0 < v.nrows;
+    const bool need1 = L::RPL == 2 && !bit_of<B>(vis, r + 32) && row0 + 32 < v.nrows;
+    pull_or_scan<B>(v, it.t0, it.t1, x, need0, need1, p0, p1, lane);
+  }
+  const WT word = gather_bits<B>(p0, p1, lane);
+  unsigned long long cnt = 0;
+  if (active) {
+    if (it.slot >= 0) {
+      if (r == 0) scratch[it.slot] = word;
+    } else {
+      const WT nw = (WT)(word & ~vis & full);
+      const long long row0 = (long long)it.row * B + r;
+      if (bit_of<B>(nw, r) && row0 < v.nrows) level[row0] = lvl + 1;
+      if (L::RPL == 2 && bit_of<B>(nw, r + 32) && row0 + 32 < v.nrows) level[row0 + 32] = lvl + 1;
+      if (r == 0) {
+        out[it.row] = nw;
+        if (nw) visited[it.row] = (WT)(vis | nw);
+        cnt = popc_w(nw);
+      }
+    }
+  }
+  block_add_u64(cnt, count);
+}
+
+template <int B>
+__global__ void k_bfs_shard_finish(GView v, typename Word<B>::T* __restrict__ visited, int* __restrict__ level,
+                                   int lvl, typename Word<B>::T* __restrict__ out,
+                                   const typename Word<B>::T* __restrict__ scratch,
+                                   unsigned long long* __restrict__ count) {
+  using WT = typename Word<B>::T;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long cnt = 0;
+  if (i < v.nsplit) {
+    const gbo_split sp = v.splits[i];
+    const WT full = full_word<B>();
+    const WT vis = visited[sp.row];
+    WT w = 0;
+    if ((vis & full) != full)
+      for (int q = 0; q < sp.nslots; ++q) w |= scratch[sp.slot0 + q];
+    const WT nw = (WT)(w & ~vis & full);
+    out[sp.row] = nw;
+    if (nw) {
+      visited[sp.row] = (WT)(vis | nw);
+      for (int rr = 0; rr < B; ++rr) {
+        const long long row = (long long)sp.row * B + rr;
+        if (bit_of<B>(nw, rr) && row < v.nrows) level[row] = lvl + 1;
+      }
+      cnt = popc_w(nw);
+    }
+  }
+  block_add_u64(cnt, count);
+}
+
+template <int B>
+int bfs_shard_level_impl(gbo_graph* g, const void* x, void* visited, int32_t* level, int lvl, void* out,
+                         uint64_t* h_count, cudaStream_t s) {
+  using WT = typename Word<B>::T;
+  AlgoState* a = nullptr;
+  GBO_TRY(get_state(g, &a));
+  unsigned long long* cnt = &a->ctrl->count;
+  GBO_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), s));
+  const GView v = view_of(g);
+  auto* scratch = static_cast<WT*>(g->ws);  // split-row words (one per slot)
+  if (g->nitems > 0)
+    k_bfs_shard_step<B><<<blocks_for_warps((g->nitems + Lay<B>::G - 1) / Lay<B>::G, kTPB / 32), kTPB, 0, s>>>(
+        v, static_cast<const WT*>(x), static_cast<WT*>(visited), level, lvl, static_cast<WT*>(out), scratch, cnt);
+  if (g->nsplit > 0)
+    k_bfs_shard_finish<B><<<blocks_for(g->nsplit, kTPB), kTPB, 0, s>>>(v, static_cast<WT*>(visited), level, lvl,
+                                                                      static_cast<WT*>(out), scratch, cnt);
+  GBO_CUDA_TRY(cudaGetLastError());
+  if (h_count) {
+    unsigned long long h = 0;
+    GBO_CUDA_TRY(cudaMemcpyAsync(&h, cnt, sizeof(h), cudaMemcpyDeviceToHost, s));
+    GBO_CUDA_TRY(cudaStreamSynchronize(s));
+    *h_count = h;
+  }
+  return GBO_OK;
+}
+
 int check_algo_graph(const gbo_graph* g, bool col_ok = false) {
   if (!g) return fail(GBO_ERR_INVALID, "graph is NULL");
   if (g->layout != GBO_LAYOUT_ROW && !col_ok)
@@ -1497,4 +1600,23 @@ extern "C" int gbo_graph_last_run(const gbo_graph* g, gbo_run_stats* stats) {
   stats->nsteps = n < GBO_MAX_STEP_TIMES ? n : GBO_MAX_STEP_TIMES;
   for (int i = 0; i < stats->nsteps; ++i) stats->step_ms[i] = a->step_ms[(size_t)i];
   return GBO_OK;
+}
+
+extern "C" int gbo_bfs_shard_level(const gbo_graph* shard, const void* d_front, void* d_visited,
+                                   int32_t* d_level, int level, void* d_next, uint64_t* h_count,
+                                   gbo_stream_t stream) {
+  clear_error();
+  if (!shard) return fail(GBO_ERR_INVALID, "graph is NULL");
+  if (shard->layout != GBO_LAYOUT_ROW) return fail(GBO_ERR_UNSUPPORTED, "a BFS shard needs the ROW tile layout");
+  if ((shard->nrows > 0 && (!d_visited || !d_level || !d_next)) || (shard->ncols > 0 && !d_front) || level < 0)
+    return fail(GBO_ERR_INVALID, "gbo_bfs_shard_level: bad argument");
+  gbo_graph* g = const_cast<gbo_graph*>(shard);
+  cudaStream_t s = as_stream(stream);
+  switch (g->b) {
+    case 4: return bfs_shard_level_impl<4>(g, d_front, d_visited, d_level, level, d_next, h_count, s);
+    case 8: return bfs_shard_level_impl<8>(g, d_front, d_visited, d_level, level, d_next, h_count, s);
+    case 16: return bfs_shard_level_impl<16>(g, d_front, d_visited, d_level, level, d_next, h_count, s);
+    case 32: return bfs_shard_level_impl<32>(g, d_front, d_visited, d_level, level, d_next, h_count, s);
+    default: return bfs_shard_level_impl<64>(g, d_front, d_visited, d_level, level, d_next, h_count, s);
+  }
 }

@@ -142,6 +142,7 @@ _SIGS = {
     "gbo_ppr_backward": (_I, [_P, _P, C.c_float, C.c_float, _I, _P, C.POINTER(_I), _P]),
     "gbo_graph_last_run": (_I, [_P, C.POINTER(RunStats)]),
     "gbo_msbfs": (_I, [_P, _P, _I, _P, C.POINTER(_I), _P]),
+    "gbo_bfs_shard_level": (_I, [_P, _P, _P, _P, _I, _P, C.POINTER(C.c_uint64), _P]),
     "gbo_bmm_sum": (_I, [_P, _P, C.POINTER(C.c_uint64), _P]),
     "gbo_spgemm_nnz": (_I, [_P, _P, _P, C.POINTER(C.c_int64), _P]),
     "gbo_spgemm_fill": (_I, [_P, _P, _P, _P, _P, _P]),

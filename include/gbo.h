@@ -349,6 +349,25 @@ GBO_API int gbo_spgemm_fill(const gbo_graph* a, const gbo_graph* b,
                     const int64_t* d_rowptr, int32_t* d_colind, int32_t* d_val,
                     gbo_stream_t stream);
 
+/* Block-row sharding of BFS across GPUs (the reference runs on one GPU,
+ * algorithm/bfs.cu:508-564 is its level loop).  A shard is a graph packed
+ * from the CSR rows [row0, row0 + shard.nrows) of the whole matrix with all
+ * of its columns (row0 a multiple of the tile width, ROW layout).  One call
+ * runs one pull level over the shard:
+ *   d_front   the whole graph's frontier words of `level` (ncols/b words, the
+ *             bit-vector layout of gbo_pack_vector_*),
+ *   d_visited the shard's visited words (updated), d_level the shard's int32
+ *             levels (new vertices get level + 1), d_next the shard's
+ *             next-frontier words (written), *h_count (may be NULL) the
+ *             number of new vertices (the call then waits for the stream).
+ * Between levels every rank places the shards' d_next words at their block
+ * rows to form the next d_front (an all-gather of n/8 bytes); the loop ends
+ * when no shard finds a new vertex.  graph-bit-ops_b200/shard.py drives it
+ * over torch.distributed. */
+GBO_API int gbo_bfs_shard_level(const gbo_graph* shard, const void* d_front, void* d_visited,
+                        int32_t* d_level, int level, void* d_next, uint64_t* h_count,
+                        gbo_stream_t stream);
+
 /* Multi-source BFS (batching): k sources (1 <= k <= 1024) traversed at once.
  * The frontier is an n x k bit matrix, so every level is one B2SR x bit
  * matrix product (OR.AND semiring).  d_levels: int32[n * k], vertex-major:
