@@ -230,6 +230,7 @@ static int read_mtx_device(const char* path, int mode, int directed, int** d_row
   GBO_CUDA_TRY(cudaMemcpyAsync(&nl, dcnt, sizeof(nl), cudaMemcpyDeviceToHost, s));
   GBO_CUDA_TRY(cudaStreamSynchronize(s));
   const long long nlines = (long long)nl;
+  if (nlines > 2147483647LL) return fail(GBO_ERR_OVERFLOW, "more than 2^31-1 lines");
   // sort the line starts
   DevMem sorted(s), temp(s);
   GBO_TRY(sorted.alloc(sizeof(long long) * (size_t)std::max(nlines, 1ll)));

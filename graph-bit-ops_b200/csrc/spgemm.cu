@@ -306,6 +306,7 @@ int spgemm_pass(const gbo_graph* a, const gbo_graph* b, bool fill, int* rowcnt, 
     int I1 = I0 + 1;
     while (I1 < a->nbr && hp[arp[I1 + 1]] - hp[arp[I0]] <= kPairBudget) ++I1;
     const long long base = hp[arp[I0]], np = hp[arp[I1]] - base;
+    if (np > 2147483647LL) return fail(GBO_ERR_OVERFLOW, "one block row has more than 2^31-1 tile pairs");
     if (np > 0) {
       if (np > cap) {
         for (int k = 0; k < 2; ++k) {
