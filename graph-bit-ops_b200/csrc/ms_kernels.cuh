@@ -197,22 +197,16 @@ __global__ void __launch_bounds__(kTPB, KW <= 2 ? 6 : 4) k_step(Args a) {
       const unsigned* __restrict__ words = v.rowword;
       long long wb = words ? v.item_wbase[item] : 0ll;
       const unsigned openm = __ballot_sync(0xffffffffu, row_open);
-      for (int b0 = it.t0; b0 < it.t1; b0 += 32) {
-        const int t = b0 + (int)lane;
-        int cb = 0;
-        uint32_t fw = 0, mw = rm ? 0u : ~0u;
-        if (t < it.t1) {
-          cb = v.colind[t];
-          if (rm) mw = rm[t];
-          fw = fb[cb];
-        }
+      // one batch of 32 tiles from b0: lane j holds tile b0+j's block
+      // column cb, occupancy word mw and frontier word fw
+      auto batch = [&](int b0, int cb, uint32_t mw, uint32_t fw) {
         const unsigned cand = fw ? (mw & openm) : 0u;
         const int cnt = __popc(cand);
         const int total = (int)__reduce_add_sync(0xffffffffu, (unsigned)cnt);
         const long long wbat = wb;
         const int mc = words ? __popc(mw) : 0;
         if (words) wb += (long long)__reduce_add_sync(0xffffffffu, (unsigned)mc);
-        if (total == 0) continue;
+        if (total == 0) return;
         const int woff = words ? warp_incl_sum(mc, lane) - mc : 0;  // lane j: tile j's first word
         const int incl = warp_incl_sum(cnt, lane);
         const int excl = incl - cnt;
@@ -237,21 +231,35 @@ __global__ void __launch_bounds__(kTPB, KW <= 2 ? 6 : 4) k_step(Args a) {
             eff = (words ? words[rowword_index(wbat + oj, mj, r)] : val[(size_t)(b0 + j) * 32 + r]) & fj;
           }
           if constexpr (KW <= 2) {
-            // narrow frontier rows (k <= 64): each lane ORs the rows of its
-            // word's frontier vertices straight into the accumulator
+            // narrow frontier rows (k <= 64): every frontier vertex of the
+            // lane's word lands in row r, so the lane ORs their rows in
+            // registers, several loads in flight, and adds the result to
+            // the accumulator once
+            constexpr int kIn = 3;
+            uint32_t o0 = 0u, o1 = 0u;
             while (eff) {
-              const int col = __clz(eff);
-              eff &= ~(0x80000000u >> col);
-              const size_t fo = (size_t)(vbase + col) * KW;
-              if (KW == 1) {
-                const uint32_t f = F[fo];
-                if (f) atomicOr(acc + r, f);
-              } else {
-                const uint2 f = *reinterpret_cast<const uint2*>(F + fo);
-                if (f.x) atomicOr(acc + r * KW, f.x);
-                if (f.y) atomicOr(acc + r * KW + 1, f.y);
+              uint2 f[kIn];
+#pragma unroll
+              for (int u = 0; u < kIn; ++u) {
+                f[u] = make_uint2(0u, 0u);
+                if (eff) {
+                  const int col = __clz(eff);
+                  eff &= ~(0x80000000u >> col);
+                  const size_t fo = (size_t)(vbase + col) * KW;
+                  if (KW == 1)
+                    f[u].x = F[fo];
+                  else
+                    f[u] = *reinterpret_cast<const uint2*>(F + fo);
+                }
+              }
+#pragma unroll
+              for (int u = 0; u < kIn; ++u) {
+                o0 |= f[u].x;
+                o1 |= f[u].y;
               }
             }
+            if (o0) atomicOr(acc + r * KW, o0);
+            if (KW == 2 && o1) atomicOr(acc + r * KW + 1, o1);
           } else {
             while (__any_sync(0xffffffffu, eff != 0u)) {
               const int c = min(__popc(eff), kPerPass);
@@ -269,6 +277,25 @@ __global__ void __launch_bounds__(kTPB, KW <= 2 ? 6 : 4) k_step(Args a) {
             }
           }
         }
+      };
+      // two batches per step: the loads of both (block column -> frontier
+      // word, a dependent pair) are in flight together
+      for (int b0 = it.t0; b0 < it.t1; b0 += 64) {
+        const int ta = b0 + (int)lane, tb = ta + 32;
+        int ca = 0, cbb = 0;
+        uint32_t ma = rm ? 0u : ~0u, mb = ma, fa = 0u, fbb = 0u;
+        if (ta < it.t1) {
+          ca = v.colind[ta];
+          if (rm) ma = rm[ta];
+        }
+        if (tb < it.t1) {
+          cbb = v.colind[tb];
+          if (rm) mb = rm[tb];
+        }
+        if (ta < it.t1) fa = fb[ca];
+        if (tb < it.t1) fbb = fb[cbb];
+        batch(b0, ca, ma, fa);
+        if (b0 + 32 < it.t1) batch(b0 + 32, cbb, mb, fbb);
       }
       flush();
       if (it.slot >= 0) {
