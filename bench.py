@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--tc-tiles", default="8,16,32,64", help="tile widths of --workload tc")
     ap.add_argument("--ms-scale", type=int, default=21, help="R-MAT scale of --workload msbfs")
     ap.add_argument("--ms-ks", default="64,256,1024", help="source counts of --workload msbfs")
+    ap.add_argument("--ms-push", type=int, default=-1,
+                    help="push threshold of --workload msbfs, new (vertex, source) pairs below which "
+                         "a level of k <= 64 pushes (-1: the library default, pull)")
     ap.add_argument("--serve-rates", default="1000,10000,100000",
                     help="offered rates of --workload serve (queries/s, comma-separated)")
     ap.add_argument("--workload", default="bfs", choices=["bfs"] + list(SUITE),
@@ -832,6 +835,8 @@ def suite_msbfs(args):
     d_level = gbo.DeviceBuffer(4 * n)
     srcs_plain = rng.integers(0, n, 16).astype(np.int32)
     plain_ms = np.mean([_timed(gbo, lambda s=int(s): g.bfs(s, out=d_level), 1, 1) for s in srcs_plain])
+    if args.ms_push >= 0:  # after the plain runs, which keep their own default
+        g.set_bfs_direction(True, args.ms_push)
     res = {}
     deg = np.diff(csr.rowptr).astype(np.int64)
     ks = [int(k) for k in args.ms_ks.split(",")]
@@ -849,7 +854,7 @@ def suite_msbfs(args):
           {"workload": f"multi-source BFS, R-MAT scale {args.ms_scale} ef16 seed 2, k random sources "
                        "(seed 3), B2SR 32",
            "nvertices": n, "nnz": csr.nnz},
-          dtype="u32", by_k=res, plain_qps=1e3 / plain_ms)
+          dtype="u32", by_k=res, plain_qps=1e3 / plain_ms, ms_push=args.ms_push)
     g.free()
 
 

@@ -46,6 +46,16 @@ struct Args {
   const uint32_t* active;  // optional: source columns still traversing (kw words); a row
                            // counts as finished once every active column reached it
   int level_group;     // 0: levels[i*k + s]; g > 0: levels[((s/g)*n + i)*g + s%g]
+  // Direction-optimising levels (symmetric graphs): with dir set, a level
+  // whose frontier holds fewer than push_thr (vertex, source) pairs runs as
+  // a push (k_push scatters frontier rows into push_acc, nbr x 32 x KW words,
+  // zero between levels; k_push_fin finalises every block row).  ctl[6] is
+  // the current level's mode (1 push), ctl[7] is set once a push level has
+  // closed in the current slot of the captured graph, so that the pull
+  // kernels of the slot leave it alone.
+  int dir = 0;
+  long long push_thr = 0;
+  uint32_t* push_acc = nullptr;
 };
 
 // Address of the level of (vertex i, source s) in either layout.
@@ -130,6 +140,7 @@ __global__ void __launch_bounds__(kTPB, KW <= 2 ? 6 : 4) k_step(Args a) {
   __shared__ int arrived_sh;
   volatile int* c = a.ctl;
   if (c[1]) return;  // done (the same for every block)
+  if (a.dir && (c[7] || c[6] == 1)) return;  // this slot's level ran as a push
   if (threadIdx.x == 0) {
     cnt_sh = 0ull;
     arrived_sh = 0;
@@ -326,12 +337,62 @@ __global__ void __launch_bounds__(kTPB, KW <= 2 ? 6 : 4) k_step(Args a) {
   }
 }
 
+// Block count of a level and its close: the last block to arrive (arrival
+// ticket in ctl[2], no waiting) advances the level, stops at a zero count or
+// the iteration cap and, with dir, picks the next level's mode; `pushed`
+// marks a level that ran as a push, so that the slot's pull kernels skip.
+__device__ __forceinline__ void close_level(const Args& a, unsigned long long cnt, bool pushed) {
+  volatile int* c = a.ctl;
+  const unsigned lane = threadIdx.x & 31;
+  __shared__ unsigned long long sh;
+  __shared__ bool last;
+  if (threadIdx.x == 0) sh = 0;
+  __syncthreads();
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  if (lane == 0 && cnt) atomicAdd(&sh, cnt);
+  __syncthreads();
+  unsigned long long* count = reinterpret_cast<unsigned long long*>(a.ctl + 4);
+  if (threadIdx.x == 0) {
+    if (sh) atomicAdd(count, sh);
+    __threadfence();
+    last = atomicAdd(reinterpret_cast<unsigned*>(a.ctl + 2), 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    volatile unsigned long long* vc = count;
+    const unsigned long long total = *vc;
+    const int it = c[0] + 1;
+    const bool stop = total == 0ull || it >= c[3];
+    if (a.dir) {
+      c[6] = (long long)total < a.push_thr ? 1 : 0;
+      c[7] = pushed ? 1 : 0;
+    }
+    c[0] = it;
+    *vc = 0ull;
+    a.ctl[2] = 0;
+    if (stop) c[1] = 1;
+    __threadfence();
+  }
+}
+
 // Split block rows (one warp each): OR the slot accumulators and run the
 // epilogue.  The last block closes the level (arrival ticket, no waiting).
 template <int KW>
 __global__ void __launch_bounds__(kTPB) k_finish(Args a) {
   volatile int* c = a.ctl;
   if (c[1]) return;
+  if (a.dir && c[7]) {
+    // the slot's level ran as a push: every block takes a ticket and the
+    // last one clears the flag for the next slot (all blocks have read it)
+    if (threadIdx.x == 0 &&
+        atomicAdd(reinterpret_cast<unsigned*>(a.ctl + 2), 1u) == gridDim.x - 1) {
+      a.ctl[2] = 0;
+      c[7] = 0;
+      __threadfence();
+    }
+    return;
+  }
   const int lvl = c[0];
   const GView& v = a.v;
   const unsigned lane = threadIdx.x & 31;
@@ -350,31 +411,114 @@ __global__ void __launch_bounds__(kTPB) k_finish(Args a) {
       a.fbits[(size_t)((lvl + 1) & 1) * (v.nbr + 1) + sp.row] = 0u;
     }
   }
-  __shared__ unsigned long long sh;
-  __shared__ bool last;
-  if (threadIdx.x == 0) sh = 0;
-  __syncthreads();
-  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-  if (lane == 0 && cnt) atomicAdd(&sh, cnt);
-  __syncthreads();
-  unsigned long long* count = reinterpret_cast<unsigned long long*>(a.ctl + 4);
-  if (threadIdx.x == 0) {
-    if (sh) atomicAdd(count, sh);
-    __threadfence();
-    last = atomicAdd(reinterpret_cast<unsigned*>(a.ctl + 2), 1u) == gridDim.x - 1;
+  close_level(a, cnt, false);
+}
+
+// Push level, one warp per work item (a block row R, or a piece of a long
+// one) with frontier vertices in R: the (tile, row) pairs with row r in the
+// frontier and non-empty in the tile are dealt out to the lanes, and every
+// column x of the row word gets the frontier row of vertex 32R + r OR-ed
+// into push_acc[x].  On a symmetric graph push_acc[x]
+// is then the OR of the frontier rows of x's neighbours, which is what the
+// pull step accumulates for row x.  k <= 64 (KW <= 2): lane r holds vertex
+// 32R + r's frontier row in registers.
+template <int KW>
+__global__ void __launch_bounds__(kTPB) k_push(Args a) {
+  static_assert(KW <= 2, "push levels hold frontier rows in registers");
+  volatile int* c = a.ctl;
+  if (c[1] || c[7] || c[6] != 1) return;
+  const int lvl = c[0];
+  const GView& v = a.v;
+  const unsigned lane = threadIdx.x & 31;
+  const long long item = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (item >= v.nitems) return;
+  const gbo_item it = v.items[item];
+  const long long R = it.row;
+  const uint32_t fword = a.fbits[(size_t)(lvl & 1) * (v.nbr + 1) + R];
+  if (fword == 0u) return;
+  const uint32_t* __restrict__ F = a.F + (size_t)(lvl & 1) * a.fstride;
+  uint32_t fr0 = 0u, fr1 = 0u;
+  if ((fword >> (31 - lane)) & 1u) {  // only frontier rows are valid (and in bounds)
+    const size_t o = ((size_t)R * 32 + lane) * KW;
+    fr0 = F[o];
+    if (KW == 2) fr1 = F[o + 1];
   }
-  __syncthreads();
-  if (last && threadIdx.x == 0) {
-    __threadfence();
-    volatile unsigned long long* vc = count;
-    const int it = c[0] + 1;
-    const bool stop = *vc == 0ull || it >= c[3];
-    c[0] = it;
-    *vc = 0ull;
-    a.ctl[2] = 0;
-    if (stop) c[1] = 1;
-    __threadfence();
+  const unsigned frows = __brev(fword);  // bit r: vertex 32R + r in the frontier
+  const uint32_t* __restrict__ val = reinterpret_cast<const uint32_t*>(v.val);
+  const unsigned* __restrict__ rm = v.rowmask;
+  uint32_t* __restrict__ acc = a.push_acc;
+  const int t0 = it.t0, t1 = it.t1;
+  for (int b0 = t0; b0 < t1; b0 += 32) {
+    const int t = b0 + (int)lane;
+    int cb = 0;
+    unsigned cand = 0u;
+    if (t < t1) {
+      cb = v.colind[t];
+      cand = (rm ? rm[t] : 0xffffffffu) & frows;
+    }
+    const int cnt = __popc(cand);
+    const int incl = warp_incl_sum(cnt, lane);
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    const int excl = incl - cnt;
+    for (int pb = 0; pb < total; pb += 32) {
+      const int p = pb + (int)lane;
+      int j = 0;
+#pragma unroll
+      for (int st = 16; st > 0; st >>= 1) {
+        const int q = __shfl_sync(0xffffffffu, incl, j + st - 1);
+        if (q <= p) j += st;
+      }
+      const int ej = __shfl_sync(0xffffffffu, excl, j);
+      const unsigned cj = __shfl_sync(0xffffffffu, cand, j);
+      const int xbase = __shfl_sync(0xffffffffu, cb, j) * 32;
+      int r = 0;
+      uint32_t word = 0u;
+      if (p < total) {
+        r = (int)__fns(cj, 0, p - ej + 1);
+        word = val[(size_t)(b0 + j) * 32 + r];
+      }
+      const uint32_t f0 = __shfl_sync(0xffffffffu, fr0, r);
+      const uint32_t f1 = __shfl_sync(0xffffffffu, fr1, r);
+      if (!(f0 | f1)) word = 0u;
+      while (word) {
+        const int col = __clz(word);
+        word &= ~(0x80000000u >> col);
+        const size_t xo = (size_t)(xbase + col) * KW;
+        if (f0) atomicOr(acc + xo, f0);
+        if (KW == 2 && f1) atomicOr(acc + xo + 1, f1);
+      }
+    }
   }
+}
+
+// After k_push: the epilogue of every block row from push_acc (zeroed
+// again), then the level close.  Block rows without new bits only clear
+// their next-frontier word.
+template <int KW>
+__global__ void __launch_bounds__(kTPB) k_push_fin(Args a) {
+  volatile int* c = a.ctl;
+  if (c[1] || c[7] || c[6] != 1) return;
+  const int lvl = c[0];
+  const GView& v = a.v;
+  const unsigned lane = threadIdx.x & 31;
+  const long long R = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  unsigned long long cnt = 0;
+  if (R < v.nbr) {
+    uint32_t* na = a.push_acc + (size_t)R * 32 * KW;
+    uint32_t any = 0u;
+    for (int q = lane; q < 32 * KW; q += 32) any |= na[q];
+    const uint32_t vrow = a.vfull[R];
+    if (vrow != 0xffffffffu && __any_sync(0xffffffffu, any != 0u)) {
+      block_row_epilogue<KW>(a, (int)R, lvl, vrow, lane, [&](int r, int ww) { return na[r * KW + ww]; },
+                             cnt);
+      __syncwarp();
+    } else if (lane == 0) {
+      a.fbits[(size_t)((lvl + 1) & 1) * (v.nbr + 1) + R] = 0u;
+    }
+    if (__any_sync(0xffffffffu, any != 0u))
+      for (int q = lane; q < 32 * KW; q += 32) na[q] = 0u;
+  }
+  close_level(a, cnt, true);
 }
 
 // Reset: levels -1, V 0, F[0] 0, frontier bits 0, padding rows and rows
@@ -404,6 +548,8 @@ static __global__ void k_init(Args a, int kw, int max_iter) {
     a.ctl[2] = 0;
     a.ctl[3] = max_iter;
     reinterpret_cast<unsigned long long*>(a.ctl + 4)[0] = 0ull;
+    a.ctl[6] = a.dir ? 1 : 0;  // k sources: the first level pushes
+    a.ctl[7] = 0;
   }
 }
 

@@ -28,6 +28,7 @@ struct MsState {
   uint32_t* vfull = nullptr;
   uint32_t* split_acc = nullptr;
   int* slot_split = nullptr;
+  uint32_t* push_acc = nullptr;  // nbr * 32 * kw (push levels; k <= 64 on symmetric graphs)
   int* srcs = nullptr;
   int* ctl = nullptr;
   int* h_ctl = nullptr;
@@ -38,11 +39,20 @@ struct MsState {
   cudaGraphExec_t exec = nullptr;
   const void* key_levels = nullptr;
   int key_k = -1;
+  long long key_push = -1;  // push threshold the graph was captured with (0: pull only)
   std::vector<float> step_ms;
   long long launches = 0;
   int launches_per_replay = 0;
   cudaEvent_t ev[2 * kLevelsPerGraph] = {};
 };
+
+// Levels with fewer new (vertex, source) pairs than this run as pushes: on
+// symmetric graphs with k <= 64 when the caller set a positive BFS push
+// threshold (gbo_graph_set_bfs_direction); otherwise (0) every level pulls.
+long long ms_push_threshold(const gbo_graph* g, int kw) {
+  if (!g->symmetric || kw > 2 || g->bfs_push_thr <= 0) return 0;
+  return g->bfs_push_thr;
+}
 
 ms::Args make_args(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
   ms::Args a;
@@ -61,6 +71,9 @@ ms::Args make_args(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
   a.active = nullptr;
   a.live = m.live;
   a.level_group = 0;  // the API's vertex-major levels[v * k + s]
+  a.push_thr = ms_push_threshold(g, m.kw);
+  a.dir = a.push_thr > 0 ? 1 : 0;
+  a.push_acc = a.dir ? m.push_acc : nullptr;
   return a;
 }
 
@@ -70,12 +83,22 @@ int ms_capture(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
   const unsigned gi = blocks_for_warps(g->nitems, ms::kWarps);
   const unsigned gs = blocks_for_warps(g->nsplit > 0 ? g->nsplit : 1, ms::kWarps);
   cudaGraph_t graph = nullptr;
+  // with push levels a slot is push, push-finish, pull, finish (each
+  // level runs in one of the two halves) and its events bracket all four
+  const unsigned gr = blocks_for_warps(g->nbr > 0 ? g->nbr : 1, ms::kWarps);
   GBO_CUDA_TRY(cudaStreamBeginCapture(m.cap, cudaStreamCaptureModeThreadLocal));
   for (int q = 0; q < kLevelsPerGraph; ++q) {
     cudaEventRecordWithFlags(m.ev[2 * q], m.cap, cudaEventRecordExternal);
+    if constexpr (KW <= 2) {
+      if (a.dir) {
+        if (g->nitems > 0) ms::k_push<KW><<<gi, ms::kTPB, 0, m.cap>>>(a);
+        ms::k_push_fin<KW><<<gr, ms::kTPB, 0, m.cap>>>(a);
+      }
+    }
     if (g->nitems > 0) ms::k_step<KW><<<gi, ms::kTPB, 0, m.cap>>>(a);
+    if (a.dir) ms::k_finish<KW><<<gs, ms::kTPB, 0, m.cap>>>(a);
     cudaEventRecordWithFlags(m.ev[2 * q + 1], m.cap, cudaEventRecordExternal);
-    ms::k_finish<KW><<<gs, ms::kTPB, 0, m.cap>>>(a);
+    if (!a.dir) ms::k_finish<KW><<<gs, ms::kTPB, 0, m.cap>>>(a);
   }
   cudaError_t e = cudaStreamEndCapture(m.cap, &graph);
   if (e != cudaSuccess) return fail_cuda(e, "multi-source BFS capture");
@@ -84,7 +107,7 @@ int ms_capture(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
   e = cudaGraphInstantiate(&m.exec, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) return fail_cuda(e, "multi-source BFS instantiate");
-  m.launches_per_replay = kLevelsPerGraph * ((g->nitems > 0) + 1);
+  m.launches_per_replay = kLevelsPerGraph * ((g->nitems > 0) * (a.dir ? 2 : 1) + 1 + (a.dir ? 1 : 0));
   return GBO_OK;
 }
 
@@ -115,12 +138,18 @@ int msbfs_impl(gbo_graph* g, const int* h_srcs, int k, int32_t* d_levels, int* h
     cudaFree(m.V);
     cudaFree(m.split_acc);
     cudaFree(m.slot_split);
-    m.F = m.V = m.split_acc = nullptr;
+    cudaFree(m.push_acc);
+    m.F = m.V = m.split_acc = m.push_acc = nullptr;
     m.slot_split = nullptr;
     m.kw = 0;
     GBO_CUDA_TRY(cudaMalloc(&m.F, sizeof(uint32_t) * 2 * (size_t)n * kw + 16));
     GBO_CUDA_TRY(cudaMalloc(&m.V, sizeof(uint32_t) * (size_t)n * kw + 16));
     GBO_TRY(ms::split_state(g, kw, &m.split_acc, &m.slot_split, s));
+    if (kw <= 2) {  // push levels' accumulator, zero between levels
+      const size_t pw = (size_t)(g->nbr > 0 ? g->nbr : 1) * 32 * (size_t)kw;
+      GBO_CUDA_TRY(cudaMalloc(&m.push_acc, sizeof(uint32_t) * pw));
+      GBO_CUDA_TRY(cudaMemsetAsync(m.push_acc, 0, sizeof(uint32_t) * pw, s));
+    }
     m.kw = kw;
   }
   if (k > m.ksrc) {
@@ -130,7 +159,8 @@ int msbfs_impl(gbo_graph* g, const int* h_srcs, int k, int32_t* d_levels, int* h
     m.ksrc = k;
   }
   GBO_CUDA_TRY(cudaMemcpyAsync(m.srcs, h_srcs, sizeof(int) * (size_t)k, cudaMemcpyHostToDevice, s));
-  if (!m.exec || m.key_levels != d_levels || m.key_k != k) {
+  const long long push_thr = ms_push_threshold(g, kw);
+  if (!m.exec || m.key_levels != d_levels || m.key_k != k || m.key_push != push_thr) {
     int st = GBO_OK;
     switch (kw) {
       case 1: st = ms_capture<1>(g, m, d_levels, k); break;
@@ -143,6 +173,7 @@ int msbfs_impl(gbo_graph* g, const int* h_srcs, int k, int32_t* d_levels, int* h
     GBO_TRY(st);
     m.key_levels = d_levels;
     m.key_k = k;
+    m.key_push = push_thr;
   }
   const ms::Args a = make_args(g, m, d_levels, k);
   const int max_iter = n + 1;
@@ -234,6 +265,7 @@ void free_ms_state(gbo_graph* g) {
   cudaFree(m->vfull);
   cudaFree(m->split_acc);
   cudaFree(m->slot_split);
+  cudaFree(m->push_acc);
   cudaFree(m->srcs);
   cudaFree(m->ctl);
   cudaFreeHost(m->h_ctl);

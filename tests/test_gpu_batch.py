@@ -38,6 +38,53 @@ def test_msbfs_split_rows_and_duplicates(gbo, orc, gpu):
     assert np.array_equal(lv, oracle_levels(orc, csr, srcs))
 
 
+@pytest.mark.parametrize("push", [0, 64, 2**31 - 1])
+@pytest.mark.parametrize("k", [1, 5, 32, 33, 64])
+def test_msbfs_push_levels_on_symmetric_graphs(gbo, orc, gpu, k, push):
+    """On symmetric graphs with k <= 64 levels may push (frontier rows
+    scattered to the neighbours): never (0), below 64 new (vertex, source)
+    pairs, or always (2^31 - 1) -- the levels are the per-source BFS levels
+    every time."""
+    rng = np.random.default_rng(100 + k)
+    # vertices 2000..2999 of the last graph have no edges (sources there too)
+    e = rng.integers(0, 2000, (2, 12000)).astype(np.int32)
+    island = gbo.csr_from_edges(e[0], e[1], 3000, True, True)
+    graphs = (gbo.gen_rmat(12, 16, seed=0), gbo.gen_er(1000, 0.02002, 0), gbo.gen_king_mesh(33), island)
+    for csr in graphs:
+        g = gbo.Graph.from_csr(csr, 32, gbo.FLAG_SYMMETRIC)
+        g.set_bfs_direction(True, push)
+        srcs = rng.integers(0, csr.nrows, k).astype(np.int32)
+        if csr is island:
+            srcs[0] = 2500
+            srcs[-1] = srcs[0] if k > 1 else srcs[-1]  # a duplicate
+        lv, depth = g.msbfs(srcs)
+        want = oracle_levels(orc, csr, srcs)
+        assert np.array_equal(lv, want), (csr.nrows, k, push)
+        assert depth == int(want.max()) + 1
+        # a second call on the same handle (captured graph reused)
+        lv2, _ = g.msbfs(srcs)
+        assert np.array_equal(lv2, want)
+        g.free()
+
+
+def test_msbfs_push_levels_split_rows(gbo, orc, gpu):
+    n = 20000
+    src = np.zeros(n - 1, np.int32)
+    dst = np.arange(1, n, dtype=np.int32)
+    rng = np.random.default_rng(2)
+    src = np.concatenate([src, rng.integers(0, n, 30000)]).astype(np.int32)
+    dst = np.concatenate([dst, rng.integers(0, n, 30000)]).astype(np.int32)
+    csr = gbo.csr_from_edges(src, dst, n, True, True)
+    g = gbo.Graph.from_csr(csr, 32, gbo.FLAG_SYMMETRIC)
+    assert g.info().nsplit_rows > 0
+    srcs = np.array([5, 5, 0, 19999, 123] * 12 + [7, 8], np.int32)
+    want = oracle_levels(orc, csr, srcs)
+    for push in (64, 2**31 - 1, 0, -1, 64):  # the mode may change between calls
+        g.set_bfs_direction(True, push)
+        lv, _ = g.msbfs(srcs)
+        assert np.array_equal(lv, want), push
+
+
 def test_msbfs_rejects_other_tiles(gbo, gpu):
     g = gbo.Graph.from_csr(gbo.gen_er(200, 0.05, 1), 16)
     with pytest.raises(gbo.GboError) as e:
