@@ -1,0 +1,74 @@
+"""The benchmark's algorithmic-bytes model of a BFS pull step
+(bench.bfs_level_bytes), which sets the roofline's `achieved`, against a
+direct count over the tiles of a small graph (CPU only)."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+import bench  # noqa: E402
+
+
+def block_structure(csr, b):
+    """Block-row offsets and block-column indices of the B2SR tiles of a CSR."""
+    nbr = (csr.nrows + b - 1) // b
+    rows = np.repeat(np.arange(csr.nrows), np.diff(csr.rowptr))
+    keys = np.unique((rows // b).astype(np.int64) * (1 << 32) + csr.colind // b)
+    br, bc = keys >> 32, keys & 0xFFFFFFFF
+    rowptr_b = np.zeros(nbr + 1, np.int64)
+    np.add.at(rowptr_b, br + 1, 1)
+    return np.cumsum(rowptr_b), bc.astype(np.int64)
+
+
+def direct_bytes(csr, rowptr_b, colind_b, levels, b, layout):
+    """Bytes of each pull step, counted tile by tile from the model's words."""
+    n, nbr = csr.nrows, len(rowptr_b) - 1
+    wb = max(1, b // 8)
+    deg = np.diff(csr.rowptr)
+    occ = b == 32 and layout == "row"
+    out = []
+    for L in range(int(levels.max()) + 1):
+        unvisited = [(levels[v] == -1 or levels[v] > L) for v in range(n)]
+        frontier = [levels[v] == L for v in range(n)]
+        by = 4 * (nbr + 1) + 2 * wb * nbr
+        by += 4 * int((levels == L + 1).sum())
+        by += wb * sum(any(levels[v] == L + 1 for v in range(R * b, min(n, R * b + b))) for R in range(nbr))
+        for R in range(nbr):
+            rows = range(R * b, min(n, R * b + b))
+            open_rows = [v for v in rows if unvisited[v] and deg[v] > 0]
+            if not open_rows:
+                continue
+            for t in range(rowptr_b[R], rowptr_b[R + 1]):
+                C = colind_b[t]
+                cols = range(C * b, min(n, C * b + b))
+                by += 4 * (2 if occ else 1)  # block-column index (+ occupancy word)
+                fr = [u for u in cols if frontier[u]]
+                if not fr:
+                    continue
+                if occ:  # non-empty row words of unvisited rows
+                    for v in rows:
+                        if not unvisited[v]:
+                            continue
+                        nb = csr.colind[csr.rowptr[v]:csr.rowptr[v + 1]]
+                        if np.any((nb >= C * b) & (nb < C * b + b)):
+                            by += wb
+                elif layout == "col":
+                    by += wb * len(fr)
+                else:
+                    by += wb * len(open_rows)
+        out.append(by)
+    return out
+
+
+@pytest.mark.parametrize("b,layout", [(8, "row"), (32, "row"), (16, "col"), (32, "col")])
+def test_bfs_level_bytes_matches_direct_count(gbo, orc, b, layout):
+    csr = gbo.gen_rmat(9, 6, seed=4)
+    levels, _ = orc.bfs_csr(csr.rowptr, csr.colind, csr.nrows, 0)
+    levels = np.asarray(levels, np.int64)
+    rowptr_b, colind_b = block_structure(csr, b)
+    live = np.diff(csr.rowptr) > 0
+    got = bench.bfs_level_bytes(rowptr_b, colind_b, levels, csr.nrows, b, live, layout, csr)
+    want = direct_bytes(csr, rowptr_b, colind_b, levels, b, layout)
+    assert got == want
