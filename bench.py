@@ -244,6 +244,24 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ CPU legs
+def cpu_bfs_single(csr, tile):
+    """One run of the same CPU BFS on one thread: (GTEPS, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    bs = oracle.pack(csr.rowptr, csr.colind, csr.nrows, csr.ncols, tile)
+    lv, _ = oracle.bfs_b2sr(bs, 0)
+    threads = oracle.max_threads()
+    oracle.set_threads(1)
+    try:
+        t0 = time.perf_counter()
+        oracle.bfs_b2sr(bs, 0)
+        t = time.perf_counter() - t0
+    finally:
+        oracle.set_threads(threads)
+    return traversed_edges(csr, lv) / t / 1e9, t
+
+
 def cpu_bfs(csr, tile, samples):
     """The oracle's port of the reference BFS loop (algorithm/bfs.cu:508-564)
     on B2SR with OpenMP over block rows; returns (GTEPS, seconds, threads)."""
@@ -601,9 +619,11 @@ def run_ours(args, ws, rank, local):
     }
     if rank == 0 and ws == 1 and not args.no_cpu:
         v, t, cores, _ = cpu_bfs(csr, args.tile, args.cpu_samples)
+        v1, t1 = cpu_bfs_single(csr, args.tile)
         line["cpu_baseline"] = {"value": v, "unit": "GTEPS", "cores": cores, "kind": "port",
                                 "sample": f"{args.cpu_samples} full BFS runs from vertex 0 "
-                                          f"(median {t:.2f} s), oracle port of algorithm/bfs.cu:508-564"}
+                                          f"(median {t:.2f} s), oracle port of algorithm/bfs.cu:508-564",
+                                "single_thread": {"value": v1, "unit": "GTEPS", "seconds": t1}}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if g_row is not g:

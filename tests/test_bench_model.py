@@ -72,3 +72,11 @@ def test_bfs_level_bytes_matches_direct_count(gbo, orc, b, layout):
     got = bench.bfs_level_bytes(rowptr_b, colind_b, levels, csr.nrows, b, live, layout, csr)
     want = direct_bytes(csr, rowptr_b, colind_b, levels, b, layout)
     assert got == want
+
+
+def test_cpu_baseline_single_thread_restores_threads(gbo, orc):
+    csr = gbo.gen_rmat(10, 8, seed=1)
+    before = orc.max_threads()
+    v1, t1 = bench.cpu_bfs_single(csr, 32)
+    assert v1 > 0 and t1 > 0
+    assert orc.max_threads() == before
