@@ -57,7 +57,10 @@ def parse():
                          "a level of k <= 64 pushes (-1: the library default, pull)")
     ap.add_argument("--serve-rates", default="1000,10000,100000",
                     help="offered rates of --workload serve (queries/s, comma-separated)")
-    ap.add_argument("--workload", default="bfs", choices=["bfs"] + list(SUITE),
+    ap.add_argument("--ref-scale", type=int, default=21,
+                    help="R-MAT scale of --impl reference --workload refgpu (int32 word offsets of the reference)")
+    ap.add_argument("--ref-widths", default="4,8,16,32,64", help="tile widths of the refgpu BMV pairs")
+    ap.add_argument("--workload", default="bfs", choices=["bfs", "refgpu"] + list(SUITE),
                     help="bfs: the headline line; the others print one line each for the "
                          "remaining workloads (SSSP/CC/PR on R-MAT 22, TC, MS-BFS, many-graph "
                          "batch, PPR forward/adjoint, served streams)")
@@ -244,71 +247,77 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ CPU legs
-def cpu_bfs_single(csr, tile):
-    """One run of the same CPU BFS on one thread: (GTEPS, seconds)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-
-    bs = oracle.pack(csr.rowptr, csr.colind, csr.nrows, csr.ncols, tile)
-    lv, _ = oracle.bfs_b2sr(bs, 0)
-    threads = oracle.max_threads()
-    oracle.set_threads(1)
+def cpu_bfs_single(orc, bs, csr, samples):
+    """The same CPU BFS on one thread, median of `samples` runs: (GTEPS, seconds)."""
+    lv, _ = orc.bfs_b2sr(bs, 0)
+    threads = orc.max_threads()
+    orc.set_threads(1)
+    times = []
     try:
-        t0 = time.perf_counter()
-        oracle.bfs_b2sr(bs, 0)
-        t = time.perf_counter() - t0
+        for _ in range(max(1, samples)):
+            t0 = time.perf_counter()
+            orc.bfs_b2sr(bs, 0)
+            times.append(time.perf_counter() - t0)
     finally:
-        oracle.set_threads(threads)
+        orc.set_threads(threads)
+    t = float(np.median(times))
     return traversed_edges(csr, lv) / t / 1e9, t
 
 
-def cpu_bfs(csr, tile, samples):
+def cpu_bfs(orc, bs, csr, samples):
     """The oracle's port of the reference BFS loop (algorithm/bfs.cu:508-564)
-    on B2SR with OpenMP over block rows; returns (GTEPS, seconds, threads)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-
-    bs = oracle.pack(csr.rowptr, csr.colind, csr.nrows, csr.ncols, tile)
-    lv, _ = oracle.bfs_b2sr(bs, 0)
+    on B2SR with OpenMP over block rows; returns (GTEPS, seconds, threads,
+    levels, depth)."""
+    lv, depth = orc.bfs_b2sr(bs, 0)
     edges = traversed_edges(csr, lv)
     times = []
     for _ in range(max(1, samples)):
         t0 = time.perf_counter()
-        oracle.bfs_b2sr(bs, 0)
+        orc.bfs_b2sr(bs, 0)
         times.append(time.perf_counter() - t0)
     t = float(np.median(times))
-    return edges / t / 1e9, t, oracle.max_threads(), edges
+    return edges / t / 1e9, t, orc.max_threads(), lv, depth
+
+
+def bfs_config(args, n, nnz, nblocks, edges, depth, ws):
+    """The `config` object of the BFS line, shared by both arms so that the
+    same workload is named by the same keys and values."""
+    nbr = (n + args.tile - 1) // args.tile
+    wb = max(1, args.tile // 8)
+    return {"workload": workload_name(args.scale, args.tile, args.layout), "scale": args.scale,
+            "tile_bits": args.tile, "layout": args.layout, "nvertices": n, "nnz": int(nnz),
+            "nblocks": int(nblocks), "b2sr_gb": (4 * (nbr + 1) + 4 * nblocks + nblocks * args.tile * wb) / 1e9,
+            "traversed_edges": int(edges), "bfs_depth": int(depth),
+            "l2": "inputs larger than L2 (B2SR tiles far above 126 MB)",
+            "parallelism": "replicas" if ws > 1 else "single"}
 
 
 def run_reference(args, ws, rank):
     """--impl reference: the reference path's CPU restatement (the reference
     has no CPU implementation of its own; its drivers need a GPU and removed
-    cuSPARSE APIs), all host threads, same workload, metric and unit."""
+    cuSPARSE APIs), all host threads, same workload, metric and unit.  The
+    input graph, the packing and the traversal all come from the oracle, so
+    this arm loads no product library."""
     if rank != 0:
         return
-    import gbo
-
-    csr = gbo.gen_rmat(args.scale, EDGE_FACTOR, seed=SEED, **RMAT)
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-
-    bs = oracle.pack(csr.rowptr, csr.colind, csr.nrows, csr.ncols, args.tile)
-    lv, _ = oracle.bfs_b2sr(bs, 0)
+    orc = _oracle()
+    csr = orc.gen_rmat(args.scale, EDGE_FACTOR, seed=SEED, **RMAT)
+    bs = orc.pack(csr.rowptr, csr.colind, csr.nrows, csr.ncols, args.tile)
+    lv, depth = orc.bfs_b2sr(bs, 0)
     edges = traversed_edges(csr, lv)
     for _ in range(args.warmup):
-        oracle.bfs_b2sr(bs, 0)
+        orc.bfs_b2sr(bs, 0)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        oracle.bfs_b2sr(bs, 0)
+        orc.bfs_b2sr(bs, 0)
     dt = (time.perf_counter() - t0) / args.steps
     v = edges / dt / 1e9
     line = {
         "impl": "reference", "metric": "GTEPS", "value": v, "unit": "GTEPS", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": workload_name(args.scale, args.tile, args.layout), "scale": args.scale,
-                   "tile_bits": args.tile, "traversed_edges": edges},
-        "cpu_baseline": {"value": v, "unit": "GTEPS", "cores": oracle.max_threads(), "kind": "port",
+        "config": bfs_config(args, csr.nrows, csr.nnz, bs.nblk, edges, depth, ws),
+        "cpu_baseline": {"value": v, "unit": "GTEPS", "cores": orc.max_threads(), "kind": "port",
                          "sample": f"{args.steps} full BFS runs from vertex 0 (oracle port of "
                                    "algorithm/bfs.cu:508-564 on B2SR, OpenMP over block rows)"},
         "e2e": {"value": v, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -418,7 +427,7 @@ def run_ours(args, ws, rank, local):
     n = csr.nrows
     d_level = gbo.DeviceBuffer(4 * n)
 
-    # correctness of the timed path against an independent CPU BFS (rank 0)
+    # levels of the timed workload (compared with the oracle in the CPU leg)
     levels, depth = g.bfs(0)
     edges = traversed_edges(csr, levels)
 
@@ -517,6 +526,7 @@ def run_ours(args, ws, rank, local):
     # batched: k sources per multi-source BFS (bit frontier matrix) vs one
     # source per plain BFS, same graph, queries per second
     batched = {}
+    ms_sample = None
     rng = np.random.default_rng(3)
     for kq in (64, 1024):
         srcs = rng.integers(0, n, kq).astype(np.int32)
@@ -532,6 +542,9 @@ def run_ours(args, ws, rank, local):
         mms = ev0.elapsed_ms(ev1) / reps
         batched[f"k{kq}"] = {"ms": mms, "qps": kq / (mms / 1e3),
                             "qps_vs_plain": (kq / mms) / (1.0 / ms)}
+        if kq == 1024:  # 16 seeded columns kept for the CPU leg's parity check
+            ms_cols = np.random.default_rng(17).choice(kq, 16, replace=False)
+            ms_sample = (srcs[ms_cols], ms_columns(gbo, d_lv, n, kq, ms_cols))
         d_lv.free()
 
     # permuted variant (reported beside the headline, never as it): the same
@@ -588,14 +601,11 @@ def run_ours(args, ws, rank, local):
         "metric": "GTEPS", "value": gteps, "unit": "GTEPS", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": workload_name(args.scale, args.tile, args.layout), "scale": args.scale,
-                   "tile_bits": args.tile, "layout": args.layout, "nvertices": n, "nnz": csr.nnz,
-                   "nblocks": int(info.nblocks), "b2sr_gb": info.b2sr_bytes / 1e9,
-                   "traversed_edges": edges, "bfs_depth": depth,
-                   "l2": "inputs larger than L2 (B2SR tiles far above 126 MB)",
-                   "parallelism": "replicas" if ws > 1 else "single"},
+        "config": bfs_config(args, n, csr.nnz, int(info.nblocks), edges, depth, ws),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
+                     "traffic_source": ("scaled from the R-MAT 20 ncu capture in profiles/ by algorithmic bytes"
+                                        if traffic is not None else None),
                      "kernel": f"k_bfs_step<{args.tile}> (BFS pull step, mean over levels)",
                      "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": float(np.mean(lvl_bytes[:k])),
@@ -618,12 +628,34 @@ def run_ours(args, ws, rank, local):
         "permuted_variant": permuted,
     }
     if rank == 0 and ws == 1 and not args.no_cpu:
-        v, t, cores, _ = cpu_bfs(csr, args.tile, args.cpu_samples)
-        v1, t1 = cpu_bfs_single(csr, args.tile)
+        # CPU leg: the oracle's port of the reference BFS loop, timed, and its
+        # levels (plus an independent queue BFS on the CSR) compared with the
+        # GPU's levels of the timed workload
+        orc = _oracle()
+        bs = orc.pack(csr.rowptr, csr.colind, csr.nrows, csr.ncols, args.tile)
+        v, t, cores, lv_port, d_port = cpu_bfs(orc, bs, csr, args.cpu_samples)
+        v1, t1 = cpu_bfs_single(orc, bs, csr, max(3, args.cpu_samples))
+        if ms_sample is not None:
+            ok = all(np.array_equal(col, orc.bfs_b2sr(bs, int(src))[0])
+                     for src, col in zip(ms_sample[0], ms_sample[1].T))
+            line["batched_bfs"]["parity"] = {
+                "checked": "16 seeded columns of the k = 1024 multi-source BFS against one oracle BFS each",
+                "equal": bool(ok)}
+        del bs
+        lv_q, d_q = orc.bfs_csr(csr.rowptr, csr.colind, n, 0)
         line["cpu_baseline"] = {"value": v, "unit": "GTEPS", "cores": cores, "kind": "port",
                                 "sample": f"{args.cpu_samples} full BFS runs from vertex 0 "
                                           f"(median {t:.2f} s), oracle port of algorithm/bfs.cu:508-564",
-                                "single_thread": {"value": v1, "unit": "GTEPS", "seconds": t1}}
+                                "single_thread": {"value": v1, "unit": "GTEPS", "seconds": t1,
+                                                  "samples": max(3, args.cpu_samples)}}
+        line["parity"] = {
+            "checked": f"int32 BFS levels of all {n} vertices from gbo_bfs against the oracle's port of "
+                       "algorithm/bfs.cu:508-564 on B2SR and against a queue BFS on the CSR",
+            "equal": bool(np.array_equal(levels, lv_port) and np.array_equal(levels, lv_q)
+                          and depth == d_port == d_q),
+            "mismatched_vertices": int(np.count_nonzero(levels != lv_q))}
+    else:
+        line["parity"] = {"checked": False, "why": "CPU leg skipped (--no-cpu or N > 1)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if g_row is not g:
@@ -743,9 +775,14 @@ def suite_config2(args, which):
         cfg["workload"] = f"unit-weight SSSP from vertex 0 (min-plus BMV), R-MAT scale {args.scale}"
         extra = {"iterations": it.value, "traversed_edges": edges, "dtype": "u32"}
         if bs is not None:
-            t = _cpu(lambda: orc.sssp_b2sr(bs, 0))
+            got = buf.to_numpy(np.uint32, n)
+            res = {}
+            t = _cpu(lambda: res.update(d=orc.sssp_b2sr(bs, 0)[0]))
             extra["cpu_baseline"] = {"value": edges / t / 1e9, "unit": "GTEPS", "cores": orc.max_threads(),
                                      "kind": "port", "sample": "1 SSSP from vertex 0 (sssp.cu:420-470 port)"}
+            extra["parity"] = {"checked": f"uint32 distances of all {n} vertices against the oracle's "
+                                          "min-plus SSSP port (sssp.cu:420-470)",
+                               "equal": bool(np.array_equal(got, res["d"]))}
         _line("GTEPS", edges / (ms / 1e3) / 1e9, "GTEPS", True, ms, args, cfg, **extra)
     elif which == "cc":
         ms = _timed(gbo, lambda: gbo.check(gbo.lib().gbo_cc(g.h, buf.ptr, C.byref(it), None)),
@@ -754,9 +791,16 @@ def suite_config2(args, which):
         cfg["workload"] = f"connected components (FastSV, min label), R-MAT scale {args.scale}"
         extra = {"iterations": it.value, "undirected_edges": und, "dtype": "i32"}
         if bs is not None:
-            t = _cpu(lambda: orc.cc(csr.rowptr, csr.colind, n))
+            got = buf.to_numpy(np.int32, n)
+            res = {}
+            t = _cpu(lambda: res.update(lab=orc.cc(csr.rowptr, csr.colind, n)))
             extra["cpu_baseline"] = {"value": und / t / 1e9, "unit": "GTEPS", "cores": orc.max_threads(),
                                      "kind": "port", "sample": "1 CC run (label propagation, min id)"}
+            bad, ncomp = orc.verify_cc(csr.rowptr, csr.colind, n, got)
+            extra["parity"] = {"checked": f"int32 labels of all {n} vertices against the oracle's minimum "
+                                          "vertex id per component, and SimpleVerifyCc (cc.cu:21-60)",
+                               "equal": bool(np.array_equal(got, res["lab"]) and bad == 0),
+                               "components": ncomp}
         _line("GTEPS", und / (ms / 1e3) / 1e9, "GTEPS", True, ms, args, cfg, **extra)
     else:
         iters = 20
@@ -775,11 +819,17 @@ def suite_config2(args, which):
                               "kernel": "PageRank iteration (semiring BMV + update)", "peak_source": psrc,
                               "algorithmic_bytes_per_launch": by, "ms_per_launch": step}}
         if bs is not None:
+            got = buf.to_numpy(np.float32, n).astype(np.float64)
             outdeg = np.bincount(csr.colind, minlength=n).astype(np.int32)
             t = _cpu(lambda: orc.pagerank_b2sr_f32(bs, outdeg, 0.85, iters, -1.0))
             extra["cpu_baseline"] = {"value": iters * csr.nnz / t / 1e9, "unit": "GTEPS",
                                      "cores": orc.max_threads(), "kind": "port",
                                      "sample": "20 PageRank iterations (pr.cu:449-513 port)"}
+            ref, _ = orc.pagerank_f64(csr.rowptr, csr.colind, n, outdeg, 0.85, iters, -1.0)
+            rel = float(np.abs(got - ref).sum() / np.abs(ref).sum())
+            extra["parity"] = {"checked": "20-iteration PageRank vector against the oracle's fp64 PageRank "
+                                          "(pr.cu:449-513 recurrence), relative L1, tolerance 1e-5",
+                               "rel_l1": rel, "equal": bool(rel <= 1e-5)}
         _line("GTEPS", iters * csr.nnz / (ms / 1e3) / 1e9, "GTEPS", True, ms, args, cfg, **extra)
     g.free()
 
@@ -819,13 +869,31 @@ def suite_tc(args):
         extra = {"triangles": count, "tile_table": table, "best": best, "model_tile_input_order": model_best,
                  "dtype": "u64"}
         if not args.no_cpu:
-            t = _cpu(lambda: orc.tc_csr(csr.rowptr, csr.colind, csr.nrows))
+            res = {}
+            t = _cpu(lambda: res.update(n=orc.tc_csr(csr.rowptr, csr.colind, csr.nrows)))
             extra["cpu_baseline"] = {"value": lower_edges / t / 1e9, "unit": "G lower edges/s",
                                      "cores": orc.max_threads(), "kind": "port",
                                      "sample": "1 full count (sorted-adjacency intersection on L)"}
+            extra["parity"] = {"checked": "uint64 triangle count of every tile width and vertex order against "
+                                          "the oracle's sorted-adjacency count"
+                                          + (" and the closed form 4(n-1)^2" if known is not None else ""),
+                               "oracle": res["n"], "equal": bool(count == res["n"])}
         _line("G lower edges/s", lower_edges / (ms / 1e3) / 1e9, "G lower edges/s", True, ms, args,
               {"workload": f"triangle count (masked B2SR SpGEMM on L), {name}", "nvertices": csr.nrows,
                "nnz": csr.nnz}, **extra)
+
+
+def ms_columns(gbo, out, n, k, cols, rows=65536):
+    """Columns `cols` of an (n, k) int32 level matrix on the device, read
+    back in row chunks: an (n, len(cols)) array."""
+    res = np.empty((n, len(cols)), np.int32)
+    for r0 in range(0, n, rows):
+        m = min(rows, n - r0)
+        chunk = np.empty((m, k), np.int32)
+        gbo.check(gbo.lib().gbo_memcpy_d2h(chunk.ctypes.data, out.ptr + 4 * r0 * k, chunk.nbytes, None), "d2h")
+        gbo.check(gbo.lib().gbo_stream_sync(None), "sync")
+        res[r0:r0 + m] = chunk[:, cols]
+    return res
 
 
 def _ms_edges(gbo, out, deg, n, k, rows=65536):
@@ -868,13 +936,24 @@ def suite_msbfs(args):
         edges = _ms_edges(gbo, out, deg, n, k)
         res[k] = {"ms": ms, "qps": k / (ms / 1e3), "gteps_x_k": edges / (ms / 1e3) / 1e9,
                   "speedup_vs_plain": (k / (ms / 1e3)) / (1e3 / plain_ms), "levels_ms": levels_ms}
+        if not args.no_cpu:
+            cols = np.random.default_rng(100 + k).choice(k, min(k, 16), replace=False)
+            got = ms_columns(gbo, out, n, k, cols)
+            orc = _oracle()
+            ok = all(np.array_equal(got[:, i], orc.bfs_csr(csr.rowptr, csr.colind, n, int(srcs[c]))[0])
+                     for i, c in enumerate(cols))
+            res[k]["parity"] = {"checked": f"{len(cols)} seeded columns against one oracle queue BFS each",
+                                "equal": bool(ok)}
         del out
     best = res[max(ks)]
     _line("qps", best["qps"], "queries/s", True, best["ms"], args,
           {"workload": f"multi-source BFS, R-MAT scale {args.ms_scale} ef16 seed 2, k random sources "
                        "(seed 3), B2SR 32",
            "nvertices": n, "nnz": csr.nnz},
-          dtype="u32", by_k=res, plain_qps=1e3 / plain_ms, ms_push=args.ms_push)
+          dtype="u32", by_k=res, plain_qps=1e3 / plain_ms, ms_push=args.ms_push,
+          parity=({"checked": "16 seeded columns per k against one oracle queue BFS each",
+                   "equal": all(r["parity"]["equal"] for r in res.values())}
+                  if not args.no_cpu else {"checked": False}))
     g.free()
 
 
@@ -896,10 +975,11 @@ def suite_batch(args):
     ms = _timed(gbo, lambda: g.bfs_multi(seeds, out=d_level), args.steps, args.warmup)
     info = g.info()
     g.free()
+    union_levels = d_level.to_numpy(np.int32, n)
     # one graph per handle and per BFS call, on a sample of 100 graphs
     rp = csr.rowptr
     ci = csr.colind
-    per = []
+    per, checked = [], []
     rng = np.random.default_rng(7)
     for i in rng.choice(count, 100, replace=False):
         lo, hi = int(off[i]), int(off[i + 1])
@@ -910,13 +990,18 @@ def suite_batch(args):
         buf = gbo.DeviceBuffer(4 * (hi - lo))
         per.append(_timed(gbo, lambda: gs.bfs(0, out=buf), 3, 1))
         gs.free()
+        if not args.no_cpu:
+            want, _ = _oracle().bfs_csr(sub_rp, sub_ci, hi - lo, 0)
+            checked.append(bool(np.array_equal(union_levels[lo:hi], want)))
     one_ms = float(np.mean(per))
     _line("graphs/s", count / (ms / 1e3), "graphs/s", True, ms, args,
           {"workload": "BFS from vertex 0 of each of 10000 ER graphs (n log-uniform 32..65536, avg degree 8, "
                        "seeds 1000+i) packed block-diagonally as one B2SR graph, tile width from the tuner",
            "tile_bits": b, "tuner_bytes": {k: (v if np.isfinite(v) else None) for k, v in tune_cost.items()},
            "nvertices": n, "nnz": csr.nnz, "nblocks": int(info.nblocks), "generate_s": gen_s},
-          dtype="bits", one_by_one_graphs_per_s=1e3 / one_ms, speedup=(count / (ms / 1e3)) / (1e3 / one_ms))
+          dtype="bits", one_by_one_graphs_per_s=1e3 / one_ms, speedup=(count / (ms / 1e3)) / (1e3 / one_ms),
+          parity=({"checked": "levels of 100 seeded graphs of the union against one oracle queue BFS per graph",
+                   "equal": all(checked)} if checked else {"checked": False}))
 
 
 def suite_ppr(args):
@@ -947,6 +1032,18 @@ def suite_ppr(args):
                                                                     1000, dg.ptr, C.byref(it_b), None)),
                  args.steps, args.warmup)
     grad = dg.to_numpy(np.float32, n).astype(np.float64)
+    fwd_p = dp.to_numpy(np.float32, n).astype(np.float64)
+    parity = {"checked": False}
+    if not args.no_cpu:
+        orc = _oracle()
+        outdeg = np.bincount(csr.colind, minlength=n).astype(np.int32)
+        p_ref, _ = orc.ppr_f64(csr.rowptr, csr.colind, n, outdeg, v, 0.85, 1e-13)
+        g_ref, _ = orc.ppr_adjoint_f64(csr.rowptr, csr.colind, n, outdeg, w, 0.85, 1e-13)
+        rf = float(np.abs(fwd_p - p_ref).sum() / np.abs(p_ref).sum())
+        rb = float(np.abs(grad - g_ref).sum() / np.abs(g_ref).sum())
+        parity = {"checked": "PPR vector and gradient against the oracle's fp64 forward and adjoint solves "
+                             "(tol 1e-13), relative L1, tolerance 1e-5",
+                  "forward_rel_l1": rf, "gradient_rel_l1": rb, "equal": bool(rf <= 1e-5 and rb <= 1e-5)}
     errs = []
     for _ in range(64):
         d = np.zeros(n)
@@ -959,7 +1056,7 @@ def suite_ppr(args):
           {"workload": "PPR forward + adjoint, R-MAT scale 20 seed 1, v on 1% of vertices, alpha 0.85, tol 1e-7",
            "nvertices": n, "nnz": csr.nnz},
           dtype="f32", forward_ms=fwd, forward_iters=it_f.value, backward_ms=bwd, backward_iters=it_b.value,
-          fd_directions=64, fd_max_rel_err=float(max(errs)))
+          fd_directions=64, fd_max_rel_err=float(max(errs)), parity=parity)
     g.free()
 
 
@@ -1105,6 +1202,254 @@ def suite_ingest(args):
                         "sample": "one gbo_read_mtx of the same file (host parser, readMtx.hpp:351-423 semantics)"})
 
 
+def suite_refgpu(args):
+    """Reference arm, same-box GPU leg (--impl reference --workload refgpu).
+
+    The reference's own kernels, compiled for sm_100a from its sources into
+    oracle/_ref (oracle/Makefile), run on the same B200 beside this
+    library's kernels on identical B2SR (packed by this library, byte-exact
+    with the reference's csr2bsr_batch layout; the reference's packer is a
+    host loop of cuSPARSE calls per block row and is not timed).  Graph: R-MAT
+    scale 21 (seed 0), the largest R-MAT scale whose 32x32 B2SR stays inside
+    the reference kernels' int32 word offsets (nblocks * 32 < 2^31).  Each
+    pair is timed the way the reference's drivers time it (launches back to
+    back between two events, bsrbmv/benchmark-bsrbmv.cu:1115-1126; the BFS
+    loop of algorithm/bfs.cu:508-564 whole, with its per-level host copy)
+    and compared output for output.  One JSON line per kernel pair."""
+    import ctypes as C
+
+    import gbo
+
+    ref_dir = os.path.join(ROOT, "oracle", "_ref")
+    paths = [os.path.join(ref_dir, f) for f in ("librefbmv.so", "librefbmm.so")]
+    if not all(os.path.exists(p) for p in paths):
+        print(json.dumps({"impl": "reference", "workload": "refgpu",
+                          "unavailable": "oracle/_ref not built (the reference checkout was absent at build time)"}),
+              flush=True)
+        return
+    rb, rm = C.CDLL(paths[0]), C.CDLL(paths[1])
+    P, I = C.c_void_p, C.c_int
+    for nm in ("ref_bmv4_sparse", "ref_bmv8_sparse", "ref_bmv16_sparse_new", "ref_bmv32_sparse_new",
+               "ref_bmv64_sparse_new"):
+        getattr(rb, nm).argtypes = [P] * 5 + [I, I]
+    rb.ref_bfs32_masked_v4.argtypes = [P, P, P, I, I, I, P, C.POINTER(C.c_float)]
+    rb.ref_bmv32_sparse_full_minplus.argtypes = [P] * 5 + [I]
+    rb.ref_bmv32_sparse_full.argtypes = [P] * 5 + [I, P, C.c_float]
+    rm.ref_bmm32_sparse_masked_v5.argtypes = [P] * 7 + [I, I, I]
+    gbo.check(gbo.lib().gbo_set_device(0), "set_device")
+    e0, e1 = gbo.Event(), gbo.Event()
+    steps, warm = max(3, args.steps), max(3, args.warmup)
+
+    def timed(fn):
+        for _ in range(warm):
+            fn()
+        gbo.sync()
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        gbo.sync()
+        return e0.elapsed_ms(e1) / steps
+
+    def chk(st, what):
+        if st != 0:
+            raise SystemExit(f"{what}: CUDA error {st}")
+
+    def dev_b2sr(g):
+        r, c, v = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        gbo.check(gbo.lib().gbo_graph_b2sr(g.h, C.byref(r), C.byref(c), C.byref(v)), "graph_b2sr")
+        return r.value, c.value, v.value
+
+    def pad(a, m, fill):
+        out = np.full(m, fill, dtype=a.dtype)
+        out[:len(a)] = a
+        return out
+
+    def emit(kernel, ref_ms, our_ms, parity, config, **extra):
+        line = {"impl": "reference", "workload": "refgpu", "metric": "ms", "unit": "ms per launch",
+                "higher_is_better": False, "kernel_pair": kernel, "reference_ms": ref_ms, "ours_ms": our_ms,
+                "speedup": ref_ms / our_ms, "steps": steps, "warmup": warm, "n_gpus": 1, "data": "synthetic",
+                "parity": parity, "config": config}
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+
+    scale = args.ref_scale
+    csr = gbo.gen_rmat(scale, EDGE_FACTOR, seed=SEED, **RMAT)
+    n = csr.nrows
+    cfg0 = {"graph": f"R-MAT scale {scale} ef16 seed {SEED} (a=0.57,b=0.19,c=0.19), symmetrised, deduplicated",
+            "nvertices": n, "nnz": csr.nnz, "l2": "inputs larger than L2 (B2SR far above 126 MB)"}
+    x01 = (np.random.default_rng(0).random(n) < 0.5).astype(np.int32)
+
+    # --- BMV count at every tile width: bmv{4,8}_sparse, bmv{16,32,64}_sparse_new
+    ref_names = {4: "ref_bmv4_sparse", 8: "ref_bmv8_sparse", 16: "ref_bmv16_sparse_new",
+                 32: "ref_bmv32_sparse_new", 64: "ref_bmv64_sparse_new"}
+    ref_src = {4: "algorithm/bsrbmv.cu:262", 8: "algorithm/bsrbmv.cu:310",
+               16: "algorithm/bsrbmv.cu:2776", 32: "algorithm/bsrbmv.cu:2937", 64: "algorithm/bsrbmv.cu:3046"}
+    peak, psrc = load_peaks()
+    for b in [int(t) for t in args.ref_widths.split(",")]:
+        g = gbo.Graph.from_csr(csr, b, gbo.FLAG_SYMMETRIC)
+        inf = g.info()
+        nblk, nbr = int(inf.nblocks), inf.nblockrows
+        if nblk * b >= 2 ** 31:
+            print(json.dumps({"impl": "reference", "workload": "refgpu", "kernel_pair": f"bmv count b={b}",
+                              "skipped": f"{nblk} tiles: past the reference kernels' int32 word offsets"}))
+            g.free()
+            continue
+        r, c, v = dev_b2sr(g)
+        dx = gbo.DeviceBuffer.from_numpy(pad(gbo.bits_from_numpy(x01, b), inf.nblockcols + 64, 0))
+        dref = gbo.DeviceBuffer.zeros(4 * (nbr + 64) * b)
+        fn = getattr(rb, ref_names[b])
+        run_ref = lambda: fn(v, dx.ptr, dref.ptr, r, c, nbr, nblk)
+        chk(run_ref(), ref_names[b])
+        gbo.sync()
+        ref_y = dref.to_numpy(np.float32, n).astype(np.int64)
+        dy = gbo.DeviceBuffer(4 * n)
+        g.bmv_count(dx, dy)
+        ours = dy.to_numpy(np.int32, n).astype(np.int64)
+        keep = np.ones(n, bool)
+        note = None
+        if b == 64:
+            # bmv64_sparse_new packs rows r and r+32 as 16-bit halves of one
+            # word (bsrbmv.cu:3084-3090): rows whose pair holds a count past
+            # 32767 overflow there and are left out of the comparison
+            big = np.zeros((nbr * 64,), bool)
+            big[:n] = ours > 32767
+            pair = big.reshape(nbr, 2, 32).any(axis=1)
+            keep = np.repeat(pair[:, None, :], 2, axis=1).reshape(-1)[:n] == False  # noqa: E712
+            note = f"{int((~keep).sum())} rows beside a count > 32767 excluded (reference 16-bit halves)"
+        mism = int(np.count_nonzero(ours[keep] != ref_y[keep]))
+        t_ref = timed(run_ref)
+        t_ours = timed(lambda: g.bmv_count(dx, dy))
+        by = _bmv_bytes(inf, b, n, max(1, b // 8) * inf.nblockcols + 4 * n)
+        emit(f"BMV count b={b}: {ref_names[b][4:]} ({ref_src[b]}) vs gbo_bmv_count", t_ref, t_ours,
+             {"checked": f"int32 row counts of all {n} rows", "mismatched_rows": mism, "equal": mism == 0,
+              **({"note": note} if note else {})},
+             dict(cfg0, tile_bits=b, nblocks=nblk),
+             algorithmic_bytes=by, ours_gbs=by / (t_ours / 1e3) / 1e9, ref_gbs=by / (t_ref / 1e3) / 1e9,
+             ours_frac=by / (t_ours / 1e3) / 1e9 / peak, ref_frac=by / (t_ref / 1e3) / 1e9 / peak,
+             peak_gbs=peak, peak_source=psrc)
+        for buf in (dx, dref, dy):
+            buf.free()
+        g.free()
+
+    # --- 32x32 graph for the BFS loop, min-plus, fp32
+    g = gbo.Graph.from_csr(csr, 32, gbo.FLAG_SYMMETRIC)
+    inf = g.info()
+    nblk, nbr = int(inf.nblocks), inf.nblockrows
+    r, c, v = dev_b2sr(g)
+    cfg = dict(cfg0, tile_bits=32, nblocks=nblk)
+
+    succ = np.zeros(64, np.int32)
+    ms = C.c_float(0)
+    it = rb.ref_bfs32_masked_v4(v, r, c, nbr, 0, 64, succ.ctypes.data, C.byref(ms))
+    if it < 0:
+        raise SystemExit("reference BFS loop: CUDA error")
+    ref_times = []
+    for _ in range(steps):
+        rb.ref_bfs32_masked_v4(v, r, c, nbr, 0, 64, succ.ctypes.data, C.byref(ms))
+        ref_times.append(ms.value)
+    lv, depth = g.bfs(0)
+    d_lv = gbo.DeviceBuffer(4 * n)
+    t_ours = timed(lambda: g.bfs(0, out=d_lv))
+    hist = np.bincount(lv[lv > 0], minlength=it + 1)[1:it + 1]
+    edges = traversed_edges(csr, lv)
+    t_ref = float(np.median(ref_times))
+    emit("BFS from vertex 0: the bfs.cu:508-564 loop (bmv32_sparse_bin_masked_v4, bsrbmv.cu:740) vs gbo_bfs",
+         t_ref, t_ours,
+         {"checked": "vertices reached per level (the reference loop's succ sequence) against gbo_bfs's level "
+                     "histogram", "reference_succ": succ[:it].tolist(), "equal": bool(np.array_equal(hist, succ[:it]))},
+         cfg, ref_gteps=edges / (t_ref / 1e3) / 1e9, ours_gteps=edges / (t_ours / 1e3) / 1e9,
+         reference_iterations=int(it), ours_depth=int(depth))
+    d_lv.free()
+
+    npad = nbr * 32
+    rng = np.random.default_rng(8)
+    # min-plus (sssp.cu:447)
+    d = rng.integers(0, 40, n).astype(np.uint32)
+    d[rng.random(n) < 0.3] = np.uint32(2147483647)
+    dd = gbo.DeviceBuffer.from_numpy(pad(d, npad, np.uint32(2147483647)))
+    dref = gbo.DeviceBuffer.zeros(4 * npad)
+    run_ref = lambda: rb.ref_bmv32_sparse_full_minplus(v, dd.ptr, dref.ptr, r, c, nbr)
+    chk(run_ref(), "minplus")
+    gbo.sync()
+    dy = gbo.DeviceBuffer(4 * n)
+    g.bmv_minplus(dd, dy)
+    rp, ci, _ = g.b2sr()
+    row_of = np.repeat(np.arange(nbr), np.diff(rp))
+    diag = np.zeros(nbr, bool)
+    diag[row_of[ci == row_of]] = True
+    rows = np.repeat(diag, 32)[:n]
+    mism = int(np.count_nonzero(dy.to_numpy(np.uint32, n)[rows] != dref.to_numpy(np.uint32, n)[rows]))
+    t_ref, t_ours = timed(run_ref), timed(lambda: g.bmv_minplus(dd, dy))
+    emit("min-plus BMV: bmv32_sparse_full_minplus (bsrbmv.cu:1083, sssp.cu:447) vs gbo_bmv_minplus", t_ref, t_ours,
+         {"checked": f"uint32 results of the {int(rows.sum())} rows whose block row stores its diagonal tile "
+                     "(the reference adds the 0-weight diagonal only there)", "mismatched_rows": mism,
+          "equal": mism == 0}, cfg)
+    for bf in (dd, dref, dy):
+        bf.free()
+
+    # fp32 PageRank BMV (pr.cu:482): y = alpha * sum p[j] / outdeg(j)
+    p = rng.random(n).astype(np.float32)
+    dp = gbo.DeviceBuffer.from_numpy(pad(p, npad, np.float32(0)))
+    drp = gbo.DeviceBuffer.from_numpy(pad(csr.rowptr, npad + 1, csr.rowptr[-1]))
+    dref = gbo.DeviceBuffer.zeros(4 * npad)
+    run_ref = lambda: rb.ref_bmv32_sparse_full(v, dp.ptr, dref.ptr, r, c, nbr, drp.ptr, 0.85)
+    chk(run_ref(), "full")
+    gbo.sync()
+    dy = gbo.DeviceBuffer(4 * n)
+    run_ours = lambda: gbo.check(gbo.lib().gbo_bmv_float_degptr(g.h, dp.ptr, dy.ptr, C.c_float(0.85), drp.ptr,
+                                                                 None), "bmv_float_degptr")
+    run_ours()
+    a64 = dy.to_numpy(np.float32, n).astype(np.float64)
+    b64 = dref.to_numpy(np.float32, n).astype(np.float64)
+    rel = float(np.abs(a64 - b64).sum() / max(np.abs(b64).sum(), 1e-300))
+    t_ref, t_ours = timed(run_ref), timed(run_ours)
+    it_c = C.c_int(0)
+    dpr = gbo.DeviceBuffer(4 * n)
+    gbo.check(gbo.lib().gbo_pagerank(g.h, C.c_float(0.85), 20, C.c_float(-1.0), dpr.ptr, C.byref(it_c), None), "pr")
+    pr_step = float(np.mean(g.last_run()["step_ms"]))
+    emit("fp32 BMV: bmv32_sparse_full (bsrbmv.cu:1239, pr.cu:482) vs gbo_bmv_float_degptr", t_ref, t_ours,
+         {"checked": f"fp32 y of all {n} rows, relative L1 (reference sums in fp32, this library in fp64)",
+          "rel_l1": rel, "equal": bool(rel <= 1e-5)}, cfg, ours_pagerank_iteration_ms=pr_step)
+    for bf in (dp, drp, dref, dy, dpr):
+        bf.free()
+    g.free()
+
+    # --- masked BMM / triangle counting (bsrbmm.cu:1214, tc.cu:948)
+    tcg = {"mesh": ("king mesh 4096x4096", lambda: gbo.gen_king_mesh(4096)),
+           "rmat": ("R-MAT scale 20 ef16 seed 1", lambda: gbo.gen_rmat(20, 16, seed=1, **RMAT))}
+    for key in args.tc_graphs.split(","):
+        name, make = tcg[key]
+        tcsr = make()
+        low = tcsr.tril()
+        ga = gbo.Graph.from_csr(low, 32)
+        gb = gbo.Graph.from_csr(low.transpose(), 32, gbo.FLAG_LAYOUT_COL)
+        ar, ac, av = dev_b2sr(ga)
+        br, bc, bv = dev_b2sr(gb)
+        ia = ga.info()
+        dcount = gbo.DeviceBuffer.zeros(4)
+        run_ref = lambda: rm.ref_bmm32_sparse_masked_v5(av, bv, dcount.ptr, ar, ac, br, bc, ia.nblockrows,
+                                                        int(ia.nblocks), tcsr.nrows)
+        chk(run_ref(), "masked_v5")
+        gbo.sync()
+        ref_tri = int(dcount.to_numpy(np.int32, 1)[0])
+        gl = gbo.Graph.from_csr(tcsr, 32, gbo.FLAG_LOWER)
+        ours = gl.tc()
+        t_ref = timed(run_ref)
+        t_ours = timed(gl.tc)
+        gd = gbo.Graph.from_csr(tcsr, 16 if key == "mesh" else 8, gbo.FLAG_LOWER | gbo.FLAG_DEGREE_ORDER)
+        t_best = timed(gd.tc)
+        emit(f"triangle count, {name}: bmm32_sparse_masked_v5 (bsrbmm.cu:1214) vs gbo_tc (b = 32, input order)",
+             t_ref, t_ours, {"checked": "triangle count", "reference": ref_tri, "ours": ours,
+                             "equal": ref_tri == ours},
+             {"graph": name, "nvertices": tcsr.nrows, "nnz": tcsr.nnz, "tile_bits": 32,
+              "nblocks_L": int(ia.nblocks)},
+             ours_degree_order_ms=t_best, ours_degree_order_tile=16 if key == "mesh" else 8,
+             speedup_degree_order=t_ref / t_best)
+        for x in (ga, gb, gl, gd):
+            x.free()
+
+
 SUITE = {
     "sssp": lambda a: suite_config2(a, "sssp"),
     "cc": lambda a: suite_config2(a, "cc"),
@@ -1123,8 +1468,14 @@ def main():
     args = parse()
     ws, rank, local = dist_env()
     if args.impl == "reference":
-        run_reference(args, ws, rank)
+        if args.workload == "refgpu":
+            if rank == 0:
+                suite_refgpu(args)
+        else:
+            run_reference(args, ws, rank)
         return
+    if args.workload == "refgpu":
+        raise SystemExit("--workload refgpu belongs to the reference arm: add --impl reference")
     if args.workload != "bfs":
         import gbo
 

@@ -24,6 +24,11 @@
 // cs+1..ce.  Every slot the second kernel reads is written by the first
 // kernel of the same call, so nothing in the scratch has to start at zero.
 //
+// Input: a well-formed B2SR (rowptr non-decreasing from 0 with rowptr[nbr]
+// == nblocks, block columns below ceil(ncols / b)).  Block columns out of
+// range read as an empty x segment; a malformed row pointer is not detected
+// (that would need a device-to-host read) and leaves y undefined.
+//
 // Limits: the scratch holds kScratchInts ints (8 MiB), so a call accepts at
 // most kScratchInts / (2 b) chunks, i.e. 2^35 / b^2 tiles (33,554,432 at
 // b = 32; 8,388,608 at b = 64); larger graphs are rejected with
@@ -233,8 +238,9 @@ extern "C" int gbo_bmv_count_noalloc(int nrows, int ncols, int tile_bits, int nb
                 "gbo_bmv_count_noalloc: " + std::to_string(nblocks) + " tiles exceed the " +
                     std::to_string(max_tiles) + " that its fixed 8 MiB scratch covers at b=" +
                     std::to_string(tile_bits) + "; use gbo_bmv_count on a graph handle");
-  const int nbr = (nrows + tile_bits - 1) / tile_bits;
-  const int nbc = (ncols + tile_bits - 1) / tile_bits;
+  // block counts in 64-bit: nrows + tile_bits - 1 overflows int near INT_MAX
+  const int nbr = (int)(((long long)nrows + tile_bits - 1) / tile_bits);
+  const int nbc = (int)(((long long)ncols + tile_bits - 1) / tile_bits);
   if (nbr == 0) return GBO_OK;
   if (!d_bsrRowPtr || !d_y || (nblocks > 0 && (!d_bsrColInd || !d_bsrVal || !d_x_bits)))
     return fail(GBO_ERR_INVALID, "NULL pointer");

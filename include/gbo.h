@@ -253,7 +253,10 @@ GBO_API int gbo_bmv_count(const gbo_graph* g, const void* d_x_bits, void* d_y,
  *     race on that array and can return wrong counts: order them;
  *   - the first call on each device looks up the array's device address
  *     (cudaGetSymbolAddress, which may load this library's device code):
- *     make that first call before any stream capture begins. */
+ *     make that first call before any stream capture begins;
+ *   - the row pointer is not validated on the device (that would need a
+ *     read back): a malformed one (not non-decreasing from 0 to nblocks)
+ *     leaves y undefined. */
 GBO_API int gbo_bmv_count_noalloc(int nrows, int ncols, int tile_bits, int nblocks,
                                   const int* d_bsrRowPtr, const int* d_bsrColInd,
                                   const void* d_bsrVal, const void* d_x_bits, void* d_y,

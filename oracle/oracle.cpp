@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <parallel/algorithm>
 #include <numeric>
 #include <queue>
 #include <unordered_set>
@@ -541,6 +542,68 @@ unsigned long long orc_bmm_sum_b2sr(const int* arp, const int* aci, const uint64
         }
     }
   return total;
+}
+
+// ---------------------------------------------------------- generators
+// R-MAT (Chakrabarti, Zhan, Faloutsos 2004) with the benchmark's seeding, so
+// that the CPU legs build their inputs without the product library: edge k
+// draws `scale` uniforms from its own xoshiro256** stream (Blackman & Vigna
+// 2018), seeded by four splitmix64 (Steele et al. 2014) outputs started at
+// seed ^ (k * 0xD1B54A32D192ED03); a uniform is the top 53 bits of an output
+// times 2^-53.  Per level: u < a top-left, < a+b top-right, < a+b+c
+// bottom-left, else bottom-right.  The edge list is made symmetric, self
+// loops dropped, duplicates removed and each row sorted (both directions
+// stored).  Returns the number of stored entries (rowptr[n]); colind must
+// hold 2 * 2^scale * edge_factor entries.
+static inline uint64_t orc_sm64(uint64_t* s) {
+  uint64_t z = (*s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+long long orc_gen_rmat(int scale, int edge_factor, double a, double b, double c, uint64_t seed,
+                       int* rowptr, int* colind) {
+  const long long n = 1ll << scale, m = n * edge_factor;
+  std::vector<uint64_t> keys((size_t)(2 * m));
+  const double ab = a + b, abc = a + b + c;
+#pragma omp parallel for schedule(static)
+  for (long long k = 0; k < m; ++k) {
+    uint64_t st = seed ^ ((uint64_t)k * 0xD1B54A32D192ED03ull), s[4];
+    for (int i = 0; i < 4; ++i) s[i] = orc_sm64(&st);
+    uint64_t row = 0, col = 0;
+    for (int l = 0; l < scale; ++l) {
+      const uint64_t x = s[1] * 5;
+      const uint64_t out = ((x << 7) | (x >> 57)) * 9;
+      const uint64_t t = s[1] << 17;
+      s[2] ^= s[0];
+      s[3] ^= s[1];
+      s[1] ^= s[2];
+      s[0] ^= s[3];
+      s[2] ^= t;
+      s[3] = (s[3] << 45) | (s[3] >> 19);
+      const double u = (double)(out >> 11) * (1.0 / 9007199254740992.0);
+      const int down = u >= ab;                           // quadrants c and d
+      const int right = (u >= a && u < ab) || u >= abc;   // quadrants b and d
+      row = row * 2 + down;
+      col = col * 2 + right;
+    }
+    // both directions; a self loop becomes two copies of a sentinel key
+    const uint64_t none = ~0ull;
+    keys[(size_t)(2 * k)] = row == col ? none : (row << 32 | col);
+    keys[(size_t)(2 * k + 1)] = row == col ? none : (col << 32 | row);
+  }
+  __gnu_parallel::sort(keys.begin(), keys.end());
+  const size_t end = (size_t)(std::unique(keys.begin(), keys.end()) - keys.begin());
+  size_t nnz = end;
+  if (nnz && keys[nnz - 1] == ~0ull) --nnz;
+  for (long long i = 0; i <= n; ++i) rowptr[i] = 0;
+  for (size_t e = 0; e < nnz; ++e) {
+    rowptr[(keys[e] >> 32) + 1]++;
+    colind[e] = (int)(keys[e] & 0xffffffffu);
+  }
+  for (long long i = 0; i < n; ++i) rowptr[i + 1] += rowptr[i];
+  return (long long)nnz;
 }
 
 int orc_max_threads(void) { return omp_get_max_threads(); }

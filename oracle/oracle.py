@@ -53,6 +53,8 @@ def lib():
             "orc_tc_b2sr": (C.c_ulonglong, [_P, _P, _P, _I, _I]),
             "orc_spgemm_csr": (None, [_P, _P, _I, _P, _P, _I, _P, _P, _P]),
             "orc_bmm_sum_b2sr": (C.c_ulonglong, [_P, _P, _P, _I, _P, _P, _P, _I]),
+            "orc_gen_rmat": (C.c_longlong, [_I, _I, C.c_double, C.c_double, C.c_double, C.c_uint64,
+                                            _P, _P]),
             "orc_max_threads": (_I, []),
             "orc_set_threads": (None, [_I]),
         }
@@ -256,6 +258,27 @@ def bmm_sum_b2sr(a: B2SR, b_col: B2SR) -> int:
     assert a.b == b_col.b and b_col.layout == 1
     return int(lib().orc_bmm_sum_b2sr(_p(a.rowptr), _p(a.colind), _p(a.words), a.nbr,
                                       _p(b_col.rowptr), _p(b_col.colind), _p(b_col.words), a.b))
+
+
+class Csr:
+    """Host CSR (int32 rowptr / colind) made by the oracle's generators."""
+
+    def __init__(self, rowptr, colind, nrows, ncols):
+        self.rowptr, self.colind, self.nrows, self.ncols = rowptr, colind, nrows, ncols
+
+    @property
+    def nnz(self):
+        return int(self.rowptr[-1])
+
+
+def gen_rmat(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=0) -> Csr:
+    """The benchmark's R-MAT graph (symmetric, no self loops, deduplicated,
+    rows sorted), built on the CPU without the product library."""
+    n = 1 << scale
+    rowptr = np.zeros(n + 1, np.int32)
+    colind = np.empty(2 * n * edge_factor, np.int32)
+    nnz = lib().orc_gen_rmat(scale, edge_factor, a, b, c, seed, _p(rowptr), _p(colind))
+    return Csr(rowptr, colind[:nnz].copy(), n, n)
 
 
 def set_threads(n: int):

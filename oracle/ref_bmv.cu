@@ -81,3 +81,61 @@ extern "C" int ref_bmv32_sparse_full(const unsigned* A, const float* B, float* C
 }
 
 extern "C" int ref_sync(void) { return (int)cudaDeviceSynchronize(); }
+
+// The BFS loop of algorithm/bfs.cu:508-564 (main32, "solution 4") on the
+// caller's B2SR (a symmetric graph, so the CSC packing the driver builds is
+// the same B2SR): per iteration OR(visited, frontier1), the masked v4 BMV
+// into frontier2, a device-to-device copy back into frontier1, fillZero,
+// resetSuccptr + reduce and a blocking copy of succ to the host, until succ
+// is 0 or max_iter iterations ran.  Launch shapes as in the driver.  The
+// driver leaves `visited` uninitialised (bfs.cu:479); it is zeroed here.
+// The per-iteration printf is left out.  succ of iteration i goes to
+// h_succ[i]; returns the number of iterations (the driver's niter - 1 when
+// it breaks on succ == 0), or -1 on a CUDA error; *ms is the loop's device
+// time measured like the driver's GpuTimer (events around the loop).
+extern "C" int ref_bfs32_masked_v4(const unsigned* A, const int* rowptr, const int* colind,
+                                   int nblockrows, int src, int max_iter, int* h_succ, float* ms) {
+  unsigned *f1 = nullptr, *f2 = nullptr, *vis = nullptr;
+  int* succptr = nullptr;
+  if (cudaMalloc(&f1, nblockrows * sizeof(unsigned)) != cudaSuccess ||
+      cudaMalloc(&f2, nblockrows * sizeof(unsigned)) != cudaSuccess ||
+      cudaMalloc(&vis, nblockrows * sizeof(unsigned)) != cudaSuccess ||
+      cudaMalloc(&succptr, sizeof(int)) != cudaSuccess)
+    return -1;
+  cudaMemset(f1, 0, nblockrows * sizeof(unsigned));
+  cudaMemset(f2, 0, nblockrows * sizeof(unsigned));
+  cudaMemset(vis, 0, nblockrows * sizeof(unsigned));
+  const unsigned bit = 1u << (31 - src % 32);
+  cudaMemcpy(f1 + src / 32, &bit, sizeof(unsigned), cudaMemcpyHostToDevice);
+  const dim3 grid_new = cube(nblockrows / 32.0);
+  const int nb1024 = (int)ceil(nblockrows / 1024.0);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaDeviceSynchronize();
+  cudaEventRecord(e0);
+  int i = 0, succ = 0;
+  for (i = 0; i < max_iter; ++i) {
+    OR<unsigned><<<nb1024, 1024>>>(vis, nblockrows, f1);
+    bmv32_sparse_bin_masked_v4<int, unsigned><<<grid_new, 1024>>>(A, f1, f2, rowptr, colind, nblockrows,
+                                                                  vis);
+    cudaMemcpy(f1, f2, nblockrows * sizeof(unsigned), cudaMemcpyDeviceToDevice);
+    fillZero<unsigned><<<nb1024, 1024>>>(f2, nblockrows);
+    resetSuccptr<<<1, 1>>>(succptr);
+    reduce<unsigned><<<nb1024, 1024>>>(f1, nblockrows, succptr);
+    cudaMemcpy(&succ, succptr, sizeof(int), cudaMemcpyDeviceToHost);
+    h_succ[i] = succ;
+    if (succ == 0) break;
+  }
+  cudaEventRecord(e1);
+  cudaEventSynchronize(e1);
+  cudaEventElapsedTime(ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  const int err = (int)cudaGetLastError();
+  cudaFree(f1);
+  cudaFree(f2);
+  cudaFree(vis);
+  cudaFree(succptr);
+  return err ? -1 : (i < max_iter ? i + 1 : i);
+}

@@ -9,7 +9,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, os.path.join(ROOT, "graph-bit-ops_b200"))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
-REF_ROOT = "/root/reference"  # present only where the reference checkout is mounted
+# the reference checkout (GBO_REF_DIR), present only where it is mounted
+REF_ROOT = os.environ.get("GBO_REF_DIR", "/root/reference")
 
 
 def pytest_configure(config):

@@ -24,7 +24,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "graph-bit-ops_b200"))
 import gbo  # noqa: E402  (host-side reader/generators only)
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GBO_REF_DIR", "/root/reference")
 
 
 def sha(a) -> str:

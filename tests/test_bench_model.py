@@ -77,6 +77,10 @@ def test_bfs_level_bytes_matches_direct_count(gbo, orc, b, layout):
 def test_cpu_baseline_single_thread_restores_threads(gbo, orc):
     csr = gbo.gen_rmat(10, 8, seed=1)
     before = orc.max_threads()
-    v1, t1 = bench.cpu_bfs_single(csr, 32)
+    bs = orc.pack(csr.rowptr, csr.colind, csr.nrows, csr.ncols, 32)
+    v1, t1 = bench.cpu_bfs_single(orc, bs, csr, 3)
     assert v1 > 0 and t1 > 0
     assert orc.max_threads() == before
+    v, t, cores, lv, depth = bench.cpu_bfs(orc, bs, csr, 2)
+    assert v > 0 and cores == before
+    assert np.array_equal(lv, orc.bfs_csr(csr.rowptr, csr.colind, csr.nrows, 0)[0])

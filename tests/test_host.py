@@ -136,6 +136,21 @@ def test_rmat_generator_matches_python_restatement(gbo):
     assert np.array_equal(ref.rowptr, got.rowptr) and np.array_equal(ref.colind, got.colind)
 
 
+@pytest.mark.parametrize("scale,ef,seed,abc", [(6, 4, 11, (0.57, 0.19, 0.19)),
+                                               (12, 16, 0, (0.57, 0.19, 0.19)),
+                                               (15, 16, 2, (0.57, 0.19, 0.19)),
+                                               (13, 8, 5, (0.45, 0.15, 0.15))])
+def test_oracle_rmat_generator_equals_library(gbo, orc, scale, ef, seed, abc):
+    """The CPU legs of the benchmark build their R-MAT inputs with the
+    oracle's generator (no product library); it must give the library's
+    graph array for array."""
+    a, b, c = abc
+    got = orc.gen_rmat(scale, ef, a, b, c, seed)
+    ref = gbo.gen_rmat(scale, ef, a, b, c, seed)
+    assert got.nrows == ref.nrows and got.nnz == ref.nnz
+    assert np.array_equal(got.rowptr, ref.rowptr) and np.array_equal(got.colind, ref.colind)
+
+
 def test_csr_transpose_and_tril(gbo):
     rng = np.random.default_rng(2)
     src = rng.integers(0, 50, 300)

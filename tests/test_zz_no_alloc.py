@@ -1,7 +1,9 @@
 """gbo_bmv_count_noalloc (static device scratch, no allocation) against
-gbo_bmv_count on the same packed graphs: identical integer counts, two calls
-in a row with different vectors so that stale scratch would show.  The file
-is named to be collected last; it also passes alone in a fresh process."""
+the oracle's BMV count and gbo_bmv_count on the same packed graphs:
+identical integer counts, two calls in a row with different vectors so that
+stale scratch would show, and a hand-built B2SR whose row lengths put every
+split-row case into the chunks.  The file is named to be collected last; it
+also passes alone in a fresh process."""
 import ctypes as C
 
 import numpy as np
@@ -31,7 +33,7 @@ def _noalloc(gbo, g, dx, dy, out_type, accumulate):
 
 
 @pytest.mark.parametrize("b", WIDTHS)
-def test_noalloc_matches_bmv_count(gbo, gpu, b):
+def test_noalloc_matches_bmv_count(gbo, orc, gpu, b):
     rng = np.random.default_rng(40 + b)
     for csr in (_star_plus_rmat(gbo), gbo.gen_rmat(12, 16, seed=2), gbo.gen_er(1001, 0.01, 3)):
         g = gbo.Graph.from_csr(csr, b)
@@ -44,7 +46,11 @@ def test_noalloc_matches_bmv_count(gbo, gpu, b):
             y = gbo.DeviceBuffer.from_numpy(np.full(n, -7, np.int32))  # overwritten
             gbo.check(_noalloc(gbo, g, dx, y, gbo.OUT_I32, False), "bmv_count_noalloc")
             ref = want.to_numpy(np.int32, n)
-            assert np.array_equal(y.to_numpy(np.int32, n), ref), (b, n, call)
+            got = y.to_numpy(np.int32, n)
+            assert np.array_equal(got, ref), (b, n, call)
+            if call == 0:  # and straight against the oracle's count on the CPU packing
+                ob = orc.pack(csr.rowptr, csr.colind, csr.nrows, csr.ncols, b)
+                assert np.array_equal(got, orc.bmv_count(ob, orc.pack_vector(x, b))), (b, n)
             # float output accumulated onto a base, as gbo_bmv_count does
             base = rng.integers(0, 5, n).astype(np.float32)
             yf = gbo.DeviceBuffer.from_numpy(base)
@@ -63,3 +69,35 @@ def test_noalloc_rejects_graphs_beyond_its_scratch(gbo, gpu):
                                              gbo.OUT_I32, 0, None)
         assert st == ERR_UNSUPPORTED
         assert "scratch" in gbo.lib().gbo_last_error().decode()
+
+
+@pytest.mark.parametrize("b", WIDTHS)
+def test_noalloc_chunk_boundaries_hand_built(gbo, orc, gpu, b):
+    """Block rows sized from the entry point's chunk of 32768 / b tiles: a row
+    ending inside chunk 0, a row starting mid-chunk and crossing into chunk 1
+    (slot 1 of chunk 0, slot 0 of chunk 1), several whole rows in chunk 1, an
+    empty row, a row starting mid-chunk that spans at least three chunks, and
+    short rows at the end.  Counts against the oracle, two calls in a row."""
+    K = 32768 // b
+    lens = [K // 2, K, 3, 5, 1, 0, 7, 3 * K + K // 3, 0, 2, 9]
+    nbr = len(lens)
+    nbc = 131072 // b  # room for 3K distinct ascending block columns
+    rng = np.random.default_rng(900 + b)
+    rowptr = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    colind = np.concatenate([np.sort(rng.choice(nbc, m, replace=False)) for m in lens]).astype(np.int32)
+    top = (1 << b) - 1 if b < 64 else (1 << 64) - 1
+    words = rng.integers(0, top, len(colind) * b, dtype=np.uint64, endpoint=True)
+    words[rng.random(len(words)) < 0.3] = 0
+    nrows, ncols = nbr * b, nbc * b
+    ob = orc.B2SR(rowptr, colind, words, nrows, ncols, b)
+    wd = ob.narrow()
+    drp, dci, dv = (gbo.DeviceBuffer.from_numpy(a) for a in (rowptr, colind, wd))
+    for call in range(2):
+        x = (rng.random(ncols) < (0.5 if call == 0 else 0.15)).astype(np.int32)
+        xw = orc.pack_vector(x, b)
+        dx = gbo.DeviceBuffer.from_numpy(xw.astype(wd.dtype))
+        y = gbo.DeviceBuffer.from_numpy(np.full(nrows, -3, np.int32))
+        st = gbo.lib().gbo_bmv_count_noalloc(nrows, ncols, b, len(colind), drp.ptr, dci.ptr, dv.ptr, dx.ptr,
+                                             y.ptr, gbo.OUT_I32, 0, None)
+        gbo.check(st, "bmv_count_noalloc")
+        assert np.array_equal(y.to_numpy(np.int32, nrows), orc.bmv_count(ob, xw)), (b, call)
