@@ -259,6 +259,118 @@ __global__ void __launch_bounds__(kTPB) k_bfs_step(GView v, typename Word<B>::T*
   block_add_u64(cnt, &ctrl->count);
 }
 
+// Pull step on the row-word slices of a b = 32 ROW graph.  A warp takes 32
+// consecutive block rows at a time from the work counter, reads their
+// visited words in one coalesced load and walks each open block row (a row
+// still unvisited) with lane r on row r: entry k of every open row comes in
+// one 256-byte load, the frontier word of its block column is gathered, two
+// entries per round; a row leaves at its first entry that meets the
+// frontier or when its entries run out (entries are in ascending block
+// column, hubs of power-law graphs first), the block row when no row is
+// left.  Rows still open after the head scan their tails: tails of up to
+// kLongTail entries one lane per row with four entries in flight, longer
+// ones by the whole warp 32 entries at a time.  Rows without entries start
+// visited (k_live), so every open row has an entry.
+constexpr int kLongTail = 64;
+
+__global__ void __launch_bounds__(kTPB) k_bfs_pull_rws(GView v, unsigned* __restrict__ front,
+                                                       unsigned* __restrict__ visited,
+                                                       int* __restrict__ level, Ctrl* __restrict__ ctrl) {
+  if (((volatile Ctrl*)ctrl)->done || ((volatile Ctrl*)ctrl)->mode) return;
+  const int lvl = ((volatile Ctrl*)ctrl)->iter;
+  const unsigned* __restrict__ x = front_buf(front, v.nbr, lvl);
+  unsigned* __restrict__ out = front_buf(front, v.nbr, lvl + 1);
+  unsigned* __restrict__ z = front_buf(front, v.nbr, lvl + 2);
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned kFull = 0xffffffffu;
+  const long long nunits = ((long long)v.nbr + 31) >> 5;
+  unsigned long long cnt = 0;
+  for (;;) {
+    unsigned long long u0 = 0;
+    if (lane == 0) u0 = atomicAdd(&ctrl->work, 1ull);
+    const long long u = (long long)__shfl_sync(kFull, u0, 0);
+    if (u >= nunits) break;
+    const long long R0 = u << 5;
+    const long long Rl = R0 + lane;
+    unsigned visl = kFull;
+    if (Rl < v.nbr) {
+      visl = visited[Rl];
+      z[Rl] = 0u;
+    }
+    unsigned openb = __ballot_sync(kFull, visl != kFull);
+    while (openb) {
+      const int j = __ffs(openb) - 1;
+      openb &= openb - 1;
+      const long long R = R0 + j;
+      const unsigned vis = __shfl_sync(kFull, visl, j);
+      bool need = !((vis >> (31 - lane)) & 1u);
+      bool hit = false;
+      const uint2* __restrict__ hp = v.rws_head + (size_t)R * (kRwsHead * 32) + lane;
+#pragma unroll
+      for (int k = 0; k < kRwsHead; k += 2) {
+        if (!__any_sync(kFull, need)) break;
+        uint2 e0 = make_uint2(kRwsNone, 0u), e1 = make_uint2(kRwsNone, 0u);
+        if (need) {
+          e0 = hp[(size_t)k * 32];
+          e1 = hp[(size_t)(k + 1) * 32];
+        }
+        const unsigned x0 = e0.x != kRwsNone ? __ldg(x + e0.x) : 0u;
+        const unsigned x1 = e1.x != kRwsNone ? __ldg(x + e1.x) : 0u;
+        hit = hit || (need && ((e0.y & x0) | (e1.y & x1)) != 0u);
+        need = need && !hit && e1.x != kRwsNone;
+      }
+      if (__any_sync(kFull, need)) {
+        const long long row = R * 32 + lane;
+        long long tb = 0, te = 0;
+        if (need) {
+          tb = v.rws_tail_ptr[row];
+          te = v.rws_tail_ptr[row + 1];
+        }
+        need = need && te > tb;
+        unsigned longm = __ballot_sync(kFull, need && te - tb > kLongTail);
+        need = need && te - tb <= kLongTail;
+        for (long long p = tb; __any_sync(kFull, need); p += 4) {
+          if (need) {
+            uint2 e[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) e[q] = p + q < te ? v.rws_tail[p + q] : make_uint2(kRwsNone, 0u);
+            unsigned a = 0u;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) a |= e[q].x != kRwsNone ? (e[q].y & __ldg(x + e[q].x)) : 0u;
+            hit = a != 0u;
+            need = !hit && p + 4 < te;
+          }
+        }
+        while (longm) {
+          const int q = __ffs(longm) - 1;
+          longm &= longm - 1;
+          const long long qb = __shfl_sync(kFull, tb, q), qe = __shfl_sync(kFull, te, q);
+          bool qhit = false;
+          for (long long p = qb; p < qe && !qhit; p += 32) {
+            bool h = false;
+            if (p + lane < qe) {
+              const uint2 e = v.rws_tail[p + lane];
+              h = (e.y & __ldg(x + e.x)) != 0u;
+            }
+            qhit = __any_sync(kFull, h);
+          }
+          if ((int)lane == q && qhit) hit = true;
+        }
+      }
+      const unsigned nw = __brev(__ballot_sync(kFull, hit)) & ~vis;
+      if (nw) {
+        if (lane == 0) {
+          out[R] = nw;
+          visited[R] = vis | nw;
+          cnt += __popc(nw);
+        }
+        if ((nw >> (31 - lane)) & 1u) level[R * 32 + lane] = lvl + 1;
+      }
+    }
+  }
+  block_add_u64(cnt, &ctrl->count);
+}
+
 // OR `val` into word idx of a b-bit word array with a 32- or 64-bit atomic
 // (words narrower than 32 bits are OR-ed inside their enclosing 32-bit word;
 // the other bytes receive zero bits and do not change).
@@ -317,45 +429,63 @@ __global__ void __launch_bounds__(kTPB) k_bfs_push(GView v, typename Word<B>::T*
   const unsigned lane = threadIdx.x & 31;
   const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
   const long long nwarps = warps_total();
-  for (long long item = warp_global(); item < v.nitems; item += nwarps) {
-    const gbo_item it = v.items[item];
-    if (lane == 0) z[it.row] = 0;
-    const WT xs = x[it.row];
-    if (!xs) continue;
-    if constexpr (B == 32) {
-      if (v.rowword) {
-        // frontier rows with a non-empty word only (bit r = row r), read from
-        // the packed row words; batches of 32 tiles give each tile's offset
-        long long wb = v.item_wbase[item];
-        const unsigned fr = __brev((unsigned)xs);
-        for (int b0 = it.t0; b0 < it.t1; b0 += 32) {
-          const int t = b0 + (int)lane;
-          const unsigned m = t < it.t1 ? v.rowmask[t] : 0u;
-          const int mc = __popc(m);
-          const int mi = warp_incl_sum(mc, lane);
-          const long long off = wb + (mi - mc);
-          wb += __shfl_sync(0xffffffffu, mi, 31);
-          unsigned sel = fr & m;
-          if (!sel) continue;
-          WT acc = 0;
-          while (sel) {
-            const int r = __ffs(sel) - 1;
-            sel &= sel - 1;
-            acc = (WT)(acc | v.rowword[rowword_index(off, m, r)]);
-          }
-          const int C = v.colind[t];
-          const WT cand = (WT)(acc & ~visited[C]);
-          if (cand) atomic_or_word<B>(out, C, cand);
-        }
-        continue;
-      }
+  // lane j reads item base + j * nwarps and its frontier word, so that one
+  // round of loads finds the (few) items with frontier rows among the warp's
+  // next 32; the stride keeps a hub's consecutive items on different warps
+  for (long long base = warp_global(); base < v.nitems; base += nwarps * 32) {
+    const long long mine = base + (long long)lane * nwarps;
+    gbo_item itl = {0, 0, 0, -2};
+    WT xl = 0;
+    if (mine < v.nitems) {
+      itl = v.items[mine];
+      z[itl.row] = 0;
+      xl = x[itl.row];
     }
-    for (int t = it.t0 + (int)lane; t < it.t1; t += 32) {
-      const int C = v.colind[t];
-      WT acc = 0;
-      for_each_col<B>(xs, [&](int r) { acc = (WT)(acc | val[(size_t)t * B + r]); });
-      const WT cand = (WT)(acc & ~visited[C]);
-      if (cand) atomic_or_word<B>(out, C, cand);
+    unsigned act = __ballot_sync(0xffffffffu, xl != 0);
+    while (act) {
+      const int jj = __ffs(act) - 1;
+      act &= act - 1;
+      const long long item = base + (long long)jj * nwarps;
+      gbo_item it;
+      it.row = __shfl_sync(0xffffffffu, itl.row, jj);
+      it.t0 = __shfl_sync(0xffffffffu, itl.t0, jj);
+      it.t1 = __shfl_sync(0xffffffffu, itl.t1, jj);
+      const WT xs = shfl_word<WT>(0xffffffffu, xl, jj, 32);
+      if constexpr (B == 32) {
+        if (v.rowword) {
+          // frontier rows with a non-empty word only (bit r = row r), read from
+          // the packed row words; batches of 32 tiles give each tile's offset
+          long long wb = v.item_wbase[item];
+          const unsigned fr = __brev((unsigned)xs);
+          for (int b0 = it.t0; b0 < it.t1; b0 += 32) {
+            const int t = b0 + (int)lane;
+            const unsigned m = t < it.t1 ? v.rowmask[t] : 0u;
+            const int mc = __popc(m);
+            const int mi = warp_incl_sum(mc, lane);
+            const long long off = wb + (mi - mc);
+            wb += __shfl_sync(0xffffffffu, mi, 31);
+            unsigned sel = fr & m;
+            if (!sel) continue;
+            WT acc = 0;
+            while (sel) {
+              const int r = __ffs(sel) - 1;
+              sel &= sel - 1;
+              acc = (WT)(acc | v.rowword[rowword_index(off, m, r)]);
+            }
+            const int C = v.colind[t];
+            const WT cand = (WT)(acc & ~visited[C]);
+            if (cand) atomic_or_word<B>(out, C, cand);
+          }
+          continue;
+        }
+      }
+      for (int t = it.t0 + (int)lane; t < it.t1; t += 32) {
+        const int C = v.colind[t];
+        WT acc = 0;
+        for_each_col<B>(xs, [&](int r) { acc = (WT)(acc | val[(size_t)t * B + r]); });
+        const WT cand = (WT)(acc & ~visited[C]);
+        if (cand) atomic_or_word<B>(out, C, cand);
+      }
     }
   }
 }
@@ -686,6 +816,88 @@ __global__ void __launch_bounds__(kTPB) k_pr_step(GView v, float* __restrict__ p
           e += pr_row_update(row0 + 32, a1, x, y, ys, inv, pv, alpha, add, adds, norm, row_scale);
       }
     }
+  }
+  block_add_f64(e, &ctrl->err);
+}
+
+// The same iteration over the row-word slices of a b = 32 ROW graph: a warp
+// per block row, lane r sums row r's columns entry by entry (the head's
+// entry k of the 32 rows in one 256-byte load, two entries in flight), then
+// its tail; tails longer than kLongTail are summed by the whole warp, 32
+// entries at a time, the lanes' partial sums combined by a fixed shuffle
+// tree.  Every row's sum has a fixed order (fp64), whatever the grid.
+__device__ __forceinline__ double pr_word_sum(unsigned c, unsigned w, const float* __restrict__ xg) {
+  double a = 0.0;
+  const size_t base = (size_t)c * 32;
+  while (w) {
+    const int j = __clz(w);
+    a += (double)__ldg(xg + base + j);
+    w &= ~(0x80000000u >> j);
+  }
+  return a;
+}
+
+__global__ void __launch_bounds__(kTPB) k_pr_step_rws(GView v, float* __restrict__ pr, float* __restrict__ prs,
+                                                      const float* __restrict__ inv,
+                                                      const float* __restrict__ pv, Ctrl* __restrict__ ctrl) {
+  if (((volatile Ctrl*)ctrl)->done) return;
+  const int itn = ((volatile Ctrl*)ctrl)->iter;
+  const double alpha = ctrl->alpha, add = ctrl->add, adds = ctrl->add_scale;
+  const int norm = ctrl->norm, row_scale = ctrl->row_scale;
+  const int n = v.nrows;
+  const float* __restrict__ x = pr + (size_t)(itn & 1) * n;
+  float* __restrict__ y = pr + (size_t)((itn + 1) & 1) * n;
+  float* __restrict__ ys = prs + (size_t)((itn + 1) & 1) * n;
+  const float* __restrict__ xg = row_scale ? x : prs + (size_t)(itn & 1) * n;
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned kFull = 0xffffffffu;
+  double e = 0.0;
+  const long long nwarps = warps_total();
+  for (long long R = warp_global(); R < v.nbr; R += nwarps) {
+    const long long row = R * 32 + lane;
+    const uint2* __restrict__ hp = v.rws_head + (size_t)R * (kRwsHead * 32) + lane;
+    double a = 0.0;
+    bool more = true;
+#pragma unroll
+    for (int k = 0; k < kRwsHead; k += 2) {
+      if (!__any_sync(kFull, more)) break;
+      uint2 e0 = make_uint2(kRwsNone, 0u), e1 = make_uint2(kRwsNone, 0u);
+      if (more) {
+        e0 = hp[(size_t)k * 32];
+        e1 = hp[(size_t)(k + 1) * 32];
+      }
+      if (e0.x != kRwsNone) a += pr_word_sum(e0.x, e0.y, xg);
+      if (e1.x != kRwsNone) a += pr_word_sum(e1.x, e1.y, xg);
+      more = more && e1.x != kRwsNone;
+    }
+    long long tb = 0, te = 0;
+    if (more) {
+      tb = v.rws_tail_ptr[row];
+      te = v.rws_tail_ptr[row + 1];
+    }
+    unsigned longm = __ballot_sync(kFull, te - tb > kLongTail);
+    if (te - tb <= kLongTail) {
+      for (long long p = tb; p < te; p += 2) {
+        const uint2 e0 = v.rws_tail[p];
+        const uint2 e1 = p + 1 < te ? v.rws_tail[p + 1] : make_uint2(kRwsNone, 0u);
+        a += pr_word_sum(e0.x, e0.y, xg);
+        if (e1.x != kRwsNone) a += pr_word_sum(e1.x, e1.y, xg);
+      }
+    }
+    while (longm) {
+      const int q = __ffs(longm) - 1;
+      longm &= longm - 1;
+      const long long qb = __shfl_sync(kFull, tb, q), qe = __shfl_sync(kFull, te, q);
+      double part = 0.0;
+      for (long long p = qb + lane; p < qe; p += 32) {
+        const uint2 ee = v.rws_tail[p];
+        part += pr_word_sum(ee.x, ee.y, xg);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
+      if ((int)lane == q) a += part;
+    }
+    if (row < n) e += pr_row_update(row, a, x, y, ys, inv, pv, alpha, add, adds, norm, row_scale);
   }
   block_add_f64(e, &ctrl->err);
 }
@@ -1093,7 +1305,9 @@ struct StepTimer {
 
 // Replay the captured iterations until the device sets `done`.
 int run_until_done(AlgoState* a, int id, cudaStream_t s, int max_iter, int* iters) {
-  const long long max_launch = (long long)max_iter / kStepsPerGraph + 2;
+  long long max_launch = (long long)max_iter / kStepsPerGraph + 2;
+  const long long cap = inject_replay_cap();
+  if (cap > 0 && cap < max_launch) max_launch = cap;
   a->step_ms.clear();
   a->replays = 0;
   a->launches = 1;  // the init kernel
@@ -1147,8 +1361,16 @@ int bfs_impl(gbo_graph* g, int src, const int* h_seeds, int nseeds, int32_t* d_l
   WT* scratch = (WT*)a->scratch;
   // the COL tile layout has its own pull and push kernels (column words)
   const bool col = g->layout == GBO_LAYOUT_COL;
+  // b = 32 ROW graphs pull over their row-word slices (built on first use)
+  if (B == 32 && !col) GBO_TRY(build_rws(g, s));
+  const bool rws = B == 32 && !col && g->rws_head != nullptr;
+  if (rws) v = view_of(g);
+  // the slice pull step finishes every block row itself: no split partials
+  GView vfin = v;
+  if (rws) vfin.nsplit = 0;
   const unsigned gi = col ? grid_persistent(k_bfs_step_col<B>, g->nitems)
-                          : grid_items_persistent(k_bfs_step<B>, g->nitems, B);
+                          : rws ? grid_persistent(k_bfs_pull_rws, ((long long)g->nbr + 31) / 32)
+                                : grid_items_persistent(k_bfs_step<B>, g->nitems, B);
   // push steps (symmetric graphs) finalise every block row in k_bfs_finish
   const bool push_ok = g->symmetric;
   const unsigned gs = blocks_for(std::max<long long>(g->nsplit, push_ok ? g->nbr : 0), kTPB);
@@ -1158,6 +1380,9 @@ int bfs_impl(gbo_graph* g, int src, const int* h_seeds, int nseeds, int32_t* d_l
     tm.begin();
     if (g->nitems > 0) {
       if (col) k_bfs_step_col<B><<<gi, kTPB, 0, cs>>>(v, front, vis, level, ctrl, scratch);
+      else if (rws)
+        k_bfs_pull_rws<<<gi, kTPB, 0, cs>>>(v, reinterpret_cast<unsigned*>(front),
+                                            reinterpret_cast<unsigned*>(vis), level, ctrl);
       else k_bfs_step<B><<<gi, kTPB, 0, cs>>>(v, front, vis, level, ctrl, scratch);
     }
     if (push_ok && g->nitems > 0) {
@@ -1165,7 +1390,7 @@ int bfs_impl(gbo_graph* g, int src, const int* h_seeds, int nseeds, int32_t* d_l
       else k_bfs_push<B><<<gp, kTPB, 0, cs>>>(v, front, vis, ctrl);
     }
     tm.end();
-    k_bfs_finish<B><<<gs, kTPB, 0, cs>>>(v, front, vis, level, ctrl, scratch);
+    k_bfs_finish<B><<<gs, kTPB, 0, cs>>>(vfin, front, vis, level, ctrl, scratch);
     *nl += (g->nitems > 0) + 1 + (push_ok ? (g->nitems > 0) : 0);
     GBO_CUDA_TRY(cudaGetLastError());
     return GBO_OK;
@@ -1220,14 +1445,24 @@ int pr_impl(gbo_graph* g, const float* d_v, float alpha, int max_iter, float tol
   const float* inv = g->invdeg;
   Ctrl* ctrl = a->ctrl;
   double* scratch = (double*)a->scratch;
-  const unsigned gi = grid_items_persistent(k_pr_step<B>, g->nitems, B);
-  const unsigned gs = blocks_for((long long)g->nsplit * B, kTPB);
+  // b = 32 ROW graphs iterate over their row-word slices (no split rows)
+  if (B == 32 && g->layout == GBO_LAYOUT_ROW) GBO_TRY(build_rws(g, s));
+  const bool rws = B == 32 && g->layout == GBO_LAYOUT_ROW && g->rws_head != nullptr;
+  if (rws) v = view_of(g);
+  GView vfin = v;
+  if (rws) vfin.nsplit = 0;
+  const unsigned gi = rws ? grid_persistent(k_pr_step_rws, g->nbr)
+                          : grid_items_persistent(k_pr_step<B>, g->nitems, B);
+  const unsigned gs = blocks_for((long long)vfin.nsplit * B, kTPB);
   GBO_TRY(get_exec(a, id, d_v, [&](cudaStream_t cs, int k, int* nl) -> int {
     StepTimer tm{a, cs, k};
     tm.begin();
-    if (g->nitems > 0) k_pr_step<B><<<gi, kTPB, 0, cs>>>(v, pr, prs, inv, d_v, ctrl, scratch);
+    if (g->nitems > 0) {
+      if (rws) k_pr_step_rws<<<gi, kTPB, 0, cs>>>(v, pr, prs, inv, d_v, ctrl);
+      else k_pr_step<B><<<gi, kTPB, 0, cs>>>(v, pr, prs, inv, d_v, ctrl, scratch);
+    }
     tm.end();
-    k_pr_finish<B><<<gs, kTPB, 0, cs>>>(v, pr, prs, inv, d_v, ctrl, scratch);
+    k_pr_finish<B><<<gs, kTPB, 0, cs>>>(vfin, pr, prs, inv, d_v, ctrl, scratch);
     *nl += (g->nitems > 0) + 1;
     GBO_CUDA_TRY(cudaGetLastError());
     return GBO_OK;
@@ -1261,15 +1496,23 @@ int ppr_backward_impl(gbo_graph* g, const float* d_w, float alpha, float tol, in
     const float* inv = g->invdeg;
     Ctrl* ctrl = a->ctrl;
     double* scratch = (double*)a->scratch;
+    if (B == 32 && g->layout == GBO_LAYOUT_ROW) GBO_TRY(build_rws(g, s));
+    const bool rws = B == 32 && g->layout == GBO_LAYOUT_ROW && g->rws_head != nullptr;
     GView v = view_of(g);
-    const unsigned gi = grid_items_persistent(k_pr_step<B>, g->nitems, B);
-    const unsigned gs = blocks_for((long long)g->nsplit * B, kTPB);
+    GView vfin = v;
+    if (rws) vfin.nsplit = 0;
+    const unsigned gi = rws ? grid_persistent(k_pr_step_rws, g->nbr)
+                            : grid_items_persistent(k_pr_step<B>, g->nitems, B);
+    const unsigned gs = blocks_for((long long)vfin.nsplit * B, kTPB);
     GBO_TRY(get_exec(a, A_PPR_BG, d_w, [&](cudaStream_t cs, int k, int* nl) -> int {
       StepTimer tm{a, cs, k};
       tm.begin();
-      if (g->nitems > 0) k_pr_step<B><<<gi, kTPB, 0, cs>>>(v, pr, prs, inv, d_w, ctrl, scratch);
+      if (g->nitems > 0) {
+        if (rws) k_pr_step_rws<<<gi, kTPB, 0, cs>>>(v, pr, prs, inv, d_w, ctrl);
+        else k_pr_step<B><<<gi, kTPB, 0, cs>>>(v, pr, prs, inv, d_w, ctrl, scratch);
+      }
       tm.end();
-      k_pr_finish<B><<<gs, kTPB, 0, cs>>>(v, pr, prs, inv, d_w, ctrl, scratch);
+      k_pr_finish<B><<<gs, kTPB, 0, cs>>>(vfin, pr, prs, inv, d_w, ctrl, scratch);
       *nl += (g->nitems > 0) + 1;
       GBO_CUDA_TRY(cudaGetLastError());
       return GBO_OK;

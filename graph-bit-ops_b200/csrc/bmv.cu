@@ -98,6 +98,81 @@ __global__ void __launch_bounds__(kTPB) k_count(GView v, const typename Word<B>:
   }
 }
 
+// Narrow tiles (b = 4, 8, 16: 4, 8 or 32 bytes per tile): a warp per work
+// item and a lane per tile, so that a lane reads its whole tile with one
+// 4-, 8- or two 16-byte loads (consecutive lanes, consecutive tiles: the
+// warp's loads are one contiguous run) instead of b lanes reading one or two
+// bytes each.  The lane adds popc(row word & x segment) into b counters; the
+// item's counters are summed across the warp at the end.
+template <int B>
+__device__ __forceinline__ void tile_counts(const void* __restrict__ val, long long t, unsigned xs,
+                                            unsigned (&c)[B]) {
+  if constexpr (B == 4) {
+    const unsigned w = reinterpret_cast<const unsigned*>(val)[t];  // row r = byte r (low nibble)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) c[r] += __popc((w >> (8 * r)) & xs & 0xfu);
+  } else if constexpr (B == 8) {
+    const unsigned long long w = reinterpret_cast<const unsigned long long*>(val)[t];  // row r = byte r
+    const unsigned long long xr = 0x0101010101010101ull * (xs & 0xffu);
+    const unsigned long long a = w & xr;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) c[r] += __popc((unsigned)(a >> (8 * r)) & 0xffu);
+  } else {
+    const uint4* q = reinterpret_cast<const uint4*>(val) + 2 * t;  // row r = halfword r
+    const uint4 lo = q[0], hi = q[1];
+    const unsigned xx = (xs & 0xffffu) * 0x10001u;
+    const unsigned w[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const unsigned a = w[k] & xx;
+      c[2 * k] += __popc(a & 0xffffu);
+      c[2 * k + 1] += __popc(a >> 16);
+    }
+  }
+}
+
+template <int B, bool OUTF>
+__global__ void __launch_bounds__(kTPB) k_count_narrow(GView v, const typename Word<B>::T* __restrict__ x,
+                                                       void* __restrict__ yv, int accumulate,
+                                                       int* __restrict__ scratch) {
+  const unsigned lane = threadIdx.x & 31;
+  const long long item = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (item >= v.nitems) return;
+  const gbo_item it = v.items[item];
+  unsigned c[B];
+#pragma unroll
+  for (int r = 0; r < B; ++r) c[r] = 0u;
+  int t = it.t0 + (int)lane;
+  for (; t + 32 < it.t1; t += 64) {  // two tiles per lane in flight
+    const int c0 = v.colind[t], c1 = v.colind[t + 32];
+    const unsigned x0 = x[c0], x1 = x[c1];
+    tile_counts<B>(v.val, t, x0, c);
+    tile_counts<B>(v.val, t + 32, x1, c);
+  }
+  if (t < it.t1) tile_counts<B>(v.val, t, x[v.colind[t]], c);
+  unsigned mine = 0u;
+#pragma unroll
+  for (int r = 0; r < B; ++r) {
+    const unsigned s = __reduce_add_sync(0xffffffffu, c[r]);
+    if ((int)lane == r) mine = s;
+  }
+  if ((int)lane >= B) return;
+  const int r = (int)lane;
+  if (it.slot >= 0) {
+    scratch[(size_t)it.slot * B + r] = (int)mine;
+    return;
+  }
+  const long long row = (long long)it.row * B + r;
+  if (row >= v.nrows) return;
+  if (OUTF) {
+    float* y = reinterpret_cast<float*>(yv);
+    y[row] = (accumulate ? y[row] : 0.f) + (float)mine;
+  } else {
+    int* y = reinterpret_cast<int*>(yv);
+    y[row] = (accumulate ? y[row] : 0) + (int)mine;
+  }
+}
+
 template <int B, bool OUTF>
 __global__ void k_count_reduce(GView v, const int* __restrict__ scratch, void* __restrict__ yv,
                                int accumulate) {
@@ -343,10 +418,26 @@ int count_impl(const GView& v, const void* x, void* y, int out_type, int accumul
                int* scratch, cudaStream_t s) {
   using WT = typename Word<B>::T;
   if (v.nitems > 0) {
-    if (out_type == GBO_OUT_F32)
-      k_count<B, true><<<grid_items<B>(v), kTPB, 0, s>>>(v, (const WT*)x, y, accumulate, scratch);
-    else
-      k_count<B, false><<<grid_items<B>(v), kTPB, 0, s>>>(v, (const WT*)x, y, accumulate, scratch);
+    // whole-tile loads need the tile array aligned to a tile (4, 8 or 16
+    // bytes); a caller's wrapped B2SR may not be
+    bool narrow = false;
+    if constexpr (B <= 16) {
+      constexpr uintptr_t kAlign = B == 4 ? 4 : B == 8 ? 8 : 16;
+      narrow = (reinterpret_cast<uintptr_t>(v.val) % kAlign) == 0;
+      if (narrow) {
+        const unsigned grid = blocks_for_warps(v.nitems, kTPB / 32);
+        if (out_type == GBO_OUT_F32)
+          k_count_narrow<B, true><<<grid, kTPB, 0, s>>>(v, (const WT*)x, y, accumulate, scratch);
+        else
+          k_count_narrow<B, false><<<grid, kTPB, 0, s>>>(v, (const WT*)x, y, accumulate, scratch);
+      }
+    }
+    if (!narrow) {
+      if (out_type == GBO_OUT_F32)
+        k_count<B, true><<<grid_items<B>(v), kTPB, 0, s>>>(v, (const WT*)x, y, accumulate, scratch);
+      else
+        k_count<B, false><<<grid_items<B>(v), kTPB, 0, s>>>(v, (const WT*)x, y, accumulate, scratch);
+    }
   }
   if (v.nsplit > 0) {
     unsigned g = blocks_for((long long)v.nsplit * B, 256);
@@ -417,6 +508,9 @@ GView view_of(const gbo_graph* g) {
   v.rowmask = g->rowmask;
   v.rowword = g->rowword;
   v.item_wbase = g->item_wbase;
+  v.rws_head = g->rws_head;
+  v.rws_tail = g->rws_tail;
+  v.rws_tail_ptr = g->rws_tail_ptr;
   return v;
 }
 

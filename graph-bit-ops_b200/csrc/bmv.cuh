@@ -23,6 +23,10 @@ struct GView {
   // inside a tile) and the index of every work item's first word
   const unsigned* __restrict__ rowword = nullptr;
   const long long* __restrict__ item_wbase = nullptr;
+  // row-word slices (b = 32 ROW, once built): see gbo_graph::rws_head
+  const uint2* __restrict__ rws_head = nullptr;
+  const uint2* __restrict__ rws_tail = nullptr;
+  const long long* __restrict__ rws_tail_ptr = nullptr;
 };
 
 // Index in rowword of row r's word of a tile with occupancy word m whose

@@ -1,4 +1,5 @@
 // Error reporting, version and the device plumbing part of the C ABI.
+#include <atomic>
 #include <cstring>
 #include <string>
 
@@ -34,6 +35,22 @@ void clear_error() {
   (void)cudaGetLastError();
 }
 
+// Host-side fault injection state (gbo_debug_inject).
+namespace {
+std::atomic<long long> g_inject_alloc{0};
+std::atomic<long long> g_inject_replay_cap{0};
+std::atomic<int> g_inject_hold{0};
+}  // namespace
+
+bool inject_host_alloc_fails() {
+  long long v = g_inject_alloc.load();
+  while (v > 0)
+    if (g_inject_alloc.compare_exchange_weak(v, v - 1)) return v == 1;
+  return false;
+}
+long long inject_replay_cap() { return g_inject_replay_cap.load(); }
+bool inject_server_hold() { return g_inject_hold.load() != 0; }
+
 int num_sms() {
   static thread_local int cached = 0;
   if (cached == 0) {
@@ -63,11 +80,23 @@ extern "C" const char* gbo_status_string(int status) {
     case GBO_ERR_UNSUPPORTED: return "GBO_ERR_UNSUPPORTED";
     case GBO_ERR_OVERFLOW: return "GBO_ERR_OVERFLOW";
     case GBO_ERR_NOTREADY: return "GBO_ERR_NOTREADY";
+    case GBO_ERR_FULL: return "GBO_ERR_FULL";
   }
   return "GBO_ERR_UNKNOWN";
 }
 
 extern "C" const char* gbo_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" int gbo_debug_inject(int what, long long n) {
+  clear_error();
+  if (n < 0) return fail(GBO_ERR_INVALID, "injection count must be >= 0");
+  switch (what) {
+    case GBO_INJECT_HOST_ALLOC: g_inject_alloc.store(n); return GBO_OK;
+    case GBO_INJECT_REPLAY_CAP: g_inject_replay_cap.store(n); return GBO_OK;
+    case GBO_INJECT_SERVER_HOLD: g_inject_hold.store(n ? 1 : 0); return GBO_OK;
+  }
+  return fail(GBO_ERR_INVALID, "unknown injection");
+}
 
 extern "C" int gbo_version(void) { return 100; }
 

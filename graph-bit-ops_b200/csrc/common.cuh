@@ -81,6 +81,13 @@ inline unsigned blocks_for(long long n, int tpb) {
 
 int num_sms();
 
+// Host-side fault injection (gbo_debug_inject): true when this host CSR
+// allocation is the one armed to fail; the replay cap of the iteration
+// loops (0: none); whether server workers hold admission.
+bool inject_host_alloc_fails();
+long long inject_replay_cap();
+bool inject_server_hold();
+
 // Exclusive scan of n int32 counts into out[0..n] (out[n] = total) with the
 // total also returned through d_total (int64).  No spin waits: three kernels.
 int exclusive_scan_i32(const int* d_in, int* d_out, long long n, long long* d_total,

@@ -111,6 +111,9 @@ void destroy(gbo_graph* g) {
   cudaFree(g->rowmask);
   cudaFree(g->rowword);
   cudaFree(g->item_wbase);
+  cudaFree(g->rws_head);
+  cudaFree(g->rws_tail);
+  cudaFree(g->rws_tail_ptr);
   cudaFree(g->invdeg);
   cudaFree(g->items);
   cudaFree(g->splits);

@@ -34,6 +34,13 @@ struct gbo_graph {
   unsigned* rowword = nullptr;  // b = 32 ROW: the non-empty row words, packed in tile order
   long long* item_wbase = nullptr;  // index in rowword of every work item's first word
   long long nrowword = 0;
+  // b = 32 ROW, built on first BFS use (build_rws): every row's non-empty
+  // row words with their block columns in ascending block-column order; the
+  // first kRwsHead entries of the 32 rows of a block row entry-major, the
+  // rest in per-row tails
+  uint2* rws_head = nullptr;       // nbr * kRwsHead * 32 entries {block column, row word}
+  uint2* rws_tail = nullptr;       // entries past the head, row after row
+  long long* rws_tail_ptr = nullptr;  // nbr * 32 + 1 offsets into rws_tail
   int last_run_ms = 0;     // 1: the last traversal was a multi-source BFS
   bool tc_mma = false;     // GBO_FLAG_TC_MMA: dense 32x32 mask tiles on the 1-bit MMA
   bool owns_outdeg = true;
@@ -77,6 +84,14 @@ int build_rowmask(gbo_graph* g, cudaStream_t stream);
 // Packed non-empty row words -> g->rowword, g->item_wbase (needs rowmask and
 // the schedule; no-op without them).
 int build_rowwords(gbo_graph* g, cudaStream_t stream);
+
+// Entries per row held entry-major in the row-word slices' head, and the
+// block column that marks a missing entry.
+constexpr int kRwsHead = 8;
+constexpr unsigned kRwsNone = 0xffffffffu;
+// Row-word slices of a b = 32 ROW graph -> g->rws_* (no-op for other graphs
+// or when built).  Needs g->rowmask.
+int build_rws(gbo_graph* g, cudaStream_t stream);
 
 // Ensure g->ws has at least `bytes` (contents undefined).
 int ensure_workspace(gbo_graph* g, size_t bytes, cudaStream_t stream);

@@ -8,6 +8,7 @@
 namespace gbo {
 int fail(int status, const std::string& msg);
 void clear_error();
+bool inject_host_alloc_fails();  // gbo_debug_inject(GBO_INJECT_HOST_ALLOC)
 
 #define GBO_HOST_TRY(call)          \
   do {                              \

@@ -66,6 +66,7 @@ struct Xoshiro {
 };
 
 gbo_csr* new_csr(int nrows, int ncols, long long nnz) {
+  if (inject_host_alloc_fails()) return nullptr;
   gbo_csr* c = (gbo_csr*)calloc(1, sizeof(gbo_csr));
   if (!c) return nullptr;
   c->nrows = nrows;

@@ -185,7 +185,9 @@ int msbfs_impl(gbo_graph* g, const int* h_srcs, int k, int32_t* d_levels, int* h
   m.step_ms.clear();
   m.launches = 3;
   int it0 = 0;
-  const long long max_launch = (long long)max_iter / kLevelsPerGraph + 2;
+  long long max_launch = (long long)max_iter / kLevelsPerGraph + 2;
+  const long long cap = inject_replay_cap();
+  if (cap > 0 && cap < max_launch) max_launch = cap;
   bool done = false;
   for (long long q = 0; q < max_launch; ++q) {
     GBO_CUDA_TRY(cudaGraphLaunch(m.exec, s));

@@ -712,6 +712,93 @@ int build_rowwords(gbo_graph* g, cudaStream_t s) {
   return GBO_OK;
 }
 
+// Row-word slices, pass 1: warp per block row; per batch of 32 tiles (lane
+// j: tile j's occupancy word) the number of tiles in which row r is
+// non-empty is popc of the ballot of bit r, kept by lane r.  Writes the
+// tail length max(count - kRwsHead, 0) of every padded row.
+__global__ void k_rws_count(const int* __restrict__ rowptr, int nbr, const unsigned* __restrict__ mask,
+                            int* __restrict__ tail_len) {
+  const unsigned lane = threadIdx.x & 31;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long R = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; R < nbr; R += nwarps) {
+    const int rs = rowptr[R], re = rowptr[R + 1];
+    int c = 0;
+    for (int t0 = rs; t0 < re; t0 += 32) {
+      const unsigned m = t0 + (int)lane < re ? mask[t0 + lane] : 0u;
+#pragma unroll
+      for (int r = 0; r < 32; ++r) {
+        const unsigned b = __ballot_sync(0xffffffffu, (m >> r) & 1u);
+        if ((int)lane == r) c += __popc(b);
+      }
+    }
+    tail_len[R * 32 + lane] = c > kRwsHead ? c - kRwsHead : 0;
+  }
+}
+
+// Row-word slices, pass 2: warp per block row, lane r walks row r's word of
+// every tile in order (one coalesced 128-byte load per tile, four tiles in
+// flight) and appends the non-empty ones with their block column: the first
+// kRwsHead to the head (entry-major), the rest to the row's tail.  Unused
+// head entries get kRwsNone.
+__global__ void k_rws_fill(const int* __restrict__ rowptr, const int* __restrict__ colind, int nbr,
+                           const unsigned* __restrict__ val, const long long* __restrict__ tail_ptr,
+                           uint2* __restrict__ head, uint2* __restrict__ tail) {
+  const unsigned lane = threadIdx.x & 31;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long R = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; R < nbr; R += nwarps) {
+    const int rs = rowptr[R], re = rowptr[R + 1];
+    uint2* hp = head + (size_t)R * kRwsHead * 32 + lane;
+    uint2* tp = tail + tail_ptr[R * 32 + lane];
+    int k = 0;
+    for (int t = rs; t < re; t += 4) {
+      unsigned w[4];
+      int c[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        w[u] = t + u < re ? val[(size_t)(t + u) * 32 + lane] : 0u;
+        c[u] = t + u < re ? colind[t + u] : 0;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (!w[u]) continue;
+        const uint2 e = make_uint2((unsigned)c[u], w[u]);
+        if (k < kRwsHead) hp[(size_t)k * 32] = e;
+        else tp[k - kRwsHead] = e;
+        ++k;
+      }
+    }
+    for (; k < kRwsHead; ++k) hp[(size_t)k * 32] = make_uint2(kRwsNone, 0u);
+  }
+}
+
+int build_rws(gbo_graph* g, cudaStream_t s) {
+  if (g->b != 32 || g->layout != GBO_LAYOUT_ROW || !g->rowmask || g->rws_head || g->nbr <= 0) return GBO_OK;
+  const long long rows = (long long)g->nbr * 32;
+  int* len = nullptr;
+  long long* tot = nullptr;
+  GBO_CUDA_TRY(cudaMallocAsync(&len, sizeof(int) * (size_t)rows, s));
+  GBO_CUDA_TRY(cudaMallocAsync(&tot, sizeof(long long), s));
+  GBO_CUDA_TRY(cudaMalloc(&g->rws_tail_ptr, sizeof(long long) * (size_t)(rows + 1)));
+  GBO_CUDA_TRY(cudaMalloc(&g->rws_head, sizeof(uint2) * (size_t)rows * kRwsHead));
+  g->device_bytes += 8LL * (rows + 1) + 8LL * rows * kRwsHead;
+  int nsm = 148, dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = (int)std::min<long long>(((long long)g->nbr + 7) / 8, 16LL * nsm);
+  k_rws_count<<<grid, 256, 0, s>>>(g->rowptr, g->nbr, g->rowmask, len);
+  GBO_TRY(exclusive_scan_i32_to_i64(len, g->rws_tail_ptr, rows, tot, s));
+  long long nt = 0;
+  GBO_CUDA_TRY(cudaMemcpyAsync(&nt, tot, sizeof(nt), cudaMemcpyDeviceToHost, s));
+  GBO_CUDA_TRY(cudaStreamSynchronize(s));
+  cudaFreeAsync(len, s);
+  cudaFreeAsync(tot, s);
+  GBO_CUDA_TRY(cudaMalloc(&g->rws_tail, sizeof(uint2) * (size_t)(nt > 0 ? nt : 1)));
+  g->device_bytes += 8LL * (nt > 0 ? nt : 1);
+  k_rws_fill<<<grid, 256, 0, s>>>(g->rowptr, g->colind, g->nbr, static_cast<const unsigned*>(g->val),
+                                  g->rws_tail_ptr, g->rws_head, g->rws_tail);
+  GBO_CUDA_TRY(cudaGetLastError());
+  return GBO_OK;
+}
+
 int build_rowmask(gbo_graph* g, cudaStream_t s) {
   if (g->b != 32 || g->layout != GBO_LAYOUT_ROW || g->rowmask) return GBO_OK;
   GBO_CUDA_TRY(cudaMalloc(&g->rowmask, sizeof(unsigned) * (size_t)(g->nblk > 0 ? g->nblk : 1)));

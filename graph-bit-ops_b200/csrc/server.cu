@@ -394,6 +394,7 @@ struct Result {
 struct gbo_server {
   gbo_graph* g = nullptr;
   int n = 0, nbr = 0;
+  long long max_pending = 0;  // per engine; 0 = unbounded (gbo_server_set_queue_limit)
   float alpha = 0.85f, tol = 1e-7f;
   int ppr_max_iter = 1000;
   // one worker thread per engine (0 BFS, 1 PPR), each with its own stream,
@@ -747,7 +748,7 @@ void worker_main(gbo_server* S, int kind) {
         if (S->stop || S->worker_status != GBO_OK) return;
         const int bp = blocked_pool(S, kind);
         if (bp >= 0) move_results_to_host(S, bp, lk);
-        const bool can_admit = !S->pending[kind].empty() && budget() > 0;
+        const bool can_admit = !S->pending[kind].empty() && budget() > 0 && !inject_server_hold();
         const bool work = can_admit || unfinished() || (occupied() && blocked_pool(S, kind) < 0);
         if (work) {
           stall_since = -1.0;
@@ -771,7 +772,7 @@ void worker_main(gbo_server* S, int kind) {
       // admission into free slots, arrival order, within the buffer budget
       size_t nx = 0;
       std::deque<Query>& pend = S->pending[kind];
-      long long room = budget();
+      long long room = inject_server_hold() ? 0 : budget();
       while (!pend.empty() && room > 0) {
         while (nx < tab.size() && tab[nx] != 0) ++nx;
         if (nx >= tab.size()) break;
@@ -981,6 +982,8 @@ extern "C" int gbo_server_create(const gbo_graph* gc, int bfs_slots, int ppr_slo
 static int submit(gbo_server* S, Query&& q, int64_t* ticket) {
   std::lock_guard<std::mutex> lk(S->mu);
   if (S->worker_status != GBO_OK) return fail(S->worker_status, S->worker_error);
+  if (S->max_pending > 0 && (long long)S->pending[q.kind].size() >= S->max_pending)
+    return fail(GBO_ERR_FULL, "admission queue full (" + std::to_string(S->max_pending) + " pending queries)");
   q.ticket = S->next_ticket++;
   q.t_submit = now_ms();
   S->submit_time[q.ticket] = q.t_submit;
@@ -988,6 +991,14 @@ static int submit(gbo_server* S, Query&& q, int64_t* ticket) {
   const int kind = q.kind;
   S->pending[kind].push_back(std::move(q));
   S->cv_work.notify_all();
+  return GBO_OK;
+}
+
+extern "C" int gbo_server_set_queue_limit(gbo_server* S, long long max_pending) {
+  clear_error();
+  if (!S || max_pending < 0) return fail(GBO_ERR_INVALID, "bad argument");
+  std::lock_guard<std::mutex> lk(S->mu);
+  S->max_pending = max_pending;
   return GBO_OK;
 }
 
@@ -1079,6 +1090,15 @@ struct ClientCopy {
     if (*err == cudaSuccess) *err = wait_stream(st, done);
     return pinned;
   }
+  // Copy `n` bytes from device memory straight into pinned host memory.
+  cudaError_t copy_into(void* dst, const void* src, size_t n) {
+    cudaError_t e = cudaSuccess;
+    if (!st) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !done) e = cudaEventCreateWithFlags(&done, cudaEventBlockingSync | cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = wait_stream(st, done);
+    return e;
+  }
 };
 
 // Per client thread for device delivery: a stream (when the caller gives
@@ -1143,9 +1163,21 @@ static cudaError_t deliver_device(gbo_server* S, const Result& r, void* d_out, c
 // copy it from the device buffer (widening byte levels to int32) outside the
 // lock -- to host memory (h_out) or, with `device`, to the caller's device
 // buffer d_out -- then give the buffer back to the pool.
+// True when p is page-locked host memory the device can copy into directly.
+static bool is_pinned(const void* p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost;
+}
+
+// The result of `ticket` (present, not moving) into h_out (byte levels when
+// bytes_out), then its buffer back to the pool.
 static int take_result(gbo_server* S, std::unique_lock<std::mutex>& lk, int64_t ticket, void* h_out,
                        double* latency_ms, int* iterations, bool device = false,
-                       cudaStream_t ds = nullptr) {
+                       cudaStream_t ds = nullptr, bool bytes_out = false) {
   auto it = S->results.find(ticket);
   const Result r = std::move(it->second);
   S->results.erase(it);
@@ -1157,6 +1189,24 @@ static int take_result(gbo_server* S, std::unique_lock<std::mutex>& lk, int64_t 
   if (device) {
     if (h_out) e = deliver_device(S, r, h_out, ds);
     t2 = t1 = now_ms();
+  } else if (bytes_out) {  // byte levels as stored
+    if (r.buf < 0) {
+      if (h_out) memcpy(h_out, r.host.data(), (size_t)S->n);
+    } else {
+      const char* src = S->dpool[r.pool] + (size_t)r.buf * S->dbytes[r.pool];
+      e = cudaEventSynchronize(r.ev);
+      t1 = now_ms();
+      if (e == cudaSuccess && h_out) {
+        thread_local ClientCopy cc;
+        if (is_pinned(h_out)) {
+          e = cc.copy_into(h_out, src, (size_t)S->n);
+        } else {
+          const void* h = cc.fetch(src, (size_t)S->n, &e);
+          if (e == cudaSuccess) memcpy(h_out, h, (size_t)S->n);
+        }
+      }
+      t2 = now_ms();
+    }
   } else if (r.buf < 0) {  // already in host memory
     if (h_out && r.u8) {
       int* o = static_cast<int*>(h_out);
@@ -1226,6 +1276,24 @@ extern "C" int gbo_server_wait(gbo_server* S, int64_t ticket, void* h_out, doubl
   if (S->worker_status != GBO_OK) return fail(S->worker_status, S->worker_error);
   if (!ok) return fail(GBO_ERR_TIMEOUT, "query not finished within the timeout");
   return take_result(S, lk, ticket, h_out, latency_ms, iterations);
+}
+
+extern "C" int gbo_server_wait_u8(gbo_server* S, int64_t ticket, uint8_t* h_out, double* latency_ms,
+                                  int* iterations, double timeout_s) {
+  clear_error();
+  if (!S) return fail(GBO_ERR_INVALID, "NULL server");
+  std::unique_lock<std::mutex> lk(S->mu);
+  const bool ok = S->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] {
+    if (S->worker_status != GBO_OK) return true;
+    auto it = S->results.find(ticket);
+    return it != S->results.end() && !it->second.moving;
+  });
+  if (S->worker_status != GBO_OK) return fail(S->worker_status, S->worker_error);
+  if (!ok) return fail(GBO_ERR_TIMEOUT, "query not finished within the timeout");
+  const Result& r = S->results.find(ticket)->second;
+  if (r.kind != 0) return fail(GBO_ERR_INVALID, "gbo_server_wait_u8 takes BFS tickets");
+  if (!r.u8) return fail(GBO_ERR_OVERFLOW, "levels past 254: collect this result with gbo_server_wait");
+  return take_result(S, lk, ticket, h_out, latency_ms, iterations, false, nullptr, true);
 }
 
 extern "C" int gbo_server_wait_device(gbo_server* S, int64_t ticket, void* d_out,

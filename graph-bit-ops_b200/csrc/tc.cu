@@ -106,6 +106,40 @@ __global__ void __launch_bounds__(kTPB) k_tc(GView v, long long nblk, const int*
     const bool probe_a = (a1 - a0) <= (b1 - b0);
     const int p0 = probe_a ? a0 : b0, p1 = probe_a ? a1 : b1;
     const int s0 = probe_a ? b0 : a0, s1 = probe_a ? b1 : a1;
+    if constexpr (B == 32) {
+      if (npairs < 0) {
+        // dense 32x32 mask: lane r accumulates P[r][c] = sum over hits of
+        // popc(A[r] & B[c]) for all 32 columns (B rows broadcast by 32
+        // unrolled shuffles, no data-dependent loop), masked once at the end
+        unsigned cm[32];
+#pragma unroll
+        for (int c = 0; c < 32; ++c) cm[c] = 0u;
+        for (int base = p0; base < p1; base += 32) {
+          const int p = base + (int)lane;
+          int hit = -1;
+          if (p < p1) {
+            const int J = v.colind[p];
+            const int q = lower_bound_dev(v.colind, s0, s1, J);
+            if (q < s1 && v.colind[q] == J) hit = q;
+          }
+          unsigned found = __ballot_sync(0xffffffffu, hit >= 0);
+          while (found) {
+            const int src = __ffs(found) - 1;
+            found &= found - 1;
+            const int ph = __shfl_sync(0xffffffffu, p, src);
+            const int qh = __shfl_sync(0xffffffffu, hit, src);
+            const unsigned ar = (unsigned)val[(size_t)(probe_a ? ph : qh) * 32 + lane];
+            const unsigned br = (unsigned)val[(size_t)(probe_a ? qh : ph) * 32 + lane];
+#pragma unroll
+            for (int c = 0; c < 32; ++c) cm[c] += __popc(ar & __shfl_sync(0xffffffffu, br, c));
+          }
+        }
+        const unsigned mr = (unsigned)M0;
+#pragma unroll
+        for (int c = 0; c < 32; ++c) acc += ((mr >> (31 - c)) & 1u) ? cm[c] : 0u;
+        continue;
+      }
+    }
     for (int base = p0; base < p1; base += 32) {
       const int p = base + (int)lane;
       int hit = -1;

@@ -26,6 +26,10 @@ GBO_ERR_IO = 7
 GBO_ERR_UNSUPPORTED = 8
 GBO_ERR_OVERFLOW = 9
 GBO_ERR_NOTREADY = 10
+GBO_ERR_FULL = 11
+INJECT_HOST_ALLOC = 1
+INJECT_REPLAY_CAP = 2
+INJECT_SERVER_HOLD = 3
 
 LAYOUT_ROW = 0
 LAYOUT_COL = 1
@@ -75,6 +79,22 @@ class ServerStats(C.Structure):
                 ("bfs_round_ms", C.c_double), ("ppr_round_ms", C.c_double),
                 ("retire_ms", C.c_double), ("copy_ms", C.c_double), ("copy_wait_ms", C.c_double),
                 ("copy_d2h_ms", C.c_double), ("copy_widen_ms", C.c_double)]
+
+
+# Sharded BFS: the loop's operations and the data plane (include/gbo.h).
+SHARD_LEVEL_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_uint64))
+SHARD_ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_uint64))
+SHARD_EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p)
+SHARD_ALLGATHER_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p)
+
+
+class ShardOps(C.Structure):
+    _fields_ = [("user", C.c_void_p), ("level", SHARD_LEVEL_FN), ("allreduce_sum_u64", SHARD_ALLREDUCE_FN),
+                ("exchange", SHARD_EXCHANGE_FN)]
+
+
+class ShardComm(C.Structure):
+    _fields_ = [("user", C.c_void_p), ("allreduce_sum_u64", SHARD_ALLREDUCE_FN), ("allgather", SHARD_ALLGATHER_FN)]
 
 
 class CsrStruct(C.Structure):
@@ -143,15 +163,22 @@ _SIGS = {
     "gbo_graph_last_run": (_I, [_P, C.POINTER(RunStats)]),
     "gbo_msbfs": (_I, [_P, _P, _I, _P, C.POINTER(_I), _P]),
     "gbo_bfs_shard_level": (_I, [_P, _P, _P, _P, _I, _P, C.POINTER(C.c_uint64), _P]),
+    "gbo_bfs_shard_loop": (_I, [_P, _I, C.POINTER(_I)]),
+    "gbo_bfs_sharded": (_I, [_P, _I, _I, _P, _I, _P, C.POINTER(_I), _P, _P]),
+    "gbo_nccl_unique_id": (_I, [_P]),
+    "gbo_nccl_comm_create": (_I, [_I, _I, _P, C.POINTER(_P)]),
+    "gbo_nccl_comm_destroy": (_I, [_P]),
     "gbo_bmm_sum": (_I, [_P, _P, C.POINTER(C.c_uint64), _P]),
     "gbo_spgemm_nnz": (_I, [_P, _P, _P, C.POINTER(C.c_int64), _P]),
     "gbo_spgemm_fill": (_I, [_P, _P, _P, _P, _P, _P]),
     "gbo_bfs_multi": (_I, [_P, _P, _I, _P, C.POINTER(_I), _P]),
     "gbo_server_create": (_I, [_P, _I, _I, C.c_float, C.c_float, _I, C.POINTER(_P)]),
+    "gbo_server_set_queue_limit": (_I, [_P, C.c_longlong]),
     "gbo_server_submit_bfs": (_I, [_P, _I, C.POINTER(C.c_int64)]),
     "gbo_server_submit_ppr": (_I, [_P, _P, _P, _I, C.POINTER(C.c_int64)]),
     "gbo_server_poll": (_I, [_P, C.c_int64, _P, C.POINTER(C.c_double), C.POINTER(_I)]),
     "gbo_server_wait": (_I, [_P, C.c_int64, _P, C.POINTER(C.c_double), C.POINTER(_I), C.c_double]),
+    "gbo_server_wait_u8": (_I, [_P, C.c_int64, _P, C.POINTER(C.c_double), C.POINTER(_I), C.c_double]),
     "gbo_server_wait_device": (_I, [_P, C.c_int64, _P, C.POINTER(C.c_double), C.POINTER(_I),
                                     C.c_double, _P]),
     "gbo_server_get_stats": (_I, [_P, C.POINTER(ServerStats)]),
@@ -170,6 +197,7 @@ _SIGS = {
     "gbo_gen_er_avgdeg": (_I, [_I, C.c_double, C.c_uint64, C.POINTER(C.POINTER(CsrStruct))]),
     "gbo_gen_king_mesh": (_I, [_I, C.POINTER(C.POINTER(CsrStruct))]),
     "gbo_gen_er_batch": (_I, [_I, _I, _I, C.c_double, C.c_uint64, C.POINTER(C.POINTER(CsrStruct)), _P]),
+    "gbo_debug_inject": (_I, [_I, C.c_longlong]),
 }
 
 _lib = None
@@ -272,6 +300,11 @@ def device_to_numpy(ptr: int, dtype, count: int, stream=None) -> np.ndarray:
         check(lib().gbo_memcpy_d2h(_ptr(out), ptr, out.nbytes, stream), "d2h")
     check(lib().gbo_stream_sync(stream), "sync")
     return out
+
+
+def debug_inject(what: int, n: int) -> None:
+    """Host-side fault injection (INJECT_*); n = 0 disarms."""
+    check(lib().gbo_debug_inject(int(what), int(n)), "debug_inject")
 
 
 def device_count() -> int:
@@ -726,6 +759,11 @@ class Server:
         self.graph = graph
         self.n = graph.info().nrows
 
+    def set_queue_limit(self, max_pending: int) -> None:
+        """Submissions past max_pending queries not yet admitted return
+        GBO_ERR_FULL (0: unbounded)."""
+        check(lib().gbo_server_set_queue_limit(self.h, int(max_pending)), "server_set_queue_limit")
+
     def submit_bfs(self, src: int) -> int:
         t = C.c_int64(0)
         check(lib().gbo_server_submit_bfs(self.h, int(src), C.byref(t)), "server_submit_bfs")
@@ -747,6 +785,17 @@ class Server:
         lat, it = C.c_double(0), C.c_int(0)
         check(lib().gbo_server_wait(self.h, ticket, _ptr(out), C.byref(lat), C.byref(it), timeout),
               "server_wait")
+        return out, lat.value, it.value
+
+    def wait_u8(self, ticket: int, timeout=120.0, out=None):
+        """BFS levels as uint8 (255 = unreachable): (levels, latency_ms,
+        iterations).  `out` may be a uint8 array or a host pointer (int) of
+        n bytes, e.g. pinned memory from gbo_host_alloc."""
+        lat, it = C.c_double(0), C.c_int(0)
+        if out is None:
+            out = np.empty(self.n, np.uint8)
+        ptr = out if isinstance(out, int) else _ptr(out)
+        check(lib().gbo_server_wait_u8(self.h, ticket, ptr, C.byref(lat), C.byref(it), timeout), "server_wait_u8")
         return out, lat.value, it.value
 
     def wait_device(self, ticket: int, out, timeout=120.0):

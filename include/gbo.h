@@ -46,7 +46,8 @@ enum gbo_status {
   GBO_ERR_IO = 7,            /* file missing or malformed */
   GBO_ERR_UNSUPPORTED = 8,   /* combination not provided (e.g. layout) */
   GBO_ERR_OVERFLOW = 9,      /* a count does not fit the int32 B2SR indices */
-  GBO_ERR_NOTREADY = 10      /* server: result not yet available */
+  GBO_ERR_NOTREADY = 10,     /* server: result not yet available */
+  GBO_ERR_FULL = 11          /* server: the admission queue is at its limit */
 };
 
 #if defined(__GNUC__)
@@ -368,11 +369,58 @@ GBO_API int gbo_spgemm_fill(const gbo_graph* a, const gbo_graph* b,
  *             number of new vertices (the call then waits for the stream).
  * Between levels every rank places the shards' d_next words at their block
  * rows to form the next d_front (an all-gather of n/8 bytes); the loop ends
- * when no shard finds a new vertex.  graph-bit-ops_b200/shard.py drives it
- * over torch.distributed. */
+ * when no shard finds a new vertex.  gbo_bfs_sharded (below) runs that loop. */
 GBO_API int gbo_bfs_shard_level(const gbo_graph* shard, const void* d_front, void* d_visited,
                         int32_t* d_level, int level, void* d_next, uint64_t* h_count,
                         gbo_stream_t stream);
+
+/* The level loop of a block-row sharded BFS over caller-supplied operations
+ * (one rank; every rank of the job calls it):
+ *   level(user, L, &count)     one pull level of this rank's shard against the
+ *                              frontier of level L; count = its new vertices
+ *   allreduce_sum_u64(user, &v) v summed over all ranks, in place (host)
+ *   exchange(user)             every rank's next-frontier words into every
+ *                              rank's frontier of the next level
+ * The loop stops when the summed count is 0 (*h_depth = levels) or after
+ * max_levels levels (GBO_ERR_TIMEOUT).  A rank whose level step fails adds
+ * an error mark to the sum instead of its count, so all ranks leave at the
+ * same level with the same error.  gbo_bfs_sharded runs it on the GPU; the
+ * operations can also be a CPU step over any transport (the tests run it
+ * over gloo).  The reference has no multi-GPU path (its loop is
+ * algorithm/bfs.cu:508-564). */
+typedef struct gbo_shard_ops {
+  void* user;
+  int (*level)(void* user, int level, uint64_t* new_vertices);
+  int (*allreduce_sum_u64)(void* user, uint64_t* value);
+  int (*exchange)(void* user);
+} gbo_shard_ops;
+GBO_API int gbo_bfs_shard_loop(const gbo_shard_ops* ops, int max_levels, int* h_depth);
+
+/* The data plane of a sharded BFS: a sum of one host uint64 over all ranks,
+ * and an all-gather of `bytes` device bytes per rank (rank r's bytes at
+ * d_recv + r * bytes) on `stream`.  gbo_nccl_comm_create makes one over
+ * NCCL (NVLink / NVSwitch between GPUs); callers may supply their own. */
+typedef struct gbo_shard_comm {
+  void* user;
+  int (*allreduce_sum_u64)(void* user, uint64_t* value);
+  int (*allgather)(void* user, const void* d_send, void* d_recv, size_t bytes, gbo_stream_t stream);
+} gbo_shard_comm;
+/* BFS from src over all ranks, this rank holding rows [h_bounds[rank],
+ * h_bounds[rank+1]) of an n = h_bounds[world] vertex graph (every column;
+ * bounds on tile boundaries, e.g. balanced by stored entries) as `shard`.
+ * d_level gets the int32 levels of the shard's rows (-1 unreachable), every
+ * rank *h_depth.  Allocates its frontier and exchange buffers on `stream`
+ * (stream-ordered) for the call; returns after the stream has finished. */
+GBO_API int gbo_bfs_sharded(const gbo_graph* shard, int rank, int world, const int* h_bounds, int src,
+                            int32_t* d_level, int* h_depth, const gbo_shard_comm* comm,
+                            gbo_stream_t stream);
+/* NCCL data plane: gbo_nccl_unique_id fills 128 bytes on one rank, which
+ * the caller hands to every rank (any host channel); each rank then makes
+ * its communicator (its CUDA device current).  NCCL is loaded at run time
+ * (libnccl.so.2): GBO_ERR_UNSUPPORTED without it. */
+GBO_API int gbo_nccl_unique_id(void* h_id128);
+GBO_API int gbo_nccl_comm_create(int world, int rank, const void* h_id128, gbo_shard_comm** out);
+GBO_API int gbo_nccl_comm_destroy(gbo_shard_comm* comm);
 
 /* Multi-source BFS (batching): k sources (1 <= k <= 1024) traversed at once.
  * The frontier is an n x k bit matrix, so every level is one B2SR x bit
@@ -420,6 +468,11 @@ typedef struct gbo_server_stats {
 GBO_API int gbo_server_create(const gbo_graph* g, int bfs_slots, int ppr_slots,
                       float alpha, float tol, int ppr_max_iter,
                       gbo_server** out);
+/* Bound the admission queue: a submit that finds max_pending queries not
+ * yet admitted returns GBO_ERR_FULL and queues nothing (0: unbounded, the
+ * default).  The reference has no server; this is its request-overflow
+ * policy. */
+GBO_API int gbo_server_set_queue_limit(gbo_server* s, long long max_pending);
 GBO_API int gbo_server_submit_bfs(gbo_server* s, int src, int64_t* ticket);
 GBO_API int gbo_server_submit_ppr(gbo_server* s, const int* verts,
                           const float* weights, int count, int64_t* ticket);
@@ -428,6 +481,14 @@ GBO_API int gbo_server_poll(gbo_server* s, int64_t ticket, void* h_out,
                     double* latency_ms, int* iterations);
 GBO_API int gbo_server_wait(gbo_server* s, int64_t ticket, void* h_out,
                     double* latency_ms, int* iterations, double timeout_s);
+/* As gbo_server_wait for a BFS query, with the levels as one byte per
+ * vertex (uint8[n]; 255 = unreachable): a quarter of the int32 result's
+ * bytes over the host link and no widening.  When h_out is pinned
+ * (gbo_host_alloc) the device copies straight into it.  A query deeper than
+ * 254 levels keeps its result and returns GBO_ERR_OVERFLOW: collect it with
+ * gbo_server_wait.  PPR tickets return GBO_ERR_INVALID. */
+GBO_API int gbo_server_wait_u8(gbo_server* s, int64_t ticket, uint8_t* h_out,
+                               double* latency_ms, int* iterations, double timeout_s);
 /* As gbo_server_wait, but the result goes to the caller's device buffer
  * d_out (BFS int32[n] levels, PPR float[n]), for consumers that stay on the
  * GPU: no host copy.  The copy runs on `stream` (0: a high-priority stream
@@ -515,6 +576,22 @@ GBO_API int gbo_gen_king_mesh(int side, gbo_csr** out);
  * offsets[count+1] receives each graph's first vertex. */
 GBO_API int gbo_gen_er_batch(int count, int nmin, int nmax, double avg_degree,
                      uint64_t seed, gbo_csr** out, int* offsets);
+
+/* ------------------------------------------------ host-side fault injection
+ * For failure-path tests (the reference has no failure handling: its error
+ * checks compile away, utility.cu:17-30).  Nothing here makes a GPU fault,
+ * trap or hang; each knob changes a host-side decision.  Process-wide, off
+ * by default; n = 0 disarms.
+ *   GBO_INJECT_HOST_ALLOC  (n >= 1) the n-th host CSR allocation from now on
+ *       (readers, generators, CSR utilities) fails: the call returns
+ *       GBO_ERR_NOMEM and leaves its output untouched;
+ *   GBO_INJECT_REPLAY_CAP  (n >= 1) the iteration loops (BFS, SSSP,
+ *       PageRank, PPR, CC) replay their captured iterations at most n times
+ *       and return GBO_ERR_TIMEOUT when the device has not finished by then;
+ *   GBO_INJECT_SERVER_HOLD (n = 1) server workers admit no new query:
+ *       submissions stay pending (queries already in flight finish). */
+enum { GBO_INJECT_HOST_ALLOC = 1, GBO_INJECT_REPLAY_CAP = 2, GBO_INJECT_SERVER_HOLD = 3 };
+GBO_API int gbo_debug_inject(int what, long long n);
 
 #ifdef __cplusplus
 }

@@ -544,6 +544,42 @@ unsigned long long orc_bmm_sum_b2sr(const int* arp, const int* aci, const uint64
   return total;
 }
 
+// One pull level of a block-row BFS shard on the CPU, the contract of the
+// library's gbo_bfs_shard_level (the masked BMV step of algorithm/bfs.cu:
+// 508-564 restricted to the shard's rows): rows [0, nrows) of the shard CSR
+// (global column indices), words as one uint64 per b-bit word, `front` the
+// whole frontier, `visited` / `level` / `next` the shard's.  Returns the new
+// vertices.
+unsigned long long orc_bfs_shard_level(const int* rowptr, const int* colind, int nrows, int b,
+                                       const uint64_t* front, uint64_t* visited, int32_t* level, int lvl,
+                                       uint64_t* next) {
+  const int nbr = (nrows + b - 1) / b;
+  unsigned long long cnt = 0;
+  for (int R = 0; R < nbr; ++R) {
+    uint64_t o = 0;
+    for (int r = 0; r < b; ++r) {
+      const long long i = (long long)R * b + r;
+      if (i >= nrows) break;
+      if ((visited[R] >> (b - 1 - r)) & 1) continue;
+      for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+        const int j = colind[k];
+        if ((front[j / b] >> (b - 1 - j % b)) & 1) {
+          o |= 1ull << (b - 1 - r);
+          break;
+        }
+      }
+    }
+    next[R] = o;
+    if (o) {
+      visited[R] |= o;
+      for (int r = 0; r < b; ++r)
+        if ((o >> (b - 1 - r)) & 1) level[(long long)R * b + r] = lvl + 1;
+      cnt += (unsigned long long)popc64(o);
+    }
+  }
+  return cnt;
+}
+
 // ---------------------------------------------------------- generators
 // R-MAT (Chakrabarti, Zhan, Faloutsos 2004) with the benchmark's seeding, so
 // that the CPU legs build their inputs without the product library: edge k

@@ -55,6 +55,7 @@ def lib():
             "orc_bmm_sum_b2sr": (C.c_ulonglong, [_P, _P, _P, _I, _P, _P, _P, _I]),
             "orc_gen_rmat": (C.c_longlong, [_I, _I, C.c_double, C.c_double, C.c_double, C.c_uint64,
                                             _P, _P]),
+            "orc_bfs_shard_level": (C.c_ulonglong, [_P, _P, _I, _I, _P, _P, _P, _I, _P]),
             "orc_max_threads": (_I, []),
             "orc_set_threads": (None, [_I]),
         }
@@ -258,6 +259,14 @@ def bmm_sum_b2sr(a: B2SR, b_col: B2SR) -> int:
     assert a.b == b_col.b and b_col.layout == 1
     return int(lib().orc_bmm_sum_b2sr(_p(a.rowptr), _p(a.colind), _p(a.words), a.nbr,
                                       _p(b_col.rowptr), _p(b_col.colind), _p(b_col.words), a.b))
+
+
+def bfs_shard_level(rowptr, colind, nrows, b, front, visited, level, lvl, nxt) -> int:
+    """One pull level of a block-row BFS shard (uint64 words; visited, level
+    and nxt are updated in place)."""
+    rowptr, colind = _i32(rowptr), _i32(colind)
+    return int(lib().orc_bfs_shard_level(_p(rowptr), _p(colind), nrows, b, _p(front), _p(visited),
+                                         _p(level), lvl, _p(nxt)))
 
 
 class Csr:

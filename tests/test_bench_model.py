@@ -84,3 +84,29 @@ def test_cpu_baseline_single_thread_restores_threads(gbo, orc):
     v, t, cores, lv, depth = bench.cpu_bfs(orc, bs, csr, 2)
     assert v > 0 and cores == before
     assert np.array_equal(lv, orc.bfs_csr(csr.rowptr, csr.colind, csr.nrows, 0)[0])
+
+
+def test_bfs_level_bytes_rws_matches_direct_count(gbo, orc):
+    """The row-word slice pull model against a row-by-row walk."""
+    csr = gbo.gen_rmat(9, 6, seed=4)
+    n = csr.nrows
+    levels = np.asarray(orc.bfs_csr(csr.rowptr, csr.colind, n, 0)[0], np.int64)
+    got = bench.bfs_level_bytes_rws(csr, levels, head=3)
+    nbr = (n + 31) // 32
+    want = []
+    for L in range(int(levels.max()) + 1):
+        by = 8 * nbr + 4 * int((levels == L + 1).sum())
+        by += 8 * sum(any(levels[v] == L + 1 for v in range(R * 32, min(n, R * 32 + 32))) for R in range(nbr))
+        for v in range(n):
+            nb = csr.colind[csr.rowptr[v]:csr.rowptr[v + 1]]
+            if len(nb) == 0 or not (levels[v] == -1 or levels[v] > L):
+                continue
+            blocks = sorted(set(int(c) // 32 for c in nb))
+            seen = 0
+            for C in blocks:
+                seen += 1
+                if any(levels[u] == L for u in nb if u // 32 == C):
+                    break
+            by += 8 * seen + (16 if seen > 3 else 0)
+        want.append(by)
+    assert got == want

@@ -178,7 +178,7 @@ def test_bfs_direction_optimizing(gbo, orc, gpu, graphs, b):
 def test_bfs_push_every_level(gbo, orc, gpu, graphs, b):
     """Threshold above n: every level is a top-down step (atomics into the
     next frontier), including the dense middle levels."""
-    for name in ("rmat14", "mesh33", "star20000", "er1000"):
+    for name in ("rmat14", "mesh33", "star20000", "er1000", "latehub"):
         csr = graphs[name]
         g = gbo.Graph.from_csr(csr, b)
         g.set_bfs_direction(True, csr.nrows + 1)

@@ -135,3 +135,50 @@ def test_server_device_delivery_matches_host_delivery(gbo, orc, gpu):
             want, _ = orc.bfs_csr(csr.rowptr, csr.colind, n, arg)
             assert np.array_equal(dev, want)
     srv.close()
+
+
+def test_server_byte_levels_match_int32_levels(gbo, orc, gpu):
+    """gbo_server_wait_u8 delivers the same levels as bytes (255 =
+    unreachable), into numpy memory and into pinned memory; a query deeper
+    than 254 levels is refused with GBO_ERR_OVERFLOW and stays collectable
+    as int32; a PPR ticket is refused."""
+    import ctypes as C
+
+    csr = gbo.gen_rmat(12, 16, seed=7)
+    n = csr.nrows
+    g = gbo.Graph.from_csr(csr, 32)
+    srv = gbo.Server(g, bfs_slots=64, ppr_slots=32)
+    srcs = np.random.default_rng(21).integers(0, n, 40)
+    t8 = [srv.submit_bfs(int(s)) for s in srcs]
+    t32 = [srv.submit_bfs(int(s)) for s in srcs]
+    pin = C.c_void_p()
+    gbo.check(gbo.lib().gbo_host_alloc(C.byref(pin), n), "host_alloc")
+    try:
+        for i, (s, a, b) in enumerate(zip(srcs, t8, t32)):
+            if i % 2:
+                got, lat, it = srv.wait_u8(a, out=pin.value)
+                got = np.ctypeslib.as_array(C.cast(pin.value, C.POINTER(C.c_uint8)), (n,)).copy()
+            else:
+                got, lat, it = srv.wait_u8(a)
+            want, _, _ = srv.wait(b, "bfs")
+            assert np.array_equal(np.where(got == 255, -1, got.astype(np.int32)), want), int(s)
+            assert np.array_equal(want, orc.bfs_csr(csr.rowptr, csr.colind, n, int(s))[0])
+        tp = srv.submit_ppr([1, 2], [0.5, 0.5])
+        with pytest.raises(gbo.GboError) as e:
+            srv.wait_u8(tp)
+        assert e.value.status == gbo.GBO_ERR_INVALID
+        srv.wait(tp, "ppr")
+    finally:
+        gbo.lib().gbo_host_free(pin.value)
+    srv.close()
+    m = 300  # a path: 299 levels
+    path = gbo.csr_from_edges(np.arange(m - 1, dtype=np.int32), np.arange(1, m, dtype=np.int32), m, True, True)
+    gp = gbo.Graph.from_csr(path, 32)
+    sp = gbo.Server(gp, bfs_slots=32, ppr_slots=0)
+    t = sp.submit_bfs(0)
+    with pytest.raises(gbo.GboError) as e:
+        sp.wait_u8(t)
+    assert e.value.status == gbo.GBO_ERR_OVERFLOW
+    lv, _, _ = sp.wait(t, "bfs")
+    assert np.array_equal(lv, np.arange(m))
+    sp.close()
