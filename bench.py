@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--no-permuted", action="store_true", help="skip the degree-ordered variant")
     ap.add_argument("--serve-qps", type=float, default=8000.0, help="offered BFS query rate")
     ap.add_argument("--serve-s", type=float, default=1.5, help="seconds of arrivals per stream")
+    ap.add_argument("--serve-slots", type=int, default=64, help="BFS slots of the served streams' server")
     ap.add_argument("--tc-graphs", default="mesh,rmat", help="graphs of --workload tc (mesh, rmat)")
     ap.add_argument("--tc-variants", default="input,degree", help="vertex orders of --workload tc")
     ap.add_argument("--tc-tiles", default="8,16,32,64", help="tile widths of --workload tc")
@@ -378,7 +379,7 @@ def run_reference(args, ws, rank):
 
 
 # --------------------------------------------------------------- serving
-def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed, delivery="host", sample_every=0):
+def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed, delivery="host", sample_every=0, slots=64):
     """Poisson arrivals of BFS sources and PPR sets (1..64 vertices, Dirichlet
     weights) into the continuous-batching server.  `delivery`: "host" (int32
     levels in host memory, gbo_server_wait), "u8" (byte levels in pinned
@@ -403,7 +404,7 @@ def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed, delivery="host
                                rng.dirichlet(np.ones(m)).astype(np.float32))))
         else:
             qs.append(("bfs", int(rng.integers(0, n))))
-    srv = gbo.Server(g, bfs_slots=1024, ppr_slots=32 if ppr_frac > 0 else 0, alpha=0.85, tol=1e-7)
+    srv = gbo.Server(g, bfs_slots=slots, ppr_slots=32 if ppr_frac > 0 else 0, alpha=0.85, tol=1e-7)
     # one queue and consumer pool per kind, so clients waiting on slow PPR
     # results never hold BFS results back (each pool collects in order)
     tq = {"bfs": queue.Queue(), "ppr": queue.Queue()}
@@ -479,7 +480,7 @@ def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed, delivery="host
     st = srv.stats()
     srv.close()
     span = max(done_t) - first_arrival if done_t else float("nan")
-    out = {"offered_qps": rate_qps, "queries": nq, "delivery": delivery, "qps": len(done_t) / span,
+    out = {"offered_qps": rate_qps, "queries": nq, "delivery": delivery, "bfs_slots": slots, "qps": len(done_t) / span,
            "span_s": span, "rounds": st["rounds"], "kernel_launches": st["kernel_launches"],
            "phase_ms": {k: round(st[k], 1) for k in ("bfs_round_ms", "ppr_round_ms", "retire_ms", "copy_ms",
                                                      "copy_wait_ms", "copy_d2h_ms", "copy_widen_ms")}}
@@ -493,7 +494,7 @@ def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed, delivery="host
     return out, samples
 
 
-def served_suite(gbo, g, n, plain_ms, rate, dur, check_fn, seed=5):
+def served_suite(gbo, g, n, plain_ms, rate, dur, check_fn, seed=5, slots=64):
     """Capacity of the server with each delivery (a stream offered above it),
     then streams offered at 50 % and 90 % of that capacity (p50/p99 of
     service latency, not of a queue), and a 10 % PPR mix.  Every stream's
@@ -502,18 +503,19 @@ def served_suite(gbo, g, n, plain_ms, rate, dur, check_fn, seed=5):
     res = {"plain_bfs_qps": plain_qps, "qps_definition": "completed queries / (last completion - first arrival)"}
     ok = True
     for delivery, offered in (("device", 2.0 * rate), ("u8", rate), ("host", rate)):
-        cap, smp = serve_stream(gbo, g, n, offered, dur, 0.0, seed, delivery, sample_every=97)
+        cap, smp = serve_stream(gbo, g, n, offered, dur, 0.0, seed, delivery, sample_every=97, slots=slots)
         ok = ok and all(check_fn(src, lv) for src, lv in smp)
         cap["vs_plain_bfs_qps"] = cap["qps"] / plain_qps
         res[f"capacity_{delivery}"] = cap
         if delivery == "host":
             continue
         for frac in (0.5, 0.9):
-            r, smp = serve_stream(gbo, g, n, frac * cap["qps"], dur, 0.0, seed + 1, delivery, sample_every=97)
+            r, smp = serve_stream(gbo, g, n, frac * cap["qps"], dur, 0.0, seed + 1, delivery, sample_every=97,
+                                  slots=slots)
             ok = ok and all(check_fn(src, lv) for src, lv in smp)
             r["vs_plain_bfs_qps"] = r["qps"] / plain_qps
             res[f"{delivery}_{int(frac * 100)}pct"] = r
-    mixed, smp = serve_stream(gbo, g, n, rate / 8, dur, 0.1, seed + 2, "u8", sample_every=13)
+    mixed, smp = serve_stream(gbo, g, n, rate / 8, dur, 0.1, seed + 2, "u8", sample_every=13, slots=slots)
     ok = ok and all(check_fn(src, lv) for src, lv in smp)
     res["mixed_10pct_ppr"] = mixed
     res["parity"] = {"checked": "every 97th BFS result of each stream (13th of the mix) against gbo_bfs of "
@@ -547,20 +549,24 @@ def run_ours(args, ws, rank, local):
     for _ in range(args.warmup):
         g.bfs(0, out=d_level)
     ev0, ev1 = gbo.Event(), gbo.Event()
-    step_ms_all, launches = [], 0
     dist.barrier()
     gbo.sync()
     ev0.record()
     for _ in range(args.steps):
-        g.bfs(0, out=d_level)
-        st = g.last_run()
-        step_ms_all.extend(st["step_ms"])
-        launches += st["kernel_launches"]
+        g.bfs(0, out=d_level, wait=False)  # queued back to back: the loop runs on the device
     ev1.record()
     gbo.sync()
     dist.barrier()
     ms = ev0.elapsed_ms(ev1) / args.steps
     ms_max = dist.max(ms)
+    # per-level times (device clock stamps at every level's end) and kernel
+    # launches per BFS, from the same call run once more per step
+    step_ms_all, launches = [], 0
+    for _ in range(args.steps):
+        g.bfs(0, out=d_level)
+        st = g.last_run()
+        step_ms_all.extend(st["step_ms"])
+        launches += st["kernel_launches"]
 
     # e2e: same call with every step's levels read back into pinned host
     # memory.  Two result buffers and a copy stream: the read-back of step i
@@ -574,7 +580,7 @@ def run_ours(args, ws, rank, local):
     gbo.sync()
     ev0.record()
     for i in range(args.steps):
-        g.bfs(0, out=d_levels[i % 2])
+        g.bfs(0, out=d_levels[i % 2])  # returns when the levels are written
         copy_stream.sync()
         gbo.check(gbo.lib().gbo_memcpy_d2h(h_levels[i % 2].ptr, d_levels[i % 2].ptr, 4 * n,
                                            copy_stream.ptr), "d2h")
@@ -715,7 +721,8 @@ def run_ours(args, ws, rank, local):
             g_row.bfs(int(src), out=alone)
             return bool(np.array_equal(alone.to_numpy(np.int32, n), lv))
 
-        served = served_suite(gbo, g_row, n, ms, args.serve_qps, args.serve_s, same_as_alone)
+        served = served_suite(gbo, g_row, n, ms, args.serve_qps, args.serve_s, same_as_alone,
+                              slots=args.serve_slots)
         alone.free()
     wb = max(1, args.tile // 8)
     bmv_bytes = (int(info.nblocks) * (args.tile * args.tile // 8 + 4) + 4 * (info.nblockrows + 1)
@@ -1226,7 +1233,7 @@ def suite_serve(args):
     out = {}
     rates = [float(r) for r in args.serve_rates.split(",")]
     for rate in rates:
-        r, _ = serve_stream(gbo, g, n, rate, min(args.serve_s, 2e4 / rate), 0.1, 11, "u8")
+        r, _ = serve_stream(gbo, g, n, rate, min(args.serve_s, 2e4 / rate), 0.1, 11, "u8", slots=args.serve_slots)
         r["bfs_vs_plain"] = r.get("bfs_qps", 0.0) / plain["bfs_qps"]
         r["ppr_vs_plain"] = r.get("ppr_qps", 0.0) / plain["ppr_qps"]
         out[int(rate)] = r

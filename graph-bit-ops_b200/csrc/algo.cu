@@ -3,12 +3,12 @@
 // The reference loops (algorithm/bfs.cu:508-564, sssp.cu:420-470,
 // pr.cu:449-513, cc.cu:223-287) launch 5-9 kernels per iteration and copy a
 // convergence scalar to the host every iteration.  Here each iteration is one
-// fused BMV kernel over the balanced work items plus a small kernel that
-// finishes split block rows; the last block of that kernel (atomic ticket)
-// decides termination on the device.  K iterations are captured once into a
-// CUDA graph (every kernel exits at once when the device "done" flag is set)
-// and the host replays the graph, reading the flag from pinned memory once
-// per replay instead of once per iteration.
+// fused step kernel plus a small kernel that finishes split block rows; the
+// last block of that kernel (atomic ticket) decides termination on the
+// device.  One iteration is captured once as the body of a conditional WHILE
+// node of a CUDA graph, and the deciding block clears the node's condition
+// when the loop stops: a whole traversal or solve is one graph launch with
+// no host round trip and no idle iterations.
 #include <string.h>
 
 #include <algorithm>
@@ -38,7 +38,14 @@ struct Ctrl {
   int row_scale;  // PR-type step: 0 = columns scaled (PageRank), 1 = rows (adjoint on P = P^T)
   int mode;       // BFS: 0 = pull (bottom-up) step, 1 = push (top-down) step
   int push_thr;   // BFS: push while the frontier has fewer vertices (0 = never)
+  // the running loop's CUDA graph condition (cleared when the loop stops)
+  // and its iteration end times (globaltimer ns; [0] = loop start)
+  unsigned long long cond;
+  unsigned long long* stamps;
 };
+
+// Iteration end times kept per loop run (more iterations run untimed).
+constexpr int kStampCap = 4096;
 
 }  // namespace gbo
 
@@ -63,12 +70,15 @@ struct AlgoState {
   int* seeds = nullptr;  // multi-seed BFS sources
   int nseeds_cap = 0;
   double* acc64 = nullptr;  // PPR adjoint scatter accumulator
+  double* pr_part = nullptr;  // row-word slices: one partial sum per long-row chunk
   void* scratch = nullptr;  // split partials (nslots * b * 8 bytes)
   cudaGraphExec_t exec[8] = {};
   const void* exec_key[8] = {};
-  // events recorded around the main kernel of every captured iteration
-  cudaEvent_t ev[16] = {};
-  int ev_ready = 0;
+  unsigned long long cond[8] = {};       // each loop graph's condition handle
+  unsigned long long* stamps = nullptr;  // kStampCap + 1 iteration end times
+  int launches_per_iter = 0;             // kernels of one loop iteration
+  bool stats_pending = false;            // step times not yet read back
+
   // statistics of the last algorithm run
   std::vector<float> step_ms;
   int replays = 0;
@@ -81,6 +91,7 @@ namespace gbo {
 namespace {
 
 constexpr int kTPB = 256;
+// Iterations per unit of the injected loop cap (gbo_debug_inject).
 constexpr int kStepsPerGraph = 8;
 
 enum AlgoId { A_BFS = 0, A_SSSP = 1, A_PR = 2, A_CC = 3, A_PPR_F = 4, A_PPR_B = 5, A_PPR_BG = 6 };
@@ -180,9 +191,29 @@ __device__ __forceinline__ void close_iteration(Ctrl* ctrl, Decide decide) {
     c->count = 0ull;
     c->work = 0ull;
     c->ticket = 0u;
-    if (stop) c->done = 1;
+    if (c->stamps && it <= kStampCap) {
+      unsigned long long t;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+      c->stamps[it] = t;
+    }
+    if (stop) {
+      c->done = 1;
+      cudaGraphSetConditional((cudaGraphConditionalHandle)c->cond, 0u);
+    }
     __threadfence();
   }
+}
+
+// Before a loop graph runs: its condition handle and the start stamp; an
+// injected cap (gbo_debug_inject) cuts the loop's iteration limit.
+__global__ void k_loop_begin(Ctrl* ctrl, unsigned long long cond, unsigned long long* stamps, int cap_iters) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  ctrl->cond = cond;
+  ctrl->stamps = stamps;
+  if (cap_iters > 0 && cap_iters < ctrl->max_iter) ctrl->max_iter = cap_iters;
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  stamps[0] = t;
 }
 
 // ============================================================== BFS
@@ -259,21 +290,21 @@ __global__ void __launch_bounds__(kTPB) k_bfs_step(GView v, typename Word<B>::T*
   block_add_u64(cnt, &ctrl->count);
 }
 
-// Pull step on the row-word slices of a b = 32 ROW graph.  A warp takes 32
-// consecutive block rows at a time from the work counter, reads their
-// visited words in one coalesced load and walks each open block row (a row
-// still unvisited) with lane r on row r: entry k of every open row comes in
-// one 256-byte load, the frontier word of its block column is gathered, two
-// entries per round; a row leaves at its first entry that meets the
+// Pull step on the row-word slices of a b = 32 ROW graph.  A warp reads the
+// visited words of its next 32 block rows (strided over the grid) in one
+// round of loads and walks each open block row (a row still unvisited) with
+// lane r on row r: entry k of every open row comes in one 256-byte load,
+// the frontier word of its block column is gathered, four entries per
+// round; a row leaves at its first entry that meets the
 // frontier or when its entries run out (entries are in ascending block
 // column, hubs of power-law graphs first), the block row when no row is
 // left.  Rows still open after the head scan their tails: tails of up to
 // kLongTail entries one lane per row with four entries in flight, longer
 // ones by the whole warp 32 entries at a time.  Rows without entries start
 // visited (k_live), so every open row has an entry.
-constexpr int kLongTail = 64;
+constexpr int kLongTail = kRwsLongTail;
 
-__global__ void __launch_bounds__(kTPB) k_bfs_pull_rws(GView v, unsigned* __restrict__ front,
+__global__ void __launch_bounds__(kTPB, 6) k_bfs_pull_rws(GView v, unsigned* __restrict__ front,
                                                        unsigned* __restrict__ visited,
                                                        int* __restrict__ level, Ctrl* __restrict__ ctrl) {
   if (((volatile Ctrl*)ctrl)->done || ((volatile Ctrl*)ctrl)->mode) return;
@@ -283,15 +314,13 @@ __global__ void __launch_bounds__(kTPB) k_bfs_pull_rws(GView v, unsigned* __rest
   unsigned* __restrict__ z = front_buf(front, v.nbr, lvl + 2);
   const unsigned lane = threadIdx.x & 31;
   const unsigned kFull = 0xffffffffu;
-  const long long nunits = ((long long)v.nbr + 31) >> 5;
+  const long long nwarps = warps_total();
   unsigned long long cnt = 0;
-  for (;;) {
-    unsigned long long u0 = 0;
-    if (lane == 0) u0 = atomicAdd(&ctrl->work, 1ull);
-    const long long u = (long long)__shfl_sync(kFull, u0, 0);
-    if (u >= nunits) break;
-    const long long R0 = u << 5;
-    const long long Rl = R0 + lane;
+  // lane j reads the visited word of block row base + j * nwarps: one round
+  // of loads finds the warp's open block rows among its next 32, and the
+  // stride spreads neighbouring (similar) block rows over the warps
+  for (long long base = warp_global(); base < v.nbr; base += 32 * nwarps) {
+    const long long Rl = base + (long long)lane * nwarps;
     unsigned visl = kFull;
     if (Rl < v.nbr) {
       visl = visited[Rl];
@@ -301,23 +330,24 @@ __global__ void __launch_bounds__(kTPB) k_bfs_pull_rws(GView v, unsigned* __rest
     while (openb) {
       const int j = __ffs(openb) - 1;
       openb &= openb - 1;
-      const long long R = R0 + j;
+      const long long R = base + (long long)j * nwarps;
       const unsigned vis = __shfl_sync(kFull, visl, j);
       bool need = !((vis >> (31 - lane)) & 1u);
       bool hit = false;
       const uint2* __restrict__ hp = v.rws_head + (size_t)R * (kRwsHead * 32) + lane;
+      // four entries per round: most rows of a dense level are answered by
+      // the first round, so its loads are issued together
 #pragma unroll
-      for (int k = 0; k < kRwsHead; k += 2) {
+      for (int k = 0; k < kRwsHead; k += 4) {
         if (!__any_sync(kFull, need)) break;
-        uint2 e0 = make_uint2(kRwsNone, 0u), e1 = make_uint2(kRwsNone, 0u);
-        if (need) {
-          e0 = hp[(size_t)k * 32];
-          e1 = hp[(size_t)(k + 1) * 32];
-        }
-        const unsigned x0 = e0.x != kRwsNone ? __ldg(x + e0.x) : 0u;
-        const unsigned x1 = e1.x != kRwsNone ? __ldg(x + e1.x) : 0u;
-        hit = hit || (need && ((e0.y & x0) | (e1.y & x1)) != 0u);
-        need = need && !hit && e1.x != kRwsNone;
+        uint2 e[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) e[q] = need ? hp[(size_t)(k + q) * 32] : make_uint2(kRwsNone, 0u);
+        unsigned a = 0u;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) a |= e[q].x != kRwsNone ? (e[q].y & __ldg(x + e[q].x)) : 0u;
+        hit = hit || (need && a != 0u);
+        need = need && !hit && e[3].x != kRwsNone;
       }
       if (__any_sync(kFull, need)) {
         const long long row = R * 32 + lane;
@@ -823,9 +853,9 @@ __global__ void __launch_bounds__(kTPB) k_pr_step(GView v, float* __restrict__ p
 // The same iteration over the row-word slices of a b = 32 ROW graph: a warp
 // per block row, lane r sums row r's columns entry by entry (the head's
 // entry k of the 32 rows in one 256-byte load, two entries in flight), then
-// its tail; tails longer than kLongTail are summed by the whole warp, 32
-// entries at a time, the lanes' partial sums combined by a fixed shuffle
-// tree.  Every row's sum has a fixed order (fp64), whatever the grid.
+// its tail.  Rows with tails longer than kRwsLongTail (hubs) are left to
+// k_pr_long_chunks / k_pr_long_rows, which spread them over many warps.
+// Every row's sum has a fixed order (fp64), whatever the grid.
 __device__ __forceinline__ double pr_word_sum(unsigned c, unsigned w, const float* __restrict__ xg) {
   double a = 0.0;
   const size_t base = (size_t)c * 32;
@@ -837,18 +867,61 @@ __device__ __forceinline__ double pr_word_sum(unsigned c, unsigned w, const floa
   return a;
 }
 
+// Four entries at once: the gathered operand of one set column per entry
+// per round, four gathers in flight; the adds follow a fixed order (round,
+// then entry), so a row's sum depends on the graph only.
+__device__ __forceinline__ double pr_entries4(const uint2 (&e)[4], const float* __restrict__ xg) {
+  uint32_t m[4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) m[u] = e[u].x != kRwsNone ? e[u].y : 0u;
+  double a = 0.0;
+  while (m[0] | m[1] | m[2] | m[3]) {
+    float g[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      g[u] = 0.f;
+      if (m[u]) {
+        const int j = __clz(m[u]);
+        m[u] &= ~(0x80000000u >> j);
+        g[u] = __ldg(xg + (size_t)e[u].x * 32 + j);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) a += (double)g[u];
+  }
+  return a;
+}
+
+struct PrIter {  // the iterate's buffers and coefficients of iteration itn
+  const float* x;
+  float* y;
+  float* ys;
+  const float* xg;
+  double alpha, add, adds;
+  int norm, row_scale;
+};
+
+__device__ __forceinline__ PrIter pr_iter(float* pr, float* prs, const Ctrl* ctrl, int n) {
+  PrIter p;
+  const int itn = ((volatile Ctrl*)ctrl)->iter;
+  p.alpha = ctrl->alpha;
+  p.add = ctrl->add;
+  p.adds = ctrl->add_scale;
+  p.norm = ctrl->norm;
+  p.row_scale = ctrl->row_scale;
+  p.x = pr + (size_t)(itn & 1) * n;
+  p.y = pr + (size_t)((itn + 1) & 1) * n;
+  p.ys = prs + (size_t)((itn + 1) & 1) * n;
+  p.xg = p.row_scale ? p.x : prs + (size_t)(itn & 1) * n;
+  return p;
+}
+
 __global__ void __launch_bounds__(kTPB) k_pr_step_rws(GView v, float* __restrict__ pr, float* __restrict__ prs,
                                                       const float* __restrict__ inv,
                                                       const float* __restrict__ pv, Ctrl* __restrict__ ctrl) {
   if (((volatile Ctrl*)ctrl)->done) return;
-  const int itn = ((volatile Ctrl*)ctrl)->iter;
-  const double alpha = ctrl->alpha, add = ctrl->add, adds = ctrl->add_scale;
-  const int norm = ctrl->norm, row_scale = ctrl->row_scale;
   const int n = v.nrows;
-  const float* __restrict__ x = pr + (size_t)(itn & 1) * n;
-  float* __restrict__ y = pr + (size_t)((itn + 1) & 1) * n;
-  float* __restrict__ ys = prs + (size_t)((itn + 1) & 1) * n;
-  const float* __restrict__ xg = row_scale ? x : prs + (size_t)(itn & 1) * n;
+  const PrIter P = pr_iter(pr, prs, ctrl, n);
   const unsigned lane = threadIdx.x & 31;
   const unsigned kFull = 0xffffffffu;
   double e = 0.0;
@@ -859,45 +932,77 @@ __global__ void __launch_bounds__(kTPB) k_pr_step_rws(GView v, float* __restrict
     double a = 0.0;
     bool more = true;
 #pragma unroll
-    for (int k = 0; k < kRwsHead; k += 2) {
+    for (int k = 0; k < kRwsHead; k += 4) {
       if (!__any_sync(kFull, more)) break;
-      uint2 e0 = make_uint2(kRwsNone, 0u), e1 = make_uint2(kRwsNone, 0u);
-      if (more) {
-        e0 = hp[(size_t)k * 32];
-        e1 = hp[(size_t)(k + 1) * 32];
-      }
-      if (e0.x != kRwsNone) a += pr_word_sum(e0.x, e0.y, xg);
-      if (e1.x != kRwsNone) a += pr_word_sum(e1.x, e1.y, xg);
-      more = more && e1.x != kRwsNone;
+      uint2 e[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) e[u] = more ? hp[(size_t)(k + u) * 32] : make_uint2(kRwsNone, 0u);
+      a += pr_entries4(e, P.xg);
+      more = more && e[3].x != kRwsNone;
     }
     long long tb = 0, te = 0;
     if (more) {
       tb = v.rws_tail_ptr[row];
       te = v.rws_tail_ptr[row + 1];
     }
-    unsigned longm = __ballot_sync(kFull, te - tb > kLongTail);
-    if (te - tb <= kLongTail) {
-      for (long long p = tb; p < te; p += 2) {
-        const uint2 e0 = v.rws_tail[p];
-        const uint2 e1 = p + 1 < te ? v.rws_tail[p + 1] : make_uint2(kRwsNone, 0u);
-        a += pr_word_sum(e0.x, e0.y, xg);
-        if (e1.x != kRwsNone) a += pr_word_sum(e1.x, e1.y, xg);
-      }
-    }
-    while (longm) {
-      const int q = __ffs(longm) - 1;
-      longm &= longm - 1;
-      const long long qb = __shfl_sync(kFull, tb, q), qe = __shfl_sync(kFull, te, q);
-      double part = 0.0;
-      for (long long p = qb + lane; p < qe; p += 32) {
-        const uint2 ee = v.rws_tail[p];
-        part += pr_word_sum(ee.x, ee.y, xg);
-      }
+    if (te - tb > kRwsLongTail) continue;  // a long row: the chunk kernels own it
+    for (long long p = tb; p < te; p += 4) {
+      uint2 e[4];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
-      if ((int)lane == q) a += part;
+      for (int u = 0; u < 4; ++u) e[u] = p + u < te ? v.rws_tail[p + u] : make_uint2(kRwsNone, 0u);
+      a += pr_entries4(e, P.xg);
     }
-    if (row < n) e += pr_row_update(row, a, x, y, ys, inv, pv, alpha, add, adds, norm, row_scale);
+    if (row < n)
+      e += pr_row_update(row, a, P.x, P.y, P.ys, inv, pv, P.alpha, P.add, P.adds, P.norm, P.row_scale);
+  }
+  block_add_f64(e, &ctrl->err);
+}
+
+// Long rows, part 1: a warp per chunk of a long row's tail sums its entries
+// (lanes strided, partial sums combined by a fixed shuffle tree); the first
+// chunk of a row also sums the row's head.  One fp64 partial per chunk.
+__global__ void __launch_bounds__(kTPB) k_pr_long_chunks(GView v, float* __restrict__ pr,
+                                                         float* __restrict__ prs, Ctrl* __restrict__ ctrl,
+                                                         double* __restrict__ part) {
+  if (((volatile Ctrl*)ctrl)->done) return;
+  const PrIter P = pr_iter(pr, prs, ctrl, v.nrows);
+  const unsigned lane = threadIdx.x & 31;
+  const long long nwarps = warps_total();
+  for (long long q = warp_global(); q < v.rws_nchunk; q += nwarps) {
+    const long long row = v.rws_chunk_row[q];
+    const long long b = v.rws_chunk_beg[q], e = v.rws_chunk_end[q];
+    double a = 0.0;
+    if (b == v.rws_tail_ptr[row] && lane < kRwsHead) {
+      const uint2 h = v.rws_head[((size_t)(row >> 5) * kRwsHead + lane) * 32 + (row & 31)];
+      a += pr_word_sum(h.x, h.y, P.xg);  // a long row fills its head
+    }
+    for (long long p = b + lane; p < e; p += 128) {
+      uint2 t[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) t[u] = p + 32 * u < e ? v.rws_tail[p + 32 * u] : make_uint2(kRwsNone, 0u);
+      a += pr_entries4(t, P.xg);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) part[q] = a;
+  }
+}
+
+// Long rows, part 2: a thread per long row adds its chunks' partials in
+// chunk order and updates the row.
+__global__ void k_pr_long_rows(GView v, float* __restrict__ pr, float* __restrict__ prs,
+                               const float* __restrict__ inv, const float* __restrict__ pv,
+                               Ctrl* __restrict__ ctrl, const double* __restrict__ part) {
+  if (((volatile Ctrl*)ctrl)->done) return;
+  const PrIter P = pr_iter(pr, prs, ctrl, v.nrows);
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0.0;
+  if (q < v.rws_nlong) {
+    const long long row = v.rws_long_row[q];
+    double a = 0.0;
+    for (long long c = v.rws_long_chunk0[q]; c < v.rws_long_chunk0[q + 1]; ++c) a += part[c];
+    if (row < v.nrows)
+      e = pr_row_update(row, a, P.x, P.y, P.ys, inv, pv, P.alpha, P.add, P.adds, P.norm, P.row_scale);
   }
   block_add_f64(e, &ctrl->err);
 }
@@ -1191,8 +1296,7 @@ int get_state(gbo_graph* g, AlgoState** out) {
     const size_t sb = (size_t)g->nslots * (size_t)g->b * 8 + 64;
     GBO_CUDA_TRY(cudaMalloc(&a->scratch, sb));
     g->device_bytes += (long long)sb + (long long)sizeof(Ctrl);
-    for (auto& e : a->ev) GBO_CUDA_TRY(cudaEventCreate(&e));
-    a->ev_ready = 1;
+    GBO_CUDA_TRY(cudaMalloc(&a->stamps, sizeof(unsigned long long) * (kStampCap + 1)));
   }
   *out = g->algo;
   return GBO_OK;
@@ -1258,6 +1362,13 @@ int ensure_pr_vectors(gbo_graph* g, AlgoState* a) {
   return GBO_OK;
 }
 
+int ensure_pr_part(gbo_graph* g, AlgoState* a) {
+  if (a->pr_part || g->rws_nchunk <= 0) return GBO_OK;
+  GBO_CUDA_TRY(cudaMalloc(&a->pr_part, sizeof(double) * (size_t)g->rws_nchunk));
+  g->device_bytes += 8LL * g->rws_nchunk;
+  return GBO_OK;
+}
+
 int ensure_vec_i32(gbo_graph* g, int** p) {
   if (!*p) {
     GBO_CUDA_TRY(cudaMalloc(p, sizeof(int) * (size_t)(g->nrows > 0 ? g->nrows : 1)));
@@ -1266,7 +1377,11 @@ int ensure_vec_i32(gbo_graph* g, int** p) {
   return GBO_OK;
 }
 
-// Capture kStepsPerGraph iterations of `body` once per (graph, algorithm).
+// One loop graph per (graph, algorithm): a conditional WHILE node whose
+// body is one iteration of `body`, captured once.  The iteration's closing
+// kernel clears the condition when the loop stops (close_iteration), so the
+// whole loop runs on the device from one launch: no host round trip per
+// iteration and no iterations past the last.
 template <typename Body>
 int get_exec(AlgoState* a, int id, const void* key, Body body) {
   if (a->exec[id] && a->exec_key[id] == key) return GBO_OK;
@@ -1275,63 +1390,75 @@ int get_exec(AlgoState* a, int id, const void* key, Body body) {
     a->exec[id] = nullptr;
   }
   cudaGraph_t graph = nullptr;
-  GBO_CUDA_TRY(cudaStreamBeginCapture(a->cap, cudaStreamCaptureModeThreadLocal));
-  int st = GBO_OK;
-  int launches = 0;
-  for (int k = 0; k < kStepsPerGraph && st == GBO_OK; ++k) st = body(a->cap, k, &launches);
-  cudaError_t e = cudaStreamEndCapture(a->cap, &graph);
-  if (st != GBO_OK) {
-    if (graph) cudaGraphDestroy(graph);
-    return st;
+  GBO_CUDA_TRY(cudaGraphCreate(&graph, 0));
+  cudaGraphConditionalHandle handle;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault);
+  cudaGraphNodeParams p = {};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = handle;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  if (e == cudaSuccess) e = cudaGraphAddNode(&node, graph, nullptr, 0, &p);
+  if (e == cudaSuccess)
+    e = cudaStreamBeginCaptureToGraph(a->cap, p.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    return fail_cuda(e, "loop graph");
   }
-  if (e != cudaSuccess) return fail_cuda(e, "cudaStreamEndCapture");
+  int launches = 0;
+  const int st = body(a->cap, 0, &launches);
+  cudaGraph_t body_graph = p.conditional.phGraph_out[0];
+  e = cudaStreamEndCapture(a->cap, &body_graph);
+  if (st != GBO_OK || e != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    return st != GBO_OK ? st : fail_cuda(e, "cudaStreamEndCapture");
+  }
   e = cudaGraphInstantiate(&a->exec[id], graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) return fail_cuda(e, "cudaGraphInstantiate");
   a->exec_key[id] = key;
-  a->launches_per_replay = launches;
+  a->cond[id] = (unsigned long long)handle;
+  a->launches_per_iter = launches;
   return GBO_OK;
 }
 
-// Brackets the main kernel of captured iteration k with events (timing of
-// the iteration's BMV launch, read back after each replay).
-struct StepTimer {
-  AlgoState* a;
-  cudaStream_t s;
-  int k;
-  void begin() const { cudaEventRecordWithFlags(a->ev[2 * k], s, cudaEventRecordExternal); }
-  void end() const { cudaEventRecordWithFlags(a->ev[2 * k + 1], s, cudaEventRecordExternal); }
-};
-
-// Replay the captured iterations until the device sets `done`.
+// Run a loop graph on s (after the algorithm's init kernel).  With `iters`
+// the call waits for the loop and returns its iteration count; otherwise it
+// returns at once (stream-ordered).  An injected iteration cap that cuts the
+// loop returns GBO_ERR_TIMEOUT.
 int run_until_done(AlgoState* a, int id, cudaStream_t s, int max_iter, int* iters) {
-  long long max_launch = (long long)max_iter / kStepsPerGraph + 2;
   const long long cap = inject_replay_cap();
-  if (cap > 0 && cap < max_launch) max_launch = cap;
-  a->step_ms.clear();
-  a->replays = 0;
-  a->launches = 1;  // the init kernel
-  int it0 = 0;
-  for (long long k = 0; k < max_launch; ++k) {
-    GBO_CUDA_TRY(cudaGraphLaunch(a->exec[id], s));
-    GBO_CUDA_TRY(cudaMemcpyAsync(a->h_ctrl, a->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
-    GBO_CUDA_TRY(cudaStreamSynchronize(s));
-    ++a->replays;
-    a->launches += a->launches_per_replay;
-    const int it1 = a->h_ctrl->iter;
-    for (int q = 0; q < it1 - it0 && q < kStepsPerGraph; ++q) {
-      float ms = 0.f;
-      if (cudaEventElapsedTime(&ms, a->ev[2 * q], a->ev[2 * q + 1]) != cudaSuccess) {
-        ms = -1.f;
-        (void)cudaGetLastError();
-      }
-      a->step_ms.push_back(ms);
-    }
-    it0 = it1;
-    if (a->h_ctrl->done) break;
-  }
+  const int cap_iters = cap > 0 ? (int)std::min<long long>(cap * kStepsPerGraph, 1 << 30) : 0;
+  k_loop_begin<<<1, 32, 0, s>>>(a->ctrl, a->cond[id], a->stamps, cap_iters);
+  GBO_CUDA_TRY(cudaGetLastError());
+  GBO_CUDA_TRY(cudaGraphLaunch(a->exec[id], s));
+  a->replays = 1;
+  a->stats_pending = true;
+  if (!iters && cap_iters == 0) return GBO_OK;
+  GBO_CUDA_TRY(cudaMemcpyAsync(a->h_ctrl, a->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
+  GBO_CUDA_TRY(cudaStreamSynchronize(s));
   if (!a->h_ctrl->done) return fail(GBO_ERR_TIMEOUT, "iteration loop did not terminate");
+  if (cap_iters > 0 && cap_iters < max_iter && a->h_ctrl->iter >= cap_iters)
+    return fail(GBO_ERR_TIMEOUT, "iteration loop cut off by the injected cap");
   if (iters) *iters = a->h_ctrl->iter;
+  return GBO_OK;
+}
+
+// Step times and counts of the last loop run, read back on first request.
+int collect_stats(AlgoState* a) {
+  if (!a->stats_pending) return GBO_OK;
+  a->stats_pending = false;
+  GBO_CUDA_TRY(cudaDeviceSynchronize());
+  GBO_CUDA_TRY(cudaMemcpy(a->h_ctrl, a->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+  const int it = a->h_ctrl->iter;
+  const int nst = std::min(it, kStampCap);
+  std::vector<unsigned long long> t((size_t)nst + 1);
+  GBO_CUDA_TRY(cudaMemcpy(t.data(), a->stamps, sizeof(unsigned long long) * t.size(), cudaMemcpyDeviceToHost));
+  a->step_ms.clear();
+  for (int q = 0; q < nst; ++q) a->step_ms.push_back((float)((double)(t[(size_t)q + 1] - t[(size_t)q]) * 1e-6));
+  a->launches = 2 + (long long)it * a->launches_per_iter;  // init and loop start kernels
   return GBO_OK;
 }
 
@@ -1376,8 +1503,6 @@ int bfs_impl(gbo_graph* g, int src, const int* h_seeds, int nseeds, int32_t* d_l
   const unsigned gs = blocks_for(std::max<long long>(g->nsplit, push_ok ? g->nbr : 0), kTPB);
   const unsigned gp = col ? grid_persistent(k_bfs_push_col<B>, g->nitems) : grid_persistent(k_bfs_push<B>, g->nitems);
   GBO_TRY(get_exec(a, A_BFS, nullptr, [&](cudaStream_t cs, int k, int* nl) -> int {
-    StepTimer tm{a, cs, k};
-    tm.begin();
     if (g->nitems > 0) {
       if (col) k_bfs_step_col<B><<<gi, kTPB, 0, cs>>>(v, front, vis, level, ctrl, scratch);
       else if (rws)
@@ -1389,7 +1514,6 @@ int bfs_impl(gbo_graph* g, int src, const int* h_seeds, int nseeds, int32_t* d_l
       if (col) k_bfs_push_col<B><<<gp, kTPB, 0, cs>>>(v, front, vis, ctrl);
       else k_bfs_push<B><<<gp, kTPB, 0, cs>>>(v, front, vis, ctrl);
     }
-    tm.end();
     k_bfs_finish<B><<<gs, kTPB, 0, cs>>>(vfin, front, vis, level, ctrl, scratch);
     *nl += (g->nitems > 0) + 1 + (push_ok ? (g->nitems > 0) : 0);
     GBO_CUDA_TRY(cudaGetLastError());
@@ -1415,7 +1539,9 @@ int bfs_impl(gbo_graph* g, int src, const int* h_seeds, int nseeds, int32_t* d_l
   }
   GBO_CUDA_TRY(cudaGetLastError());
   int iters = 0;
-  GBO_TRY(run_until_done(a, A_BFS, s, max_iter, &iters));
+  // without h_depth the call is asynchronous: the loop and the level copy
+  // are queued on s and the call returns
+  GBO_TRY(run_until_done(a, A_BFS, s, max_iter, h_depth ? &iters : nullptr));
   if (g->nrows > 0)
     GBO_CUDA_TRY(cudaMemcpyAsync(d_level, level, sizeof(int) * (size_t)g->nrows,
                                  cudaMemcpyDeviceToDevice, s));
@@ -1451,17 +1577,24 @@ int pr_impl(gbo_graph* g, const float* d_v, float alpha, int max_iter, float tol
   if (rws) v = view_of(g);
   GView vfin = v;
   if (rws) vfin.nsplit = 0;
+  if (rws) GBO_TRY(ensure_pr_part(g, a));
   const unsigned gi = rws ? grid_persistent(k_pr_step_rws, g->nbr)
                           : grid_items_persistent(k_pr_step<B>, g->nitems, B);
+  const unsigned gc = rws ? grid_persistent(k_pr_long_chunks, std::max<long long>(g->rws_nchunk, 1)) : 1;
   const unsigned gs = blocks_for((long long)vfin.nsplit * B, kTPB);
   GBO_TRY(get_exec(a, id, d_v, [&](cudaStream_t cs, int k, int* nl) -> int {
-    StepTimer tm{a, cs, k};
-    tm.begin();
     if (g->nitems > 0) {
-      if (rws) k_pr_step_rws<<<gi, kTPB, 0, cs>>>(v, pr, prs, inv, d_v, ctrl);
-      else k_pr_step<B><<<gi, kTPB, 0, cs>>>(v, pr, prs, inv, d_v, ctrl, scratch);
+      if (rws) {
+        k_pr_step_rws<<<gi, kTPB, 0, cs>>>(v, pr, prs, inv, d_v, ctrl);
+        if (g->rws_nchunk > 0) {
+          k_pr_long_chunks<<<gc, kTPB, 0, cs>>>(v, pr, prs, ctrl, a->pr_part);
+          k_pr_long_rows<<<blocks_for(g->rws_nlong, kTPB), kTPB, 0, cs>>>(v, pr, prs, inv, d_v, ctrl, a->pr_part);
+          *nl += 2;
+        }
+      } else {
+        k_pr_step<B><<<gi, kTPB, 0, cs>>>(v, pr, prs, inv, d_v, ctrl, scratch);
+      }
     }
-    tm.end();
     k_pr_finish<B><<<gs, kTPB, 0, cs>>>(vfin, pr, prs, inv, d_v, ctrl, scratch);
     *nl += (g->nitems > 0) + 1;
     GBO_CUDA_TRY(cudaGetLastError());
@@ -1501,17 +1634,24 @@ int ppr_backward_impl(gbo_graph* g, const float* d_w, float alpha, float tol, in
     GView v = view_of(g);
     GView vfin = v;
     if (rws) vfin.nsplit = 0;
+    if (rws) GBO_TRY(ensure_pr_part(g, a));
     const unsigned gi = rws ? grid_persistent(k_pr_step_rws, g->nbr)
                             : grid_items_persistent(k_pr_step<B>, g->nitems, B);
+    const unsigned gc = rws ? grid_persistent(k_pr_long_chunks, std::max<long long>(g->rws_nchunk, 1)) : 1;
     const unsigned gs = blocks_for((long long)vfin.nsplit * B, kTPB);
     GBO_TRY(get_exec(a, A_PPR_BG, d_w, [&](cudaStream_t cs, int k, int* nl) -> int {
-      StepTimer tm{a, cs, k};
-      tm.begin();
       if (g->nitems > 0) {
-        if (rws) k_pr_step_rws<<<gi, kTPB, 0, cs>>>(v, pr, prs, inv, d_w, ctrl);
-        else k_pr_step<B><<<gi, kTPB, 0, cs>>>(v, pr, prs, inv, d_w, ctrl, scratch);
+        if (rws) {
+          k_pr_step_rws<<<gi, kTPB, 0, cs>>>(v, pr, prs, inv, d_w, ctrl);
+          if (g->rws_nchunk > 0) {
+            k_pr_long_chunks<<<gc, kTPB, 0, cs>>>(v, pr, prs, ctrl, a->pr_part);
+            k_pr_long_rows<<<blocks_for(g->rws_nlong, kTPB), kTPB, 0, cs>>>(v, pr, prs, inv, d_w, ctrl, a->pr_part);
+            *nl += 2;
+          }
+        } else {
+          k_pr_step<B><<<gi, kTPB, 0, cs>>>(v, pr, prs, inv, d_w, ctrl, scratch);
+        }
       }
-      tm.end();
       k_pr_finish<B><<<gs, kTPB, 0, cs>>>(vfin, pr, prs, inv, d_w, ctrl, scratch);
       *nl += (g->nitems > 0) + 1;
       GBO_CUDA_TRY(cudaGetLastError());
@@ -1539,11 +1679,8 @@ int ppr_backward_impl(gbo_graph* g, const float* d_w, float alpha, float tol, in
   Ctrl* ctrl = a->ctrl;
   const unsigned gi = grid_items_persistent(k_adj_scatter<B>, g->nitems, B);
   GBO_TRY(get_exec(a, A_PPR_B, d_w, [&](cudaStream_t cs, int k, int* nl) -> int {
-    StepTimer tm{a, cs, k};
     k_adj_prep<<<gv, kTPB, 0, cs>>>(pr, d_w, n, ctrl, acc);
-    tm.begin();
     if (g->nitems > 0) k_adj_scatter<B><<<gi, kTPB, 0, cs>>>(v, pr, ctrl, acc);
-    tm.end();
     k_adj_apply<<<gv, kTPB, 0, cs>>>(pr, d_w, inv, n, ctrl, acc);
     *nl += (g->nitems > 0) + 2;
     GBO_CUDA_TRY(cudaGetLastError());
@@ -1577,10 +1714,7 @@ int cc_impl(gbo_graph* g, int32_t* d_label, int* h_iters, cudaStream_t s) {
   const unsigned gs = blocks_for((long long)g->nsplit * B, kTPB);
   const unsigned gv = grid_vertex(n);
   GBO_TRY(get_exec(a, A_CC, nullptr, [&](cudaStream_t cs, int k, int* nl) -> int {
-    StepTimer tm{a, cs, k};
-    tm.begin();
     if (g->nitems > 0) k_cc_mngf<B><<<gi, kTPB, 0, cs>>>(v, gf, mngf, ctrl, scratch);
-    tm.end();
     *nl += (g->nitems > 0) + (g->nsplit > 0) + 3;
     if (g->nsplit > 0) k_cc_mngf_finish<B><<<gs, kTPB, 0, cs>>>(v, mngf, ctrl, scratch);
     k_cc_hook<<<gv, kTPB, 0, cs>>>(f, mngf, n, ctrl);
@@ -1716,8 +1850,7 @@ void free_algo_state(gbo_graph* g) {
   if (!a) return;
   for (auto& e : a->exec)
     if (e) cudaGraphExecDestroy(e);
-  for (auto& e : a->ev)
-    if (e) cudaEventDestroy(e);
+  cudaFree(a->stamps);
   cudaFree(a->ctrl);
   cudaFreeHost(a->h_ctrl);
   cudaFree(a->front);
@@ -1731,6 +1864,7 @@ void free_algo_state(gbo_graph* g) {
   cudaFree(a->gf);
   cudaFree(a->mngf);
   cudaFree(a->acc64);
+  cudaFree(a->pr_part);
   cudaFree(a->seeds);
   cudaFree(a->scratch);
   if (a->cap) cudaStreamDestroy(a->cap);
@@ -1834,8 +1968,9 @@ extern "C" int gbo_graph_last_run(const gbo_graph* g, gbo_run_stats* stats) {
   if (!g || !stats) return fail(GBO_ERR_INVALID, "NULL argument");
   memset(stats, 0, sizeof(*stats));
   if (g->last_run_ms) return ms_last_run(g, stats);
-  const AlgoState* a = g->algo;
+  AlgoState* a = g->algo;
   if (!a) return GBO_OK;
+  GBO_TRY(collect_stats(a));
   stats->iterations = a->h_ctrl ? a->h_ctrl->iter : 0;
   stats->graph_replays = a->replays;
   stats->kernel_launches = a->launches;

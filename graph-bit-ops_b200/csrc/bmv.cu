@@ -511,6 +511,13 @@ GView view_of(const gbo_graph* g) {
   v.rws_head = g->rws_head;
   v.rws_tail = g->rws_tail;
   v.rws_tail_ptr = g->rws_tail_ptr;
+  v.rws_nlong = g->rws_nlong;
+  v.rws_nchunk = g->rws_nchunk;
+  v.rws_long_row = g->rws_long_row;
+  v.rws_long_chunk0 = g->rws_long_chunk0;
+  v.rws_chunk_row = g->rws_chunk_row;
+  v.rws_chunk_beg = g->rws_chunk_beg;
+  v.rws_chunk_end = g->rws_chunk_end;
   return v;
 }
 

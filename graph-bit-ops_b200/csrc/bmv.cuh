@@ -27,6 +27,13 @@ struct GView {
   const uint2* __restrict__ rws_head = nullptr;
   const uint2* __restrict__ rws_tail = nullptr;
   const long long* __restrict__ rws_tail_ptr = nullptr;
+  int rws_nlong = 0;
+  long long rws_nchunk = 0;
+  const int* __restrict__ rws_long_row = nullptr;
+  const long long* __restrict__ rws_long_chunk0 = nullptr;
+  const int* __restrict__ rws_chunk_row = nullptr;
+  const long long* __restrict__ rws_chunk_beg = nullptr;
+  const long long* __restrict__ rws_chunk_end = nullptr;
 };
 
 // Index in rowword of row r's word of a tile with occupancy word m whose

@@ -114,6 +114,11 @@ void destroy(gbo_graph* g) {
   cudaFree(g->rws_head);
   cudaFree(g->rws_tail);
   cudaFree(g->rws_tail_ptr);
+  cudaFree(g->rws_long_row);
+  cudaFree(g->rws_long_chunk0);
+  cudaFree(g->rws_chunk_row);
+  cudaFree(g->rws_chunk_beg);
+  cudaFree(g->rws_chunk_end);
   cudaFree(g->invdeg);
   cudaFree(g->items);
   cudaFree(g->splits);

@@ -41,6 +41,16 @@ struct gbo_graph {
   uint2* rws_head = nullptr;       // nbr * kRwsHead * 32 entries {block column, row word}
   uint2* rws_tail = nullptr;       // entries past the head, row after row
   long long* rws_tail_ptr = nullptr;  // nbr * 32 + 1 offsets into rws_tail
+  // rows whose tails are longer than kRwsLongTail, cut into chunks of at most
+  // kRwsChunk tail entries, for kernels that must read whole rows (PageRank):
+  // long row q owns chunks [rws_long_chunk0[q], rws_long_chunk0[q + 1])
+  int rws_nlong = 0;
+  long long rws_nchunk = 0;
+  int* rws_long_row = nullptr;         // rws_nlong rows
+  long long* rws_long_chunk0 = nullptr;  // rws_nlong + 1
+  int* rws_chunk_row = nullptr;        // row of every chunk
+  long long* rws_chunk_beg = nullptr;  // tail entries [beg, end) of every chunk
+  long long* rws_chunk_end = nullptr;
   int last_run_ms = 0;     // 1: the last traversal was a multi-source BFS
   bool tc_mma = false;     // GBO_FLAG_TC_MMA: dense 32x32 mask tiles on the 1-bit MMA
   bool owns_outdeg = true;
@@ -89,6 +99,10 @@ int build_rowwords(gbo_graph* g, cudaStream_t stream);
 // block column that marks a missing entry.
 constexpr int kRwsHead = 8;
 constexpr unsigned kRwsNone = 0xffffffffu;
+// Tails longer than this are walked by a whole warp (BFS) or cut into
+// chunks of kRwsChunk entries spread over warps (PageRank).
+constexpr int kRwsLongTail = 64;
+constexpr int kRwsChunk = 2048;
 // Row-word slices of a b = 32 ROW graph -> g->rws_* (no-op for other graphs
 // or when built).  Needs g->rowmask.
 int build_rws(gbo_graph* g, cudaStream_t stream);

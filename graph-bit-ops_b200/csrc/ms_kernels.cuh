@@ -56,6 +56,10 @@ struct Args {
   int dir = 0;
   long long push_thr = 0;
   uint32_t* push_acc = nullptr;
+  // row-word slice steps: the frontier rows gathered from the tails of long
+  // rows (rws_nlong x KW words, zero between levels; k_long_chunks ORs into
+  // them, k_step_rws reads them, a memset after the step clears them)
+  uint32_t* long_acc = nullptr;
 };
 
 // Address of the level of (vertex i, source s) in either layout.
@@ -325,6 +329,215 @@ __global__ void __launch_bounds__(kTPB, KW <= 2 ? 6 : 4) k_step(Args a) {
   }
   // block count without a closing barrier: warps add and leave; the last
   // warp of the block to arrive adds the block's count to the level total
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  if (lane == 0) {
+    if (cnt) atomicAdd(&cnt_sh, cnt);
+    __threadfence_block();
+    if (atomicAdd(&arrived_sh, 1) == kWarps - 1) {
+      __threadfence_block();
+      const unsigned long long tot = atomicAdd(&cnt_sh, 0ull);
+      if (tot) atomicAdd(reinterpret_cast<unsigned long long*>(a.ctl + 4), tot);
+    }
+  }
+}
+
+// Pull step over the row-word slices of a 32x32 ROW graph, k <= 64 (KW <= 2
+// words per frontier row): a warp per block row and lane r on row r.  The
+// lane walks the row's entries {block column, row word} in ascending block
+// column (head entry-major, two per round, then the tail; the tails of
+// rows longer than kMsLongTail come from k_long_chunks), keeps the
+// bits of each word whose vertex has a non-empty frontier row (fbits) and
+// ORs those frontier rows in registers; the row leaves once every active
+// source has reached it (seen | gathered covers them) or its entries run
+// out.  The gathered rows go through the same block-row epilogue as k_step.
+constexpr int kMsLongTail = kRwsLongTail;  // the slices' long-row chunking
+
+template <int KW>
+__device__ __forceinline__ void or_rows(const uint32_t* __restrict__ F, unsigned col_base, uint32_t m,
+                                        uint32_t& f0, uint32_t& f1) {
+  while (m) {
+    uint2 g[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      g[u] = make_uint2(0u, 0u);
+      if (m) {
+        const int col = __clz(m);
+        m &= ~(0x80000000u >> col);
+        const size_t fo = (size_t)(col_base + col) * KW;
+        if (KW == 1) g[u].x = __ldg(F + fo);
+        else g[u] = __ldg(reinterpret_cast<const uint2*>(F + fo));
+      }
+    }
+    f0 |= g[0].x | g[1].x;
+    f1 |= g[0].y | g[1].y;
+  }
+}
+
+// Four entries at once: their block columns' frontier bits gathered
+// together, then their frontier rows one set bit per entry per round, the
+// four gathers of a round in flight together.
+template <int KW>
+__device__ __forceinline__ void or_entries4(const uint32_t* __restrict__ F, const uint32_t* __restrict__ fb,
+                                            const uint2 (&e)[4], uint32_t& f0, uint32_t& f1) {
+  uint32_t m[4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) m[u] = e[u].x != kRwsNone ? e[u].y & __ldg(fb + e[u].x) : 0u;
+  while (m[0] | m[1] | m[2] | m[3]) {
+    uint2 g[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      g[u] = make_uint2(0u, 0u);
+      if (m[u]) {
+        const int col = __clz(m[u]);
+        m[u] &= ~(0x80000000u >> col);
+        const size_t fo = ((size_t)e[u].x * 32 + col) * KW;
+        if (KW == 1) g[u].x = __ldg(F + fo);
+        else g[u] = __ldg(reinterpret_cast<const uint2*>(F + fo));
+      }
+    }
+    f0 |= g[0].x | g[1].x | g[2].x | g[3].x;
+    f1 |= g[0].y | g[1].y | g[2].y | g[3].y;
+  }
+}
+
+// Tails of long rows (more than kMsLongTail entries), a warp per chunk of
+// kRwsChunk entries: the frontier rows of the chunk's frontier neighbours
+// OR-ed into the row's long_acc words, the chunk left early once the row is
+// covered.  Runs before k_step_rws in every pull level.
+template <int KW>
+__global__ void __launch_bounds__(kTPB) k_long_chunks(Args a) {
+  volatile int* c = a.ctl;
+  if (c[1]) return;
+  if (a.dir && (c[7] || c[6] == 1)) return;
+  const int lvl = c[0];
+  const GView& v = a.v;
+  const uint32_t* __restrict__ F = a.F + (size_t)(lvl & 1) * a.fstride;
+  const uint32_t* __restrict__ fb = a.fbits + (size_t)(lvl & 1) * (v.nbr + 1);
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned kFull = 0xffffffffu;
+  const uint32_t need0 = src_mask(0, a.k) & (a.active ? a.active[0] : kFull);
+  const uint32_t need1 = KW == 2 ? src_mask(1, a.k) & (a.active ? a.active[1] : kFull) : 0u;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long q = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < v.rws_nchunk; q += nwarps) {
+    const long long i = v.rws_chunk_row[q];
+    if ((a.vfull[i >> 5] >> (31 - (i & 31))) & 1u) continue;  // row finished
+    const uint32_t s0 = a.V[(size_t)i * KW], s1 = KW == 2 ? a.V[(size_t)i * KW + 1] : 0u;
+    if ((s0 & need0) == need0 && (s1 & need1) == need1) continue;
+    const long long b = v.rws_chunk_beg[q], e = v.rws_chunk_end[q];
+    uint32_t g0 = 0u, g1 = 0u;
+    for (long long p = b; p < e; p += 128) {
+      uint2 t[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const long long pp = p + lane + 32 * u;
+        t[u] = pp < e ? v.rws_tail[pp] : make_uint2(kRwsNone, 0u);
+      }
+      or_entries4<KW>(F, fb, t, g0, g1);
+      const uint32_t r0 = __reduce_or_sync(kFull, g0), r1 = __reduce_or_sync(kFull, g1);
+      if (((s0 | r0) & need0) == need0 && ((s1 | r1) & need1) == need1) break;
+    }
+    g0 = __reduce_or_sync(kFull, g0);
+    g1 = __reduce_or_sync(kFull, g1);
+    if (lane == 0) {
+      int lo = 0, hi = v.rws_nlong;  // the row's index among the long rows
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (v.rws_long_row[mid] <= i) lo = mid;
+        else hi = mid;
+      }
+      if (g0) atomicOr(a.long_acc + (size_t)lo * KW, g0);
+      if (KW == 2 && g1) atomicOr(a.long_acc + (size_t)lo * KW + 1, g1);
+    }
+  }
+}
+
+template <int KW>
+__global__ void __launch_bounds__(kTPB, 6) k_step_rws(Args a) {
+  static_assert(KW <= 2, "one lane per row holds the row's frontier words in registers");
+  __shared__ uint32_t acc_sh[kWarps][32 * KW];
+  __shared__ unsigned long long cnt_sh;
+  __shared__ int arrived_sh;
+  volatile int* c = a.ctl;
+  if (c[1]) return;
+  if (a.dir && (c[7] || c[6] == 1)) return;  // this slot's level ran as a push
+  if (threadIdx.x == 0) {
+    cnt_sh = 0ull;
+    arrived_sh = 0;
+  }
+  __syncthreads();
+  const int lvl = c[0];
+  const GView& v = a.v;
+  const uint32_t* __restrict__ F = a.F + (size_t)(lvl & 1) * a.fstride;
+  const uint32_t* __restrict__ fb = a.fbits + (size_t)(lvl & 1) * (v.nbr + 1);
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned kFull = 0xffffffffu;
+  uint32_t* acc = acc_sh[threadIdx.x >> 5];
+  const long long R = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  unsigned long long cnt = 0;
+  if (R < v.nbr) {
+    const uint32_t vrow = a.vfull[R];
+    if (vrow != kFull) {
+      const long long i = R * 32 + lane;
+      const uint32_t need0 = src_mask(0, a.k) & (a.active ? a.active[0] : kFull);
+      const uint32_t need1 = KW == 2 ? src_mask(1, a.k) & (a.active ? a.active[1] : kFull) : 0u;
+      bool go = !((vrow >> (31 - lane)) & 1u);
+      uint32_t s0 = 0u, s1 = 0u;  // seen (visited) words of the row
+      if (go) {
+        s0 = a.V[(size_t)i * KW];
+        if (KW == 2) s1 = a.V[(size_t)i * KW + 1];
+      }
+      uint32_t f0 = 0u, f1 = 0u;  // OR of the neighbours' frontier rows
+      auto covered = [&]() { return ((s0 | f0) & need0) == need0 && ((s1 | f1) & need1) == need1; };
+      go = go && !covered();
+      const uint2* __restrict__ hp = v.rws_head + (size_t)R * (kRwsHead * 32) + lane;
+#pragma unroll
+      for (int k = 0; k < kRwsHead; k += 4) {
+        if (!__any_sync(kFull, go)) break;
+        uint2 e[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) e[u] = go ? hp[(size_t)(k + u) * 32] : make_uint2(kRwsNone, 0u);
+        or_entries4<KW>(F, fb, e, f0, f1);
+        go = go && e[3].x != kRwsNone && !covered();
+      }
+      if (__any_sync(kFull, go)) {
+        long long tb = 0, te = 0;
+        if (go) {
+          tb = v.rws_tail_ptr[i];
+          te = v.rws_tail_ptr[i + 1];
+        }
+        go = go && te > tb;
+        if (go && te - tb > kMsLongTail) {
+          // a long row: k_long_chunks gathered its tail over many warps
+          int lo = 0, hi = v.rws_nlong;  // its index among the long rows
+          while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (v.rws_long_row[mid] <= i) lo = mid;
+            else hi = mid;
+          }
+          const uint32_t* la = a.long_acc + (size_t)lo * KW;
+          f0 |= la[0];
+          if (KW == 2) f1 |= la[1];
+          go = false;
+        }
+        for (long long p = tb; __any_sync(kFull, go); p += 4) {
+          if (go) {
+            uint2 e[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) e[u] = p + u < te ? v.rws_tail[p + u] : make_uint2(kRwsNone, 0u);
+            or_entries4<KW>(F, fb, e, f0, f1);
+            go = p + 4 < te && !covered();
+          }
+        }
+      }
+      acc[lane * KW] = f0;
+      if (KW == 2) acc[lane * KW + 1] = f1;
+      __syncwarp();
+      block_row_epilogue<KW>(a, (int)R, lvl, vrow, lane, [&](int r, int ww) { return acc[r * KW + ww]; }, cnt);
+    } else if (lane == 0) {
+      a.fbits[(size_t)((lvl + 1) & 1) * (v.nbr + 1) + R] = 0u;
+    }
+  }
+  // block count without a closing barrier (as k_step)
   for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
   if (lane == 0) {
     if (cnt) atomicAdd(&cnt_sh, cnt);

@@ -29,6 +29,7 @@ struct MsState {
   uint32_t* split_acc = nullptr;
   int* slot_split = nullptr;
   uint32_t* push_acc = nullptr;  // nbr * 32 * kw (push levels; k <= 64 on symmetric graphs)
+  uint32_t* long_acc = nullptr;  // rws_nlong * kw (slice steps, k <= 64)
   int* srcs = nullptr;
   int* ctl = nullptr;
   int* h_ctl = nullptr;
@@ -74,14 +75,21 @@ ms::Args make_args(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
   a.push_thr = ms_push_threshold(g, m.kw);
   a.dir = a.push_thr > 0 ? 1 : 0;
   a.push_acc = a.dir ? m.push_acc : nullptr;
+  a.long_acc = m.long_acc;
   return a;
 }
 
 template <int KW>
 int ms_capture(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
   const ms::Args a = make_args(g, m, d_levels, k);
-  const unsigned gi = blocks_for_warps(g->nitems, ms::kWarps);
-  const unsigned gs = blocks_for_warps(g->nsplit > 0 ? g->nsplit : 1, ms::kWarps);
+  // k <= 64 on a graph with row-word slices: the pull step walks rows
+  // (k_step_rws, whole block rows: no split partials for the finish kernel)
+  const bool rws = KW <= 2 && g->rws_head != nullptr;
+  ms::Args af = a;
+  if (rws) af.v.nsplit = 0;
+  const unsigned gi = rws ? blocks_for_warps(g->nbr > 0 ? g->nbr : 1, ms::kWarps)
+                          : blocks_for_warps(g->nitems, ms::kWarps);
+  const unsigned gs = blocks_for_warps(af.v.nsplit > 0 ? af.v.nsplit : 1, ms::kWarps);
   cudaGraph_t graph = nullptr;
   // with push levels a slot is push, push-finish, pull, finish (each
   // level runs in one of the two halves) and its events bracket all four
@@ -95,10 +103,22 @@ int ms_capture(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
         ms::k_push_fin<KW><<<gr, ms::kTPB, 0, m.cap>>>(a);
       }
     }
-    if (g->nitems > 0) ms::k_step<KW><<<gi, ms::kTPB, 0, m.cap>>>(a);
-    if (a.dir) ms::k_finish<KW><<<gs, ms::kTPB, 0, m.cap>>>(a);
+    if (g->nitems > 0) {
+      if constexpr (KW <= 2) {
+        if (rws && g->rws_nchunk > 0)
+          ms::k_long_chunks<KW><<<blocks_for_warps(std::min<long long>(g->rws_nchunk, 1 << 20), ms::kWarps),
+                                  ms::kTPB, 0, m.cap>>>(a);
+        if (rws) ms::k_step_rws<KW><<<gi, ms::kTPB, 0, m.cap>>>(a);
+        else ms::k_step<KW><<<gi, ms::kTPB, 0, m.cap>>>(a);
+        if (rws && g->rws_nchunk > 0)
+          cudaMemsetAsync(m.long_acc, 0, sizeof(uint32_t) * (size_t)g->rws_nlong * KW, m.cap);
+      } else {
+        ms::k_step<KW><<<gi, ms::kTPB, 0, m.cap>>>(a);
+      }
+    }
+    if (a.dir) ms::k_finish<KW><<<gs, ms::kTPB, 0, m.cap>>>(af);
     cudaEventRecordWithFlags(m.ev[2 * q + 1], m.cap, cudaEventRecordExternal);
-    if (!a.dir) ms::k_finish<KW><<<gs, ms::kTPB, 0, m.cap>>>(a);
+    if (!a.dir) ms::k_finish<KW><<<gs, ms::kTPB, 0, m.cap>>>(af);
   }
   cudaError_t e = cudaStreamEndCapture(m.cap, &graph);
   if (e != cudaSuccess) return fail_cuda(e, "multi-source BFS capture");
@@ -130,6 +150,14 @@ int msbfs_impl(gbo_graph* g, const int* h_srcs, int k, int32_t* d_levels, int* h
     const void* lv = nullptr;
     GBO_TRY(live_rows(g, s, &lv));
     m.live = static_cast<const uint32_t*>(lv);
+  }
+  if (k <= 64) {
+    GBO_TRY(build_rws(g, s));
+    const size_t lw = (size_t)(g->rws_nlong > 0 ? g->rws_nlong : 1) * 2;
+    if (!m.long_acc && g->rws_head) {
+      GBO_CUDA_TRY(cudaMalloc(&m.long_acc, sizeof(uint32_t) * lw));
+      GBO_CUDA_TRY(cudaMemsetAsync(m.long_acc, 0, sizeof(uint32_t) * lw, s));
+    }
   }
   if (kw != m.kw) {  // state sized for exactly kw words per vertex
     if (m.exec) cudaGraphExecDestroy(m.exec);
@@ -268,6 +296,7 @@ void free_ms_state(gbo_graph* g) {
   cudaFree(m->split_acc);
   cudaFree(m->slot_split);
   cudaFree(m->push_acc);
+  cudaFree(m->long_acc);
   cudaFree(m->srcs);
   cudaFree(m->ctl);
   cudaFreeHost(m->h_ctl);

@@ -11,6 +11,7 @@
 // entries in block column m into its tile row word, and the group emits one
 // tile.  A count pass sizes each block row; a scan gives bsrRowPtr; a fill
 // pass writes bsrColInd and the tile words (one coalesced store of b words).
+#include <vector>
 #include <algorithm>
 #include "graph.cuh"
 
@@ -796,6 +797,38 @@ int build_rws(gbo_graph* g, cudaStream_t s) {
   k_rws_fill<<<grid, 256, 0, s>>>(g->rowptr, g->colind, g->nbr, static_cast<const unsigned*>(g->val),
                                   g->rws_tail_ptr, g->rws_head, g->rws_tail);
   GBO_CUDA_TRY(cudaGetLastError());
+  // long tails cut into chunks (a host pass over the tail offsets, once)
+  std::vector<long long> tp((size_t)rows + 1);
+  GBO_CUDA_TRY(cudaMemcpyAsync(tp.data(), g->rws_tail_ptr, sizeof(long long) * tp.size(), cudaMemcpyDeviceToHost, s));
+  GBO_CUDA_TRY(cudaStreamSynchronize(s));
+  std::vector<int> lrow, crow;
+  std::vector<long long> lc0, cbeg, cend;
+  for (long long i = 0; i < rows; ++i) {
+    const long long len = tp[(size_t)i + 1] - tp[(size_t)i];
+    if (len <= kRwsLongTail) continue;
+    lrow.push_back((int)i);
+    lc0.push_back((long long)cbeg.size());
+    for (long long b = tp[(size_t)i]; b < tp[(size_t)i + 1]; b += kRwsChunk) {
+      crow.push_back((int)i);
+      cbeg.push_back(b);
+      cend.push_back(std::min(b + kRwsChunk, tp[(size_t)i + 1]));
+    }
+  }
+  lc0.push_back((long long)cbeg.size());
+  g->rws_nlong = (int)lrow.size();
+  g->rws_nchunk = (long long)cbeg.size();
+  auto up = [&](auto** dst, const auto& src) -> int {
+    const size_t nb = sizeof(src[0]) * (src.empty() ? 1 : src.size());
+    GBO_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(dst), nb));
+    g->device_bytes += (long long)nb;
+    if (!src.empty()) GBO_CUDA_TRY(cudaMemcpy(*dst, src.data(), nb, cudaMemcpyHostToDevice));
+    return GBO_OK;
+  };
+  GBO_TRY(up(&g->rws_long_row, lrow));
+  GBO_TRY(up(&g->rws_long_chunk0, lc0));
+  GBO_TRY(up(&g->rws_chunk_row, crow));
+  GBO_TRY(up(&g->rws_chunk_beg, cbeg));
+  GBO_TRY(up(&g->rws_chunk_end, cend));
   return GBO_OK;
 }
 

@@ -395,6 +395,7 @@ struct gbo_server {
   gbo_graph* g = nullptr;
   int n = 0, nbr = 0;
   long long max_pending = 0;  // per engine; 0 = unbounded (gbo_server_set_queue_limit)
+  uint32_t* long_acc = nullptr;  // up to 64 slots: long-row tail gathers (ms::Args::long_acc)
   float alpha = 0.85f, tol = 1e-7f;
   int ppr_max_iter = 1000;
   // one worker thread per engine (0 BFS, 1 PPR), each with its own stream,
@@ -474,6 +475,7 @@ ms::Args bfs_args(gbo_server* S) {
   a.live = S->live;
   a.active = S->d_active;
   a.level_group = 8;
+  a.long_acc = S->long_acc;
   return a;
 }
 
@@ -506,10 +508,30 @@ int bfs_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
   GBO_CUDA_TRY(cudaMemcpyAsync(S->ctl, h, sizeof(h), cudaMemcpyHostToDevice, st));
   GBO_CUDA_TRY(cudaMemsetAsync(S->ctl + 4, 0, 8, st));
   GBO_CUDA_TRY(cudaMemsetAsync(S->slot_any, 0, sizeof(uint32_t) * S->kw, st));
-  const unsigned gi = blocks_for_warps(S->g->nitems, ms::kWarps);
-  const unsigned gs = blocks_for_warps(S->g->nsplit > 0 ? S->g->nsplit : 1, ms::kWarps);
-  if (S->g->nitems > 0) ms::k_step<KW><<<gi, ms::kTPB, 0, st>>>(a);
-  ms::k_finish<KW><<<gs, ms::kTPB, 0, st>>>(a);
+  // up to 64 slots with row-word slices: the row-walking step (whole block
+  // rows, so no split partials for the finish kernel)
+  const bool rws = KW <= 2 && S->g->rws_head != nullptr;
+  ms::Args af = a;
+  if (rws) af.v.nsplit = 0;
+  const unsigned gi = rws ? blocks_for_warps(S->nbr > 0 ? S->nbr : 1, ms::kWarps)
+                          : blocks_for_warps(S->g->nitems, ms::kWarps);
+  const unsigned gs = blocks_for_warps(af.v.nsplit > 0 ? af.v.nsplit : 1, ms::kWarps);
+  if (S->g->nitems > 0) {
+    if constexpr (KW <= 2) {
+      if (rws && S->g->rws_nchunk > 0) {
+        ms::k_long_chunks<KW><<<blocks_for_warps(std::min<long long>(S->g->rws_nchunk, 1 << 20), ms::kWarps),
+                                ms::kTPB, 0, st>>>(a);
+        S->launches++;
+      }
+      if (rws) ms::k_step_rws<KW><<<gi, ms::kTPB, 0, st>>>(a);
+      else ms::k_step<KW><<<gi, ms::kTPB, 0, st>>>(a);
+      if (rws && S->g->rws_nchunk > 0)
+        GBO_CUDA_TRY(cudaMemsetAsync(S->long_acc, 0, sizeof(uint32_t) * (size_t)S->g->rws_nlong * KW, st));
+    } else {
+      ms::k_step<KW><<<gi, ms::kTPB, 0, st>>>(a);
+    }
+  }
+  ms::k_finish<KW><<<gs, ms::kTPB, 0, st>>>(af);
   S->launches += 2;
   GBO_CUDA_TRY(cudaGetLastError());
   GBO_CUDA_TRY(cudaMemcpyAsync(S->h_slot_any, S->slot_any, sizeof(uint32_t) * S->kw, cudaMemcpyDeviceToHost, st));
@@ -840,6 +862,7 @@ void destroy_server(gbo_server* S) {
   cudaFree(S->levels);
   cudaFree(S->ctl);
   cudaFree(S->slot_any);
+  cudaFree(S->long_acc);
   cudaFreeHost(S->h_slot_any);
   cudaFree(S->d_active);
   cudaFree(S->d_adm_src);
@@ -922,6 +945,13 @@ extern "C" int gbo_server_create(const gbo_graph* gc, int bfs_slots, int ppr_slo
         const int st = live_rows(g, S->s[0], &lv);
         if (st != GBO_OK) throw st;
         S->live = static_cast<const uint32_t*>(lv);
+      }
+      if (kw <= 2) {  // up to 64 slots: rounds walk the row-word slices
+        const int st = build_rws(g, S->s[0]);
+        if (st != GBO_OK) throw st;
+        const size_t lw = (size_t)(g->rws_nlong > 0 ? g->rws_nlong : 1) * (size_t)kw;
+        cu(cudaMalloc(&S->long_acc, sizeof(uint32_t) * lw), "long_acc");
+        cu(cudaMemsetAsync(S->long_acc, 0, sizeof(uint32_t) * lw, S->s[0]), "long_acc");
       }
       ms::Args a = bfs_args(S);
       unsigned gv = blocks_for((long long)n * S->kb, 256);

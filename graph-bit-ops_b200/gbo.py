@@ -608,10 +608,16 @@ class Graph:
               "bmv_float_transposed")
 
     # ---- algorithms (numpy in / numpy out helpers)
-    def bfs(self, src: int, out: DeviceBuffer | None = None, stream=None):
+    def bfs(self, src: int, out: DeviceBuffer | None = None, stream=None, wait=True):
+        """BFS levels from `src`: (levels, depth), or the depth when `out` is
+        given.  wait=False (with `out`) queues the traversal and returns None
+        at once (gbo_bfs with h_depth NULL)."""
         n = self.info().nrows
         buf = out or DeviceBuffer(4 * n)
         depth = C.c_int(0)
+        if not wait and out is not None:
+            check(lib().gbo_bfs(self.h, src, buf.ptr, None, stream), "bfs")
+            return None
         check(lib().gbo_bfs(self.h, src, buf.ptr, C.byref(depth), stream), "bfs")
         if out is not None:
             return depth.value

@@ -301,7 +301,10 @@ GBO_API int gbo_bmv_float_transposed(const gbo_graph* g, const float* d_x, float
 /* Level-synchronous pull BFS on P from src: level[i] = hops, -1 unreachable.
  * Rewrites algorithm/bfs.cu:508-564 with all state on the device and
  * termination decided on the device (no per-level host copy).
- * h_depth (nullable) receives the number of levels (max level + 1).
+ * h_depth (nullable) receives the number of levels (max level + 1); the
+ * call then waits for the traversal.  With h_depth NULL it is asynchronous:
+ * the whole level loop runs on the device (one CUDA graph with a device-side
+ * loop) and the call returns once it is queued on `stream`.
  * Takes ROW- and COL-layout graphs (the other algorithms need ROW): with
  * column words a pull step reads, per tile, only the words of the
  * frontier's columns, which pays off where frontier segments are sparse in
