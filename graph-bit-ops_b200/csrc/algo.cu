@@ -945,14 +945,16 @@ __global__ void __launch_bounds__(kTPB) k_pr_step_rws(GView v, float* __restrict
       tb = v.rws_tail_ptr[row];
       te = v.rws_tail_ptr[row + 1];
     }
-    if (te - tb > kRwsLongTail) continue;  // a long row: the chunk kernels own it
-    for (long long p = tb; p < te; p += 4) {
-      uint2 e[4];
+    const bool long_row = te - tb > kRwsLongTail;  // the chunk kernels own a long row
+    if (!long_row) {
+      for (long long p = tb; p < te; p += 4) {
+        uint2 e[4];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) e[u] = p + u < te ? v.rws_tail[p + u] : make_uint2(kRwsNone, 0u);
-      a += pr_entries4(e, P.xg);
+        for (int u = 0; u < 4; ++u) e[u] = p + u < te ? v.rws_tail[p + u] : make_uint2(kRwsNone, 0u);
+        a += pr_entries4(e, P.xg);
+      }
     }
-    if (row < n)
+    if (row < n && !long_row)
       e += pr_row_update(row, a, P.x, P.y, P.ys, inv, pv, P.alpha, P.add, P.adds, P.norm, P.row_scale);
   }
   block_add_f64(e, &ctrl->err);

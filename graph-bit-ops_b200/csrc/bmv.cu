@@ -513,6 +513,7 @@ GView view_of(const gbo_graph* g) {
   v.rws_tail_ptr = g->rws_tail_ptr;
   v.rws_nlong = g->rws_nlong;
   v.rws_nchunk = g->rws_nchunk;
+  v.rws_ntail = g->rws_ntail;
   v.rws_long_row = g->rws_long_row;
   v.rws_long_chunk0 = g->rws_long_chunk0;
   v.rws_chunk_row = g->rws_chunk_row;

@@ -29,6 +29,7 @@ struct GView {
   const long long* __restrict__ rws_tail_ptr = nullptr;
   int rws_nlong = 0;
   long long rws_nchunk = 0;
+  long long rws_ntail = 0;
   const int* __restrict__ rws_long_row = nullptr;
   const long long* __restrict__ rws_long_chunk0 = nullptr;
   const int* __restrict__ rws_chunk_row = nullptr;

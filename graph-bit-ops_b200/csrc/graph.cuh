@@ -46,6 +46,7 @@ struct gbo_graph {
   // long row q owns chunks [rws_long_chunk0[q], rws_long_chunk0[q + 1])
   int rws_nlong = 0;
   long long rws_nchunk = 0;
+  long long rws_ntail = 0;  // entries in rws_tail
   int* rws_long_row = nullptr;         // rws_nlong rows
   long long* rws_long_chunk0 = nullptr;  // rws_nlong + 1
   int* rws_chunk_row = nullptr;        // row of every chunk

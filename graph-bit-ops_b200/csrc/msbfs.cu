@@ -84,7 +84,7 @@ int ms_capture(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
   const ms::Args a = make_args(g, m, d_levels, k);
   // k <= 64 on a graph with row-word slices: the pull step walks rows
   // (k_step_rws, whole block rows: no split partials for the finish kernel)
-  const bool rws = KW <= 2 && g->rws_head != nullptr;
+  const bool rws = g->rws_head != nullptr;
   ms::Args af = a;
   if (rws) af.v.nsplit = 0;
   const unsigned gi = rws ? blocks_for_warps(g->nbr > 0 ? g->nbr : 1, ms::kWarps)
@@ -113,7 +113,13 @@ int ms_capture(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
         if (rws && g->rws_nchunk > 0)
           cudaMemsetAsync(m.long_acc, 0, sizeof(uint32_t) * (size_t)g->rws_nlong * KW, m.cap);
       } else {
-        ms::k_step<KW><<<gi, ms::kTPB, 0, m.cap>>>(a);
+        if (rws && g->rws_nchunk > 0)
+          ms::k_long_chunks_wide<KW><<<blocks_for_warps(std::min<long long>(g->rws_nchunk, 1 << 20), ms::kWarps),
+                                       ms::kTPB, 0, m.cap>>>(a);
+        if (rws) ms::k_step_rws_wide<KW><<<gi, ms::kTPB, 0, m.cap>>>(a);
+        else ms::k_step<KW><<<gi, ms::kTPB, 0, m.cap>>>(a);
+        if (rws && g->rws_nchunk > 0)
+          cudaMemsetAsync(m.long_acc, 0, sizeof(uint32_t) * (size_t)g->rws_nlong * KW, m.cap);
       }
     }
     if (a.dir) ms::k_finish<KW><<<gs, ms::kTPB, 0, m.cap>>>(af);
@@ -151,13 +157,11 @@ int msbfs_impl(gbo_graph* g, const int* h_srcs, int k, int32_t* d_levels, int* h
     GBO_TRY(live_rows(g, s, &lv));
     m.live = static_cast<const uint32_t*>(lv);
   }
-  if (k <= 64) {
-    GBO_TRY(build_rws(g, s));
-    const size_t lw = (size_t)(g->rws_nlong > 0 ? g->rws_nlong : 1) * 2;
-    if (!m.long_acc && g->rws_head) {
-      GBO_CUDA_TRY(cudaMalloc(&m.long_acc, sizeof(uint32_t) * lw));
-      GBO_CUDA_TRY(cudaMemsetAsync(m.long_acc, 0, sizeof(uint32_t) * lw, s));
-    }
+  GBO_TRY(build_rws(g, s));
+  if (!m.long_acc && g->rws_head) {  // sized for the widest frontier rows (32 words)
+    const size_t lw = (size_t)(g->rws_nlong > 0 ? g->rws_nlong : 1) * 32;
+    GBO_CUDA_TRY(cudaMalloc(&m.long_acc, sizeof(uint32_t) * lw));
+    GBO_CUDA_TRY(cudaMemsetAsync(m.long_acc, 0, sizeof(uint32_t) * lw, s));
   }
   if (kw != m.kw) {  // state sized for exactly kw words per vertex
     if (m.exec) cudaGraphExecDestroy(m.exec);
@@ -232,6 +236,9 @@ int msbfs_impl(gbo_graph* g, const int* h_srcs, int k, int32_t* d_levels, int* h
       m.step_ms.push_back(ms);
     }
     it0 = it1;
+    if (m.h_ctl[9])
+      return fail(GBO_ERR_BOUNDS, "multi-source step check " + std::to_string(m.h_ctl[9]) + " at index " +
+                                      std::to_string(m.h_ctl[10]));
     if (m.h_ctl[1]) {
       done = true;
       break;

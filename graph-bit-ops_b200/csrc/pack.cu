@@ -793,6 +793,7 @@ int build_rws(gbo_graph* g, cudaStream_t s) {
   cudaFreeAsync(len, s);
   cudaFreeAsync(tot, s);
   GBO_CUDA_TRY(cudaMalloc(&g->rws_tail, sizeof(uint2) * (size_t)(nt > 0 ? nt : 1)));
+  g->rws_ntail = nt;
   g->device_bytes += 8LL * (nt > 0 ? nt : 1);
   k_rws_fill<<<grid, 256, 0, s>>>(g->rowptr, g->colind, g->nbr, static_cast<const unsigned*>(g->val),
                                   g->rws_tail_ptr, g->rws_head, g->rws_tail);
