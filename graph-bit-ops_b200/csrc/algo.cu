@@ -304,14 +304,24 @@ __global__ void __launch_bounds__(kTPB) k_bfs_step(GView v, typename Word<B>::T*
 // visited (k_live), so every open row has an entry.
 constexpr int kLongTail = kRwsLongTail;
 
-__global__ void __launch_bounds__(kTPB, 6) k_bfs_pull_rws(GView v, unsigned* __restrict__ front,
-                                                       unsigned* __restrict__ visited,
-                                                       int* __restrict__ level, Ctrl* __restrict__ ctrl) {
-  if (((volatile Ctrl*)ctrl)->done || ((volatile Ctrl*)ctrl)->mode) return;
-  const int lvl = ((volatile Ctrl*)ctrl)->iter;
-  const unsigned* __restrict__ x = front_buf(front, v.nbr, lvl);
-  unsigned* __restrict__ out = front_buf(front, v.nbr, lvl + 1);
-  unsigned* __restrict__ z = front_buf(front, v.nbr, lvl + 2);
+// Loads of the traversal state (frontier and visited words): through the
+// read-only path when the state only changes between launches, through L2
+// (coherent across SMs) inside the persistent cooperative BFS kernel, where
+// other blocks rewrite it between levels.
+template <bool COH>
+__device__ __forceinline__ unsigned ld_state(const unsigned* p) {
+  if constexpr (COH) return __ldcg(p);
+  else return __ldg(p);
+}
+
+// One pull level over the row-word slices (see k_bfs_pull_rws); returns the
+// new vertices counted by this thread.
+template <bool COH>
+__device__ __forceinline__ unsigned long long pull_rws_level(const GView& v, unsigned* front, unsigned* visited,
+                                                             int* level, int lvl) {
+  const unsigned* x = front_buf(front, v.nbr, lvl);
+  unsigned* out = front_buf(front, v.nbr, lvl + 1);
+  unsigned* z = front_buf(front, v.nbr, lvl + 2);
   const unsigned lane = threadIdx.x & 31;
   const unsigned kFull = 0xffffffffu;
   const long long nwarps = warps_total();
@@ -323,7 +333,7 @@ __global__ void __launch_bounds__(kTPB, 6) k_bfs_pull_rws(GView v, unsigned* __r
     const long long Rl = base + (long long)lane * nwarps;
     unsigned visl = kFull;
     if (Rl < v.nbr) {
-      visl = visited[Rl];
+      visl = COH ? __ldcg(visited + Rl) : visited[Rl];
       z[Rl] = 0u;
     }
     unsigned openb = __ballot_sync(kFull, visl != kFull);
@@ -345,7 +355,7 @@ __global__ void __launch_bounds__(kTPB, 6) k_bfs_pull_rws(GView v, unsigned* __r
         for (int q = 0; q < 4; ++q) e[q] = need ? hp[(size_t)(k + q) * 32] : make_uint2(kRwsNone, 0u);
         unsigned a = 0u;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) a |= e[q].x != kRwsNone ? (e[q].y & __ldg(x + e[q].x)) : 0u;
+        for (int q = 0; q < 4; ++q) a |= e[q].x != kRwsNone ? (e[q].y & ld_state<COH>(x + e[q].x)) : 0u;
         hit = hit || (need && a != 0u);
         need = need && !hit && e[3].x != kRwsNone;
       }
@@ -366,7 +376,7 @@ __global__ void __launch_bounds__(kTPB, 6) k_bfs_pull_rws(GView v, unsigned* __r
             for (int q = 0; q < 4; ++q) e[q] = p + q < te ? v.rws_tail[p + q] : make_uint2(kRwsNone, 0u);
             unsigned a = 0u;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) a |= e[q].x != kRwsNone ? (e[q].y & __ldg(x + e[q].x)) : 0u;
+            for (int q = 0; q < 4; ++q) a |= e[q].x != kRwsNone ? (e[q].y & ld_state<COH>(x + e[q].x)) : 0u;
             hit = a != 0u;
             need = !hit && p + 4 < te;
           }
@@ -380,7 +390,7 @@ __global__ void __launch_bounds__(kTPB, 6) k_bfs_pull_rws(GView v, unsigned* __r
             bool h = false;
             if (p + lane < qe) {
               const uint2 e = v.rws_tail[p + lane];
-              h = (e.y & __ldg(x + e.x)) != 0u;
+              h = (e.y & ld_state<COH>(x + e.x)) != 0u;
             }
             qhit = __any_sync(kFull, h);
           }
@@ -398,6 +408,15 @@ __global__ void __launch_bounds__(kTPB, 6) k_bfs_pull_rws(GView v, unsigned* __r
       }
     }
   }
+  return cnt;
+}
+
+__global__ void __launch_bounds__(kTPB, 6) k_bfs_pull_rws(GView v, unsigned* __restrict__ front,
+                                                       unsigned* __restrict__ visited,
+                                                       int* __restrict__ level, Ctrl* __restrict__ ctrl) {
+  if (((volatile Ctrl*)ctrl)->done || ((volatile Ctrl*)ctrl)->mode) return;
+  const int lvl = ((volatile Ctrl*)ctrl)->iter;
+  const unsigned long long cnt = pull_rws_level<false>(v, front, visited, level, lvl);
   block_add_u64(cnt, &ctrl->count);
 }
 
