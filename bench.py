@@ -42,6 +42,9 @@ def parse():
                     help="tile layout of the BFS graph (COL: pull steps read only the frontier's column words)")
     ap.add_argument("--direction", default="auto", choices=["auto", "pull"],
                     help="auto: top-down steps while the frontier is small (graph is symmetric)")
+    ap.add_argument("--bfs-loop", default="auto", choices=["auto", "graph", "coop"],
+                    help="BFS level loop: loop graph of per-level kernels or one cooperative launch")
+    ap.add_argument("--coop-blocks", type=int, default=0, help="cooperative BFS grid (0: sized by the graph)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving streams")
     ap.add_argument("--no-permuted", action="store_true", help="skip the degree-ordered variant")
@@ -537,6 +540,8 @@ def run_ours(args, ws, rank, local):
         flags |= gbo.FLAG_LAYOUT_COL
     g = gbo.Graph.from_csr(csr, args.tile, flags)
     build_s = time.perf_counter() - t0
+    loops = {"auto": gbo.BFS_LOOP_AUTO, "graph": gbo.BFS_LOOP_GRAPH, "coop": gbo.BFS_LOOP_COOP}
+    g.set_bfs_loop(loops[args.bfs_loop], args.coop_blocks)
     info = g.info()
     n = csr.nrows
     d_level = gbo.DeviceBuffer(4 * n)
@@ -590,6 +595,27 @@ def run_ours(args, ws, rank, local):
     dist.barrier()
     e2e_ms = dist.max(ev0.elapsed_ms(ev1) / args.steps)
 
+    # the other level loop on the same BFS (b = 32 ROW graphs have both): the
+    # loop graph of per-level kernels beside the cooperative launch
+    other_loop = None
+    if args.tile == 32 and args.layout == "row":
+        cur = g.last_run()["kernel_launches"] == 3  # the cooperative form launches 3 kernels
+        g.set_bfs_loop(gbo.BFS_LOOP_GRAPH if cur else gbo.BFS_LOOP_COOP, args.coop_blocks)
+        for _ in range(3):
+            g.bfs(0, out=d_level)
+        gbo.sync()
+        ev0.record()
+        for _ in range(args.steps):
+            g.bfs(0, out=d_level, wait=False)
+        ev1.record()
+        gbo.sync()
+        oms = ev0.elapsed_ms(ev1) / args.steps
+        olv = g.bfs(0)[0]
+        other_loop = {"loop": "graph" if cur else "cooperative", "ms_per_bfs": oms,
+                      "gteps": edges / (oms / 1e3) / 1e9, "levels_equal": bool(np.array_equal(olv, levels)),
+                      "headline_loop": "cooperative" if cur else "graph"}
+        g.set_bfs_loop(loops[args.bfs_loop], args.coop_blocks)
+
     # pull-only runs of the same BFS (every level a bottom-up step): per-level
     # times beside the direction-optimising ones
     g.set_bfs_direction(False)
@@ -620,7 +646,9 @@ def run_ours(args, ws, rank, local):
                    if not (thr > 0 and 0 < sizes[L] < thr)]
         rl_bytes = [lvl_bytes[L] for L in pull_lv]
         rl_ms = [float(auto_lvl_ms[L]) for L in pull_lv]
-        kernel_name = "k_bfs_pull_rws (BFS pull step over row-word slices, pull levels of the timed runs)"
+        kernel_name = ("k_bfs_coop (cooperative BFS loop; its pull levels over row-word slices)"
+                       if other_loop and other_loop["headline_loop"] == "cooperative" else
+                       "k_bfs_pull_rws (BFS pull step over row-word slices, pull levels of the timed runs)")
         traffic = load_traffic("k_bfs_pull_rws_rmat20_ncu.md")
         traffic_note = "scaled from the R-MAT 20 ncu capture in profiles/ by algorithmic bytes"
     else:
@@ -752,6 +780,8 @@ def run_ours(args, ws, rank, local):
         "batched_bfs": dict(batched, plain_qps=1e3 / ms),
         "served": served,
         "direction": args.direction,
+        "bfs_loop": other_loop["headline_loop"] if other_loop else "graph",
+        "other_loop": other_loop,
         "levels_ms": [float(v) for v in auto_lvl_ms],
         "levels_gb": [b / 1e9 for b in lvl_bytes],
         "pull_only": {"ms_per_bfs": pull_ms, "gteps": edges / (pull_ms / 1e3) / 1e9,

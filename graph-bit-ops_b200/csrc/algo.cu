@@ -42,6 +42,13 @@ struct Ctrl {
   // and its iteration end times (globaltimer ns; [0] = loop start)
   unsigned long long cond;
   unsigned long long* stamps;
+  // cooperative BFS: grid barrier (arrivals, generation, give-up flag) and
+  // the new-vertex counts of three consecutive levels
+  unsigned bar_arrive;
+  unsigned bar_gen;
+  unsigned bar_err;
+  unsigned long long lvl_count[3];
+  unsigned long long push_acc[3];  // push list: rows << 40 | tail entries
 };
 
 // Iteration end times kept per loop run (more iterations run untimed).
@@ -71,12 +78,14 @@ struct AlgoState {
   int nseeds_cap = 0;
   double* acc64 = nullptr;  // PPR adjoint scatter accumulator
   double* pr_part = nullptr;  // row-word slices: one partial sum per long-row chunk
+  long long* push_list = nullptr;  // cooperative BFS: (start, tail offset) per listed long row
   void* scratch = nullptr;  // split partials (nslots * b * 8 bytes)
   cudaGraphExec_t exec[8] = {};
   const void* exec_key[8] = {};
   unsigned long long cond[8] = {};       // each loop graph's condition handle
   unsigned long long* stamps = nullptr;  // kStampCap + 1 iteration end times
   int launches_per_iter = 0;             // kernels of one loop iteration
+  int fixed_launches = 2;                // kernels of a run outside its iterations
   bool stats_pending = false;            // step times not yet read back
 
   // statistics of the last algorithm run
@@ -93,6 +102,10 @@ namespace {
 constexpr int kTPB = 256;
 // Iterations per unit of the injected loop cap (gbo_debug_inject).
 constexpr int kStepsPerGraph = 8;
+// GBO_BFS_LOOP_AUTO runs b = 32 ROW BFS as one cooperative launch of at
+// most this many blocks per SM.
+constexpr bool kCoopBfsDefault = true;
+constexpr int kCoopBlocksPerSM = 4;
 
 enum AlgoId { A_BFS = 0, A_SSSP = 1, A_PR = 2, A_CC = 3, A_PPR_F = 4, A_PPR_B = 5, A_PPR_BG = 6 };
 
@@ -305,12 +318,13 @@ __global__ void __launch_bounds__(kTPB) k_bfs_step(GView v, typename Word<B>::T*
 constexpr int kLongTail = kRwsLongTail;
 
 // Loads of the traversal state (frontier and visited words): through the
-// read-only path when the state only changes between launches, through L2
-// (coherent across SMs) inside the persistent cooperative BFS kernel, where
-// other blocks rewrite it between levels.
+// read-only path when the state only changes between launches; as plain
+// (weak, L1-cached) loads inside the cooperative BFS kernel, where other
+// blocks rewrite it between levels -- the grid barrier's fences order those
+// writes before the loads, which the read-only path does not promise.
 template <bool COH>
 __device__ __forceinline__ unsigned ld_state(const unsigned* p) {
-  if constexpr (COH) return __ldcg(p);
+  if constexpr (COH) return *p;
   else return __ldg(p);
 }
 
@@ -333,7 +347,7 @@ __device__ __forceinline__ unsigned long long pull_rws_level(const GView& v, uns
     const long long Rl = base + (long long)lane * nwarps;
     unsigned visl = kFull;
     if (Rl < v.nbr) {
-      visl = COH ? __ldcg(visited + Rl) : visited[Rl];
+      visl = visited[Rl];
       z[Rl] = 0u;
     }
     unsigned openb = __ballot_sync(kFull, visl != kFull);
@@ -466,15 +480,12 @@ __global__ void __launch_bounds__(kTPB) k_live(GView v, typename Word<B>::T* __r
 // frontier, minus vertices already visited.  One warp per work item, one
 // lane per tile; k_bfs_finish then keeps the unvisited bits.
 template <int B>
-__global__ void __launch_bounds__(kTPB) k_bfs_push(GView v, typename Word<B>::T* __restrict__ front,
-                                                   const typename Word<B>::T* __restrict__ visited,
-                                                   Ctrl* __restrict__ ctrl) {
+__device__ __forceinline__ void push_level(const GView& v, typename Word<B>::T* front,
+                                           const typename Word<B>::T* visited, int lvl) {
   using WT = typename Word<B>::T;
-  if (((volatile Ctrl*)ctrl)->done || !((volatile Ctrl*)ctrl)->mode) return;
-  const int lvl = ((volatile Ctrl*)ctrl)->iter;
-  const WT* __restrict__ x = front_buf(front, v.nbr, lvl);
+  const WT* x = front_buf(front, v.nbr, lvl);
   WT* out = front_buf(front, v.nbr, lvl + 1);
-  WT* __restrict__ z = front_buf(front, v.nbr, lvl + 2);
+  WT* z = front_buf(front, v.nbr, lvl + 2);
   const unsigned lane = threadIdx.x & 31;
   const WT* __restrict__ val = reinterpret_cast<const WT*>(v.val);
   const long long nwarps = warps_total();
@@ -537,6 +548,14 @@ __global__ void __launch_bounds__(kTPB) k_bfs_push(GView v, typename Word<B>::T*
       }
     }
   }
+}
+
+template <int B>
+__global__ void __launch_bounds__(kTPB) k_bfs_push(GView v, typename Word<B>::T* __restrict__ front,
+                                                   const typename Word<B>::T* __restrict__ visited,
+                                                   Ctrl* __restrict__ ctrl) {
+  if (((volatile Ctrl*)ctrl)->done || !((volatile Ctrl*)ctrl)->mode) return;
+  push_level<B>(v, front, visited, ((volatile Ctrl*)ctrl)->iter);
 }
 
 // ------------------------------------------------ COL tile layout (BFS)
@@ -696,6 +715,36 @@ __global__ void __launch_bounds__(kTPB) k_bfs_push_col(GView v, typename Word<B>
   }
 }
 
+// After a push step: keep the unvisited bits of every next-frontier word,
+// mark them visited and give their vertices level lvl + 1 (a thread per
+// block row, grid-stride); returns the new vertices counted by this thread.
+template <int B>
+__device__ __forceinline__ unsigned long long finish_push_rows(const GView& v, typename Word<B>::T* front,
+                                                               typename Word<B>::T* visited, int* level,
+                                                               int lvl) {
+  using WT = typename Word<B>::T;
+  WT* out = front_buf(front, v.nbr, lvl + 1);
+  const WT full = full_word<B>();
+  unsigned long long cnt = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < v.nbr;
+       i += (long long)gridDim.x * blockDim.x) {
+    const WT o = out[i];
+    if (!o) continue;
+    const WT vis = visited[i];
+    const WT nw = (WT)(o & ~vis & full);
+    out[i] = nw;
+    if (nw) {
+      visited[i] = (WT)(vis | nw);
+      for (int r = 0; r < B; ++r) {
+        const long long row = i * B + r;
+        if (bit_of<B>(nw, r) && row < v.nrows) level[row] = lvl + 1;
+      }
+      cnt += popc_w(nw);
+    }
+  }
+  return cnt;
+}
+
 template <int B>
 __global__ void k_bfs_finish(GView v, typename Word<B>::T* __restrict__ front,
                              typename Word<B>::T* __restrict__ visited, int* __restrict__ level,
@@ -708,21 +757,7 @@ __global__ void k_bfs_finish(GView v, typename Word<B>::T* __restrict__ front,
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long cnt = 0;
   if (push) {
-    // keep the unvisited bits of every next-frontier word
-    if (i < v.nbr) {
-      const WT full = full_word<B>();
-      const WT vis = visited[i];
-      const WT nw = (WT)(out[i] & ~vis & full);
-      out[i] = nw;
-      if (nw) {
-        visited[i] = (WT)(vis | nw);
-        for (int r = 0; r < B; ++r) {
-          const long long row = i * B + r;
-          if (bit_of<B>(nw, r) && row < v.nrows) level[row] = lvl + 1;
-        }
-        cnt = popc_w(nw);
-      }
-    }
+    cnt = finish_push_rows<B>(v, front, visited, level, lvl);
   } else if (i < v.nsplit) {
     const gbo_split sp = v.splits[i];
     const WT full = full_word<B>();
@@ -791,6 +826,227 @@ __global__ void k_bfs_init(typename Word<B>::T* front, typename Word<B>::T* visi
     ctrl->push_thr = push_thr;
     ctrl->mode = mode0;
     ctrl->work = 0ull;
+    ctrl->bar_arrive = 0u;
+    ctrl->bar_err = 0u;
+    for (int q = 0; q < 3; ++q) ctrl->lvl_count[q] = ctrl->push_acc[q] = 0ull;
+  }
+}
+
+// --------------------------------------------- cooperative BFS (b = 32)
+// The whole level loop of a b = 32 ROW BFS in one cooperative launch (one
+// grid of co-resident blocks).  Each level runs its step over the grid,
+// sums the new vertices and meets the other blocks at a grid barrier, after
+// which every block reads the same count and takes the same decision (stop,
+// direction of the next level).  Per level this replaces the loop graph's
+// kernel launches and conditional node with one barrier (pull levels) or
+// two (push levels).  The frontier and visited words are read with plain
+// loads (ld_state<true>): the barrier's fences make the other blocks' writes
+// of the previous level visible to them.
+//
+// Push levels walk the row-word slices of the frontier rows only (not the
+// tiles of their block rows): each entry (block column C, row word w) ORs
+// w & ~visited[C] into next-frontier word C, and the bits that this atomic
+// newly sets are vertices found here first, so the lane that set them marks
+// them visited and writes their level -- no finishing pass.  Rows whose
+// tails are long (hubs) are listed in phase A and their tails spread over
+// the whole grid after the phase barrier (phase B).
+//
+// Three level counts (and push-list counters) rotate like the frontier
+// buffers: level L adds into slot L % 3 and every block reads it after the
+// barrier; block 0 then clears slot (L + 2) % 3, which every block read at
+// level L - 1, before arriving at this level's barrier, and which level L + 2
+// fills after the next barrier.
+
+// A grid barrier gives up after this long (or this many polls).
+constexpr unsigned long long kBarrierLimitNs = 5000000000ull;
+constexpr long long kBarrierPollCap = 1ll << 28;
+// Push list counter: listed rows in the high bits, tail entries in the low 40.
+constexpr int kListShift = 40;
+constexpr unsigned long long kListMask = (1ull << kListShift) - 1ull;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Barrier over every block of a cooperative launch (arrival count and
+// generation in Ctrl; the last block to arrive resets the count and bumps
+// the generation).  A block that waits past the limit, or sees that another
+// block gave up, sets bar_err and returns false: the caller leaves the
+// kernel, so every block ends within about one limit of the first failure.
+__device__ __forceinline__ bool grid_barrier(Ctrl* c) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = &c->bar_gen;
+    volatile unsigned* err = &c->bar_err;
+    const unsigned g0 = *gen;
+    __threadfence();
+    const unsigned t = atomicAdd(&c->bar_arrive, 1u);
+    int res = 1;
+    if (t == gridDim.x - 1) {
+      atomicExch(&c->bar_arrive, 0u);
+      __threadfence();
+      atomicAdd(&c->bar_gen, 1u);
+    } else {
+      const unsigned long long t0 = global_ns();
+      for (long long k = 0; *gen == g0; ++k) {
+        if (*err || k >= kBarrierPollCap || global_ns() - t0 > kBarrierLimitNs) {
+          atomicExch(&c->bar_err, 1u);
+          res = 0;
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+    ok = res;
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// Push one row word into next-frontier word C; the vertices this call finds
+// first are marked visited and get level lvl + 1.  Returns their number.
+__device__ __forceinline__ unsigned push_word(unsigned* out, unsigned* visited, int* level, int lvl, unsigned C,
+                                              unsigned w) {
+  const unsigned cand = w & ~visited[C];
+  if (!cand) return 0u;
+  const unsigned nw = cand & ~atomicOr(out + C, cand);
+  if (!nw) return 0u;
+  atomicOr(visited + C, nw);
+  for (unsigned m = nw; m; m &= m - 1) level[(long long)C * 32 + (32 - __ffs(m))] = lvl + 1;
+  return (unsigned)__popc(nw);
+}
+
+// Push phase A: block rows with frontier bits (a lane per block row picks
+// them, strided over the grid like the pull step); the head entries and
+// short tails of their frontier rows form one list per block row that the
+// warp's lanes take 32 entries at a time.  Frontier rows with long tails go
+// on the push list (start in the list's entry space, tail offset).
+__device__ __forceinline__ unsigned long long push_rws_rows(const GView& v, unsigned* front, unsigned* visited,
+                                                            int* level, int lvl, unsigned long long* list_acc,
+                                                            long long* list) {
+  const unsigned* x = front_buf(front, v.nbr, lvl);
+  unsigned* out = front_buf(front, v.nbr, lvl + 1);
+  unsigned* z = front_buf(front, v.nbr, lvl + 2);
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned kFull = 0xffffffffu;
+  const long long nwarps = warps_total();
+  unsigned long long cnt = 0;
+  for (long long base = warp_global(); base < v.nbr; base += 32 * nwarps) {
+    const long long Rl = base + (long long)lane * nwarps;
+    unsigned xl = 0u;
+    if (Rl < v.nbr) {
+      xl = x[Rl];
+      z[Rl] = 0u;
+    }
+    unsigned act = __ballot_sync(kFull, xl != 0u);
+    while (act) {
+      const int j = __ffs(act) - 1;
+      act &= act - 1;
+      const long long R = base + (long long)j * nwarps;
+      const unsigned fr = __shfl_sync(kFull, xl, j);
+      const bool mine = (fr >> (31 - lane)) & 1u;
+      long long tb = 0, tl = 0;
+      if (mine) {
+        tb = v.rws_tail_ptr[R * 32 + lane];
+        tl = v.rws_tail_ptr[R * 32 + lane + 1] - tb;
+      }
+      const bool lng = tl > kRwsLongTail;
+      if (lng) {
+        const unsigned long long old = atomicAdd(list_acc, (1ull << kListShift) | (unsigned long long)tl);
+        const long long q = (long long)(old >> kListShift);
+        list[2 * q] = (long long)(old & kListMask);
+        list[2 * q + 1] = tb;
+      }
+      const int len = mine ? kRwsHead + (lng ? 0 : (int)tl) : 0;
+      const int incl = warp_incl_sum(len, lane);
+      const int total = __shfl_sync(kFull, incl, 31);
+      const uint2* hb = v.rws_head + (size_t)R * (kRwsHead * 32);
+      for (int p = 0; p < total; p += 32) {
+        const int q = p + (int)lane;
+        // r = the first lane whose inclusive sum exceeds q (the entry's row)
+        int r = 0;
+#pragma unroll
+        for (int st = 16; st > 0; st >>= 1)
+          if (__shfl_sync(kFull, incl, r + st - 1) <= q) r += st;
+        const int rin = __shfl_sync(kFull, incl, r);
+        const int rlen = __shfl_sync(kFull, len, r);
+        const long long rtb = __shfl_sync(kFull, tb, r);
+        if (q < total) {
+          const int slot = q - (rin - rlen);
+          const uint2 e = slot < kRwsHead ? hb[(size_t)slot * 32 + r] : v.rws_tail[rtb + (slot - kRwsHead)];
+          if (e.x != kRwsNone) cnt += push_word(out, visited, level, lvl, e.x, e.y);
+        }
+      }
+    }
+  }
+  return cnt;
+}
+
+// Push phase B: the listed long tails as one entry space over every thread
+// of the grid; a thread finds its entry's row by binary search over the
+// list's starts.
+__device__ __forceinline__ unsigned long long push_rws_long(const GView& v, unsigned* front, unsigned* visited,
+                                                            int* level, int lvl, unsigned long long acc,
+                                                            const long long* list) {
+  unsigned* out = front_buf(front, v.nbr, lvl + 1);
+  const long long nl = (long long)(acc >> kListShift);
+  const long long total = (long long)(acc & kListMask);
+  unsigned long long cnt = 0;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+       q += (long long)gridDim.x * blockDim.x) {
+    long long lo = 0, hi = nl - 1;
+    while (lo < hi) {
+      const long long mid = (lo + hi + 1) >> 1;
+      if (list[2 * mid] <= q) lo = mid;
+      else hi = mid - 1;
+    }
+    const uint2 e = v.rws_tail[list[2 * lo + 1] + (q - list[2 * lo])];
+    cnt += push_word(out, visited, level, lvl, e.x, e.y);
+  }
+  return cnt;
+}
+
+__global__ void __launch_bounds__(kTPB, 6) k_bfs_coop(GView v, unsigned* front, unsigned* visited, int* level,
+                                                   Ctrl* ctrl, long long* push_list) {
+  volatile Ctrl* vc = ctrl;
+  if (vc->done) return;
+  int lvl = vc->iter;
+  int mode = vc->mode;
+  const int max_iter = vc->max_iter;
+  const unsigned long long push_thr = vc->push_thr > 0 ? (unsigned long long)vc->push_thr : 0ull;
+  unsigned long long* stamps = vc->stamps;
+  for (;;) {
+    unsigned long long cnt;
+    if (!mode) {
+      cnt = pull_rws_level<true>(v, front, visited, level, lvl);
+    } else {
+      cnt = push_rws_rows(v, front, visited, level, lvl, &ctrl->push_acc[lvl % 3], push_list);
+      if (!grid_barrier(ctrl)) return;
+      const unsigned long long acc = __ldcg(&ctrl->push_acc[lvl % 3]);
+      if (acc) cnt += push_rws_long(v, front, visited, level, lvl, acc, push_list);
+    }
+    block_add_u64(cnt, &ctrl->lvl_count[lvl % 3]);
+    if (!grid_barrier(ctrl)) return;
+    const unsigned long long nf = __ldcg(&ctrl->lvl_count[lvl % 3]);
+    const int it = lvl + 1;
+    const bool stop = nf == 0ull || it >= max_iter;
+    mode = (nf > 0ull && nf < push_thr) ? 1 : 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      ctrl->lvl_count[(lvl + 2) % 3] = 0ull;
+      ctrl->push_acc[(lvl + 2) % 3] = 0ull;
+      vc->iter = it;
+      vc->mode = mode;
+      vc->count = nf;
+      if (stop) vc->done = 1;
+      if (stamps && it <= kStampCap) stamps[it] = global_ns();
+      __threadfence();
+    }
+    if (stop) return;
+    lvl = it;
   }
 }
 
@@ -1313,6 +1569,7 @@ int get_state(gbo_graph* g, AlgoState** out) {
     g->algo = a;
     GBO_CUDA_TRY(cudaStreamCreateWithFlags(&a->cap, cudaStreamNonBlocking));
     GBO_CUDA_TRY(cudaMalloc(&a->ctrl, sizeof(Ctrl)));
+    GBO_CUDA_TRY(cudaMemset(a->ctrl, 0, sizeof(Ctrl)));
     GBO_CUDA_TRY(cudaHostAlloc(&a->h_ctrl, sizeof(Ctrl), cudaHostAllocDefault));
     const size_t sb = (size_t)g->nslots * (size_t)g->b * 8 + 64;
     GBO_CUDA_TRY(cudaMalloc(&a->scratch, sb));
@@ -1449,22 +1706,79 @@ int get_exec(AlgoState* a, int id, const void* key, Body body) {
 // the call waits for the loop and returns its iteration count; otherwise it
 // returns at once (stream-ordered).  An injected iteration cap that cuts the
 // loop returns GBO_ERR_TIMEOUT.
-int run_until_done(AlgoState* a, int id, cudaStream_t s, int max_iter, int* iters) {
+int injected_cap_iters() {
   const long long cap = inject_replay_cap();
-  const int cap_iters = cap > 0 ? (int)std::min<long long>(cap * kStepsPerGraph, 1 << 30) : 0;
-  k_loop_begin<<<1, 32, 0, s>>>(a->ctrl, a->cond[id], a->stamps, cap_iters);
-  GBO_CUDA_TRY(cudaGetLastError());
-  GBO_CUDA_TRY(cudaGraphLaunch(a->exec[id], s));
+  return cap > 0 ? (int)std::min<long long>(cap * kStepsPerGraph, 1 << 30) : 0;
+}
+
+// After a loop run was queued: wait for it when the caller wants the
+// iteration count or a cap was injected, and check how it ended.
+int finish_loop(AlgoState* a, cudaStream_t s, int max_iter, int cap_iters, int* iters, bool coop = false) {
   a->replays = 1;
   a->stats_pending = true;
   if (!iters && cap_iters == 0) return GBO_OK;
   GBO_CUDA_TRY(cudaMemcpyAsync(a->h_ctrl, a->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
   GBO_CUDA_TRY(cudaStreamSynchronize(s));
+  if (coop && a->h_ctrl->bar_err) return fail(GBO_ERR_TIMEOUT, "cooperative BFS: a grid barrier gave up");
   if (!a->h_ctrl->done) return fail(GBO_ERR_TIMEOUT, "iteration loop did not terminate");
   if (cap_iters > 0 && cap_iters < max_iter && a->h_ctrl->iter >= cap_iters)
     return fail(GBO_ERR_TIMEOUT, "iteration loop cut off by the injected cap");
   if (iters) *iters = a->h_ctrl->iter;
   return GBO_OK;
+}
+
+int run_until_done(AlgoState* a, int id, cudaStream_t s, int max_iter, int* iters) {
+  const int cap_iters = injected_cap_iters();
+  k_loop_begin<<<1, 32, 0, s>>>(a->ctrl, a->cond[id], a->stamps, cap_iters);
+  GBO_CUDA_TRY(cudaGetLastError());
+  GBO_CUDA_TRY(cudaGraphLaunch(a->exec[id], s));
+  a->fixed_launches = 2;  // init and loop start kernels
+  return finish_loop(a, s, max_iter, cap_iters, iters);
+}
+
+// Blocks of the cooperative BFS: every block resident at once (the grid
+// barrier needs it) and at most kCoopBlocksPerSM per SM -- a barrier costs
+// 2.4 us over 148 blocks and 4.0 us over 888 on B200, and R-MAT 22 BFS runs
+// fastest at 4-5 blocks per SM -- and about one warp per 4 block rows or 32
+// work items; or the caller's choice (gbo_graph_set_bfs_loop) within the
+// resident limit.
+int coop_grid(const gbo_graph* g, unsigned* grid) {
+  int per_sm = 0, coop = 0, dev = 0;
+  GBO_CUDA_TRY(cudaGetDevice(&dev));
+  GBO_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  if (!coop) return fail(GBO_ERR_UNSUPPORTED, "device has no cooperative launch");
+  GBO_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bfs_coop, kTPB, 0));
+  if (per_sm < 1) return fail(GBO_ERR_UNSUPPORTED, "cooperative BFS kernel does not fit an SM");
+  const unsigned cap = (unsigned)num_sms() * (unsigned)per_sm;
+  const long long warps = std::max<long long>(((long long)g->nbr + 3) / 4, ((long long)g->nitems + 31) / 32);
+  unsigned want = blocks_for_warps(std::max<long long>(warps, 1), kTPB / 32);
+  want = std::min(want, (unsigned)num_sms() * (unsigned)kCoopBlocksPerSM);
+  if (g->bfs_coop_blocks > 0) want = (unsigned)g->bfs_coop_blocks;
+  *grid = want < cap ? want : cap;
+  return GBO_OK;
+}
+
+// The BFS level loop as one cooperative launch (k_bfs_coop) on s.
+int run_bfs_coop(gbo_graph* g, AlgoState* a, const GView& v, unsigned* front, unsigned* vis, int* level,
+                 cudaStream_t s, int max_iter, int* iters) {
+  unsigned grid = 0;
+  GBO_TRY(coop_grid(g, &grid));
+  if (!a->push_list) {
+    const size_t nb = sizeof(long long) * 2 * (size_t)std::max(g->rws_nlong, 1);
+    GBO_CUDA_TRY(cudaMalloc(&a->push_list, nb));
+    g->device_bytes += (long long)nb;
+  }
+  long long* list = a->push_list;
+  const int cap_iters = injected_cap_iters();
+  k_loop_begin<<<1, 32, 0, s>>>(a->ctrl, 0ull, a->stamps, cap_iters);
+  GBO_CUDA_TRY(cudaGetLastError());
+  GView va = v;
+  Ctrl* ctrl = a->ctrl;
+  void* args[] = {&va, &front, &vis, &level, &ctrl, &list};
+  GBO_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_bfs_coop, dim3(grid), dim3(kTPB), args, 0, s));
+  a->fixed_launches = 3;  // init, loop start and the cooperative loop
+  a->launches_per_iter = 0;
+  return finish_loop(a, s, max_iter, cap_iters, iters, true);
 }
 
 // Step times and counts of the last loop run, read back on first request.
@@ -1479,7 +1793,7 @@ int collect_stats(AlgoState* a) {
   GBO_CUDA_TRY(cudaMemcpy(t.data(), a->stamps, sizeof(unsigned long long) * t.size(), cudaMemcpyDeviceToHost));
   a->step_ms.clear();
   for (int q = 0; q < nst; ++q) a->step_ms.push_back((float)((double)(t[(size_t)q + 1] - t[(size_t)q]) * 1e-6));
-  a->launches = 2 + (long long)it * a->launches_per_iter;  // init and loop start kernels
+  a->launches = a->fixed_launches + (long long)it * a->launches_per_iter;
   return GBO_OK;
 }
 
@@ -1513,6 +1827,12 @@ int bfs_impl(gbo_graph* g, int src, const int* h_seeds, int nseeds, int32_t* d_l
   if (B == 32 && !col) GBO_TRY(build_rws(g, s));
   const bool rws = B == 32 && !col && g->rws_head != nullptr;
   if (rws) v = view_of(g);
+  // the level loop in one cooperative launch (its push list counts rows in
+  // 24 bits and tail entries in 40)
+  const bool coop = rws && g->nitems > 0 && g->rws_nlong < (1 << 23) && g->rws_ntail < (1ll << 39) &&
+                    (g->bfs_loop == GBO_BFS_LOOP_COOP || (g->bfs_loop == GBO_BFS_LOOP_AUTO && kCoopBfsDefault));
+  if (g->bfs_loop == GBO_BFS_LOOP_COOP && !rws)
+    return fail(GBO_ERR_UNSUPPORTED, "the cooperative BFS loop needs a b = 32 ROW graph");
   // the slice pull step finishes every block row itself: no split partials
   GView vfin = v;
   if (rws) vfin.nsplit = 0;
@@ -1523,7 +1843,7 @@ int bfs_impl(gbo_graph* g, int src, const int* h_seeds, int nseeds, int32_t* d_l
   const bool push_ok = g->symmetric;
   const unsigned gs = blocks_for(std::max<long long>(g->nsplit, push_ok ? g->nbr : 0), kTPB);
   const unsigned gp = col ? grid_persistent(k_bfs_push_col<B>, g->nitems) : grid_persistent(k_bfs_push<B>, g->nitems);
-  GBO_TRY(get_exec(a, A_BFS, nullptr, [&](cudaStream_t cs, int k, int* nl) -> int {
+  if (!coop) GBO_TRY(get_exec(a, A_BFS, nullptr, [&](cudaStream_t cs, int k, int* nl) -> int {
     if (g->nitems > 0) {
       if (col) k_bfs_step_col<B><<<gi, kTPB, 0, cs>>>(v, front, vis, level, ctrl, scratch);
       else if (rws)
@@ -1562,7 +1882,13 @@ int bfs_impl(gbo_graph* g, int src, const int* h_seeds, int nseeds, int32_t* d_l
   int iters = 0;
   // without h_depth the call is asynchronous: the loop and the level copy
   // are queued on s and the call returns
-  GBO_TRY(run_until_done(a, A_BFS, s, max_iter, h_depth ? &iters : nullptr));
+  if (coop) {
+    if constexpr (B == 32)
+      GBO_TRY(run_bfs_coop(g, a, v, reinterpret_cast<unsigned*>(front), reinterpret_cast<unsigned*>(vis), level,
+                           s, max_iter, h_depth ? &iters : nullptr));
+  } else {
+    GBO_TRY(run_until_done(a, A_BFS, s, max_iter, h_depth ? &iters : nullptr));
+  }
   if (g->nrows > 0)
     GBO_CUDA_TRY(cudaMemcpyAsync(d_level, level, sizeof(int) * (size_t)g->nrows,
                                  cudaMemcpyDeviceToDevice, s));
@@ -1886,6 +2212,7 @@ void free_algo_state(gbo_graph* g) {
   cudaFree(a->mngf);
   cudaFree(a->acc64);
   cudaFree(a->pr_part);
+  cudaFree(a->push_list);
   cudaFree(a->seeds);
   cudaFree(a->scratch);
   if (a->cap) cudaStreamDestroy(a->cap);

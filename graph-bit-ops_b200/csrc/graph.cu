@@ -354,6 +354,18 @@ extern "C" int gbo_graph_set_bfs_direction(gbo_graph* g, int symmetric, int push
   return GBO_OK;
 }
 
+extern "C" int gbo_graph_set_bfs_loop(gbo_graph* g, int loop, int coop_blocks) {
+  clear_error();
+  if (!g) return fail(GBO_ERR_INVALID, "NULL graph");
+  if (loop < GBO_BFS_LOOP_AUTO || loop > GBO_BFS_LOOP_COOP) return fail(GBO_ERR_INVALID, "unknown BFS loop");
+  if (coop_blocks < 0) return fail(GBO_ERR_INVALID, "coop_blocks must be >= 0");
+  if (loop == GBO_BFS_LOOP_COOP && (g->b != 32 || g->layout != GBO_LAYOUT_ROW))
+    return fail(GBO_ERR_UNSUPPORTED, "the cooperative BFS loop needs a b = 32 ROW graph");
+  g->bfs_loop = loop;
+  g->bfs_coop_blocks = coop_blocks;
+  return GBO_OK;
+}
+
 // ------------------------------------------------------------ BMV C ABI
 static int check_graph(const gbo_graph* g) {
   if (!g) return fail(GBO_ERR_INVALID, "graph is NULL");

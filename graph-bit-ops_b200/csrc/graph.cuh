@@ -28,6 +28,8 @@ struct gbo_graph {
   bool owns_b2sr = true;
   bool symmetric = false;  // caller asserts P == P^T (enables push BFS steps)
   int bfs_push_thr = -1;   // push below this frontier size (-1: nrows / 64)
+  int bfs_loop = 0;        // GBO_BFS_LOOP_* (gbo_graph_set_bfs_loop)
+  int bfs_coop_blocks = 0; // cooperative BFS grid (0: sized by the graph)
   int* perm = nullptr;     // GBO_FLAG_DEGREE_ORDER: new label of every input vertex
   int* tile_row = nullptr; // block row of every tile (triangle counting)
   unsigned* rowmask = nullptr;  // b = 32 ROW: non-empty row words of every tile

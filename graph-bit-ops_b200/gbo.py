@@ -30,6 +30,9 @@ GBO_ERR_FULL = 11
 INJECT_HOST_ALLOC = 1
 INJECT_REPLAY_CAP = 2
 INJECT_SERVER_HOLD = 3
+BFS_LOOP_AUTO = 0
+BFS_LOOP_GRAPH = 1
+BFS_LOOP_COOP = 2
 
 LAYOUT_ROW = 0
 LAYOUT_COL = 1
@@ -142,6 +145,7 @@ _SIGS = {
     "gbo_graph_b2sr": (_I, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
     "gbo_graph_outdeg": (_I, [_P, C.POINTER(_P)]),
     "gbo_graph_set_bfs_direction": (_I, [_P, _I, _I]),
+    "gbo_graph_set_bfs_loop": (_I, [_P, _I, _I]),
     "gbo_graph_permutation": (_I, [_P, C.POINTER(_P)]),
     "gbo_tune_tile_width": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _P, C.POINTER(_I), _P]),
     "gbo_bmv_count": (_I, [_P, _P, _P, _I, _I, _P]),
@@ -560,6 +564,12 @@ class Graph:
         frontier vertices (-1: nrows / 64; 0: pull only)."""
         check(lib().gbo_graph_set_bfs_direction(self.h, int(bool(symmetric)), push_threshold),
               "graph_set_bfs_direction")
+
+    def set_bfs_loop(self, loop: int, coop_blocks: int = 0) -> None:
+        """BFS level loop: BFS_LOOP_GRAPH (per-level kernels in a loop graph),
+        BFS_LOOP_COOP (one cooperative launch, b = 32 ROW graphs) or
+        BFS_LOOP_AUTO; coop_blocks > 0 sets the cooperative grid."""
+        check(lib().gbo_graph_set_bfs_loop(self.h, int(loop), int(coop_blocks)), "graph_set_bfs_loop")
 
     def last_run(self) -> dict:
         st = RunStats()

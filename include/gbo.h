@@ -211,6 +211,24 @@ GBO_API int gbo_graph_permutation(const gbo_graph* g, const int** d_new_of_old);
  * Rejected (GBO_ERR_UNSUPPORTED) for a non-square graph. */
 GBO_API int gbo_graph_set_bfs_direction(gbo_graph* g, int symmetric, int push_threshold);
 
+/* How gbo_bfs / gbo_bfs_multi / gbo_sssp run their level loop (no
+ * counterpart in the reference, whose BFS loop copies a flag to the host
+ * after every level).
+ *   GBO_BFS_LOOP_GRAPH: the level's kernels (pull, push, finish) in a CUDA
+ *     graph whose conditional WHILE node repeats them until a level adds no
+ *     vertex; every graph.
+ *   GBO_BFS_LOOP_COOP: the whole loop in one cooperative launch whose blocks
+ *     meet at a grid barrier after each level; b = 32 ROW graphs only
+ *     (GBO_ERR_UNSUPPORTED otherwise).  coop_blocks > 0 sets its grid (capped
+ *     at the blocks that fit on the device at once), 0 sizes it by the graph.
+ *     A barrier that waits longer than 5 s gives up: the call returns
+ *     GBO_ERR_TIMEOUT (synchronous form) and the levels are incomplete.
+ *   GBO_BFS_LOOP_AUTO (the default): GBO_BFS_LOOP_COOP where it applies,
+ *     else GBO_BFS_LOOP_GRAPH.
+ * Both loops give the same levels. */
+enum { GBO_BFS_LOOP_AUTO = 0, GBO_BFS_LOOP_GRAPH = 1, GBO_BFS_LOOP_COOP = 2 };
+GBO_API int gbo_graph_set_bfs_loop(gbo_graph* g, int loop, int coop_blocks);
+
 /* Tile-width tuner (no counterpart in the reference, whose drivers take b
  * from the command line).  Ranks b = 4, 8, 16, 32, 64 for the CSR matrix
  * (same arguments and flags as gbo_graph_from_csr) and an operation:

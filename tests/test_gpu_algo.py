@@ -40,9 +40,10 @@ def test_bfs_golden(gbo, gpu, golden):
         g = gbo.Graph.from_csr(csr, 32)
         lv, depth = g.bfs(0)
         assert sha(lv) == golden[key]["bfs_levels_sha"] and depth == golden[key]["bfs_depth"]
-        st = g.last_run()  # per-level kernel times from events inside the loop graph
+        st = g.last_run()  # per-level times from device clock stamps at each level's end
         assert st["iterations"] == depth and len(st["step_ms"]) == depth
-        assert all(ms >= 0 for ms in st["step_ms"]) and st["kernel_launches"] > depth
+        # the cooperative loop launches 3 kernels, the loop graph 2 or 3 per level
+        assert all(ms >= 0 for ms in st["step_ms"]) and st["kernel_launches"] in (3, 2 + 2 * depth, 2 + 3 * depth)
 
 
 def test_bfs_transpose_directed(gbo, orc, gpu, graphs):
@@ -189,6 +190,56 @@ def test_bfs_push_every_level(gbo, orc, gpu, graphs, b):
         g.set_bfs_direction(False)
         lv, _ = g.bfs(1)
         assert np.array_equal(lv, orc.bfs_csr(csr.rowptr, csr.colind, csr.nrows, 1)[0])
+
+
+def test_bfs_cooperative_loop(gbo, orc, gpu, graphs):
+    """The level loop as one cooperative launch (b = 32 ROW) gives the levels
+    of the loop-graph form and of the oracle: pull-only, direction-optimising
+    and every level pushed, single and many seeds, SSSP, and grids from one
+    block to the device's limit."""
+    cs = dict(graphs)
+    cs["rmat18"] = gbo.gen_rmat(18, 16, seed=7)
+    for name, csr in cs.items():
+        sym = name != "ragged1001"
+        g = gbo.Graph.from_csr(csr, 32, gbo.FLAG_SYMMETRIC if sym else 0)
+        srcs = (0, csr.nrows // 2, csr.nrows - 1)
+        for thr in ((-1, csr.nrows + 1, 0) if sym else (0,)):
+            g.set_bfs_direction(sym and thr != 0, thr)
+            for blocks in (0, 1, 7, 1 << 20):
+                g.set_bfs_loop(gbo.BFS_LOOP_COOP, blocks)
+                for src in srcs:
+                    want, d = orc.bfs_csr(csr.rowptr, csr.colind, csr.nrows, src)
+                    lv, depth = g.bfs(src)
+                    assert np.array_equal(lv, want) and depth == d, (name, thr, blocks, src)
+                    st = g.last_run()
+                    assert st["iterations"] == depth and len(st["step_ms"]) == min(depth, 4096)
+                    assert st["kernel_launches"] == 3
+            g.set_bfs_loop(gbo.BFS_LOOP_GRAPH)
+            lv, depth = g.bfs(srcs[1])
+            assert np.array_equal(lv, orc.bfs_csr(csr.rowptr, csr.colind, csr.nrows, srcs[1])[0]), (name, thr)
+        g.set_bfs_loop(gbo.BFS_LOOP_COOP)
+        dist, _ = g.sssp(1 % csr.nrows)
+        want, _ = orc.bfs_csr(csr.rowptr, csr.colind, csr.nrows, 1 % csr.nrows)
+        assert np.array_equal(dist, np.where(want < 0, INF, want).astype(np.uint32)), name
+        seeds = np.arange(0, csr.nrows, max(1, csr.nrows // 5), dtype=np.int32)
+        lv, _ = g.bfs_multi(seeds)
+        ref = np.full(csr.nrows, -1, np.int64)
+        for s in seeds:
+            x, _ = orc.bfs_csr(csr.rowptr, csr.colind, csr.nrows, int(s))
+            ref = np.where((ref < 0) | ((x >= 0) & (x < ref)), x, ref)
+        assert np.array_equal(lv, ref), name
+        g.free()
+
+
+def test_bfs_cooperative_loop_rejected(gbo, gpu, graphs):
+    g = gbo.Graph.from_csr(graphs["er1000"], 8)
+    with pytest.raises(gbo.GboError) as e:
+        g.set_bfs_loop(gbo.BFS_LOOP_COOP)
+    assert e.value.status == gbo.GBO_ERR_UNSUPPORTED
+    with pytest.raises(gbo.GboError):
+        g.set_bfs_loop(7)
+    g.set_bfs_loop(gbo.BFS_LOOP_GRAPH)
+    g.free()
 
 
 @pytest.mark.parametrize("b", WIDTHS)
