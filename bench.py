@@ -181,6 +181,31 @@ def bfs_level_bytes(rowptr_b, colind_b, levels, nrows, b, row_live, layout="row"
     return out
 
 
+def bfs_push_bytes_rws(csr, levels, L, head=8, long_tail=64):
+    """Algorithmic bytes of the cooperative loop's push step at level L over
+    the row-word slices: the frontier word of every block row read and one
+    frontier word cleared (8 bytes per block row); for every frontier row its
+    16-byte tail offsets and its `head` head slots (8 bytes each, sentinels
+    included), then every tail entry (8 bytes; a tail longer than
+    `long_tail` goes through the push list, 16 bytes more); 4 bytes of level
+    per new vertex and 8 bytes (next-frontier and visited words) per changed
+    block row.  Visited-word gathers and next-frontier atomics are excluded
+    (512 KB vectors that L2 holds), as in the pull model."""
+    n = csr.nrows
+    nbr = (n + 31) // 32
+    front = levels == L
+    bc = (csr.colind // 32).astype(np.int64)
+    prow = np.repeat(np.arange(n, dtype=np.int64), np.diff(csr.rowptr))
+    first = np.ones(len(bc), bool)
+    first[1:] = (bc[1:] != bc[:-1]) | (prow[1:] != prow[:-1])
+    npairs = np.bincount(prow[first], minlength=n).astype(np.int64)
+    tail = np.maximum(npairs - head, 0)[front]
+    newv = levels == L + 1
+    changed = int(np.count_nonzero(np.pad(newv, (0, nbr * 32 - n)).reshape(nbr, 32).any(axis=1)))
+    return (8 * nbr + int(front.sum()) * (16 + 8 * head) + 8 * int(tail.sum())
+            + 16 * int(np.count_nonzero(tail > long_tail)) + 4 * int(newv.sum()) + 8 * changed)
+
+
 def bfs_level_bytes_rws(csr, levels, head=8):
     """Algorithmic bytes of each BFS pull step over the row-word slices of a
     32x32 ROW graph (every row's non-empty row words with their block
@@ -242,19 +267,31 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def load_traffic(name):
-    """Per-launch DRAM bytes of a kernel from a committed ncu summary, if any."""
+def load_traffic(name, algorithmic=None):
+    """Per-launch DRAM bytes of a kernel from a committed ncu summary, if any
+    (its `traffic_bytes_per_launch:` line).  With `algorithmic` (this run's
+    algorithmic bytes per launch) and an `algorithmic_bytes_per_launch:` line
+    in the summary, the captured traffic is scaled by their ratio: the
+    capture ran a smaller case of the same kernel."""
     p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
+    vals = {}
     with open(p) as f:
         for line in f:
-            if line.startswith("traffic_bytes_per_launch:"):
-                try:
-                    return float(line.split(":", 1)[1])
-                except ValueError:
-                    return None
-    return None
+            for key in ("traffic_bytes_per_launch", "algorithmic_bytes_per_launch"):
+                if line.startswith(key + ":"):
+                    try:
+                        vals[key] = float(line.split(":", 1)[1])
+                    except ValueError:
+                        pass
+    t = vals.get("traffic_bytes_per_launch")
+    a = vals.get("algorithmic_bytes_per_launch")
+    if t is None:
+        return None
+    if algorithmic is not None and a:
+        return t * algorithmic / a
+    return t
 
 
 # ----------------------------------------------------------------- clocks
@@ -635,22 +672,34 @@ def run_ours(args, ws, rank, local):
     pull_lvl_ms = np.array(step_ms_all, np.float64).reshape(args.steps, -1).mean(axis=0)
     auto_lvl_ms = np.array(auto_step_ms, np.float64).reshape(args.steps, -1).mean(axis=0)
     rws = args.tile == 32 and args.layout == "row"
+    coop = rws and other_loop is not None and other_loop["headline_loop"] == "cooperative"
+    rl_launch = None
     if rws:
-        # 32x32 ROW graphs pull over their row-word slices (k_bfs_pull_rws);
-        # the roofline covers the pull levels of the timed (headline) runs:
-        # level L pushes iff 0 < |level L| < n/64 (the library's default)
+        # 32x32 ROW graphs traverse their row-word slices; level L pushes iff
+        # 0 < |level L| < n/64 (the library's default)
         lvl_bytes = bfs_level_bytes_rws(csr, levels)
         sizes = np.bincount(levels[levels >= 0], minlength=len(lvl_bytes))
         thr = max(1, n // 64) if args.direction == "auto" else 0
-        pull_lv = [L for L in range(min(len(lvl_bytes), len(auto_lvl_ms)))
-                   if not (thr > 0 and 0 < sizes[L] < thr)]
-        rl_bytes = [lvl_bytes[L] for L in pull_lv]
-        rl_ms = [float(auto_lvl_ms[L]) for L in pull_lv]
-        kernel_name = ("k_bfs_coop (cooperative BFS loop; its pull levels over row-word slices)"
-                       if other_loop and other_loop["headline_loop"] == "cooperative" else
-                       "k_bfs_pull_rws (BFS pull step over row-word slices, pull levels of the timed runs)")
-        traffic = load_traffic("k_bfs_pull_rws_rmat20_ncu.md")
-        traffic_note = "scaled from the R-MAT 20 ncu capture in profiles/ by algorithmic bytes"
+        nlv = min(len(lvl_bytes), len(auto_lvl_ms))
+        pushed = [thr > 0 and 0 < sizes[L] < thr for L in range(nlv)]
+        if coop:
+            # one launch (k_bfs_coop) is the whole BFS: every level, pull or push
+            for L in range(nlv):
+                if pushed[L]:
+                    lvl_bytes[L] = bfs_push_bytes_rws(csr, levels, L)
+            pull_lv = list(range(nlv))
+            rl_bytes = [float(sum(lvl_bytes[:nlv]))]
+            rl_ms = [float(np.sum(auto_lvl_ms[:nlv]))]
+            rl_launch = {"levels_pushed": [L for L in range(nlv) if pushed[L]]}
+            kernel_name = "k_bfs_coop (cooperative BFS loop over row-word slices, one launch per BFS)"
+            traffic = load_traffic("k_bfs_coop_rmat20_ncu.md", rl_bytes[0])
+        else:
+            pull_lv = [L for L in range(nlv) if not pushed[L]]
+            rl_bytes = [lvl_bytes[L] for L in pull_lv]
+            rl_ms = [float(auto_lvl_ms[L]) for L in pull_lv]
+            kernel_name = "k_bfs_pull_rws (BFS pull step over row-word slices, pull levels of the timed runs)"
+            traffic = None
+        traffic_note = "ncu capture of the same kernel at R-MAT 20 in profiles/, scaled by algorithmic bytes"
     else:
         r = C_void()
         c = C_void()
@@ -767,7 +816,7 @@ def run_ours(args, ws, rank, local):
                      "frac": achieved / peak, "traffic": traffic,
                      "traffic_source": traffic_note if traffic is not None else None,
                      "kernel": kernel_name, "peak_source": peak_src,
-                     "levels": pull_lv,
+                     "levels": pull_lv, "launch": rl_launch,
                      "algorithmic_bytes_per_launch": float(np.mean(rl_bytes)),
                      "ms_per_launch": float(np.mean(rl_ms))},
         "e2e": {"value": ws * edges / (e2e_ms / 1e3) / 1e9, "unit": "GTEPS",
@@ -987,8 +1036,8 @@ def suite_config2(args, which):
         extra = {"iterations": it.value, "dtype": "f32",
                  "roofline": {"bound": "hbm", "achieved": by / (step / 1e3) / 1e9, "peak": peak,
                               "unit": "GB/s", "frac": by / (step / 1e3) / 1e9 / peak,
-                              "traffic": (load_traffic("k_pr_step_rws_rmat20_ncu.md")
-                                          if args.scale == SCALE and args.tile == 32 else None),
+                              "traffic": (load_traffic("k_pr_step_rws_rmat20_ncu.md", by)
+                                          if args.tile == 32 else None),
                               "kernel": kname, "peak_source": psrc,
                               "algorithmic_bytes_per_launch": by, "ms_per_launch": step}}
         if bs is not None:

@@ -110,3 +110,21 @@ def test_bfs_level_bytes_rws_matches_direct_count(gbo, orc):
             by += 8 * seen + (16 if seen > 3 else 0)
         want.append(by)
     assert got == want
+
+
+def test_bfs_push_bytes_rws_matches_direct_count(gbo, orc):
+    """The slice push model (cooperative loop) against a row-by-row walk."""
+    csr = gbo.gen_rmat(9, 6, seed=4)
+    n = csr.nrows
+    levels = np.asarray(orc.bfs_csr(csr.rowptr, csr.colind, n, 0)[0], np.int64)
+    nbr = (n + 31) // 32
+    for head, long_tail in ((8, 64), (2, 3)):
+        for L in range(int(levels.max()) + 1):
+            got = bench.bfs_push_bytes_rws(csr, levels, L, head=head, long_tail=long_tail)
+            by = 8 * nbr + 4 * int((levels == L + 1).sum())
+            by += 8 * sum(any(levels[v] == L + 1 for v in range(R * 32, min(n, R * 32 + 32))) for R in range(nbr))
+            for v in np.flatnonzero(levels == L):
+                blocks = set(int(c) // 32 for c in csr.colind[csr.rowptr[v]:csr.rowptr[v + 1]])
+                tail = max(0, len(blocks) - head)
+                by += 16 + 8 * head + 8 * tail + (16 if tail > long_tail else 0)
+            assert got == by, (head, L)
