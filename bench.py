@@ -46,11 +46,12 @@ def parse():
                     help="BFS level loop: loop graph of per-level kernels or one cooperative launch")
     ap.add_argument("--coop-blocks", type=int, default=0, help="cooperative BFS grid (0: sized by the graph)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
+    ap.add_argument("--nvtx", action="store_true", help="NVTX range 'timed' around the suites' timed loops")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving streams")
     ap.add_argument("--no-permuted", action="store_true", help="skip the degree-ordered variant")
     ap.add_argument("--serve-qps", type=float, default=8000.0, help="offered BFS query rate")
     ap.add_argument("--serve-s", type=float, default=1.5, help="seconds of arrivals per stream")
-    ap.add_argument("--serve-slots", type=int, default=64, help="BFS slots of the served streams' server")
+    ap.add_argument("--serve-slots", type=int, default=256, help="BFS slots of the served streams' server")
     ap.add_argument("--tc-graphs", default="mesh,rmat", help="graphs of --workload tc (mesh, rmat)")
     ap.add_argument("--tc-variants", default="input,degree", help="vertex orders of --workload tc")
     ap.add_argument("--tc-tiles", default="8,16,32,64", help="tile widths of --workload tc")
@@ -918,16 +919,36 @@ class C_pinned:
 # oracle's OpenMP restatement on one bounded sample.
 
 
+class _Nvtx:
+    """An NVTX range named "timed" around a suite's timed loop when --nvtx
+    is given (so that ncu --nvtx --nvtx-include timed/ selects its launches,
+    whole CUDA graphs included); nothing otherwise."""
+    on = False
+
+    def __enter__(self):
+        if _Nvtx.on:
+            import torch.cuda.nvtx as nv
+            nv.range_push("timed")
+        return self
+
+    def __exit__(self, *exc):
+        if _Nvtx.on:
+            import torch.cuda.nvtx as nv
+            nv.range_pop()
+        return False
+
+
 def _timed(gbo, fn, steps, warmup):
     for _ in range(warmup):
         fn()
     gbo.sync()
     e0, e1 = gbo.Event(), gbo.Event()
-    e0.record()
-    for _ in range(steps):
-        fn()
-    e1.record()
-    gbo.sync()
+    with _Nvtx():
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        gbo.sync()
     return e0.elapsed_ms(e1) / steps
 
 
@@ -1290,7 +1311,7 @@ def suite_serve(args):
 
     csr = gbo.gen_rmat(21, 16, seed=2, **RMAT)
     n = csr.nrows
-    g = gbo.Graph.from_csr(csr, 32)
+    g = gbo.Graph.from_csr(csr, 32, gbo.FLAG_SYMMETRIC)  # symmetrised R-MAT: the plain BFS may push
     # plain per-query kernels on the same graph and GPU: one BFS per source,
     # one PPR forward solve per personalization set (same tolerance)
     rng = np.random.default_rng(13)
@@ -1693,6 +1714,7 @@ SUITE = {
 
 def main():
     args = parse()
+    _Nvtx.on = args.nvtx
     ws, rank, local = dist_env()
     if args.impl == "reference":
         if args.workload == "refgpu":

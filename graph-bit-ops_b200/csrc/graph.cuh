@@ -105,7 +105,7 @@ constexpr unsigned kRwsNone = 0xffffffffu;
 // Tails longer than this are walked by a whole warp (BFS) or cut into
 // chunks of kRwsChunk entries spread over warps (PageRank).
 constexpr int kRwsLongTail = 64;
-constexpr int kRwsChunk = 2048;
+constexpr int kRwsChunk = 512;
 // Row-word slices of a b = 32 ROW graph -> g->rws_* (no-op for other graphs
 // or when built).  Needs g->rowmask.
 int build_rws(gbo_graph* g, cudaStream_t stream);

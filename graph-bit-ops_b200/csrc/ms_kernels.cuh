@@ -43,8 +43,13 @@ struct Args {
   const int* slot_split;   // split index of every work item's slot
   uint32_t* slot_any;  // optional: OR of the new bits of every source word
   const uint32_t* live;  // optional: rows of P with an entry (others can never be reached)
-  const uint32_t* active;  // optional: source columns still traversing (kw words); a row
-                           // counts as finished once every active column reached it
+  uint32_t* active;  // optional: source columns still traversing (kw words); a row
+                     // counts as finished once every active column reached it
+  // with retire set (and active, slot_any), the level close drops the
+  // columns that found no new vertex in the level (active &= slot_any) and
+  // clears slot_any: a source whose traversal ended (an isolated source, or
+  // one whose component is exhausted) no longer keeps every row open
+  int retire = 0;
   int level_group;     // 0: levels[i*k + s]; g > 0: levels[((s/g)*n + i)*g + s%g]
   // Direction-optimising levels (symmetric graphs): with dir set, a level
   // whose frontier holds fewer than push_thr (vertex, source) pairs runs as
@@ -88,7 +93,7 @@ __device__ __forceinline__ void block_row_epilogue(const Args& a, int R, int lvl
   const int s = lane / KW;
   const unsigned wmask = seg_mask<KW>();
   uint32_t* Fn = a.F + (size_t)((lvl + 1) & 1) * a.fstride;
-  uint32_t fword = 0, vword = vrow;
+  uint32_t fword = 0, vword = vrow, anyw = 0;
   const uint32_t need = src_mask(w, a.k) & (a.active ? a.active[w] : 0xffffffffu);
   for (int rr = 0; rr < 32; rr += S) {
     const int r = rr + s;
@@ -109,7 +114,7 @@ __device__ __forceinline__ void block_row_epilogue(const Args& a, int R, int lvl
     if (nw) {
       a.V[o] = vn;
       cnt += __popc(nw);
-      if (a.slot_any) atomicOr(a.slot_any + w, nw);
+      anyw |= nw;
       uint32_t m = nw;
       while (m) {
         const int p = __ffs(m) - 1;
@@ -127,6 +132,17 @@ __device__ __forceinline__ void block_row_epilogue(const Args& a, int R, int lvl
   if (lane == 0) {
     a.fbits[(size_t)((lvl + 1) & 1) * (a.v.nbr + 1) + R] = fword;
     a.vfull[R] = vword;
+  }
+  if (a.slot_any) {
+    // the block row's new bits per source word (lanes w, w + KW, ... hold
+    // word w), added only where the word does not have them yet: most
+    // columns are marked early in a level, so few atomics reach one address
+#pragma unroll
+    for (int o = KW; o < 32; o <<= 1) anyw |= __shfl_xor_sync(0xffffffffu, anyw, o);
+    if (s == 0 && anyw) {
+      const uint32_t cur = __ldcg(a.slot_any + w);
+      if (anyw & ~cur) atomicOr(a.slot_any + w, anyw);
+    }
   }
 }
 
@@ -550,238 +566,6 @@ __global__ void __launch_bounds__(kTPB, 6) k_step_rws(Args a) {
   }
 }
 
-// The row-word slice step for wide frontier rows (k > 64: KW = 4..32 words
-// per vertex).  Lane (s, w) = (lane / KW, lane % KW) works on word w of row
-// rr + s, S = 32 / KW rows per pass, so a frontier row (KW words) is one
-// coalesced load by its group.  Each group walks its row's entries (the
-// group's lanes load the same entry), keeps the bits of each word whose
-// vertex has a non-empty frontier row and ORs those rows' words; the row
-// leaves once every active source has reached it.  Long rows' tails come
-// from k_long_chunks_wide.  Same epilogue as k_step.
-//
-// Every index these two kernels compute is checked against its array before
-// the access (a bad one is skipped and recorded in ctl[9] / ctl[10], which
-// the host reads after the level loop), and their warp loops run on a
-// budget: a loop past it stops and records the fact the same way.
-constexpr int kWatchBounds = 1, kWatchBudget = 2;
-constexpr long long kWarpBudget = 1ll << 16;
-
-__device__ __forceinline__ void watch_fail(const Args& a, int code, long long idx) {
-  if (atomicCAS(a.ctl + 9, 0, code) == 0) a.ctl[10] = (int)(idx & 0x7fffffff);
-}
-
-template <int KW>
-__device__ __forceinline__ void or_entries4_wide(const Args& a, const uint32_t* __restrict__ F,
-                                                 const uint32_t* __restrict__ fb, const uint2 (&e)[4], int w,
-                                                 uint32_t& f) {
-  const GView& v = a.v;
-  uint32_t m[4];
-#pragma unroll
-  for (int u = 0; u < 4; ++u) {
-    m[u] = 0u;
-    if (e[u].x != kRwsNone) {
-      if (e[u].x > (unsigned)v.nbr) watch_fail(a, kWatchBounds, e[u].x);
-      else m[u] = e[u].y & __ldg(fb + e[u].x);
-    }
-  }
-  const size_t fsize = (size_t)v.nrows * KW;
-  while (m[0] | m[1] | m[2] | m[3]) {
-    uint32_t g[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      g[u] = 0u;
-      if (m[u]) {
-        const int col = __clz(m[u]);
-        m[u] &= ~(0x80000000u >> col);
-        const size_t fo = ((size_t)e[u].x * 32 + col) * KW + w;
-        if (fo >= fsize) watch_fail(a, kWatchBounds, (long long)fo);
-        else g[u] = __ldg(F + fo);
-      }
-    }
-    f |= g[0] | g[1] | g[2] | g[3];
-  }
-}
-
-__device__ __forceinline__ uint2 tail_entry(const Args& a, long long p) {
-  if (p < 0 || p >= a.v.rws_ntail) {
-    watch_fail(a, kWatchBounds, p);
-    return make_uint2(kRwsNone, 0u);
-  }
-  return a.v.rws_tail[p];
-}
-
-// Index of long row i among the long rows (i is one of them).
-__device__ __forceinline__ int long_row_index(const GView& v, long long i) {
-  int lo = 0, hi = v.rws_nlong;
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (v.rws_long_row[mid] <= i) lo = mid;
-    else hi = mid;
-  }
-  return lo;
-}
-
-template <int KW>
-__global__ void __launch_bounds__(kTPB, 4) k_step_rws_wide(Args a) {
-  static_assert(KW >= 4 && KW <= 32, "wide frontier rows");
-  constexpr int S = 32 / KW;
-  __shared__ uint32_t acc_sh[kWarps][32 * KW];
-  __shared__ unsigned long long cnt_sh;
-  __shared__ int arrived_sh;
-  volatile int* c = a.ctl;
-  if (c[1]) return;
-  if (threadIdx.x == 0) {
-    cnt_sh = 0ull;
-    arrived_sh = 0;
-  }
-  __syncthreads();
-  const int lvl = c[0];
-  const GView& v = a.v;
-  const uint32_t* __restrict__ F = a.F + (size_t)(lvl & 1) * a.fstride;
-  const uint32_t* __restrict__ fb = a.fbits + (size_t)(lvl & 1) * (v.nbr + 1);
-  const unsigned lane = threadIdx.x & 31;
-  const unsigned kFull = 0xffffffffu;
-  const int w = lane % KW, gs = lane / KW;
-  const unsigned gmask = (KW == 32 ? kFull : ((1u << KW) - 1u)) << (gs * KW);
-  uint32_t* acc = acc_sh[threadIdx.x >> 5];
-  const uint32_t need = src_mask(w, a.k) & (a.active ? a.active[w] : kFull);
-  const long long R = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  long long budget = kWarpBudget;  // warp-uniform
-  unsigned long long cnt = 0;
-  if (R < v.nbr) {
-    const uint32_t vrow = a.vfull[R];
-    if (vrow != kFull) {
-      for (int rr = 0; rr < 32; rr += S) {
-        const int r = rr + gs;
-        const long long i = R * 32 + r;
-        const bool open = !((vrow >> (31 - r)) & 1u) && i < v.nrows;
-        const uint32_t sv = open ? a.V[(size_t)i * KW + w] : kFull;
-        uint32_t f = 0u;
-        auto group_covered = [&]() {
-          const unsigned b = __ballot_sync(kFull, ((sv | f) & need) == need);
-          return (b & gmask) == gmask;
-        };
-        // the ballot inside group_covered needs every lane: evaluate it
-        // before the test of `open` (no short circuit around it)
-        const bool cov0 = group_covered();
-        bool go = open && !cov0;
-        const uint2* __restrict__ hp = v.rws_head + (size_t)R * (kRwsHead * 32) + r;
-#pragma unroll
-        for (int k = 0; k < kRwsHead; k += 4) {
-          if (!__any_sync(kFull, go)) break;
-          uint2 e[4];
-#pragma unroll
-          for (int u = 0; u < 4; ++u) e[u] = go ? hp[(size_t)(k + u) * 32] : make_uint2(kRwsNone, 0u);
-          or_entries4_wide<KW>(a, F, fb, e, w, f);
-          const bool cov = group_covered();
-          go = go && e[3].x != kRwsNone && !cov;
-        }
-        if (__any_sync(kFull, go)) {
-          long long tb = 0, te = 0;
-          if (go) {
-            tb = v.rws_tail_ptr[i];
-            te = v.rws_tail_ptr[i + 1];
-          }
-          go = go && te > tb;
-          if (go && te - tb > kMsLongTail) {
-            const int lq = long_row_index(v, i);
-            if (lq < 0 || lq >= v.rws_nlong || v.rws_long_row[lq] != i) watch_fail(a, kWatchBounds, i);
-            else f |= a.long_acc[(size_t)lq * KW + w];
-            go = false;
-          }
-          for (long long p = tb; __any_sync(kFull, go); p += 4) {
-            if (--budget <= 0) {
-              if (lane == 0) watch_fail(a, kWatchBudget, R);
-              break;
-            }
-            uint2 e[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) e[u] = go && p + u < te ? tail_entry(a, p + u) : make_uint2(kRwsNone, 0u);
-            or_entries4_wide<KW>(a, F, fb, e, w, f);
-            const bool cov = group_covered();
-            go = go && p + 4 < te && !cov;
-          }
-        }
-        acc[r * KW + w] = f;
-      }
-      __syncwarp();
-      block_row_epilogue<KW>(a, (int)R, lvl, vrow, lane, [&](int r, int ww) { return acc[r * KW + ww]; }, cnt);
-    } else if (lane == 0) {
-      a.fbits[(size_t)((lvl + 1) & 1) * (v.nbr + 1) + R] = 0u;
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-  if (lane == 0) {
-    if (cnt) atomicAdd(&cnt_sh, cnt);
-    __threadfence_block();
-    if (atomicAdd(&arrived_sh, 1) == kWarps - 1) {
-      __threadfence_block();
-      const unsigned long long tot = atomicAdd(&cnt_sh, 0ull);
-      if (tot) atomicAdd(reinterpret_cast<unsigned long long*>(a.ctl + 4), tot);
-    }
-  }
-}
-
-// Long rows' tails for the wide step: a warp per chunk, group s of KW lanes
-// takes entries s, s + S, ... of each batch of 32, the groups' words are
-// OR-ed across the warp and into the row's long_acc words.
-template <int KW>
-__global__ void __launch_bounds__(kTPB) k_long_chunks_wide(Args a) {
-  constexpr int S = 32 / KW;
-  volatile int* c = a.ctl;
-  if (c[1]) return;
-  const int lvl = c[0];
-  const GView& v = a.v;
-  const uint32_t* __restrict__ F = a.F + (size_t)(lvl & 1) * a.fstride;
-  const uint32_t* __restrict__ fb = a.fbits + (size_t)(lvl & 1) * (v.nbr + 1);
-  const unsigned lane = threadIdx.x & 31;
-  const unsigned kFull = 0xffffffffu;
-  const int w = lane % KW, gs = lane / KW;
-  const uint32_t need = src_mask(w, a.k) & (a.active ? a.active[w] : kFull);
-  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-  long long budget = kWarpBudget;  // warp-uniform
-  for (long long q = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < v.rws_nchunk; q += nwarps) {
-    const long long i = v.rws_chunk_row[q];
-    if (i < 0 || i >= v.nrows) {
-      if (lane == 0) watch_fail(a, kWatchBounds, i);
-      continue;
-    }
-    if ((a.vfull[i >> 5] >> (31 - (i & 31))) & 1u) continue;  // row finished
-    const uint32_t sv = a.V[(size_t)i * KW + w];
-    if (__all_sync(kFull, (sv & need) == need)) continue;
-    const long long b = v.rws_chunk_beg[q], e = v.rws_chunk_end[q];
-    uint32_t f = 0u;
-    for (long long p = b; p < e; p += 32) {
-      if (--budget <= 0) {
-        if (lane == 0) watch_fail(a, kWatchBudget, q);
-        break;
-      }
-      const uint2 mine = p + lane < e ? tail_entry(a, p + lane) : make_uint2(kRwsNone, 0u);
-      for (int q4 = 0; q4 < KW; q4 += 4) {  // this group's entries gs + S * j, j < KW (32 / S)
-        uint2 t[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int src = gs + S * (q4 + u);
-          t[u].x = __shfl_sync(kFull, mine.x, src);
-          t[u].y = __shfl_sync(kFull, mine.y, src);
-        }
-        or_entries4_wide<KW>(a, F, fb, t, w, f);
-      }
-      uint32_t all = f;
-#pragma unroll
-      for (int o = KW; o < 32; o <<= 1) all |= __shfl_xor_sync(kFull, all, o);
-      if (__all_sync(kFull, ((sv | all) & need) == need)) break;
-    }
-#pragma unroll
-    for (int o = KW; o < 32; o <<= 1) f |= __shfl_xor_sync(kFull, f, o);
-    if (lane < (unsigned)KW && f) {
-      const int lq = long_row_index(v, i);
-      if (lq < 0 || lq >= v.rws_nlong || v.rws_long_row[lq] != i) watch_fail(a, kWatchBounds, i);
-      else atomicOr(a.long_acc + (size_t)lq * KW + w, f);
-    }
-  }
-}
-
 // Block count of a level and its close: the last block to arrive (arrival
 // ticket in ctl[2], no waiting) advances the level, stops at a zero count or
 // the iteration cap and, with dir, picks the next level's mode; `pushed`
@@ -817,6 +601,13 @@ __device__ __forceinline__ void close_level(const Args& a, unsigned long long cn
     *vc = 0ull;
     a.ctl[2] = 0;
     if (stop) c[1] = 1;
+    if (a.retire && a.active && a.slot_any) {
+      volatile uint32_t* any = a.slot_any;
+      for (int w = 0; w < (a.k + 31) / 32; ++w) {
+        a.active[w] &= any[w];
+        any[w] = 0u;
+      }
+    }
     __threadfence();
   }
 }
@@ -987,6 +778,10 @@ static __global__ void k_init(Args a, int kw, int max_iter) {
     if (a.live && q < nbr) pad |= ~a.live[q];
     a.vfull[q] = pad;
   }
+  if (a.retire && i < kw) {
+    a.active[i] = src_mask((int)i, a.k);
+    a.slot_any[i] = 0u;
+  }
   if (i == 0) {
     a.ctl[0] = 0;
     a.ctl[1] = 0;
@@ -995,8 +790,6 @@ static __global__ void k_init(Args a, int kw, int max_iter) {
     reinterpret_cast<unsigned long long*>(a.ctl + 4)[0] = 0ull;
     a.ctl[6] = a.dir ? 1 : 0;  // k sources: the first level pushes
     a.ctl[7] = 0;
-    a.ctl[9] = 0;   // watch: code of a bad index or an exhausted loop budget
-    a.ctl[10] = 0;  // watch: the index
   }
 }
 

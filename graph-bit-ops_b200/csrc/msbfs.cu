@@ -29,7 +29,9 @@ struct MsState {
   uint32_t* split_acc = nullptr;
   int* slot_split = nullptr;
   uint32_t* push_acc = nullptr;  // nbr * 32 * kw (push levels; k <= 64 on symmetric graphs)
-  uint32_t* long_acc = nullptr;  // rws_nlong * kw (slice steps, k <= 64)
+  uint32_t* long_acc = nullptr;  // rws_nlong * 2 (slice steps, k <= 64)
+  uint32_t* active = nullptr;    // 32 words: source columns still traversing
+  uint32_t* slot_any = nullptr;  // 32 words: columns with a new vertex in the level
   int* srcs = nullptr;
   int* ctl = nullptr;
   int* h_ctl = nullptr;
@@ -68,8 +70,9 @@ ms::Args make_args(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
   a.ctl = m.ctl;
   a.split_acc = m.split_acc;
   a.slot_split = m.slot_split;
-  a.slot_any = nullptr;
-  a.active = nullptr;
+  a.slot_any = m.slot_any;
+  a.active = m.active;
+  a.retire = 1;  // columns whose traversal ended stop keeping rows open
   a.live = m.live;
   a.level_group = 0;  // the API's vertex-major levels[v * k + s]
   a.push_thr = ms_push_threshold(g, m.kw);
@@ -83,8 +86,10 @@ template <int KW>
 int ms_capture(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
   const ms::Args a = make_args(g, m, d_levels, k);
   // k <= 64 on a graph with row-word slices: the pull step walks rows
-  // (k_step_rws, whole block rows: no split partials for the finish kernel)
-  const bool rws = g->rws_head != nullptr;
+  // (k_step_rws, whole block rows: no split partials for the finish kernel);
+  // wider frontier rows go through the tiles (k_step), which measured 2x
+  // faster than walking the slices at k = 256 and 1024 on R-MAT 21
+  const bool rws = KW <= 2 && g->rws_head != nullptr;
   ms::Args af = a;
   if (rws) af.v.nsplit = 0;
   const unsigned gi = rws ? blocks_for_warps(g->nbr > 0 ? g->nbr : 1, ms::kWarps)
@@ -99,7 +104,8 @@ int ms_capture(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
     cudaEventRecordWithFlags(m.ev[2 * q], m.cap, cudaEventRecordExternal);
     if constexpr (KW <= 2) {
       if (a.dir) {
-        if (g->nitems > 0) ms::k_push<KW><<<gi, ms::kTPB, 0, m.cap>>>(a);
+        // a warp per work item (gi counts block rows on slice graphs)
+        if (g->nitems > 0) ms::k_push<KW><<<blocks_for_warps(g->nitems, ms::kWarps), ms::kTPB, 0, m.cap>>>(a);
         ms::k_push_fin<KW><<<gr, ms::kTPB, 0, m.cap>>>(a);
       }
     }
@@ -113,13 +119,7 @@ int ms_capture(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
         if (rws && g->rws_nchunk > 0)
           cudaMemsetAsync(m.long_acc, 0, sizeof(uint32_t) * (size_t)g->rws_nlong * KW, m.cap);
       } else {
-        if (rws && g->rws_nchunk > 0)
-          ms::k_long_chunks_wide<KW><<<blocks_for_warps(std::min<long long>(g->rws_nchunk, 1 << 20), ms::kWarps),
-                                       ms::kTPB, 0, m.cap>>>(a);
-        if (rws) ms::k_step_rws_wide<KW><<<gi, ms::kTPB, 0, m.cap>>>(a);
-        else ms::k_step<KW><<<gi, ms::kTPB, 0, m.cap>>>(a);
-        if (rws && g->rws_nchunk > 0)
-          cudaMemsetAsync(m.long_acc, 0, sizeof(uint32_t) * (size_t)g->rws_nlong * KW, m.cap);
+        ms::k_step<KW><<<gi, ms::kTPB, 0, m.cap>>>(a);
       }
     }
     if (a.dir) ms::k_finish<KW><<<gs, ms::kTPB, 0, m.cap>>>(af);
@@ -158,8 +158,12 @@ int msbfs_impl(gbo_graph* g, const int* h_srcs, int k, int32_t* d_levels, int* h
     m.live = static_cast<const uint32_t*>(lv);
   }
   GBO_TRY(build_rws(g, s));
-  if (!m.long_acc && g->rws_head) {  // sized for the widest frontier rows (32 words)
-    const size_t lw = (size_t)(g->rws_nlong > 0 ? g->rws_nlong : 1) * 32;
+  if (!m.active) {
+    GBO_CUDA_TRY(cudaMalloc(&m.active, sizeof(uint32_t) * 64));
+    m.slot_any = m.active + 32;
+  }
+  if (!m.long_acc && g->rws_head) {  // slice steps: frontier rows of up to 2 words
+    const size_t lw = (size_t)(g->rws_nlong > 0 ? g->rws_nlong : 1) * 2;
     GBO_CUDA_TRY(cudaMalloc(&m.long_acc, sizeof(uint32_t) * lw));
     GBO_CUDA_TRY(cudaMemsetAsync(m.long_acc, 0, sizeof(uint32_t) * lw, s));
   }
@@ -236,9 +240,6 @@ int msbfs_impl(gbo_graph* g, const int* h_srcs, int k, int32_t* d_levels, int* h
       m.step_ms.push_back(ms);
     }
     it0 = it1;
-    if (m.h_ctl[9])
-      return fail(GBO_ERR_BOUNDS, "multi-source step check " + std::to_string(m.h_ctl[9]) + " at index " +
-                                      std::to_string(m.h_ctl[10]));
     if (m.h_ctl[1]) {
       done = true;
       break;
@@ -304,6 +305,7 @@ void free_ms_state(gbo_graph* g) {
   cudaFree(m->slot_split);
   cudaFree(m->push_acc);
   cudaFree(m->long_acc);
+  cudaFree(m->active);
   cudaFree(m->srcs);
   cudaFree(m->ctl);
   cudaFreeHost(m->h_ctl);

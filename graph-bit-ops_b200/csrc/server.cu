@@ -510,7 +510,7 @@ int bfs_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
   GBO_CUDA_TRY(cudaMemsetAsync(S->slot_any, 0, sizeof(uint32_t) * S->kw, st));
   // up to 64 slots with row-word slices: the row-walking step (whole block
   // rows, so no split partials for the finish kernel)
-  const bool rws = S->g->rws_head != nullptr;
+  const bool rws = KW <= 2 && S->g->rws_head != nullptr;
   ms::Args af = a;
   if (rws) af.v.nsplit = 0;
   const unsigned gi = rws ? blocks_for_warps(S->nbr > 0 ? S->nbr : 1, ms::kWarps)
@@ -528,15 +528,7 @@ int bfs_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
       if (rws && S->g->rws_nchunk > 0)
         GBO_CUDA_TRY(cudaMemsetAsync(S->long_acc, 0, sizeof(uint32_t) * (size_t)S->g->rws_nlong * KW, st));
     } else {
-      if (rws && S->g->rws_nchunk > 0) {
-        ms::k_long_chunks_wide<KW><<<blocks_for_warps(std::min<long long>(S->g->rws_nchunk, 1 << 20), ms::kWarps),
-                                     ms::kTPB, 0, st>>>(a);
-        S->launches++;
-      }
-      if (rws) ms::k_step_rws_wide<KW><<<gi, ms::kTPB, 0, st>>>(a);
-      else ms::k_step<KW><<<gi, ms::kTPB, 0, st>>>(a);
-      if (rws && S->g->rws_nchunk > 0)
-        GBO_CUDA_TRY(cudaMemsetAsync(S->long_acc, 0, sizeof(uint32_t) * (size_t)S->g->rws_nlong * KW, st));
+      ms::k_step<KW><<<gi, ms::kTPB, 0, st>>>(a);
     }
   }
   ms::k_finish<KW><<<gs, ms::kTPB, 0, st>>>(af);
@@ -954,10 +946,10 @@ extern "C" int gbo_server_create(const gbo_graph* gc, int bfs_slots, int ppr_slo
         if (st != GBO_OK) throw st;
         S->live = static_cast<const uint32_t*>(lv);
       }
-      {  // rounds walk the row-word slices
+      {  // rounds of up to 64 slots walk the row-word slices
         const int st = build_rws(g, S->s[0]);
         if (st != GBO_OK) throw st;
-        const size_t lw = (size_t)(g->rws_nlong > 0 ? g->rws_nlong : 1) * (size_t)kw;
+        const size_t lw = (size_t)(g->rws_nlong > 0 ? g->rws_nlong : 1) * (size_t)std::min(kw, 2);
         cu(cudaMalloc(&S->long_acc, sizeof(uint32_t) * lw), "long_acc");
         cu(cudaMemsetAsync(S->long_acc, 0, sizeof(uint32_t) * lw, S->s[0]), "long_acc");
       }

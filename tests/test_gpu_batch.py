@@ -85,6 +85,27 @@ def test_msbfs_push_levels_split_rows(gbo, orc, gpu):
         assert np.array_equal(lv, want), push
 
 
+def test_msbfs_push_covers_every_work_item(gbo, orc, gpu):
+    """More work items than block rows (hub block row split into pieces) at a
+    block-row count that fills whole blocks: every item must be pushed."""
+    n = 32768  # 1024 block rows = 128 blocks of 8 warps
+    hubs = np.repeat(np.arange(10, dtype=np.int32), n - 10)
+    leaves = np.tile(np.arange(10, n, dtype=np.int32), 10)
+    rng = np.random.default_rng(5)
+    src = np.concatenate([hubs, rng.integers(0, n, 20000)]).astype(np.int32)
+    dst = np.concatenate([leaves, rng.integers(0, n, 20000)]).astype(np.int32)
+    csr = gbo.csr_from_edges(src, dst, n, True, True)
+    g = gbo.Graph.from_csr(csr, 32, gbo.FLAG_SYMMETRIC)
+    assert g.info().nsplit_rows > 0 and g.info().nitems > 1024
+    srcs = rng.integers(0, n, 64).astype(np.int32)
+    want = oracle_levels(orc, csr, srcs)
+    for push in (2**31 - 1, 4096, 0):
+        g.set_bfs_direction(True, push)
+        lv, _ = g.msbfs(srcs)
+        assert np.array_equal(lv, want), push
+    g.free()
+
+
 def test_msbfs_rejects_other_tiles(gbo, gpu):
     g = gbo.Graph.from_csr(gbo.gen_er(200, 0.05, 1), 16)
     with pytest.raises(gbo.GboError) as e:
