@@ -351,6 +351,17 @@ __device__ __forceinline__ unsigned long long pull_rws_level(const GView& v, uns
       z[Rl] = 0u;
     }
     unsigned openb = __ballot_sync(kFull, visl != kFull);
+    // with COH (the cooperative kernel, which has the registers) the first
+    // four head entries of the next open block row are loaded while the
+    // current one is walked
+    uint2 pf[4];
+    if (COH && openb) {
+      const int j0 = __ffs(openb) - 1;
+      const bool n0 = !((__shfl_sync(kFull, visl, j0) >> (31 - lane)) & 1u);
+      const uint2* h0 = v.rws_head + (size_t)(base + (long long)j0 * nwarps) * (kRwsHead * 32) + lane;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) pf[q] = n0 ? h0[(size_t)q * 32] : make_uint2(kRwsNone, 0u);
+    }
     while (openb) {
       const int j = __ffs(openb) - 1;
       openb &= openb - 1;
@@ -359,14 +370,31 @@ __device__ __forceinline__ unsigned long long pull_rws_level(const GView& v, uns
       bool need = !((vis >> (31 - lane)) & 1u);
       bool hit = false;
       const uint2* __restrict__ hp = v.rws_head + (size_t)R * (kRwsHead * 32) + lane;
+      uint2 cur[4];
+      if constexpr (COH) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) cur[q] = pf[q];
+        if (openb) {
+          const int jn = __ffs(openb) - 1;
+          const bool nn = !((__shfl_sync(kFull, visl, jn) >> (31 - lane)) & 1u);
+          const uint2* hn = v.rws_head + (size_t)(base + (long long)jn * nwarps) * (kRwsHead * 32) + lane;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) pf[q] = nn ? hn[(size_t)q * 32] : make_uint2(kRwsNone, 0u);
+        }
+      }
       // four entries per round: most rows of a dense level are answered by
       // the first round, so its loads are issued together
 #pragma unroll
       for (int k = 0; k < kRwsHead; k += 4) {
         if (!__any_sync(kFull, need)) break;
         uint2 e[4];
+        if (COH && k == 0) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) e[q] = need ? hp[(size_t)(k + q) * 32] : make_uint2(kRwsNone, 0u);
+          for (int q = 0; q < 4; ++q) e[q] = cur[q];
+        } else {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) e[q] = need ? hp[(size_t)(k + q) * 32] : make_uint2(kRwsNone, 0u);
+        }
         unsigned a = 0u;
 #pragma unroll
         for (int q = 0; q < 4; ++q) a |= e[q].x != kRwsNone ? (e[q].y & ld_state<COH>(x + e[q].x)) : 0u;
@@ -1010,8 +1038,8 @@ __device__ __forceinline__ unsigned long long push_rws_long(const GView& v, unsi
   return cnt;
 }
 
-__global__ void __launch_bounds__(kTPB, 6) k_bfs_coop(GView v, unsigned* front, unsigned* visited, int* level,
-                                                   Ctrl* ctrl, long long* push_list) {
+__global__ void __launch_bounds__(kTPB, kCoopBlocksPerSM) k_bfs_coop(GView v, unsigned* front, unsigned* visited,
+                                                                  int* level, Ctrl* ctrl, long long* push_list) {
   volatile Ctrl* vc = ctrl;
   if (vc->done) return;
   int lvl = vc->iter;
@@ -1167,6 +1195,30 @@ __device__ __forceinline__ double pr_entries4(const uint2 (&e)[4], const float* 
   return a;
 }
 
+// The whole head (eight entries) at once: PageRank reads every entry of a
+// row, so the second half is not worth a round trip of its own.
+__device__ __forceinline__ double pr_entries8(const uint2 (&e)[8], const float* __restrict__ xg) {
+  uint32_t m[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) m[u] = e[u].x != kRwsNone ? e[u].y : 0u;
+  double a = 0.0;
+  while (m[0] | m[1] | m[2] | m[3] | m[4] | m[5] | m[6] | m[7]) {
+    float g[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      g[u] = 0.f;
+      if (m[u]) {
+        const int j = __clz(m[u]);
+        m[u] &= ~(0x80000000u >> j);
+        g[u] = __ldg(xg + (size_t)e[u].x * 32 + j);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) a += (double)g[u];
+  }
+  return a;
+}
+
 struct PrIter {  // the iterate's buffers and coefficients of iteration itn
   const float* x;
   float* y;
@@ -1198,28 +1250,18 @@ __global__ void __launch_bounds__(kTPB) k_pr_step_rws(GView v, float* __restrict
   const int n = v.nrows;
   const PrIter P = pr_iter(pr, prs, ctrl, n);
   const unsigned lane = threadIdx.x & 31;
-  const unsigned kFull = 0xffffffffu;
   double e = 0.0;
   const long long nwarps = warps_total();
   for (long long R = warp_global(); R < v.nbr; R += nwarps) {
     const long long row = R * 32 + lane;
     const uint2* __restrict__ hp = v.rws_head + (size_t)R * (kRwsHead * 32) + lane;
-    double a = 0.0;
-    bool more = true;
+    // the head's eight entries and the tail offsets in one round of loads
+    static_assert(kRwsHead == 8, "pr_entries8 takes the whole head");
+    uint2 h8[8];
 #pragma unroll
-    for (int k = 0; k < kRwsHead; k += 4) {
-      if (!__any_sync(kFull, more)) break;
-      uint2 e[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) e[u] = more ? hp[(size_t)(k + u) * 32] : make_uint2(kRwsNone, 0u);
-      a += pr_entries4(e, P.xg);
-      more = more && e[3].x != kRwsNone;
-    }
-    long long tb = 0, te = 0;
-    if (more) {
-      tb = v.rws_tail_ptr[row];
-      te = v.rws_tail_ptr[row + 1];
-    }
+    for (int u = 0; u < 8; ++u) h8[u] = hp[(size_t)u * 32];
+    const long long tb = v.rws_tail_ptr[row], te = v.rws_tail_ptr[row + 1];
+    double a = pr_entries8(h8, P.xg);
     const bool long_row = te - tb > kRwsLongTail;  // the chunk kernels own a long row
     if (!long_row) {
       for (long long p = tb; p < te; p += 4) {

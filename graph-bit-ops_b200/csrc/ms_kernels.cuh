@@ -419,7 +419,8 @@ __device__ __forceinline__ void or_entries4(const uint32_t* __restrict__ F, cons
 // Tails of long rows (more than kMsLongTail entries), a warp per chunk of
 // kRwsChunk entries: the frontier rows of the chunk's frontier neighbours
 // OR-ed into the row's long_acc words, the chunk left early once the row is
-// covered.  Runs before k_step_rws in every pull level.
+// covered.  Runs before k_step_rws in every pull level, on a resident grid
+// (warps stride over the chunks).
 template <int KW>
 __global__ void __launch_bounds__(kTPB) k_long_chunks(Args a) {
   volatile int* c = a.ctl;

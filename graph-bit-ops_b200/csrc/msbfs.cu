@@ -112,7 +112,7 @@ int ms_capture(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
     if (g->nitems > 0) {
       if constexpr (KW <= 2) {
         if (rws && g->rws_nchunk > 0)
-          ms::k_long_chunks<KW><<<blocks_for_warps(std::min<long long>(g->rws_nchunk, 1 << 20), ms::kWarps),
+          ms::k_long_chunks<KW><<<std::min(blocks_for_warps(g->rws_nchunk, ms::kWarps), (unsigned)num_sms() * 8u),
                                   ms::kTPB, 0, m.cap>>>(a);
         if (rws) ms::k_step_rws<KW><<<gi, ms::kTPB, 0, m.cap>>>(a);
         else ms::k_step<KW><<<gi, ms::kTPB, 0, m.cap>>>(a);

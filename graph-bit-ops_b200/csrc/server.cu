@@ -519,7 +519,7 @@ int bfs_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
   if (S->g->nitems > 0) {
     if constexpr (KW <= 2) {
       if (rws && S->g->rws_nchunk > 0) {
-        ms::k_long_chunks<KW><<<blocks_for_warps(std::min<long long>(S->g->rws_nchunk, 1 << 20), ms::kWarps),
+        ms::k_long_chunks<KW><<<std::min(blocks_for_warps(S->g->rws_nchunk, ms::kWarps), (unsigned)num_sms() * 8u),
                                 ms::kTPB, 0, st>>>(a);
         S->launches++;
       }
