@@ -42,13 +42,14 @@ struct Ctrl {
   // and its iteration end times (globaltimer ns; [0] = loop start)
   unsigned long long cond;
   unsigned long long* stamps;
-  // cooperative BFS: grid barrier (arrivals, generation, give-up flag) and
-  // the new-vertex counts of three consecutive levels
+  // cooperative BFS: grid barrier (arrival word, give-up flag) and the
+  // new-vertex counts of three consecutive levels
   unsigned bar_arrive;
-  unsigned bar_gen;
   unsigned bar_err;
-  unsigned long long lvl_count[3];
   unsigned long long push_acc[3];  // push list: rows << 40 | tail entries
+  // new-vertex counts of three consecutive levels, each spread over eight
+  // counters on their own 128-byte lines (block b adds into counter b % 8)
+  unsigned long long lvl_part[3][8][16];
 };
 
 // Iteration end times kept per loop run (more iterations run untimed).
@@ -856,8 +857,9 @@ __global__ void k_bfs_init(typename Word<B>::T* front, typename Word<B>::T* visi
     ctrl->work = 0ull;
     ctrl->bar_arrive = 0u;
     ctrl->bar_err = 0u;
-    for (int q = 0; q < 3; ++q) ctrl->lvl_count[q] = ctrl->push_acc[q] = 0ull;
+    for (int q = 0; q < 3; ++q) ctrl->push_acc[q] = 0ull;
   }
+  if (i < 3 * 8) ctrl->lvl_part[i / 8][i % 8][0] = 0ull;
 }
 
 // --------------------------------------------- cooperative BFS (b = 32)
@@ -898,40 +900,43 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-// Barrier over every block of a cooperative launch (arrival count and
-// generation in Ctrl; the last block to arrive resets the count and bumps
-// the generation).  A block that waits past the limit, or sees that another
-// block gave up, sets bar_err and returns false: the caller leaves the
-// kernel, so every block ends within about one limit of the first failure.
-__device__ __forceinline__ bool grid_barrier(Ctrl* c) {
+// Barrier over every block of a cooperative launch on one arrival word:
+// block 0 adds 2^31 - (blocks - 1), every other block adds 1, so the sum of
+// one barrier's arrivals flips the word's top bit and leaves the low bits
+// as they were -- the block that arrives last completes the flip, with no
+// reset or second atomic on the way out.  A block that waits past the limit,
+// or sees that another block gave up, sets bar_err and returns false: the
+// caller leaves the kernel, so every block ends within about one limit of
+// the first failure.
+__device__ __forceinline__ bool grid_barrier(Ctrl* c, const unsigned long long* sum_src = nullptr, int nsum = 0,
+                                             int sum_stride = 1, unsigned long long* sum = nullptr) {
   __shared__ int ok;
+  __shared__ unsigned long long sh_sum;
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned* gen = &c->bar_gen;
+    const unsigned inc = blockIdx.x == 0 ? 0x80000000u - (gridDim.x - 1u) : 1u;
+    volatile unsigned* word = &c->bar_arrive;
     volatile unsigned* err = &c->bar_err;
-    const unsigned g0 = *gen;
     __threadfence();
-    const unsigned t = atomicAdd(&c->bar_arrive, 1u);
+    const unsigned old = atomicAdd(&c->bar_arrive, inc);
     int res = 1;
-    if (t == gridDim.x - 1) {
-      atomicExch(&c->bar_arrive, 0u);
-      __threadfence();
-      atomicAdd(&c->bar_gen, 1u);
-    } else {
-      const unsigned long long t0 = global_ns();
-      for (long long k = 0; *gen == g0; ++k) {
-        if (*err || k >= kBarrierPollCap || global_ns() - t0 > kBarrierLimitNs) {
-          atomicExch(&c->bar_err, 1u);
-          res = 0;
-          break;
-        }
-        __nanosleep(32);
+    const unsigned long long t0 = global_ns();
+    for (long long k = 0; ((old ^ *word) & 0x80000000u) == 0u; ++k) {
+      if (*err || k >= kBarrierPollCap || global_ns() - t0 > kBarrierLimitNs) {
+        atomicExch(&c->bar_err, 1u);
+        res = 0;
+        break;
       }
     }
     __threadfence();
     ok = res;
+    // one read of the counters per block, shared with its threads
+    unsigned long long t = 0;
+    for (int q = 0; q < nsum; ++q) t += __ldcg(sum_src + (size_t)q * sum_stride);
+    sh_sum = t;
   }
   __syncthreads();
+  if (sum) *sum = sh_sum;
   return ok != 0;
 }
 
@@ -1040,31 +1045,34 @@ __device__ __forceinline__ unsigned long long push_rws_long(const GView& v, unsi
 
 __global__ void __launch_bounds__(kTPB, kCoopBlocksPerSM) k_bfs_coop(GView v, unsigned* front, unsigned* visited,
                                                                   int* level, Ctrl* ctrl, long long* push_list) {
+  // the loop's starting state: written before the launch and changed by
+  // block 0 only after the first barrier, so plain (cached) loads -- one
+  // L2 request per SM instead of one per warp
   volatile Ctrl* vc = ctrl;
-  if (vc->done) return;
-  int lvl = vc->iter;
-  int mode = vc->mode;
-  const int max_iter = vc->max_iter;
-  const unsigned long long push_thr = vc->push_thr > 0 ? (unsigned long long)vc->push_thr : 0ull;
-  unsigned long long* stamps = vc->stamps;
+  if (ctrl->done) return;
+  int lvl = ctrl->iter;
+  int mode = ctrl->mode;
+  const int max_iter = ctrl->max_iter;
+  const unsigned long long push_thr = ctrl->push_thr > 0 ? (unsigned long long)ctrl->push_thr : 0ull;
+  unsigned long long* stamps = ctrl->stamps;
   for (;;) {
     unsigned long long cnt;
     if (!mode) {
       cnt = pull_rws_level<true>(v, front, visited, level, lvl);
     } else {
       cnt = push_rws_rows(v, front, visited, level, lvl, &ctrl->push_acc[lvl % 3], push_list);
-      if (!grid_barrier(ctrl)) return;
-      const unsigned long long acc = __ldcg(&ctrl->push_acc[lvl % 3]);
+      unsigned long long acc = 0;
+      if (!grid_barrier(ctrl, &ctrl->push_acc[lvl % 3], 1, 1, &acc)) return;
       if (acc) cnt += push_rws_long(v, front, visited, level, lvl, acc, push_list);
     }
-    block_add_u64(cnt, &ctrl->lvl_count[lvl % 3]);
-    if (!grid_barrier(ctrl)) return;
-    const unsigned long long nf = __ldcg(&ctrl->lvl_count[lvl % 3]);
+    block_add_u64(cnt, &ctrl->lvl_part[lvl % 3][blockIdx.x & 7][0]);
+    unsigned long long nf = 0;
+    if (!grid_barrier(ctrl, &ctrl->lvl_part[lvl % 3][0][0], 8, 16, &nf)) return;
     const int it = lvl + 1;
     const bool stop = nf == 0ull || it >= max_iter;
     mode = (nf > 0ull && nf < push_thr) ? 1 : 0;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-      ctrl->lvl_count[(lvl + 2) % 3] = 0ull;
+      for (int q = 0; q < 8; ++q) ctrl->lvl_part[(lvl + 2) % 3][q][0] = 0ull;
       ctrl->push_acc[(lvl + 2) % 3] = 0ull;
       vc->iter = it;
       vc->mode = mode;
