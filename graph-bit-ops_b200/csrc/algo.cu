@@ -318,6 +318,11 @@ __global__ void __launch_bounds__(kTPB) k_bfs_step(GView v, typename Word<B>::T*
 // visited (k_live), so every open row has an entry.
 constexpr int kLongTail = kRwsLongTail;
 
+// The cooperative loop's level counts carry, above this bit, the number of
+// new vertices with long tails (hubs).
+constexpr int kLongShift = 40;
+constexpr unsigned long long kLongMask = (1ull << kLongShift) - 1ull;
+
 // Loads of the traversal state (frontier and visited words): through the
 // read-only path when the state only changes between launches; as plain
 // (weak, L1-cached) loads inside the cooperative BFS kernel, where other
@@ -446,6 +451,9 @@ __device__ __forceinline__ unsigned long long pull_rws_level(const GView& v, uns
           out[R] = nw;
           visited[R] = vis | nw;
           cnt += __popc(nw);
+          // the cooperative loop also counts the new vertices with long
+          // tails (a push level after this one skips its hub phase at none)
+          if (COH) cnt += (unsigned long long)__popc(nw & v.rws_longbits[R]) << kLongShift;
         }
         if ((nw >> (31 - lane)) & 1u) level[R * 32 + lane] = lvl + 1;
       }
@@ -942,15 +950,17 @@ __device__ __forceinline__ bool grid_barrier(Ctrl* c, const unsigned long long* 
 
 // Push one row word into next-frontier word C; the vertices this call finds
 // first are marked visited and get level lvl + 1.  Returns their number.
-__device__ __forceinline__ unsigned push_word(unsigned* out, unsigned* visited, int* level, int lvl, unsigned C,
-                                              unsigned w) {
+// Returns their number plus, shifted by kLongShift, how many of them have
+// long tails.
+__device__ __forceinline__ unsigned long long push_word(const GView& v, unsigned* out, unsigned* visited,
+                                                        int* level, int lvl, unsigned C, unsigned w) {
   const unsigned cand = w & ~visited[C];
-  if (!cand) return 0u;
+  if (!cand) return 0ull;
   const unsigned nw = cand & ~atomicOr(out + C, cand);
-  if (!nw) return 0u;
+  if (!nw) return 0ull;
   atomicOr(visited + C, nw);
   for (unsigned m = nw; m; m &= m - 1) level[(long long)C * 32 + (32 - __ffs(m))] = lvl + 1;
-  return (unsigned)__popc(nw);
+  return (unsigned long long)__popc(nw) + ((unsigned long long)__popc(nw & v.rws_longbits[C]) << kLongShift);
 }
 
 // Push phase A: block rows with frontier bits (a lane per block row picks
@@ -1011,7 +1021,7 @@ __device__ __forceinline__ unsigned long long push_rws_rows(const GView& v, unsi
         if (q < total) {
           const int slot = q - (rin - rlen);
           const uint2 e = slot < kRwsHead ? hb[(size_t)slot * 32 + r] : v.rws_tail[rtb + (slot - kRwsHead)];
-          if (e.x != kRwsNone) cnt += push_word(out, visited, level, lvl, e.x, e.y);
+          if (e.x != kRwsNone) cnt += push_word(v, out, visited, level, lvl, e.x, e.y);
         }
       }
     }
@@ -1038,7 +1048,7 @@ __device__ __forceinline__ unsigned long long push_rws_long(const GView& v, unsi
       else hi = mid - 1;
     }
     const uint2 e = v.rws_tail[list[2 * lo + 1] + (q - list[2 * lo])];
-    cnt += push_word(out, visited, level, lvl, e.x, e.y);
+    cnt += push_word(v, out, visited, level, lvl, e.x, e.y);
   }
   return cnt;
 }
@@ -1055,19 +1065,24 @@ __global__ void __launch_bounds__(kTPB, kCoopBlocksPerSM) k_bfs_coop(GView v, un
   const int max_iter = ctrl->max_iter;
   const unsigned long long push_thr = ctrl->push_thr > 0 ? (unsigned long long)ctrl->push_thr : 0ull;
   unsigned long long* stamps = ctrl->stamps;
+  bool hubs = true;  // the frontier may hold rows with long tails (unknown at the start)
   for (;;) {
     unsigned long long cnt;
     if (!mode) {
       cnt = pull_rws_level<true>(v, front, visited, level, lvl);
     } else {
       cnt = push_rws_rows(v, front, visited, level, lvl, &ctrl->push_acc[lvl % 3], push_list);
-      unsigned long long acc = 0;
-      if (!grid_barrier(ctrl, &ctrl->push_acc[lvl % 3], 1, 1, &acc)) return;
-      if (acc) cnt += push_rws_long(v, front, visited, level, lvl, acc, push_list);
+      if (hubs) {  // the listed long tails, after every block listed its rows
+        unsigned long long acc = 0;
+        if (!grid_barrier(ctrl, &ctrl->push_acc[lvl % 3], 1, 1, &acc)) return;
+        if (acc) cnt += push_rws_long(v, front, visited, level, lvl, acc, push_list);
+      }
     }
     block_add_u64(cnt, &ctrl->lvl_part[lvl % 3][blockIdx.x & 7][0]);
-    unsigned long long nf = 0;
-    if (!grid_barrier(ctrl, &ctrl->lvl_part[lvl % 3][0][0], 8, 16, &nf)) return;
+    unsigned long long tot = 0;
+    if (!grid_barrier(ctrl, &ctrl->lvl_part[lvl % 3][0][0], 8, 16, &tot)) return;
+    const unsigned long long nf = tot & kLongMask;
+    hubs = (tot >> kLongShift) != 0ull;
     const int it = lvl + 1;
     const bool stop = nf == 0ull || it >= max_iter;
     mode = (nf > 0ull && nf < push_thr) ? 1 : 0;

@@ -519,6 +519,7 @@ GView view_of(const gbo_graph* g) {
   v.rws_chunk_row = g->rws_chunk_row;
   v.rws_chunk_beg = g->rws_chunk_beg;
   v.rws_chunk_end = g->rws_chunk_end;
+  v.rws_longbits = g->rws_longbits;
   return v;
 }
 

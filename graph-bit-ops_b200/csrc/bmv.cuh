@@ -35,6 +35,7 @@ struct GView {
   const int* __restrict__ rws_chunk_row = nullptr;
   const long long* __restrict__ rws_chunk_beg = nullptr;
   const long long* __restrict__ rws_chunk_end = nullptr;
+  const unsigned* __restrict__ rws_longbits = nullptr;
 };
 
 // Index in rowword of row r's word of a tile with occupancy word m whose

@@ -119,6 +119,7 @@ void destroy(gbo_graph* g) {
   cudaFree(g->rws_chunk_row);
   cudaFree(g->rws_chunk_beg);
   cudaFree(g->rws_chunk_end);
+  cudaFree(g->rws_longbits);
   cudaFree(g->invdeg);
   cudaFree(g->items);
   cudaFree(g->splits);

@@ -54,6 +54,7 @@ struct gbo_graph {
   int* rws_chunk_row = nullptr;        // row of every chunk
   long long* rws_chunk_beg = nullptr;  // tail entries [beg, end) of every chunk
   long long* rws_chunk_end = nullptr;
+  unsigned* rws_longbits = nullptr;    // nbr words: bit 31 - r set when row 32R + r is long
   int last_run_ms = 0;     // 1: the last traversal was a multi-source BFS
   bool tc_mma = false;     // GBO_FLAG_TC_MMA: dense 32x32 mask tiles on the 1-bit MMA
   bool owns_outdeg = true;

@@ -803,11 +803,13 @@ int build_rws(gbo_graph* g, cudaStream_t s) {
   GBO_CUDA_TRY(cudaMemcpyAsync(tp.data(), g->rws_tail_ptr, sizeof(long long) * tp.size(), cudaMemcpyDeviceToHost, s));
   GBO_CUDA_TRY(cudaStreamSynchronize(s));
   std::vector<int> lrow, crow;
+  std::vector<unsigned> lbits((size_t)g->nbr, 0u);
   std::vector<long long> lc0, cbeg, cend;
   for (long long i = 0; i < rows; ++i) {
     const long long len = tp[(size_t)i + 1] - tp[(size_t)i];
     if (len <= kRwsLongTail) continue;
     lrow.push_back((int)i);
+    lbits[(size_t)(i / 32)] |= 1u << (31 - i % 32);
     lc0.push_back((long long)cbeg.size());
     for (long long b = tp[(size_t)i]; b < tp[(size_t)i + 1]; b += kRwsChunk) {
       crow.push_back((int)i);
@@ -830,6 +832,7 @@ int build_rws(gbo_graph* g, cudaStream_t s) {
   GBO_TRY(up(&g->rws_chunk_row, crow));
   GBO_TRY(up(&g->rws_chunk_beg, cbeg));
   GBO_TRY(up(&g->rws_chunk_end, cend));
+  GBO_TRY(up(&g->rws_longbits, lbits));
   return GBO_OK;
 }
 
