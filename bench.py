@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--serve-qps", type=float, default=8000.0, help="offered BFS query rate")
     ap.add_argument("--serve-s", type=float, default=1.5, help="seconds of arrivals per stream")
     ap.add_argument("--serve-slots", type=int, default=256, help="BFS slots of the served streams' server")
+    ap.add_argument("--serve-admit", type=float, default=None,
+                    help="server BFS admission batching (free-slot fraction; default: the library's)")
     ap.add_argument("--tc-graphs", default="mesh,rmat", help="graphs of --workload tc (mesh, rmat)")
     ap.add_argument("--tc-variants", default="input,degree", help="vertex orders of --workload tc")
     ap.add_argument("--tc-tiles", default="8,16,32,64", help="tile widths of --workload tc")
@@ -420,7 +422,8 @@ def run_reference(args, ws, rank):
 
 
 # --------------------------------------------------------------- serving
-def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed, delivery="host", sample_every=0, slots=64):
+def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed, delivery="host", sample_every=0, slots=64,
+                 admit=None):
     """Poisson arrivals of BFS sources and PPR sets (1..64 vertices, Dirichlet
     weights) into the continuous-batching server.  `delivery`: "host" (int32
     levels in host memory, gbo_server_wait), "u8" (byte levels in pinned
@@ -446,6 +449,8 @@ def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed, delivery="host
         else:
             qs.append(("bfs", int(rng.integers(0, n))))
     srv = gbo.Server(g, bfs_slots=slots, ppr_slots=32 if ppr_frac > 0 else 0, alpha=0.85, tol=1e-7)
+    if admit is not None:
+        srv.set_admission(admit)
     # one queue and consumer pool per kind, so clients waiting on slow PPR
     # results never hold BFS results back (each pool collects in order)
     tq = {"bfs": queue.Queue(), "ppr": queue.Queue()}
@@ -535,7 +540,7 @@ def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed, delivery="host
     return out, samples
 
 
-def served_suite(gbo, g, n, plain_ms, rate, dur, check_fn, seed=5, slots=64):
+def served_suite(gbo, g, n, plain_ms, rate, dur, check_fn, seed=5, slots=64, admit=None):
     """Capacity of the server with each delivery (a stream offered above it),
     then streams offered at 50 % and 90 % of that capacity (p50/p99 of
     service latency, not of a queue), and a 10 % PPR mix.  Every stream's
@@ -544,7 +549,8 @@ def served_suite(gbo, g, n, plain_ms, rate, dur, check_fn, seed=5, slots=64):
     res = {"plain_bfs_qps": plain_qps, "qps_definition": "completed queries / (last completion - first arrival)"}
     ok = True
     for delivery, offered in (("device", 2.0 * rate), ("u8", rate), ("host", rate)):
-        cap, smp = serve_stream(gbo, g, n, offered, dur, 0.0, seed, delivery, sample_every=97, slots=slots)
+        cap, smp = serve_stream(gbo, g, n, offered, dur, 0.0, seed, delivery, sample_every=97, slots=slots,
+                                admit=admit)
         ok = ok and all(check_fn(src, lv) for src, lv in smp)
         cap["vs_plain_bfs_qps"] = cap["qps"] / plain_qps
         res[f"capacity_{delivery}"] = cap
@@ -552,11 +558,12 @@ def served_suite(gbo, g, n, plain_ms, rate, dur, check_fn, seed=5, slots=64):
             continue
         for frac in (0.5, 0.9):
             r, smp = serve_stream(gbo, g, n, frac * cap["qps"], dur, 0.0, seed + 1, delivery, sample_every=97,
-                                  slots=slots)
+                                  slots=slots, admit=admit)
             ok = ok and all(check_fn(src, lv) for src, lv in smp)
             r["vs_plain_bfs_qps"] = r["qps"] / plain_qps
             res[f"{delivery}_{int(frac * 100)}pct"] = r
-    mixed, smp = serve_stream(gbo, g, n, rate / 8, dur, 0.1, seed + 2, "u8", sample_every=13, slots=slots)
+    mixed, smp = serve_stream(gbo, g, n, rate / 8, dur, 0.1, seed + 2, "u8", sample_every=13, slots=slots,
+                              admit=admit)
     ok = ok and all(check_fn(src, lv) for src, lv in smp)
     res["mixed_10pct_ppr"] = mixed
     res["parity"] = {"checked": "every 97th BFS result of each stream (13th of the mix) against gbo_bfs of "
@@ -637,7 +644,7 @@ def run_ours(args, ws, rank, local):
     # loop graph of per-level kernels beside the cooperative launch
     other_loop = None
     if args.tile == 32 and args.layout == "row":
-        cur = g.last_run()["kernel_launches"] == 3  # the cooperative form launches 3 kernels
+        cur = g.last_run()["kernel_launches"] == 2  # the cooperative form launches 2 kernels
         g.set_bfs_loop(gbo.BFS_LOOP_GRAPH if cur else gbo.BFS_LOOP_COOP, args.coop_blocks)
         for _ in range(3):
             g.bfs(0, out=d_level)
@@ -800,7 +807,7 @@ def run_ours(args, ws, rank, local):
             return bool(np.array_equal(alone.to_numpy(np.int32, n), lv))
 
         served = served_suite(gbo, g_row, n, ms, args.serve_qps, args.serve_s, same_as_alone,
-                              slots=args.serve_slots)
+                              slots=args.serve_slots, admit=args.serve_admit)
         alone.free()
     wb = max(1, args.tile // 8)
     bmv_bytes = (int(info.nblocks) * (args.tile * args.tile // 8 + 4) + 4 * (info.nblockrows + 1)
@@ -1333,7 +1340,8 @@ def suite_serve(args):
     out = {}
     rates = [float(r) for r in args.serve_rates.split(",")]
     for rate in rates:
-        r, _ = serve_stream(gbo, g, n, rate, min(args.serve_s, 2e4 / rate), 0.1, 11, "u8", slots=args.serve_slots)
+        r, _ = serve_stream(gbo, g, n, rate, min(args.serve_s, 2e4 / rate), 0.1, 11, "u8", slots=args.serve_slots,
+                            admit=args.serve_admit)
         r["bfs_vs_plain"] = r.get("bfs_qps", 0.0) / plain["bfs_qps"]
         r["ppr_vs_plain"] = r.get("ppr_qps", 0.0) / plain["ppr_qps"]
         out[int(rate)] = r

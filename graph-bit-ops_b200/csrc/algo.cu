@@ -840,7 +840,8 @@ __global__ void k_bfs_seed(const int* __restrict__ seeds, int nseeds, typename W
 template <int B>
 __global__ void k_bfs_init(typename Word<B>::T* front, typename Word<B>::T* visited, int* level,
                            const typename Word<B>::T* __restrict__ live, int nbr, int n, int src,
-                           Ctrl* ctrl, int max_iter, int push_thr, int mode0) {
+                           Ctrl* ctrl, int max_iter, int push_thr, int mode0,
+                           unsigned long long* stamps = nullptr, int cap_iters = 0) {
   using WT = typename Word<B>::T;
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -856,7 +857,14 @@ __global__ void k_bfs_init(typename Word<B>::T* front, typename Word<B>::T* visi
     ctrl->iter = 0;
     ctrl->done = 0;
     ctrl->ticket = 0;
-    ctrl->max_iter = max_iter;
+    ctrl->max_iter = cap_iters > 0 && cap_iters < max_iter ? cap_iters : max_iter;
+    if (stamps) {  // the cooperative loop's start
+      ctrl->cond = 0ull;
+      ctrl->stamps = stamps;
+      unsigned long long t;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+      stamps[0] = t;
+    }
     ctrl->count = 0;
     ctrl->err = 0;
     ctrl->last_err = 0;
@@ -1825,7 +1833,7 @@ int coop_grid(const gbo_graph* g, unsigned* grid) {
 
 // The BFS level loop as one cooperative launch (k_bfs_coop) on s.
 int run_bfs_coop(gbo_graph* g, AlgoState* a, const GView& v, unsigned* front, unsigned* vis, int* level,
-                 cudaStream_t s, int max_iter, int* iters) {
+                 cudaStream_t s, int max_iter, int cap_iters, int* iters) {
   unsigned grid = 0;
   GBO_TRY(coop_grid(g, &grid));
   if (!a->push_list) {
@@ -1834,14 +1842,11 @@ int run_bfs_coop(gbo_graph* g, AlgoState* a, const GView& v, unsigned* front, un
     g->device_bytes += (long long)nb;
   }
   long long* list = a->push_list;
-  const int cap_iters = injected_cap_iters();
-  k_loop_begin<<<1, 32, 0, s>>>(a->ctrl, 0ull, a->stamps, cap_iters);
-  GBO_CUDA_TRY(cudaGetLastError());
   GView va = v;
   Ctrl* ctrl = a->ctrl;
   void* args[] = {&va, &front, &vis, &level, &ctrl, &list};
   GBO_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_bfs_coop, dim3(grid), dim3(kTPB), args, 0, s));
-  a->fixed_launches = 3;  // init, loop start and the cooperative loop
+  a->fixed_launches = 2;  // init and the cooperative loop
   a->launches_per_iter = 0;
   return finish_loop(a, s, max_iter, cap_iters, iters, true);
 }
@@ -1884,7 +1889,6 @@ int bfs_impl(gbo_graph* g, int src, const int* h_seeds, int nseeds, int32_t* d_l
   WT* front = (WT*)a->front;
   WT* vis = (WT*)a->visited;
   Ctrl* ctrl = a->ctrl;
-  int* level = a->level;
   WT* scratch = (WT*)a->scratch;
   // the COL tile layout has its own pull and push kernels (column words)
   const bool col = g->layout == GBO_LAYOUT_COL;
@@ -1898,6 +1902,12 @@ int bfs_impl(gbo_graph* g, int src, const int* h_seeds, int nseeds, int32_t* d_l
                     (g->bfs_loop == GBO_BFS_LOOP_COOP || (g->bfs_loop == GBO_BFS_LOOP_AUTO && kCoopBfsDefault));
   if (g->bfs_loop == GBO_BFS_LOOP_COOP && !rws)
     return fail(GBO_ERR_UNSUPPORTED, "the cooperative BFS loop needs a b = 32 ROW graph");
+  // the cooperative loop writes the caller's level array itself; the loop
+  // graph (captured once) writes the graph's own and copies it out
+  int* level = coop ? d_level : a->level;
+  // cooperative loop: the init kernel also starts the step clock and
+  // applies an injected iteration cap (no loop-start kernel)
+  const int cap_iters = coop ? injected_cap_iters() : 0;
   // the slice pull step finishes every block row itself: no split partials
   GView vfin = v;
   if (rws) vfin.nsplit = 0;
@@ -1931,7 +1941,7 @@ int bfs_impl(gbo_graph* g, int src, const int* h_seeds, int nseeds, int32_t* d_l
   const int nstart = src >= 0 ? 1 : nseeds;
   k_bfs_init<B><<<grid_vertex(std::max(g->nrows, g->nbr)), kTPB, 0, s>>>(
       front, vis, level, (const WT*)a->live, g->nbr, g->nrows, src, ctrl, max_iter, push_thr,
-      push_ok && nstart < push_thr ? 1 : 0);
+      push_ok && nstart < push_thr ? 1 : 0, coop ? a->stamps : nullptr, cap_iters);
   if (src < 0) {
     if (a->nseeds_cap < nseeds) {
       cudaFree(a->seeds);
@@ -1950,13 +1960,13 @@ int bfs_impl(gbo_graph* g, int src, const int* h_seeds, int nseeds, int32_t* d_l
   if (coop) {
     if constexpr (B == 32)
       GBO_TRY(run_bfs_coop(g, a, v, reinterpret_cast<unsigned*>(front), reinterpret_cast<unsigned*>(vis), level,
-                           s, max_iter, h_depth ? &iters : nullptr));
+                           s, max_iter, cap_iters, h_depth ? &iters : nullptr));
   } else {
     GBO_TRY(run_until_done(a, A_BFS, s, max_iter, h_depth ? &iters : nullptr));
+    if (g->nrows > 0)
+      GBO_CUDA_TRY(cudaMemcpyAsync(d_level, level, sizeof(int) * (size_t)g->nrows,
+                                   cudaMemcpyDeviceToDevice, s));
   }
-  if (g->nrows > 0)
-    GBO_CUDA_TRY(cudaMemcpyAsync(d_level, level, sizeof(int) * (size_t)g->nrows,
-                                 cudaMemcpyDeviceToDevice, s));
   if (h_depth) *h_depth = iters;
   return GBO_OK;
 }

@@ -16,6 +16,7 @@
 #include <chrono>
 #include <condition_variable>
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <deque>
 #include <map>
@@ -395,6 +396,7 @@ struct gbo_server {
   gbo_graph* g = nullptr;
   int n = 0, nbr = 0;
   long long max_pending = 0;  // per engine; 0 = unbounded (gbo_server_set_queue_limit)
+  float bfs_admit_free = 0.5f;  // gbo_server_set_admission
   uint32_t* long_acc = nullptr;  // up to 64 slots: long-row tail gathers (ms::Args::long_acc)
   float alpha = 0.85f, tol = 1e-7f;
   int ppr_max_iter = 1000;
@@ -761,6 +763,14 @@ void worker_main(gbo_server* S, int kind) {
     for (long long t : tab) inflight += t > 0;
     return (long long)S->pool_free[rpool].size() - inflight;
   };
+  // BFS admission batching (gbo_server_set_admission): enough free slots,
+  // or nothing left traversing
+  auto batch_ready = [&]() {
+    long long nfree = 0;
+    for (long long t : tab) nfree += t == 0;
+    const double need = std::ceil((double)S->bfs_admit_free * (double)tab.size());
+    return (double)nfree >= std::max(need, 1.0) || !unfinished();
+  };
   double stall_since = -1.0;
   while (true) {
     std::vector<std::pair<int, Query>> adm;
@@ -770,7 +780,8 @@ void worker_main(gbo_server* S, int kind) {
         if (S->stop || S->worker_status != GBO_OK) return;
         const int bp = blocked_pool(S, kind);
         if (bp >= 0) move_results_to_host(S, bp, lk);
-        const bool can_admit = !S->pending[kind].empty() && budget() > 0 && !inject_server_hold();
+        const bool can_admit = !S->pending[kind].empty() && budget() > 0 && !inject_server_hold() &&
+                               (kind != 0 || batch_ready());
         const bool work = can_admit || unfinished() || (occupied() && blocked_pool(S, kind) < 0);
         if (work) {
           stall_since = -1.0;
@@ -1029,6 +1040,15 @@ extern "C" int gbo_server_set_queue_limit(gbo_server* S, long long max_pending) 
   if (!S || max_pending < 0) return fail(GBO_ERR_INVALID, "bad argument");
   std::lock_guard<std::mutex> lk(S->mu);
   S->max_pending = max_pending;
+  return GBO_OK;
+}
+
+extern "C" int gbo_server_set_admission(gbo_server* S, float min_free_fraction) {
+  clear_error();
+  if (!S || !(min_free_fraction >= 0.f && min_free_fraction <= 1.f)) return fail(GBO_ERR_INVALID, "bad argument");
+  std::lock_guard<std::mutex> lk(S->mu);
+  S->bfs_admit_free = min_free_fraction;
+  S->cv_work.notify_all();
   return GBO_OK;
 }
 

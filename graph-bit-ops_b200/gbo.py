@@ -178,6 +178,7 @@ _SIGS = {
     "gbo_bfs_multi": (_I, [_P, _P, _I, _P, C.POINTER(_I), _P]),
     "gbo_server_create": (_I, [_P, _I, _I, C.c_float, C.c_float, _I, C.POINTER(_P)]),
     "gbo_server_set_queue_limit": (_I, [_P, C.c_longlong]),
+    "gbo_server_set_admission": (_I, [_P, C.c_float]),
     "gbo_server_submit_bfs": (_I, [_P, _I, C.POINTER(C.c_int64)]),
     "gbo_server_submit_ppr": (_I, [_P, _P, _P, _I, C.POINTER(C.c_int64)]),
     "gbo_server_poll": (_I, [_P, C.c_int64, _P, C.POINTER(C.c_double), C.POINTER(_I)]),
@@ -779,6 +780,11 @@ class Server:
         """Submissions past max_pending queries not yet admitted return
         GBO_ERR_FULL (0: unbounded)."""
         check(lib().gbo_server_set_queue_limit(self.h, int(max_pending)), "server_set_queue_limit")
+
+    def set_admission(self, min_free_fraction: float) -> None:
+        """Pending BFS queries enter when at least this fraction of the slots
+        is free or the engine is idle (0: every round, 1: batch after batch)."""
+        check(lib().gbo_server_set_admission(self.h, C.c_float(min_free_fraction)), "server_set_admission")
 
     def submit_bfs(self, src: int) -> int:
         t = C.c_int64(0)

@@ -494,6 +494,13 @@ GBO_API int gbo_server_create(const gbo_graph* g, int bfs_slots, int ppr_slots,
  * default).  The reference has no server; this is its request-overflow
  * policy. */
 GBO_API int gbo_server_set_queue_limit(gbo_server* s, long long max_pending);
+/* BFS admission batching: pending BFS queries enter the engine when at
+ * least ceil(min_free_fraction * bfs_slots) slots are free, or when no
+ * admitted query is still traversing.  0 admits into any free slot every
+ * round; 1 admits only into an idle engine (batch after batch); values in
+ * between trade a little latency for fewer rounds in which freshly admitted
+ * sources keep every row of the graph open.  Default 0.5. */
+GBO_API int gbo_server_set_admission(gbo_server* s, float min_free_fraction);
 GBO_API int gbo_server_submit_bfs(gbo_server* s, int src, int64_t* ticket);
 GBO_API int gbo_server_submit_ppr(gbo_server* s, const int* verts,
                           const float* weights, int count, int64_t* ticket);

@@ -182,3 +182,23 @@ def test_server_byte_levels_match_int32_levels(gbo, orc, gpu):
     lv, _, _ = sp.wait(t, "bfs")
     assert np.array_equal(lv, np.arange(m))
     sp.close()
+
+
+@pytest.mark.parametrize("admit", [0.0, 0.5, 1.0])
+def test_server_admission_batching_keeps_results(gbo, orc, gpu, admit):
+    """Admission into any free slot, into half-free engines or only into idle
+    ones: every BFS result is the oracle's levels."""
+    csr = gbo.gen_rmat(12, 16, seed=3)
+    n = csr.nrows
+    g = gbo.Graph.from_csr(csr, 32, gbo.FLAG_SYMMETRIC)
+    srv = gbo.Server(g, bfs_slots=64, ppr_slots=0)
+    srv.set_admission(admit)
+    srcs = np.random.default_rng(7).integers(0, n, 200)
+    tickets = [srv.submit_bfs(int(s)) for s in srcs]
+    for s, t in zip(srcs, tickets):
+        res, _, _ = srv.wait(t, "bfs")
+        assert np.array_equal(res, orc.bfs_csr(csr.rowptr, csr.colind, n, int(s))[0]), (admit, int(s))
+    with pytest.raises(gbo.GboError):
+        srv.set_admission(1.5)
+    srv.close()
+    g.free()
