@@ -1277,10 +1277,12 @@ __device__ __forceinline__ PrIter pr_iter(float* pr, float* prs, const Ctrl* ctr
 __global__ void __launch_bounds__(kTPB) k_pr_step_rws(GView v, float* __restrict__ pr, float* __restrict__ prs,
                                                       const float* __restrict__ inv,
                                                       const float* __restrict__ pv, Ctrl* __restrict__ ctrl) {
+  __shared__ double pr_tail_sh[kTPB / 32][32];
   if (((volatile Ctrl*)ctrl)->done) return;
   const int n = v.nrows;
   const PrIter P = pr_iter(pr, prs, ctrl, n);
   const unsigned lane = threadIdx.x & 31;
+  const unsigned kFull = 0xffffffffu;
   double e = 0.0;
   const long long nwarps = warps_total();
   for (long long R = warp_global(); R < v.nbr; R += nwarps) {
@@ -1294,14 +1296,46 @@ __global__ void __launch_bounds__(kTPB) k_pr_step_rws(GView v, float* __restrict
     const long long tb = v.rws_tail_ptr[row], te = v.rws_tail_ptr[row + 1];
     double a = pr_entries8(h8, P.xg);
     const bool long_row = te - tb > kRwsLongTail;  // the chunk kernels own a long row
-    if (!long_row) {
-      for (long long p = tb; p < te; p += 4) {
-        uint2 e[4];
+    // The block row's short tails as one list, 32 entries per round over the
+    // warp's lanes (a lane per row would wait for the block row's longest
+    // tail): lane q of a round finds its entry's row r by a binary search
+    // over the tails' inclusive sums, and a segmented scan across the lanes
+    // adds each row's entries of the round, in lane order, into tsum[r].
+    const int len = long_row ? 0 : (int)(te - tb);
+    const int incl = warp_incl_sum(len, lane);
+    const int total = __shfl_sync(kFull, incl, 31);
+    double* tsum = pr_tail_sh[threadIdx.x >> 5];
+    tsum[lane] = 0.0;
+    __syncwarp();
+    for (int p0 = 0; p0 < total; p0 += 32) {
+      const int q = p0 + (int)lane;
+      int r = 0;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) e[u] = p + u < te ? v.rws_tail[p + u] : make_uint2(kRwsNone, 0u);
-        a += pr_entries4(e, P.xg);
+      for (int st = 16; st > 0; st >>= 1)
+        if (__shfl_sync(kFull, incl, r + st - 1) <= q) r += st;
+      const int rin = __shfl_sync(kFull, incl, r);
+      const int rlen = __shfl_sync(kFull, len, r);
+      const long long rtb = __shfl_sync(kFull, tb, r);
+      double val = 0.0;
+      if (q < total) {
+        const uint2 t = v.rws_tail[rtb + (q - (rin - rlen))];
+        for (uint32_t m = t.y; m;) {
+          const int j = __clz(m);
+          m &= ~(0x80000000u >> j);
+          val += (double)__ldg(P.xg + (size_t)t.x * 32 + j);
+        }
       }
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const double y = __shfl_up_sync(kFull, val, o);
+        const int ry = __shfl_up_sync(kFull, r, o);
+        if ((int)lane >= o && ry == r) val += y;
+      }
+      const int rn = __shfl_down_sync(kFull, r, 1);
+      if (q < total && (lane == 31 || q + 1 == total || rn != r)) tsum[r] += val;
+      __syncwarp();
     }
+    a += tsum[lane];
     if (row < n && !long_row)
       e += pr_row_update(row, a, P.x, P.y, P.ys, inv, pv, P.alpha, P.add, P.adds, P.norm, P.row_scale);
   }
