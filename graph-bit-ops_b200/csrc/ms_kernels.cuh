@@ -758,6 +758,43 @@ __global__ void __launch_bounds__(kTPB) k_push_fin(Args a) {
   close_level(a, cnt, true);
 }
 
+// Level 0 of a multi-source BFS on a symmetric slice graph as a push: the
+// sources' own entries (a warp per (source, piece of its tail); piece 0
+// also takes the head) OR the source's bit into push_acc of every
+// neighbour, which on P = P^T is what the level's pull step would gather
+// for that neighbour -- but without walking every row of the graph for a
+// frontier of k vertices.  k_push_fin then runs the block-row epilogue and
+// closes the level; this kernel sets the level's mode so that it does.
+template <int KW>
+__global__ void __launch_bounds__(kTPB) k_seed_push(Args a, const int* __restrict__ srcs, int nsrc, int pieces) {
+  const unsigned lane = threadIdx.x & 31;
+  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w == 0 && lane == 0) a.ctl[6] = 1;
+  if (w >= (long long)nsrc * pieces) return;
+  const int q = (int)(w / pieces), piece = (int)(w % pieces);
+  const int v0 = srcs[q];
+  const GView& v = a.v;
+  if (v0 < 0 || v0 >= v.nrows) return;
+  const uint32_t bit = 1u << (q % 32);
+  uint32_t* acc = a.push_acc + q / 32;
+  auto push = [&](uint2 e) {
+    for (uint32_t m = e.y; m;) {
+      const int c = __clz(m);
+      m &= ~(0x80000000u >> c);
+      atomicOr(acc + ((size_t)e.x * 32 + c) * KW, bit);
+    }
+  };
+  if (piece == 0 && lane < kRwsHead) {
+    const uint2 e = v.rws_head[((size_t)(v0 / 32) * kRwsHead + lane) * 32 + v0 % 32];
+    if (e.x != kRwsNone) push(e);
+  }
+  const long long tb = v.rws_tail_ptr[v0], te = v.rws_tail_ptr[v0 + 1];
+  const long long per = (te - tb + pieces - 1) / pieces;
+  const long long pb = tb + (long long)piece * per;
+  const long long pe = pb + per < te ? pb + per : te;
+  for (long long p = pb + lane; p < pe; p += 32) push(v.rws_tail[p]);
+}
+
 // Reset: levels -1, V 0, F[0] 0, frontier bits 0, padding rows and rows
 // without entries marked full (no source can reach them).  A source in such
 // a row reopens it in k_seed.

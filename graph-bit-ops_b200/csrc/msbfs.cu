@@ -46,7 +46,9 @@ struct MsState {
   std::vector<float> step_ms;
   long long launches = 0;
   int launches_per_replay = 0;
+  int fixed_launches = 3;  // launches of a run outside its graph replays
   cudaEvent_t ev[2 * kLevelsPerGraph] = {};
+  cudaEvent_t ev0[2] = {};  // level 0 when it runs as a seed push
 };
 
 // Levels with fewer new (vertex, source) pairs than this run as pushes: on
@@ -77,7 +79,7 @@ ms::Args make_args(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
   a.level_group = 0;  // the API's vertex-major levels[v * k + s]
   a.push_thr = ms_push_threshold(g, m.kw);
   a.dir = a.push_thr > 0 ? 1 : 0;
-  a.push_acc = a.dir ? m.push_acc : nullptr;
+  a.push_acc = m.push_acc;
   a.long_acc = m.long_acc;
   return a;
 }
@@ -151,6 +153,7 @@ int msbfs_impl(gbo_graph* g, const int* h_srcs, int k, int32_t* d_levels, int* h
     GBO_CUDA_TRY(cudaMalloc(&m.fbits, sizeof(uint32_t) * 2 * (size_t)(g->nbr + 1)));
     GBO_CUDA_TRY(cudaMalloc(&m.vfull, sizeof(uint32_t) * (size_t)(g->nbr + 1)));
     for (auto& e : m.ev) GBO_CUDA_TRY(cudaEventCreate(&e));
+    for (auto& e : m.ev0) GBO_CUDA_TRY(cudaEventCreate(&e));
   }
   if (!m.live) {
     const void* lv = nullptr;
@@ -181,7 +184,7 @@ int msbfs_impl(gbo_graph* g, const int* h_srcs, int k, int32_t* d_levels, int* h
     GBO_CUDA_TRY(cudaMalloc(&m.F, sizeof(uint32_t) * 2 * (size_t)n * kw + 16));
     GBO_CUDA_TRY(cudaMalloc(&m.V, sizeof(uint32_t) * (size_t)n * kw + 16));
     GBO_TRY(ms::split_state(g, kw, &m.split_acc, &m.slot_split, s));
-    if (kw <= 2) {  // push levels' accumulator, zero between levels
+    if (kw <= 2 || (g->symmetric && g->rws_head)) {  // push levels' accumulator, zero between levels
       const size_t pw = (size_t)(g->nbr > 0 ? g->nbr : 1) * 32 * (size_t)kw;
       GBO_CUDA_TRY(cudaMalloc(&m.push_acc, sizeof(uint32_t) * pw));
       GBO_CUDA_TRY(cudaMemsetAsync(m.push_acc, 0, sizeof(uint32_t) * pw, s));
@@ -220,7 +223,39 @@ int msbfs_impl(gbo_graph* g, const int* h_srcs, int k, int32_t* d_levels, int* h
   GBO_CUDA_TRY(cudaGetLastError());
   m.step_ms.clear();
   m.launches = 3;
-  int it0 = 0;
+  // symmetric slice graphs whose levels all pull: level 0 pushes from the k
+  // sources instead (k_seed_push, then the push epilogue) -- a pull would
+  // walk every row of the graph for a frontier of k vertices
+  const bool seed_push = g->symmetric && g->rws_head && !a.dir && g->nitems > 0 && m.push_acc;
+  if (seed_push) {
+    constexpr int kPieces = 64;  // warps per source: hubs' tails are split
+    GBO_CUDA_TRY(cudaEventRecord(m.ev0[0], s));
+    switch (kw) {
+      case 1: ms::k_seed_push<1><<<blocks_for_warps((long long)k * kPieces, ms::kWarps), ms::kTPB, 0, s>>>(a, m.srcs, k, kPieces); break;
+      case 2: ms::k_seed_push<2><<<blocks_for_warps((long long)k * kPieces, ms::kWarps), ms::kTPB, 0, s>>>(a, m.srcs, k, kPieces); break;
+      case 4: ms::k_seed_push<4><<<blocks_for_warps((long long)k * kPieces, ms::kWarps), ms::kTPB, 0, s>>>(a, m.srcs, k, kPieces); break;
+      case 8: ms::k_seed_push<8><<<blocks_for_warps((long long)k * kPieces, ms::kWarps), ms::kTPB, 0, s>>>(a, m.srcs, k, kPieces); break;
+      case 16: ms::k_seed_push<16><<<blocks_for_warps((long long)k * kPieces, ms::kWarps), ms::kTPB, 0, s>>>(a, m.srcs, k, kPieces); break;
+      default: ms::k_seed_push<32><<<blocks_for_warps((long long)k * kPieces, ms::kWarps), ms::kTPB, 0, s>>>(a, m.srcs, k, kPieces); break;
+    }
+    const unsigned gr = blocks_for_warps(g->nbr > 0 ? g->nbr : 1, ms::kWarps);
+    switch (kw) {
+      case 1: ms::k_push_fin<1><<<gr, ms::kTPB, 0, s>>>(a); break;
+      case 2: ms::k_push_fin<2><<<gr, ms::kTPB, 0, s>>>(a); break;
+      case 4: ms::k_push_fin<4><<<gr, ms::kTPB, 0, s>>>(a); break;
+      case 8: ms::k_push_fin<8><<<gr, ms::kTPB, 0, s>>>(a); break;
+      case 16: ms::k_push_fin<16><<<gr, ms::kTPB, 0, s>>>(a); break;
+      default: ms::k_push_fin<32><<<gr, ms::kTPB, 0, s>>>(a); break;
+    }
+    GBO_CUDA_TRY(cudaGetLastError());
+    GBO_CUDA_TRY(cudaEventRecord(m.ev0[1], s));
+    m.launches += 2;
+  }
+  m.fixed_launches = (int)m.launches;
+  int it0 = seed_push ? 1 : 0;
+  if (seed_push) {  // level 0's time (read once the loop has synchronised)
+    m.step_ms.push_back(-1.f);
+  }
   long long max_launch = (long long)max_iter / kLevelsPerGraph + 2;
   const long long cap = inject_replay_cap();
   if (cap > 0 && cap < max_launch) max_launch = cap;
@@ -246,6 +281,10 @@ int msbfs_impl(gbo_graph* g, const int* h_srcs, int k, int32_t* d_levels, int* h
     }
   }
   if (!done) return fail(GBO_ERR_TIMEOUT, "multi-source BFS did not terminate");
+  if (seed_push && cudaEventElapsedTime(&m.step_ms[0], m.ev0[0], m.ev0[1]) != cudaSuccess) {
+    m.step_ms[0] = -1.f;
+    (void)cudaGetLastError();
+  }
   if (h_depth) *h_depth = m.h_ctl[0];
   g->last_run_ms = 1;
   return GBO_OK;
@@ -257,7 +296,8 @@ int ms_last_run(const gbo_graph* g, gbo_run_stats* st) {
   const MsState* m = reinterpret_cast<const MsState*>(g->ms);
   if (!m) return GBO_OK;
   st->iterations = m->h_ctl ? m->h_ctl[0] : 0;
-  st->graph_replays = (int)((m->launches - 3) / (m->launches_per_replay > 0 ? m->launches_per_replay : 1));
+  st->graph_replays =
+      (int)((m->launches - m->fixed_launches) / (m->launches_per_replay > 0 ? m->launches_per_replay : 1));
   st->kernel_launches = m->launches;
   const int n = (int)m->step_ms.size();
   st->nsteps = n < GBO_MAX_STEP_TIMES ? n : GBO_MAX_STEP_TIMES;
@@ -304,6 +344,8 @@ void free_ms_state(gbo_graph* g) {
   cudaFree(m->split_acc);
   cudaFree(m->slot_split);
   cudaFree(m->push_acc);
+  for (auto& e : m->ev0)
+    if (e) cudaEventDestroy(e);
   cudaFree(m->long_acc);
   cudaFree(m->active);
   cudaFree(m->srcs);

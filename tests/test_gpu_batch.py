@@ -22,6 +22,33 @@ def test_msbfs_matches_per_source_bfs(gbo, orc, gpu, k):
         assert depth == int(want.max()) + 1
 
 
+@pytest.mark.parametrize("k", [1, 64, 100, 256, 1024])
+def test_msbfs_seed_push_on_symmetric_graphs(gbo, orc, gpu, k):
+    """On symmetric graphs whose levels all pull, level 0 pushes from the
+    sources (hubs' tails split over warps, isolated sources, duplicates);
+    every level matches one oracle BFS per source."""
+    rng = np.random.default_rng(300 + k)
+    e = rng.integers(0, 2000, (2, 12000)).astype(np.int32)
+    island = gbo.csr_from_edges(e[0], e[1], 3000, True, True)  # 2000..2999 isolated
+    hub = np.repeat(np.arange(3, dtype=np.int32), 19997)  # three hubs joined to every vertex
+    leaves = np.tile(np.arange(3, 20000, dtype=np.int32), 3)
+    star = gbo.csr_from_edges(hub, leaves, 20000, True, True)
+    for csr in (gbo.gen_rmat(12, 16, seed=0), island, star):
+        g = gbo.Graph.from_csr(csr, 32, gbo.FLAG_SYMMETRIC)
+        g.set_bfs_direction(True, 0)  # every level pulls: level 0 is the seed push
+        srcs = rng.integers(0, csr.nrows, k).astype(np.int32)
+        srcs[0] = 0 if csr is not island else 2500  # a hub, or an isolated vertex
+        if k > 1:
+            srcs[-1] = srcs[0]
+        lv, depth = g.msbfs(srcs)
+        want = oracle_levels(orc, csr, srcs)
+        assert np.array_equal(lv, want), (csr.nrows, k)
+        assert depth == int(want.max()) + 1
+        st = g.last_run()
+        assert len(st["step_ms"]) == depth
+        g.free()
+
+
 def test_msbfs_split_rows_and_duplicates(gbo, orc, gpu):
     # a hub vertex makes block row 0 long enough to be split across warps
     n = 20000
