@@ -728,6 +728,77 @@ __global__ void __launch_bounds__(kTPB) k_push(Args a) {
   }
 }
 
+// Push level over the row-word slices (symmetric graphs, any k): the
+// frontier rows of the level's frontier vertices are OR-ed into push_acc of
+// their neighbours, as k_push does from the tiles, but walking only the
+// frontier vertices' own entries.  push_one ORs vertex u's non-zero
+// frontier words (nz: which of its KW words) into neighbour word w's
+// accumulators; the words are read through L1 (every lane the same).
+template <int KW>
+__device__ __forceinline__ void push_entry(const Args& a, const uint32_t* __restrict__ fu, uint32_t nz, uint2 e) {
+  if (e.x == kRwsNone) return;
+  for (uint32_t m = e.y; m;) {
+    const int c = __clz(m);
+    m &= ~(0x80000000u >> c);
+    uint32_t* dst = a.push_acc + ((size_t)e.x * 32 + c) * KW;
+    for (uint32_t jm = nz; jm; jm &= jm - 1) {
+      const int j = __ffs(jm) - 1;
+      atomicOr(dst + j, fu[j]);
+    }
+  }
+}
+
+// Part 1, a warp per block row with frontier vertices: for each of them the
+// head (eight entries, one per lane) and a tail of up to kMsLongTail entries
+// (32 per round); longer tails are k_push_chunks'.
+template <int KW>
+__global__ void __launch_bounds__(kTPB) k_push_rows(Args a) {
+  volatile int* c = a.ctl;
+  if (c[1] || c[7] || c[6] != 1) return;
+  const int lvl = c[0];
+  const GView& v = a.v;
+  const unsigned lane = threadIdx.x & 31;
+  const long long R = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (R >= v.nbr) return;
+  const uint32_t fw = a.fbits[(size_t)(lvl & 1) * (v.nbr + 1) + R];
+  if (!fw) return;
+  const uint32_t* __restrict__ F = a.F + (size_t)(lvl & 1) * a.fstride;
+  for (uint32_t rm = fw; rm;) {
+    const int r = __clz(rm);  // bit 31 - r: row r
+    rm &= ~(0x80000000u >> r);
+    const long long u = R * 32 + r;
+    const uint32_t* fu = F + (size_t)u * KW;
+    const uint32_t nz = __ballot_sync(0xffffffffu, (int)lane < KW && fu[lane < KW ? lane : 0] != 0u);
+    if (!nz) continue;
+    if (lane < kRwsHead) push_entry<KW>(a, fu, nz, v.rws_head[((size_t)R * kRwsHead + lane) * 32 + r]);
+    const long long tb = v.rws_tail_ptr[u], te = v.rws_tail_ptr[u + 1];
+    if (te - tb > kMsLongTail) continue;  // k_push_chunks walks long tails
+    for (long long p = tb + lane; p < te; p += 32) push_entry<KW>(a, fu, nz, v.rws_tail[p]);
+  }
+}
+
+// Part 2, a warp per long-tail chunk whose row is a frontier vertex.
+template <int KW>
+__global__ void __launch_bounds__(kTPB) k_push_chunks(Args a) {
+  volatile int* c = a.ctl;
+  if (c[1] || c[7] || c[6] != 1) return;
+  const int lvl = c[0];
+  const GView& v = a.v;
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t* __restrict__ fb = a.fbits + (size_t)(lvl & 1) * (v.nbr + 1);
+  const uint32_t* __restrict__ F = a.F + (size_t)(lvl & 1) * a.fstride;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long q = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < v.rws_nchunk; q += nwarps) {
+    const long long u = v.rws_chunk_row[q];
+    if (!((fb[u >> 5] >> (31 - (u & 31))) & 1u)) continue;
+    const uint32_t* fu = F + (size_t)u * KW;
+    const uint32_t nz = __ballot_sync(0xffffffffu, (int)lane < KW && fu[lane < KW ? lane : 0] != 0u);
+    if (!nz) continue;
+    for (long long p = v.rws_chunk_beg[q] + lane; p < v.rws_chunk_end[q]; p += 32)
+      push_entry<KW>(a, fu, nz, v.rws_tail[p]);
+  }
+}
+
 // After k_push: the epilogue of every block row from push_acc (zeroed
 // again), then the level close.  Block rows without new bits only clear
 // their next-frontier word.

@@ -55,7 +55,8 @@ struct MsState {
 // symmetric graphs with k <= 64 when the caller set a positive BFS push
 // threshold (gbo_graph_set_bfs_direction); otherwise (0) every level pulls.
 long long ms_push_threshold(const gbo_graph* g, int kw) {
-  if (!g->symmetric || kw > 2 || g->bfs_push_thr <= 0) return 0;
+  if (!g->symmetric || g->bfs_push_thr <= 0) return 0;
+  if (kw > 2 && !g->rws_head) return 0;  // wide frontier rows push over the slices only
   return g->bfs_push_thr;
 }
 
@@ -104,12 +105,17 @@ int ms_capture(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
   GBO_CUDA_TRY(cudaStreamBeginCapture(m.cap, cudaStreamCaptureModeThreadLocal));
   for (int q = 0; q < kLevelsPerGraph; ++q) {
     cudaEventRecordWithFlags(m.ev[2 * q], m.cap, cudaEventRecordExternal);
-    if constexpr (KW <= 2) {
-      if (a.dir) {
-        // a warp per work item (gi counts block rows on slice graphs)
+    if (a.dir) {
+      if (g->rws_head) {  // push over the frontier vertices' own slice entries
+        if (g->nitems > 0) ms::k_push_rows<KW><<<gr, ms::kTPB, 0, m.cap>>>(a);
+        if (g->rws_nchunk > 0)
+          ms::k_push_chunks<KW><<<std::min(blocks_for_warps(g->rws_nchunk, ms::kWarps), (unsigned)num_sms() * 8u),
+                                  ms::kTPB, 0, m.cap>>>(a);
+      } else if constexpr (KW <= 2) {
+        // a warp per work item over the tiles
         if (g->nitems > 0) ms::k_push<KW><<<blocks_for_warps(g->nitems, ms::kWarps), ms::kTPB, 0, m.cap>>>(a);
-        ms::k_push_fin<KW><<<gr, ms::kTPB, 0, m.cap>>>(a);
       }
+      ms::k_push_fin<KW><<<gr, ms::kTPB, 0, m.cap>>>(a);
     }
     if (g->nitems > 0) {
       if constexpr (KW <= 2) {

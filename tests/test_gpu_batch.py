@@ -35,17 +35,20 @@ def test_msbfs_seed_push_on_symmetric_graphs(gbo, orc, gpu, k):
     star = gbo.csr_from_edges(hub, leaves, 20000, True, True)
     for csr in (gbo.gen_rmat(12, 16, seed=0), island, star):
         g = gbo.Graph.from_csr(csr, 32, gbo.FLAG_SYMMETRIC)
-        g.set_bfs_direction(True, 0)  # every level pulls: level 0 is the seed push
         srcs = rng.integers(0, csr.nrows, k).astype(np.int32)
         srcs[0] = 0 if csr is not island else 2500  # a hub, or an isolated vertex
         if k > 1:
             srcs[-1] = srcs[0]
-        lv, depth = g.msbfs(srcs)
         want = oracle_levels(orc, csr, srcs)
-        assert np.array_equal(lv, want), (csr.nrows, k)
-        assert depth == int(want.max()) + 1
-        st = g.last_run()
-        assert len(st["step_ms"]) == depth
+        # 0: every level pulls after the seed push; the others push the
+        # levels below the threshold over the slices (every level at 2^31-1)
+        for push in (0, 4096, 2**31 - 1):
+            g.set_bfs_direction(True, push)
+            lv, depth = g.msbfs(srcs)
+            assert np.array_equal(lv, want), (csr.nrows, k, push)
+            assert depth == int(want.max()) + 1
+            if push == 0:
+                assert len(g.last_run()["step_ms"]) == depth
         g.free()
 
 
