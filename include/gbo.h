@@ -205,9 +205,11 @@ GBO_API int gbo_graph_permutation(const gbo_graph* g, const int** d_new_of_old);
  * does for gbo_graph_from_csr; needed for wrapped graphs), 0 restores
  * pull-only BFS.  A level whose frontier holds fewer than push_threshold
  * vertices is expanded top-down; -1 selects the default nrows / 64.
- * gbo_msbfs with k <= 64 on a symmetric graph pushes a level with fewer than
- * push_threshold new (vertex, source) pairs when push_threshold > 0, and
- * pulls every level otherwise (-1 and 0).
+ * gbo_msbfs on a symmetric graph pushes a level with fewer than
+ * push_threshold new (vertex, source) pairs when push_threshold > 0 (any k
+ * on b = 32 ROW graphs, k <= 64 on others), and otherwise (-1 and 0) pulls
+ * every level, except that level 0 on a b = 32 ROW graph pushes from the
+ * sources.
  * Rejected (GBO_ERR_UNSUPPORTED) for a non-square graph. */
 GBO_API int gbo_graph_set_bfs_direction(gbo_graph* g, int symmetric, int push_threshold);
 
