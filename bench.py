@@ -1,5 +1,6 @@
 """Benchmark: BFS GTEPS on B2SR (bit-packed BSR) on B200, plus the roofline of
-the BFS pull kernel, the plain BSR-BMV roofline and a CPU baseline.
+the BFS kernel (the cooperative level loop on 32x32 ROW graphs), the plain
+BSR-BMV roofline and a CPU baseline.
 
 Workload (one GPU): BFS from vertex 0 on an R-MAT graph of scale 22 (edge
 factor 16, a=0.57 b=0.19 c=0.19, seed 0; symmetrised, deduplicated, no
