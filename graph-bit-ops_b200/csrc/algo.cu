@@ -1564,6 +1564,67 @@ __global__ void __launch_bounds__(kTPB) k_cc_mngf(GView v, const int* __restrict
   }
 }
 
+// The same minimum over the row-word slices of a 32x32 ROW graph: a warp per
+// block row, lane r over row r's entries (the whole head in one round, then
+// tails of up to kRwsLongTail entries four at a time), the grandparent of
+// every column of each entry gathered; longer tails are k_cc_mngf_chunks'.
+__device__ __forceinline__ int cc_min_entries(const uint2* e, int ne, const int* __restrict__ gf, int a) {
+  for (int u = 0; u < ne; ++u) {
+    if (e[u].x == kRwsNone) continue;
+    for (uint32_t m = e[u].y; m;) {
+      const int j = __clz(m);
+      m &= ~(0x80000000u >> j);
+      a = min(a, __ldg(gf + (size_t)e[u].x * 32 + j));
+    }
+  }
+  return a;
+}
+
+__global__ void __launch_bounds__(kTPB) k_cc_mngf_rws(GView v, const int* __restrict__ gf, int* __restrict__ mngf,
+                                                      Ctrl* __restrict__ ctrl) {
+  if (((volatile Ctrl*)ctrl)->done) return;
+  const unsigned lane = threadIdx.x & 31;
+  const long long nwarps = warps_total();
+  for (long long R = warp_global(); R < v.nbr; R += nwarps) {
+    const long long row = R * 32 + lane;
+    const uint2* __restrict__ hp = v.rws_head + (size_t)R * (kRwsHead * 32) + lane;
+    uint2 h8[kRwsHead];
+#pragma unroll
+    for (int u = 0; u < kRwsHead; ++u) h8[u] = hp[(size_t)u * 32];
+    const long long tb = v.rws_tail_ptr[row], te = v.rws_tail_ptr[row + 1];
+    int a = cc_min_entries(h8, kRwsHead, gf, kINF);
+    if (te - tb <= kRwsLongTail) {
+      for (long long p = tb; p < te; p += 4) {
+        uint2 e[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) e[u] = p + u < te ? v.rws_tail[p + u] : make_uint2(kRwsNone, 0u);
+        a = cc_min_entries(e, 4, gf, a);
+      }
+    }
+    if (row < v.nrows && a < mngf[row]) mngf[row] = a;
+  }
+}
+
+// Long tails: a warp per chunk, the chunk's minimum folded into its row with
+// atomicMin (after k_cc_mngf_rws wrote the row's head and short part).
+__global__ void __launch_bounds__(kTPB) k_cc_mngf_chunks(GView v, const int* __restrict__ gf,
+                                                         int* __restrict__ mngf, Ctrl* __restrict__ ctrl) {
+  if (((volatile Ctrl*)ctrl)->done) return;
+  const unsigned lane = threadIdx.x & 31;
+  const long long nwarps = warps_total();
+  for (long long q = warp_global(); q < v.rws_nchunk; q += nwarps) {
+    const long long e0 = v.rws_chunk_end[q];
+    int a = kINF;
+    for (long long p = v.rws_chunk_beg[q] + lane; p < e0; p += 32) {
+      const uint2 e = v.rws_tail[p];
+      a = cc_min_entries(&e, 1, gf, a);
+    }
+    a = __reduce_min_sync(0xffffffffu, a);
+    const long long row = v.rws_chunk_row[q];
+    if (lane == 0 && row < v.nrows && a < mngf[row]) atomicMin(mngf + row, a);
+  }
+}
+
 template <int B>
 __global__ void k_cc_mngf_finish(GView v, int* __restrict__ mngf, Ctrl* __restrict__ ctrl,
                                  const int* __restrict__ scratch) {
@@ -2166,13 +2227,24 @@ int cc_impl(gbo_graph* g, int32_t* d_label, int* h_iters, cudaStream_t s) {
   Ctrl* ctrl = a->ctrl;
   int* scratch = (int*)a->scratch;
   const int n = g->nrows;
-  const unsigned gi = grid_items_persistent(k_cc_mngf<B>, g->nitems, B);
+  // 32x32 ROW graphs take the neighbours' minimum over their row-word slices
+  if (B == 32 && g->layout == GBO_LAYOUT_ROW) GBO_TRY(build_rws(g, s));
+  const bool rws = B == 32 && g->layout == GBO_LAYOUT_ROW && g->rws_head != nullptr;
+  if (rws) v = view_of(g);
+  const unsigned gi = rws ? grid_persistent(k_cc_mngf_rws, g->nbr) : grid_items_persistent(k_cc_mngf<B>, g->nitems, B);
+  const unsigned gc = rws && g->rws_nchunk > 0 ? grid_persistent(k_cc_mngf_chunks, g->rws_nchunk) : 0u;
   const unsigned gs = blocks_for((long long)g->nsplit * B, kTPB);
   const unsigned gv = grid_vertex(n);
   GBO_TRY(get_exec(a, A_CC, nullptr, [&](cudaStream_t cs, int k, int* nl) -> int {
-    if (g->nitems > 0) k_cc_mngf<B><<<gi, kTPB, 0, cs>>>(v, gf, mngf, ctrl, scratch);
-    *nl += (g->nitems > 0) + (g->nsplit > 0) + 3;
-    if (g->nsplit > 0) k_cc_mngf_finish<B><<<gs, kTPB, 0, cs>>>(v, mngf, ctrl, scratch);
+    if (rws) {
+      if (g->nitems > 0) k_cc_mngf_rws<<<gi, kTPB, 0, cs>>>(v, gf, mngf, ctrl);
+      if (gc > 0) k_cc_mngf_chunks<<<gc, kTPB, 0, cs>>>(v, gf, mngf, ctrl);
+      *nl += (g->nitems > 0) + (gc > 0) + 3;
+    } else {
+      if (g->nitems > 0) k_cc_mngf<B><<<gi, kTPB, 0, cs>>>(v, gf, mngf, ctrl, scratch);
+      *nl += (g->nitems > 0) + (g->nsplit > 0) + 3;
+      if (g->nsplit > 0) k_cc_mngf_finish<B><<<gs, kTPB, 0, cs>>>(v, mngf, ctrl, scratch);
+    }
     k_cc_hook<<<gv, kTPB, 0, cs>>>(f, mngf, n, ctrl);
     k_cc_shortcut<<<gv, kTPB, 0, cs>>>(f, mngf, gf, n, ctrl);
     k_cc_grand<<<gv, kTPB, 0, cs>>>(f, gf, n, ctrl);
