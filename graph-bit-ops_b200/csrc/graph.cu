@@ -450,6 +450,28 @@ extern "C" int gbo_bmv_float_transposed(const gbo_graph* g, const float* d_x, fl
 // column indices + block-row offsets), from the packer's count pass alone;
 // TIMED packs the matrix at every width and times the operation with CUDA
 // events (one warm-up, three timed runs), keeping the fastest.
+// Row words of a 32x32 packing: distinct (row, column / 32) pairs of a
+// column-sorted CSR (a thread per row; one atomic add per block).
+__global__ void k_count_row_words32(const int* __restrict__ rowptr, const int* __restrict__ colind, int nrows,
+                                    unsigned long long* __restrict__ out) {
+  unsigned long long c = 0;
+  for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < nrows;
+       u += (long long)gridDim.x * blockDim.x) {
+    int prev = -1;
+    for (int p = rowptr[u]; p < rowptr[u + 1]; ++p) {
+      const int w = colind[p] >> 5;
+      c += w != prev;
+      prev = w;
+    }
+  }
+  __shared__ unsigned long long sh;
+  if (threadIdx.x == 0) sh = 0;
+  __syncthreads();
+  if (c) atomicAdd(&sh, c);
+  __syncthreads();
+  if (threadIdx.x == 0 && sh) atomicAdd(out, sh);
+}
+
 extern "C" int gbo_tune_tile_width(const int* rowptr, const int* colind, int nrows, int ncols,
                                    int nnz, int flags, int op, int mode, gbo_stream_t stream,
                                    int* best_bits, double* cost) {
@@ -480,6 +502,24 @@ extern "C" int gbo_tune_tile_width(const int* rowptr, const int* colind, int nro
       if (st == GBO_OK) {
         const double wb = b >= 8 ? b / 8 : 1;
         c[k] = (double)nblk * (b * wb + 4.0) + 4.0 * ((nrows + b - 1) / b + 1);
+        if (op == GBO_TUNE_BFS && b == 32 && !(flags & GBO_FLAG_LAYOUT_COL) && nrows > 0) {
+          // 32x32 ROW BFS walks row-word slices: 8 bytes per non-empty row
+          // word and 8 per row of tail offsets in one pass (its pull steps
+          // stop at a row's first frontier neighbour, so a BFS reads less)
+          unsigned long long* d = nullptr;
+          unsigned long long rw = 0;
+          if (cudaMallocAsync(&d, sizeof(rw), s) != cudaSuccess || cudaMemsetAsync(d, 0, sizeof(rw), s) != cudaSuccess) {
+            st = fail(GBO_ERR_NOMEM, "tuner counter");
+          } else {
+            const int grid = (int)std::min<long long>(((long long)nrows + 255) / 256, 4096);
+            k_count_row_words32<<<grid, 256, 0, s>>>(use->rowptr, use->colind, nrows, d);
+            if (cudaMemcpyAsync(&rw, d, sizeof(rw), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess)
+              st = fail(GBO_ERR_CUDA, "tuner row-word count");
+            cudaFreeAsync(d, s);
+            if (st == GBO_OK) c[k] = 8.0 * (double)rw + 8.0 * ((double)nrows + 1.0);
+          }
+        }
       } else if (st == GBO_ERR_OVERFLOW) {
         c[k] = INFINITY;
         st = GBO_OK;

@@ -235,8 +235,12 @@ GBO_API int gbo_graph_set_bfs_loop(gbo_graph* g, int loop, int coop_blocks);
  * from the command line).  Ranks b = 4, 8, 16, 32, 64 for the CSR matrix
  * (same arguments and flags as gbo_graph_from_csr) and an operation:
  *   mode GBO_TUNE_MODEL: algorithmic bytes of one sweep over the packing
- *     (nblocks(b) * (b words + 4-byte column index) + block-row offsets),
- *     from the packer's count pass only -- nothing is packed;
+ *     (nblocks(b) * (b words + 4-byte column index) + block-row offsets;
+ *     for GBO_TUNE_BFS at b = 32 in the ROW layout, the row-word slices that
+ *     its BFS walks: 8 bytes per non-empty row word + 8 per row), from count
+ *     passes only -- nothing is packed.  A BFS reads less than one sweep
+ *     (pull steps stop at a row's first frontier neighbour), so
+ *     GBO_TUNE_TIMED ranks BFS widths more faithfully;
  *   mode GBO_TUNE_TIMED: packs at every width and times the operation
  *     (one warm-up, mean of three runs, CUDA events on `stream`).
  * op GBO_TUNE_TC packs the lower triangle and never picks b = 4.
