@@ -35,3 +35,17 @@ def test_timed_picks_fastest(gbo, gpu):
         allowed = WIDTHS if op != gbo.TUNE_TC else WIDTHS[1:]
         assert all(ms[b] > 0 and math.isfinite(ms[b]) for b in allowed)
         assert best == min(allowed, key=lambda b: ms[b])
+
+
+def test_bfs_model_counts_row_word_slices_at_32(gbo, gpu):
+    """For BFS at b = 32 the model prices the row-word slices: 8 bytes per
+    distinct (row, column / 32) pair and 8 per row; other widths stay tiles."""
+    csr = gbo.gen_rmat(12, 16, seed=5)
+    best, cost = gbo.tune_tile_width(csr, gbo.TUNE_BFS, gbo.TUNE_MODEL)
+    rows = np.repeat(np.arange(csr.nrows), np.diff(csr.rowptr))
+    words = len(set(zip(rows.tolist(), (csr.colind // 32).tolist())))
+    assert cost[32] == 8 * words + 8 * (csr.nrows + 1)
+    for b in (4, 8, 16, 64):
+        nblk = int(gbo.Graph.from_csr(csr, b).info().nblocks)
+        assert cost[b] == _sweep_bytes(nblk, b, csr.nrows), b
+    assert best == min(WIDTHS, key=lambda b: cost[b])
