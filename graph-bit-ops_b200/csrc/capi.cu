@@ -1,5 +1,6 @@
 // Error reporting, version and the device plumbing part of the C ABI.
 #include <atomic>
+#include <mutex>
 #include <cstring>
 #include <string>
 
@@ -50,6 +51,36 @@ bool inject_host_alloc_fails() {
 }
 long long inject_replay_cap() { return g_inject_replay_cap.load(); }
 bool inject_server_hold() { return g_inject_hold.load() != 0; }
+
+cudaError_t pool_malloc_async(void** p, size_t bytes, cudaStream_t s) {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaMallocAsync(p, bytes, s);
+  cudaMemPool_t pool = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pools[dev]) {
+      cudaMemPoolProps props = {};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.handleTypes = cudaMemHandleTypeNone;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = dev;
+      e = cudaMemPoolCreate(&pools[dev], &props);
+      if (e != cudaSuccess) {
+        pools[dev] = nullptr;
+        return e;
+      }
+      unsigned long long keep = kPoolKeepBytes;
+      e = cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+      if (e != cudaSuccess) return e;
+    }
+    pool = pools[dev];
+  }
+  return cudaMallocFromPoolAsync(p, bytes, pool, s);
+}
 
 int num_sms() {
   static thread_local int cached = 0;

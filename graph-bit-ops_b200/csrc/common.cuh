@@ -81,6 +81,19 @@ inline unsigned blocks_for(long long n, int tpb) {
 
 int num_sms();
 
+// Stream-ordered temporaries come from a pool of the library's own (one per
+// device, created on first use) that keeps up to kPoolKeepBytes of freed
+// memory mapped: the default pool returns freed memory at every
+// synchronisation, so calls that allocate and synchronise (packing, SpGEMM,
+// the GPU reader) mapped fresh memory each time, at a cost that varied
+// severalfold from run to run.  Free with cudaFreeAsync.
+constexpr unsigned long long kPoolKeepBytes = 8ull << 30;
+cudaError_t pool_malloc_async(void** p, size_t bytes, cudaStream_t s);
+template <typename T>
+inline cudaError_t pool_malloc_async(T** p, size_t bytes, cudaStream_t s) {
+  return pool_malloc_async(reinterpret_cast<void**>(p), bytes, s);
+}
+
 // Host-side fault injection (gbo_debug_inject): true when this host CSR
 // allocation is the one armed to fail; the replay cap of the iteration
 // loops (0: none); whether server workers hold admission.

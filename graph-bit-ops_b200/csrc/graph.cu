@@ -77,11 +77,11 @@ int upload_csr(const int* rowptr, const int* colind, int nrows, long long nnz, b
 
 int tril_device(const DevCsr& in, int nrows, cudaStream_t s, DevCsr* out) {
   int* cnt = nullptr;
-  GBO_CUDA_TRY(cudaMallocAsync(&cnt, sizeof(int) * ((size_t)nrows + 1), s));
+  GBO_CUDA_TRY(pool_malloc_async(&cnt, sizeof(int) * ((size_t)nrows + 1), s));
   GBO_CUDA_TRY(cudaMalloc(&out->rowptr, sizeof(int) * ((size_t)nrows + 1)));
   out->owned = true;
   long long* tot = nullptr;
-  GBO_CUDA_TRY(cudaMallocAsync(&tot, sizeof(long long), s));
+  GBO_CUDA_TRY(pool_malloc_async(&tot, sizeof(long long), s));
   if (nrows > 0) k_tril_count<<<blocks_for_warps(nrows, 8), 256, 0, s>>>(in.rowptr, in.colind, nrows, cnt);
   GBO_TRY(exclusive_scan_i32(cnt, out->rowptr, nrows, tot, s));
   long long h = 0;
@@ -508,7 +508,7 @@ extern "C" int gbo_tune_tile_width(const int* rowptr, const int* colind, int nro
           // stop at a row's first frontier neighbour, so a BFS reads less)
           unsigned long long* d = nullptr;
           unsigned long long rw = 0;
-          if (cudaMallocAsync(&d, sizeof(rw), s) != cudaSuccess || cudaMemsetAsync(d, 0, sizeof(rw), s) != cudaSuccess) {
+          if (pool_malloc_async(&d, sizeof(rw), s) != cudaSuccess || cudaMemsetAsync(d, 0, sizeof(rw), s) != cudaSuccess) {
             st = fail(GBO_ERR_NOMEM, "tuner counter");
           } else {
             const int grid = (int)std::min<long long>(((long long)nrows + 255) / 256, 4096);

@@ -163,7 +163,7 @@ struct DevMem {
   int alloc(size_t bytes) {
     if (p) cudaFreeAsync(p, s);
     p = nullptr;
-    GBO_CUDA_TRY(cudaMallocAsync(&p, bytes ? bytes : 1, s));
+    GBO_CUDA_TRY(pool_malloc_async(&p, bytes ? bytes : 1, s));
     return GBO_OK;
   }
 };

@@ -416,7 +416,7 @@ int exclusive_scan(const int* d_in, OutT* d_out, long long n, long long* d_total
   long long nb = (n + kScanTPB - 1) / kScanTPB;
   if (nb < 1) nb = 1;
   long long* sums = nullptr;
-  GBO_CUDA_TRY(cudaMallocAsync(&sums, sizeof(long long) * nb, s));
+  GBO_CUDA_TRY(pool_malloc_async(&sums, sizeof(long long) * nb, s));
   k_scan_block_sums<<<(unsigned)nb, kScanTPB, 0, s>>>(d_in, n, sums);
   k_scan_sums<<<1, kScanTPB, 0, s>>>(sums, nb, d_total);
   k_scan_apply<OutT><<<(unsigned)nb, kScanTPB, 0, s>>>(d_in, n, sums, d_out, d_total);
@@ -444,8 +444,8 @@ static int nnzb_impl(const int* rowptr, const int* colind, int nrows, int ncols,
   int* counts = nullptr;
   long long* d_total = nullptr;
   unsigned* derr = nullptr;
-  GBO_CUDA_TRY(cudaMallocAsync(&counts, sizeof(int) * (size_t)(nbr > 0 ? nbr : 1), s));
-  GBO_CUDA_TRY(cudaMallocAsync(&d_total, sizeof(long long) + sizeof(unsigned) * 2, s));
+  GBO_CUDA_TRY(pool_malloc_async(&counts, sizeof(int) * (size_t)(nbr > 0 ? nbr : 1), s));
+  GBO_CUDA_TRY(pool_malloc_async(&d_total, sizeof(long long) + sizeof(unsigned) * 2, s));
   derr = reinterpret_cast<unsigned*>(d_total + 1);
   GBO_CUDA_TRY(cudaMemsetAsync(derr, 0, sizeof(unsigned), s));
   int st = GBO_OK;
@@ -481,7 +481,7 @@ int count_tiles(const int* d_rowptr, const int* d_colind, int nrows, int ncols, 
                 long long* nblk, cudaStream_t s) {
   const int nbr = (nrows + b - 1) / b;
   int* tmp = nullptr;
-  GBO_CUDA_TRY(cudaMallocAsync(&tmp, sizeof(int) * ((size_t)nbr + 1), s));
+  GBO_CUDA_TRY(pool_malloc_async(&tmp, sizeof(int) * ((size_t)nbr + 1), s));
   const int st = nnzb_impl(d_rowptr, d_colind, nrows, ncols, nnz, b, tmp, nblk, s);
   cudaFreeAsync(tmp, s);
   return st;
@@ -493,7 +493,7 @@ static int fill_impl(const int* rowptr, const int* colind, int nrows, int ncols,
   const int nbr = (nrows + b - 1) / b;
   if (nbr == 0) return GBO_OK;
   unsigned* derr = nullptr;
-  GBO_CUDA_TRY(cudaMallocAsync(&derr, sizeof(unsigned), s));
+  GBO_CUDA_TRY(pool_malloc_async(&derr, sizeof(unsigned), s));
   GBO_CUDA_TRY(cudaMemsetAsync(derr, 0, sizeof(unsigned), s));
   int st = dispatch_pack(b, true, rowptr, colind, nrows, ncols, nnz, nbr, nullptr, bsr_rowptr,
                          bsr_colind, bsr_val, layout, derr, s);
@@ -587,13 +587,13 @@ int build_schedule(gbo_graph* g, cudaStream_t s) {
   int *item_off = nullptr, *slot_off = nullptr, *split_off = nullptr;
   long long* tot = nullptr;
   size_t n1 = (size_t)nbr + 1;
-  GBO_CUDA_TRY(cudaMallocAsync(&nchunk, sizeof(int) * n1 * 6, s));
+  GBO_CUDA_TRY(pool_malloc_async(&nchunk, sizeof(int) * n1 * 6, s));
   nslot = nchunk + n1;
   issplit = nslot + n1;
   item_off = issplit + n1;
   slot_off = item_off + n1;
   split_off = slot_off + n1;
-  GBO_CUDA_TRY(cudaMallocAsync(&tot, sizeof(long long) * 3, s));
+  GBO_CUDA_TRY(pool_malloc_async(&tot, sizeof(long long) * 3, s));
   k_sched_counts<<<blocks_for(nbr, 256), 256, 0, s>>>(g->rowptr, nbr, g->chunk, nchunk, nslot,
                                                       issplit);
   GBO_TRY(exclusive_scan_i32(nchunk, item_off, nbr, tot + 0, s));
@@ -690,8 +690,8 @@ int build_rowwords(gbo_graph* g, cudaStream_t s) {
   if (!g->rowmask || g->rowword || g->nitems <= 0) return GBO_OK;
   int* cnt = nullptr;
   long long* tot = nullptr;
-  GBO_CUDA_TRY(cudaMallocAsync(&cnt, sizeof(int) * (size_t)g->nitems, s));
-  GBO_CUDA_TRY(cudaMallocAsync(&tot, sizeof(long long), s));
+  GBO_CUDA_TRY(pool_malloc_async(&cnt, sizeof(int) * (size_t)g->nitems, s));
+  GBO_CUDA_TRY(pool_malloc_async(&tot, sizeof(long long), s));
   GBO_CUDA_TRY(cudaMalloc(&g->item_wbase, sizeof(long long) * ((size_t)g->nitems + 1)));
   g->device_bytes += 8LL * (g->nitems + 1);
   int nsm = 148, dev = 0;
@@ -777,8 +777,8 @@ int build_rws(gbo_graph* g, cudaStream_t s) {
   const long long rows = (long long)g->nbr * 32;
   int* len = nullptr;
   long long* tot = nullptr;
-  GBO_CUDA_TRY(cudaMallocAsync(&len, sizeof(int) * (size_t)rows, s));
-  GBO_CUDA_TRY(cudaMallocAsync(&tot, sizeof(long long), s));
+  GBO_CUDA_TRY(pool_malloc_async(&len, sizeof(int) * (size_t)rows, s));
+  GBO_CUDA_TRY(pool_malloc_async(&tot, sizeof(long long), s));
   GBO_CUDA_TRY(cudaMalloc(&g->rws_tail_ptr, sizeof(long long) * (size_t)(rows + 1)));
   GBO_CUDA_TRY(cudaMalloc(&g->rws_head, sizeof(uint2) * (size_t)rows * kRwsHead));
   g->device_bytes += 8LL * (rows + 1) + 8LL * rows * kRwsHead;
@@ -965,7 +965,7 @@ extern "C" int gbo_invdeg_from_rowptr(const int* d_rowptr, int n, float* d_inv, 
   if (n == 0) return GBO_OK;
   cudaStream_t s = as_stream(stream);
   int* deg = nullptr;
-  GBO_CUDA_TRY(cudaMallocAsync(&deg, sizeof(int) * (size_t)n, s));
+  GBO_CUDA_TRY(pool_malloc_async(&deg, sizeof(int) * (size_t)n, s));
   k_row_len<<<blocks_for(n, 256), 256, 0, s>>>(d_rowptr, n, deg);
   k_inv<<<blocks_for(n, 256), 256, 0, s>>>(deg, n, d_inv);
   cudaError_t e = cudaGetLastError();

@@ -244,7 +244,7 @@ extern "C" int gbo_bfs_sharded(const gbo_graph* shard, int rank, int world, cons
                            wb * (size_t)S.width * (size_t)world + 8, sizeof(int) * ((size_t)world + 1)};
   int st = GBO_OK;
   for (int i = 0; i < 6 && st == GBO_OK; ++i) {
-    const cudaError_t e = cudaMallocAsync(&mem[i], sizes[i], S.s);
+    const cudaError_t e = pool_malloc_async(&mem[i], sizes[i], S.s);
     if (e != cudaSuccess) st = fail_cuda(e, "gbo_bfs_sharded buffers");
   }
   if (st == GBO_OK) {

@@ -253,7 +253,7 @@ struct DevBuf {
   int alloc(size_t bytes, cudaStream_t st) {
     release();
     s = st;
-    GBO_CUDA_TRY(cudaMallocAsync(&p, bytes ? bytes : 1, st));
+    GBO_CUDA_TRY(pool_malloc_async(&p, bytes ? bytes : 1, st));
     return GBO_OK;
   }
 };

@@ -366,7 +366,7 @@ extern "C" int gbo_tc(const gbo_graph* lower, uint64_t* h_count, gbo_stream_t st
   if (!h_count) return fail(GBO_ERR_INVALID, "count is NULL");
   cudaStream_t s = as_stream(stream);
   unsigned long long* d = nullptr;
-  GBO_CUDA_TRY(cudaMallocAsync(&d, sizeof(unsigned long long), s));
+  GBO_CUDA_TRY(pool_malloc_async(&d, sizeof(unsigned long long), s));
   int st = tc_launch(const_cast<gbo_graph*>(lower), d, s);
   unsigned long long h = 0;
   if (st == GBO_OK) {
