@@ -827,7 +827,11 @@ def run_ours(args, ws, rank, local):
                      "kernel": kernel_name, "peak_source": peak_src,
                      "levels": pull_lv, "launch": rl_launch,
                      "algorithmic_bytes_per_launch": float(np.mean(rl_bytes)),
-                     "ms_per_launch": float(np.mean(rl_ms))},
+                     "ms_per_launch": float(np.mean(rl_ms)),
+                     # the DRAM traffic (scaled capture) over the same time:
+                     # how busy HBM is, beside the algorithmic fraction
+                     "traffic_frac": (traffic / (float(np.mean(rl_ms)) / 1e3) / 1e9 / peak
+                                      if traffic is not None else None)},
         "e2e": {"value": ws * edges / (e2e_ms / 1e3) / 1e9, "unit": "GTEPS",
                 "h2d_bytes_per_step": 4, "d2h_bytes_per_step": 4 * n,
                 "overlap": "read-back of step i on a copy stream during step i+1 (two level buffers)"},
