@@ -1274,7 +1274,11 @@ __device__ __forceinline__ PrIter pr_iter(float* pr, float* prs, const Ctrl* ctr
   return p;
 }
 
-__global__ void __launch_bounds__(kTPB) k_pr_step_rws(GView v, float* __restrict__ pr, float* __restrict__ prs,
+// Five blocks per SM (48 registers, a few spilled): the step is bound by the
+// latency of its gathers, and R-MAT 22 iterations took 1.05 ms at the 71
+// registers (3 blocks per SM) the compiler chose unbounded, 0.97 ms at 4
+// blocks and 0.90 ms at 5 to 8.
+__global__ void __launch_bounds__(kTPB, 5) k_pr_step_rws(GView v, float* __restrict__ pr, float* __restrict__ prs,
                                                       const float* __restrict__ inv,
                                                       const float* __restrict__ pv, Ctrl* __restrict__ ctrl) {
   __shared__ double pr_tail_sh[kTPB / 32][32];
