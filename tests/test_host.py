@@ -1,6 +1,7 @@
 """CPU-side checks of libgbo: the C ABI loads and exports every symbol in
 include/gbo.h, and the host input path (readers, CSR utilities, generators)
 matches the oracle's restatements.  No device calls."""
+import ctypes
 import os
 import re
 
@@ -171,3 +172,13 @@ def test_csr_transpose_and_tril(gbo):
 def test_mesh_edge_count_closed_form(gbo):
     m = gbo.gen_king_mesh(64)
     assert m.nnz // 2 == 2 * 64 * 63 + 2 * 63 * 63
+
+
+def test_null_handles_are_rejected_without_a_gpu(gbo):
+    """The setters validate their arguments on the host: a NULL graph or
+    server handle is GBO_ERR_INVALID, with no device touched."""
+    lib = gbo.lib()
+    assert lib.gbo_graph_set_bfs_loop(None, gbo.BFS_LOOP_COOP, 0) == gbo.GBO_ERR_INVALID
+    assert lib.gbo_graph_set_bfs_direction(None, 1, -1) == gbo.GBO_ERR_INVALID
+    assert lib.gbo_server_set_admission(None, ctypes.c_float(0.5)) == gbo.GBO_ERR_INVALID
+    assert lib.gbo_server_set_queue_limit(None, 10) == gbo.GBO_ERR_INVALID
