@@ -115,12 +115,15 @@ __device__ __forceinline__ void block_row_epilogue(const Args& a, int R, int lvl
       a.V[o] = vn;
       cnt += __popc(nw);
       anyw |= nw;
-      uint32_t m = nw;
-      while (m) {
-        const int p = __ffs(m) - 1;
-        m &= m - 1;
-        a.levels[level_index(a, i, w * 32 + p)] = lvl + 1;
-      }
+    }
+    // levels of the pass's new (vertex, source) pairs: in step t every lane
+    // takes one bit of lane t's word (row rr + t / KW, word t % KW), so
+    // consecutive lanes write consecutive sources of one vertex
+    for (int t = 0; t < 32; ++t) {
+      const uint32_t wt = __shfl_sync(0xffffffffu, nw, t);
+      if (!wt) continue;
+      if ((wt >> lane) & 1u)
+        a.levels[level_index(a, (long long)R * 32 + rr + t / KW, (t % KW) * 32 + (int)lane)] = lvl + 1;
     }
 #pragma unroll
     for (int q = 0; q < S; ++q) {
