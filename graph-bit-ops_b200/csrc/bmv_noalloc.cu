@@ -9,8 +9,10 @@
 // arrays (as the reference's bmv{b}_sparse launches do) and allocates no
 // device or host memory at any call.
 //
-// Work split: the tile range [0, nblocks) is cut into fixed chunks of
-// kChunk<B> tiles; a group of W = min(b, 32) lanes takes one chunk (lane r
+// Work split: the tile range [0, nblocks) is cut into chunks of `chunk`
+// tiles, sized per call: enough chunks for every lane group the GPU holds
+// at once (so that a graph of 10^5 tiles is not one warp per SM), between
+// 64 and 32768 / b tiles; a group of W = min(b, 32) lanes takes one chunk (lane r
 // owns tile row r, and r + 32 for b = 64).  A block row that lies wholly
 // inside a chunk is written to y directly.  A block row that crosses a
 // chunk boundary leaves one partial per chunk it touches in a file-scope
@@ -57,9 +59,11 @@ struct NL {  // lane layout: W lanes per chunk, G chunks per warp
   static constexpr int RPL = B > 32 ? 2 : 1;
 };
 
-// Tiles per chunk: 32768 / b (1024 tiles of 32 words at b = 32).
+// Tiles per chunk: at most 32768 / b (1024 tiles of 32 words at b = 32),
+// which bounds a call's chunks by the scratch, and at least kMinChunk.
 template <int B>
 constexpr long long kChunk = 32768 / B;
+constexpr long long kMinChunk = 64;
 
 __device__ __forceinline__ int count_bits(unsigned long long w) { return __popcll(w); }
 
@@ -91,7 +95,7 @@ template <int B, bool OUTF>
 __global__ void __launch_bounds__(kTPB) k_count_chunks(
     const int* __restrict__ rowptr, const int* __restrict__ colind,
     const typename Word<B>::T* __restrict__ val, const typename Word<B>::T* __restrict__ x,
-    void* __restrict__ y, int nrows, int nbr, int nbc, long long nblk, long long nchunks,
+    void* __restrict__ y, int nrows, int nbr, int nbc, long long nblk, long long nchunks, long long chunk,
     int accumulate, int* __restrict__ scratch) {
   using WT = typename Word<B>::T;
   using L = NL<B>;
@@ -100,8 +104,8 @@ __global__ void __launch_bounds__(kTPB) k_count_chunks(
   const long long c = warp * L::G + lane / L::W;
   if (c >= nchunks) return;
   const int r = lane % L::W;
-  const long long t0 = c * kChunk<B>;
-  const long long t1 = t0 + kChunk<B> < nblk ? t0 + kChunk<B> : nblk;
+  const long long t0 = c * chunk;
+  const long long t1 = t0 + chunk < nblk ? t0 + chunk : nblk;
   int R = row_of(rowptr, nbr, t0);
   long long t = t0;
   while (t < t1 && R < nbr) {
@@ -147,7 +151,7 @@ __global__ void __launch_bounds__(kTPB) k_count_chunks(
 // when accumulating); rows split over chunks get the sum of their partials.
 template <int B, bool OUTF>
 __global__ void k_count_rows(const int* __restrict__ rowptr, void* __restrict__ y, int nrows,
-                             int nbr, long long nblk, int accumulate,
+                             int nbr, long long nblk, long long chunk, int accumulate,
                              const int* __restrict__ scratch) {
   const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (gid >= (long long)nbr * B) return;
@@ -159,7 +163,7 @@ __global__ void k_count_rows(const int* __restrict__ rowptr, void* __restrict__ 
     put<B, OUTF>(y, (long long)R * B + r, nrows, 0, accumulate);
     return;
   }
-  const long long cs = rs / kChunk<B>, ce = (re - 1) / kChunk<B>;
+  const long long cs = rs / chunk, ce = (re - 1) / chunk;
   if (cs == ce) return;  // written by k_count_chunks
   long long s = scratch[(cs * 2 + 1) * B + r];
   for (long long q = cs + 1; q <= ce; ++q) s += scratch[(q * 2) * B + r];
@@ -171,23 +175,31 @@ int launch(int nrows, int nbr, int nbc, long long nblk, const int* rowptr, const
            const void* x, void* y, int out_type, int accumulate, int* scratch, cudaStream_t s) {
   using WT = typename Word<B>::T;
   using L = NL<B>;
-  const long long nchunks = (nblk + kChunk<B> - 1) / kChunk<B>;
+  // enough chunks for every lane group resident on the GPU, within
+  // [kMinChunk, kChunk<B>] tiles (the upper bound keeps 2 * nchunks * b
+  // partial ints inside the scratch: nblk was checked against it)
+  const long long groups = (long long)num_sms() * 64 * L::G;
+  long long chunk = (nblk + groups - 1) / groups;
+  chunk = chunk < kMinChunk ? kMinChunk : chunk > kChunk<B> ? kChunk<B> : chunk;
+  const long long fit = (nblk * 2 * B + kScratchInts - 1) / kScratchInts;  // chunks must fit the scratch
+  if (chunk < fit) chunk = fit;
+  const long long nchunks = (nblk + chunk - 1) / chunk;
   if (nchunks > 0) {
     const long long warps = (nchunks + L::G - 1) / L::G;
     const unsigned grid = blocks_for_warps(warps, kTPB / 32);
     if (out_type == GBO_OUT_F32)
       k_count_chunks<B, true><<<grid, kTPB, 0, s>>>(rowptr, colind, (const WT*)val, (const WT*)x, y,
-                                                    nrows, nbr, nbc, nblk, nchunks, accumulate, scratch);
+                                                    nrows, nbr, nbc, nblk, nchunks, chunk, accumulate, scratch);
     else
       k_count_chunks<B, false><<<grid, kTPB, 0, s>>>(rowptr, colind, (const WT*)val, (const WT*)x, y,
-                                                     nrows, nbr, nbc, nblk, nchunks, accumulate, scratch);
+                                                     nrows, nbr, nbc, nblk, nchunks, chunk, accumulate, scratch);
   }
   if (nbr > 0) {
     const unsigned grid = blocks_for((long long)nbr * B, kTPB);
     if (out_type == GBO_OUT_F32)
-      k_count_rows<B, true><<<grid, kTPB, 0, s>>>(rowptr, y, nrows, nbr, nblk, accumulate, scratch);
+      k_count_rows<B, true><<<grid, kTPB, 0, s>>>(rowptr, y, nrows, nbr, nblk, chunk, accumulate, scratch);
     else
-      k_count_rows<B, false><<<grid, kTPB, 0, s>>>(rowptr, y, nrows, nbr, nblk, accumulate, scratch);
+      k_count_rows<B, false><<<grid, kTPB, 0, s>>>(rowptr, y, nrows, nbr, nblk, chunk, accumulate, scratch);
   }
   GBO_CUDA_TRY(cudaGetLastError());
   return GBO_OK;

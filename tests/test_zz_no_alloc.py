@@ -73,11 +73,14 @@ def test_noalloc_rejects_graphs_beyond_its_scratch(gbo, gpu):
 
 @pytest.mark.parametrize("b", WIDTHS)
 def test_noalloc_chunk_boundaries_hand_built(gbo, orc, gpu, b):
-    """Block rows sized from the entry point's chunk of 32768 / b tiles: a row
-    ending inside chunk 0, a row starting mid-chunk and crossing into chunk 1
-    (slot 1 of chunk 0, slot 0 of chunk 1), several whole rows in chunk 1, an
-    empty row, a row starting mid-chunk that spans at least three chunks, and
-    short rows at the end.  Counts against the oracle, two calls in a row."""
+    """Block rows sized from the entry point's largest chunk, K = 32768 / b
+    tiles (what large graphs run at): a row ending inside the first K tiles,
+    a row crossing into the second, several short rows, an empty row, a row
+    spanning at least three K, and short rows at the end.  A graph this small
+    runs at the smallest chunk (64 tiles), so its long rows cross many chunk
+    boundaries (slot 1 of their first chunk, slot 0 of the others) and short
+    rows sit whole or split inside chunks.  Counts against the oracle, two
+    calls in a row."""
     K = 32768 // b
     lens = [K // 2, K, 3, 5, 1, 0, 7, 3 * K + K // 3, 0, 2, 9]
     nbr = len(lens)
