@@ -1723,6 +1723,41 @@ def suite_refgpu(args):
             x.free()
 
 
+def suite_noalloc(args):
+    """BMV count straight from caller-owned B2SR arrays (gbo_bmv_count_noalloc,
+    no allocation) against the graph-handle BMV (gbo_bmv_count) on R-MAT 14,
+    17 and 20 at b = 32, x of density 0.5: time per call and equal counts."""
+    import gbo
+
+    peak, psrc = load_peaks()
+    rows = {}
+    for scale in (14, 17, 20):
+        csr = gbo.gen_rmat(scale, EDGE_FACTOR, seed=SEED, **RMAT)
+        g = gbo.Graph.from_csr(csr, 32)
+        rp, ci, w = g.b2sr()
+        n = csr.nrows
+        drp, dci, dv = (gbo.DeviceBuffer.from_numpy(a) for a in (rp, ci, w))
+        x = (np.random.default_rng(0).random(n) < 0.5).astype(np.int32)
+        dx = gbo.DeviceBuffer.from_numpy(gbo.bits_from_numpy(x, 32))
+        y1, y2 = gbo.DeviceBuffer(4 * n), gbo.DeviceBuffer(4 * n)
+        handle_ms = _timed(gbo, lambda: g.bmv_count(dx, y1), 20, args.warmup)
+        na_ms = _timed(gbo, lambda: gbo.check(gbo.lib().gbo_bmv_count_noalloc(
+            n, n, 32, len(ci), drp.ptr, dci.ptr, dv.ptr, dx.ptr, y2.ptr, gbo.OUT_I32, 0, None), "bmv_noalloc"),
+            20, args.warmup)
+        # the BMV model: tiles (128-byte words + 4-byte column), block-row
+        # offsets, x words (one per block column) and y
+        by = len(ci) * (32 * 32 // 8 + 4) + 4 * len(rp) + 4 * (len(rp) - 1) + 4 * n
+        rows[f"rmat{scale}"] = {"tiles": int(len(ci)), "noalloc_ms": na_ms, "handle_ms": handle_ms,
+                                "noalloc_frac": by / (na_ms / 1e3) / 1e9 / peak,
+                                "equal": bool(np.array_equal(y1.to_numpy(np.int32, n), y2.to_numpy(np.int32, n)))}
+        g.free()
+    top = rows["rmat20"]
+    _line("ms", top["noalloc_ms"], "ms per call", False, top["noalloc_ms"], args,
+          {"workload": "gbo_bmv_count_noalloc vs gbo_bmv_count, R-MAT 14/17/20 (seed 0), B2SR 32, x density 0.5"},
+          dtype="u32", by_graph=rows, peak_source=psrc,
+          parity={"checked": "int32 counts of the two entry points, every row", "equal": all(r["equal"] for r in rows.values())})
+
+
 SUITE = {
     "sssp": lambda a: suite_config2(a, "sssp"),
     "cc": lambda a: suite_config2(a, "cc"),
@@ -1734,6 +1769,7 @@ SUITE = {
     "serve": suite_serve,
     "spgemm": suite_spgemm,
     "ingest": suite_ingest,
+    "noalloc": suite_noalloc,
 }
 
 
