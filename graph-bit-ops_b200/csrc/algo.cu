@@ -87,6 +87,7 @@ struct AlgoState {
   unsigned long long* stamps = nullptr;  // kStampCap + 1 iteration end times
   int launches_per_iter = 0;             // kernels of one loop iteration
   int fixed_launches = 2;                // kernels of a run outside its iterations
+  bool coop_run = false;                 // the last run was a cooperative BFS
   bool stats_pending = false;            // step times not yet read back
 
   // statistics of the last algorithm run
@@ -924,7 +925,8 @@ __device__ __forceinline__ unsigned long long global_ns() {
 // or sees that another block gave up, sets bar_err and returns false: the
 // caller leaves the kernel, so every block ends within about one limit of
 // the first failure.
-__device__ __forceinline__ bool grid_barrier(Ctrl* c, const unsigned long long* sum_src = nullptr, int nsum = 0,
+__device__ __forceinline__ bool grid_barrier(Ctrl* c, unsigned long long limit_ns,
+                                             const unsigned long long* sum_src = nullptr, int nsum = 0,
                                              int sum_stride = 1, unsigned long long* sum = nullptr) {
   __shared__ int ok;
   __shared__ unsigned long long sh_sum;
@@ -938,7 +940,7 @@ __device__ __forceinline__ bool grid_barrier(Ctrl* c, const unsigned long long* 
     int res = 1;
     const unsigned long long t0 = global_ns();
     for (long long k = 0; ((old ^ *word) & 0x80000000u) == 0u; ++k) {
-      if (*err || k >= kBarrierPollCap || global_ns() - t0 > kBarrierLimitNs) {
+      if (*err || k >= kBarrierPollCap || global_ns() - t0 > limit_ns) {
         atomicExch(&c->bar_err, 1u);
         res = 0;
         break;
@@ -1061,8 +1063,13 @@ __device__ __forceinline__ unsigned long long push_rws_long(const GView& v, unsi
   return cnt;
 }
 
+// limit_ns bounds every barrier wait (kBarrierLimitNs; shorter in the
+// failure-path test, which also names a block that leaves at once, before
+// the first barrier: skip_block, -1 for none).
 __global__ void __launch_bounds__(kTPB, kCoopBlocksPerSM) k_bfs_coop(GView v, unsigned* front, unsigned* visited,
-                                                                  int* level, Ctrl* ctrl, long long* push_list) {
+                                                                  int* level, Ctrl* ctrl, long long* push_list,
+                                                                  unsigned long long limit_ns, int skip_block) {
+  if ((int)blockIdx.x == skip_block) return;
   // the loop's starting state: written before the launch and changed by
   // block 0 only after the first barrier, so plain (cached) loads -- one
   // L2 request per SM instead of one per warp
@@ -1082,13 +1089,13 @@ __global__ void __launch_bounds__(kTPB, kCoopBlocksPerSM) k_bfs_coop(GView v, un
       cnt = push_rws_rows(v, front, visited, level, lvl, &ctrl->push_acc[lvl % 3], push_list);
       if (hubs) {  // the listed long tails, after every block listed its rows
         unsigned long long acc = 0;
-        if (!grid_barrier(ctrl, &ctrl->push_acc[lvl % 3], 1, 1, &acc)) return;
+        if (!grid_barrier(ctrl, limit_ns, &ctrl->push_acc[lvl % 3], 1, 1, &acc)) return;
         if (acc) cnt += push_rws_long(v, front, visited, level, lvl, acc, push_list);
       }
     }
     block_add_u64(cnt, &ctrl->lvl_part[lvl % 3][blockIdx.x & 7][0]);
     unsigned long long tot = 0;
-    if (!grid_barrier(ctrl, &ctrl->lvl_part[lvl % 3][0][0], 8, 16, &tot)) return;
+    if (!grid_barrier(ctrl, limit_ns, &ctrl->lvl_part[lvl % 3][0][0], 8, 16, &tot)) return;
     const unsigned long long nf = tot & kLongMask;
     hubs = (tot >> kLongShift) != 0ull;
     const int it = lvl + 1;
@@ -1447,6 +1454,7 @@ __global__ void k_pr_init(float* pr, float* prs, const float* inv, const float* 
     ctrl->count = 0;
     ctrl->err = 0;
     ctrl->last_err = 0;
+    ctrl->bar_err = 0u;
     ctrl->tol = tol;
     ctrl->alpha = alpha;
     ctrl->add = add;
@@ -1696,6 +1704,7 @@ __global__ void k_cc_init(int* f, int* gf, int* mngf, int n, Ctrl* ctrl, int max
     ctrl->count = 0;
     ctrl->err = 0;
     ctrl->last_err = 0;
+    ctrl->bar_err = 0u;
   }
 }
 
@@ -1884,11 +1893,13 @@ int injected_cap_iters() {
 }
 
 // After a loop run was queued: wait for it when the caller wants the
-// iteration count or a cap was injected, and check how it ended.
-int finish_loop(AlgoState* a, cudaStream_t s, int max_iter, int cap_iters, int* iters, bool coop = false) {
+// iteration count or a cap or a barrier skip was injected, and check how it
+// ended.
+int finish_loop(AlgoState* a, cudaStream_t s, int max_iter, int cap_iters, int* iters, bool coop = false,
+                bool must_wait = false) {
   a->replays = 1;
   a->stats_pending = true;
-  if (!iters && cap_iters == 0) return GBO_OK;
+  if (!iters && cap_iters == 0 && !must_wait) return GBO_OK;
   GBO_CUDA_TRY(cudaMemcpyAsync(a->h_ctrl, a->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, s));
   GBO_CUDA_TRY(cudaStreamSynchronize(s));
   if (coop && a->h_ctrl->bar_err) return fail(GBO_ERR_TIMEOUT, "cooperative BFS: a grid barrier gave up");
@@ -1905,6 +1916,7 @@ int run_until_done(AlgoState* a, int id, cudaStream_t s, int max_iter, int* iter
   GBO_CUDA_TRY(cudaGetLastError());
   GBO_CUDA_TRY(cudaGraphLaunch(a->exec[id], s));
   a->fixed_launches = 2;  // init and loop start kernels
+  a->coop_run = false;
   return finish_loop(a, s, max_iter, cap_iters, iters);
 }
 
@@ -1943,11 +1955,17 @@ int run_bfs_coop(gbo_graph* g, AlgoState* a, const GView& v, unsigned* front, un
   long long* list = a->push_list;
   GView va = v;
   Ctrl* ctrl = a->ctrl;
-  void* args[] = {&va, &front, &vis, &level, &ctrl, &list};
+  // failure-path test (GBO_INJECT_BARRIER_SKIP): a block that never arrives
+  // and a 100 ms limit, so that the others' bounded wait runs out
+  const long long skip = take_inject_barrier_skip();
+  unsigned long long limit_ns = skip > 0 ? 100000000ull : kBarrierLimitNs;
+  int skip_block = skip > 0 ? (int)std::min<long long>(skip - 1, (long long)grid - 1) : -1;
+  void* args[] = {&va, &front, &vis, &level, &ctrl, &list, &limit_ns, &skip_block};
   GBO_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_bfs_coop, dim3(grid), dim3(kTPB), args, 0, s));
   a->fixed_launches = 2;  // init and the cooperative loop
+  a->coop_run = true;
   a->launches_per_iter = 0;
-  return finish_loop(a, s, max_iter, cap_iters, iters, true);
+  return finish_loop(a, s, max_iter, cap_iters, iters, true, skip > 0);
 }
 
 // Step times and counts of the last loop run, read back on first request.
@@ -1956,6 +1974,8 @@ int collect_stats(AlgoState* a) {
   a->stats_pending = false;
   GBO_CUDA_TRY(cudaDeviceSynchronize());
   GBO_CUDA_TRY(cudaMemcpy(a->h_ctrl, a->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+  // a stream-ordered cooperative BFS whose grid barrier gave up reports it here
+  if (a->coop_run && a->h_ctrl->bar_err) return fail(GBO_ERR_TIMEOUT, "cooperative BFS: a grid barrier gave up");
   const int it = a->h_ctrl->iter;
   const int nst = std::min(it, kStampCap);
   std::vector<unsigned long long> t((size_t)nst + 1);

@@ -41,6 +41,7 @@ namespace {
 std::atomic<long long> g_inject_alloc{0};
 std::atomic<long long> g_inject_replay_cap{0};
 std::atomic<int> g_inject_hold{0};
+std::atomic<long long> g_inject_barrier{0};
 }  // namespace
 
 bool inject_host_alloc_fails() {
@@ -51,6 +52,7 @@ bool inject_host_alloc_fails() {
 }
 long long inject_replay_cap() { return g_inject_replay_cap.load(); }
 bool inject_server_hold() { return g_inject_hold.load() != 0; }
+long long take_inject_barrier_skip() { return g_inject_barrier.exchange(0); }
 
 cudaError_t pool_malloc_async(void** p, size_t bytes, cudaStream_t s) {
   static std::mutex mu;
@@ -125,6 +127,7 @@ extern "C" int gbo_debug_inject(int what, long long n) {
     case GBO_INJECT_HOST_ALLOC: g_inject_alloc.store(n); return GBO_OK;
     case GBO_INJECT_REPLAY_CAP: g_inject_replay_cap.store(n); return GBO_OK;
     case GBO_INJECT_SERVER_HOLD: g_inject_hold.store(n ? 1 : 0); return GBO_OK;
+    case GBO_INJECT_BARRIER_SKIP: g_inject_barrier.store(n); return GBO_OK;
   }
   return fail(GBO_ERR_INVALID, "unknown injection");
 }

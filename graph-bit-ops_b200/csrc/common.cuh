@@ -100,6 +100,8 @@ inline cudaError_t pool_malloc_async(T** p, size_t bytes, cudaStream_t s) {
 bool inject_host_alloc_fails();
 long long inject_replay_cap();
 bool inject_server_hold();
+// Armed GBO_INJECT_BARRIER_SKIP value (0: none), disarmed by the read.
+long long take_inject_barrier_skip();
 
 // Exclusive scan of n int32 counts into out[0..n] (out[n] = total) with the
 // total also returned through d_total (int64).  No spin waits: three kernels.

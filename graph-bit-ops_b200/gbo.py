@@ -30,6 +30,7 @@ GBO_ERR_FULL = 11
 INJECT_HOST_ALLOC = 1
 INJECT_REPLAY_CAP = 2
 INJECT_SERVER_HOLD = 3
+INJECT_BARRIER_SKIP = 4
 BFS_LOOP_AUTO = 0
 BFS_LOOP_GRAPH = 1
 BFS_LOOP_COOP = 2
@@ -308,7 +309,8 @@ def device_to_numpy(ptr: int, dtype, count: int, stream=None) -> np.ndarray:
 
 
 def debug_inject(what: int, n: int) -> None:
-    """Host-side fault injection (INJECT_*); n = 0 disarms."""
+    """Fault injection (INJECT_*): host-side failures, or (INJECT_BARRIER_SKIP)
+    a bounded device wait that runs out; n = 0 disarms."""
     check(lib().gbo_debug_inject(int(what), int(n)), "debug_inject")
 
 

@@ -614,8 +614,8 @@ GBO_API int gbo_gen_er_batch(int count, int nmin, int nmax, double avg_degree,
 /* ------------------------------------------------ host-side fault injection
  * For failure-path tests (the reference has no failure handling: its error
  * checks compile away, utility.cu:17-30).  Nothing here makes a GPU fault,
- * trap or hang; each knob changes a host-side decision.  Process-wide, off
- * by default; n = 0 disarms.
+ * trap or hang; each knob changes a host-side decision (the last one a
+ * launch argument).  Process-wide, off by default; n = 0 disarms.
  *   GBO_INJECT_HOST_ALLOC  (n >= 1) the n-th host CSR allocation from now on
  *       (readers, generators, CSR utilities) fails: the call returns
  *       GBO_ERR_NOMEM and leaves its output untouched;
@@ -623,8 +623,14 @@ GBO_API int gbo_gen_er_batch(int count, int nmin, int nmax, double avg_degree,
  *       PageRank, PPR, CC) replay their captured iterations at most n times
  *       and return GBO_ERR_TIMEOUT when the device has not finished by then;
  *   GBO_INJECT_SERVER_HOLD (n = 1) server workers admit no new query:
- *       submissions stay pending (queries already in flight finish). */
-enum { GBO_INJECT_HOST_ALLOC = 1, GBO_INJECT_REPLAY_CAP = 2, GBO_INJECT_SERVER_HOLD = 3 };
+ *       submissions stay pending (queries already in flight finish);
+ *   GBO_INJECT_BARRIER_SKIP (n >= 1) the next cooperative BFS launch (one
+ *       shot) is told that block n - 1 leaves before the first grid barrier
+ *       and that the barrier gives up after 100 ms instead of 5 s: the other
+ *       blocks' bounded wait runs out, every block leaves, and the
+ *       synchronous call returns GBO_ERR_TIMEOUT with the context usable. */
+enum { GBO_INJECT_HOST_ALLOC = 1, GBO_INJECT_REPLAY_CAP = 2, GBO_INJECT_SERVER_HOLD = 3,
+       GBO_INJECT_BARRIER_SKIP = 4 };
 GBO_API int gbo_debug_inject(int what, long long n);
 
 #ifdef __cplusplus

@@ -72,6 +72,29 @@ def test_replay_cap_returns_timeout_then_recovers(gbo, orc, gpu):
 
 
 @pytest.mark.gpu
+def test_cooperative_bfs_barrier_timeout_then_recovers(gbo, orc, gpu):
+    """A block of the cooperative BFS that leaves before its first grid
+    barrier: the other blocks' bounded wait (100 ms under the injection) runs
+    out, they set the barrier error and return, and gbo_bfs reports
+    GBO_ERR_TIMEOUT with the context usable.  The next BFS is exact."""
+    csr = gbo.gen_rmat(14, 16, seed=4)
+    g = gbo.Graph.from_csr(csr, 32, gbo.FLAG_SYMMETRIC)
+    g.set_bfs_loop(gbo.BFS_LOOP_COOP)
+    ref = orc.bfs_csr(csr.rowptr, csr.colind, csr.nrows, 0)[0]
+    for skip in (1, 3):  # block 0 (which completes the arrival word) and block 2
+        try:
+            gbo.debug_inject(gbo.INJECT_BARRIER_SKIP, skip)
+            with pytest.raises(gbo.GboError) as e:
+                g.bfs(0)
+            assert e.value.status == gbo.GBO_ERR_TIMEOUT
+        finally:
+            gbo.debug_inject(gbo.INJECT_BARRIER_SKIP, 0)
+        lv, _ = g.bfs(0)
+        assert np.array_equal(lv, ref)
+        assert g.last_run()["kernel_launches"] == 2
+
+
+@pytest.mark.gpu
 def test_server_timeout_hold_and_bounded_queue(gbo, orc, gpu):
     """While admission is held, submissions queue up to the limit and the
     next one returns GBO_ERR_FULL; waits give up with GBO_ERR_TIMEOUT and
