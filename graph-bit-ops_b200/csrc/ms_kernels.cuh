@@ -871,8 +871,10 @@ __global__ void __launch_bounds__(kTPB) k_seed_push(Args a, const int* __restric
 
 // Reset: levels -1, V 0, F[0] 0, frontier bits 0, padding rows and rows
 // without entries marked full (no source can reach them).  A source in such
-// a row reopens it in k_seed.
-static __global__ void k_init(Args a, int kw, int max_iter) {
+// a row reopens it in k_seed.  The level counter starts at lvl0 (levels are
+// written as lvl0 + hops; the query server's batches keep its absolute
+// level count) and the loop stops at max_iter.
+static __global__ void k_init(Args a, int kw, int max_iter, int lvl0 = 0) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long stride = (long long)gridDim.x * blockDim.x;
   const int n = a.v.nrows, nbr = a.v.nbr;
@@ -895,7 +897,7 @@ static __global__ void k_init(Args a, int kw, int max_iter) {
     a.slot_any[i] = 0u;
   }
   if (i == 0) {
-    a.ctl[0] = 0;
+    a.ctl[0] = lvl0;
     a.ctl[1] = 0;
     a.ctl[2] = 0;
     a.ctl[3] = max_iter;

@@ -42,6 +42,7 @@ struct MsState {
   cudaGraphExec_t exec = nullptr;
   const void* key_levels = nullptr;
   int key_k = -1;
+  int key_group = -1;
   long long key_push = -1;  // push threshold the graph was captured with (0: pull only)
   std::vector<float> step_ms;
   long long launches = 0;
@@ -60,7 +61,9 @@ long long ms_push_threshold(const gbo_graph* g, int kw) {
   return g->bfs_push_thr;
 }
 
-ms::Args make_args(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
+// level_group 0: the API's vertex-major levels[v * k + s]; 8: the query
+// server's layout (8 sources per 32-byte sector, ms::level_index)
+ms::Args make_args(gbo_graph* g, MsState& m, int32_t* d_levels, int k, int level_group) {
   ms::Args a;
   a.v = view_of(g);
   a.F = m.F;
@@ -77,7 +80,7 @@ ms::Args make_args(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
   a.active = m.active;
   a.retire = 1;  // columns whose traversal ended stop keeping rows open
   a.live = m.live;
-  a.level_group = 0;  // the API's vertex-major levels[v * k + s]
+  a.level_group = level_group;
   a.push_thr = ms_push_threshold(g, m.kw);
   a.dir = a.push_thr > 0 ? 1 : 0;
   a.push_acc = m.push_acc;
@@ -86,8 +89,8 @@ ms::Args make_args(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
 }
 
 template <int KW>
-int ms_capture(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
-  const ms::Args a = make_args(g, m, d_levels, k);
+int ms_capture(gbo_graph* g, MsState& m, int32_t* d_levels, int k, int level_group) {
+  const ms::Args a = make_args(g, m, d_levels, k, level_group);
   // k <= 64 on a graph with row-word slices: the pull step walks rows
   // (k_step_rws, whole block rows: no split partials for the finish kernel);
   // wider frontier rows go through the tiles (k_step), which measured 2x
@@ -145,10 +148,10 @@ int ms_capture(gbo_graph* g, MsState& m, int32_t* d_levels, int k) {
   return GBO_OK;
 }
 
-int msbfs_impl(gbo_graph* g, const int* h_srcs, int k, int32_t* d_levels, int* h_depth,
-               cudaStream_t s) {
-  if (!g->ms) g->ms = new MsState();
-  MsState& m = *reinterpret_cast<MsState*>(g->ms);
+// One multi-source BFS with state m.  Levels are written as lvl0 + hops in
+// the layout level_group selects; sources < 0 are empty columns.
+int msbfs_impl(gbo_graph* g, MsState& m, const int* h_srcs, int k, int32_t* d_levels, int level_group, int lvl0,
+               int* h_depth, cudaStream_t s) {
   int kw = 1;
   while (kw * 32 < k) kw <<= 1;
   const int n = g->nrows;
@@ -205,27 +208,29 @@ int msbfs_impl(gbo_graph* g, const int* h_srcs, int k, int32_t* d_levels, int* h
   }
   GBO_CUDA_TRY(cudaMemcpyAsync(m.srcs, h_srcs, sizeof(int) * (size_t)k, cudaMemcpyHostToDevice, s));
   const long long push_thr = ms_push_threshold(g, kw);
-  if (!m.exec || m.key_levels != d_levels || m.key_k != k || m.key_push != push_thr) {
+  if (!m.exec || m.key_levels != d_levels || m.key_k != k || m.key_push != push_thr ||
+      m.key_group != level_group) {
     int st = GBO_OK;
     switch (kw) {
-      case 1: st = ms_capture<1>(g, m, d_levels, k); break;
-      case 2: st = ms_capture<2>(g, m, d_levels, k); break;
-      case 4: st = ms_capture<4>(g, m, d_levels, k); break;
-      case 8: st = ms_capture<8>(g, m, d_levels, k); break;
-      case 16: st = ms_capture<16>(g, m, d_levels, k); break;
-      default: st = ms_capture<32>(g, m, d_levels, k); break;
+      case 1: st = ms_capture<1>(g, m, d_levels, k, level_group); break;
+      case 2: st = ms_capture<2>(g, m, d_levels, k, level_group); break;
+      case 4: st = ms_capture<4>(g, m, d_levels, k, level_group); break;
+      case 8: st = ms_capture<8>(g, m, d_levels, k, level_group); break;
+      case 16: st = ms_capture<16>(g, m, d_levels, k, level_group); break;
+      default: st = ms_capture<32>(g, m, d_levels, k, level_group); break;
     }
     GBO_TRY(st);
     m.key_levels = d_levels;
     m.key_k = k;
     m.key_push = push_thr;
+    m.key_group = level_group;
   }
-  const ms::Args a = make_args(g, m, d_levels, k);
-  const int max_iter = n + 1;
+  const ms::Args a = make_args(g, m, d_levels, k, level_group);
+  const int max_iter = lvl0 + n + 1;
   unsigned gv = blocks_for((long long)n * k, 256);
   if (gv > (unsigned)num_sms() * 16u) gv = (unsigned)num_sms() * 16u;
-  ms::k_init<<<gv, 256, 0, s>>>(a, kw, max_iter);
-  ms::seed_sources(a, m.srcs, nullptr, k, kw, 0, s);
+  ms::k_init<<<gv, 256, 0, s>>>(a, kw, max_iter, lvl0);
+  ms::seed_sources(a, m.srcs, nullptr, k, kw, lvl0, s);
   GBO_CUDA_TRY(cudaGetLastError());
   m.step_ms.clear();
   m.launches = 3;
@@ -258,7 +263,7 @@ int msbfs_impl(gbo_graph* g, const int* h_srcs, int k, int32_t* d_levels, int* h
     m.launches += 2;
   }
   m.fixed_launches = (int)m.launches;
-  int it0 = seed_push ? 1 : 0;
+  int it0 = lvl0 + (seed_push ? 1 : 0);
   if (seed_push) {  // level 0's time (read once the loop has synchronised)
     m.step_ms.push_back(-1.f);
   }
@@ -291,9 +296,31 @@ int msbfs_impl(gbo_graph* g, const int* h_srcs, int k, int32_t* d_levels, int* h
     m.step_ms[0] = -1.f;
     (void)cudaGetLastError();
   }
-  if (h_depth) *h_depth = m.h_ctl[0];
-  g->last_run_ms = 1;
+  if (h_depth) *h_depth = m.h_ctl[0] - lvl0;
   return GBO_OK;
+}
+
+void destroy_ms(MsState* m) {
+  if (!m) return;
+  if (m->exec) cudaGraphExecDestroy(m->exec);
+  for (auto& e : m->ev)
+    if (e) cudaEventDestroy(e);
+  cudaFree(m->F);
+  cudaFree(m->V);
+  cudaFree(m->fbits);
+  cudaFree(m->vfull);
+  cudaFree(m->split_acc);
+  cudaFree(m->slot_split);
+  cudaFree(m->push_acc);
+  for (auto& e : m->ev0)
+    if (e) cudaEventDestroy(e);
+  cudaFree(m->long_acc);
+  cudaFree(m->active);
+  cudaFree(m->srcs);
+  cudaFree(m->ctl);
+  cudaFreeHost(m->h_ctl);
+  if (m->cap) cudaStreamDestroy(m->cap);
+  delete m;
 }
 
 }  // namespace
@@ -338,28 +365,28 @@ int split_state(const gbo_graph* g, int kw, uint32_t** acc, int** slot_split, cu
 }  // namespace ms
 
 void free_ms_state(gbo_graph* g) {
-  MsState* m = reinterpret_cast<MsState*>(g->ms);
-  if (!m) return;
-  if (m->exec) cudaGraphExecDestroy(m->exec);
-  for (auto& e : m->ev)
-    if (e) cudaEventDestroy(e);
-  cudaFree(m->F);
-  cudaFree(m->V);
-  cudaFree(m->fbits);
-  cudaFree(m->vfull);
-  cudaFree(m->split_acc);
-  cudaFree(m->slot_split);
-  cudaFree(m->push_acc);
-  for (auto& e : m->ev0)
-    if (e) cudaEventDestroy(e);
-  cudaFree(m->long_acc);
-  cudaFree(m->active);
-  cudaFree(m->srcs);
-  cudaFree(m->ctl);
-  cudaFreeHost(m->h_ctl);
-  if (m->cap) cudaStreamDestroy(m->cap);
-  delete m;
+  destroy_ms(reinterpret_cast<MsState*>(g->ms));
   g->ms = nullptr;
+}
+
+// A multi-source BFS state of the caller's own (the query server's batch
+// engine), apart from the graph's, so that the server's worker thread and
+// the graph's own calls never share one.  live: the graph's rows with an
+// entry (live_rows), read by the init kernel.
+void* ms_batch_create(const uint32_t* live) {
+  MsState* m = new MsState();
+  m->live = live;
+  return m;
+}
+
+void ms_batch_destroy(void* state) { destroy_ms(static_cast<MsState*>(state)); }
+
+int ms_batch_run(gbo_graph* g, void* state, const int* h_srcs, int k, int32_t* d_levels, int level_group, int lvl0,
+                 int* h_depth, long long* launches, cudaStream_t s) {
+  MsState& m = *static_cast<MsState*>(state);
+  const int st = msbfs_impl(g, m, h_srcs, k, d_levels, level_group, lvl0, h_depth, s);
+  *launches = m.launches;
+  return st;
 }
 
 }  // namespace gbo
@@ -378,7 +405,11 @@ extern "C" int gbo_msbfs(const gbo_graph* gc, const int* h_srcs, int k, int32_t*
   if (!h_srcs || !d_levels) return fail(GBO_ERR_INVALID, "NULL argument");
   for (int s = 0; s < k; ++s)
     if (h_srcs[s] < 0 || h_srcs[s] >= g->nrows) return fail(GBO_ERR_INVALID, "source out of range");
-  return msbfs_impl(g, h_srcs, k, d_levels, h_depth, as_stream(stream));
+  if (!g->ms) g->ms = new MsState();
+  const int st = msbfs_impl(g, *reinterpret_cast<MsState*>(g->ms), h_srcs, k, d_levels, 0, 0, h_depth,
+                            as_stream(stream));
+  if (st == GBO_OK) g->last_run_ms = 1;
+  return st;
 }
 
 extern "C" int gbo_bfs_multi(const gbo_graph* gc, const int* h_seeds, int nseeds, int32_t* d_level,

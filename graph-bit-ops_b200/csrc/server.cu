@@ -11,6 +11,11 @@
 // slots for the next queries.  A query's result does not depend on the other
 // queries in flight: every column is computed independently and in the same
 // order (BFS bit-exact; PPR identical arithmetic per column).
+//
+// Batch mode (gbo_server_set_admission with 1): BFS queries enter only an
+// idle engine, and each batch runs as one multi-source BFS (msbfs.cu: level
+// 0 pushed from the sources, finished columns retired) in the server's level
+// store; the batch's queries all finish in that call and retire as above.
 #include <string.h>
 
 #include <chrono>
@@ -27,6 +32,13 @@
 #include "ms_kernels.cuh"
 
 namespace gbo {
+
+// msbfs.cu: a multi-source BFS state of the server's own
+void* ms_batch_create(const uint32_t* live);
+void ms_batch_destroy(void* state);
+int ms_batch_run(gbo_graph* g, void* state, const int* h_srcs, int k, int32_t* d_levels, int level_group, int lvl0,
+                 int* h_depth, long long* launches, cudaStream_t s);
+
 namespace {
 
 constexpr int kPprSlots = 32;
@@ -398,6 +410,7 @@ struct gbo_server {
   long long max_pending = 0;  // per engine; 0 = unbounded (gbo_server_set_queue_limit)
   float bfs_admit_free = 0.5f;  // gbo_server_set_admission
   uint32_t* long_acc = nullptr;  // up to 64 slots: long-row tail gathers (ms::Args::long_acc)
+  void* msb = nullptr;           // batch mode's multi-source BFS state (created on first use)
   float alpha = 0.85f, tol = 1e-7f;
   int ppr_max_iter = 1000;
   // one worker thread per engine (0 BFS, 1 PPR), each with its own stream,
@@ -543,6 +556,26 @@ int bfs_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
   for (int q = 0; q < S->kb; ++q)
     if (S->bslot_ticket[q] > 0 && !S->bslot_finished[q] && !((S->h_slot_any[q / 32] >> (q % 32)) & 1u))
       S->bslot_finished[q] = 1;
+  return GBO_OK;
+}
+
+// Batch mode: the admitted queries (the engine was idle, so their slots are
+// the only ones occupied) as one multi-source BFS over every slot column,
+// empty columns with no source.  Levels land in the server's level store as
+// absolute levels from the current level on, so retirement reads them as
+// for a round-by-round query, and the level counter moves past the batch.
+int bfs_batch(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
+  if (!S->msb) S->msb = ms_batch_create(S->live);
+  std::vector<int> src((size_t)S->kb, -1);
+  for (auto& q : adm) src[(size_t)q.first] = q.second.src;
+  const int lvl0 = S->level;
+  int depth = 0;
+  long long nl = 0;
+  GBO_TRY(ms_batch_run(S->g, S->msb, src.data(), S->kb, S->levels, 8, lvl0, &depth, &nl, S->s[0]));
+  S->launches += nl;
+  S->level = lvl0 + depth;
+  std::lock_guard<std::mutex> lk(S->mu);
+  for (auto& q : adm) S->bslot_finished[(size_t)q.first] = 1;
   return GBO_OK;
 }
 
@@ -764,8 +797,9 @@ void worker_main(gbo_server* S, int kind) {
     return (long long)S->pool_free[rpool].size() - inflight;
   };
   // BFS admission batching (gbo_server_set_admission): enough free slots,
-  // or nothing left traversing
+  // or nothing left traversing; batch mode: every slot free and retired
   auto batch_ready = [&]() {
+    if (S->bfs_admit_free >= 1.f) return !occupied();
     long long nfree = 0;
     for (long long t : tab) nfree += t == 0;
     const double need = std::ceil((double)S->bfs_admit_free * (double)tab.size());
@@ -774,6 +808,7 @@ void worker_main(gbo_server* S, int kind) {
   double stall_since = -1.0;
   while (true) {
     std::vector<std::pair<int, Query>> adm;
+    bool batch = false;  // the admitted queries run as one multi-source BFS
     {
       std::unique_lock<std::mutex> lk(S->mu);
       for (;;) {
@@ -819,12 +854,15 @@ void worker_main(gbo_server* S, int kind) {
         adm.emplace_back(slot, std::move(q));
         --room;
       }
+      batch = kind == 0 && !adm.empty() && S->bfs_admit_free >= 1.f;
     }
     int st = GBO_OK;
     const bool busy = !adm.empty() || unfinished();
     const double t0 = now_ms();
     if (busy) {
-      if (kind == 0) {
+      if (batch) {
+        st = bfs_batch(S, adm);
+      } else if (kind == 0) {
         switch (S->kw) {
           case 1: st = bfs_round<1>(S, adm); break;
           case 2: st = bfs_round<2>(S, adm); break;
@@ -864,6 +902,7 @@ void destroy_server(gbo_server* S) {
     if (S->worker[e].joinable()) S->worker[e].join();
     if (S->s[e]) cudaStreamSynchronize(S->s[e]);
   }
+  if (S->msb) ms_batch_destroy(S->msb);
   cudaFree(S->F);
   cudaFree(S->V);
   cudaFree(S->fbits);

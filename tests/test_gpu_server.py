@@ -202,3 +202,49 @@ def test_server_admission_batching_keeps_results(gbo, orc, gpu, admit):
         srv.set_admission(1.5)
     srv.close()
     g.free()
+
+
+@pytest.mark.gpu
+def test_server_batch_mode_switches_and_deep_queries(gbo, orc, gpu):
+    """Batch mode (admission 1: each batch one multi-source BFS) with 256
+    slots, switched to round-by-round admission and back while queries are
+    in flight: every result is the oracle's levels, isolated sources
+    included.  On a path of 300 vertices a batch query deeper than 254
+    levels lands in the word pool (wait_u8 answers GBO_ERR_OVERFLOW)."""
+    csr = gbo.gen_rmat(12, 16, seed=5)
+    n = csr.nrows
+    g = gbo.Graph.from_csr(csr, 32, gbo.FLAG_SYMMETRIC)
+    srv = gbo.Server(g, bfs_slots=256, ppr_slots=0)
+    rng = np.random.default_rng(21)
+    deg = np.diff(csr.rowptr)
+    iso = np.flatnonzero(deg == 0)[:4]
+    srcs, tickets = [], []
+    for admit in (1.0, 0.0, 1.0, 0.5, 1.0):
+        srv.set_admission(admit)
+        part = rng.integers(0, n, 300)
+        if admit == 1.0 and len(iso):
+            part[: len(iso)] = iso
+        srcs += [int(x) for x in part]
+        tickets += [srv.submit_bfs(int(x)) for x in part]
+    for s, t in zip(srcs, tickets):
+        res, _, _ = srv.wait(t, "bfs")
+        assert np.array_equal(res, orc.bfs_csr(csr.rowptr, csr.colind, n, s)[0]), s
+    st = srv.stats()
+    assert st["bfs_completed"] == len(srcs)
+    srv.close()
+    g.free()
+    m = 300
+    path = gbo.csr_from_edges(np.arange(m - 1, dtype=np.int32), np.arange(1, m, dtype=np.int32), m, True, True)
+    gp = gbo.Graph.from_csr(path, 32, gbo.FLAG_SYMMETRIC)
+    sp = gbo.Server(gp, bfs_slots=64, ppr_slots=0)
+    sp.set_admission(1.0)
+    t0, t1 = sp.submit_bfs(0), sp.submit_bfs(150)
+    with pytest.raises(gbo.GboError) as e:
+        sp.wait_u8(t0)
+    assert e.value.status == gbo.GBO_ERR_OVERFLOW
+    lv, _, _ = sp.wait(t0, "bfs")
+    assert np.array_equal(lv, np.arange(m))
+    lv, _, _ = sp.wait(t1, "bfs")
+    assert np.array_equal(lv, np.abs(np.arange(m) - 150))
+    sp.close()
+    gp.free()
