@@ -432,6 +432,11 @@ struct gbo_server {
   const uint32_t* live = nullptr;  // rows of P with an entry (owned by the graph)
   int *d_adm_src = nullptr, *d_adm_slot = nullptr;
   int level = 0;
+  // the round-by-round engine reads the frontier buffer of parity level & 1,
+  // written by the round before; after a batch of odd depth the next round
+  // moves one level further, so that it reads the buffer its last round left
+  // empty
+  bool parity_fix = false;
   std::vector<long long> bslot_ticket;
   std::vector<int> bslot_start;
   std::vector<char> bslot_finished;
@@ -496,6 +501,11 @@ ms::Args bfs_args(gbo_server* S) {
 
 template <int KW>
 int bfs_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
+  if (S->parity_fix) {
+    S->level += 1;
+    S->parity_fix = false;
+    for (auto& q : adm) S->bslot_start[(size_t)q.first] = S->level;
+  }
   const ms::Args a = bfs_args(S);
   cudaStream_t st = S->s[0];
   // columns still traversing; rows marked finished for the old set reopen
@@ -574,6 +584,7 @@ int bfs_batch(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
   GBO_TRY(ms_batch_run(S->g, S->msb, src.data(), S->kb, S->levels, 8, lvl0, &depth, &nl, S->s[0]));
   S->launches += nl;
   S->level = lvl0 + depth;
+  S->parity_fix = (S->parity_fix != ((depth & 1) != 0));
   std::lock_guard<std::mutex> lk(S->mu);
   for (auto& q : adm) S->bslot_finished[(size_t)q.first] = 1;
   return GBO_OK;
@@ -840,7 +851,9 @@ void worker_main(gbo_server* S, int kind) {
       // admission into free slots, arrival order, within the buffer budget
       size_t nx = 0;
       std::deque<Query>& pend = S->pending[kind];
-      long long room = inject_server_hold() ? 0 : budget();
+      // BFS admission waits for its batching condition here too: the worker
+      // also gets here with queries still traversing
+      long long room = inject_server_hold() || (kind == 0 && !batch_ready()) ? 0 : budget();
       while (!pend.empty() && room > 0) {
         while (nx < tab.size() && tab[nx] != 0) ++nx;
         if (nx >= tab.size()) break;
