@@ -410,7 +410,10 @@ struct gbo_server {
   long long max_pending = 0;  // per engine; 0 = unbounded (gbo_server_set_queue_limit)
   float bfs_admit_free = 0.5f;  // gbo_server_set_admission
   uint32_t* long_acc = nullptr;  // up to 64 slots: long-row tail gathers (ms::Args::long_acc)
-  void* msb = nullptr;           // batch mode's multi-source BFS state (created on first use)
+  // batch mode's multi-source BFS states, one per frontier width (1..32
+  // words per vertex, created on first use): a batch of m queries runs
+  // with the narrowest width that holds m columns
+  void* msb[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   float alpha = 0.85f, tol = 1e-7f;
   int ppr_max_iter = 1000;
   // one worker thread per engine (0 BFS, 1 PPR), each with its own stream,
@@ -438,6 +441,7 @@ struct gbo_server {
   // empty
   bool parity_fix = false;
   std::vector<long long> bslot_ticket;
+  std::vector<char> bslot_batch;  // the slot's query ran in a batch (its visited bits were never set)
   std::vector<int> bslot_start;
   std::vector<char> bslot_finished;
   // PPR engine
@@ -575,13 +579,22 @@ int bfs_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
 // absolute levels from the current level on, so retirement reads them as
 // for a round-by-round query, and the level counter moves past the batch.
 int bfs_batch(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
-  if (!S->msb) S->msb = ms_batch_create(S->live);
-  std::vector<int> src((size_t)S->kb, -1);
-  for (auto& q : adm) src[(size_t)q.first] = q.second.src;
+  // the engine was idle, so admission took the lowest slots: columns
+  // 0 .. top of the batch, in whole words rounded up to a power of two
+  int top = 0;
+  for (auto& q : adm) top = std::max(top, q.first + 1);
+  int w = 1, wi = 0;
+  while (w * 32 < top) w <<= 1, ++wi;
+  if (!S->msb[wi]) S->msb[wi] = ms_batch_create(S->live);
+  std::vector<int> src((size_t)w * 32, -1);
+  for (auto& q : adm) {
+    src[(size_t)q.first] = q.second.src;
+    S->bslot_batch[(size_t)q.first] = 1;
+  }
   const int lvl0 = S->level;
   int depth = 0;
   long long nl = 0;
-  GBO_TRY(ms_batch_run(S->g, S->msb, src.data(), S->kb, S->levels, 8, lvl0, &depth, &nl, S->s[0]));
+  GBO_TRY(ms_batch_run(S->g, S->msb[wi], src.data(), w * 32, S->levels, 8, lvl0, &depth, &nl, S->s[0]));
   S->launches += nl;
   S->level = lvl0 + depth;
   S->parity_fix = (S->parity_fix != ((depth & 1) != 0));
@@ -671,7 +684,7 @@ int retire(gbo_server* S, int kind) {
       r.slot[r.count] = (int)q;
       r.start[r.count] = kind == 0 ? S->bslot_start[q] : 0;
       r.out[r.count] = S->dpool[p] + (size_t)b * S->dbytes[p];
-      if (kind == 0) r.clr[q / 32] |= 1u << (q % 32);
+      if (kind == 0 && !S->bslot_batch[q]) r.clr[q / 32] |= 1u << (q % 32);
       bufs[p].push_back(b);
       r.count++;
     }
@@ -862,7 +875,10 @@ void worker_main(gbo_server* S, int kind) {
         const int slot = (int)nx++;
         tab[(size_t)slot] = q.ticket;
         fin[(size_t)slot] = 0;
-        if (kind == 0) S->bslot_start[(size_t)slot] = S->level;
+        if (kind == 0) {
+          S->bslot_start[(size_t)slot] = S->level;
+          S->bslot_batch[(size_t)slot] = 0;
+        }
         else S->pslot_iters[(size_t)slot] = 0;
         adm.emplace_back(slot, std::move(q));
         --room;
@@ -915,7 +931,8 @@ void destroy_server(gbo_server* S) {
     if (S->worker[e].joinable()) S->worker[e].join();
     if (S->s[e]) cudaStreamSynchronize(S->s[e]);
   }
-  if (S->msb) ms_batch_destroy(S->msb);
+  for (void* m : S->msb)
+    if (m) ms_batch_destroy(m);
   cudaFree(S->F);
   cudaFree(S->V);
   cudaFree(S->fbits);
@@ -1029,6 +1046,7 @@ extern "C" int gbo_server_create(const gbo_graph* gc, int bfs_slots, int ppr_slo
     S->bslot_ticket.assign((size_t)S->kb, 0);
     S->bslot_start.assign((size_t)S->kb, 0);
     S->bslot_finished.assign((size_t)S->kb, 0);
+    S->bslot_batch.assign((size_t)S->kb, 0);
     if (ppr_slots) {
       cu(cudaMalloc(&S->X, sizeof(float) * 2 * n * kPprSlots), "X");
       cu(cudaMemsetAsync(S->X, 0, sizeof(float) * 2 * n * kPprSlots, S->s[1]), "X");
