@@ -348,6 +348,41 @@ __global__ void __launch_bounds__(256) k_bfs_retire(const int* __restrict__ leve
   }
 }
 
+// Batch mode: every query of a batch retires at once into the byte pool.
+// Columns 0 .. 8 * ngroups - 1 of the level store, levels from `start` on
+// (every query of the batch shallower than 255 levels); bufidx[s] is column
+// s's buffer in the byte pool (-1: no query).  A block takes 32 rows: its
+// threads read each (row, level group) sector once, coalesced across rows,
+// and keep the bytes in shared memory as [column][row]; each column's 32
+// bytes then go out as one full 32-byte sector of its buffer.  One pass over
+// the batch's level columns instead of one per 128 retiring slots.
+constexpr int kBatchCols = 1024;
+__global__ void __launch_bounds__(256) k_bfs_retire_batch(const int* __restrict__ levels, int n, int ngroups,
+                                                          int start, const int* __restrict__ bufidx,
+                                                          uint8_t* __restrict__ pool, size_t stride) {
+  __shared__ __align__(16) uint8_t sm[kBatchCols][kRetRows];
+  const long long i0 = (long long)blockIdx.x * kRetRows;
+  for (int q = threadIdx.x; q < kRetRows * ngroups; q += blockDim.x) {
+    const int gi = q / kRetRows, ii = q % kRetRows;
+    const long long i = i0 + ii;
+    if (i >= n) continue;
+    const int4* p = reinterpret_cast<const int4*>(levels + ((size_t)gi * n + i) * 8);
+    const int4 a = p[0], b = p[1];
+    const int lv[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+    for (int w = 0; w < 8; ++w) sm[gi * 8 + w][ii] = lv[w] >= start ? (uint8_t)(lv[w] - start) : (uint8_t)255;
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < ngroups * 8; c += blockDim.x) {
+    const int b = bufidx[c];
+    if (b < 0) continue;
+    uint4* dst = reinterpret_cast<uint4*>(pool + (size_t)b * stride + i0);
+    const uint4* src = reinterpret_cast<const uint4*>(&sm[c][0]);
+    dst[0] = src[0];
+    dst[1] = src[1];
+  }
+}
+
 // PPR: out[f][i] = X[i][slot f] of the current iterate.
 __global__ void __launch_bounds__(256) k_ppr_retire(const float* X, int n, RetireList rl) {
   __shared__ float sm[kRetire][kRetRows + 1];
@@ -434,6 +469,7 @@ struct gbo_server {
   bool reopen = false;           // active set grew: rows marked finished reopen
   const uint32_t* live = nullptr;  // rows of P with an entry (owned by the graph)
   int *d_adm_src = nullptr, *d_adm_slot = nullptr;
+  int* d_bufidx = nullptr;  // batch retirement: byte-pool buffer of each slot column
   int level = 0;
   // the round-by-round engine reads the frontier buffer of parity level & 1,
   // written by the round before; after a batch of odd depth the next round
@@ -573,6 +609,55 @@ int bfs_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
   return GBO_OK;
 }
 
+// Batch mode: every query of the batch into the byte pool with one kernel
+// (k_bfs_retire_batch); a query left without a buffer stays finished for the
+// per-round retirement.
+int retire_batch(gbo_server* S, const std::vector<std::pair<int, gbo::Query>>& adm, int ncols, int lvl0,
+                 int depth) {
+  std::vector<int> idx((size_t)ncols, -1);
+  std::vector<std::pair<int, int>> took;  // slot, buffer
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    for (auto& q : adm) {
+      if (S->pool_free[0].empty()) break;
+      const int b = S->pool_free[0].back();
+      S->pool_free[0].pop_back();
+      idx[(size_t)q.first] = b;
+      took.emplace_back(q.first, b);
+    }
+  }
+  if (took.empty()) return GBO_OK;
+  cudaStream_t st = S->s[0];
+  GBO_CUDA_TRY(cudaMemcpyAsync(S->d_bufidx, idx.data(), sizeof(int) * (size_t)ncols, cudaMemcpyHostToDevice, st));
+  k_bfs_retire_batch<<<blocks_for(S->n, kRetRows), 256, 0, st>>>(S->levels, S->n, ncols / 8, lvl0, S->d_bufidx,
+                                                                  reinterpret_cast<uint8_t*>(S->dpool[0]),
+                                                                  S->dbytes[0]);
+  S->launches++;
+  GBO_CUDA_TRY(cudaGetLastError());
+  for (auto& t : took) GBO_CUDA_TRY(cudaEventRecord(S->pool_ev[0][(size_t)t.second], st));
+  const double t_now = now_ms();
+  std::lock_guard<std::mutex> lk(S->mu);
+  for (auto& t : took) {
+    const int q = t.first;
+    const long long tk = S->bslot_ticket[(size_t)q];
+    Result r;
+    r.kind = 0;
+    r.pool = 0;
+    r.buf = t.second;
+    r.u8 = 1;
+    r.ev = S->pool_ev[0][(size_t)t.second];
+    r.t_submit = S->submit_time[tk];
+    r.t_done = t_now;
+    r.iters = depth;
+    S->results[tk] = r;
+    S->bslot_ticket[(size_t)q] = 0;
+    S->bslot_finished[(size_t)q] = 0;
+    S->bfs_done++;
+  }
+  S->cv_done.notify_all();
+  return GBO_OK;
+}
+
 // Batch mode: the admitted queries (the engine was idle, so their slots are
 // the only ones occupied) as one multi-source BFS over every slot column,
 // empty columns with no source.  Levels land in the server's level store as
@@ -598,8 +683,10 @@ int bfs_batch(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
   S->launches += nl;
   S->level = lvl0 + depth;
   S->parity_fix = (S->parity_fix != ((depth & 1) != 0));
+  if (depth < 255) GBO_TRY(retire_batch(S, adm, w * 32, lvl0, depth));
   std::lock_guard<std::mutex> lk(S->mu);
-  for (auto& q : adm) S->bslot_finished[(size_t)q.first] = 1;
+  for (auto& q : adm)
+    if (S->bslot_ticket[(size_t)q.first] > 0) S->bslot_finished[(size_t)q.first] = 1;
   return GBO_OK;
 }
 
@@ -947,6 +1034,7 @@ void destroy_server(gbo_server* S) {
   cudaFree(S->d_active);
   cudaFree(S->d_adm_src);
   cudaFree(S->d_adm_slot);
+  cudaFree(S->d_bufidx);
   cudaFree(S->X);
   cudaFree(S->P);
   cudaFree(S->err);
@@ -1020,6 +1108,7 @@ extern "C" int gbo_server_create(const gbo_graph* gc, int bfs_slots, int ppr_slo
       cu(cudaHostAlloc(&S->h_slot_any, sizeof(uint32_t) * kw, cudaHostAllocDefault), "h_slot_any");
       cu(cudaMalloc(&S->d_adm_src, sizeof(int) * S->kb), "adm");
       cu(cudaMalloc(&S->d_adm_slot, sizeof(int) * S->kb), "adm");
+      cu(cudaMalloc(&S->d_bufidx, sizeof(int) * S->kb), "bufidx");
       {
         const void* lv = nullptr;
         const int st = live_rows(g, S->s[0], &lv);
