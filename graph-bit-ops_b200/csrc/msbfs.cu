@@ -61,8 +61,8 @@ long long ms_push_threshold(const gbo_graph* g, int kw) {
   return g->bfs_push_thr;
 }
 
-// level_group 0: the API's vertex-major levels[v * k + s]; 8: the query
-// server's layout (8 sources per 32-byte sector, ms::level_index)
+// level_group 0: the API's vertex-major levels[v * k + s]; 32: the query
+// server's layout (32-source planes, ms::level_index)
 ms::Args make_args(gbo_graph* g, MsState& m, int32_t* d_levels, int k, int level_group) {
   ms::Args a;
   a.v = view_of(g);

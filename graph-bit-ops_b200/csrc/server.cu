@@ -288,13 +288,22 @@ __global__ void k_ppr_admit_set(float* X, size_t xstride, int parity, float* P, 
 constexpr int kRetire = 128;
 constexpr int kRetRows = 32;  // rows per block of the transposing kernels
 
+// The BFS level store: 32 slots per plane, levels[((s / 32) * n + i) * 32 +
+// s % 32] (ms::Args::level_group 32), so that the 32 lanes of a level write
+// cover 128 contiguous bytes.  Sector of 8-slot group gid (slots 8 gid ..
+// 8 gid + 7) in vertex i's plane row.
+__device__ __forceinline__ const int* level_sector(const int* levels, int n, int gid, long long i) {
+  return levels + ((size_t)(gid >> 2) * n + i) * 32 + (gid & 3) * 8;
+}
+
 struct RetireList {
   int count;
   int slot[kRetire];    // ascending, so the slots of one level group are adjacent
   int start[kRetire];
   uint32_t clr[32];     // visited bits to clear, per source word
   void* out[kRetire];   // destination buffer of each retired slot
-  // BFS: the level groups (8 slots per 32-byte sector) holding retired slots:
+  // BFS: the 8-slot groups (one 32-byte sector of a vertex's level row
+  // within its 32-slot plane) holding retired slots:
   // group id, index of its first retired slot, which of its 8 slots retire
   int ngroups;
   int group[kRetire];
@@ -307,7 +316,7 @@ struct RetireList {
 // (the server's level counter), so a slot's column never needs clearing: a
 // value older than the query's start level was left by an earlier query of
 // the slot and reads as unreachable.  Each thread loads the 32-byte sector of
-// one (row, level group) and keeps the group's retiring slots; results go
+// one (row, 8-slot group) and keeps the group's retiring slots; results go
 // out through shared memory row-contiguous.  When every retired query is
 // shallower than 255 levels (u8), a result is one byte per vertex (255 =
 // unreachable), a quarter of the bytes the client copies.
@@ -319,7 +328,7 @@ __global__ void __launch_bounds__(256) k_bfs_retire(const int* __restrict__ leve
     const int gi = q / kRetRows, ii = q % kRetRows;
     const long long i = i0 + ii;
     if (i >= n) continue;
-    const int4* p = reinterpret_cast<const int4*>(levels + ((size_t)rl.group[gi] * n + i) * 8);
+    const int4* p = reinterpret_cast<const int4*>(level_sector(levels, n, rl.group[gi], i));
     const int4 a = p[0], b = p[1];
     const int lv[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
     const unsigned m = rl.mask8[gi];
@@ -354,7 +363,9 @@ __global__ void __launch_bounds__(256) k_bfs_retire(const int* __restrict__ leve
 // s's buffer in the byte pool (-1: no query).  A block takes 32 rows: its
 // threads read each (row, level group) sector once, coalesced across rows,
 // and keep the bytes in shared memory as [column][row]; each column's 32
-// bytes then go out as one full 32-byte sector of its buffer.  One pass over
+// bytes then go out as one full 32-byte sector of its buffer.  Four threads
+// in a row read one vertex's 128-byte plane row, a warp eight consecutive
+// rows of a plane (1 KB contiguous).  One pass over
 // the batch's level columns instead of one per 128 retiring slots.
 constexpr int kBatchCols = 1024;
 __global__ void __launch_bounds__(256) k_bfs_retire_batch(const int* __restrict__ levels, int n, int ngroups,
@@ -363,10 +374,11 @@ __global__ void __launch_bounds__(256) k_bfs_retire_batch(const int* __restrict_
   __shared__ __align__(16) uint8_t sm[kBatchCols][kRetRows];
   const long long i0 = (long long)blockIdx.x * kRetRows;
   for (int q = threadIdx.x; q < kRetRows * ngroups; q += blockDim.x) {
-    const int gi = q / kRetRows, ii = q % kRetRows;
+    const int sub = q & 3, rest = q >> 2;
+    const int ii = rest % kRetRows, gi = (rest / kRetRows) * 4 + sub;
     const long long i = i0 + ii;
     if (i >= n) continue;
-    const int4* p = reinterpret_cast<const int4*>(levels + ((size_t)gi * n + i) * 8);
+    const int4* p = reinterpret_cast<const int4*>(level_sector(levels, n, gi, i));
     const int4 a = p[0], b = p[1];
     const int lv[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 #pragma unroll
@@ -456,7 +468,7 @@ struct gbo_server {
   cudaStream_t s[2] = {nullptr, nullptr};
   cudaEvent_t sync_ev[2] = {nullptr, nullptr};  // blocking-sync events of the workers
   int dev = 0;
-  // BFS engine (levels grouped 8 sources per 32-byte sector)
+  // BFS engine (levels in 32-slot planes, level_sector)
   int kb = 0, kw = 0;
   uint32_t *F = nullptr, *V = nullptr, *fbits = nullptr, *vfull = nullptr, *split_acc = nullptr;
   int* slot_split = nullptr;
@@ -534,7 +546,7 @@ ms::Args bfs_args(gbo_server* S) {
   a.slot_any = S->slot_any;
   a.live = S->live;
   a.active = S->d_active;
-  a.level_group = 8;
+  a.level_group = 32;
   a.long_acc = S->long_acc;
   return a;
 }
@@ -679,7 +691,7 @@ int bfs_batch(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
   const int lvl0 = S->level;
   int depth = 0;
   long long nl = 0;
-  GBO_TRY(ms_batch_run(S->g, S->msb[wi], src.data(), w * 32, S->levels, 8, lvl0, &depth, &nl, S->s[0]));
+  GBO_TRY(ms_batch_run(S->g, S->msb[wi], src.data(), w * 32, S->levels, 32, lvl0, &depth, &nl, S->s[0]));
   S->launches += nl;
   S->level = lvl0 + depth;
   S->parity_fix = (S->parity_fix != ((depth & 1) != 0));
