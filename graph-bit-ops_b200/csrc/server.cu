@@ -357,41 +357,57 @@ __global__ void __launch_bounds__(256) k_bfs_retire(const int* __restrict__ leve
   }
 }
 
-// Batch mode: every query of a batch retires at once into the byte pool.
-// Columns 0 .. 8 * ngroups - 1 of the level store, levels from `start` on
-// (every query of the batch shallower than 255 levels); bufidx[s] is column
-// s's buffer in the byte pool (-1: no query).  A block takes 32 rows: its
-// threads read each (row, level group) sector once, coalesced across rows,
-// and keep the bytes in shared memory as [column][row]; each column's 32
-// bytes then go out as one full 32-byte sector of its buffer.  Four threads
-// in a row read one vertex's 128-byte plane row, a warp eight consecutive
-// rows of a plane (1 KB contiguous).  One pass over
-// the batch's level columns instead of one per 128 retiring slots.
+// Batch mode retirement.  A batch's levels sit vertex-major in their own
+// store (blevels[i * k + c], k = the batch's width, the multi-source BFS's
+// own layout, whose level writes cover whole 4 KB rows at k = 1,024).  A
+// block takes 32 rows and columns c0 .. c0 + ncols - 1: its threads read the
+// rows contiguously (16 bytes each), keep the values relative to `start` in
+// shared memory as [row][column], and each column's 32 values then go out to
+// its buffer as one run (32 bytes as u8, 255 = unreachable; 128 bytes as
+// int32, -1).  bufidx[c]: column c's buffer in the pool, -1 for none.  T is
+// uint8_t (MAXC 1,024 columns per launch) or int (256).
 constexpr int kBatchCols = 1024;
-__global__ void __launch_bounds__(256) k_bfs_retire_batch(const int* __restrict__ levels, int n, int ngroups,
-                                                          int start, const int* __restrict__ bufidx,
-                                                          uint8_t* __restrict__ pool, size_t stride) {
-  __shared__ __align__(16) uint8_t sm[kBatchCols][kRetRows];
+template <typename T, int MAXC>
+__global__ void __launch_bounds__(256) k_bfs_retire_batch(const int* __restrict__ levels, int n, int k, int c0,
+                                                          int ncols, int start, const int* __restrict__ bufidx,
+                                                          char* __restrict__ pool, size_t stride) {
+  __shared__ __align__(16) T sm[kRetRows][MAXC];
   const long long i0 = (long long)blockIdx.x * kRetRows;
-  for (int q = threadIdx.x; q < kRetRows * ngroups; q += blockDim.x) {
-    const int sub = q & 3, rest = q >> 2;
-    const int ii = rest % kRetRows, gi = (rest / kRetRows) * 4 + sub;
+  const int nq = ncols / 4;
+  for (int q = threadIdx.x; q < kRetRows * nq; q += blockDim.x) {
+    const int ii = q / nq, c4 = q % nq;
     const long long i = i0 + ii;
     if (i >= n) continue;
-    const int4* p = reinterpret_cast<const int4*>(level_sector(levels, n, gi, i));
-    const int4 a = p[0], b = p[1];
-    const int lv[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    const int4 v = *reinterpret_cast<const int4*>(levels + (size_t)i * k + c0 + 4 * c4);
+    const int lv[4] = {v.x, v.y, v.z, v.w};
+    T o[4];
 #pragma unroll
-    for (int w = 0; w < 8; ++w) sm[gi * 8 + w][ii] = lv[w] >= start ? (uint8_t)(lv[w] - start) : (uint8_t)255;
+    for (int j = 0; j < 4; ++j) o[j] = lv[j] >= start ? (T)(lv[j] - start) : (T)(sizeof(T) == 1 ? 255 : -1);
+    if constexpr (sizeof(T) == 1) {
+      *reinterpret_cast<uint32_t*>(&sm[ii][4 * c4]) =
+          (uint32_t)o[0] | (uint32_t)o[1] << 8 | (uint32_t)o[2] << 16 | (uint32_t)o[3] << 24;
+    } else {
+      *reinterpret_cast<int4*>(&sm[ii][4 * c4]) = make_int4(o[0], o[1], o[2], o[3]);
+    }
   }
   __syncthreads();
-  for (int c = threadIdx.x; c < ngroups * 8; c += blockDim.x) {
-    const int b = bufidx[c];
+  for (int c = threadIdx.x; c < ncols; c += blockDim.x) {
+    const int b = bufidx[c0 + c];
     if (b < 0) continue;
-    uint4* dst = reinterpret_cast<uint4*>(pool + (size_t)b * stride + i0);
-    const uint4* src = reinterpret_cast<const uint4*>(&sm[c][0]);
-    dst[0] = src[0];
-    dst[1] = src[1];
+    T* dst = reinterpret_cast<T*>(pool + (size_t)b * stride) + i0;
+    if constexpr (sizeof(T) == 1) {
+      uint32_t w[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r)
+        w[r] = (uint32_t)sm[4 * r][c] | (uint32_t)sm[4 * r + 1][c] << 8 | (uint32_t)sm[4 * r + 2][c] << 16 |
+               (uint32_t)sm[4 * r + 3][c] << 24;
+      reinterpret_cast<uint4*>(dst)[0] = make_uint4(w[0], w[1], w[2], w[3]);
+      reinterpret_cast<uint4*>(dst)[1] = make_uint4(w[4], w[5], w[6], w[7]);
+    } else {
+#pragma unroll
+      for (int r = 0; r < kRetRows; r += 4)
+        reinterpret_cast<int4*>(dst)[r / 4] = make_int4(sm[r][c], sm[r + 1][c], sm[r + 2][c], sm[r + 3][c]);
+    }
   }
 }
 
@@ -481,7 +497,12 @@ struct gbo_server {
   bool reopen = false;           // active set grew: rows marked finished reopen
   const uint32_t* live = nullptr;  // rows of P with an entry (owned by the graph)
   int *d_adm_src = nullptr, *d_adm_slot = nullptr;
-  int* d_bufidx = nullptr;  // batch retirement: byte-pool buffer of each slot column
+  int* d_bufidx = nullptr;  // batch retirement: pool buffer of each slot column
+  // batch mode: the level store of the last batch (vertex-major, n x width;
+  // created on first use), and that batch while its results retire
+  int* blevels = nullptr;
+  bool bpend = false;
+  int blvl0 = 0, bdepth = 0, bwidth = 0;
   int level = 0;
   // the round-by-round engine reads the frontier buffer of parity level & 1,
   // written by the round before; after a batch of odd depth the next round
@@ -621,32 +642,56 @@ int bfs_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
   return GBO_OK;
 }
 
-// Batch mode: every query of the batch into the byte pool with one kernel
-// (k_bfs_retire_batch); a query left without a buffer stays finished for the
-// per-round retirement.
-int retire_batch(gbo_server* S, const std::vector<std::pair<int, gbo::Query>>& adm, int ncols, int lvl0,
-                 int depth) {
-  std::vector<int> idx((size_t)ncols, -1);
+// Pool of a finished BFS slot's result: bytes when the query is shallower
+// than 255 levels (a batch query: the batch's depth).
+int bfs_slot_pool(const gbo_server* S, int q) {
+  const int depth = S->bslot_batch[(size_t)q] ? S->bdepth : S->level - S->bslot_start[(size_t)q];
+  return depth < 255 ? 0 : 1;
+}
+
+// Batch mode: the finished queries of the last batch into their pool, as
+// many as have a free buffer (the rest wait, like round-by-round results,
+// for clients or the move to host memory), with one launch for byte results
+// and one per 256 columns for int32 ones.
+int retire_batch(gbo_server* S) {
+  if (!S->bpend) return GBO_OK;
+  const int p = S->bdepth < 255 ? 0 : 1;
+  const int width = S->bwidth;
+  std::vector<int> idx((size_t)width, -1);
   std::vector<std::pair<int, int>> took;  // slot, buffer
+  bool left = false;
   {
     std::lock_guard<std::mutex> lk(S->mu);
-    for (auto& q : adm) {
-      if (S->pool_free[0].empty()) break;
-      const int b = S->pool_free[0].back();
-      S->pool_free[0].pop_back();
-      idx[(size_t)q.first] = b;
-      took.emplace_back(q.first, b);
+    for (int q = 0; q < width; ++q) {
+      if (!S->bslot_batch[(size_t)q] || S->bslot_ticket[(size_t)q] <= 0 || !S->bslot_finished[(size_t)q]) continue;
+      if (S->pool_free[p].empty()) {
+        left = true;
+        break;
+      }
+      const int b = S->pool_free[p].back();
+      S->pool_free[p].pop_back();
+      idx[(size_t)q] = b;
+      took.emplace_back(q, b);
     }
   }
+  if (!left) S->bpend = false;
   if (took.empty()) return GBO_OK;
   cudaStream_t st = S->s[0];
-  GBO_CUDA_TRY(cudaMemcpyAsync(S->d_bufidx, idx.data(), sizeof(int) * (size_t)ncols, cudaMemcpyHostToDevice, st));
-  k_bfs_retire_batch<<<blocks_for(S->n, kRetRows), 256, 0, st>>>(S->levels, S->n, ncols / 8, lvl0, S->d_bufidx,
-                                                                  reinterpret_cast<uint8_t*>(S->dpool[0]),
-                                                                  S->dbytes[0]);
-  S->launches++;
+  GBO_CUDA_TRY(cudaMemcpyAsync(S->d_bufidx, idx.data(), sizeof(int) * (size_t)width, cudaMemcpyHostToDevice, st));
+  const unsigned grid = blocks_for(S->n, kRetRows);
+  if (p == 0) {
+    k_bfs_retire_batch<uint8_t, kBatchCols><<<grid, 256, 0, st>>>(S->blevels, S->n, width, 0, width, S->blvl0,
+                                                                  S->d_bufidx, S->dpool[0], S->dbytes[0]);
+    S->launches++;
+  } else {
+    for (int c0 = 0; c0 < width; c0 += 256) {
+      k_bfs_retire_batch<int, 256><<<grid, 256, 0, st>>>(S->blevels, S->n, width, c0, std::min(256, width - c0),
+                                                         S->blvl0, S->d_bufidx, S->dpool[1], S->dbytes[1]);
+      S->launches++;
+    }
+  }
   GBO_CUDA_TRY(cudaGetLastError());
-  for (auto& t : took) GBO_CUDA_TRY(cudaEventRecord(S->pool_ev[0][(size_t)t.second], st));
+  for (auto& t : took) GBO_CUDA_TRY(cudaEventRecord(S->pool_ev[p][(size_t)t.second], st));
   const double t_now = now_ms();
   std::lock_guard<std::mutex> lk(S->mu);
   for (auto& t : took) {
@@ -654,13 +699,13 @@ int retire_batch(gbo_server* S, const std::vector<std::pair<int, gbo::Query>>& a
     const long long tk = S->bslot_ticket[(size_t)q];
     Result r;
     r.kind = 0;
-    r.pool = 0;
+    r.pool = p;
     r.buf = t.second;
-    r.u8 = 1;
-    r.ev = S->pool_ev[0][(size_t)t.second];
+    r.u8 = p == 0;
+    r.ev = S->pool_ev[p][(size_t)t.second];
     r.t_submit = S->submit_time[tk];
     r.t_done = t_now;
-    r.iters = depth;
+    r.iters = S->bdepth;
     S->results[tk] = r;
     S->bslot_ticket[(size_t)q] = 0;
     S->bslot_finished[(size_t)q] = 0;
@@ -670,18 +715,18 @@ int retire_batch(gbo_server* S, const std::vector<std::pair<int, gbo::Query>>& a
   return GBO_OK;
 }
 
-// Batch mode: the admitted queries (the engine was idle, so their slots are
-// the only ones occupied) as one multi-source BFS over every slot column,
-// empty columns with no source.  Levels land in the server's level store as
-// absolute levels from the current level on, so retirement reads them as
-// for a round-by-round query, and the level counter moves past the batch.
+// Batch mode: the admitted queries (the engine was idle, so admission took
+// the lowest slots) as one multi-source BFS of the narrowest width that holds
+// them, empty columns with no source, into the batch level store (vertex-
+// major, apart from the round-by-round engine's).  Every query finishes
+// here; the level counter moves past the batch (with the frontier parity
+// kept for the round-by-round engine).
 int bfs_batch(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
-  // the engine was idle, so admission took the lowest slots: columns
-  // 0 .. top of the batch, in whole words rounded up to a power of two
   int top = 0;
   for (auto& q : adm) top = std::max(top, q.first + 1);
   int w = 1, wi = 0;
   while (w * 32 < top) w <<= 1, ++wi;
+  if (!S->blevels) GBO_CUDA_TRY(cudaMalloc(&S->blevels, sizeof(int) * (size_t)S->n * S->kb + 16));
   if (!S->msb[wi]) S->msb[wi] = ms_batch_create(S->live);
   std::vector<int> src((size_t)w * 32, -1);
   for (auto& q : adm) {
@@ -691,15 +736,19 @@ int bfs_batch(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
   const int lvl0 = S->level;
   int depth = 0;
   long long nl = 0;
-  GBO_TRY(ms_batch_run(S->g, S->msb[wi], src.data(), w * 32, S->levels, 32, lvl0, &depth, &nl, S->s[0]));
+  GBO_TRY(ms_batch_run(S->g, S->msb[wi], src.data(), w * 32, S->blevels, 0, lvl0, &depth, &nl, S->s[0]));
   S->launches += nl;
   S->level = lvl0 + depth;
   S->parity_fix = (S->parity_fix != ((depth & 1) != 0));
-  if (depth < 255) GBO_TRY(retire_batch(S, adm, w * 32, lvl0, depth));
-  std::lock_guard<std::mutex> lk(S->mu);
-  for (auto& q : adm)
-    if (S->bslot_ticket[(size_t)q.first] > 0) S->bslot_finished[(size_t)q.first] = 1;
-  return GBO_OK;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    for (auto& q : adm) S->bslot_finished[(size_t)q.first] = 1;
+    S->bpend = true;
+    S->blvl0 = lvl0;
+    S->bdepth = depth;
+    S->bwidth = w * 32;
+  }
+  return retire_batch(S);
 }
 
 int ppr_round(gbo_server* S, std::vector<std::pair<int, gbo::Query>>& adm) {
@@ -774,8 +823,8 @@ int retire(gbo_server* S, int kind) {
   {
     std::lock_guard<std::mutex> lk(S->mu);
     for (size_t q = 0; q < tick.size(); ++q) {
-      if (tick[q] <= 0 || !fin[q]) continue;
-      const int p = kind == 0 && S->level - S->bslot_start[q] < 255 ? 0 : 1;
+      if (tick[q] <= 0 || !fin[q] || (kind == 0 && S->bslot_batch[q])) continue;  // batches: retire_batch
+      const int p = kind == 0 ? bfs_slot_pool(S, (int)q) : 1;
       if (rl[p].count >= kRetire || S->pool_free[p].empty()) continue;
       const int b = S->pool_free[p].back();
       S->pool_free[p].pop_back();
@@ -843,7 +892,7 @@ int blocked_pool(gbo_server* S, int kind) {
   const std::vector<char>& fin = kind == 0 ? S->bslot_finished : S->pslot_finished;
   for (size_t q = 0; q < tab.size(); ++q) {
     if (tab[q] <= 0 || !fin[q]) continue;
-    const int p = kind == 0 && S->level - S->bslot_start[q] < 255 ? 0 : 1;
+    const int p = kind == 0 ? bfs_slot_pool(S, (int)q) : 1;
     if (S->pool_free[p].empty()) return p;
   }
   return -1;
@@ -1005,6 +1054,7 @@ void worker_main(gbo_server* S, int kind) {
     }
     const double t1 = now_ms();
     if (st == GBO_OK) st = retire(S, kind);
+    if (st == GBO_OK && kind == 0) st = retire_batch(S);
     const double t2 = now_ms();
     if (st != GBO_OK) {
       failw(st);
@@ -1047,6 +1097,7 @@ void destroy_server(gbo_server* S) {
   cudaFree(S->d_adm_src);
   cudaFree(S->d_adm_slot);
   cudaFree(S->d_bufidx);
+  cudaFree(S->blevels);
   cudaFree(S->X);
   cudaFree(S->P);
   cudaFree(S->err);
@@ -1166,7 +1217,9 @@ extern "C" int gbo_server_create(const gbo_graph* gc, int bfs_slots, int ppr_slo
     S->pslot_finished.assign((size_t)kPprSlots, 0);
     // device result pools: every slot can hold a finished result plus two
     // rounds of retirements waiting for their clients
-    const int nbuf[2] = {S->kb > 0 ? S->kb + 2 * kRetire : 0, (ppr_slots ? kPprSlots : 0) + 2 * kRetire};
+    // (BFS: a whole batch's results can wait for their clients while the
+    // next batch runs)
+    const int nbuf[2] = {S->kb > 0 ? 2 * S->kb + 2 * kRetire : 0, (ppr_slots ? kPprSlots : 0) + 2 * kRetire};
     S->dbytes[0] = (n + 255) / 256 * 256;
     S->dbytes[1] = (sizeof(int) * n + 255) / 256 * 256;
     for (int p = 0; p < 2; ++p) {
