@@ -17,6 +17,12 @@ from __future__ import annotations
 import argparse
 import json
 import os
+
+# The query server's clients deliver results on streams of their own beside
+# the engine's: with CUDA's default 8 hardware queues, 14 client streams
+# share queues with the engine, and a client's small copy kernel waits behind
+# a whole traversal graph queued ahead of it.  Set before CUDA starts.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 import subprocess
 import sys
 import time
@@ -50,11 +56,12 @@ def parse():
     ap.add_argument("--nvtx", action="store_true", help="NVTX range 'timed' around the suites' timed loops")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving streams")
     ap.add_argument("--no-permuted", action="store_true", help="skip the degree-ordered variant")
-    ap.add_argument("--serve-qps", type=float, default=8000.0, help="offered BFS query rate")
+    ap.add_argument("--serve-qps", type=float, default=16000.0, help="offered BFS query rate")
     ap.add_argument("--serve-s", type=float, default=1.5, help="seconds of arrivals per stream")
-    ap.add_argument("--serve-slots", type=int, default=256, help="BFS slots of the served streams' server")
-    ap.add_argument("--serve-admit", type=float, default=None,
-                    help="server BFS admission batching (free-slot fraction; default: the library's)")
+    ap.add_argument("--serve-slots", type=int, default=1024, help="BFS slots of the served streams' server")
+    ap.add_argument("--serve-admit", type=float, default=1.0,
+                    help="server BFS admission (free-slot fraction; 1: batch mode, each batch one "
+                         "multi-source BFS)")
     ap.add_argument("--tc-graphs", default="mesh,rmat", help="graphs of --workload tc (mesh, rmat)")
     ap.add_argument("--tc-variants", default="input,degree", help="vertex orders of --workload tc")
     ap.add_argument("--tc-tiles", default="8,16,32,64", help="tile widths of --workload tc")

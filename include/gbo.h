@@ -503,9 +503,17 @@ GBO_API int gbo_server_set_queue_limit(gbo_server* s, long long max_pending);
 /* BFS admission batching: pending BFS queries enter the engine when at
  * least ceil(min_free_fraction * bfs_slots) slots are free, or when no
  * admitted query is still traversing.  0 admits into any free slot every
- * round; 1 admits only into an idle engine (batch after batch); values in
- * between trade a little latency for fewer rounds in which freshly admitted
- * sources keep every row of the graph open.  Default 0.5. */
+ * round; values below 1 trade a little latency for fewer rounds in which
+ * freshly admitted sources keep every row of the graph open.  1 is batch
+ * mode: queries enter only an idle engine whose results have all retired,
+ * and each batch runs as one multi-source BFS (level 0 pushed from the
+ * sources, finished columns retired, the narrowest frontier width that
+ * holds the batch) into a level store of its own, then retires in one pass;
+ * iterations then report the batch's depth.  Batch mode has the highest
+ * capacity; clients that take results with gbo_server_wait_device on
+ * streams of their own want more hardware queues than CUDA's default 8
+ * (CUDA_DEVICE_MAX_CONNECTIONS=32 in the environment before CUDA starts),
+ * or their copies queue behind the engine's traversal.  Default 0.5. */
 GBO_API int gbo_server_set_admission(gbo_server* s, float min_free_fraction);
 GBO_API int gbo_server_submit_bfs(gbo_server* s, int src, int64_t* ticket);
 GBO_API int gbo_server_submit_ppr(gbo_server* s, const int* verts,
