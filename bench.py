@@ -558,7 +558,8 @@ def serve_stream(gbo, g, n, rate_qps, duration_s, ppr_frac, seed, delivery="host
         st = {k: st[k] - st0[k] if k not in ("pending", "in_flight") else st[k] for k in st}
     srv.close()
     span = max(done_t) - first_arrival if done_t else float("nan")
-    out = {"offered_qps": rate_qps, "queries": nq, "delivery": delivery, "bfs_slots": slots, "qps": len(done_t) / span,
+    out = {"offered_qps": rate_qps, "queries": nq, "delivery": delivery, "bfs_slots": slots,
+           "admission": "batch mode (warmed)" if st0 is not None else admit, "qps": len(done_t) / span,
            "span_s": span, "rounds": st["rounds"], "kernel_launches": st["kernel_launches"],
            "phase_ms": {k: round(st[k], 1) for k in ("bfs_round_ms", "ppr_round_ms", "retire_ms", "copy_ms",
                                                      "copy_wait_ms", "copy_d2h_ms", "copy_widen_ms")}}

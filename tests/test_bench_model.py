@@ -128,3 +128,65 @@ def test_bfs_push_bytes_rws_matches_direct_count(gbo, orc):
                 tail = max(0, len(blocks) - head)
                 by += 16 + 8 * head + 8 * tail + (16 if tail > long_tail else 0)
             assert got == by, (head, L)
+
+
+@pytest.mark.parametrize("slots", [32, 64, 256, 1024])
+def test_warm_server_runs_one_batch_per_frontier_width(slots):
+    """bench.warm_server submits batches of 1, 33, 65, ... queries, each
+    collected before the next, so that a batch-mode server has run one batch
+    at every frontier width (32, 64, ... slots columns) before a stream."""
+    class FakeLib:
+        def __init__(self):
+            self.waited = []
+
+        def gbo_server_wait(self, h, t, out, lat, it, timeout):
+            self.waited.append(t)
+            return 0
+
+    class FakeGbo:
+        def __init__(self):
+            self._lib = FakeLib()
+
+        def lib(self):
+            return self._lib
+
+        @staticmethod
+        def check(st, what):
+            assert st == 0, what
+
+    class FakeServer:
+        h = None
+
+        def __init__(self):
+            self.batches, self.next = [], 1
+
+        def submit_bfs(self, src):
+            self.batches[-1].append(self.next)
+            self.next += 1
+            return self.next - 1
+
+    fg, srv = FakeGbo(), FakeServer()
+    orig = srv.submit_bfs
+    sizes = []
+
+    def submit(src):
+        if not sizes or len(fg.lib().waited) == sum(sizes):
+            sizes.append(0)
+            srv.batches.append([])
+        sizes[-1] += 1
+        return orig(src)
+
+    srv.submit_bfs = submit
+    bench.warm_server(fg, srv, 1000, slots, 0)
+    widths = set()
+    for m in sizes:
+        w = 32
+        while w < m:
+            w *= 2
+        widths.add(w)
+    want, w = set(), 32
+    while w <= slots:
+        want.add(w)
+        w *= 2
+    assert widths == want, (sizes, widths)
+    assert fg.lib().waited == list(range(1, sum(sizes) + 1))
