@@ -32,6 +32,9 @@ def test_injected_host_allocation_failure_in_readers(gbo, tmp_path):
 
 
 def test_injection_arguments(gbo):
+    for what in (gbo.INJECT_HOST_ALLOC, gbo.INJECT_REPLAY_CAP, gbo.INJECT_SERVER_HOLD, gbo.INJECT_BARRIER_SKIP):
+        assert gbo.lib().gbo_debug_inject(what, 1) == gbo.GBO_OK  # arming and disarming touch no GPU
+        assert gbo.lib().gbo_debug_inject(what, 0) == gbo.GBO_OK
     assert gbo.lib().gbo_debug_inject(99, 1) == gbo.GBO_ERR_INVALID
     assert gbo.lib().gbo_debug_inject(gbo.INJECT_REPLAY_CAP, -1) == gbo.GBO_ERR_INVALID
     assert gbo.lib().gbo_status_string(gbo.GBO_ERR_FULL) == b"GBO_ERR_FULL"
